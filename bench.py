@@ -1,0 +1,303 @@
+#!/usr/bin/env python
+"""Throughput of the FIT-TD step on the plain-method-at-scale workload.
+
+One step = one full leapfrog step of the brick-box workload
+(:func:`magnelio_b200.workloads.brick_box`): E update with the CPML psi
+recursion on six 10-layer slabs, the lumped gap source, H update with its
+CPML part, and three 64-frequency running-DFT E-field monitors on the
+mid-planes, for one field set of ``size^3`` cells.  The metric is
+Gcell-updates/s = cells x steps / device time (CUDA events on the engine's
+stream), summed over GPUs.  Multi-GPU runs are independent replicas (one
+problem per GPU, no exchange), timed as the max over ranks.
+
+``--impl reference`` times the CPU port of the reference's algorithm
+(``oracle/``) on the host cores instead, on a bounded sample of steps of the
+same workload.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+if str(ROOT) not in sys.path:
+    sys.path.insert(0, str(ROOT))
+
+METRIC = "Gcell-updates/s"
+BYTES_PER_CELL = 96  # E(3) H(3) read+write, alpha/beta E/H (12) read, float32
+BYTES_PER_CPML_CELL = 32  # 2 psi_E + 2 psi_H read+write per slab cell per face, float32
+
+
+def _peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def _traffic(kernel_key: str, n: int):
+    """DRAM bytes per cell from a committed ncu summary, if one exists."""
+    p = ROOT / "profiles" / "traffic.json"
+    if not p.exists():
+        return None
+    d = json.loads(p.read_text())
+    v = d.get(kernel_key)
+    return None if v is None else float(v) * n**3
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, local_rank: int):
+        vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+        idx = vis.split(",")[local_rank] if vis else str(local_rank)
+        self.proc = None
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={idx}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        sm, smax, reasons = [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for line in out.strip().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def _dist():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def _max_over_ranks(x: float, world: int, local: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def cpu_threads() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:  # pragma: no cover
+        return os.cpu_count() or 1
+
+
+def cpu_port_rate(prob, budget_s: float = 20.0, max_steps: int = 200, warmup: int = 2):
+    """Gcell-updates/s of the CPU port of the reference's step (C + OpenMP
+    on every host thread, float32 as the reference's default precision) on
+    the full-size workload: whole steps, timed until ``budget_s`` elapses."""
+    from oracle.cport import CPortRun
+
+    threads = cpu_threads()
+    os.environ.setdefault("OMP_NUM_THREADS", str(threads))
+    run = CPortRun(prob, "single", max_steps + warmup + 1)
+    run.run(warmup)
+    n = 0
+    t0 = time.perf_counter()
+    while n < max_steps:
+        run.run(1)
+        n += 1
+        if time.perf_counter() - t0 > budget_s:
+            break
+    dt = time.perf_counter() - t0
+    cells = prob.nx * prob.ny * prob.nz
+    return cells * n / dt / 1e9, n, dt, threads
+
+
+def run_reference(args, world, rank, local):
+    if rank != 0:
+        return 0
+    from magnelio_b200 import workloads
+
+    prob = workloads.brick_box(args.size, steps=args.steps + args.warmup + 8)
+    budget = min(args.cpu_budget * 6, 120.0)
+    rate, n, secs, threads = cpu_port_rate(prob, budget_s=budget, max_steps=max(args.steps, 1), warmup=min(args.warmup, 3))
+    line = {
+        "impl": "reference", "metric": METRIC, "value": rate, "unit": METRIC, "n_gpus": world,
+        "steps": n, "warmup": min(args.warmup, 3), "ms_per_step": secs / n * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded brick box)",
+        "config": _config(args, prob),
+        "cpu_baseline": {"value": rate, "unit": METRIC, "cores": threads, "kind": "port",
+                         "sample": f"{n} full steps of the {args.size}^3 workload (of {args.steps} asked, "
+                                   f"bounded to {budget:.0f} s) after {min(args.warmup, 3)} warm-up steps; "
+                                   f"C+OpenMP port, float32, {threads} threads"},
+        "e2e": {"value": rate, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def _config(args, prob):
+    from magnelio_b200 import workloads
+
+    return {
+        "workload": f"brick_box_{args.size}",
+        "grid": f"{prob.nx}x{prob.ny}x{prob.nz} non-uniform (0.8-1.2 mm, centre-graded)",
+        "bricks": "32 dielectric, eps_r U[1,10], cat-1 conformal fill U[0,1]",
+        "cpml": f"10 layers x 6 faces ({workloads.cells_in_cpml(prob)} slab cells)",
+        "source": "lumped z gap, 50 ohm, modulated Gaussian 1-7.5 GHz",
+        "monitors": "3 mid-plane E-field DFT monitors x 64 freq, every step",
+        "field_sets": 1,
+        "parallelism": "replicas" if args.gpus > 1 else "single",
+        "l2": "inputs larger than L2 (working set >1 GB per GPU)",
+    }
+
+
+def main() -> int:
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", choices=("b200", "reference"), default="b200")
+    ap.add_argument("--size", type=int, default=256)
+    ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of CPU-port timing")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+    world, rank, local = _dist()
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    try:
+        if args.impl == "reference":
+            return run_reference(args, world, rank, local)
+        return run_b200(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+
+
+def run_b200(args, world, rank, local):
+    from magnelio_b200 import workloads
+
+    n = args.size
+    total = args.warmup + 2 * args.steps + 64
+    prob = workloads.brick_box(n, steps=total)
+    eng = prob.build_engine("single", device=local)
+    cells = n**3
+    # warm-up (graph capture, clocks)
+    eng.step(args.warmup)
+    eng.sync()
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+    sampler = ClockSampler(local)
+    l0 = eng.launch_count
+    ms = eng.step_timed(args.steps)
+    launches = eng.launch_count - l0
+    clocks = sampler.stop()
+    ms = _max_over_ranks(ms, world, local)
+    value = cells * args.steps * world / (ms * 1e-3) / 1e9
+
+    # end to end through the public API: every step streams its source
+    # sample host->device from pinned memory and reads its recorded V/I back
+    import torch
+
+    pinned = torch.empty(args.steps, dtype=torch.float64, pin_memory=True)
+    base = eng.steps_done
+    pinned.copy_(torch.from_numpy(np.ascontiguousarray(prob.lumped[0].v_src[0][base:base + args.steps])))
+    stride = pinned.element_size()
+    eng.sync()
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+    t0 = time.perf_counter()
+    vi = []
+    for s in range(args.steps):
+        eng.push_lumped_samples(0, 0, base + s, 1, pinned.data_ptr() + s * stride)
+        eng.step(1)
+        vi.append(eng.read_vi(0, base + s, 1))
+    e2e_s = _max_over_ranks(time.perf_counter() - t0, world, local)
+    e2e = cells * args.steps * world / e2e_s / 1e9
+    nch = eng.n_channels
+
+    # stencil roofline: E and H updates timed alone (advances the fields,
+    # after all measured runs)
+    t_e, t_h = eng.time_stencil(20)
+    t_pair = t_e + t_h
+    cpml_cells = workloads.cells_in_cpml(prob)
+    alg_bytes = BYTES_PER_CELL * cells + BYTES_PER_CPML_CELL * cpml_cells
+    achieved = alg_bytes / (t_pair * 1e-3) / 1e9
+    peak, peak_kind = _peaks()
+    traffic = _traffic("update_E+update_H", n)
+    roofline = {"bound": "hbm", "kernel": "update_E + update_H (one stencil step)", "achieved": achieved,
+                "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": traffic, "algorithmic_bytes": alg_bytes, "ms_E": t_e, "ms_H": t_h,
+                "step_share": t_pair / (ms / args.steps)}
+    eng.close()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        rate, ns, secs, threads = cpu_port_rate(prob, budget_s=args.cpu_budget)
+        cpu = {"value": rate, "unit": METRIC, "cores": threads, "kind": "port",
+               "sample": f"{ns} full steps of the {n}^3 workload after 2 warm-up steps "
+                         f"(C+OpenMP port, float32, {threads} threads, {secs:.1f} s)"}
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded brick box, host-built coefficients)",
+            "config": _config(args, prob), "roofline": roofline, "cpu_baseline": cpu,
+            "e2e": {"value": e2e, "unit": METRIC, "h2d_bytes_per_step": 8, "d2h_bytes_per_step": 16 * nch,
+                    "how": "per step: pinned H2D of the source sample, one fitb_step, D2H of the step's V/I"},
+            "gpu_launches": launches, "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,227 @@
+/*
+ * fitb200.h -- C ABI of the B200-native FIT-TD (Yee leapfrog) time-stepping
+ * engine behind Magnelio's FITTimeDomainSolver.
+ *
+ * Conventions
+ *   - Every function returns an int status: FITB_OK (0) or a negative
+ *     FITB_ERR_* code.  fitb_last_error() returns the message of the most
+ *     recent failure on the calling thread.
+ *   - Host pointers are borrowed for the duration of the call only.  All
+ *     device memory is owned by the handle and released by fitb_destroy().
+ *   - Array layouts are the reference's: the flat E vector is
+ *     [Ex | Ey | Ez] with Ex (Nx, Ny+1, Nz+1), Ey (Nx+1, Ny, Nz+1),
+ *     Ez (Nx+1, Ny+1, Nz); the flat H vector is [Hx | Hy | Hz] with
+ *     Hx (Nx+1, Ny, Nz), Hy (Nx, Ny+1, Nz), Hz (Nx, Ny, Nz+1); C order,
+ *     k (z) fastest  (reference: src/magnelio/_fields/field_arrays.py:1-17).
+ *   - Field buffers passed by the caller have the handle's precision
+ *     (float32 when precision == 4, float64 when precision == 8).
+ *     Setup constants (coefficients, profiles, CPML tables, waveform
+ *     samples) are passed as float64 and rounded once on upload, as the
+ *     reference builds them in float64 and casts
+ *     (reference: src/magnelio/solver/fit_td.py:468-479).
+ *   - One CUDA stream per handle; calls on one handle are not thread-safe.
+ *   - A handle carries B field sets ("batch") that share one coefficient set;
+ *     every per-field-set argument takes the field-set index b in [0, B).
+ */
+#ifndef FITB200_H
+#define FITB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FITB_ABI_VERSION 1
+
+#define FITB_OK 0
+#define FITB_ERR_ARG (-1)      /* invalid argument / size mismatch          */
+#define FITB_ERR_CUDA (-2)     /* CUDA runtime error                         */
+#define FITB_ERR_STATE (-3)    /* call not valid in the handle's state      */
+#define FITB_ERR_NOMEM (-4)    /* device allocation failed                   */
+#define FITB_ERR_NODEV (-5)    /* no usable CUDA device                      */
+#define FITB_ERR_LIMIT (-6)    /* a fixed capacity of the engine exceeded    */
+
+typedef struct fitb_handle fitb_handle;
+
+/* Grid and run description.  Replaces the mesh / dt / precision fields of
+ * FITTimeDomainSolver (reference: src/magnelio/solver/fit_td.py:174-234,
+ * setup at :302-324). */
+typedef struct fitb_desc {
+    int32_t nx, ny, nz;   /* cell counts                                    */
+    int32_t batch;        /* field sets sharing the coefficients (>= 1)     */
+    int32_t precision;    /* 4 = float32 fields, 8 = float64 fields         */
+    int32_t device;       /* CUDA device ordinal                            */
+    double dt;            /* time step [s]                                  */
+} fitb_desc;
+
+/* Modal (waveguide) port.  Mirrors PortOperatorModal's per-step data
+ * (reference: src/magnelio/ports/_modal/operator.py:510-640 constructor,
+ * :1351-1536 update_e, :1253-1321 projections).  All index arrays are flat
+ * indices into the reference E or H vector.  The interior plane has the
+ * same (u, v) sample counts as the port plane. */
+typedef struct fitb_modal_desc {
+    int32_t n_modes;
+    int32_t n_e_u, n_e_v;        /* port-plane E samples, u then v           */
+    int32_t n_h_u, n_h_v;        /* port-plane dual-edge H samples           */
+    const int64_t* port_e_idx;   /* [n_e_u + n_e_v]   plane.e_u/e_v_indices   */
+    const int64_t* int_e_idx;    /* [n_e_u + n_e_v]   interior plane indices  */
+    const int64_t* port_h_idx;   /* [n_h_u + n_h_v]   plane.h_u/h_v_indices   */
+    const double* me_port;       /* [n_e_u + n_e_v]   M_eps at port plane     */
+    const double* me_int;        /* [n_e_u + n_e_v]   M_eps at interior plane */
+    const double* mh_port;       /* [n_h_u + n_h_v]   M_mu at port dual edges */
+    const double* e_profile;     /* [n_modes][n_e]    reconstruction profile  */
+    const double* v_profile;     /* [n_modes][n_e]    projection profile (dual basis, or primal) */
+    const double* h_profile;     /* [n_modes][n_h]    current profile         */
+    const double* mur_r;         /* [n_modes]                                 */
+    const double* tau;           /* [n_modes]  TF/SF delay tau_m [s]          */
+    const double* record_scale;  /* [n_modes]                                 */
+    const int32_t* is_dtbc;      /* [n_modes]  1: exact DTBC, 0: modal Mur    */
+    const double* dtbc_r;        /* [n_modes]                                 */
+    const double* dtbc_q;        /* [n_modes]                                 */
+    int32_t dtbc_n_kernel_init;  /* initial kernel length (power of two)      */
+    int32_t has_complement;      /* complement absorber configured            */
+    const double* comp_r;        /* [n_e] per-edge Mur coefficient            */
+    const double* comp_live;     /* [n_e] 0/1 live mask                       */
+    int64_t max_steps;           /* history capacity in steps                 */
+} fitb_modal_desc;
+
+/* Running-DFT field monitor over a cell box (reference:
+ * src/magnelio/monitors/field_frequency.py:249-294 record,
+ * src/magnelio/monitors/base.py:51-168 cell-centre interpolation,
+ * src/magnelio/monitors/_dft.py:37-52 accumulate). */
+typedef struct fitb_dft_desc {
+    int32_t i0, i1, j0, j1, k0, k1;  /* cell-index box, stop-exclusive      */
+    int32_t comp_mask;               /* bit c set = record component c,
+                                        c = 0..5 for Ex,Ey,Ez,Hx,Hy,Hz      */
+    int32_t n_freq;
+    const double* freqs;             /* [n_freq] Hz                          */
+    int32_t stride;                  /* record every stride-th step (>= 1)   */
+    int32_t kahan;                   /* 1: compensated float32 bins          */
+    const double* dx;                /* [nx] primal widths                   */
+    const double* dy;                /* [ny]                                 */
+    const double* dz;                /* [nz]                                 */
+} fitb_dft_desc;
+
+/* ---- lifetime ------------------------------------------------------- */
+int fitb_abi_version(void);
+/* Replaces FITTimeDomainSolver.setup() allocation (fit_td.py:302-324). */
+int fitb_create(const fitb_desc* desc, fitb_handle** out);
+int fitb_destroy(fitb_handle* h);
+int fitb_last_error(char* buf, size_t len);
+/* Number of this library's kernel launches issued so far on the handle. */
+int fitb_launch_count(const fitb_handle* h, int64_t* out);
+
+/* ---- coefficients and fields ---------------------------------------- */
+/* alpha/beta of the leapfrog update and the mass diagonals for the energy
+ * check (fit_td.py:383-514).  Lengths n_E and n_H of the reference flat
+ * layout.  m_eps / m_mu may be NULL (energy then reports 0). */
+int fitb_set_coeffs(fitb_handle* h, const double* alpha_e, const double* beta_e,
+                    const double* alpha_h, const double* beta_h,
+                    const double* m_eps, const double* m_mu);
+/* Same, with the arrays already in the field dtype (float32 / float64):
+ * the reference casts its float64 build to the field dtype before the
+ * march (fit_td.py:468-479), so its cast arrays upload as they are. */
+int fitb_set_coeffs_native(fitb_handle* h, const void* alpha_e, const void* beta_e,
+                           const void* alpha_h, const void* beta_h,
+                           const void* m_eps, const void* m_mu);
+/* FieldState e_flat / h_flat of field set b (field_arrays.py:98-106). */
+int fitb_set_fields(fitb_handle* h, int32_t b, const void* e, size_t e_bytes,
+                    const void* hf, size_t h_bytes);
+int fitb_read_fields(fitb_handle* h, int32_t b, void* e, size_t e_bytes,
+                     void* hf, size_t h_bytes);
+
+/* ---- boundaries ----------------------------------------------------- */
+/* CFS-PML face (reference: src/magnelio/boundaries/cpml.py:92-195
+ * initialize, :213-310 set_pec_mask, :343-516 update_E/update_H).
+ * face: 0..5 = xmin,xmax,ymin,ymax,zmin,zmax.  b/c/ck: per-layer tables of
+ * length n_pml.  air_*: 0/1 masks in the reference psi shapes
+ * (e.g. z face: psi_Ex (Nx,Ny+1,n), psi_Ey (Nx+1,Ny,n), psi_Hx (Nx+1,Ny,n),
+ * psi_Hy (Nx,Ny+1,n)); NULL = all ones. */
+int fitb_add_cpml(fitb_handle* h, int32_t face, int32_t n_pml,
+                  const double* b, const double* c, const double* ck,
+                  const uint8_t* air_e1, const uint8_t* air_e2,
+                  const uint8_t* air_h1, const uint8_t* air_h2);
+
+/* ---- lumped ports --------------------------------------------------- */
+/* Thevenin lumped element with a series R-L-C companion (reference:
+ * src/magnelio/ports/_lumped/operator.py:134-166 update_e,
+ * src/magnelio/circuit/companion.py SeriesRLC).  r, l, c < 0 = absent. */
+int fitb_add_lumped(fitb_handle* h, int32_t n_edges, const int64_t* flat_e_idx,
+                    const double* signs, const double* betas,
+                    double r, double l, double c, double record_scale,
+                    int32_t* out_id);
+/* Source voltage samples v_src[n] = waveform((n+1)*dt) for steps
+ * n = 0..n_samples-1 (zero beyond). */
+int fitb_set_lumped_source(fitb_handle* h, int32_t id, int32_t b,
+                           int64_t n_samples, const double* v_src);
+
+/* Stream source samples into an existing table: v_src[step0 .. step0+n) of
+ * field set b is overwritten by an asynchronous copy, on the handle's
+ * stream, from `host` (which should be pinned memory and must stay valid
+ * until the next fitb_sync / fitb_read_* call).  For co-simulation, where
+ * the next step's source voltage is produced on the host while the device
+ * steps.  The table must already be long enough (fitb_set_lumped_source). */
+int fitb_push_lumped_samples(fitb_handle* h, int32_t id, int32_t b, int64_t step0,
+                             int64_t n, const double* host);
+
+/* ---- modal ports ---------------------------------------------------- */
+int fitb_add_modal_port(fitb_handle* h, const fitb_modal_desc* d, int32_t* out_id);
+/* DTBC convolution kernel l_m (m = 0..n_kernel-1) of mode `mode` for the
+ * table length n_kernel (reference: src/magnelio/ports/_modal/dtbc.py:125-156,
+ * auto-extension :351-363).  One call per power-of-two length. */
+int fitb_set_dtbc_kernel(fitb_handle* h, int32_t port, int32_t mode,
+                         int32_t n_kernel, const double* l);
+/* Excite mode `mode` of field set b with waveform samples
+ * w[n] = waveform(n*dt), n = 0..n_samples-1 (zero beyond); mode = -1 clears
+ * (operator.py:1140-1182 set_excitation / clear_excitation). */
+int fitb_set_modal_source(fitb_handle* h, int32_t port, int32_t b, int32_t mode,
+                          int64_t n_samples, const double* w);
+
+/* ---- monitors ------------------------------------------------------- */
+int fitb_add_dft_monitor(fitb_handle* h, const fitb_dft_desc* d, int32_t* out_id);
+/* Complex bins of monitor `mon`, field set b, component c (0..5), shape
+ * (n_freq, ni, nj, nk); re / im arrays of that many doubles. */
+int fitb_read_dft(fitb_handle* h, int32_t mon, int32_t b, int32_t comp,
+                  double* re, double* im, size_t count);
+
+/* ---- time stepping -------------------------------------------------- */
+/* Advance all field sets by n_steps leapfrog steps (the body of the loop
+ * at fit_td.py:950-1007), replaying captured CUDA graphs. */
+int fitb_step(fitb_handle* h, int64_t n_steps);
+int fitb_sync(fitb_handle* h);
+/* fitb_step bracketed by CUDA events on the handle's stream; blocks until
+ * the steps are done and returns their device time in milliseconds. */
+int fitb_step_timed(fitb_handle* h, int64_t n_steps, double* ms);
+/* Measurement helper: device time of n_iter back-to-back launches of the E
+ * update alone and of the H update alone (ms per launch).  It advances the
+ * fields like n_iter half steps each, so call it only after the run whose
+ * results are wanted. */
+int fitb_time_stencil(fitb_handle* h, int32_t n_iter, double* ms_e, double* ms_h);
+int fitb_steps_done(fitb_handle* h, int64_t* out);
+/* 0.5 * (sum M_eps e^2 + sum M_mu h^2), float64 accumulation
+ * (fit_td.py:1014-1018). */
+int fitb_energy(fitb_handle* h, int32_t b, double* out);
+/* max |V| * record_scale over all modal ports of field set b since the last
+ * poll, then reset (operator.py:1323-1334 poll_signal_absmax). */
+int fitb_poll_signal_absmax(fitb_handle* h, int32_t b, double* out);
+/* Recorded V/I per channel for steps [step0, step0 + n): channel order is
+ * port registration order, modes within a port (lumped ports: one channel).
+ * V and I are [n][n_channels] (reference: src/magnelio/ports/recorder.py
+ * :216-285). */
+int fitb_channel_count(fitb_handle* h, int32_t* out);
+int fitb_read_vi(fitb_handle* h, int32_t b, int64_t step0, int64_t n,
+                 double* V, double* I);
+
+/* ---- checkpoint ----------------------------------------------------- */
+/* Byte size of the full evolving state (fields, psi, port and monitor
+ * state, step count) and its export / import (fit_td.py:1264-1353). */
+int fitb_state_size(fitb_handle* h, size_t* out);
+int fitb_state_export(fitb_handle* h, void* buf, size_t len);
+int fitb_state_import(fitb_handle* h, const void* buf, size_t len);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FITB200_H */

@@ -1,0 +1,225 @@
+"""Bridge from a set-up Magnelio ``FITTimeDomainSolver`` to a
+:class:`~magnelio_b200.problem.FitProblem`.
+
+``problem_from_solver`` reads the host-built constants the reference's own
+``setup()`` produced (``src/magnelio/solver/fit_td.py:302-631``): the
+leapfrog coefficients, the mass diagonals, the CPML tables and air masks,
+the modal / lumped port operators and the field monitors.  The engine then
+owns all evolving state on the device.  Supported per-step hooks are the
+ones on the FIT-TD hot path: PEC / PMC / CPML boundaries, modal
+(Mur / DTBC / complement absorber) and series-RLC lumped ports, running-DFT
+field monitors.  Anything else raises ``NotImplementedError`` instead of
+being silently skipped.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+
+from magnelio_b200 import host
+from magnelio_b200.problem import CpmlFace, DftMonitor, FitProblem, LumpedPort, ModalPort
+
+_FACE_EDGES = {
+    # tangential E components zeroed by PECBoundary.apply (pec.py:51-78)
+    "xmin": (("Ey", 0, 0), ("Ez", 0, 0)),
+    "xmax": (("Ey", 0, -1), ("Ez", 0, -1)),
+    "ymin": (("Ex", 1, 0), ("Ez", 1, 0)),
+    "ymax": (("Ex", 1, -1), ("Ez", 1, -1)),
+    "zmin": (("Ex", 2, 0), ("Ey", 2, 0)),
+    "zmax": (("Ex", 2, -1), ("Ey", 2, -1)),
+}
+
+
+def _pec_face_flat_indices(nx, ny, nz, face) -> np.ndarray:
+    shapes = {"Ex": (nx, ny + 1, nz + 1), "Ey": (nx + 1, ny, nz + 1), "Ez": (nx + 1, ny + 1, nz)}
+    offs = {"Ex": 0}
+    offs["Ey"] = int(np.prod(shapes["Ex"]))
+    offs["Ez"] = offs["Ey"] + int(np.prod(shapes["Ey"]))
+    out = []
+    for comp, axis, pos in _FACE_EDGES[face]:
+        shp = shapes[comp]
+        idx = np.arange(int(np.prod(shp))).reshape(shp)
+        sl = [slice(None)] * 3
+        sl[axis] = pos
+        out.append(offs[comp] + idx[tuple(sl)].ravel())
+    return np.concatenate(out)
+
+
+def _np(a):
+    if a is None:
+        return None
+    if hasattr(a, "get"):
+        a = a.get()
+    return np.asarray(a)
+
+
+def _recorder_scale(recorder, op):
+    """Per-mode factor the recorder applies on top of ``op.record_scale``
+    (the symmetry full-model scale, ``recorder.py:148-157``)."""
+    if recorder is None:
+        return 1.0
+    for p, s in zip(recorder._ports, recorder._scales):
+        if p is op:
+            rs = getattr(op, "record_scale", None)
+            if s is None:
+                return 1.0 if rs is None else 1.0 / np.asarray(rs, float)
+            s = np.asarray(s, float)
+            return s if rs is None else s / np.asarray(rs, float)
+    return 1.0
+
+
+def problem_from_solver(solver, n_steps: int) -> FitProblem:
+    """Build the engine problem of a reference solver after ``setup()``.
+
+    ``n_steps`` sizes the waveform sample tables and the DTBC kernel tables
+    (the run must not exceed it without calling :func:`extend_sources`).
+    """
+    from magnelio.boundaries.cpml import CPMLBoundary
+    from magnelio.boundaries.pec import PECBoundary
+    from magnelio.boundaries.pmc import PMCBoundary
+    from magnelio.monitors.field_frequency import MonitorFieldFrequency
+    from magnelio.ports._lumped.operator import LumpedElementOperator
+    from magnelio.ports._modal.operator import PortOperatorModal
+    from magnelio.circuit.companion import SeriesRLC
+
+    s = solver
+    if s._fields is None:
+        raise RuntimeError("problem_from_solver needs a solver after setup()")
+    if s._dispersion is not None or s._dispersion_mu is not None or s._sibc is not None:
+        raise NotImplementedError("dispersive materials / SIBC walls are not on the device engine yet")
+    if s.sources:
+        raise NotImplementedError("TF/SF plane-wave sources are not on the device engine yet")
+    grid = s.mesh.grid
+    nx, ny, nz = s.mesh.Nx, s.mesh.Ny, s.mesh.Nz
+    dt = float(s.dt)
+    aE = np.array(_np(s._alpha_E), dtype=np.float64)
+    bE = np.array(_np(s._beta_E), dtype=np.float64)
+    aH = np.array(_np(s._alpha_H), dtype=np.float64)
+    bH = np.array(_np(s._beta_H), dtype=np.float64)
+    prob = FitProblem(
+        nx=nx, ny=ny, nz=nz, dt=dt,
+        dx=np.asarray(grid.dx, float), dy=np.asarray(grid.dy, float), dz=np.asarray(grid.dz, float),
+        alpha_E=aE, beta_E=bE, alpha_H=aH, beta_H=bH,
+        M_eps=np.array(_np(s._M_eps_diag), dtype=np.float64),
+        M_mu=np.array(_np(s._M_mu_diag), dtype=np.float64),
+    )
+    # Boundaries.  A PEC face writes exact zeros on its tangential edges
+    # after every E update; folding alpha_E = beta_E = 0 onto those edges
+    # keeps them at +0.0 through the same update (fit_td.py:497-513).
+    for face, bc in s.boundary_conditions.items():
+        if isinstance(bc, CPMLBoundary):
+            air = tuple(_np(getattr(bc, f"_air_{n}")) for n in ("E1", "E2", "H1", "H2"))
+            prob.cpml.append(CpmlFace(face, np.asarray(bc._b, float), np.asarray(bc._c, float),
+                                      np.asarray(bc._ck, float), air))
+        elif isinstance(bc, PECBoundary):
+            if face not in s._port_faces:
+                idx = _pec_face_flat_indices(nx, ny, nz, face)
+                aE[idx] = 0.0
+                bE[idx] = 0.0
+        elif isinstance(bc, PMCBoundary):
+            pass
+        else:
+            raise NotImplementedError(f"boundary {type(bc).__name__} on {face} is not on the device engine")
+    if s._pec_reenforce_after_bc:
+        raise NotImplementedError("boundary types that write E without beta_E are not supported")
+    # Ports, modal first (the order update_e runs them in is irrelevant:
+    # their planes are disjoint), then lumped elements.
+    for op in s.ports:
+        if isinstance(op, PortOperatorModal):
+            prob.modal.append(_modal_from_op(op, s.recorder, dt, n_steps))
+    for op in s.ports:
+        if isinstance(op, PortOperatorModal):
+            continue
+        if isinstance(op, LumpedElementOperator):
+            el = op.element
+            if not isinstance(el, SeriesRLC):
+                raise NotImplementedError("only series R-L-C lumped elements are on the device engine")
+            scale = _recorder_scale(s.recorder, op)
+            t = np.arange(n_steps + 1) * dt
+            fn = op._waveform_fn
+            v = np.array([fn(tt + dt) for tt in t]) if fn is not None else np.zeros(0)
+            prob.lumped.append(LumpedPort(
+                flat_idx=np.asarray(op.flat_edge_indices, np.int64),
+                signs=np.asarray(op.edge_signs, float),
+                betas=np.asarray(op.beta_E, float),
+                R=el.R, L=el.L, C=el.C,
+                record_scale=float(np.asarray(scale, float).ravel()[0]),
+                v_src=[v],
+            ))
+        else:
+            raise NotImplementedError(f"port type {type(op).__name__} is not on the device engine")
+    for mon in s.monitors:
+        if not isinstance(mon, MonitorFieldFrequency):
+            raise NotImplementedError(f"monitor {type(mon).__name__} is not on the device engine")
+        r = mon._region
+        stride = mon._step_stride if mon._step_stride is not None else mon._resolve_stride(dt)
+        mon._step_stride = stride
+        prob.monitors.append(DftMonitor(
+            box=((r.ix.start, r.ix.stop), (r.iy.start, r.iy.stop), (r.iz.start, r.iz.stop)),
+            components=tuple(mon._components),
+            freqs=np.asarray(mon.freqs, float),
+            stride=int(stride),
+        ))
+    prob.e0 = [np.array(_np(s._fields.e_flat), dtype=np.float64)]
+    prob.h0 = [np.array(_np(s._fields.h_flat), dtype=np.float64)]
+    return prob
+
+
+def _modal_from_op(op, recorder, dt, n_steps) -> ModalPort:
+    plane = op.plane
+    M = op._n_modes
+    dms = op.discrete_modes
+    e_prof = np.stack([np.concatenate([dm.e_u_profile, dm.e_v_profile]) for dm in dms])
+    v_prof = e_prof.copy()
+    if op._dual_e_profiles is not None:
+        for m, dual in enumerate(op._dual_e_profiles):
+            if dual is not None:
+                v_prof[m] = np.concatenate([dual[0], dual[1]])
+    h_prof = np.stack([np.concatenate([dm.h_u_profile, dm.h_v_profile]) for dm in dms])
+    is_dtbc = np.array([t is not None for t in op._dtbc], dtype=np.int32)
+    r = np.array([t.r if t is not None else 0.0 for t in op._dtbc])
+    q = np.array([t.q if t is not None else 0.0 for t in op._dtbc])
+    # All terms of an operator start from the same n_kernel_init.
+    n0 = next((int(t._n_kernel) for t in op._dtbc if t is not None), 4096)
+    kernels = {}
+    for m, t in enumerate(op._dtbc):
+        if t is not None:
+            kernels[m] = host.dtbc_tables(t.r, t.q, n0, n_steps)
+    comp = None
+    if op._comp_r_u is not None:
+        comp = (np.concatenate([op._comp_r_u, op._comp_r_v]), np.concatenate([op._comp_live_u, op._comp_live_v]))
+    exc = None
+    if op._excitation_mode is not None:
+        m_exc = int(op._excitation_mode)
+        fn = op._excitation_waveform
+        k = np.arange(n_steps + 2)
+        if op._dtbc[m_exc] is not None:
+            # DTBC source at chain time t - dt with t = n dt + dt (operator.py:1473-1482)
+            w = np.array([fn((kk * dt + dt) - dt) for kk in k])
+        else:
+            # Mur TF/SF source at t = (k - 1) dt + dt (operator.py:1435-1437)
+            w = np.array([fn((kk - 1) * dt + dt) if kk > 0 else fn(0.0) for kk in k])
+        exc = (m_exc, w)
+    return ModalPort(
+        port_e_idx=np.asarray(op._g_port_e, np.int64),
+        int_e_idx=np.asarray(op._g_int_e, np.int64),
+        n_e_u=int(plane.e_u_indices.size),
+        port_h_idx=np.asarray(op._g_port_h, np.int64),
+        n_h_u=int(plane.h_u_indices.size),
+        me_port=np.concatenate([op._me_u_port, op._me_v_port]),
+        me_int=np.concatenate([op._me_u_int, op._me_v_int]),
+        mh_port=np.concatenate([op._mh_u, op._mh_v]),
+        e_profile=e_prof,
+        v_profile=v_prof,
+        h_profile=h_prof,
+        mur_r=np.asarray(op._mur_r, float),
+        tau=np.asarray(op._tau_m, float),
+        record_scale=np.asarray(op.record_scale, float),
+        is_dtbc=is_dtbc,
+        dtbc_r=r,
+        dtbc_q=q,
+        dtbc_n_kernel_init=n0,
+        dtbc_kernels=kernels,
+        complement=comp,
+        excitation=[exc],
+    )

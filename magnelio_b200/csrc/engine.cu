@@ -1,0 +1,1395 @@
+// Host side of the FIT-TD engine: handle lifetime, uploads, the per-step
+// launch sequence captured into CUDA graphs, readback and checkpointing.
+// Implements the C ABI declared in include/fitb200.h.
+//
+// One leapfrog step (reference loop body: src/magnelio/solver/fit_td.py
+// :950-1007) is the launch sequence
+//   update_E (+ CPML psi_E)         fit_td.py:843-876
+//   modal ports, lumped ports       fit_td.py:975-976 (+ recorder :981-982)
+//   update_H (+ CPML psi_H)         fit_td.py:893-920
+//   DFT stage / flush per monitor   fit_td.py:1001-1002
+//   step counter advance
+// PEC faces are folded into the coefficients by the caller (alpha_E = beta_E
+// = 0 on their tangential edges), which holds them at exact +0.0 the way the
+// reference's frozen PEC edges are (fit_td.py:497-513).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/fitb200.h"
+#include "fitb_common.cuh"
+
+namespace fitb {
+
+namespace {
+
+thread_local std::string g_last_error;
+
+struct Error : std::runtime_error {
+    int code;
+    Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+[[noreturn]] void fail(int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    throw Error(code, buf);
+}
+
+void ck(cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return;
+    if (e == cudaErrorMemoryAllocation) {
+        cudaGetLastError();
+        fail(FITB_ERR_NOMEM, "%s: %s", what, cudaGetErrorString(e));
+    }
+    fail(FITB_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+// Owning device buffer.
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    ~DevBuf() { release(); }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    void alloc(size_t n, bool zero = true) {
+        release();
+        if (n == 0) return;
+        ck(cudaMalloc(&p, n), "cudaMalloc");
+        bytes = n;
+        if (zero) ck(cudaMemset(p, 0, n), "cudaMemset");
+    }
+    template <typename U>
+    U* as() const {
+        return static_cast<U*>(p);
+    }
+};
+
+template <typename U>
+void upload(DevBuf& d, const std::vector<U>& v) {
+    d.alloc(v.size() * sizeof(U), false);
+    if (!v.empty()) ck(cudaMemcpy(d.p, v.data(), v.size() * sizeof(U), cudaMemcpyHostToDevice), "upload");
+}
+
+long long round_up(long long x, long long m) { return (x + m - 1) / m * m; }
+
+struct FaceHost {
+    int face = 0;
+    FaceDev dev{};
+    DevBuf psi, air, bcc;
+};
+
+struct LumpedHost {
+    LumpedDev dev{};
+    DevBuf off, sign, beta, src, st;
+    std::vector<double> src_host;  // [B][n_src]
+};
+
+struct ModalHost {
+    ModalDev dev{};
+    int n_modes = 0;
+    DevBuf port_e, int_e, port_h, me_port, me_int, mh_port, eprof, vprof, hprof;
+    DevBuf comp_r, comp_live;
+    DevBuf st, whist, shist, comp_state, scratch, exc, wf, buflen;
+    std::vector<std::vector<double>> ktabs;  // per mode: concatenated tables
+    std::vector<int> n_tables_mode;
+    DevBuf ktab[kMaxModes];
+    std::vector<int> exc_host, buflen_host;
+    std::vector<double> wf_host;  // [B][n_wf]
+    long long n_wf = 0;
+};
+
+struct DftHost {
+    DftDev dev{};
+    DevBuf omega, inv, dual, stage, wst, bins, cmp, base;
+    long long base_host = 0;
+    std::vector<int> comps;
+    int i0, i1, j0, j1, k0, k1;
+};
+
+}  // namespace
+
+struct Handle {
+    fitb_desc desc{};
+    int prec = 4;
+    size_t esz = 4;
+    Geom g{};
+    int B = 1;
+    double dt = 0.0;
+    cudaStream_t stream = nullptr;
+    DevBuf e, h, aE, bE, aH, bH, meps, mmu, staging;
+    bool coeffs_set = false;
+    std::vector<std::unique_ptr<FaceHost>> faces;
+    std::vector<std::unique_ptr<LumpedHost>> lumped;
+    std::vector<std::unique_ptr<ModalHost>> modal;
+    std::vector<std::unique_ptr<DftHost>> dft;
+    DevBuf d_lumped, d_modal;
+    bool port_tables_dirty = true;
+    DevBuf step;          // long long
+    long long steps_done = 0;
+    DevBuf recV, recI;    // [B][cap][nch]
+    long long cap = 0;
+    int nch = 0;
+    DevBuf absmax;        // [B]
+    DevBuf energy_partials, energy_out;
+    int energy_blocks = 1184;
+    cudaGraphExec_t graph_chunk = nullptr;
+    cudaGraphExec_t graph_one = nullptr;
+    int chunk = 16;
+    bool graphs_valid = false;
+    long long launches = 0;
+    int ichunk = 16;
+
+    ~Handle() {
+        if (graph_chunk) cudaGraphExecDestroy(graph_chunk);
+        if (graph_one) cudaGraphExecDestroy(graph_one);
+        if (stream) cudaStreamDestroy(stream);
+    }
+
+    long long e_block() const { return 3 * g.vol; }
+    long long nE() const {
+        return (long long)g.nx * (g.ny + 1) * (g.nz + 1) + (long long)(g.nx + 1) * g.ny * (g.nz + 1) +
+               (long long)(g.nx + 1) * (g.ny + 1) * g.nz;
+    }
+    long long nH() const {
+        return (long long)(g.nx + 1) * g.ny * g.nz + (long long)g.nx * (g.ny + 1) * g.nz +
+               (long long)g.nx * g.ny * (g.nz + 1);
+    }
+    long long comp_size(int c) const {
+        int ni, nj, nk;
+        comp_shape(g, c, ni, nj, nk);
+        return (long long)ni * nj * nk;
+    }
+    // Flat reference index (within E or H vector) -> offset into the padded
+    // field-set block (component * vol + padded index).
+    long long flat_to_off(bool is_h, long long flat) const {
+        int c0 = is_h ? 3 : 0;
+        long long rem = flat;
+        for (int q = 0; q < 3; ++q) {
+            long long sz = comp_size(c0 + q);
+            if (rem < sz) {
+                int ni, nj, nk;
+                comp_shape(g, c0 + q, ni, nj, nk);
+                int k = (int)(rem % nk);
+                long long r = rem / nk;
+                int j = (int)(r % nj);
+                int i = (int)(r / nj);
+                return (long long)q * g.vol + pidx(g, i, j, k);
+            }
+            rem -= sz;
+        }
+        fail(FITB_ERR_ARG, "flat index %lld out of range for %s (size %lld)", flat, is_h ? "H" : "E",
+             is_h ? nH() : nE());
+    }
+};
+
+}  // namespace fitb
+
+struct fitb_handle {
+    fitb::Handle impl;
+};
+
+using fitb::fail;
+using fitb::ck;
+
+namespace fitb {
+namespace {
+
+template <typename T>
+std::vector<T> cast_vec(const double* src, long long n) {
+    std::vector<T> v((size_t)n);
+    for (long long q = 0; q < n; ++q) v[(size_t)q] = (T)src[q];
+    return v;
+}
+
+// Upload a host array in the reference flat layout (three components,
+// starting at component c0) into a padded [3][vol] device array.
+template <typename T>
+void pack3(Handle& H, const T* host_flat, T* dev_padded, int c0) {
+    long long n = (c0 == 0) ? H.nE() : H.nH();
+    ck(cudaMemcpyAsync(H.staging.p, host_flat, (size_t)n * sizeof(T), cudaMemcpyHostToDevice, H.stream),
+       "H2D staging");
+    long long off = 0;
+    for (int q = 0; q < 3; ++q) {
+        launch_pack<T>(H.staging.as<T>(), dev_padded + (long long)q * H.g.vol, H.g, c0 + q, off, H.stream);
+        H.launches++;
+        off += H.comp_size(c0 + q);
+    }
+    ck(cudaGetLastError(), "pack");
+    ck(cudaStreamSynchronize(H.stream), "pack sync");
+}
+
+template <typename T>
+void unpack3(Handle& H, const T* dev_padded, T* host_flat, int c0) {
+    long long n = (c0 == 0) ? H.nE() : H.nH();
+    long long off = 0;
+    for (int q = 0; q < 3; ++q) {
+        launch_unpack<T>(dev_padded + (long long)q * H.g.vol, H.staging.as<T>(), H.g, c0 + q, off, H.stream);
+        H.launches++;
+        off += H.comp_size(c0 + q);
+    }
+    ck(cudaGetLastError(), "unpack");
+    ck(cudaMemcpyAsync(host_flat, H.staging.p, (size_t)n * sizeof(T), cudaMemcpyDeviceToHost, H.stream),
+       "D2H staging");
+    ck(cudaStreamSynchronize(H.stream), "unpack sync");
+}
+
+void invalidate_graphs(Handle& H) {
+    if (H.graph_chunk) cudaGraphExecDestroy(H.graph_chunk);
+    if (H.graph_one) cudaGraphExecDestroy(H.graph_one);
+    H.graph_chunk = H.graph_one = nullptr;
+    H.graphs_valid = false;
+}
+
+// Recorder and DTBC history capacity (steps).  Growth keeps the contents
+// and invalidates the captured graphs (they hold the old pointers).
+void ensure_capacity(Handle& H, long long need) {
+    if (need <= H.cap) return;
+    long long ncap = std::max(need, std::max<long long>(2 * H.cap, 1024));
+    if (H.nch > 0) {
+        for (DevBuf* buf : {&H.recV, &H.recI}) {
+            DevBuf nb;
+            nb.alloc((size_t)H.B * ncap * H.nch * sizeof(double));
+            if (buf->p && H.cap > 0)
+                ck(cudaMemcpy2D(nb.p, (size_t)ncap * H.nch * sizeof(double), buf->p,
+                                (size_t)H.cap * H.nch * sizeof(double), (size_t)H.cap * H.nch * sizeof(double),
+                                H.B, cudaMemcpyDeviceToDevice),
+                   "grow recorder");
+            std::swap(buf->p, nb.p);
+            std::swap(buf->bytes, nb.bytes);
+        }
+    }
+    for (auto& mp : H.modal) {
+        int M = mp->n_modes;
+        for (DevBuf* buf : {&mp->whist, &mp->shist}) {
+            DevBuf nb;
+            nb.alloc((size_t)H.B * M * ncap * sizeof(double));
+            if (buf->p && H.cap > 0)
+                ck(cudaMemcpy2D(nb.p, (size_t)ncap * sizeof(double), buf->p, (size_t)H.cap * sizeof(double),
+                                (size_t)H.cap * sizeof(double), (size_t)H.B * M, cudaMemcpyDeviceToDevice),
+                   "grow DTBC history");
+            std::swap(buf->p, nb.p);
+            std::swap(buf->bytes, nb.bytes);
+        }
+    }
+    H.cap = ncap;
+    H.port_tables_dirty = true;
+    invalidate_graphs(H);
+}
+
+void refresh_port_tables(Handle& H) {
+    if (!H.port_tables_dirty) return;
+    std::vector<LumpedDev> ld;
+    for (auto& lp : H.lumped) ld.push_back(lp->dev);
+    upload(H.d_lumped, ld);
+    std::vector<ModalDev> md;
+    for (auto& mp : H.modal) {
+        ModalDev d = mp->dev;
+        d.whist = mp->whist.as<double>();
+        d.shist = mp->shist.as<double>();
+        d.cap = H.cap;
+        md.push_back(d);
+    }
+    upload(H.d_modal, md);
+    H.port_tables_dirty = false;
+}
+
+template <typename T>
+StencilArgs<T> stencil_args(Handle& H) {
+    StencilArgs<T> a{};
+    a.g = H.g;
+    a.B = H.B;
+    a.e = H.e.as<T>();
+    a.h = H.h.as<T>();
+    a.aE = H.aE.as<T>();
+    a.bE = H.bE.as<T>();
+    a.aH = H.aH.as<T>();
+    a.bH = H.bH.as<T>();
+    a.nfaces = (int)H.faces.size();
+    for (int q = 0; q < a.nfaces; ++q) a.f[q] = H.faces[q]->dev;
+    a.ichunk = H.ichunk;
+    return a;
+}
+
+PortsArgs ports_args(Handle& H) {
+    PortsArgs pa{};
+    pa.B = H.B;
+    pa.e_block = H.e_block();
+    pa.h_block = H.e_block();
+    pa.step = H.step.as<long long>();
+    pa.dt_lumped = H.dt;
+    pa.rec.V = H.recV.as<double>();
+    pa.rec.I = H.recI.as<double>();
+    pa.rec.nch = H.nch;
+    pa.rec.cap = H.cap;
+    pa.absmax = H.absmax.as<double>();
+    return pa;
+}
+
+template <typename T>
+int enqueue_step(Handle& H) {
+    int n = 0;
+    StencilArgs<T> sa = stencil_args<T>(H);
+    PortsArgs pa = ports_args(H);
+    launch_update_E<T>(sa, H.stream);
+    ++n;
+    if (!H.modal.empty()) {
+        launch_modal<T>(H.e.as<T>(), H.h.as<T>(), pa, H.d_modal.as<ModalDev>(), (int)H.modal.size(), H.stream);
+        ++n;
+    }
+    if (!H.lumped.empty()) {
+        launch_lumped<T>(H.e.as<T>(), pa, H.d_lumped.as<LumpedDev>(), (int)H.lumped.size(), H.stream);
+        ++n;
+    }
+    launch_update_H<T>(sa, H.stream);
+    ++n;
+    for (auto& m : H.dft) {
+        launch_dft_stage<T>(H.e.as<T>(), H.h.as<T>(), H.e_block(), H.e_block(), H.g, H.B, m->dev,
+                            H.step.as<long long>(), H.stream);
+        launch_dft_flush(H.B, m->dev, H.step.as<long long>(), 0, H.stream);
+        n += 2;
+    }
+    launch_advance(H.step.as<long long>(), H.stream);
+    ++n;
+    return n;
+}
+
+int enqueue_step_any(Handle& H) { return H.prec == 4 ? enqueue_step<float>(H) : enqueue_step<double>(H); }
+
+cudaGraphExec_t capture(Handle& H, int nsteps, int* launches_per) {
+    cudaGraph_t graph = nullptr;
+    ck(cudaStreamBeginCapture(H.stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+    int per = 0;
+    try {
+        for (int s = 0; s < nsteps; ++s) per = enqueue_step_any(H);
+    } catch (...) {
+        cudaStreamEndCapture(H.stream, &graph);
+        if (graph) cudaGraphDestroy(graph);
+        throw;
+    }
+    ck(cudaStreamEndCapture(H.stream, &graph), "end capture");
+    cudaGraphExec_t exec = nullptr;
+    cudaError_t err = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    ck(err, "graph instantiate");
+    *launches_per = per;
+    return exec;
+}
+
+void check_ready(Handle& H) {
+    if (!H.coeffs_set) fail(FITB_ERR_STATE, "coefficients not set (call fitb_set_coeffs first)");
+}
+
+void check_dtbc_tables(Handle& H, long long last_step) {
+    // Chain step n uses the table of length n0 * 2^t >= n + 1.
+    for (size_t p = 0; p < H.modal.size(); ++p) {
+        auto& mp = *H.modal[p];
+        long long tlen = mp.dev.n0;
+        int t = 0;
+        while (tlen < last_step + 1) {
+            tlen *= 2;
+            ++t;
+        }
+        for (int m = 0; m < mp.n_modes; ++m) {
+            if (!mp.dev.is_dtbc[m]) continue;
+            if (mp.n_tables_mode[m] <= t)
+                fail(FITB_ERR_STATE,
+                     "modal port %zu mode %d: DTBC kernel table of length %lld missing for step %lld "
+                     "(call fitb_set_dtbc_kernel)",
+                     p, m, tlen, last_step);
+        }
+    }
+}
+
+void run_steps(Handle& H, long long nsteps) {
+    check_ready(H);
+    if (nsteps < 0) fail(FITB_ERR_ARG, "n_steps must be >= 0");
+    if (nsteps > 0) check_dtbc_tables(H, H.steps_done + nsteps - 1);
+    ensure_capacity(H, H.steps_done + nsteps);
+    refresh_port_tables(H);
+    int per = 0;
+    if (!H.graphs_valid) {
+        int p1 = 0, pc = 0;
+        H.graph_one = capture(H, 1, &p1);
+        H.graph_chunk = capture(H, H.chunk, &pc);
+        H.graphs_valid = true;
+    }
+    // launches per step (same sequence in both graphs)
+    {
+        per = 1 + 1 + 1 + (H.modal.empty() ? 0 : 1) + (H.lumped.empty() ? 0 : 1) + 2 * (int)H.dft.size();
+    }
+    if (nsteps == 0) return;
+    long long left = nsteps;
+    while (left >= H.chunk) {
+        ck(cudaGraphLaunch(H.graph_chunk, H.stream), "graph launch");
+        left -= H.chunk;
+    }
+    while (left > 0) {
+        ck(cudaGraphLaunch(H.graph_one, H.stream), "graph launch");
+        --left;
+    }
+    H.launches += (long long)per * nsteps;
+    H.steps_done += nsteps;
+}
+
+template <typename T>
+void energy_impl(Handle& H, int b, double* out) {
+    launch_energy<T>(H.e.as<T>(), H.h.as<T>(), H.meps.as<T>(), H.mmu.as<T>(), H.g, b, H.e_block(),
+                     H.energy_partials.as<double>(), H.energy_blocks, H.energy_out.as<double>(), H.stream);
+    H.launches += 2;
+    ck(cudaGetLastError(), "energy");
+    ck(cudaMemcpyAsync(out, H.energy_out.p, sizeof(double), cudaMemcpyDeviceToHost, H.stream), "energy D2H");
+    ck(cudaStreamSynchronize(H.stream), "energy sync");
+}
+
+long long dft_recorded_upto(long long x, int stride) { return x < 0 ? 0 : x / stride + 1; }
+
+// Flush the partially filled slot block of every monitor and restart the
+// slot count at the next step.
+void dft_flush_pending(Handle& H) {
+    for (auto& mp : H.dft) {
+        DftHost& m = *mp;
+        long long cnt = dft_recorded_upto(H.steps_done - 1, m.dev.stride) -
+                        dft_recorded_upto(m.base_host - 1, m.dev.stride);
+        int pending = (int)(cnt % m.dev.K);
+        if (pending > 0) {
+            launch_dft_flush(H.B, m.dev, H.step.as<long long>(), pending, H.stream);
+            H.launches++;
+            ck(cudaGetLastError(), "dft flush");
+        }
+        m.base_host = H.steps_done;
+        ck(cudaMemcpyAsync(m.base.p, &m.base_host, sizeof(long long), cudaMemcpyHostToDevice, H.stream),
+           "dft base");
+        ck(cudaStreamSynchronize(H.stream), "dft flush sync");
+    }
+}
+
+int face_axis(int face) { return face / 2; }
+
+// Reference psi shape of auxiliary q (0..3 = E1,E2,H1,H2) on a face axis.
+void psi_ref_shape(const Geom& g, int axis, int n, int q, int& a, int& b, int& c) {
+    static const int comps[3][4] = {{1, 2, 4, 5}, {0, 2, 3, 5}, {0, 1, 3, 4}};
+    comp_shape(g, comps[axis][q], a, b, c);
+    if (axis == 0) a = n;
+    if (axis == 1) b = n;
+    if (axis == 2) c = n;
+}
+
+template <typename T>
+void add_cpml_impl(Handle& H, int face, int n_pml, const double* bt, const double* ct, const double* ckt,
+                   const uint8_t* const air_in[4]) {
+    auto f = std::make_unique<FaceHost>();
+    f->face = face;
+    const int axis = face_axis(face), side = face % 2;
+    const int N = axis == 0 ? H.g.nx : (axis == 1 ? H.g.ny : H.g.nz);
+    if (n_pml < 1 || n_pml > N) fail(FITB_ERR_ARG, "n_pml %d out of range [1, %d]", n_pml, N);
+    FaceDev& d = f->dev;
+    d.axis = axis;
+    d.n = n_pml;
+    d.lo = side == 0 ? 0 : N - n_pml;
+    d.dI = axis == 0 ? n_pml : H.g.nx + 1;
+    d.dJ = axis == 1 ? n_pml : H.g.ny + 1;
+    d.dK = axis == 2 ? n_pml : H.g.nz + 1;
+    d.slab = (long long)d.dI * d.dJ * d.dK;
+    f->psi.alloc((size_t)H.B * 4 * d.slab * sizeof(T));
+    std::vector<uint8_t> air((size_t)(4 * d.slab), 0);
+    for (int q = 0; q < 4; ++q) {
+        int ra, rb, rc;
+        psi_ref_shape(H.g, axis, n_pml, q, ra, rb, rc);
+        for (int x = 0; x < ra; ++x)
+            for (int y = 0; y < rb; ++y)
+                for (int z = 0; z < rc; ++z) {
+                    long long src = ((long long)x * rb + y) * rc + z;
+                    long long dst = (long long)q * d.slab + ((long long)x * d.dJ + y) * d.dK + z;
+                    air[(size_t)dst] = air_in[q] ? (air_in[q][src] ? 1 : 0) : 1;
+                }
+    }
+    upload(f->air, air);
+    std::vector<T> bcc((size_t)(3 * n_pml));
+    for (int l = 0; l < n_pml; ++l) {
+        bcc[(size_t)l] = (T)bt[l];
+        bcc[(size_t)(n_pml + l)] = (T)ct[l];
+        bcc[(size_t)(2 * n_pml + l)] = (T)ckt[l];
+    }
+    upload(f->bcc, bcc);
+    d.psi = f->psi.p;
+    d.air = f->air.as<unsigned char>();
+    d.bcc = f->bcc.p;
+    H.faces.push_back(std::move(f));
+}
+
+// ---- state serialisation ----------------------------------------------
+struct Writer {
+    std::vector<char>* out = nullptr;  // sizing pass when null
+    size_t n = 0;
+    void put(const void* p, size_t bytes) {
+        if (out) out->insert(out->end(), (const char*)p, (const char*)p + bytes);
+        n += bytes;
+    }
+    template <typename U>
+    void pod(const U& v) {
+        put(&v, sizeof(U));
+    }
+};
+
+void dev_get(Writer& w, const void* dptr, size_t bytes) {
+    if (!w.out) {
+        w.n += bytes;
+        return;
+    }
+    size_t at = w.out->size();
+    w.out->resize(at + bytes);
+    if (bytes) ck(cudaMemcpy(w.out->data() + at, dptr, bytes, cudaMemcpyDeviceToHost), "state D2H");
+    w.n += bytes;
+}
+
+template <typename T>
+void write_state(Handle& H, Writer& w) {
+    const unsigned long long magic = 0x46495442'32303031ULL;  // "FITB2001"
+    w.pod(magic);
+    w.pod((int)H.prec);
+    w.pod((int)H.B);
+    w.pod(H.g.nx);
+    w.pod(H.g.ny);
+    w.pod(H.g.nz);
+    w.pod(H.steps_done);
+    // fields in the reference flat layout
+    for (int b = 0; b < H.B; ++b) {
+        std::vector<T> ev, hv;
+        if (w.out) {
+            ev.resize((size_t)H.nE());
+            hv.resize((size_t)H.nH());
+            unpack3<T>(H, H.e.as<T>() + (long long)b * H.e_block(), ev.data(), 0);
+            unpack3<T>(H, H.h.as<T>() + (long long)b * H.e_block(), hv.data(), 3);
+        }
+        if (w.out) {
+            w.put(ev.data(), ev.size() * sizeof(T));
+            w.put(hv.data(), hv.size() * sizeof(T));
+        } else {
+            w.n += (size_t)(H.nE() + H.nH()) * sizeof(T);
+        }
+    }
+    for (auto& f : H.faces) dev_get(w, f->psi.p, f->psi.bytes);
+    for (auto& lp : H.lumped) dev_get(w, lp->st.p, lp->st.bytes);
+    for (auto& mp : H.modal) {
+        dev_get(w, mp->st.p, mp->st.bytes);
+        dev_get(w, mp->comp_state.p, mp->comp_state.bytes);
+        // histories up to the completed step count, per (b, mode)
+        int M = mp->n_modes;
+        for (int b = 0; b < H.B; ++b)
+            for (int m = 0; m < M; ++m) {
+                size_t off = (((size_t)b * M + m) * (size_t)H.cap) * sizeof(double);
+                dev_get(w, mp->whist.as<char>() + off, (size_t)H.steps_done * sizeof(double));
+                dev_get(w, mp->shist.as<char>() + off, (size_t)H.steps_done * sizeof(double));
+            }
+    }
+    for (auto& m : H.dft) {
+        dev_get(w, m->bins.p, m->bins.bytes);
+        dev_get(w, m->cmp.p, m->cmp.bytes);
+    }
+    dev_get(w, H.absmax.p, H.absmax.bytes);
+}
+
+struct Reader {
+    const char* p;
+    size_t left;
+    void get(void* dst, size_t bytes) {
+        if (bytes > left) fail(FITB_ERR_ARG, "state buffer too short");
+        memcpy(dst, p, bytes);
+        p += bytes;
+        left -= bytes;
+    }
+    void dev(void* dptr, size_t bytes) {
+        if (bytes > left) fail(FITB_ERR_ARG, "state buffer too short");
+        if (bytes) ck(cudaMemcpy(dptr, p, bytes, cudaMemcpyHostToDevice), "state H2D");
+        p += bytes;
+        left -= bytes;
+    }
+    template <typename U>
+    U pod() {
+        U v;
+        get(&v, sizeof(U));
+        return v;
+    }
+};
+
+template <typename T>
+void read_state(Handle& H, Reader& r) {
+    const unsigned long long magic = 0x46495442'32303031ULL;
+    if (r.pod<unsigned long long>() != magic) fail(FITB_ERR_ARG, "not a fitb200 state buffer");
+    int prec = r.pod<int>(), B = r.pod<int>(), nx = r.pod<int>(), ny = r.pod<int>(), nz = r.pod<int>();
+    if (prec != H.prec || B != H.B || nx != H.g.nx || ny != H.g.ny || nz != H.g.nz)
+        fail(FITB_ERR_ARG, "state buffer was written by a differently configured handle");
+    long long steps = r.pod<long long>();
+    ensure_capacity(H, steps + 1);
+    for (int b = 0; b < H.B; ++b) {
+        std::vector<T> ev((size_t)H.nE()), hv((size_t)H.nH());
+        r.get(ev.data(), ev.size() * sizeof(T));
+        r.get(hv.data(), hv.size() * sizeof(T));
+        pack3<T>(H, ev.data(), H.e.as<T>() + (long long)b * H.e_block(), 0);
+        pack3<T>(H, hv.data(), H.h.as<T>() + (long long)b * H.e_block(), 3);
+    }
+    for (auto& f : H.faces) r.dev(f->psi.p, f->psi.bytes);
+    for (auto& lp : H.lumped) r.dev(lp->st.p, lp->st.bytes);
+    for (auto& mp : H.modal) {
+        r.dev(mp->st.p, mp->st.bytes);
+        r.dev(mp->comp_state.p, mp->comp_state.bytes);
+        int M = mp->n_modes;
+        ck(cudaMemset(mp->whist.p, 0, mp->whist.bytes), "clear history");
+        ck(cudaMemset(mp->shist.p, 0, mp->shist.bytes), "clear history");
+        for (int b = 0; b < H.B; ++b)
+            for (int m = 0; m < M; ++m) {
+                size_t off = (((size_t)b * M + m) * (size_t)H.cap) * sizeof(double);
+                r.dev(mp->whist.as<char>() + off, (size_t)steps * sizeof(double));
+                r.dev(mp->shist.as<char>() + off, (size_t)steps * sizeof(double));
+            }
+    }
+    for (auto& m : H.dft) {
+        r.dev(m->bins.p, m->bins.bytes);
+        r.dev(m->cmp.p, m->cmp.bytes);
+    }
+    r.dev(H.absmax.p, H.absmax.bytes);
+    H.steps_done = steps;
+    ck(cudaMemcpy(H.step.p, &steps, sizeof(long long), cudaMemcpyHostToDevice), "step counter");
+    for (auto& m : H.dft) {
+        m->base_host = steps;
+        ck(cudaMemcpy(m->base.p, &steps, sizeof(long long), cudaMemcpyHostToDevice), "dft base");
+    }
+}
+
+}  // namespace
+}  // namespace fitb
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+using fitb::Handle;
+
+#define FITB_TRY try {
+#define FITB_CATCH                                                   \
+    }                                                                \
+    catch (const fitb::Error& ex) {                                  \
+        fitb::g_last_error = ex.what();                              \
+        return ex.code;                                              \
+    }                                                                \
+    catch (const std::bad_alloc&) {                                  \
+        fitb::g_last_error = "host allocation failed";               \
+        return FITB_ERR_NOMEM;                                       \
+    }                                                                \
+    catch (const std::exception& ex) {                               \
+        fitb::g_last_error = ex.what();                              \
+        return FITB_ERR_STATE;                                       \
+    }                                                                \
+    return FITB_OK;
+
+static Handle& H_of(fitb_handle* h) {
+    if (!h) fail(FITB_ERR_ARG, "null handle");
+    ck(cudaSetDevice(h->impl.desc.device), "cudaSetDevice");
+    return h->impl;
+}
+
+extern "C" {
+
+int fitb_abi_version(void) { return FITB_ABI_VERSION; }
+
+int fitb_last_error(char* buf, size_t len) {
+    if (!buf || len == 0) return FITB_ERR_ARG;
+    snprintf(buf, len, "%s", fitb::g_last_error.c_str());
+    return FITB_OK;
+}
+
+int fitb_create(const fitb_desc* desc, fitb_handle** out) {
+    FITB_TRY
+    if (!desc || !out) fail(FITB_ERR_ARG, "null argument");
+    *out = nullptr;
+    if (desc->nx < 1 || desc->ny < 1 || desc->nz < 1) fail(FITB_ERR_ARG, "grid must have >= 1 cell per axis");
+    if (desc->batch < 1) fail(FITB_ERR_ARG, "batch must be >= 1");
+    if (desc->precision != 4 && desc->precision != 8) fail(FITB_ERR_ARG, "precision must be 4 or 8");
+    if (!(desc->dt > 0.0)) fail(FITB_ERR_ARG, "dt must be positive");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        fail(FITB_ERR_NODEV, "no CUDA device available");
+    }
+    if (desc->device < 0 || desc->device >= ndev) fail(FITB_ERR_ARG, "device %d out of range", desc->device);
+    ck(cudaSetDevice(desc->device), "cudaSetDevice");
+    auto owner = std::make_unique<fitb_handle>();
+    Handle& H = owner->impl;
+    H.desc = *desc;
+    H.prec = desc->precision;
+    H.esz = (size_t)desc->precision;
+    H.B = desc->batch;
+    H.dt = desc->dt;
+    fitb::Geom& g = H.g;
+    g.nx = desc->nx;
+    g.ny = desc->ny;
+    g.nz = desc->nz;
+    g.njp = g.ny + 2;
+    g.nkp = (int)fitb::round_up(g.nz + 2, 4);
+    g.sj = g.nkp;
+    g.si = (long long)g.njp * g.nkp;
+    g.vol = (long long)(g.nx + 3) * g.si;
+    ck(cudaStreamCreateWithFlags(&H.stream, cudaStreamNonBlocking), "stream");
+    const size_t blk = (size_t)H.e_block() * H.esz;
+    H.e.alloc(blk * H.B);
+    H.h.alloc(blk * H.B);
+    H.aE.alloc(blk);
+    H.bE.alloc(blk);
+    H.aH.alloc(blk);
+    H.bH.alloc(blk);
+    H.meps.alloc(blk);
+    H.mmu.alloc(blk);
+    H.staging.alloc((size_t)std::max(H.nE(), H.nH()) * H.esz, false);
+    H.step.alloc(sizeof(long long));
+    H.absmax.alloc(sizeof(double) * H.B);
+    H.energy_partials.alloc(sizeof(double) * H.energy_blocks);
+    H.energy_out.alloc(sizeof(double));
+    *out = owner.release();
+    FITB_CATCH
+}
+
+int fitb_destroy(fitb_handle* h) {
+    FITB_TRY
+    if (!h) return FITB_OK;
+    cudaSetDevice(h->impl.desc.device);
+    cudaStreamSynchronize(h->impl.stream);
+    delete h;
+    FITB_CATCH
+}
+
+int fitb_launch_count(const fitb_handle* h, int64_t* out) {
+    FITB_TRY
+    if (!h || !out) fail(FITB_ERR_ARG, "null argument");
+    *out = h->impl.launches;
+    FITB_CATCH
+}
+
+int fitb_set_coeffs(fitb_handle* h, const double* alpha_e, const double* beta_e, const double* alpha_h,
+                    const double* beta_h, const double* m_eps, const double* m_mu) {
+    FITB_TRY
+    Handle& H = H_of(h);
+    if (!alpha_e || !beta_e || !alpha_h || !beta_h) fail(FITB_ERR_ARG, "null coefficient array");
+    const long long nE = H.nE(), nH = H.nH();
+    auto put = [&](fitb::DevBuf& dst, const double* src, long long n, int c0) {
+        if (H.prec == 4) {
+            std::vector<float> v = fitb::cast_vec<float>(src, n);
+            fitb::pack3<float>(H, v.data(), dst.as<float>(), c0);
+        } else {
+            fitb::pack3<double>(H, src, dst.as<double>(), c0);
+        }
+    };
+    put(H.aE, alpha_e, nE, 0);
+    put(H.bE, beta_e, nE, 0);
+    put(H.aH, alpha_h, nH, 3);
+    put(H.bH, beta_h, nH, 3);
+    if (m_eps) put(H.meps, m_eps, nE, 0);
+    if (m_mu) put(H.mmu, m_mu, nH, 3);
+    H.coeffs_set = true;
+    FITB_CATCH
+}
+
+int fitb_set_coeffs_native(fitb_handle* h, const void* alpha_e, const void* beta_e, const void* alpha_h,
+                           const void* beta_h, const void* m_eps, const void* m_mu) {
+    FITB_TRY
+    Handle& H = H_of(h);
+    if (!alpha_e || !beta_e || !alpha_h || !beta_h) fail(FITB_ERR_ARG, "null coefficient array");
+    auto put = [&](fitb::DevBuf& dst, const void* src, int c0) {
+        if (H.prec == 4)
+            fitb::pack3<float>(H, (const float*)src, dst.as<float>(), c0);
+        else
+            fitb::pack3<double>(H, (const double*)src, dst.as<double>(), c0);
+    };
+    put(H.aE, alpha_e, 0);
+    put(H.bE, beta_e, 0);
+    put(H.aH, alpha_h, 3);
+    put(H.bH, beta_h, 3);
+    if (m_eps) put(H.meps, m_eps, 0);
+    if (m_mu) put(H.mmu, m_mu, 3);
+    H.coeffs_set = true;
+    FITB_CATCH
+}
+
+int fitb_set_fields(fitb_handle* h, int32_t b, const void* e, size_t e_bytes, const void* hf, size_t h_bytes) {
+    FITB_TRY
+    Handle& H = H_of(h);
+    if (b < 0 || b >= H.B) fail(FITB_ERR_ARG, "field set %d out of range", b);
+    if (e) {
+        if (e_bytes != (size_t)H.nE() * H.esz) fail(FITB_ERR_ARG, "e buffer is %zu bytes, expected %zu", e_bytes, (size_t)H.nE() * H.esz);
+        if (H.prec == 4)
+            fitb::pack3<float>(H, (const float*)e, H.e.as<float>() + (long long)b * H.e_block(), 0);
+        else
+            fitb::pack3<double>(H, (const double*)e, H.e.as<double>() + (long long)b * H.e_block(), 0);
+    }
+    if (hf) {
+        if (h_bytes != (size_t)H.nH() * H.esz) fail(FITB_ERR_ARG, "h buffer is %zu bytes, expected %zu", h_bytes, (size_t)H.nH() * H.esz);
+        if (H.prec == 4)
+            fitb::pack3<float>(H, (const float*)hf, H.h.as<float>() + (long long)b * H.e_block(), 3);
+        else
+            fitb::pack3<double>(H, (const double*)hf, H.h.as<double>() + (long long)b * H.e_block(), 3);
+    }
+    FITB_CATCH
+}
+
+int fitb_read_fields(fitb_handle* h, int32_t b, void* e, size_t e_bytes, void* hf, size_t h_bytes) {
+    FITB_TRY
+    Handle& H = H_of(h);
+    if (b < 0 || b >= H.B) fail(FITB_ERR_ARG, "field set %d out of range", b);
+    if (e) {
+        if (e_bytes != (size_t)H.nE() * H.esz) fail(FITB_ERR_ARG, "e buffer size mismatch");
+        if (H.prec == 4)
+            fitb::unpack3<float>(H, H.e.as<float>() + (long long)b * H.e_block(), (float*)e, 0);
+        else
+            fitb::unpack3<double>(H, H.e.as<double>() + (long long)b * H.e_block(), (double*)e, 0);
+    }
+    if (hf) {
+        if (h_bytes != (size_t)H.nH() * H.esz) fail(FITB_ERR_ARG, "h buffer size mismatch");
+        if (H.prec == 4)
+            fitb::unpack3<float>(H, H.h.as<float>() + (long long)b * H.e_block(), (float*)hf, 3);
+        else
+            fitb::unpack3<double>(H, H.h.as<double>() + (long long)b * H.e_block(), (double*)hf, 3);
+    }
+    FITB_CATCH
+}
+
+int fitb_add_cpml(fitb_handle* h, int32_t face, int32_t n_pml, const double* b, const double* c, const double* ck_,
+                  const uint8_t* air_e1, const uint8_t* air_e2, const uint8_t* air_h1, const uint8_t* air_h2) {
+    FITB_TRY
+    Handle& H = H_of(h);
+    if (face < 0 || face > 5) fail(FITB_ERR_ARG, "face must be 0..5");
+    if (!b || !c || !ck_) fail(FITB_ERR_ARG, "null CPML table");
+    if ((int)H.faces.size() >= fitb::kMaxFaces) fail(FITB_ERR_LIMIT, "at most %d CPML faces", fitb::kMaxFaces);
+    for (auto& f : H.faces)
+        if (f->face == face) fail(FITB_ERR_ARG, "CPML face %d already added", face);
+    if (H.steps_done != 0) fail(FITB_ERR_STATE, "boundaries must be added before the first step");
+    const uint8_t* air[4] = {air_e1, air_e2, air_h1, air_h2};
+    if (H.prec == 4)
+        fitb::add_cpml_impl<float>(H, face, n_pml, b, c, ck_, air);
+    else
+        fitb::add_cpml_impl<double>(H, face, n_pml, b, c, ck_, air);
+    fitb::invalidate_graphs(H);
+    FITB_CATCH
+}
+
+int fitb_add_lumped(fitb_handle* h, int32_t n_edges, const int64_t* flat_e_idx, const double* signs,
+                    const double* betas, double r, double l, double c, double record_scale, int32_t* out_id) {
+    FITB_TRY
+    Handle& H = H_of(h);
+    if (n_edges < 1 || !flat_e_idx || !signs || !betas) fail(FITB_ERR_ARG, "lumped port needs >= 1 edge");
+    if (r < 0 && l < 0 && c < 0) fail(FITB_ERR_ARG, "lumped element needs at least one of R, L, C");
+    if (H.steps_done != 0) fail(FITB_ERR_STATE, "ports must be added before the first step");
+    auto lp = std::make_unique<fitb::LumpedHost>();
+    std::vector<long long> off((size_t)n_edges);
+    double bsum = 0.0;
+    for (int q = 0; q < n_edges; ++q) {
+        off[(size_t)q] = H.flat_to_off(false, flat_e_idx[q]);
+        bsum += betas[q];
+    }
+    fitb::upload(lp->off, off);
+    fitb::upload(lp->sign, std::vector<double>(signs, signs + n_edges));
+    fitb::upload(lp->beta, std::vector<double>(betas, betas + n_edges));
+    lp->st.alloc(sizeof(double) * 4 * H.B);
+    lp->src_host.assign((size_t)H.B, 0.0);
+    fitb::upload(lp->src, lp->src_host);
+    fitb::LumpedDev& d = lp->dev;
+    d.n_edges = n_edges;
+    d.off = lp->off.as<long long>();
+    d.sign = lp->sign.as<double>();
+    d.beta = lp->beta.as<double>();
+    d.beta_sum = bsum;
+    d.R = r;
+    d.L = l;
+    d.C = c;
+    d.rec_scale = record_scale;
+    d.src = lp->src.as<double>();
+    d.n_src = 1;
+    d.st = lp->st.as<double>();
+    d.channel = H.nch;
+    H.nch += 1;
+    if (out_id) *out_id = (int32_t)H.lumped.size();
+    H.lumped.push_back(std::move(lp));
+    H.cap = 0;
+    H.recV.release();
+    H.recI.release();
+    H.port_tables_dirty = true;
+    fitb::invalidate_graphs(H);
+    FITB_CATCH
+}
+
+int fitb_set_lumped_source(fitb_handle* h, int32_t id, int32_t b, int64_t n_samples, const double* v_src) {
+    FITB_TRY
+    Handle& H = H_of(h);
+    if (id < 0 || id >= (int)H.lumped.size()) fail(FITB_ERR_ARG, "lumped port %d does not exist", id);
+    if (b < 0 || b >= H.B) fail(FITB_ERR_ARG, "field set %d out of range", b);
+    if (n_samples < 0 || (n_samples > 0 && !v_src)) fail(FITB_ERR_ARG, "bad source samples");
+    fitb::LumpedHost& lp = *H.lumped[id];
+    long long n_old = lp.dev.n_src;
+    long long n_new = std::max<long long>(n_old, std::max<int64_t>(n_samples, 1));
+    std::vector<double> tab((size_t)(H.B * n_new), 0.0);
+    for (int q = 0; q < H.B; ++q)
+        for (long long t = 0; t < n_old; ++t) tab[(size_t)(q * n_new + t)] = lp.src_host[(size_t)(q * n_old + t)];
+    for (long long t = 0; t < n_new; ++t) tab[(size_t)(b * n_new + t)] = t < n_samples ? v_src[t] : 0.0;
+    lp.src_host = tab;
+    fitb::upload(lp.src, tab);
+    lp.dev.src = lp.src.as<double>();
+    lp.dev.n_src = n_new;
+    H.port_tables_dirty = true;
+    fitb::invalidate_graphs(H);
+    FITB_CATCH
+}
+
+int fitb_push_lumped_samples(fitb_handle* h, int32_t id, int32_t b, int64_t step0, int64_t n, const double* host) {
+    FITB_TRY
+    Handle& H = H_of(h);
+    if (id < 0 || id >= (int)H.lumped.size()) fail(FITB_ERR_ARG, "lumped port %d does not exist", id);
+    if (b < 0 || b >= H.B) fail(FITB_ERR_ARG, "field set %d out of range", b);
+    fitb::LumpedHost& lp = *H.lumped[id];
+    if (n < 0 || step0 < 0 || step0 + n > lp.dev.n_src || (n > 0 && !host))
+        fail(FITB_ERR_ARG, "samples [%lld, %lld) outside the source table of %lld", (long long)step0,
+             (long long)(step0 + n), lp.dev.n_src);
+    if (n == 0) return FITB_OK;
+    ck(cudaMemcpyAsync(lp.src.as<double>() + (size_t)b * lp.dev.n_src + step0, host, (size_t)n * sizeof(double),
+                       cudaMemcpyHostToDevice, H.stream),
+       "push samples");
+    FITB_CATCH
+}
+
+int fitb_add_modal_port(fitb_handle* h, const fitb_modal_desc* d, int32_t* out_id) {
+    FITB_TRY
+    Handle& H = H_of(h);
+    if (!d) fail(FITB_ERR_ARG, "null descriptor");
+    if (d->n_modes < 1 || d->n_modes > fitb::kMaxModes) fail(FITB_ERR_LIMIT, "n_modes must be 1..%d", fitb::kMaxModes);
+    if (H.steps_done != 0) fail(FITB_ERR_STATE, "ports must be added before the first step");
+    const int M = d->n_modes;
+    const int ne = d->n_e_u + d->n_e_v, nh = d->n_h_u + d->n_h_v;
+    if (ne < 1) fail(FITB_ERR_ARG, "modal port without plane samples");
+    if (!d->port_e_idx || !d->int_e_idx || !d->me_port || !d->me_int || !d->e_profile || !d->v_profile ||
+        !d->mur_r || !d->tau || !d->record_scale || !d->is_dtbc)
+        fail(FITB_ERR_ARG, "modal descriptor has a null array");
+    if (nh > 0 && (!d->port_h_idx || !d->mh_port || !d->h_profile)) fail(FITB_ERR_ARG, "modal descriptor: null H arrays");
+    auto mp = std::make_unique<fitb::ModalHost>();
+    mp->n_modes = M;
+    std::vector<long long> pe((size_t)ne), ie((size_t)ne), ph((size_t)nh);
+    for (int p = 0; p < ne; ++p) {
+        pe[(size_t)p] = H.flat_to_off(false, d->port_e_idx[p]);
+        ie[(size_t)p] = H.flat_to_off(false, d->int_e_idx[p]);
+    }
+    for (int p = 0; p < nh; ++p) ph[(size_t)p] = H.flat_to_off(true, d->port_h_idx[p]);
+    fitb::upload(mp->port_e, pe);
+    fitb::upload(mp->int_e, ie);
+    fitb::upload(mp->port_h, ph);
+    fitb::upload(mp->me_port, std::vector<double>(d->me_port, d->me_port + ne));
+    fitb::upload(mp->me_int, std::vector<double>(d->me_int, d->me_int + ne));
+    fitb::upload(mp->mh_port, nh ? std::vector<double>(d->mh_port, d->mh_port + nh) : std::vector<double>(1, 0.0));
+    fitb::upload(mp->eprof, std::vector<double>(d->e_profile, d->e_profile + (size_t)M * ne));
+    fitb::upload(mp->vprof, std::vector<double>(d->v_profile, d->v_profile + (size_t)M * ne));
+    fitb::upload(mp->hprof, nh ? std::vector<double>(d->h_profile, d->h_profile + (size_t)M * nh) : std::vector<double>(1, 0.0));
+    bool any_mur = false;
+    fitb::ModalDev& md = mp->dev;
+    md.n_modes = M;
+    md.n_e = ne;
+    md.n_e_u = d->n_e_u;
+    md.n_h = nh;
+    md.n_h_u = d->n_h_u;
+    md.dt = H.dt;
+    mp->n_tables_mode.assign((size_t)M, 0);
+    mp->ktabs.assign((size_t)M, {});
+    for (int m = 0; m < M; ++m) {
+        md.mur_r[m] = d->mur_r[m];
+        md.tau[m] = d->tau[m];
+        md.rec_scale[m] = d->record_scale[m];
+        md.is_dtbc[m] = d->is_dtbc[m] ? 1 : 0;
+        if (md.is_dtbc[m]) {
+            if (!d->dtbc_r || !d->dtbc_q) fail(FITB_ERR_ARG, "DTBC mode without r/q");
+            md.r2[m] = d->dtbc_r[m] * d->dtbc_r[m];
+            md.q2[m] = d->dtbc_q[m] * d->dtbc_q[m];
+        } else {
+            any_mur = true;
+        }
+    }
+    int n0 = d->dtbc_n_kernel_init > 0 ? d->dtbc_n_kernel_init : 4096;
+    md.n0 = n0;
+    md.comp_on = (d->has_complement && any_mur) ? 1 : 0;
+    if (d->has_complement) {
+        if (!d->comp_r || !d->comp_live) fail(FITB_ERR_ARG, "complement absorber arrays missing");
+        fitb::upload(mp->comp_r, std::vector<double>(d->comp_r, d->comp_r + ne));
+        fitb::upload(mp->comp_live, std::vector<double>(d->comp_live, d->comp_live + ne));
+    }
+    mp->st.alloc(sizeof(double) * H.B * 4 * fitb::kMaxModes);
+    mp->comp_state.alloc(sizeof(double) * H.B * 2 * ne);
+    mp->scratch.alloc(sizeof(double) * H.B * 2 * ne);
+    mp->exc_host.assign((size_t)H.B, -1);
+    mp->buflen_host.assign((size_t)H.B, 5);
+    mp->n_wf = 1;
+    mp->wf_host.assign((size_t)H.B, 0.0);
+    fitb::upload(mp->exc, mp->exc_host);
+    fitb::upload(mp->buflen, mp->buflen_host);
+    fitb::upload(mp->wf, mp->wf_host);
+    md.port_e = mp->port_e.as<long long>();
+    md.int_e = mp->int_e.as<long long>();
+    md.port_h = mp->port_h.as<long long>();
+    md.me_port = mp->me_port.as<double>();
+    md.me_int = mp->me_int.as<double>();
+    md.mh_port = mp->mh_port.as<double>();
+    md.eprof = mp->eprof.as<double>();
+    md.vprof = mp->vprof.as<double>();
+    md.hprof = mp->hprof.as<double>();
+    md.comp_r = mp->comp_r.as<double>();
+    md.comp_live = mp->comp_live.as<double>();
+    md.st = mp->st.as<double>();
+    md.comp_state = mp->comp_state.as<double>();
+    md.scratch = mp->scratch.as<double>();
+    md.exc_mode = mp->exc.as<int>();
+    md.wf = mp->wf.as<double>();
+    md.n_wf = 1;
+    md.buf_len = mp->buflen.as<int>();
+    md.channel0 = H.nch;
+    H.nch += M;
+    if (out_id) *out_id = (int32_t)H.modal.size();
+    // history buffers are (re)allocated by ensure_capacity
+    long long want = std::max<long long>(H.cap, d->max_steps > 0 ? d->max_steps : 1024);
+    H.modal.push_back(std::move(mp));
+    H.cap = 0;
+    H.recV.release();
+    H.recI.release();
+    for (auto& other : H.modal) {
+        other->whist.release();
+        other->shist.release();
+    }
+    fitb::ensure_capacity(H, want);
+    H.port_tables_dirty = true;
+    fitb::invalidate_graphs(H);
+    FITB_CATCH
+}
+
+int fitb_set_dtbc_kernel(fitb_handle* h, int32_t port, int32_t mode, int32_t n_kernel, const double* l) {
+    FITB_TRY
+    Handle& H = H_of(h);
+    if (port < 0 || port >= (int)H.modal.size()) fail(FITB_ERR_ARG, "modal port %d does not exist", port);
+    fitb::ModalHost& mp = *H.modal[port];
+    if (mode < 0 || mode >= mp.n_modes || !mp.dev.is_dtbc[mode]) fail(FITB_ERR_ARG, "mode %d is not a DTBC mode", mode);
+    if (!l) fail(FITB_ERR_ARG, "null kernel");
+    // Tables are appended in order n0, 2 n0, 4 n0, ...
+    long long expect = (long long)mp.dev.n0 << mp.n_tables_mode[(size_t)mode];
+    if (n_kernel != expect) fail(FITB_ERR_ARG, "expected the DTBC table of length %lld next, got %d", expect, n_kernel);
+    auto& tab = mp.ktabs[(size_t)mode];
+    tab.insert(tab.end(), l, l + n_kernel);
+    mp.n_tables_mode[(size_t)mode] += 1;
+    fitb::upload(mp.ktab[mode], tab);
+    mp.dev.ktab[mode] = mp.ktab[mode].as<double>();
+    mp.dev.n_tables = *std::max_element(mp.n_tables_mode.begin(), mp.n_tables_mode.end());
+    H.port_tables_dirty = true;
+    fitb::invalidate_graphs(H);
+    FITB_CATCH
+}
+
+int fitb_set_modal_source(fitb_handle* h, int32_t port, int32_t b, int32_t mode, int64_t n_samples, const double* w) {
+    FITB_TRY
+    Handle& H = H_of(h);
+    if (port < 0 || port >= (int)H.modal.size()) fail(FITB_ERR_ARG, "modal port %d does not exist", port);
+    if (b < 0 || b >= H.B) fail(FITB_ERR_ARG, "field set %d out of range", b);
+    fitb::ModalHost& mp = *H.modal[port];
+    if (mode < -1 || mode >= mp.n_modes) fail(FITB_ERR_ARG, "mode_idx %d out of range [0, %d)", mode, mp.n_modes);
+    if (mode >= 0 && (n_samples < 1 || !w)) fail(FITB_ERR_ARG, "excitation needs waveform samples");
+    mp.exc_host[(size_t)b] = mode;
+    if (mode >= 0) {
+        // set_excitation: buf_len = max(ceil((tau + dt) / dt) + 3, 5)
+        double tau = mp.dev.tau[mode];
+        int bl = (int)std::ceil((tau + H.dt) / H.dt) + 3;
+        mp.buflen_host[(size_t)b] = std::max(bl, 5);
+        long long n_old = mp.n_wf, n_new = std::max<long long>(n_old, n_samples);
+        std::vector<double> tab((size_t)(H.B * n_new), 0.0);
+        for (int q = 0; q < H.B; ++q)
+            for (long long t = 0; t < n_old; ++t) tab[(size_t)(q * n_new + t)] = mp.wf_host[(size_t)(q * n_old + t)];
+        for (long long t = 0; t < n_new; ++t) tab[(size_t)(b * n_new + t)] = t < n_samples ? w[t] : 0.0;
+        mp.wf_host = tab;
+        mp.n_wf = n_new;
+        fitb::upload(mp.wf, tab);
+        mp.dev.wf = mp.wf.as<double>();
+        mp.dev.n_wf = n_new;
+    }
+    fitb::upload(mp.exc, mp.exc_host);
+    fitb::upload(mp.buflen, mp.buflen_host);
+    mp.dev.exc_mode = mp.exc.as<int>();
+    mp.dev.buf_len = mp.buflen.as<int>();
+    H.port_tables_dirty = true;
+    fitb::invalidate_graphs(H);
+    FITB_CATCH
+}
+
+int fitb_add_dft_monitor(fitb_handle* h, const fitb_dft_desc* d, int32_t* out_id) {
+    FITB_TRY
+    Handle& H = H_of(h);
+    if (!d || !d->freqs || !d->dx || !d->dy || !d->dz) fail(FITB_ERR_ARG, "null monitor argument");
+    if (d->n_freq < 1) fail(FITB_ERR_ARG, "freqs must be a non-empty 1D array");
+    if (d->stride < 1) fail(FITB_ERR_ARG, "stride must be >= 1");
+    if (!(0 <= d->i0 && d->i0 < d->i1 && d->i1 <= H.g.nx && 0 <= d->j0 && d->j0 < d->j1 && d->j1 <= H.g.ny &&
+          0 <= d->k0 && d->k0 < d->k1 && d->k1 <= H.g.nz))
+        fail(FITB_ERR_ARG, "monitor box outside the grid");
+    if ((d->comp_mask & 63) == 0) fail(FITB_ERR_ARG, "monitor records no component");
+    if (H.steps_done != 0) fail(FITB_ERR_STATE, "monitors must be added before the first step");
+    auto m = std::make_unique<fitb::DftHost>();
+    fitb::DftDev& dv = m->dev;
+    dv.i0 = d->i0;
+    dv.j0 = d->j0;
+    dv.k0 = d->k0;
+    dv.ni = d->i1 - d->i0;
+    dv.nj = d->j1 - d->j0;
+    dv.nk = d->k1 - d->k0;
+    dv.ncell = (long long)dv.ni * dv.nj * dv.nk;
+    dv.ncomp = 0;
+    for (int c = 0; c < 6; ++c)
+        if (d->comp_mask & (1 << c)) dv.comps[dv.ncomp++] = c;
+    dv.nf = d->n_freq;
+    dv.stride = d->stride;
+    dv.kahan = d->kahan ? 1 : 0;
+    int K = (int)(49152 / (16 * (long long)dv.nf));
+    dv.K = std::max(1, std::min(32, K));
+    dv.dt = H.dt;
+    std::vector<double> om((size_t)dv.nf);
+    for (int f = 0; f < dv.nf; ++f) om[(size_t)f] = 2.0 * M_PI * d->freqs[f];
+    fitb::upload(m->omega, om);
+    int ld = std::max(H.g.nx, std::max(H.g.ny, H.g.nz)) + 1;
+    dv.inv_ld = ld;
+    std::vector<double> inv((size_t)(3 * ld), 1.0), dual((size_t)(3 * ld), 1.0);
+    const double* ds[3] = {d->dx, d->dy, d->dz};
+    const int ns[3] = {H.g.nx, H.g.ny, H.g.nz};
+    for (int a = 0; a < 3; ++a) {
+        const int n = ns[a];
+        for (int q = 0; q < n; ++q) inv[(size_t)(a * ld + q)] = ds[a][q];
+        // solver dual widths: boundary = full end cell (monitors/base.py:31-48)
+        dual[(size_t)(a * ld)] = ds[a][0];
+        for (int q = 1; q < n; ++q) dual[(size_t)(a * ld + q)] = 0.5 * (ds[a][q - 1] + ds[a][q]);
+        dual[(size_t)(a * ld + n)] = ds[a][n - 1];
+    }
+    fitb::upload(m->inv, inv);
+    fitb::upload(m->dual, dual);
+    m->stage.alloc(sizeof(float) * (size_t)H.B * dv.K * dv.ncomp * dv.ncell);
+    m->wst.alloc(sizeof(float2) * (size_t)dv.K * 2 * dv.nf);
+    m->bins.alloc(sizeof(float2) * (size_t)H.B * dv.ncomp * dv.nf * dv.ncell);
+    m->cmp.alloc(sizeof(float2) * (size_t)H.B * dv.ncomp * dv.nf * dv.ncell);
+    m->base.alloc(sizeof(long long));
+    dv.omega = m->omega.as<double>();
+    dv.inv = m->inv.as<double>();
+    dv.dual = m->dual.as<double>();
+    dv.stage = m->stage.as<float>();
+    dv.wst = m->wst.as<float2>();
+    dv.bins = m->bins.as<float2>();
+    dv.cmp = m->cmp.as<float2>();
+    dv.base = m->base.as<long long>();
+    m->i0 = d->i0; m->i1 = d->i1; m->j0 = d->j0; m->j1 = d->j1; m->k0 = d->k0; m->k1 = d->k1;
+    if (out_id) *out_id = (int32_t)H.dft.size();
+    H.dft.push_back(std::move(m));
+    fitb::invalidate_graphs(H);
+    FITB_CATCH
+}
+
+int fitb_read_dft(fitb_handle* h, int32_t mon, int32_t b, int32_t comp, double* re, double* im, size_t count) {
+    FITB_TRY
+    Handle& H = H_of(h);
+    if (mon < 0 || mon >= (int)H.dft.size()) fail(FITB_ERR_ARG, "monitor %d does not exist", mon);
+    if (b < 0 || b >= H.B) fail(FITB_ERR_ARG, "field set %d out of range", b);
+    fitb::DftHost& m = *H.dft[mon];
+    int ci = -1;
+    for (int q = 0; q < m.dev.ncomp; ++q)
+        if (m.dev.comps[q] == comp) ci = q;
+    if (ci < 0) fail(FITB_ERR_ARG, "monitor %d does not record component %d", mon, comp);
+    size_t n = (size_t)m.dev.nf * m.dev.ncell;
+    if (count != n || !re || !im) fail(FITB_ERR_ARG, "expected %zu bins", n);
+    fitb::dft_flush_pending(H);
+    std::vector<float2> bins(n);
+    size_t off = ((size_t)b * m.dev.ncomp + ci) * n;
+    ck(cudaMemcpy(bins.data(), m.bins.as<float2>() + off, n * sizeof(float2), cudaMemcpyDeviceToHost), "read bins");
+    for (size_t q = 0; q < n; ++q) {
+        re[q] = bins[q].x;
+        im[q] = bins[q].y;
+    }
+    FITB_CATCH
+}
+
+int fitb_step(fitb_handle* h, int64_t n_steps) {
+    FITB_TRY
+    Handle& H = H_of(h);
+    fitb::run_steps(H, n_steps);
+    ck(cudaGetLastError(), "step launch");
+    FITB_CATCH
+}
+
+int fitb_step_timed(fitb_handle* h, int64_t n_steps, double* ms) {
+    FITB_TRY
+    Handle& H = H_of(h);
+    if (!ms) fail(FITB_ERR_ARG, "null argument");
+    cudaEvent_t a, b;
+    ck(cudaEventCreate(&a), "event");
+    ck(cudaEventCreate(&b), "event");
+    try {
+        // prepare graphs / capacity outside the bracket
+        fitb::run_steps(H, 0);
+        ck(cudaEventRecord(a, H.stream), "event record");
+        fitb::run_steps(H, n_steps);
+        ck(cudaEventRecord(b, H.stream), "event record");
+        ck(cudaEventSynchronize(b), "event sync");
+        float f = 0.f;
+        ck(cudaEventElapsedTime(&f, a, b), "elapsed");
+        *ms = f;
+    } catch (...) {
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+        throw;
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    FITB_CATCH
+}
+
+int fitb_time_stencil(fitb_handle* h, int32_t n_iter, double* ms_e, double* ms_h) {
+    FITB_TRY
+    Handle& H = H_of(h);
+    fitb::check_ready(H);
+    if (n_iter < 1 || !ms_e || !ms_h) fail(FITB_ERR_ARG, "bad argument");
+    cudaEvent_t ev[3];
+    for (auto& x : ev) ck(cudaEventCreate(&x), "event");
+    ck(cudaEventRecord(ev[0], H.stream), "event record");
+    for (int q = 0; q < n_iter; ++q) {
+        if (H.prec == 4) fitb::launch_update_E<float>(fitb::stencil_args<float>(H), H.stream);
+        else fitb::launch_update_E<double>(fitb::stencil_args<double>(H), H.stream);
+    }
+    ck(cudaEventRecord(ev[1], H.stream), "event record");
+    for (int q = 0; q < n_iter; ++q) {
+        if (H.prec == 4) fitb::launch_update_H<float>(fitb::stencil_args<float>(H), H.stream);
+        else fitb::launch_update_H<double>(fitb::stencil_args<double>(H), H.stream);
+    }
+    ck(cudaEventRecord(ev[2], H.stream), "event record");
+    ck(cudaEventSynchronize(ev[2]), "event sync");
+    H.launches += 2LL * n_iter;
+    float f1 = 0.f, f2 = 0.f;
+    ck(cudaEventElapsedTime(&f1, ev[0], ev[1]), "elapsed");
+    ck(cudaEventElapsedTime(&f2, ev[1], ev[2]), "elapsed");
+    for (auto& x : ev) cudaEventDestroy(x);
+    *ms_e = f1 / n_iter;
+    *ms_h = f2 / n_iter;
+    FITB_CATCH
+}
+
+int fitb_sync(fitb_handle* h) {
+    FITB_TRY
+    Handle& H = H_of(h);
+    ck(cudaStreamSynchronize(H.stream), "sync");
+    FITB_CATCH
+}
+
+int fitb_steps_done(fitb_handle* h, int64_t* out) {
+    FITB_TRY
+    Handle& H = H_of(h);
+    if (!out) fail(FITB_ERR_ARG, "null argument");
+    *out = H.steps_done;
+    FITB_CATCH
+}
+
+int fitb_energy(fitb_handle* h, int32_t b, double* out) {
+    FITB_TRY
+    Handle& H = H_of(h);
+    if (b < 0 || b >= H.B || !out) fail(FITB_ERR_ARG, "bad argument");
+    if (H.prec == 4)
+        fitb::energy_impl<float>(H, b, out);
+    else
+        fitb::energy_impl<double>(H, b, out);
+    FITB_CATCH
+}
+
+int fitb_poll_signal_absmax(fitb_handle* h, int32_t b, double* out) {
+    FITB_TRY
+    Handle& H = H_of(h);
+    if (b < 0 || b >= H.B || !out) fail(FITB_ERR_ARG, "bad argument");
+    ck(cudaMemcpyAsync(out, H.absmax.as<double>() + b, sizeof(double), cudaMemcpyDeviceToHost, H.stream), "absmax");
+    ck(cudaMemsetAsync(H.absmax.as<double>() + b, 0, sizeof(double), H.stream), "absmax reset");
+    ck(cudaStreamSynchronize(H.stream), "absmax sync");
+    FITB_CATCH
+}
+
+int fitb_channel_count(fitb_handle* h, int32_t* out) {
+    FITB_TRY
+    Handle& H = H_of(h);
+    if (!out) fail(FITB_ERR_ARG, "null argument");
+    *out = H.nch;
+    FITB_CATCH
+}
+
+int fitb_read_vi(fitb_handle* h, int32_t b, int64_t step0, int64_t n, double* V, double* I) {
+    FITB_TRY
+    Handle& H = H_of(h);
+    if (b < 0 || b >= H.B) fail(FITB_ERR_ARG, "field set %d out of range", b);
+    if (step0 < 0 || n < 0 || step0 + n > H.steps_done) fail(FITB_ERR_ARG, "steps [%lld, %lld) not recorded", (long long)step0, (long long)(step0 + n));
+    if (H.nch == 0 || n == 0) return FITB_OK;
+    ck(cudaStreamSynchronize(H.stream), "sync");
+    size_t off = ((size_t)b * H.cap + step0) * H.nch;
+    size_t cnt = (size_t)n * H.nch;
+    if (V) ck(cudaMemcpy(V, H.recV.as<double>() + off, cnt * sizeof(double), cudaMemcpyDeviceToHost), "read V");
+    if (I) ck(cudaMemcpy(I, H.recI.as<double>() + off, cnt * sizeof(double), cudaMemcpyDeviceToHost), "read I");
+    FITB_CATCH
+}
+
+int fitb_state_size(fitb_handle* h, size_t* out) {
+    FITB_TRY
+    Handle& H = H_of(h);
+    if (!out) fail(FITB_ERR_ARG, "null argument");
+    fitb::Writer w;
+    if (H.prec == 4)
+        fitb::write_state<float>(H, w);
+    else
+        fitb::write_state<double>(H, w);
+    *out = w.n;
+    FITB_CATCH
+}
+
+int fitb_state_export(fitb_handle* h, void* buf, size_t len) {
+    FITB_TRY
+    Handle& H = H_of(h);
+    if (!buf) fail(FITB_ERR_ARG, "null buffer");
+    ck(cudaStreamSynchronize(H.stream), "sync");
+    fitb::dft_flush_pending(H);
+    std::vector<char> out;
+    fitb::Writer w;
+    w.out = &out;
+    if (H.prec == 4)
+        fitb::write_state<float>(H, w);
+    else
+        fitb::write_state<double>(H, w);
+    if (out.size() != len) fail(FITB_ERR_ARG, "state buffer is %zu bytes, expected %zu", len, out.size());
+    memcpy(buf, out.data(), out.size());
+    FITB_CATCH
+}
+
+int fitb_state_import(fitb_handle* h, const void* buf, size_t len) {
+    FITB_TRY
+    Handle& H = H_of(h);
+    if (!buf) fail(FITB_ERR_ARG, "null buffer");
+    ck(cudaStreamSynchronize(H.stream), "sync");
+    fitb::Reader r{(const char*)buf, len};
+    if (H.prec == 4)
+        fitb::read_state<float>(H, r);
+    else
+        fitb::read_state<double>(H, r);
+    if (r.left != 0) fail(FITB_ERR_ARG, "state buffer has %zu trailing bytes", r.left);
+    fitb::invalidate_graphs(H);
+    H.port_tables_dirty = true;
+    FITB_CATCH
+}
+
+}  // extern "C"

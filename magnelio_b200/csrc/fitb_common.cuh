@@ -1,0 +1,216 @@
+// Shared device-side definitions of the FIT-TD engine: the padded field
+// layout, the per-feature device descriptors, and the launcher prototypes
+// implemented in stencil.cu, ports.cu and monitors.cu.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace fitb {
+
+// ---------------------------------------------------------------------------
+// Padded uniform layout.
+//
+// Every one of the six Yee components (and every coefficient array) is
+// stored in one common padded box indexed (i, j, k), k fastest:
+//   i in [-1, nx+1]  (one zero guard plane on each side),
+//   j in [0, njp)    with njp = ny + 2,
+//   k in [0, nkp)    with nkp = round_up(nz + 2, 4).
+// A component occupies the sub-box of its reference shape; every other
+// entry is a pad that holds +0 forever (its update coefficients are 0).
+// Consequences used by the kernels:
+//   * the reference's conditional dual curl ("a missing H neighbour counts
+//     as 0", numba_kernels.py:51-58) becomes a plain 4-term stencil, since
+//     index j-1 = -1 lands in the previous plane's pad row j = ny+1 and
+//     k-1 = -1 in the previous row's pad tail k >= nz+1;
+//   * every row starts on a 16-byte boundary (nkp is a multiple of 4).
+// ---------------------------------------------------------------------------
+struct Geom {
+    int nx, ny, nz;
+    int njp, nkp;
+    long long si, sj;  // plane and row strides (elements); sk = 1
+    long long vol;     // elements of one padded component
+};
+
+__host__ __device__ __forceinline__ long long pidx(const Geom& g, int i, int j, int k) {
+    return (long long)(i + 1) * g.si + (long long)j * g.sj + (long long)k;
+}
+
+// One CPML face as the stencil kernels see it.  The psi state of all four
+// auxiliary components lives in a uniform slab of dims (dI, dJ, dK) =
+// (nx+1, ny+1, nz+1) with the face axis replaced by the layer count n.
+struct FaceDev {
+    int axis;       // 0 = x, 1 = y, 2 = z
+    int lo;         // first layer index along the axis
+    int n;          // layer count
+    int dI, dJ, dK; // slab dims
+    long long slab; // dI * dJ * dK
+    void* psi;      // [B][4][slab] field dtype: E1, E2, H1, H2
+    const unsigned char* air;  // [4][slab] 0/1
+    const void* bcc;           // [3][n] field dtype: b, c, ck
+};
+
+constexpr int kMaxFaces = 6;
+
+template <typename T>
+struct StencilArgs {
+    Geom g;
+    int B;
+    T* e;  // [B][3][vol]
+    T* h;  // [B][3][vol]
+    const T* aE;
+    const T* bE;  // [3][vol]
+    const T* aH;
+    const T* bH;  // [3][vol]
+    int nfaces;
+    FaceDev f[kMaxFaces];
+    int ichunk;  // planes per CTA along i
+};
+
+template <typename T>
+void launch_update_E(const StencilArgs<T>& a, cudaStream_t s);
+template <typename T>
+void launch_update_H(const StencilArgs<T>& a, cudaStream_t s);
+
+// ---------------------------------------------------------------------------
+// Lumped ports (Thevenin element with a series R-L-C companion).
+// ---------------------------------------------------------------------------
+struct LumpedDev {
+    int n_edges;
+    const long long* off;   // [n_edges] offset into the field set's E block
+    const double* sign;     // [n_edges]
+    const double* beta;     // [n_edges]
+    double beta_sum;
+    double R, L, C;         // < 0: absent
+    double rec_scale;
+    const double* src;      // [B][n_src]
+    long long n_src;
+    double* st;             // [B][4]: i_prev, vL, vC, last_I
+    int channel;            // recorder channel
+};
+
+// ---------------------------------------------------------------------------
+// Modal ports (projection, modal Mur / TF-SF, exact DTBC, reconstruction,
+// complement absorber, V/I recording).
+// ---------------------------------------------------------------------------
+constexpr int kMaxModes = 16;
+
+struct ModalDev {
+    int n_modes;
+    int n_e, n_e_u;   // port-plane E samples (u + v), u count
+    int n_h, n_h_u;
+    const long long* port_e;  // [n_e] offsets into the E block
+    const long long* int_e;   // [n_e]
+    const long long* port_h;  // [n_h] offsets into the H block
+    const double* me_port;    // [n_e]
+    const double* me_int;     // [n_e]
+    const double* mh_port;    // [n_h]
+    const double* eprof;      // [M][n_e]
+    const double* vprof;      // [M][n_e]
+    const double* hprof;      // [M][n_h]
+    double mur_r[kMaxModes];
+    double tau[kMaxModes];
+    double rec_scale[kMaxModes];
+    int is_dtbc[kMaxModes];
+    double r2[kMaxModes], q2[kMaxModes];
+    // DTBC kernels: per mode, the concatenation of the tables of length
+    // n0, 2 n0, 4 n0, ... (n_tables of them).
+    const double* ktab[kMaxModes];
+    int n0;
+    int n_tables;
+    int comp_on;
+    const double* comp_r;     // [n_e]
+    const double* comp_live;  // [n_e]
+    // per field set state and sources
+    double* st;               // [B][ST_SIZE] scalars (see ports.cu)
+    double* whist;            // [B][M][cap]
+    double* shist;            // [B][M][cap]
+    double* comp_state;       // [B][2][n_e] complement int_prev, port_prev
+    double* scratch;          // [B][2][n_e] gathered interior samples, new plane values
+    const int* exc_mode;      // [B] excited mode or -1
+    const double* wf;         // [B][n_wf] waveform(n dt)
+    long long n_wf;
+    const int* buf_len;       // [B] TF/SF source buffer length
+    long long cap;            // history capacity (steps)
+    int channel0;             // first recorder channel
+    double dt;
+};
+
+struct RecorderDev {
+    double* V;  // [B][cap][nch]
+    double* I;  // [B][cap][nch]
+    int nch;
+    long long cap;
+};
+
+struct PortsArgs {
+    int B;
+    long long e_block;  // elements per field set (3 * vol)
+    long long h_block;
+    const long long* step;  // device step counter (completed steps)
+    double dt_lumped;       // solver time step
+    RecorderDev rec;
+    double* absmax;  // [B]
+};
+
+template <typename T>
+void launch_lumped(T* e, const PortsArgs& pa, const LumpedDev* d, int n_lumped, cudaStream_t s);
+template <typename T>
+void launch_modal(T* e, const T* h, const PortsArgs& pa, const ModalDev* d, int n_modal,
+                  cudaStream_t s);
+
+// ---------------------------------------------------------------------------
+// Running-DFT monitors, staged in blocks of K recorded samples.
+// ---------------------------------------------------------------------------
+struct DftDev {
+    int i0, j0, k0, ni, nj, nk;
+    long long ncell;
+    int ncomp;
+    int comps[6];
+    int nf;
+    const double* omega;  // [nf]
+    int stride;
+    int kahan;
+    int K;
+    const long long* base;  // device: first step from which slots are counted
+    const double* inv;    // [3][max(nx,ny,nz)+1] primal widths dx,dy,dz and
+    const double* dual;   // [3][max+1] solver dual widths
+    int inv_ld;           // leading dimension of inv/dual
+    float* stage;         // [B][K][ncomp][ncell]
+    float2* wst;          // [K][2][nf] phasor weights (E time, H time)
+    float2* bins;         // [B][ncomp][nf][ncell]
+    float2* cmp;          // Kahan compensation, same shape
+    double dt;
+};
+
+template <typename T>
+void launch_dft_stage(const T* e, const T* h, long long e_block, long long h_block, const Geom& g,
+                      int B, const DftDev& d, const long long* step, cudaStream_t s);
+void launch_dft_flush(int B, const DftDev& d, const long long* step, int forced_count,
+                      cudaStream_t s);
+
+// Energy: per field set 0.5 (sum m_eps e^2 + sum m_mu h^2) in float64.
+template <typename T>
+void launch_energy(const T* e, const T* h, const T* meps, const T* mmu, const Geom& g, int b,
+                   long long e_block, double* partials, int nblocks, double* out,
+                   cudaStream_t s);
+
+void launch_advance(long long* step, cudaStream_t s);
+
+// Layout conversion between the reference flat layout and the padded box.
+template <typename T>
+void launch_pack(const T* flat, T* padded, const Geom& g, int comp, long long flat_off,
+                 cudaStream_t s);
+template <typename T>
+void launch_unpack(const T* padded, T* flat, const Geom& g, int comp, long long flat_off,
+                   cudaStream_t s);
+
+// Reference shapes of component c (0..5 = Ex,Ey,Ez,Hx,Hy,Hz).
+__host__ __device__ __forceinline__ void comp_shape(const Geom& g, int c, int& ni, int& nj,
+                                                    int& nk) {
+    ni = g.nx + ((c == 1 || c == 2 || c == 3) ? 1 : 0);
+    nj = g.ny + ((c == 0 || c == 2 || c == 4) ? 1 : 0);
+    nk = g.nz + ((c == 0 || c == 1 || c == 5) ? 1 : 0);
+}
+
+}  // namespace fitb

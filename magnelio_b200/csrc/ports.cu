@@ -1,0 +1,274 @@
+// Port terminations on the device, run between the E and H updates.
+//
+// Lumped ports: LumpedElementOperator.update_e
+//   (src/magnelio/ports/_lumped/operator.py:134-166) with the series R-L-C
+//   trapezoidal companion (src/magnelio/circuit/companion.py SeriesRLC).
+// Modal ports: PortOperatorModal.update_e
+//   (src/magnelio/ports/_modal/operator.py:1351-1536): interior-plane
+//   projection, modal Mur-1 / TF-SF, the exact DTBC chain step
+//   (src/magnelio/ports/_modal/dtbc.py:417-463), modal reconstruction of the
+//   port plane, the complement absorber, then the V/I samples the recorder
+//   takes right after update_e (src/magnelio/ports/recorder.py:216-252).
+// All port arithmetic is float64, as in the reference; only the field
+// gathers/scatters touch the field dtype.
+#include "fitb_common.cuh"
+
+namespace fitb {
+
+namespace {
+
+constexpr int kPortThreads = 512;
+
+__device__ __forceinline__ void atomic_max_nonneg(double* addr, double v) {
+    // Non-negative doubles order like their bit patterns.
+    atomicMax(reinterpret_cast<unsigned long long*>(addr), (unsigned long long)__double_as_longlong(v));
+}
+
+// Block-wide sum of `n` per-thread values; result valid in red[m] for all
+// threads after return.  red must hold kMaxModes * 2 doubles; warp partials
+// use wred [32][kMaxModes*2].
+template <int NV>
+__device__ void block_sum(double (&v)[NV], int n, double* red, double (*wred)[NV]) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int nwarps = blockDim.x >> 5;
+    for (int m = 0; m < n; ++m) {
+        double x = v[m];
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+        if (lane == 0) wred[warp][m] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x < n) {
+        double acc = 0.0;
+        for (int w = 0; w < nwarps; ++w) acc += wred[w][threadIdx.x];
+        red[threadIdx.x] = acc;
+    }
+    __syncthreads();
+}
+
+template <typename T>
+__global__ void k_lumped(T* __restrict__ e, PortsArgs pa, const LumpedDev* __restrict__ ports) {
+    const LumpedDev& d = ports[blockIdx.x];
+    const int b = blockIdx.y;
+    if (threadIdx.x != 0) return;
+    const long long n = *pa.step;
+    T* E = e + (long long)b * pa.e_block;
+    double v_total = 0.0;
+    for (int q = 0; q < d.n_edges; ++q) v_total += d.sign[q] * (double)E[d.off[q]];
+    const double v_src = (n < d.n_src) ? d.src[(long long)b * d.n_src + n] : 0.0;
+    double* st = d.st + 4 * b;
+    const double dt = pa.dt_lumped;
+    const double i_prev = st[0];
+    double r_eq = (d.R >= 0.0) ? d.R : 0.0;
+    if (d.L >= 0.0) r_eq += 2.0 * d.L / dt;
+    if (d.C >= 0.0) r_eq += dt / (2.0 * d.C);
+    double v_hist = 0.0;
+    if (d.L >= 0.0) v_hist += -(2.0 * d.L / dt) * i_prev - st[1];
+    if (d.C >= 0.0) v_hist += st[2] + (dt / (2.0 * d.C)) * i_prev;
+    const double z_eff = r_eq + d.beta_sum;
+    const double i_port = (v_src - v_hist - v_total) / z_eff;
+    for (int q = 0; q < d.n_edges; ++q) {
+        const long long o = d.off[q];
+        E[o] = (T)((double)E[o] + d.sign[q] * d.beta[q] * i_port);
+    }
+    if (d.L >= 0.0) st[1] = (2.0 * d.L / dt) * (i_port - i_prev) - st[1];
+    if (d.C >= 0.0) st[2] = st[2] + (dt / (2.0 * d.C)) * (i_port + i_prev);
+    st[0] = i_port;
+    st[3] = i_port;
+    // Recorder: V re-projected from the corrected field, I = cached current.
+    double v = 0.0;
+    for (int q = 0; q < d.n_edges; ++q) v += d.sign[q] * (double)E[d.off[q]];
+    const long long r = ((long long)b * pa.rec.cap + n) * pa.rec.nch + d.channel;
+    pa.rec.V[r] = v * d.rec_scale;
+    pa.rec.I[r] = i_port * d.rec_scale;
+}
+
+// _interp_delayed (operator.py:1539-1562) on the source history
+// wf[0..n+1], whose deque holds the last `maxlen` samples.
+__device__ __forceinline__ double interp_delayed(const double* wf, long long n_wf, long long n,
+                                                 int maxlen, double delay, double dt) {
+    const long long len = min(n + 1, (long long)maxlen);
+    const double idx_frac = delay / dt;
+    const long long i0 = (long long)floor(idx_frac);
+    const double alpha = idx_frac - (double)i0;
+    if (len - 1 - i0 < 0) return 0.0;
+    const long long t0 = n + 1 - i0;
+    const double v0 = (t0 >= 0 && t0 < n_wf) ? wf[t0] : 0.0;
+    double v1 = 0.0;
+    if (len - 2 - i0 >= 0) {
+        const long long t1 = n - i0;
+        v1 = (t1 >= 0 && t1 < n_wf) ? wf[t1] : 0.0;
+    }
+    return (1.0 - alpha) * v0 + alpha * v1;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kPortThreads)
+    k_modal(T* __restrict__ e, const T* __restrict__ h, PortsArgs pa,
+            const ModalDev* __restrict__ ports) {
+    const ModalDev& d = ports[blockIdx.x];
+    const int b = blockIdx.y;
+    const long long n = *pa.step;
+    const int M = d.n_modes, ne = d.n_e, nh = d.n_h;
+    T* E = e + (long long)b * pa.e_block;
+    const T* H = h + (long long)b * pa.h_block;
+    double* st = d.st + (long long)b * 4 * kMaxModes;
+    double* Vport_prev = st;
+    double* Vint_prev = st + kMaxModes;
+    double* u = st + 2 * kMaxModes;
+    double* u_prev = st + 3 * kMaxModes;
+    double* eint = d.scratch + (long long)b * 2 * ne;
+    double* enew = eint + ne;
+
+    __shared__ double red[2 * kMaxModes];
+    __shared__ double wred[kPortThreads / 32][2 * kMaxModes];
+    __shared__ double s_vint[kMaxModes];
+    __shared__ double s_vc[kMaxModes];
+
+    // 1. Interior-plane projection V_int_new[m] = sum me_int * (p_m * e_int).
+    double acc[2 * kMaxModes];
+    for (int m = 0; m < 2 * kMaxModes; ++m) acc[m] = 0.0;
+    for (int p = threadIdx.x; p < ne; p += blockDim.x) {
+        const double v = (double)E[d.int_e[p]];
+        eint[p] = v;
+        const double me = d.me_int[p];
+        for (int m = 0; m < M; ++m) acc[m] += me * (d.vprof[(long long)m * ne + p] * v);
+    }
+    block_sum<2 * kMaxModes>(acc, M, red, wred);
+    if (threadIdx.x < M) s_vint[threadIdx.x] = red[threadIdx.x];
+    __syncthreads();
+
+    // 2. DTBC boundary convolutions: conv_w = sum_{m=1..n} l_m w[n-m],
+    //    u_inc = sum l_m s[n-m] with the kernel table in effect at chain
+    //    step n (auto-extended by doubling, dtbc.py:351-363).
+    long long tlen = d.n0;
+    long long toff = 0;
+    while (tlen < n + 1) {
+        toff += tlen;
+        tlen *= 2;
+    }
+    const int exc = d.exc_mode[b];
+    for (int m = 0; m < 2 * kMaxModes; ++m) acc[m] = 0.0;
+    for (int m = 0; m < M; ++m) {
+        if (!d.is_dtbc[m]) continue;
+        const double* lt = d.ktab[m] + toff;
+        const double* wh = d.whist + ((long long)b * M + m) * d.cap;
+        const double* sh = d.shist + ((long long)b * M + m) * d.cap;
+        double aw = 0.0, as = 0.0;
+        for (long long i = threadIdx.x; i < n; i += blockDim.x) {
+            const double l = lt[n - i];
+            aw += l * wh[i];
+            as += l * sh[i];
+        }
+        acc[2 * m] = aw;
+        acc[2 * m + 1] = as;
+    }
+    block_sum<2 * kMaxModes>(acc, 2 * M, red, wred);
+
+    // 3. Per-mode boundary value (one thread; scalar float64 recursions).
+    if (threadIdx.x == 0) {
+        const double* wf = d.wf + (long long)b * d.n_wf;
+        for (int m = 0; m < M; ++m) {
+            const double vin = s_vint[m];
+            double vc = Vint_prev[m] + d.mur_r[m] * (vin - Vport_prev[m]);
+            if (m == exc && !d.is_dtbc[m]) {
+                const long long t1 = n + 1;
+                const double src_new = (t1 < d.n_wf) ? wf[t1] : 0.0;
+                const int maxlen = d.buf_len[b];
+                const double inc_int_now = interp_delayed(wf, d.n_wf, n, maxlen, d.tau[m], d.dt);
+                const double inc_int_prev =
+                    interp_delayed(wf, d.n_wf, n, maxlen, d.tau[m] + d.dt, d.dt);
+                const double inc_face_prev = interp_delayed(wf, d.n_wf, n, maxlen, d.dt, d.dt);
+                const double scat_int_now = vin - inc_int_now;
+                const double scat_int_prev = Vint_prev[m] - inc_int_prev;
+                const double scat_face_prev = Vport_prev[m] - inc_face_prev;
+                vc = src_new + scat_int_prev + d.mur_r[m] * (scat_int_now - scat_face_prev);
+            }
+            if (d.is_dtbc[m]) {
+                const double src = (m == exc && n < d.n_wf) ? wf[n] : 0.0;
+                const double conv_w = red[2 * m], u_inc = red[2 * m + 1];
+                const double ghost = src + conv_w;
+                double* wh = d.whist + ((long long)b * M + m) * d.cap;
+                double* sh = d.shist + ((long long)b * M + m) * d.cap;
+                wh[n] = u[m] - u_inc;
+                sh[n] = src;
+                double un = (2.0 - 2.0 * d.r2[m] - d.q2[m]) * u[m];
+                un = un - u_prev[m];
+                un = un + d.r2[m] * (ghost + Vint_prev[m]);
+                u_prev[m] = u[m];
+                u[m] = un;
+                vc = un;
+            }
+            s_vc[m] = vc;
+        }
+    }
+    __syncthreads();
+
+    // 4. Reconstruct the port plane from the modal expansion (+ complement).
+    for (int p = threadIdx.x; p < ne; p += blockDim.x) {
+        double v = 0.0;
+        for (int m = 0; m < M; ++m) v += s_vc[m] * d.eprof[(long long)m * ne + p];
+        if (d.comp_on) {
+            double* cs = d.comp_state + (long long)b * 2 * ne;
+            double ci = eint[p];
+            for (int m = 0; m < M; ++m) ci -= s_vint[m] * d.eprof[(long long)m * ne + p];
+            const double cp = d.comp_live[p] * (cs[p] + d.comp_r[p] * (ci - cs[ne + p]));
+            v += cp;
+            cs[p] = ci;
+            cs[ne + p] = cp;
+        }
+        enew[p] = v;
+        E[d.port_e[p]] = (T)v;
+    }
+    __syncthreads();
+
+    // 5. Recorder samples: V from the corrected port plane, I from h^{n+1/2}.
+    for (int m = 0; m < 2 * kMaxModes; ++m) acc[m] = 0.0;
+    for (int p = threadIdx.x; p < ne; p += blockDim.x) {
+        const double v = (double)E[d.port_e[p]];
+        const double me = d.me_port[p];
+        for (int m = 0; m < M; ++m) acc[m] += me * (d.vprof[(long long)m * ne + p] * v);
+    }
+    for (int p = threadIdx.x; p < nh; p += blockDim.x) {
+        const double v = (double)H[d.port_h[p]];
+        const double mh = d.mh_port[p];
+        for (int m = 0; m < M; ++m) acc[M + m] += mh * (d.hprof[(long long)m * nh + p] * v);
+    }
+    block_sum<2 * kMaxModes>(acc, 2 * M, red, wred);
+    if (threadIdx.x == 0) {
+        double amax = 0.0;
+        for (int m = 0; m < M; ++m) {
+            const long long r = ((long long)b * pa.rec.cap + n) * pa.rec.nch + d.channel0 + m;
+            pa.rec.V[r] = red[m] * d.rec_scale[m];
+            pa.rec.I[r] = red[M + m] * d.rec_scale[m];
+            Vport_prev[m] = s_vc[m];
+            Vint_prev[m] = s_vint[m];
+            amax = fmax(amax, fabs(s_vc[m]) * d.rec_scale[m]);
+        }
+        atomic_max_nonneg(pa.absmax + b, amax);
+    }
+}
+
+}  // namespace
+
+template <typename T>
+void launch_lumped(T* e, const PortsArgs& pa, const LumpedDev* d, int n_lumped, cudaStream_t s) {
+    if (n_lumped <= 0) return;
+    k_lumped<T><<<dim3(n_lumped, pa.B), 32, 0, s>>>(e, pa, d);
+}
+
+template <typename T>
+void launch_modal(T* e, const T* h, const PortsArgs& pa, const ModalDev* d, int n_modal,
+                  cudaStream_t s) {
+    if (n_modal <= 0) return;
+    k_modal<T><<<dim3(n_modal, pa.B), kPortThreads, 0, s>>>(e, h, pa, d);
+}
+
+template void launch_lumped<float>(float*, const PortsArgs&, const LumpedDev*, int, cudaStream_t);
+template void launch_lumped<double>(double*, const PortsArgs&, const LumpedDev*, int,
+                                    cudaStream_t);
+template void launch_modal<float>(float*, const float*, const PortsArgs&, const ModalDev*, int,
+                                  cudaStream_t);
+template void launch_modal<double>(double*, const double*, const PortsArgs&, const ModalDev*, int,
+                                   cudaStream_t);
+
+}  // namespace fitb

@@ -1,0 +1,380 @@
+"""Python handle over the C ABI: one :class:`FitEngine` = one device-resident
+FIT-TD problem with ``batch`` field sets sharing a coefficient set.
+
+This is the thin host layer the solver front-end
+(:mod:`magnelio_b200.solver`) and the benchmark drive.  Arrays cross the
+boundary in the reference's layouts (flat ``[Ex|Ey|Ez]`` / ``[Hx|Hy|Hz]``
+vectors, reference psi slab shapes, flat edge indices), and every call
+raises :class:`~magnelio_b200._lib.FitbError` on failure.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from magnelio_b200 import _lib
+from magnelio_b200._lib import check, f64p, i32p, i64p, u8p
+
+FACES = ("xmin", "xmax", "ymin", "ymax", "zmin", "zmax")
+COMPONENTS = ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz")
+
+
+def component_shapes(nx: int, ny: int, nz: int) -> dict[str, tuple[int, int, int]]:
+    """Reference Yee component shapes (``field_arrays.py:1-17``)."""
+    return {
+        "Ex": (nx, ny + 1, nz + 1),
+        "Ey": (nx + 1, ny, nz + 1),
+        "Ez": (nx + 1, ny + 1, nz),
+        "Hx": (nx + 1, ny, nz),
+        "Hy": (nx, ny + 1, nz),
+        "Hz": (nx, ny, nz + 1),
+    }
+
+
+def _f64(a) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(a, dtype=np.float64))
+
+
+class FitEngine:
+    """Device-resident FIT-TD state on one GPU.
+
+    Parameters
+    ----------
+    nx, ny, nz : int
+        Cell counts.
+    dt : float
+        Time step [s].
+    batch : int
+        Number of field sets that advance together on one coefficient set.
+    precision : ``"single"`` or ``"double"``
+        Field and coefficient storage type on the device.
+    device : int
+        CUDA device ordinal.
+    """
+
+    def __init__(self, nx, ny, nz, dt, *, batch=1, precision="single", device=0):
+        if precision not in ("single", "double"):
+            raise ValueError(f"precision must be 'single' or 'double', got {precision!r}")
+        self._lib = _lib.load()
+        self.nx, self.ny, self.nz = int(nx), int(ny), int(nz)
+        self.dt = float(dt)
+        self.batch = int(batch)
+        self.precision = precision
+        self.dtype = np.float32 if precision == "single" else np.float64
+        desc = _lib.FitbDesc(
+            self.nx, self.ny, self.nz, self.batch, 4 if precision == "single" else 8, int(device), self.dt
+        )
+        h = C.c_void_p()
+        check(self._lib.fitb_create(C.byref(desc), C.byref(h)))
+        self._h = h
+        shapes = component_shapes(self.nx, self.ny, self.nz)
+        self.shapes = shapes
+        self.n_E = sum(int(np.prod(shapes[c])) for c in COMPONENTS[:3])
+        self.n_H = sum(int(np.prod(shapes[c])) for c in COMPONENTS[3:])
+        self._lumped = []
+        self._modal = []
+        self._monitors = []
+
+    # ---- lifetime -------------------------------------------------------
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            check(self._lib.fitb_destroy(self._h))
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def launch_count(self) -> int:
+        v = C.c_int64()
+        check(self._lib.fitb_launch_count(self._h, C.byref(v)))
+        return int(v.value)
+
+    # ---- coefficients and fields ---------------------------------------
+    def set_coefficients(self, alpha_E, beta_E, alpha_H, beta_H, M_eps=None, M_mu=None) -> None:
+        arrs = [_f64(a) for a in (alpha_E, beta_E, alpha_H, beta_H)]
+        if arrs[0].size != self.n_E or arrs[1].size != self.n_E:
+            raise ValueError(f"alpha_E/beta_E must have {self.n_E} entries")
+        if arrs[2].size != self.n_H or arrs[3].size != self.n_H:
+            raise ValueError(f"alpha_H/beta_H must have {self.n_H} entries")
+        me = None if M_eps is None else _f64(M_eps)
+        mm = None if M_mu is None else _f64(M_mu)
+        check(self._lib.fitb_set_coeffs(self._h, *[f64p(a) for a in arrs], f64p(me), f64p(mm)))
+
+    def set_coefficients_native(self, alpha_E, beta_E, alpha_H, beta_H, M_eps=None, M_mu=None) -> None:
+        """Upload coefficient arrays that are already in the field dtype."""
+        arrs = [np.ascontiguousarray(a) for a in (alpha_E, beta_E, alpha_H, beta_H, M_eps, M_mu) if a is not None]
+        for a in arrs:
+            if a.dtype != self.dtype:
+                raise TypeError(f"native coefficients must be {np.dtype(self.dtype).name}, got {a.dtype}")
+        sizes = [self.n_E, self.n_E, self.n_H, self.n_H, self.n_E, self.n_H]
+        ptrs = []
+        for a, n in zip((alpha_E, beta_E, alpha_H, beta_H, M_eps, M_mu), sizes):
+            if a is None:
+                ptrs.append(None)
+                continue
+            a = np.ascontiguousarray(a)
+            if a.size != n:
+                raise ValueError(f"coefficient array has {a.size} entries, expected {n}")
+            ptrs.append(a.ctypes.data)
+        keep = arrs  # noqa: F841 (kept alive across the call)
+        check(self._lib.fitb_set_coeffs_native(self._h, *ptrs))
+
+    def set_fields(self, e=None, h=None, b: int = 0) -> None:
+        ea = None if e is None else np.ascontiguousarray(np.asarray(e, dtype=self.dtype).ravel())
+        ha = None if h is None else np.ascontiguousarray(np.asarray(h, dtype=self.dtype).ravel())
+        check(
+            self._lib.fitb_set_fields(
+                self._h,
+                int(b),
+                None if ea is None else ea.ctypes.data,
+                0 if ea is None else ea.nbytes,
+                None if ha is None else ha.ctypes.data,
+                0 if ha is None else ha.nbytes,
+            )
+        )
+
+    def read_fields(self, b: int = 0) -> tuple[np.ndarray, np.ndarray]:
+        e = np.empty(self.n_E, dtype=self.dtype)
+        h = np.empty(self.n_H, dtype=self.dtype)
+        check(self._lib.fitb_read_fields(self._h, int(b), e.ctypes.data, e.nbytes, h.ctypes.data, h.nbytes))
+        return e, h
+
+    # ---- boundaries ----------------------------------------------------
+    def add_cpml(self, face: str, b, c, ck, air=(None, None, None, None)) -> None:
+        """Add one CFS-PML face with per-layer tables and optional air masks.
+
+        ``air`` holds the masks of (E1, E2, H1, H2) in the reference psi
+        shapes (``cpml.py:173-187``), any entry may be None (= all ones).
+        """
+        fi = FACES.index(face)
+        bt, ct, kt = _f64(b), _f64(c), _f64(ck)
+        masks = [None if a is None else np.ascontiguousarray(np.asarray(a) != 0, dtype=np.uint8) for a in air]
+        check(
+            self._lib.fitb_add_cpml(
+                self._h, fi, int(bt.size), f64p(bt), f64p(ct), f64p(kt), *[u8p(m) for m in masks]
+            )
+        )
+
+    # ---- ports -----------------------------------------------------------
+    def add_lumped(self, flat_e_idx, signs, betas, *, R=None, L=None, C_=None, record_scale=1.0) -> int:
+        idx = np.ascontiguousarray(np.asarray(flat_e_idx, dtype=np.int64))
+        sg, bt = _f64(signs), _f64(betas)
+        out = C.c_int32()
+        neg = -1.0
+        check(
+            self._lib.fitb_add_lumped(
+                self._h,
+                int(idx.size),
+                i64p(idx),
+                f64p(sg),
+                f64p(bt),
+                neg if R is None else float(R),
+                neg if L is None else float(L),
+                neg if C_ is None else float(C_),
+                float(record_scale),
+                C.byref(out),
+            )
+        )
+        self._lumped.append(int(out.value))
+        return int(out.value)
+
+    def set_lumped_source(self, port: int, b: int, v_src) -> None:
+        v = _f64(v_src)
+        check(self._lib.fitb_set_lumped_source(self._h, int(port), int(b), int(v.size), f64p(v)))
+
+    def push_lumped_samples(self, port: int, b: int, step0: int, n: int, host_ptr: int) -> None:
+        """Asynchronous H2D of ``n`` source samples from a (pinned) host
+        address into the table of lumped port ``port``, starting at
+        ``step0``."""
+        check(self._lib.fitb_push_lumped_samples(self._h, int(port), int(b), int(step0), int(n), host_ptr))
+
+    def add_modal_port(
+        self,
+        *,
+        port_e_idx,
+        int_e_idx,
+        n_e_u,
+        port_h_idx,
+        n_h_u,
+        me_port,
+        me_int,
+        mh_port,
+        e_profile,
+        v_profile,
+        h_profile,
+        mur_r,
+        tau,
+        record_scale,
+        is_dtbc,
+        dtbc_r,
+        dtbc_q,
+        dtbc_n_kernel_init=4096,
+        complement=None,
+        max_steps=0,
+    ) -> int:
+        pe = np.ascontiguousarray(np.asarray(port_e_idx, dtype=np.int64))
+        ie = np.ascontiguousarray(np.asarray(int_e_idx, dtype=np.int64))
+        ph = np.ascontiguousarray(np.asarray(port_h_idx, dtype=np.int64))
+        M = int(np.asarray(mur_r).size)
+        ne, nh = pe.size, ph.size
+        keep = {
+            "me_port": _f64(me_port),
+            "me_int": _f64(me_int),
+            "mh_port": _f64(mh_port) if nh else np.zeros(1),
+            "e_profile": _f64(e_profile).reshape(M, ne),
+            "v_profile": _f64(v_profile).reshape(M, ne),
+            "h_profile": _f64(h_profile).reshape(M, nh) if nh else np.zeros((M, 1)),
+            "mur_r": _f64(mur_r),
+            "tau": _f64(tau),
+            "record_scale": _f64(record_scale),
+            "is_dtbc": np.ascontiguousarray(np.asarray(is_dtbc, dtype=np.int32)),
+            "dtbc_r": _f64(dtbc_r),
+            "dtbc_q": _f64(dtbc_q),
+        }
+        comp_r = comp_live = None
+        if complement is not None:
+            comp_r, comp_live = _f64(complement[0]), _f64(complement[1])
+        d = _lib.FitbModalDesc(
+            M,
+            int(n_e_u),
+            int(ne - n_e_u),
+            int(n_h_u),
+            int(nh - n_h_u),
+            i64p(pe),
+            i64p(ie),
+            i64p(ph),
+            f64p(keep["me_port"]),
+            f64p(keep["me_int"]),
+            f64p(keep["mh_port"]),
+            f64p(keep["e_profile"]),
+            f64p(keep["v_profile"]),
+            f64p(keep["h_profile"]),
+            f64p(keep["mur_r"]),
+            f64p(keep["tau"]),
+            f64p(keep["record_scale"]),
+            i32p(keep["is_dtbc"]),
+            f64p(keep["dtbc_r"]),
+            f64p(keep["dtbc_q"]),
+            int(dtbc_n_kernel_init),
+            1 if complement is not None else 0,
+            f64p(comp_r),
+            f64p(comp_live),
+            int(max_steps),
+        )
+        out = C.c_int32()
+        check(self._lib.fitb_add_modal_port(self._h, C.byref(d), C.byref(out)))
+        self._modal.append(int(out.value))
+        return int(out.value)
+
+    def set_dtbc_kernel(self, port: int, mode: int, kernel) -> None:
+        k = _f64(kernel)
+        check(self._lib.fitb_set_dtbc_kernel(self._h, int(port), int(mode), int(k.size), f64p(k)))
+
+    def set_modal_source(self, port: int, b: int, mode: int, samples=None) -> None:
+        w = None if samples is None else _f64(samples)
+        check(
+            self._lib.fitb_set_modal_source(
+                self._h, int(port), int(b), int(mode), 0 if w is None else int(w.size), f64p(w)
+            )
+        )
+
+    # ---- monitors --------------------------------------------------------
+    def add_dft_monitor(self, box, components, freqs, dx, dy, dz, *, stride=1, kahan=True) -> int:
+        (i0, i1), (j0, j1), (k0, k1) = box
+        mask = 0
+        for c in components:
+            mask |= 1 << COMPONENTS.index(c)
+        fr, dxa, dya, dza = _f64(freqs), _f64(dx), _f64(dy), _f64(dz)
+        d = _lib.FitbDftDesc(
+            int(i0), int(i1), int(j0), int(j1), int(k0), int(k1), mask, int(fr.size), f64p(fr),
+            int(stride), 1 if kahan else 0, f64p(dxa), f64p(dya), f64p(dza),
+        )
+        out = C.c_int32()
+        check(self._lib.fitb_add_dft_monitor(self._h, C.byref(d), C.byref(out)))
+        self._monitors.append((int(out.value), (i1 - i0, j1 - j0, k1 - k0), fr.size))
+        return int(out.value)
+
+    def read_dft(self, mon: int, comp: str, b: int = 0) -> np.ndarray:
+        _, shape, nf = self._monitors[mon]
+        n = int(nf * np.prod(shape))
+        re = np.empty(n)
+        im = np.empty(n)
+        check(self._lib.fitb_read_dft(self._h, int(mon), int(b), COMPONENTS.index(comp), f64p(re), f64p(im), n))
+        return (re + 1j * im).reshape(nf, *shape)
+
+    # ---- stepping --------------------------------------------------------
+    def step(self, n: int) -> None:
+        check(self._lib.fitb_step(self._h, int(n)))
+
+    def sync(self) -> None:
+        check(self._lib.fitb_sync(self._h))
+
+    def step_timed(self, n: int) -> float:
+        """Advance ``n`` steps; device milliseconds from CUDA events on the
+        engine's stream."""
+        ms = C.c_double()
+        check(self._lib.fitb_step_timed(self._h, int(n), C.byref(ms)))
+        return float(ms.value)
+
+    def time_stencil(self, n_iter: int = 20) -> tuple[float, float]:
+        """Per-launch device ms of the E and of the H update alone
+        (measurement helper; advances the fields)."""
+        a, b = C.c_double(), C.c_double()
+        check(self._lib.fitb_time_stencil(self._h, int(n_iter), C.byref(a), C.byref(b)))
+        return float(a.value), float(b.value)
+
+    @property
+    def steps_done(self) -> int:
+        v = C.c_int64()
+        check(self._lib.fitb_steps_done(self._h, C.byref(v)))
+        return int(v.value)
+
+    def energy(self, b: int = 0) -> float:
+        v = C.c_double()
+        check(self._lib.fitb_energy(self._h, int(b), C.byref(v)))
+        return float(v.value)
+
+    def poll_signal_absmax(self, b: int = 0) -> float:
+        v = C.c_double()
+        check(self._lib.fitb_poll_signal_absmax(self._h, int(b), C.byref(v)))
+        return float(v.value)
+
+    @property
+    def n_channels(self) -> int:
+        v = C.c_int32()
+        check(self._lib.fitb_channel_count(self._h, C.byref(v)))
+        return int(v.value)
+
+    def read_vi(self, b: int = 0, step0: int = 0, n: int | None = None) -> tuple[np.ndarray, np.ndarray]:
+        if n is None:
+            n = self.steps_done - step0
+        nch = self.n_channels
+        V = np.zeros((n, nch))
+        I = np.zeros((n, nch))
+        if nch and n:
+            check(self._lib.fitb_read_vi(self._h, int(b), int(step0), int(n), f64p(V), f64p(I)))
+        return V, I
+
+    # ---- checkpoint ------------------------------------------------------
+    def state_export(self) -> bytes:
+        n = C.c_size_t()
+        check(self._lib.fitb_state_size(self._h, C.byref(n)))
+        buf = C.create_string_buffer(n.value)
+        check(self._lib.fitb_state_export(self._h, buf, n.value))
+        return buf.raw
+
+    def state_import(self, blob: bytes) -> None:
+        buf = C.create_string_buffer(blob, len(blob))
+        check(self._lib.fitb_state_import(self._h, buf, len(blob)))

@@ -1,0 +1,275 @@
+"""Self-contained description of one FIT-TD run: grid, coefficients,
+boundaries, ports, monitors, sources and initial state.
+
+It carries exactly the host-built constants the device engine consumes
+(the reference builds them in ``FITTimeDomainSolver.setup``,
+``src/magnelio/solver/fit_td.py:302-631``), so one problem can be run by the
+engine, checked against the CPU oracle, and stored as an ``.npz`` fixture
+without the reference package being importable.
+"""
+
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from magnelio_b200.engine import FitEngine
+
+FACES = ("xmin", "xmax", "ymin", "ymax", "zmin", "zmax")
+
+
+@dataclass
+class CpmlFace:
+    face: str
+    b: np.ndarray
+    c: np.ndarray
+    ck: np.ndarray
+    air: tuple = (None, None, None, None)  # E1, E2, H1, H2 in reference psi shapes
+
+
+@dataclass
+class LumpedPort:
+    flat_idx: np.ndarray
+    signs: np.ndarray
+    betas: np.ndarray
+    R: float | None = None
+    L: float | None = None
+    C: float | None = None
+    record_scale: float = 1.0
+    # per field set: v_src[n] = waveform((n+1) dt) (source volts)
+    v_src: list = field(default_factory=list)
+
+
+@dataclass
+class ModalPort:
+    port_e_idx: np.ndarray
+    int_e_idx: np.ndarray
+    n_e_u: int
+    port_h_idx: np.ndarray
+    n_h_u: int
+    me_port: np.ndarray
+    me_int: np.ndarray
+    mh_port: np.ndarray
+    e_profile: np.ndarray  # (M, n_e)
+    v_profile: np.ndarray  # (M, n_e)
+    h_profile: np.ndarray  # (M, n_h)
+    mur_r: np.ndarray
+    tau: np.ndarray
+    record_scale: np.ndarray
+    is_dtbc: np.ndarray
+    dtbc_r: np.ndarray
+    dtbc_q: np.ndarray
+    dtbc_n_kernel_init: int = 4096
+    # {mode: [table n0, table 2 n0, ...]}
+    dtbc_kernels: dict = field(default_factory=dict)
+    complement: tuple | None = None  # (r, live)
+    # per field set: (mode or -1, samples w[n] = waveform(n dt))
+    excitation: list = field(default_factory=list)
+
+    @property
+    def n_modes(self) -> int:
+        return int(np.asarray(self.mur_r).size)
+
+
+@dataclass
+class DftMonitor:
+    box: tuple  # ((i0, i1), (j0, j1), (k0, k1)) cell indices, stop-exclusive
+    components: tuple
+    freqs: np.ndarray
+    stride: int = 1
+
+
+@dataclass
+class FitProblem:
+    nx: int
+    ny: int
+    nz: int
+    dt: float
+    dx: np.ndarray
+    dy: np.ndarray
+    dz: np.ndarray
+    alpha_E: np.ndarray
+    beta_E: np.ndarray
+    alpha_H: np.ndarray
+    beta_H: np.ndarray
+    M_eps: np.ndarray | None = None
+    M_mu: np.ndarray | None = None
+    cpml: list = field(default_factory=list)
+    lumped: list = field(default_factory=list)
+    modal: list = field(default_factory=list)
+    monitors: list = field(default_factory=list)
+    batch: int = 1
+    e0: list = field(default_factory=list)  # per field set initial e (or empty)
+    h0: list = field(default_factory=list)
+
+    # ---- engine ---------------------------------------------------------
+    def build_engine(self, precision: str = "single", device: int = 0, max_steps: int = 0) -> FitEngine:
+        """Create a :class:`FitEngine` holding this problem."""
+        eng = FitEngine(self.nx, self.ny, self.nz, self.dt, batch=self.batch, precision=precision, device=device)
+        try:
+            eng.set_coefficients(self.alpha_E, self.beta_E, self.alpha_H, self.beta_H, self.M_eps, self.M_mu)
+            for f in self.cpml:
+                eng.add_cpml(f.face, f.b, f.c, f.ck, f.air)
+            for mp in self.modal:
+                pid = eng.add_modal_port(
+                    port_e_idx=mp.port_e_idx,
+                    int_e_idx=mp.int_e_idx,
+                    n_e_u=mp.n_e_u,
+                    port_h_idx=mp.port_h_idx,
+                    n_h_u=mp.n_h_u,
+                    me_port=mp.me_port,
+                    me_int=mp.me_int,
+                    mh_port=mp.mh_port,
+                    e_profile=mp.e_profile,
+                    v_profile=mp.v_profile,
+                    h_profile=mp.h_profile,
+                    mur_r=mp.mur_r,
+                    tau=mp.tau,
+                    record_scale=mp.record_scale,
+                    is_dtbc=mp.is_dtbc,
+                    dtbc_r=mp.dtbc_r,
+                    dtbc_q=mp.dtbc_q,
+                    dtbc_n_kernel_init=mp.dtbc_n_kernel_init,
+                    complement=mp.complement,
+                    max_steps=max_steps,
+                )
+                for m, tables in sorted(mp.dtbc_kernels.items()):
+                    for t in tables:
+                        eng.set_dtbc_kernel(pid, int(m), t)
+                for b, exc in enumerate(mp.excitation):
+                    if exc is not None and exc[0] >= 0:
+                        eng.set_modal_source(pid, b, int(exc[0]), exc[1])
+            for lp in self.lumped:
+                lid = eng.add_lumped(
+                    lp.flat_idx, lp.signs, lp.betas, R=lp.R, L=lp.L, C_=lp.C, record_scale=lp.record_scale
+                )
+                for b, v in enumerate(lp.v_src):
+                    if v is not None and len(v):
+                        eng.set_lumped_source(lid, b, v)
+            for mon in self.monitors:
+                eng.add_dft_monitor(mon.box, mon.components, mon.freqs, self.dx, self.dy, self.dz, stride=mon.stride)
+            for b in range(self.batch):
+                e = self.e0[b] if b < len(self.e0) else None
+                h = self.h0[b] if b < len(self.h0) else None
+                if e is not None or h is not None:
+                    eng.set_fields(e, h, b)
+        except Exception:
+            eng.close()
+            raise
+        return eng
+
+    # ---- npz round trip ---------------------------------------------------
+    def to_arrays(self, prefix: str = "p.") -> dict:
+        out = {}
+
+        def put(k, v):
+            out[prefix + k] = np.asarray(v)
+
+        for k in ("nx", "ny", "nz", "dt", "batch"):
+            put(k, getattr(self, k))
+        for k in ("dx", "dy", "dz", "alpha_E", "beta_E", "alpha_H", "beta_H"):
+            put(k, getattr(self, k))
+        if self.M_eps is not None:
+            put("M_eps", self.M_eps)
+            put("M_mu", self.M_mu)
+        put("n_cpml", len(self.cpml))
+        for q, f in enumerate(self.cpml):
+            put(f"cpml{q}.face", FACES.index(f.face))
+            for k in ("b", "c", "ck"):
+                put(f"cpml{q}.{k}", getattr(f, k))
+            for a, m in enumerate(f.air):
+                if m is not None:
+                    put(f"cpml{q}.air{a}", np.asarray(m, dtype=np.uint8))
+        put("n_lumped", len(self.lumped))
+        for q, lp in enumerate(self.lumped):
+            for k in ("flat_idx", "signs", "betas", "record_scale"):
+                put(f"lumped{q}.{k}", getattr(lp, k))
+            for k in ("R", "L", "C"):
+                put(f"lumped{q}.{k}", -1.0 if getattr(lp, k) is None else getattr(lp, k))
+            for b, v in enumerate(lp.v_src):
+                put(f"lumped{q}.v_src{b}", v)
+        put("n_modal", len(self.modal))
+        for q, mp in enumerate(self.modal):
+            for k in (
+                "port_e_idx", "int_e_idx", "n_e_u", "port_h_idx", "n_h_u", "me_port", "me_int", "mh_port",
+                "e_profile", "v_profile", "h_profile", "mur_r", "tau", "record_scale", "is_dtbc", "dtbc_r",
+                "dtbc_q", "dtbc_n_kernel_init",
+            ):
+                put(f"modal{q}.{k}", getattr(mp, k))
+            for m, tables in mp.dtbc_kernels.items():
+                for t, tab in enumerate(tables):
+                    put(f"modal{q}.kern{m}.{t}", tab)
+            if mp.complement is not None:
+                put(f"modal{q}.comp_r", mp.complement[0])
+                put(f"modal{q}.comp_live", mp.complement[1])
+            for b, exc in enumerate(mp.excitation):
+                if exc is not None:
+                    put(f"modal{q}.exc{b}.mode", exc[0])
+                    put(f"modal{q}.exc{b}.w", exc[1])
+        put("n_mon", len(self.monitors))
+        for q, mon in enumerate(self.monitors):
+            put(f"mon{q}.box", np.asarray(mon.box, dtype=np.int64))
+            put(f"mon{q}.comps", np.array([["Ex", "Ey", "Ez", "Hx", "Hy", "Hz"].index(c) for c in mon.components]))
+            put(f"mon{q}.freqs", mon.freqs)
+            put(f"mon{q}.stride", mon.stride)
+        for b, e in enumerate(self.e0):
+            if e is not None:
+                put(f"e0.{b}", e)
+        for b, h in enumerate(self.h0):
+            if h is not None:
+                put(f"h0.{b}", h)
+        return out
+
+    @classmethod
+    def from_arrays(cls, d, prefix: str = "p.") -> "FitProblem":
+        def g(k, default=None):
+            return d[prefix + k] if (prefix + k) in d else default
+
+        nx, ny, nz = int(g("nx")), int(g("ny")), int(g("nz"))
+        p = cls(
+            nx=nx, ny=ny, nz=nz, dt=float(g("dt")),
+            dx=g("dx"), dy=g("dy"), dz=g("dz"),
+            alpha_E=g("alpha_E"), beta_E=g("beta_E"), alpha_H=g("alpha_H"), beta_H=g("beta_H"),
+            M_eps=g("M_eps"), M_mu=g("M_mu"), batch=int(g("batch", 1)),
+        )
+        for q in range(int(g("n_cpml", 0))):
+            air = tuple(g(f"cpml{q}.air{a}") for a in range(4))
+            p.cpml.append(CpmlFace(FACES[int(g(f"cpml{q}.face"))], g(f"cpml{q}.b"), g(f"cpml{q}.c"), g(f"cpml{q}.ck"), air))
+        for q in range(int(g("n_lumped", 0))):
+            rlc = [float(g(f"lumped{q}.{k}")) for k in ("R", "L", "C")]
+            p.lumped.append(
+                LumpedPort(
+                    flat_idx=g(f"lumped{q}.flat_idx"), signs=g(f"lumped{q}.signs"), betas=g(f"lumped{q}.betas"),
+                    R=None if rlc[0] < 0 else rlc[0], L=None if rlc[1] < 0 else rlc[1], C=None if rlc[2] < 0 else rlc[2],
+                    record_scale=float(g(f"lumped{q}.record_scale")),
+                    v_src=[g(f"lumped{q}.v_src{b}") for b in range(p.batch)],
+                )
+            )
+        for q in range(int(g("n_modal", 0))):
+            kw = {k: g(f"modal{q}.{k}") for k in (
+                "port_e_idx", "int_e_idx", "port_h_idx", "me_port", "me_int", "mh_port", "e_profile",
+                "v_profile", "h_profile", "mur_r", "tau", "record_scale", "is_dtbc", "dtbc_r", "dtbc_q")}
+            mp = ModalPort(n_e_u=int(g(f"modal{q}.n_e_u")), n_h_u=int(g(f"modal{q}.n_h_u")),
+                           dtbc_n_kernel_init=int(g(f"modal{q}.dtbc_n_kernel_init")), **kw)
+            for m in range(mp.n_modes):
+                tabs = []
+                t = 0
+                while g(f"modal{q}.kern{m}.{t}") is not None:
+                    tabs.append(g(f"modal{q}.kern{m}.{t}"))
+                    t += 1
+                if tabs:
+                    mp.dtbc_kernels[m] = tabs
+            if g(f"modal{q}.comp_r") is not None:
+                mp.complement = (g(f"modal{q}.comp_r"), g(f"modal{q}.comp_live"))
+            for b in range(p.batch):
+                mode = g(f"modal{q}.exc{b}.mode")
+                mp.excitation.append(None if mode is None else (int(mode), g(f"modal{q}.exc{b}.w")))
+            p.modal.append(mp)
+        for q in range(int(g("n_mon", 0))):
+            box = g(f"mon{q}.box")
+            comps = tuple(["Ex", "Ey", "Ez", "Hx", "Hy", "Hz"][int(c)] for c in g(f"mon{q}.comps"))
+            p.monitors.append(DftMonitor(tuple(tuple(int(v) for v in r) for r in box), comps, g(f"mon{q}.freqs"), int(g(f"mon{q}.stride"))))
+        p.e0 = [g(f"e0.{b}") for b in range(p.batch)]
+        p.h0 = [g(f"h0.{b}") for b in range(p.batch)]
+        return p

@@ -1,0 +1,399 @@
+"""Generate the golden fixtures by running the reference package itself.
+
+Run from the repository root in an environment where the reference is
+importable (its ``src`` directory on ``PYTHONPATH``)::
+
+    PYTHONPATH=<reference>/src NUMBA_CACHE_DIR=/tmp/numba python tests/golden/make_golden.py
+
+Every case builds a small problem with the reference's own classes, takes
+the host-built constants from its ``FITTimeDomainSolver.setup()`` through
+:func:`magnelio_b200.adapter.problem_from_solver`, then marches the
+reference (float64, NumPy backend) and stores inputs and outputs in
+``tests/golden/<case>.npz``.  The fixtures pin both the CPU oracle
+(``oracle/fit_oracle.py``) and the device engine.
+"""
+
+from __future__ import annotations
+
+import dataclasses
+import os
+import sys
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+sys.path.insert(0, str(HERE.parents[1]))
+
+from magnelio_b200.adapter import problem_from_solver  # noqa: E402
+
+FACES = ("xmin", "xmax", "ymin", "ymax", "zmin", "zmax")
+
+
+def _grid(rng, n, h0=1e-3):
+    from magnelio.mesh.grid import GridLines
+
+    ax = [np.concatenate([[0.0], np.cumsum(h0 * rng.uniform(0.8, 1.2, k))]) for k in n]
+    return GridLines(x=ax[0], y=ax[1], z=ax[2])
+
+
+def _outputs(solver, prob, out):
+    f = solver._fields
+    out["out.e"] = np.asarray(f.e_flat, float).copy()
+    out["out.h"] = np.asarray(f.h_flat, float).copy()
+    out["out.energy"] = np.asarray(0.5 * (
+        float(np.sum(solver._M_eps_diag * f.e_flat * f.e_flat)) + float(np.sum(solver._M_mu_diag * f.h_flat * f.h_flat)))
+    )
+    for face, bsd in solver.state_dict()["boundaries"].items():
+        for k, v in bsd.items():
+            out[f"out.psi.{face}.{k}"] = np.asarray(v, float)
+    rec = solver.recorder
+    if rec is not None:
+        rec._drain_stages()
+        # channel order of the engine: modal ports in solver order, then lumped
+        from magnelio.ports._modal.operator import PortOperatorModal
+
+        order = [op for op in solver.ports if isinstance(op, PortOperatorModal)]
+        order += [op for op in solver.ports if not isinstance(op, PortOperatorModal)]
+        V = np.stack([np.asarray(rec._V_buffers[(op.name, m)]) for op in order for m in range(op.n_modes)], axis=1)
+        I = np.stack([np.asarray(rec._I_buffers[(op.name, m)]) for op in order for m in range(op.n_modes)], axis=1)
+        out["out.V"] = V
+        out["out.I"] = I
+    for q, mon in enumerate(solver.monitors):
+        for c in mon._components:
+            out[f"out.mon{q}.{c}"] = np.asarray(mon._accumulators[c].result)
+    return out
+
+
+def _save(name, prob, out, n_steps, note):
+    arrays = prob.to_arrays()
+    arrays.update(out)
+    arrays["n_steps"] = np.asarray(n_steps)
+    arrays["note"] = np.asarray(note)
+    np.savez_compressed(HERE / f"{name}.npz", **arrays)
+    print(f"{name}: {sum(a.nbytes for a in arrays.values()) / 1e3:.1f} kB raw, steps={n_steps}")
+
+
+def case_kernel_sweep():
+    """One fused sweep of the reference Numba kernels on a random state
+    (the op-order pin of tests/integration/test_tile_skip_kernels.py:42-80)."""
+    from magnelio._operators.numba_kernels import update_E_fused, update_H_fused
+
+    nx, ny, nz = 9, 7, 11
+    rng = np.random.default_rng(3)
+    shapes = {"Ex": (nx, ny + 1, nz + 1), "Ey": (nx + 1, ny, nz + 1), "Ez": (nx + 1, ny + 1, nz),
+              "Hx": (nx + 1, ny, nz), "Hy": (nx, ny + 1, nz), "Hz": (nx, ny, nz + 1)}
+    f = {k: rng.standard_normal(s) for k, s in shapes.items()}
+    co = {k: (rng.standard_normal(s), rng.standard_normal(s)) for k, s in shapes.items()}
+    out = {f"in.{k}": v.copy() for k, v in f.items()}
+    for k, (a, b) in co.items():
+        out[f"in.a{k}"] = a
+        out[f"in.b{k}"] = b
+    update_E_fused(f["Ex"], f["Ey"], f["Ez"], f["Hx"], f["Hy"], f["Hz"], *co["Ex"], *co["Ey"], *co["Ez"])
+    update_H_fused(f["Ex"], f["Ey"], f["Ez"], f["Hx"], f["Hy"], f["Hz"], *co["Hx"], *co["Hy"], *co["Hz"])
+    for k, v in f.items():
+        out[f"out.{k}"] = v
+    out["dims"] = np.array([nx, ny, nz])
+    np.savez_compressed(HERE / "kernel_sweep.npz", **out)
+    print("kernel_sweep written")
+
+
+def _box_solver(grid, regions, bc_types, bc_objs, n_steps, rng, seed_region):
+    from magnelio.mesh.mesher import Mesh
+    from magnelio.solver.fit_td import FITTimeDomainSolver
+    from magnelio.solver.stability import courant_dt
+
+    mesh = Mesh.from_grid(grid, regions=regions, boundary_conditions=bc_types)
+    s = FITTimeDomainSolver(mesh=mesh, boundary_conditions=bc_objs, total_time_steps=n_steps,
+                            dt=courant_dt(grid, "normal"), verbose=False, backend="numpy", precision="double")
+    s.setup()
+    # smooth-ish random initial field, zero on frozen edges
+    e = s._fields.e_flat
+    h = s._fields.h_flat
+    e[:] = rng.standard_normal(e.size) * (np.asarray(s._beta_E) != 0)
+    h[:] = rng.standard_normal(h.size) * (np.asarray(s._beta_H) != 0) * 1e-3
+    return s
+
+
+def case_cpml_box():
+    """CPML on all six faces, a dielectric brick and a PEC block that reaches
+    into two absorber slabs (non-trivial psi air masks)."""
+    from magnelio.boundaries.cpml import CPMLBoundary
+    from magnelio.materials.material import Material
+
+    rng = np.random.default_rng(11)
+    grid = _grid(rng, (14, 12, 16))
+    L = (grid.x[-1], grid.y[-1], grid.z[-1])
+    diel = Material(name="d", epsilon=(4.0, 4.0, 4.0))
+    pec = Material(name="metal", is_pec=True)
+    regions = [(diel, (0.3 * L[0], 0.2 * L[1], 0.3 * L[2], 0.6 * L[0], 0.7 * L[1], 0.8 * L[2])),
+               (pec, (0.0, 0.0, 0.55 * L[2], 0.2 * L[0], 0.3 * L[1], L[2]))]
+    bc_types = {f: "CPML" for f in FACES}
+    bcs = {f: CPMLBoundary(f, grid, thickness_cells=4) for f in FACES}
+    n = 40
+    s = _box_solver(grid, regions, bc_types, bcs, n, rng, None)
+    prob = problem_from_solver(s, n)
+    s.run()
+    _save("cpml_box", prob, _outputs(s, prob, {}), n, "CPML x6, dielectric + PEC block, random initial field")
+
+
+def case_mixed_box():
+    """CPML on x and zmax, PEC on ymin / zmin, PMC on ymax."""
+    from magnelio.boundaries.cpml import CPMLBoundary
+    from magnelio.boundaries.pec import PECBoundary
+    from magnelio.boundaries.pmc import PMCBoundary
+    from magnelio.materials.material import Material
+
+    rng = np.random.default_rng(12)
+    grid = _grid(rng, (13, 11, 12))
+    L = (grid.x[-1], grid.y[-1], grid.z[-1])
+    diel = Material(name="d", epsilon=(2.5, 2.5, 2.5))
+    regions = [(diel, (0.1 * L[0], 0.4 * L[1], 0.2 * L[2], 0.9 * L[0], 0.9 * L[1], 0.5 * L[2]))]
+    bc_types = {"xmin": "CPML", "xmax": "CPML", "ymin": "PEC", "ymax": "PMC", "zmin": "PEC", "zmax": "CPML"}
+    bcs = {
+        "xmin": CPMLBoundary("xmin", grid, thickness_cells=3),
+        "xmax": CPMLBoundary("xmax", grid, thickness_cells=5),
+        "ymin": PECBoundary("ymin"),
+        "ymax": PMCBoundary("ymax", grid),
+        "zmin": PECBoundary("zmin"),
+        "zmax": CPMLBoundary("zmax", grid, thickness_cells=4),
+    }
+    n = 50
+    s = _box_solver(grid, regions, bc_types, bcs, n, rng, None)
+    prob = problem_from_solver(s, n)
+    s.run()
+    _save("mixed_box", prob, _outputs(s, prob, {}), n, "mixed CPML/PEC/PMC faces")
+
+
+def case_lumped_dft():
+    """Small version of the at-scale workload: non-uniform grid, dielectric
+    brick with cat-1 conformal edges, CPML x6, a z-directed lumped source
+    at the centre, three DFT monitors (two planes, one strided box)."""
+    from magnelio._operators.material_matrices import build_M_eps, build_M_mu
+    from magnelio.boundaries.cpml import CPMLBoundary
+    from magnelio.materials.material import Material
+    from magnelio.mesh.mesher import Mesh
+    from magnelio.monitors.field_frequency import MonitorFieldFrequency
+    from magnelio.ports._lumped.factory import PortSpecLumped, build_lumped_port
+    from magnelio.ports.recorder import PortSignalRecorder
+    from magnelio.signals.waveforms import modulated_gaussian
+    from magnelio.solver.fit_td import FITTimeDomainSolver
+    from magnelio.solver.stability import courant_dt
+
+    rng = np.random.default_rng(21)
+    grid = _grid(rng, (14, 13, 15))
+    L = (grid.x[-1], grid.y[-1], grid.z[-1])
+    diel = Material(name="d", epsilon=(6.0, 6.0, 6.0))
+    regions = [(diel, (0.55 * L[0], 0.2 * L[1], 0.2 * L[2], 0.85 * L[0], 0.8 * L[1], 0.7 * L[2]))]
+    mesh = Mesh.from_grid(grid, regions=regions, boundary_conditions={f: "CPML" for f in FACES})
+    mesh = _with_cat1(mesh, rng)
+    dt = courant_dt(grid, "normal")
+    m_eps, m_mu = build_M_eps(mesh), build_M_mu(mesh)
+    ic, jc, kc = 7, 6, 7
+    spec = PortSpecLumped(name="src", start=(grid.x[ic], grid.y[jc], grid.z[kc]),
+                          end=(grid.x[ic], grid.y[jc], grid.z[kc + 1]), Z0=50.0)
+    op = build_lumped_port(spec, mesh, m_eps, m_mu, dt)
+    f_max, f_min = 60e9, 5e9
+    op.set_excitation(0, lambda t: modulated_gaussian(t, f_max, f_min))
+    rec = PortSignalRecorder(dt, [op])
+    freqs = np.linspace(10e9, 50e9, 5)
+    zc = 0.5 * (grid.z[kc] + grid.z[kc + 1])
+    mons = [
+        MonitorFieldFrequency(freqs=freqs, corners=((None, None, zc), (None, None, zc)), fields=["E"], name="zmid"),
+        MonitorFieldFrequency(freqs=freqs, corners=((0.5 * L[0], None, None), (0.5 * L[0], None, None)), fields=["E", "H"], name="xmid"),
+        MonitorFieldFrequency(freqs=freqs, corners=((0.2 * L[0], 0.3 * L[1], 0.3 * L[2]), (0.6 * L[0], 0.6 * L[1], 0.5 * L[2])),
+                              fields=["H"], interval=2.5 * dt, name="box"),
+    ]
+    bcs = {f: CPMLBoundary(f, grid, thickness_cells=3) for f in FACES}
+    n = 80
+    s = FITTimeDomainSolver(mesh=mesh, boundary_conditions=bcs, ports=[op], recorder=rec, monitors=mons,
+                            total_time_steps=n, dt=dt, verbose=False, backend="numpy", precision="double")
+    s.setup()
+    prob = problem_from_solver(s, n)
+    s.run()
+    _save("lumped_dft", prob, _outputs(s, prob, {}), n, "lumped z-source, cat-1 conformal brick, CPML x6, 3 DFT monitors")
+
+
+def _with_cat1(mesh, rng):
+    """Attach EdgeMaterialData with cat-1 fill fractions on the E-edges
+    whose clamped owner cells differ in material across the edge's dual
+    face (the brick boundary)."""
+    from magnelio._operators.material_matrices import build_M_eps
+    from magnelio.geo._subcell import EdgeMaterialData
+
+    n_E = build_M_eps(mesh).size
+    mid = mesh.material_id
+    nx, ny, nz = mid.shape
+    eps_tab = {k: m.epsilon[0] for k, m in mesh.material_library.items()}
+    cat = np.zeros(n_E, dtype=np.int8)
+    eps_avg = np.full(n_E, np.nan)
+    # Ex edges (i, j, k): dual face spans cells (i, j-1..j, k-1..k)
+    idx = 0
+    for comp, shape in (("x", (nx, ny + 1, nz + 1)), ("y", (nx + 1, ny, nz + 1)), ("z", (nx + 1, ny + 1, nz))):
+        for flat in range(int(np.prod(shape))):
+            i, j, k = np.unravel_index(flat, shape)
+            cells = []
+            rng_i = [i] if comp == "x" else [max(i - 1, 0), min(i, nx - 1)]
+            rng_j = [j] if comp == "y" else [max(j - 1, 0), min(j, ny - 1)]
+            rng_k = [k] if comp == "z" else [max(k - 1, 0), min(k, nz - 1)]
+            for a in rng_i:
+                for b in rng_j:
+                    for c in rng_k:
+                        cells.append(mid[a, b, c])
+            vals = [eps_tab[c] for c in cells]
+            if max(vals) != min(vals):
+                f = rng.uniform(0.0, 1.0)
+                cat[idx + flat] = 1
+                eps_avg[idx + flat] = f * max(vals) + (1.0 - f) * min(vals)
+        idx += int(np.prod(shape))
+    nanv = np.full(n_E, np.nan)
+    em = EdgeMaterialData(
+        category=cat, eps_avg=eps_avg, sigma_avg=np.where(cat == 1, 0.0, np.nan), A_free=nanv.copy(),
+        L_free=nanv.copy(), f_A=np.where(cat == 1, 1.0, np.nan), pec_mask=mesh.pec_mask_edges.copy(),
+        enlarged_cell_donor=np.full(n_E, -1, dtype=np.int64), enlarged_cell_area=np.zeros(n_E),
+    )
+    return dataclasses.replace(mesh, edge_material=em)
+
+
+def _wr90(nx=9, ny=4, nz=12, length=24e-3):
+    from magnelio.mesh.grid import GridLines
+    from magnelio.mesh.mesher import Mesh
+
+    A, B = 22.86e-3, 10.16e-3
+    grid = GridLines(x=np.linspace(0, A, nx + 1), y=np.linspace(0, B, ny + 1), z=np.linspace(0, length, nz + 1))
+    return Mesh.from_grid(grid, boundary_conditions={"xmin": "PEC", "xmax": "PEC", "ymin": "PEC", "ymax": "PEC",
+                                                     "zmin": "PMC", "zmax": "PMC"})
+
+
+def _wg_solver(mesh, excited, n, modify=None):
+    import magnelio.analysis.scattering_td as std
+    from magnelio._operators.material_matrices import build_M_eps, build_M_mu
+    from magnelio.ports.declarative import PortWaveguide
+    from magnelio.solver.fit_td import FITTimeDomainSolver
+    from magnelio.solver.stability import spectral_dt
+
+    ports = [PortWaveguide("p1", "zmin", n_modes=2), PortWaveguide("p2", "zmax", n_modes=2)]
+    an = std.AnalysisScatteringTD(mesh=mesh, f_max=25e9, ports=ports, verbose=False, backend="numpy",
+                                  precision="double", n_freq=11)
+    m_eps, m_mu = build_M_eps(mesh), build_M_mu(mesh)
+    dt = spectral_dt(mesh, "normal", m_eps=m_eps, m_mu=m_mu)
+    ops, el_ops, wf, n_est, rec, *_ = an._prepare_excitation_run(excited, None, m_eps, m_mu, dt, 25e9)
+    if modify is not None:
+        modify(ops)
+    s = FITTimeDomainSolver(mesh=mesh, boundary_conditions=an._resolve_bc(), ports=ops + el_ops, recorder=rec,
+                            total_time_steps=n, dt=dt, energy_stop_db=None, port_signal_stop_db=None,
+                            verbose=False, backend="numpy", precision="double")
+    s.setup()
+    return s
+
+
+def case_wg_dtbc():
+    """WR-90 section, two waveguide ports x 2 modes, exact DTBC on all
+    channels, port p1 mode 0 excited."""
+    mesh = _wr90()
+    n = 300
+    s = _wg_solver(mesh, ("p1", 0), n)
+    prob = problem_from_solver(s, n)
+    s.run()
+    _save("wg_dtbc", prob, _outputs(s, prob, {}), n, "WR-90 2 ports x 2 modes, DTBC, p1 mode 0 excited")
+
+
+def case_wg_mur():
+    """Same guide with mode 1 of each port on modal Mur (complement absorber
+    live), the Mur mode 1 of p1 excited through TF/SF, and the DTBC kernels
+    started at 64 samples so the run crosses three kernel doublings."""
+
+    def modify(ops):
+        for op in ops:
+            op._dtbc[1] = None
+            for t in op._dtbc:
+                if t is not None:
+                    t._n_kernel = 64
+                    t._rebuild_kernel()
+                    t._w_hist = np.zeros(64)
+                    t._s_hist = np.zeros(64)
+
+    mesh = _wr90()
+    n = 300
+    s = _wg_solver(mesh, ("p1", 1), n, modify)
+    prob = problem_from_solver(s, n)
+    s.run()
+    _save("wg_mur", prob, _outputs(s, prob, {}), n, "WR-90, mode 1 Mur + complement, TF/SF excited, DTBC from 64")
+
+
+def case_dtbc_advance():
+    """DTBCTermination.advance on random interior / source sequences with the
+    kernel auto-extended from 64 samples (tests/unit/test_dtbc.py:231-260)."""
+    from magnelio.ports._modal.dtbc import DTBCTermination, dtbc_kernel
+
+    r, q = 0.8, 0.1
+    rng = np.random.default_rng(3)
+    n = 300
+    u_int = rng.standard_normal(n)
+    src = rng.standard_normal(n)
+    term = DTBCTermination(r, q, n_kernel_init=64)
+    got = np.array([term.advance(u_int[k], src[k]) for k in range(n)])
+    out = {"r": np.asarray(r), "q": np.asarray(q), "u_int": u_int, "src": src, "out": got}
+    for L in (64, 128, 256, 512):
+        out[f"kernel{L}"] = dtbc_kernel(r, q, L)
+    np.savez_compressed(HERE / "dtbc_advance.npz", **out)
+    print("dtbc_advance written")
+
+
+def case_host_setup():
+    """Material matrices (cat-0 staircase + cat-1 override), CPML tables,
+    Courant dt and waveform samples of a brick mesh."""
+    from magnelio._operators.material_matrices import build_M_eps, build_M_mu
+    from magnelio.boundaries.cpml import CPMLBoundary
+    from magnelio.materials.material import Material
+    from magnelio.mesh.mesher import Mesh
+    from magnelio.signals.waveforms import modulated_gaussian
+    from magnelio.solver.stability import courant_dt
+
+    rng = np.random.default_rng(31)
+    grid = _grid(rng, (10, 9, 8))
+    L = (grid.x[-1], grid.y[-1], grid.z[-1])
+    bricks = []
+    mats = []
+    for q in range(4):
+        lo = rng.uniform(0, 0.7, 3) * L
+        hi = lo + rng.uniform(0.1, 0.4, 3) * L
+        er = float(rng.uniform(1, 10))
+        mats.append(Material(name=f"b{q}", epsilon=(er, er, er)))
+        bricks.append((tuple(lo), tuple(hi)))
+    regions = [(m, (*lo, *hi)) for m, (lo, hi) in zip(mats, bricks)]
+    mesh = Mesh.from_grid(grid, regions=regions, boundary_conditions={f: "CPML" for f in FACES})
+    mesh = _with_cat1(mesh, rng)
+    dt = courant_dt(grid, "normal")
+    out = {"x": grid.x, "y": grid.y, "z": grid.z, "dt": np.asarray(dt), "eps_r": np.array([m.epsilon[0] for m in mats]),
+           "lo": np.array([b[0] for b in bricks]), "hi": np.array([b[1] for b in bricks]),
+           "mat_id": mesh.material_id, "M_eps": build_M_eps(mesh), "M_mu": build_M_mu(mesh),
+           "cat1_idx": np.nonzero(mesh.edge_material.category == 1)[0],
+           "cat1_eps": mesh.edge_material.eps_avg[mesh.edge_material.category == 1]}
+    for face in FACES:
+        bc = CPMLBoundary(face, grid, thickness_cells=5)
+        bc.initialize(dt)
+        out[f"cpml.{face}.b"], out[f"cpml.{face}.c"], out[f"cpml.{face}.ck"] = bc._b, bc._c, bc._ck
+    t = np.arange(200) * dt
+    out["wave_t"] = t
+    out["wave_mg"] = np.array([modulated_gaussian(tt, 7.5e9, 1.0e9) for tt in t])
+    np.savez_compressed(HERE / "host_setup.npz", **out)
+    print("host_setup written")
+
+
+CASES = {
+    "kernel_sweep": case_kernel_sweep,
+    "cpml_box": case_cpml_box,
+    "mixed_box": case_mixed_box,
+    "lumped_dft": case_lumped_dft,
+    "wg_dtbc": case_wg_dtbc,
+    "wg_mur": case_wg_mur,
+    "dtbc_advance": case_dtbc_advance,
+    "host_setup": case_host_setup,
+}
+
+if __name__ == "__main__":
+    os.environ.setdefault("NUMBA_CACHE_DIR", "/tmp/numba_cache")
+    names = sys.argv[1:] or list(CASES)
+    for nm in names:
+        CASES[nm]()

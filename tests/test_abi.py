@@ -1,0 +1,56 @@
+"""The C-ABI library loads and exports every entry point the header
+declares, and the binding's signatures cover exactly those (no GPU calls)."""
+
+from __future__ import annotations
+
+import ctypes
+import re
+from pathlib import Path
+
+import pytest
+
+ROOT = Path(__file__).resolve().parents[1]
+
+
+def _declared():
+    names = set()
+    for h in (ROOT / "include").glob("*.h"):
+        names |= set(re.findall(r"^int\s+(fitb_\w+)\s*\(", h.read_text(), flags=re.M))
+    return names
+
+
+def test_header_declares_entry_points():
+    assert {"fitb_create", "fitb_step", "fitb_destroy", "fitb_read_fields"} <= _declared()
+
+
+def test_library_exports_every_declared_symbol():
+    from magnelio_b200 import _build, _lib
+
+    _build.build()
+    lib = ctypes.CDLL(str(_lib.LIB_PATH))
+    missing = [n for n in sorted(_declared()) if not hasattr(lib, n)]
+    assert not missing, missing
+    assert set(_lib.SIGNATURES) == _declared()
+    assert lib.fitb_abi_version() == 1
+
+
+def test_errors_are_reported_without_a_device():
+    """Argument errors come back as status codes with a message, and a
+    missing device is FITB_ERR_NODEV, never a crash."""
+    from magnelio_b200 import _lib
+    from magnelio_b200.engine import FitEngine
+
+    lib = _lib.load()
+    h = ctypes.c_void_p()
+    rc = lib.fitb_create(None, ctypes.byref(h))
+    assert rc == -1 and "null" in _lib.last_error()
+    try:
+        import torch
+
+        has_gpu = torch.cuda.is_available()
+    except Exception:  # pragma: no cover
+        has_gpu = False
+    if not has_gpu:
+        with pytest.raises(_lib.FitbError) as ei:
+            FitEngine(4, 4, 4, 1e-12)
+        assert ei.value.code in (-5, -2)
