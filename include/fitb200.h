@@ -203,6 +203,23 @@ int fitb_steps_done(fitb_handle* h, int64_t* out);
 /* 0.5 * (sum M_eps e^2 + sum M_mu h^2), float64 accumulation
  * (fit_td.py:1014-1018). */
 int fitb_energy(fitb_handle* h, int32_t b, double* out);
+/* Stored energy of caller-owned device arrays, without any device
+ * allocation.  No counterpart in the reference: it exists for callers that
+ * cannot allocate device memory while they run (a fixed device-memory
+ * budget, an embedding framework that owns every device byte, or a loop
+ * that must not incur the synchronisation cudaMalloc/cudaFree may cause).
+ * e / m_eps hold n_e and h / m_mu hold n_h elements of the field dtype
+ * (precision 4 = float32, 8 = float64); out is one device double receiving
+ * 0.5 * (sum m_eps e^2 + sum m_mu h^2).  Work is enqueued on `stream`
+ * (a cudaStream_t; NULL = the legacy default stream) of the current device.
+ * The block partial sums live in a fixed 1 MiB device array inside this
+ * library (held on every device that uses it until the process exits), so
+ * at most 131072 * 4096 elements per (e, h) pair are accepted; larger
+ * sizes return FITB_ERR_LIMIT.  The first call on a device looks the array
+ * up (cudaGetSymbolAddress) and should come before any stream capture.
+ * Calls share the array: calls whose work overlaps on the GPU race. */
+int fitb_energy_noalloc(const void* e, const void* h, const void* m_eps, const void* m_mu,
+                        int64_t n_e, int64_t n_h, int32_t precision, double* out, void* stream);
 /* max |V| * record_scale over all modal ports of field set b since the last
  * poll, then reset (operator.py:1323-1334 poll_signal_absmax). */
 int fitb_poll_signal_absmax(fitb_handle* h, int32_t b, double* out);

@@ -119,6 +119,7 @@ SIGNATURES = {
     "fitb_time_stencil": ([vp, i32, P_f64, P_f64], C.c_int),
     "fitb_steps_done": ([vp, P_i64], C.c_int),
     "fitb_energy": ([vp, i32, P_f64], C.c_int),
+    "fitb_energy_noalloc": ([cvp, cvp, cvp, cvp, i64, i64, i32, vp, vp], C.c_int),
     "fitb_poll_signal_absmax": ([vp, i32, P_f64], C.c_int),
     "fitb_channel_count": ([vp, P_i32], C.c_int),
     "fitb_read_vi": ([vp, i32, i64, i64, P_f64, P_f64], C.c_int),

@@ -126,6 +126,8 @@ struct DftHost {
 
 }  // namespace
 
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+
 struct Handle {
     fitb_desc desc{};
     int prec = 4;
