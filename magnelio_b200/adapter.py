@@ -165,6 +165,36 @@ def problem_from_solver(solver, n_steps: int) -> FitProblem:
     return prob
 
 
+def refresh_sources(solver, prob, engine, n_steps: int) -> None:
+    """Extend every waveform table and the DTBC kernel list of ``prob`` to
+    cover ``n_steps`` steps and upload the extension to ``engine`` (field
+    set 0).  Used when an unbounded run outgrows its first horizon."""
+    from magnelio.ports._lumped.operator import LumpedElementOperator
+    from magnelio.ports._modal.operator import PortOperatorModal
+
+    dt = float(solver.dt)
+    modal_ops = [op for op in solver.ports if isinstance(op, PortOperatorModal)]
+    lumped_ops = [op for op in solver.ports if isinstance(op, LumpedElementOperator)]
+    for pid, (op, mp) in enumerate(zip(modal_ops, prob.modal)):
+        fresh = _modal_from_op(op, solver.recorder, dt, n_steps)
+        for m, tabs in fresh.dtbc_kernels.items():
+            have = len(mp.dtbc_kernels.get(m, []))
+            for t in tabs[have:]:
+                engine.set_dtbc_kernel(pid, m, t)
+            mp.dtbc_kernels[m] = tabs
+        if fresh.excitation[0] is not None:
+            engine.set_modal_source(pid, 0, fresh.excitation[0][0], fresh.excitation[0][1])
+        mp.excitation = fresh.excitation
+    for lid, (op, lp) in enumerate(zip(lumped_ops, prob.lumped)):
+        fn = op._waveform_fn
+        if fn is None:
+            continue
+        t = np.arange(n_steps + 1) * dt
+        v = np.array([fn(tt + dt) for tt in t])
+        engine.set_lumped_source(lid, 0, v)
+        lp.v_src = [v]
+
+
 def _modal_from_op(op, recorder, dt, n_steps) -> ModalPort:
     plane = op.plane
     M = op._n_modes

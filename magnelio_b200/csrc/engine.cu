@@ -124,6 +124,8 @@ struct DftHost {
     int i0, i1, j0, j1, k0, k1;
 };
 
+constexpr int kModeSimple = 0, kModeStream = 1, kModeBulk = 2;
+
 }  // namespace
 
 void set_last_error(const std::string& msg) { g_last_error = msg; }
@@ -158,6 +160,12 @@ struct Handle {
     bool graphs_valid = false;
     long long launches = 0;
     int ichunk = 16;
+    // Bulk-copy pipelined stencil (single field set); status word of its
+    // bounded waits.
+    BulkPlan plan{};
+    int stencil_mode = 0;  // kModeSimple / kModeStream / kModeBulk
+    StreamPlan splan{};
+    DevBuf status;
 
     ~Handle() {
         if (graph_chunk) cudaGraphExecDestroy(graph_chunk);
@@ -214,6 +222,8 @@ using fitb::ck;
 namespace fitb {
 namespace {
 
+void check_device_status(Handle& H);
+
 template <typename T>
 std::vector<T> cast_vec(const double* src, long long n) {
     std::vector<T> v((size_t)n);
@@ -251,6 +261,7 @@ void unpack3(Handle& H, const T* dev_padded, T* host_flat, int c0) {
     ck(cudaMemcpyAsync(host_flat, H.staging.p, (size_t)n * sizeof(T), cudaMemcpyDeviceToHost, H.stream),
        "D2H staging");
     ck(cudaStreamSynchronize(H.stream), "unpack sync");
+    check_device_status(H);
 }
 
 void invalidate_graphs(Handle& H) {
@@ -345,12 +356,37 @@ PortsArgs ports_args(Handle& H) {
     return pa;
 }
 
+// One launch of the E (which == 0) or H (which == 1) update, with the
+// handle's kernel choice: the software-pipelined stencil for one field set,
+// the bulk-copy pipeline on request, the batched kernel for B > 1.
+template <typename T>
+void launch_half(Handle& H, int which) {
+    StencilArgs<T> sa = stencil_args<T>(H);
+    switch (H.stencil_mode) {
+        case kModeStream:
+            which == 0 ? launch_update_E_stream<T>(sa, H.splan, H.stream) : launch_update_H_stream<T>(sa, H.splan, H.stream);
+            break;
+        case kModeBulk:
+            which == 0 ? launch_update_E_bulk<T>(sa, H.plan, H.status.as<int>(), H.stream)
+                       : launch_update_H_bulk<T>(sa, H.plan, H.status.as<int>(), H.stream);
+            break;
+        default:
+            which == 0 ? launch_update_E<T>(sa, H.stream) : launch_update_H<T>(sa, H.stream);
+    }
+}
+
+void launch_stencil_half(Handle& H, int which) {
+    if (H.prec == 4)
+        launch_half<float>(H, which);
+    else
+        launch_half<double>(H, which);
+}
+
 template <typename T>
 int enqueue_step(Handle& H) {
     int n = 0;
-    StencilArgs<T> sa = stencil_args<T>(H);
     PortsArgs pa = ports_args(H);
-    launch_update_E<T>(sa, H.stream);
+    launch_half<T>(H, 0);
     ++n;
     if (!H.modal.empty()) {
         launch_modal<T>(H.e.as<T>(), H.h.as<T>(), pa, H.d_modal.as<ModalDev>(), (int)H.modal.size(), H.stream);
@@ -360,7 +396,7 @@ int enqueue_step(Handle& H) {
         launch_lumped<T>(H.e.as<T>(), pa, H.d_lumped.as<LumpedDev>(), (int)H.lumped.size(), H.stream);
         ++n;
     }
-    launch_update_H<T>(sa, H.stream);
+    launch_half<T>(H, 1);
     ++n;
     for (auto& m : H.dft) {
         launch_dft_stage<T>(H.e.as<T>(), H.h.as<T>(), H.e_block(), H.e_block(), H.g, H.B, m->dev,
@@ -393,6 +429,21 @@ cudaGraphExec_t capture(Handle& H, int nsteps, int* launches_per) {
     ck(err, "graph instantiate");
     *launches_per = per;
     return exec;
+}
+
+// Reads (and clears) the device status word of the pipelined stencil
+// kernels; a non-zero value means a bounded shared-memory pipeline wait
+// expired and the step's results are not valid.
+void check_device_status(Handle& H) {
+    if (H.stencil_mode != kModeBulk) return;
+    int st = 0;
+    ck(cudaMemcpyAsync(&st, H.status.p, sizeof(int), cudaMemcpyDeviceToHost, H.stream), "status D2H");
+    ck(cudaStreamSynchronize(H.stream), "status sync");
+    if (st != 0) {
+        ck(cudaMemsetAsync(H.status.p, 0, sizeof(int), H.stream), "status reset");
+        fail(FITB_ERR_CUDA, "a bounded wait in the %s-update copy pipeline expired (status %d)",
+             st == kStatusWaitTimeoutE ? "E" : "H", st);
+    }
 }
 
 void check_ready(Handle& H) {
@@ -459,6 +510,7 @@ void energy_impl(Handle& H, int b, double* out) {
     ck(cudaGetLastError(), "energy");
     ck(cudaMemcpyAsync(out, H.energy_out.p, sizeof(double), cudaMemcpyDeviceToHost, H.stream), "energy D2H");
     ck(cudaStreamSynchronize(H.stream), "energy sync");
+    check_device_status(H);
 }
 
 long long dft_recorded_upto(long long x, int stride) { return x < 0 ? 0 : x / stride + 1; }
@@ -747,7 +799,7 @@ int fitb_create(const fitb_desc* desc, fitb_handle** out) {
     g.nkp = (int)fitb::round_up(g.nz + 2, 4);
     g.sj = g.nkp;
     g.si = (long long)g.njp * g.nkp;
-    g.vol = (long long)(g.nx + 3) * g.si;
+    g.vol = (long long)(g.nx + 4) * g.si + (long long)fitb::kTailRows * g.sj;
     ck(cudaStreamCreateWithFlags(&H.stream, cudaStreamNonBlocking), "stream");
     const size_t blk = (size_t)H.e_block() * H.esz;
     H.e.alloc(blk * H.B);
@@ -763,6 +815,28 @@ int fitb_create(const fitb_desc* desc, fitb_handle** out) {
     H.absmax.alloc(sizeof(double) * H.B);
     H.energy_partials.alloc(sizeof(double) * H.energy_blocks);
     H.energy_out.alloc(sizeof(double));
+    H.status.alloc(sizeof(int));
+    {
+        // FITB_STENCIL selects the single-field-set stencil: "stream"
+        // (default), "bulk" (cp.async.bulk pipeline) or "simple".
+        const char* mode = getenv("FITB_STENCIL");
+        const std::string m = mode ? mode : "stream";
+        int sms = 148;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, desc->device);
+        H.stencil_mode = fitb::kModeSimple;
+        if (H.B == 1 && m == "bulk") {
+            H.plan = H.prec == 4 ? fitb::plan_bulk<float>(g, sms) : fitb::plan_bulk<double>(g, sms);
+            if (H.plan.stages >= 3) {
+                ck(H.prec == 4 ? fitb::prepare_bulk<float>(H.plan) : fitb::prepare_bulk<double>(H.plan),
+                   "bulk stencil smem attribute");
+                H.stencil_mode = fitb::kModeBulk;
+            }
+        } else if (H.B == 1 && m != "simple") {
+            const int occ = H.prec == 4 ? fitb::stream_occupancy<float>() : fitb::stream_occupancy<double>();
+            H.splan = fitb::plan_stream(g, sms, occ);
+            H.stencil_mode = fitb::kModeStream;
+        }
+    }
     *out = owner.release();
     FITB_CATCH
 }
@@ -1247,6 +1321,7 @@ int fitb_step_timed(fitb_handle* h, int64_t n_steps, double* ms) {
         fitb::run_steps(H, n_steps);
         ck(cudaEventRecord(b, H.stream), "event record");
         ck(cudaEventSynchronize(b), "event sync");
+        fitb::check_device_status(H);
         float f = 0.f;
         ck(cudaEventElapsedTime(&f, a, b), "elapsed");
         *ms = f;
@@ -1268,17 +1343,12 @@ int fitb_time_stencil(fitb_handle* h, int32_t n_iter, double* ms_e, double* ms_h
     cudaEvent_t ev[3];
     for (auto& x : ev) ck(cudaEventCreate(&x), "event");
     ck(cudaEventRecord(ev[0], H.stream), "event record");
-    for (int q = 0; q < n_iter; ++q) {
-        if (H.prec == 4) fitb::launch_update_E<float>(fitb::stencil_args<float>(H), H.stream);
-        else fitb::launch_update_E<double>(fitb::stencil_args<double>(H), H.stream);
-    }
+    for (int q = 0; q < n_iter; ++q) fitb::launch_stencil_half(H, 0);
     ck(cudaEventRecord(ev[1], H.stream), "event record");
-    for (int q = 0; q < n_iter; ++q) {
-        if (H.prec == 4) fitb::launch_update_H<float>(fitb::stencil_args<float>(H), H.stream);
-        else fitb::launch_update_H<double>(fitb::stencil_args<double>(H), H.stream);
-    }
+    for (int q = 0; q < n_iter; ++q) fitb::launch_stencil_half(H, 1);
     ck(cudaEventRecord(ev[2], H.stream), "event record");
     ck(cudaEventSynchronize(ev[2]), "event sync");
+    fitb::check_device_status(H);
     H.launches += 2LL * n_iter;
     float f1 = 0.f, f2 = 0.f;
     ck(cudaEventElapsedTime(&f1, ev[0], ev[1]), "elapsed");
@@ -1293,6 +1363,7 @@ int fitb_sync(fitb_handle* h) {
     FITB_TRY
     Handle& H = H_of(h);
     ck(cudaStreamSynchronize(H.stream), "sync");
+    fitb::check_device_status(H);
     FITB_CATCH
 }
 
@@ -1340,6 +1411,7 @@ int fitb_read_vi(fitb_handle* h, int32_t b, int64_t step0, int64_t n, double* V,
     if (step0 < 0 || n < 0 || step0 + n > H.steps_done) fail(FITB_ERR_ARG, "steps [%lld, %lld) not recorded", (long long)step0, (long long)(step0 + n));
     if (H.nch == 0 || n == 0) return FITB_OK;
     ck(cudaStreamSynchronize(H.stream), "sync");
+    fitb::check_device_status(H);
     size_t off = ((size_t)b * H.cap + step0) * H.nch;
     size_t cnt = (size_t)n * H.nch;
     if (V) ck(cudaMemcpy(V, H.recV.as<double>() + off, cnt * sizeof(double), cudaMemcpyDeviceToHost), "read V");

@@ -13,18 +13,24 @@ namespace fitb {
 //
 // Every one of the six Yee components (and every coefficient array) is
 // stored in one common padded box indexed (i, j, k), k fastest:
-//   i in [-1, nx+1]  (one zero guard plane on each side),
+//   i in [-2, nx+1]  (zero guard planes: two before, one after),
 //   j in [0, njp)    with njp = ny + 2,
-//   k in [0, nkp)    with nkp = round_up(nz + 2, 4).
-// A component occupies the sub-box of its reference shape; every other
-// entry is a pad that holds +0 forever (its update coefficients are 0).
-// Consequences used by the kernels:
+//   k in [0, nkp)    with nkp = round_up(nz + 2, 4),
+// followed by kTailRows zero rows.  A component occupies the sub-box of its
+// reference shape; every other entry is a pad that holds +0 forever (its
+// update coefficients are 0).  Consequences used by the kernels:
 //   * the reference's conditional dual curl ("a missing H neighbour counts
 //     as 0", numba_kernels.py:51-58) becomes a plain 4-term stencil, since
 //     index j-1 = -1 lands in the previous plane's pad row j = ny+1 and
 //     k-1 = -1 in the previous row's pad tail k >= nz+1;
-//   * every row starts on a 16-byte boundary (nkp is a multiple of 4).
+//   * every row starts on a 16-byte boundary (nkp is a multiple of 4), and a
+//     run of whole rows is one contiguous, 16-byte-aligned byte range: the
+//     bulk-copy stencil kernels move row tiles with single cp.async.bulk
+//     copies, including one row above the tile (row j0-1 of plane -1 lives
+//     in guard plane -2) and up to kTailRows rows past the last plane.
 // ---------------------------------------------------------------------------
+constexpr int kTailRows = 8;
+
 struct Geom {
     int nx, ny, nz;
     int njp, nkp;
@@ -33,7 +39,7 @@ struct Geom {
 };
 
 __host__ __device__ __forceinline__ long long pidx(const Geom& g, int i, int j, int k) {
-    return (long long)(i + 1) * g.si + (long long)j * g.sj + (long long)k;
+    return (long long)(i + 2) * g.si + (long long)j * g.sj + (long long)k;
 }
 
 // One CPML face as the stencil kernels see it.  The psi state of all four
@@ -71,6 +77,43 @@ template <typename T>
 void launch_update_E(const StencilArgs<T>& a, cudaStream_t s);
 template <typename T>
 void launch_update_H(const StencilArgs<T>& a, cudaStream_t s);
+
+// Software-pipelined register stencil for a single field set (the default).
+struct StreamPlan {
+    int ichunk;
+    int grid_x, grid_y, grid_z;
+};
+template <typename T>
+int stream_occupancy();
+StreamPlan plan_stream(const Geom& g, int sm_count, int ctas_per_sm);
+template <typename T>
+void launch_update_E_stream(StencilArgs<T> a, const StreamPlan& sp, cudaStream_t s);
+template <typename T>
+void launch_update_H_stream(StencilArgs<T> a, const StreamPlan& sp, cudaStream_t s);
+
+// Bulk-copy (TMA) pipelined stencil kernels for a single field set.
+// status: device word set non-zero when a bounded pipeline wait gives up.
+struct BulkPlan {
+    int tj;        // rows per tile (1 or 2)
+    int stages;    // shared-memory ring depth
+    int threads;   // CTA size
+    int ntiles;    // tiles along j
+    int nchunks;   // chunks along i
+    int ichunk;    // planes per chunk
+    size_t smem;   // dynamic shared memory bytes
+};
+template <typename T>
+BulkPlan plan_bulk(const Geom& g, int sm_count);
+// Sets the dynamic shared-memory limit of the bulk kernels (call before any
+// capture).
+template <typename T>
+cudaError_t prepare_bulk(const BulkPlan& plan);
+template <typename T>
+void launch_update_E_bulk(const StencilArgs<T>& a, const BulkPlan& plan, int* status, cudaStream_t s);
+template <typename T>
+void launch_update_H_bulk(const StencilArgs<T>& a, const BulkPlan& plan, int* status, cudaStream_t s);
+constexpr int kStatusWaitTimeoutE = 1;
+constexpr int kStatusWaitTimeoutH = 2;
 
 // ---------------------------------------------------------------------------
 // Lumped ports (Thevenin element with a series R-L-C companion).

@@ -321,6 +321,79 @@ def case_wg_mur():
     _save("wg_mur", prob, _outputs(s, prob, {}), n, "WR-90, mode 1 Mur + complement, TF/SF excited, DTBC from 64")
 
 
+def _stop_outputs(s, out):
+    out["stop.reason"] = np.asarray(s._stop_reason)
+    out["stop.actual_steps"] = np.asarray(s._actual_steps)
+    out["stop.peak_energy"] = np.asarray(s._peak_energy)
+    out["stop.peak_signal"] = np.asarray(s._peak_signal)
+    out["stop.final_signal_db"] = np.asarray(np.nan if s._final_signal_db is None else s._final_signal_db)
+    tr = s._energy_trace
+    out["stop.trace_step"] = np.asarray(tr["step"])
+    out["stop.trace_energy"] = np.asarray(tr["energy"])
+    return out
+
+
+def case_wg_stop():
+    """Unbounded WR-90 run ended by the port-signal criterion (40 dB below
+    peak, armed after 200 steps, checked every 25 steps, cap 3000)."""
+    import warnings
+
+    mesh = _wr90()
+    cap = 3000
+    s = _wg_solver(mesh, ("p1", 0), None)
+    s.total_time_steps = None
+    s.port_signal_stop_db = 40.0
+    s.port_signal_min_steps = 200
+    s.max_time_steps = cap
+    s.energy_check_interval = 25
+    prob = problem_from_solver(s, cap + 2)
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore")
+        s.run()
+    out = _stop_outputs(s, _outputs(s, prob, {}))
+    out["run.cap"] = np.asarray(cap)
+    out["run.port_signal_stop_db"] = np.asarray(40.0)
+    out["run.port_signal_min_steps"] = np.asarray(200)
+    out["run.check_interval"] = np.asarray(25)
+    _save("wg_stop", prob, out, int(s._actual_steps), f"port-signal stop: {s._stop_reason} at {s._actual_steps}")
+
+
+def case_cpml_stop():
+    """Lumped-source pulse in a CPML box ended by the energy criterion
+    (20 dB below peak, checked every 10 steps, cap 2000)."""
+    from magnelio._operators.material_matrices import build_M_eps, build_M_mu
+    from magnelio.boundaries.cpml import CPMLBoundary
+    from magnelio.mesh.mesher import Mesh
+    from magnelio.ports._lumped.factory import PortSpecLumped, build_lumped_port
+    from magnelio.ports.recorder import PortSignalRecorder
+    from magnelio.signals.waveforms import modulated_gaussian
+    from magnelio.solver.fit_td import FITTimeDomainSolver
+    from magnelio.solver.stability import courant_dt
+
+    rng = np.random.default_rng(41)
+    grid = _grid(rng, (12, 11, 13))
+    mesh = Mesh.from_grid(grid, boundary_conditions={f: "CPML" for f in FACES})
+    dt = courant_dt(grid, "normal")
+    m_eps, m_mu = build_M_eps(mesh), build_M_mu(mesh)
+    spec = PortSpecLumped(name="src", start=(grid.x[6], grid.y[5], grid.z[6]), end=(grid.x[6], grid.y[5], grid.z[7]))
+    op = build_lumped_port(spec, mesh, m_eps, m_mu, dt)
+    op.set_excitation(0, lambda t: modulated_gaussian(t, 80e9, 10e9))
+    rec = PortSignalRecorder(dt, [op])
+    bcs = {f: CPMLBoundary(f, grid, thickness_cells=4) for f in FACES}
+    cap = 2000
+    s = FITTimeDomainSolver(mesh=mesh, boundary_conditions=bcs, ports=[op], recorder=rec, total_time_steps=None,
+                            dt=dt, energy_stop_db=20.0, max_time_steps=cap, energy_check_interval=10,
+                            verbose=False, backend="numpy", precision="double")
+    s.setup()
+    prob = problem_from_solver(s, cap + 2)
+    s.run()
+    out = _stop_outputs(s, _outputs(s, prob, {}))
+    out["run.cap"] = np.asarray(cap)
+    out["run.energy_stop_db"] = np.asarray(20.0)
+    out["run.check_interval"] = np.asarray(10)
+    _save("cpml_stop", prob, out, int(s._actual_steps), f"energy stop: {s._stop_reason} at {s._actual_steps}")
+
+
 def case_dtbc_advance():
     """DTBCTermination.advance on random interior / source sequences with the
     kernel auto-extended from 64 samples (tests/unit/test_dtbc.py:231-260)."""
@@ -388,6 +461,8 @@ CASES = {
     "lumped_dft": case_lumped_dft,
     "wg_dtbc": case_wg_dtbc,
     "wg_mur": case_wg_mur,
+    "wg_stop": case_wg_stop,
+    "cpml_stop": case_cpml_stop,
     "dtbc_advance": case_dtbc_advance,
     "host_setup": case_host_setup,
 }

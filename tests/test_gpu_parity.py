@@ -105,6 +105,23 @@ def test_graph_chunks_and_single_steps_agree(name):
         assert np.array_equal(ea, eb) and np.array_equal(ha, hb)
 
 
+@pytest.mark.parametrize("name", ["cpml_box", "lumped_dft"])
+def test_stencil_variants_agree(name, monkeypatch):
+    """The software-pipelined stencil (default for one field set), the
+    bulk-copy pipeline and the batched kernel run the same arithmetic."""
+    p, d, n = load_golden(name)
+    outs = []
+    for mode in ("stream", "bulk", "simple"):
+        monkeypatch.setenv("FITB_STENCIL", mode)
+        with p.build_engine("single") as eng:
+            eng.step(n)
+            outs.append(eng.read_fields())
+    pe, ph = _peaks(name)
+    for other in outs[1:]:
+        assert _rel(outs[0][0], other[0], pe) < 1e-5  # FMA contraction may differ per kernel
+        assert _rel(outs[0][1], other[1], ph) < 1e-5
+
+
 @pytest.mark.parametrize("name", ["lumped_dft", "wg_mur"])
 def test_checkpoint_resume_is_bit_exact(name):
     """state_export after k steps, import into a fresh engine, continue:
@@ -127,9 +144,11 @@ def test_checkpoint_resume_is_bit_exact(name):
     assert np.array_equal(Va, Vb) and np.array_equal(Ia, Ib)
 
 
-def test_batch_field_sets_are_independent():
+def test_batch_field_sets_are_independent(monkeypatch):
     """Two field sets on one coefficient set: each equals its solo run
-    bit for bit (the arithmetic of one set does not depend on the batch)."""
+    bit for bit (the arithmetic of one set does not depend on the batch).
+    The solo runs use the batched kernel too, so the comparison is exact."""
+    monkeypatch.setenv("FITB_STENCIL", "simple")
     p, d, n = load_golden("wg_dtbc")
     rng = np.random.default_rng(5)
     solo = []
