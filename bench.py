@@ -34,6 +34,8 @@ if str(ROOT) not in sys.path:
 
 METRIC = "Gcell-updates/s"
 BYTES_PER_CELL = 96  # E(3) H(3) read+write, alpha/beta E/H (12) read, float32
+FIELD_BYTES_PER_CELL = 48  # the field part of it, per field set
+COEF_BYTES_PER_CELL = 48  # the coefficient part, shared by a batch of field sets
 BYTES_PER_CPML_CELL = 32  # 2 psi_E + 2 psi_H read+write per slab cell per face, float32
 
 
@@ -180,7 +182,8 @@ def _config(args, prob):
         "cpml": f"10 layers x 6 faces ({workloads.cells_in_cpml(prob)} slab cells)",
         "source": "lumped z gap, 50 ohm, modulated Gaussian 1-7.5 GHz",
         "monitors": "3 mid-plane E-field DFT monitors x 64 freq, every step",
-        "field_sets": 1,
+        "field_sets": getattr(args, "batch", 1),
+        "coefficients": "float32" if getattr(args, "coef", "native") == "native" else f"{args.coef} storage, float32 arithmetic",
         "parallelism": "replicas" if args.gpus > 1 else "single",
         "l2": "inputs larger than L2 (working set >1 GB per GPU)",
     }
@@ -193,8 +196,11 @@ def main() -> int:
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", choices=("b200", "reference"), default="b200")
     ap.add_argument("--size", type=int, default=256)
+    ap.add_argument("--batch", type=int, default=1, help="field sets sharing one coefficient set")
     ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of CPU-port timing")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--coef", choices=("native", "f16", "bf16"), default="native",
+                    help="coefficient storage of the stencil kernels (16-bit forms round the coefficients)")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
@@ -224,8 +230,17 @@ def run_b200(args, world, rank, local):
     n = args.size
     total = args.warmup + 2 * args.steps + 64
     prob = workloads.brick_box(n, steps=total)
+    B = args.batch
+    if B > 1:
+        # B field sets of the same mesh, each driven by its own amplitude
+        prob.batch = B
+        v = prob.lumped[0].v_src[0]
+        prob.lumped[0].v_src = [v * (1.0 + 0.1 * b) for b in range(B)]
     eng = prob.build_engine("single", device=local)
-    cells = n**3
+    if args.coef != "native":
+        eng.set_coefficient_storage(args.coef)
+    coef_bytes = COEF_BYTES_PER_CELL if args.coef == "native" else COEF_BYTES_PER_CELL // 2
+    cells = n**3 * B
     # warm-up (graph capture, clocks)
     eng.step(args.warmup)
     eng.sync()
@@ -269,7 +284,7 @@ def run_b200(args, world, rank, local):
     t_e, t_h = eng.time_stencil(20)
     t_pair = t_e + t_h
     cpml_cells = workloads.cells_in_cpml(prob)
-    alg_bytes = BYTES_PER_CELL * cells + BYTES_PER_CPML_CELL * cpml_cells
+    alg_bytes = (FIELD_BYTES_PER_CELL * B + coef_bytes) * n**3 + BYTES_PER_CPML_CELL * B * cpml_cells
     achieved = alg_bytes / (t_pair * 1e-3) / 1e9
     peak, peak_kind = _peaks()
     traffic = _traffic("update_E+update_H", n)
@@ -280,7 +295,7 @@ def run_b200(args, world, rank, local):
     eng.close()
 
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and B == 1:
         rate, ns, secs, threads = cpu_port_rate(prob, budget_s=args.cpu_budget)
         cpu = {"value": rate, "unit": METRIC, "cores": threads, "kind": "port",
                "sample": f"{ns} full steps of the {n}^3 workload after 2 warm-up steps "

@@ -126,6 +126,21 @@ int fitb_set_coeffs(fitb_handle* h, const double* alpha_e, const double* beta_e,
 int fitb_set_coeffs_native(fitb_handle* h, const void* alpha_e, const void* beta_e,
                            const void* alpha_h, const void* beta_h,
                            const void* m_eps, const void* m_mu);
+/* Storage of the four update-coefficient arrays read by the stream stencil
+ * kernels: FITB_COEF_NATIVE (field dtype, the default), FITB_COEF_F16 or
+ * FITB_COEF_BF16 (16-bit values with a power-of-two scale per component;
+ * the arithmetic stays in the field dtype).  The compact forms change the
+ * coefficients by their 16-bit rounding (relative 2^-11 for float16,
+ * 2^-8 for bfloat16), so the march is no longer the reference's to
+ * round-off; they halve the coefficient reads (96 -> 72 bytes per cell and
+ * step in float32).  No counterpart in the reference, which stores the
+ * coefficients in the field dtype (fit_td.py:468-479).  Valid before or
+ * after fitb_set_coeffs; FITB_ERR_STATE when the handle does not use the
+ * stream kernels. */
+#define FITB_COEF_NATIVE 0
+#define FITB_COEF_F16 1
+#define FITB_COEF_BF16 2
+int fitb_set_coeff_storage(fitb_handle* h, int32_t kind);
 /* FieldState e_flat / h_flat of field set b (field_arrays.py:98-106). */
 int fitb_set_fields(fitb_handle* h, int32_t b, const void* e, size_t e_bytes,
                     const void* hf, size_t h_bytes);

@@ -124,7 +124,7 @@ struct DftHost {
     int i0, i1, j0, j1, k0, k1;
 };
 
-constexpr int kModeSimple = 0, kModeStream = 1, kModeBulk = 2;
+constexpr int kModeSimple = 0, kModeStream = 1, kModeBulk = 2, kModeVec = 3;
 
 }  // namespace
 
@@ -144,7 +144,11 @@ struct Handle {
     std::vector<std::unique_ptr<LumpedHost>> lumped;
     std::vector<std::unique_ptr<ModalHost>> modal;
     std::vector<std::unique_ptr<DftHost>> dft;
-    DevBuf d_lumped, d_modal;
+    DevBuf d_lumped, d_modal, d_dft;
+    int dft_stage_blocks = 0, dft_flush_blocks = 0;
+    size_t dft_flush_smem = 0;
+    DevBuf ticket;  // CTA completion counter of the merged flush launch
+    int launches_per_step = 0;
     bool port_tables_dirty = true;
     DevBuf step;          // long long
     long long steps_done = 0;
@@ -163,9 +167,18 @@ struct Handle {
     // Bulk-copy pipelined stencil (single field set); status word of its
     // bounded waits.
     BulkPlan plan{};
-    int stencil_mode = 0;  // kModeSimple / kModeStream / kModeBulk
+    int stencil_mode = 0;  // kModeSimple / kModeStream / kModeBulk / kModeVec
+    int vec_variant = 0;   // vector width x register cap of the vec kernels
     StreamPlan splan{};
     DevBuf status;
+    // Compact coefficient storage of the stream kernels (kCoefF16 /
+    // kCoefBF16): {aE, bE, aH, bH} as 16-bit [3][vol] with power-of-two
+    // scales cs[4 * array + component]; coef_max holds the per-component
+    // max |x| of the last upload.
+    int coef_kind = 0;
+    DevBuf cq[4];
+    float cs[16] = {};
+    double coef_max[4][3] = {};
 
     ~Handle() {
         if (graph_chunk) cudaGraphExecDestroy(graph_chunk);
@@ -321,6 +334,29 @@ void refresh_port_tables(Handle& H) {
         md.push_back(d);
     }
     upload(H.d_modal, md);
+    // monitors: block ranges of the merged stage / flush launches
+    std::vector<DftDev> dd;
+    int sb = 0, fb = 0;
+    size_t smem = 0;
+    for (auto& m : H.dft) {
+        DftDev d = m->dev;
+        d.sblk0 = sb;
+        d.sblk = dft_blocks((long long)d.ncomp * d.ncell);
+        d.fblk0 = fb;
+        d.fblk = dft_blocks((long long)H.B * d.ncomp * d.ncell);
+        sb += d.sblk;
+        fb += d.fblk;
+        smem = std::max(smem, (size_t)d.K * 2 * d.nf * sizeof(float2));
+        m->dev.sblk0 = d.sblk0;
+        m->dev.sblk = d.sblk;
+        m->dev.fblk0 = d.fblk0;
+        m->dev.fblk = d.fblk;
+        dd.push_back(d);
+    }
+    upload(H.d_dft, dd);
+    H.dft_stage_blocks = sb;
+    H.dft_flush_blocks = fb;
+    H.dft_flush_smem = smem;
     H.port_tables_dirty = false;
 }
 
@@ -338,7 +374,51 @@ StencilArgs<T> stencil_args(Handle& H) {
     a.nfaces = (int)H.faces.size();
     for (int q = 0; q < a.nfaces; ++q) a.f[q] = H.faces[q]->dev;
     a.ichunk = H.ichunk;
+    a.coef_kind = (H.stencil_mode == kModeStream || H.stencil_mode == kModeVec) ? H.coef_kind : kCoefNative;
+    for (int q = 0; q < 4; ++q) a.cq[q] = H.cq[q].as<unsigned short>();
+    for (int q = 0; q < 16; ++q) a.cs[q] = H.cs[q];
     return a;
+}
+
+// Per-component max |x| of one host array in the reference flat layout.
+template <typename S>
+void comp_max(const Handle& H, const S* flat, int c0, double out[3]) {
+    long long off = 0;
+    for (int q = 0; q < 3; ++q) {
+        const long long n = H.comp_size(c0 + q);
+        double m = 0.0;
+        for (long long r = 0; r < n; ++r) m = std::max(m, std::fabs((double)flat[off + r]));
+        out[q] = m;
+        off += n;
+    }
+}
+
+// Re-encode the four update-coefficient arrays in the compact 16-bit form.
+// Each component gets the power-of-two scale that puts its largest
+// magnitude in [2^13, 2^14): far from the float16 overflow (65504) and
+// keeping values down to 2^-24 of the maximum out of the subnormal range.
+void compact_coeffs(Handle& H) {
+    if (H.coef_kind == kCoefNative || !H.coeffs_set) return;
+    DevBuf* src[4] = {&H.aE, &H.bE, &H.aH, &H.bH};
+    for (int a = 0; a < 4; ++a) {
+        if (!H.cq[a].p) H.cq[a].alloc((size_t)3 * H.g.vol * sizeof(unsigned short));
+        for (int c = 0; c < 3; ++c) {
+            const double m = H.coef_max[a][c];
+            const int e = (m > 0.0 && std::isfinite(m)) ? std::max(std::min(std::ilogb(m), 100), -100) : 13;
+            const float inv = std::ldexp(1.0f, 13 - e);
+            H.cs[4 * a + c] = std::ldexp(1.0f, e - 13);
+            unsigned short* dst = H.cq[a].as<unsigned short>() + (long long)c * H.g.vol;
+            if (H.prec == 4)
+                launch_compact<float>(src[a]->as<float>() + (long long)c * H.g.vol, dst, H.g.vol, inv, H.coef_kind,
+                                      H.stream);
+            else
+                launch_compact<double>(src[a]->as<double>() + (long long)c * H.g.vol, dst, H.g.vol, inv,
+                                       H.coef_kind, H.stream);
+            H.launches++;
+        }
+    }
+    ck(cudaGetLastError(), "compact coefficients");
+    ck(cudaStreamSynchronize(H.stream), "compact coefficients sync");
 }
 
 PortsArgs ports_args(Handle& H) {
@@ -356,6 +436,23 @@ PortsArgs ports_args(Handle& H) {
     return pa;
 }
 
+// Grid of the stream / vec kernels for the handle's batch and coefficient
+// storage (occupancy depends on the kernel instance).
+void plan_stencil(Handle& H) {
+    if (H.stencil_mode != kModeStream && H.stencil_mode != kModeVec) return;
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, H.desc.device);
+    if (H.stencil_mode == kModeStream) {
+        const int occ = H.prec == 4 ? stream_occupancy<float>(H.B, H.coef_kind)
+                                    : stream_occupancy<double>(H.B, H.coef_kind);
+        H.splan = plan_stream(H.g, sms, occ, H.B);
+    } else {
+        const int occ = H.prec == 4 ? vec_occupancy<float>(H.vec_variant, H.coef_kind)
+                                    : vec_occupancy<double>(H.vec_variant, H.coef_kind);
+        H.splan = plan_vec(H.g, sms, occ, H.B, vec_width_of(H.prec, H.coef_kind ? 0 : H.vec_variant));
+    }
+}
+
 // One launch of the E (which == 0) or H (which == 1) update, with the
 // handle's kernel choice: the software-pipelined stencil for one field set,
 // the bulk-copy pipeline on request, the batched kernel for B > 1.
@@ -364,7 +461,10 @@ void launch_half(Handle& H, int which) {
     StencilArgs<T> sa = stencil_args<T>(H);
     switch (H.stencil_mode) {
         case kModeStream:
-            which == 0 ? launch_update_E_stream<T>(sa, H.splan, H.stream) : launch_update_H_stream<T>(sa, H.splan, H.stream);
+            launch_stream_half<T>(sa, H.splan, which, H.stream);
+            break;
+        case kModeVec:
+            launch_vec_half<T>(sa, H.splan, H.vec_variant, which, H.stream);
             break;
         case kModeBulk:
             which == 0 ? launch_update_E_bulk<T>(sa, H.plan, H.status.as<int>(), H.stream)
@@ -398,14 +498,18 @@ int enqueue_step(Handle& H) {
     }
     launch_half<T>(H, 1);
     ++n;
-    for (auto& m : H.dft) {
-        launch_dft_stage<T>(H.e.as<T>(), H.h.as<T>(), H.e_block(), H.e_block(), H.g, H.B, m->dev,
-                            H.step.as<long long>(), H.stream);
-        launch_dft_flush(H.B, m->dev, H.step.as<long long>(), 0, H.stream);
+    if (!H.dft.empty()) {
+        // stage + flush of all monitors; the flush launch advances the step
+        launch_dft_stage_all<T>(H.e.as<T>(), H.h.as<T>(), H.e_block(), H.e_block(), H.g, H.B,
+                                H.d_dft.as<DftDev>(), (int)H.dft.size(), H.dft_stage_blocks, H.step.as<long long>(),
+                                H.stream);
+        launch_dft_flush_all(H.B, H.d_dft.as<DftDev>(), (int)H.dft.size(), H.dft_flush_blocks, H.dft_flush_smem,
+                             H.step.as<long long>(), H.ticket.as<unsigned>(), H.stream);
         n += 2;
+    } else {
+        launch_advance(H.step.as<long long>(), H.stream);
+        ++n;
     }
-    launch_advance(H.step.as<long long>(), H.stream);
-    ++n;
     return n;
 }
 
@@ -483,11 +587,9 @@ void run_steps(Handle& H, long long nsteps) {
         H.graph_one = capture(H, 1, &p1);
         H.graph_chunk = capture(H, H.chunk, &pc);
         H.graphs_valid = true;
+        H.launches_per_step = p1;
     }
-    // launches per step (same sequence in both graphs)
-    {
-        per = 1 + 1 + 1 + (H.modal.empty() ? 0 : 1) + (H.lumped.empty() ? 0 : 1) + 2 * (int)H.dft.size();
-    }
+    per = H.launches_per_step;
     if (nsteps == 0) return;
     long long left = nsteps;
     while (left >= H.chunk) {
@@ -524,7 +626,7 @@ void dft_flush_pending(Handle& H) {
                         dft_recorded_upto(m.base_host - 1, m.dev.stride);
         int pending = (int)(cnt % m.dev.K);
         if (pending > 0) {
-            launch_dft_flush(H.B, m.dev, H.step.as<long long>(), pending, H.stream);
+            launch_dft_flush_forced(H.B, m.dev, pending, H.stream);
             H.launches++;
             ck(cudaGetLastError(), "dft flush");
         }
@@ -816,26 +918,32 @@ int fitb_create(const fitb_desc* desc, fitb_handle** out) {
     H.energy_partials.alloc(sizeof(double) * H.energy_blocks);
     H.energy_out.alloc(sizeof(double));
     H.status.alloc(sizeof(int));
+    H.ticket.alloc(sizeof(unsigned));
     {
-        // FITB_STENCIL selects the single-field-set stencil: "stream"
-        // (default), "bulk" (cp.async.bulk pipeline) or "simple".
+        // FITB_STENCIL selects the stencil kernels: "stream" (default),
+        // "vec" (vectorised planes; FITB_VEC_VARIANT picks the vector width
+        // and register cap), "bulk" (cp.async.bulk pipeline, one field set)
+        // or "simple".
         const char* mode = getenv("FITB_STENCIL");
         const std::string m = mode ? mode : "stream";
-        int sms = 148;
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, desc->device);
         H.stencil_mode = fitb::kModeSimple;
         if (H.B == 1 && m == "bulk") {
+            int sms = 148;
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, desc->device);
             H.plan = H.prec == 4 ? fitb::plan_bulk<float>(g, sms) : fitb::plan_bulk<double>(g, sms);
             if (H.plan.stages >= 3) {
                 ck(H.prec == 4 ? fitb::prepare_bulk<float>(H.plan) : fitb::prepare_bulk<double>(H.plan),
                    "bulk stencil smem attribute");
                 H.stencil_mode = fitb::kModeBulk;
             }
-        } else if (H.B == 1 && m != "simple") {
-            const int occ = H.prec == 4 ? fitb::stream_occupancy<float>() : fitb::stream_occupancy<double>();
-            H.splan = fitb::plan_stream(g, sms, occ);
+        } else if (m == "vec" && H.B <= 8 && fitb::stream_batch_supported(H.B)) {
+            const char* v = getenv("FITB_VEC_VARIANT");
+            H.vec_variant = v ? std::max(0, std::min(3, atoi(v))) : 0;
+            H.stencil_mode = fitb::kModeVec;
+        } else if (fitb::stream_batch_supported(H.B) && m != "simple") {
             H.stencil_mode = fitb::kModeStream;
         }
+        fitb::plan_stencil(H);
     }
     *out = owner.release();
     FITB_CATCH
@@ -877,7 +985,12 @@ int fitb_set_coeffs(fitb_handle* h, const double* alpha_e, const double* beta_e,
     put(H.bH, beta_h, nH, 3);
     if (m_eps) put(H.meps, m_eps, nE, 0);
     if (m_mu) put(H.mmu, m_mu, nH, 3);
+    fitb::comp_max(H, alpha_e, 0, H.coef_max[0]);
+    fitb::comp_max(H, beta_e, 0, H.coef_max[1]);
+    fitb::comp_max(H, alpha_h, 3, H.coef_max[2]);
+    fitb::comp_max(H, beta_h, 3, H.coef_max[3]);
     H.coeffs_set = true;
+    fitb::compact_coeffs(H);
     FITB_CATCH
 }
 
@@ -898,7 +1011,31 @@ int fitb_set_coeffs_native(fitb_handle* h, const void* alpha_e, const void* beta
     put(H.bH, beta_h, 3);
     if (m_eps) put(H.meps, m_eps, 0);
     if (m_mu) put(H.mmu, m_mu, 3);
+    const void* arrs[4] = {alpha_e, beta_e, alpha_h, beta_h};
+    for (int a = 0; a < 4; ++a) {
+        if (H.prec == 4)
+            fitb::comp_max(H, (const float*)arrs[a], a < 2 ? 0 : 3, H.coef_max[a]);
+        else
+            fitb::comp_max(H, (const double*)arrs[a], a < 2 ? 0 : 3, H.coef_max[a]);
+    }
     H.coeffs_set = true;
+    fitb::compact_coeffs(H);
+    FITB_CATCH
+}
+
+int fitb_set_coeff_storage(fitb_handle* h, int32_t kind) {
+    FITB_TRY
+    Handle& H = H_of(h);
+    if (kind < fitb::kCoefNative || kind > fitb::kCoefBF16) fail(FITB_ERR_ARG, "coefficient storage kind %d", kind);
+    if (kind != fitb::kCoefNative && H.stencil_mode != fitb::kModeStream && H.stencil_mode != fitb::kModeVec)
+        fail(FITB_ERR_STATE, "compact coefficient storage needs the stream stencil kernels");
+    H.coef_kind = kind;
+    if (kind == fitb::kCoefNative) {
+        for (auto& q : H.cq) q.release();
+    }
+    fitb::plan_stencil(H);
+    fitb::compact_coeffs(H);
+    fitb::invalidate_graphs(H);
     FITB_CATCH
 }
 
@@ -1272,6 +1409,7 @@ int fitb_add_dft_monitor(fitb_handle* h, const fitb_dft_desc* d, int32_t* out_id
     m->i0 = d->i0; m->i1 = d->i1; m->j0 = d->j0; m->j1 = d->j1; m->k0 = d->k0; m->k1 = d->k1;
     if (out_id) *out_id = (int32_t)H.dft.size();
     H.dft.push_back(std::move(m));
+    H.port_tables_dirty = true;
     fitb::invalidate_graphs(H);
     FITB_CATCH
 }

@@ -71,25 +71,49 @@ struct StencilArgs {
     int nfaces;
     FaceDev f[kMaxFaces];
     int ichunk;  // planes per CTA along i
+    // Compact coefficient storage read by the stream kernels (coef_kind 1:
+    // float16, 2: bfloat16): cq = {aE, bE, aH, bH}, each [3][vol] of 16-bit
+    // values, value = stored * cs[4 * array + component] (cs[4a+3] unused).
+    int coef_kind;
+    const unsigned short* cq[4];
+    float cs[16];
 };
+
+constexpr int kCoefNative = 0, kCoefF16 = 1, kCoefBF16 = 2;
+
+// dst[q] = 16-bit(src[q] * inv_scale), round to nearest even.
+template <typename T>
+void launch_compact(const T* src, unsigned short* dst, long long n, float inv_scale, int coef_kind, cudaStream_t s);
 
 template <typename T>
 void launch_update_E(const StencilArgs<T>& a, cudaStream_t s);
 template <typename T>
 void launch_update_H(const StencilArgs<T>& a, cudaStream_t s);
 
-// Software-pipelined register stencil for a single field set (the default).
+// Software-pipelined register stencil, batched over B in {1, 2, 4, 8, 16}
+// field sets (the default kernels).
 struct StreamPlan {
     int ichunk;
     int grid_x, grid_y, grid_z;
+    int block_y;  // warp rows per CTA (grid rows x field sets)
 };
+bool stream_batch_supported(int B);
 template <typename T>
-int stream_occupancy();
-StreamPlan plan_stream(const Geom& g, int sm_count, int ctas_per_sm);
+int stream_occupancy(int B, int coef_kind);
+StreamPlan plan_stream(const Geom& g, int sm_count, int ctas_per_sm, int B);
+// which: 0 = E update, 1 = H update
 template <typename T>
-void launch_update_E_stream(StencilArgs<T> a, const StreamPlan& sp, cudaStream_t s);
+void launch_stream_half(StencilArgs<T> a, const StreamPlan& sp, int which, cudaStream_t s);
+
+// Vectorised stencil over flattened padded planes, batched like the stream
+// kernels (B <= 8); grid_y = 1 and block_y is the CTA's warp count.
+// variant: vector width x register cap (stencil_vec.cu).
+int vec_width_of(int prec, int variant);
 template <typename T>
-void launch_update_H_stream(StencilArgs<T> a, const StreamPlan& sp, cudaStream_t s);
+int vec_occupancy(int variant, int coef_kind);
+StreamPlan plan_vec(const Geom& g, int sm_count, int ctas_per_sm, int B, int vk);
+template <typename T>
+void launch_vec_half(StencilArgs<T> a, const StreamPlan& sp, int variant, int which, cudaStream_t s);
 
 // Bulk-copy (TMA) pipelined stencil kernels for a single field set.
 // status: device word set non-zero when a bounded pipeline wait gives up.
@@ -224,13 +248,20 @@ struct DftDev {
     float2* bins;         // [B][ncomp][nf][ncell]
     float2* cmp;          // Kahan compensation, same shape
     double dt;
+    int sblk0, sblk;      // this monitor's blocks in the merged stage launch
+    int fblk0, fblk;      // and in the merged flush launch
 };
 
+int dft_blocks(long long work);
+// One launch stages every monitor; one launch flushes every full monitor and
+// advances the step counter (its last CTA, through `ticket`).
 template <typename T>
-void launch_dft_stage(const T* e, const T* h, long long e_block, long long h_block, const Geom& g,
-                      int B, const DftDev& d, const long long* step, cudaStream_t s);
-void launch_dft_flush(int B, const DftDev& d, const long long* step, int forced_count,
-                      cudaStream_t s);
+void launch_dft_stage_all(const T* e, const T* h, long long e_block, long long h_block, const Geom& g, int B,
+                          const DftDev* devs, int nmon, int nblocks, const long long* step, cudaStream_t s);
+void launch_dft_flush_all(int B, const DftDev* devs, int nmon, int nblocks, size_t smem, long long* step,
+                          unsigned* ticket, cudaStream_t s);
+// Host-requested flush of the first kc slots of one monitor.
+void launch_dft_flush_forced(int B, const DftDev& d, int kc, cudaStream_t s);
 
 // Energy: per field set 0.5 (sum m_eps e^2 + sum m_mu h^2) in float64.
 template <typename T>

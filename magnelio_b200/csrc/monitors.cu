@@ -8,10 +8,12 @@
 //
 // Here each recorded step only stages the interpolated float32 samples and
 // the float64-evaluated phasors exp(j w t) dt_w of that step into a block of
-// K slots (k_dft_stage).  When the block is full, k_dft_flush forms
-// sum_s w_s[f] x_s for every bin in registers and adds it once to the bins
-// (optionally Kahan-compensated): the complex bins are read and written once
-// per K recorded steps instead of once per step.
+// K slots (k_dft_stage_all).  When a monitor's block is full,
+// k_dft_flush_all forms sum_s w_s[f] x_s for every bin in registers and adds
+// it once to the bins (optionally Kahan-compensated): the complex bins are
+// read and written once per K recorded steps instead of once per step.
+// All monitors share one stage launch and one flush launch per step; the
+// last CTA of the flush launch advances the device step counter.
 #include "fitb_common.cuh"
 
 namespace fitb {
@@ -19,6 +21,7 @@ namespace fitb {
 namespace {
 
 constexpr int kMaxK = 32;
+constexpr int kThreads = 256;
 
 __device__ __forceinline__ long long recorded_upto(long long x, int stride) {
     // Number of steps n' in [0, x] with n' % stride == 0 (0 for x < 0).
@@ -26,9 +29,8 @@ __device__ __forceinline__ long long recorded_upto(long long x, int stride) {
 }
 
 template <typename T>
-__device__ __forceinline__ double interp_sample(const T* E, const T* H, long long vol,
-                                                const Geom& g, const DftDev& d, int c, int i,
-                                                int j, int k) {
+__device__ __forceinline__ double interp_sample(const T* E, const T* H, long long vol, const Geom& g,
+                                                const DftDev& d, int c, int i, int j, int k) {
     const long long o = pidx(g, i, j, k);
     const double* dx = d.inv;
     const double* dy = d.inv + d.inv_ld;
@@ -68,15 +70,23 @@ __device__ __forceinline__ double interp_sample(const T* E, const T* H, long lon
     }
 }
 
+__device__ __forceinline__ int monitor_of_block(const DftDev* devs, int nmon, bool stage) {
+    int m = 0;
+    while (m + 1 < nmon && (int)blockIdx.x >= (stage ? devs[m + 1].sblk0 : devs[m + 1].fblk0)) ++m;
+    return m;
+}
+
 template <typename T>
-__global__ void k_dft_stage(const T* __restrict__ e, const T* __restrict__ h, long long e_block,
-                            long long h_block, Geom g, int B, DftDev d,
-                            const long long* __restrict__ step) {
+__global__ void __launch_bounds__(kThreads)
+    k_dft_stage_all(const T* __restrict__ e, const T* __restrict__ h, long long e_block, long long h_block, Geom g,
+                    int B, const DftDev* __restrict__ devs, int nmon, const long long* __restrict__ step) {
+    const DftDev& d = devs[monitor_of_block(devs, nmon, true)];
+    const int lb = blockIdx.x - d.sblk0;
     const long long n = *step;
     if (n % d.stride) return;
     const long long cnt = recorded_upto(n, d.stride) - recorded_upto(*d.base - 1, d.stride);
     const int slot = (int)((cnt - 1) % d.K);
-    if (blockIdx.x == 0) {
+    if (lb == 0) {
         const double tE = (double)n * d.dt;
         const double tH = tE + 0.5 * d.dt;
         const double dtw = (double)d.stride * d.dt;
@@ -85,13 +95,11 @@ __global__ void k_dft_stage(const T* __restrict__ e, const T* __restrict__ h, lo
             const double t = (q < d.nf) ? tE : tH;
             double sn, cs;
             sincos(d.omega[f] * t, &sn, &cs);
-            d.wst[((long long)slot * 2 + (q / d.nf)) * d.nf + f] =
-                make_float2((float)(cs * dtw), (float)(sn * dtw));
+            d.wst[((long long)slot * 2 + (q / d.nf)) * d.nf + f] = make_float2((float)(cs * dtw), (float)(sn * dtw));
         }
     }
     const long long total = (long long)d.ncomp * d.ncell;
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
-         t += (long long)gridDim.x * blockDim.x) {
+    for (long long t = lb * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)d.sblk * blockDim.x) {
         const int ci = (int)(t / d.ncell);
         const long long cell = t % d.ncell;
         const int kk = (int)(cell % d.nk);
@@ -100,31 +108,21 @@ __global__ void k_dft_stage(const T* __restrict__ e, const T* __restrict__ h, lo
         const int ii = (int)(r / d.nj);
         const int c = d.comps[ci];
         for (int b = 0; b < B; ++b) {
-            const double v = interp_sample<T>(e + (long long)b * e_block, h + (long long)b * h_block,
-                                              g.vol, g, d, c, d.i0 + ii, d.j0 + jj, d.k0 + kk);
+            const double v = interp_sample<T>(e + (long long)b * e_block, h + (long long)b * h_block, g.vol, g, d, c,
+                                              d.i0 + ii, d.j0 + jj, d.k0 + kk);
             d.stage[(((long long)b * d.K + slot) * d.ncomp + ci) * d.ncell + cell] = (float)v;
         }
     }
 }
 
-__global__ void k_dft_flush(int B, DftDev d, const long long* __restrict__ step, int forced) {
-    int kc;
-    if (forced > 0) {
-        kc = forced;
-    } else {
-        const long long n = *step;
-        if (n % d.stride) return;
-        const long long cnt = recorded_upto(n, d.stride) - recorded_upto(*d.base - 1, d.stride);
-        if ((int)((cnt - 1) % d.K) != d.K - 1) return;
-        kc = d.K;
-    }
-    extern __shared__ float2 sw[];  // [kc][2][nf]
+// Adds the kc staged slots of one monitor to its bins (threads of the
+// monitor's blocks, lb = local block index, nb = the monitor's block count).
+__device__ void flush_slots(int B, const DftDev& d, int kc, int lb, int nb, float2* sw) {
     for (int q = threadIdx.x; q < kc * 2 * d.nf; q += blockDim.x) sw[q] = d.wst[q];
     __syncthreads();
     const long long per_b = (long long)d.ncomp * d.ncell;
     const long long total = (long long)B * per_b;
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
-         t += (long long)gridDim.x * blockDim.x) {
+    for (long long t = lb * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)nb * blockDim.x) {
         const int b = (int)(t / per_b);
         const long long r = t % per_b;
         const int ci = (int)(r / d.ncell);
@@ -133,8 +131,7 @@ __global__ void k_dft_flush(int B, DftDev d, const long long* __restrict__ step,
         float x[kMaxK];
 #pragma unroll
         for (int s = 0; s < kMaxK; ++s)
-            x[s] = (s < kc) ? d.stage[(((long long)b * d.K + s) * d.ncomp + ci) * d.ncell + cell]
-                            : 0.0f;
+            x[s] = (s < kc) ? d.stage[(((long long)b * d.K + s) * d.ncomp + ci) * d.ncell + cell] : 0.0f;
         for (int f = 0; f < d.nf; ++f) {
             float re = 0.0f, im = 0.0f;
 #pragma unroll
@@ -165,34 +162,63 @@ __global__ void k_dft_flush(int B, DftDev d, const long long* __restrict__ step,
     }
 }
 
+__global__ void __launch_bounds__(kThreads)
+    k_dft_flush_all(int B, const DftDev* __restrict__ devs, int nmon, long long* step, unsigned* ticket) {
+    extern __shared__ float2 sw[];
+    const DftDev& d = devs[monitor_of_block(devs, nmon, false)];
+    const int lb = blockIdx.x - d.fblk0;
+    const long long n = *step;
+    bool go = (n % d.stride) == 0;
+    if (go) {
+        const long long cnt = recorded_upto(n, d.stride) - recorded_upto(*d.base - 1, d.stride);
+        go = (int)((cnt - 1) % d.K) == d.K - 1;
+    }
+    if (go) flush_slots(B, d, d.K, lb, d.fblk, sw);
+    // The last CTA to finish advances the step counter: every CTA has read
+    // it above, and the next launch in the stream starts after this one.
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(ticket, 1u) == gridDim.x - 1) {
+            *ticket = 0u;
+            step[0] = n + 1;
+            __threadfence();
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kThreads) k_dft_flush_forced(int B, DftDev d, int kc) {
+    extern __shared__ float2 sw[];
+    flush_slots(B, d, kc, blockIdx.x, gridDim.x, sw);
+}
+
 }  // namespace
 
+int dft_blocks(long long work) {
+    long long b = (work + kThreads - 1) / kThreads;
+    if (b > 148 * 4) b = 148 * 4;
+    return (int)(b < 1 ? 1 : b);
+}
+
 template <typename T>
-void launch_dft_stage(const T* e, const T* h, long long e_block, long long h_block, const Geom& g,
-                      int B, const DftDev& d, const long long* step, cudaStream_t s) {
-    const long long total = (long long)d.ncomp * d.ncell;
-    long long blocks = (total + 255) / 256;
-    if (blocks > 148 * 8) blocks = 148 * 8;
-    if (blocks < 1) blocks = 1;
-    k_dft_stage<T><<<(int)blocks, 256, 0, s>>>(e, h, e_block, h_block, g, B, d, step);
+void launch_dft_stage_all(const T* e, const T* h, long long e_block, long long h_block, const Geom& g, int B,
+                          const DftDev* devs, int nmon, int nblocks, const long long* step, cudaStream_t s) {
+    k_dft_stage_all<T><<<nblocks, kThreads, 0, s>>>(e, h, e_block, h_block, g, B, devs, nmon, step);
 }
 
-void launch_dft_flush(int B, const DftDev& d, const long long* step, int forced_count,
-                      cudaStream_t s) {
-    const long long total = (long long)B * d.ncomp * d.ncell;
-    long long blocks = (total + 255) / 256;
-    if (blocks > 148 * 8) blocks = 148 * 8;
-    if (blocks < 1) blocks = 1;
-    const int kc = forced_count > 0 ? forced_count : d.K;
+void launch_dft_flush_all(int B, const DftDev* devs, int nmon, int nblocks, size_t smem, long long* step,
+                          unsigned* ticket, cudaStream_t s) {
+    k_dft_flush_all<<<nblocks, kThreads, smem, s>>>(B, devs, nmon, step, ticket);
+}
+
+void launch_dft_flush_forced(int B, const DftDev& d, int kc, cudaStream_t s) {
     const size_t smem = (size_t)kc * 2 * d.nf * sizeof(float2);
-    k_dft_flush<<<(int)blocks, 256, smem, s>>>(B, d, step, forced_count);
+    k_dft_flush_forced<<<dft_blocks((long long)B * d.ncomp * d.ncell), kThreads, smem, s>>>(B, d, kc);
 }
 
-template void launch_dft_stage<float>(const float*, const float*, long long, long long,
-                                      const Geom&, int, const DftDev&, const long long*,
-                                      cudaStream_t);
-template void launch_dft_stage<double>(const double*, const double*, long long, long long,
-                                       const Geom&, int, const DftDev&, const long long*,
-                                       cudaStream_t);
+template void launch_dft_stage_all<float>(const float*, const float*, long long, long long, const Geom&, int,
+                                          const DftDev*, int, int, const long long*, cudaStream_t);
+template void launch_dft_stage_all<double>(const double*, const double*, long long, long long, const Geom&, int,
+                                           const DftDev*, int, int, const long long*, cudaStream_t);
 
 }  // namespace fitb

@@ -1,17 +1,21 @@
-// Software-pipelined leapfrog curl updates for one field set.
+// Software-pipelined leapfrog curl updates, batched over field sets.
 //
 // Same arithmetic and in-thread order as stencil.cu (reference:
 // numba_kernels.py:36-127, cpml.py:343-516).  One thread owns a (j, k)
-// column and marches over a chunk of i planes; every plane's sixteen loads
-// (the cell's own coefficients, fields and its four in-plane neighbours) are
-// issued for plane i+1 before plane i is computed, so a thread always has a
-// whole plane of independent loads in flight while it does arithmetic (two
-// planes ahead measured slower: the extra registers cost more warps than
-// the deeper queue gains).  The
-// x-neighbours come from registers: the E update marches up in i (it needs
-// H at i-1, the previous iteration's values), the H update marches down (it
-// needs E at i+1).
+// column of one field set and marches over a chunk of i planes.  Per plane
+// it loads the six update coefficients of its cell, the cell's fields and
+// its four in-plane neighbours; the next plane's loads are issued before the
+// current plane is computed, so a thread always has a full plane of
+// independent loads in flight while it does arithmetic (a deeper in-register
+// queue, and a per-thread loop over field sets, both measured slower: the
+// extra registers cost more warps than they gain).  The x-neighbours come
+// from registers: the E update marches up in i (it needs H at i-1, the
+// previous plane's values), the H update marches down (it needs E at i+1).
+// Batched form (all port x mode excitations of one mesh advancing
+// together): the B field sets of a cell run in B warps of the same CTA.
 #include "fitb_common.cuh"
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
 
 namespace fitb {
 
@@ -21,16 +25,23 @@ constexpr int kSX = 32;
 constexpr int kSY = 8;
 
 template <typename T>
-struct EPlane {
-    T ax, ay, az, bx, by, bz, ex, ey, ez, hx, hy, hz, hz_jm, hx_jm, hy_km, hx_km;
+struct Coef {
+    T ax, ay, az, bx, by, bz;
 };
 
+// Field values of one cell for the E update: own E and H, H neighbours at
+// j-1 (Hz, Hx) and k-1 (Hy, Hx).
 template <typename T>
-struct HPlane {
-    T ax, ay, az, bx, by, bz, hx, hy, hz, ex, ey, ez, ez_jp, ex_jp, ey_kp, ex_kp;
+struct EFld {
+    T ex, ey, ez, hx, hy, hz, hz_jm, hx_jm, hy_km, hx_km;
 };
 
+// For the H update: own H and E, E neighbours at j+1 (Ez, Ex), k+1 (Ey, Ex).
 template <typename T>
+struct HFld {
+    T hx, hy, hz, ex, ey, ez, ez_jp, ex_jp, ey_kp, ex_kp;
+};
+
 __device__ __forceinline__ long long slab_index_s(const FaceDev& f, int l, int i, int j, int k) {
     const int a = (f.axis == 0) ? l : i;
     const int b = (f.axis == 1) ? l : j;
@@ -39,15 +50,47 @@ __device__ __forceinline__ long long slab_index_s(const FaceDev& f, int l, int i
 }
 
 template <typename T>
-__device__ __forceinline__ void load_E_plane(EPlane<T>& q, const T* __restrict__ aE, const T* __restrict__ bE,
-                                             const T* __restrict__ E, const T* __restrict__ H, long long o,
-                                             long long vol, long long sj) {
-    q.ax = __ldg(aE + o);
-    q.ay = __ldg(aE + vol + o);
-    q.az = __ldg(aE + 2 * vol + o);
-    q.bx = __ldg(bE + o);
-    q.by = __ldg(bE + vol + o);
-    q.bz = __ldg(bE + 2 * vol + o);
+__device__ __forceinline__ void load_coef(Coef<T>& q, const T* __restrict__ a, const T* __restrict__ b, long long o,
+                                          long long vol) {
+    q.ax = __ldg(a + o);
+    q.ay = __ldg(a + vol + o);
+    q.az = __ldg(a + 2 * vol + o);
+    q.bx = __ldg(b + o);
+    q.by = __ldg(b + vol + o);
+    q.bz = __ldg(b + 2 * vol + o);
+}
+
+template <int CK>
+__device__ __forceinline__ float unpack16(unsigned short u) {
+    if constexpr (CK == kCoefF16)
+        return __half2float(__ushort_as_half(u));
+    else
+        return __bfloat162float(__ushort_as_bfloat16(u));
+}
+
+// Coefficients of one cell in the handle's storage: native, or 16-bit with a
+// per-array scale (side 0: alpha_E / beta_E, side 1: alpha_H / beta_H).
+template <typename T, int CK>
+__device__ __forceinline__ void load_coef_k(Coef<T>& q, const StencilArgs<T>& p, int side, const T* __restrict__ a,
+                                            const T* __restrict__ b, long long o, long long vol) {
+    if constexpr (CK == kCoefNative) {
+        load_coef(q, a, b, o, vol);
+    } else {
+        const unsigned short* __restrict__ qa = p.cq[2 * side];
+        const unsigned short* __restrict__ qb = p.cq[2 * side + 1];
+        const float* s = p.cs + 8 * side;
+        q.ax = (T)unpack16<CK>(__ldg(qa + o)) * (T)s[0];
+        q.ay = (T)unpack16<CK>(__ldg(qa + vol + o)) * (T)s[1];
+        q.az = (T)unpack16<CK>(__ldg(qa + 2 * vol + o)) * (T)s[2];
+        q.bx = (T)unpack16<CK>(__ldg(qb + o)) * (T)s[4];
+        q.by = (T)unpack16<CK>(__ldg(qb + vol + o)) * (T)s[5];
+        q.bz = (T)unpack16<CK>(__ldg(qb + 2 * vol + o)) * (T)s[6];
+    }
+}
+
+template <typename T>
+__device__ __forceinline__ void load_efld(EFld<T>& q, const T* E, const T* __restrict__ H, long long o, long long vol,
+                                          long long sj) {
     q.ex = E[o];
     q.ey = E[vol + o];
     q.ez = E[2 * vol + o];
@@ -61,15 +104,8 @@ __device__ __forceinline__ void load_E_plane(EPlane<T>& q, const T* __restrict__
 }
 
 template <typename T>
-__device__ __forceinline__ void load_H_plane(HPlane<T>& q, const T* __restrict__ aH, const T* __restrict__ bH,
-                                             const T* __restrict__ H, const T* __restrict__ E, long long o,
-                                             long long vol, long long sj) {
-    q.ax = __ldg(aH + o);
-    q.ay = __ldg(aH + vol + o);
-    q.az = __ldg(aH + 2 * vol + o);
-    q.bx = __ldg(bH + o);
-    q.by = __ldg(bH + vol + o);
-    q.bz = __ldg(bH + 2 * vol + o);
+__device__ __forceinline__ void load_hfld(HFld<T>& q, const T* H, const T* __restrict__ E, long long o, long long vol,
+                                          long long sj) {
     q.hx = H[o];
     q.hy = H[vol + o];
     q.hz = H[2 * vol + o];
@@ -83,24 +119,24 @@ __device__ __forceinline__ void load_H_plane(HPlane<T>& q, const T* __restrict__
 }
 
 template <typename T>
-__device__ __forceinline__ void compute_E(const StencilArgs<T>& p, const EPlane<T>& cur, T& hz_im, T& hy_im,
-                                          int i, int j, int k, long long o, long long vol) {
-    T* __restrict__ E = p.e;
+__device__ __forceinline__ void compute_E(const StencilArgs<T>& p, const Coef<T>& c, const EFld<T>& cur, T& hz_im,
+                                          T& hy_im, int b, int i, int j, int k, long long o, long long vol) {
+    T* __restrict__ E = p.e + (long long)b * 3 * vol;
     const T cx = ((cur.hz - cur.hz_jm) - cur.hy) + cur.hy_km;
     const T cy = ((cur.hx - cur.hx_km) - cur.hz) + hz_im;
     const T cz = ((cur.hy - hy_im) - cur.hx) + cur.hx_jm;
-    T ex = cur.ax * cur.ex + cur.bx * cx;
-    T ey = cur.ay * cur.ey + cur.by * cy;
-    T ez = cur.az * cur.ez + cur.bz * cz;
+    T ex = c.ax * cur.ex + c.bx * cx;
+    T ey = c.ay * cur.ey + c.by * cy;
+    T ez = c.az * cur.ez + c.bz * cz;
     for (int fi = 0; fi < p.nfaces; ++fi) {
         const FaceDev& f = p.f[fi];
         const int coord = (f.axis == 0) ? i : ((f.axis == 1) ? j : k);
         const int l = coord - f.lo;
         if ((unsigned)l >= (unsigned)f.n) continue;
-        const long long s = slab_index_s<T>(f, l, i, j, k);
+        const long long s = slab_index_s(f, l, i, j, k);
         const T* bcc = static_cast<const T*>(f.bcc);
         const T cb = bcc[l], cc = bcc[f.n + l], cck = bcc[2 * f.n + l];
-        T* psi = static_cast<T*>(f.psi);
+        T* psi = static_cast<T*>(f.psi) + (long long)b * 4 * f.slab;
         T d1, d2;
         if (f.axis == 0) {
             d1 = cur.hz - hz_im;
@@ -121,14 +157,14 @@ __device__ __forceinline__ void compute_E(const StencilArgs<T>& p, const EPlane<
         if (!f.air[f.slab + s]) p2 = T(0);
         psi[f.slab + s] = p2;
         if (f.axis == 0) {
-            ey = ey + cur.by * (cck * d1 + p1);
-            ez = ez - cur.bz * (cck * d2 + p2);
+            ey = ey + c.by * (cck * d1 + p1);
+            ez = ez - c.bz * (cck * d2 + p2);
         } else if (f.axis == 1) {
-            ex = ex - cur.bx * (cck * d1 + p1);
-            ez = ez + cur.bz * (cck * d2 + p2);
+            ex = ex - c.bx * (cck * d1 + p1);
+            ez = ez + c.bz * (cck * d2 + p2);
         } else {
-            ex = ex + cur.bx * (cck * d1 + p1);
-            ey = ey - cur.by * (cck * d2 + p2);
+            ex = ex + c.bx * (cck * d1 + p1);
+            ey = ey - c.by * (cck * d2 + p2);
         }
     }
     E[o] = ex;
@@ -139,50 +175,24 @@ __device__ __forceinline__ void compute_E(const StencilArgs<T>& p, const EPlane<
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kSX* kSY) k_update_E_stream(const StencilArgs<T> p) {
-    const Geom& g = p.g;
-    const int k = blockIdx.x * kSX + threadIdx.x;
-    const int j = blockIdx.y * kSY + threadIdx.y;
-    if (k > g.nz || j > g.ny) return;
-    const int i0 = blockIdx.z * p.ichunk;
-    const int i1 = min(i0 + p.ichunk, g.nx + 1);
-    const long long vol = g.vol, si = g.si, sj = g.sj;
-    const T* __restrict__ aE = p.aE;
-    const T* __restrict__ bE = p.bE;
-    const T* __restrict__ E = p.e;
-    const T* __restrict__ H = p.h;
-    long long o = pidx(g, i0, j, k);
-    T hz_im = __ldg(H + 2 * vol + o - si);
-    T hy_im = __ldg(H + vol + o - si);
-    EPlane<T> cur, nxt;
-    load_E_plane(cur, aE, bE, E, H, o, vol, sj);
-    for (int i = i0; i < i1; ++i) {
-        if (i + 1 < i1) load_E_plane(nxt, aE, bE, E, H, o + si, vol, sj);
-        compute_E(p, cur, hz_im, hy_im, i, j, k, o, vol);
-        cur = nxt;
-        o += si;
-    }
-}
-
-template <typename T>
-__device__ __forceinline__ void compute_H(const StencilArgs<T>& p, const HPlane<T>& cur, T& ez_ip, T& ey_ip,
-                                          int i, int j, int k, long long o, long long vol) {
-    T* __restrict__ H = p.h;
+__device__ __forceinline__ void compute_H(const StencilArgs<T>& p, const Coef<T>& c, const HFld<T>& cur, T& ez_ip,
+                                          T& ey_ip, int b, int i, int j, int k, long long o, long long vol) {
+    T* __restrict__ H = p.h + (long long)b * 3 * vol;
     const T cx = ((cur.ez_jp - cur.ez) - cur.ey_kp) + cur.ey;
     const T cy = ((cur.ex_kp - cur.ex) - ez_ip) + cur.ez;
     const T cz = ((ey_ip - cur.ey) - cur.ex_jp) + cur.ex;
-    T hx = cur.ax * cur.hx - cur.bx * cx;
-    T hy = cur.ay * cur.hy - cur.by * cy;
-    T hz = cur.az * cur.hz - cur.bz * cz;
+    T hx = c.ax * cur.hx - c.bx * cx;
+    T hy = c.ay * cur.hy - c.by * cy;
+    T hz = c.az * cur.hz - c.bz * cz;
     for (int fi = 0; fi < p.nfaces; ++fi) {
         const FaceDev& f = p.f[fi];
         const int coord = (f.axis == 0) ? i : ((f.axis == 1) ? j : k);
         const int l = coord - f.lo;
         if ((unsigned)l >= (unsigned)f.n) continue;
-        const long long s = slab_index_s<T>(f, l, i, j, k);
+        const long long s = slab_index_s(f, l, i, j, k);
         const T* bcc = static_cast<const T*>(f.bcc);
         const T cb = bcc[l], cc = bcc[f.n + l], cck = bcc[2 * f.n + l];
-        T* psi = static_cast<T*>(f.psi);
+        T* psi = static_cast<T*>(f.psi) + (long long)b * 4 * f.slab;
         T d1, d2;
         if (f.axis == 0) {
             d1 = ez_ip - cur.ez;
@@ -204,14 +214,14 @@ __device__ __forceinline__ void compute_H(const StencilArgs<T>& p, const HPlane<
         if (!f.air[s2]) p2 = T(0);
         psi[s2] = p2;
         if (f.axis == 0) {
-            hy = hy - cur.by * (cck * d1 + p1);
-            hz = hz + cur.bz * (cck * d2 + p2);
+            hy = hy - c.by * (cck * d1 + p1);
+            hz = hz + c.bz * (cck * d2 + p2);
         } else if (f.axis == 1) {
-            hx = hx + cur.bx * (cck * d1 + p1);
-            hz = hz - cur.bz * (cck * d2 + p2);
+            hx = hx + c.bx * (cck * d1 + p1);
+            hz = hz - c.bz * (cck * d2 + p2);
         } else {
-            hx = hx - cur.bx * (cck * d1 + p1);
-            hy = hy + cur.by * (cck * d2 + p2);
+            hx = hx - c.bx * (cck * d1 + p1);
+            hy = hy + c.by * (cck * d2 + p2);
         }
     }
     H[o] = hx;
@@ -221,49 +231,112 @@ __device__ __forceinline__ void compute_H(const StencilArgs<T>& p, const HPlane<
     ey_ip = cur.ey;
 }
 
-template <typename T>
-__global__ void __launch_bounds__(kSX* kSY) k_update_H_stream(const StencilArgs<T> p) {
+// Field sets map to the warps of one CTA: warp row ty handles field set
+// b = ty % B of grid row j = blockIdx.y * rows + ty / B.  Each thread runs the
+// single-field-set pipeline; the B warps that share a cell load the same
+// coefficients, which the first of them brings from HBM and the others find
+// in L1/L2, so the coefficients cross HBM once per cell for all field sets
+// while every thread keeps a full plane of loads in flight.
+template <typename T, int CK>
+__global__ void __launch_bounds__(512) k_update_E_stream(const StencilArgs<T> p) {
     const Geom& g = p.g;
+    const int B = p.B;
+    const int b = threadIdx.y % B;
     const int k = blockIdx.x * kSX + threadIdx.x;
-    const int j = blockIdx.y * kSY + threadIdx.y;
+    const int j = blockIdx.y * (blockDim.y / B) + threadIdx.y / B;
     if (k > g.nz || j > g.ny) return;
     const int i0 = blockIdx.z * p.ichunk;
     const int i1 = min(i0 + p.ichunk, g.nx + 1);
-    const long long vol = g.vol, si = g.si, sj = g.sj;
+    const long long vol = g.vol, si = g.si, sj = g.sj, fs = 3 * vol;
+    const T* __restrict__ aE = p.aE;
+    const T* __restrict__ bE = p.bE;
+    const T* E = p.e + b * fs;
+    const T* __restrict__ H = p.h + b * fs;
+    long long o = pidx(g, i0, j, k);
+    T hz_im = __ldg(H + 2 * vol + o - si);
+    T hy_im = __ldg(H + vol + o - si);
+    Coef<T> cc, cn;
+    EFld<T> fc, fn;
+    load_coef_k<T, CK>(cc, p, 0, aE, bE, o, vol);
+    load_efld(fc, E, H, o, vol, sj);
+    for (int i = i0; i < i1; ++i) {
+        if (i + 1 < i1) {
+            load_coef_k<T, CK>(cn, p, 0, aE, bE, o + si, vol);
+            load_efld(fn, E, H, o + si, vol, sj);
+        }
+        compute_E(p, cc, fc, hz_im, hy_im, b, i, j, k, o, vol);
+        cc = cn;
+        fc = fn;
+        o += si;
+    }
+}
+
+template <typename T, int CK>
+__global__ void __launch_bounds__(512) k_update_H_stream(const StencilArgs<T> p) {
+    const Geom& g = p.g;
+    const int B = p.B;
+    const int b = threadIdx.y % B;
+    const int k = blockIdx.x * kSX + threadIdx.x;
+    const int j = blockIdx.y * (blockDim.y / B) + threadIdx.y / B;
+    if (k > g.nz || j > g.ny) return;
+    const int i0 = blockIdx.z * p.ichunk;
+    const int i1 = min(i0 + p.ichunk, g.nx + 1);
+    const long long vol = g.vol, si = g.si, sj = g.sj, fs = 3 * vol;
     const T* __restrict__ aH = p.aH;
     const T* __restrict__ bH = p.bH;
-    const T* __restrict__ H = p.h;
-    const T* __restrict__ E = p.e;
+    const T* H = p.h + b * fs;
+    const T* __restrict__ E = p.e + b * fs;
     // march down: the x-neighbours (E at i+1) of the first plane
     long long o = pidx(g, i1 - 1, j, k);
     T ez_ip = __ldg(E + 2 * vol + o + si);
     T ey_ip = __ldg(E + vol + o + si);
-    HPlane<T> cur, nxt;
-    load_H_plane(cur, aH, bH, H, E, o, vol, sj);
+    Coef<T> cc, cn;
+    HFld<T> fc, fn;
+    load_coef_k<T, CK>(cc, p, 1, aH, bH, o, vol);
+    load_hfld(fc, H, E, o, vol, sj);
     for (int i = i1 - 1; i >= i0; --i) {
-        if (i - 1 >= i0) load_H_plane(nxt, aH, bH, H, E, o - si, vol, sj);
-        compute_H(p, cur, ez_ip, ey_ip, i, j, k, o, vol);
-        cur = nxt;
+        if (i - 1 >= i0) {
+            load_coef_k<T, CK>(cn, p, 1, aH, bH, o - si, vol);
+            load_hfld(fn, H, E, o - si, vol, sj);
+        }
+        compute_H(p, cc, fc, ez_ip, ey_ip, b, i, j, k, o, vol);
+        cc = cn;
+        fc = fn;
         o -= si;
     }
 }
 
+int block_rows_y(int B) { return B <= 8 ? 8 : B; }
+
 }  // namespace
 
+bool stream_batch_supported(int B) { return B == 1 || B == 2 || B == 4 || B == 8 || B == 16; }
+
 template <typename T>
-int stream_occupancy() {
-    int a = 0, b = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_update_E_stream<T>, kSX * kSY, 0);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_update_H_stream<T>, kSX * kSY, 0);
-    const int m = a < b ? a : b;
+int stream_occupancy(int B, int coef_kind) {
+    int a = 0, c = 0;
+    const int threads = kSX * block_rows_y(B);
+    if (coef_kind == kCoefF16) {
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_update_E_stream<T, kCoefF16>, threads, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, k_update_H_stream<T, kCoefF16>, threads, 0);
+    } else if (coef_kind == kCoefBF16) {
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_update_E_stream<T, kCoefBF16>, threads, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, k_update_H_stream<T, kCoefBF16>, threads, 0);
+    } else {
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_update_E_stream<T, kCoefNative>, threads, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, k_update_H_stream<T, kCoefNative>, threads, 0);
+    }
+    const int m = a < c ? a : c;
     return m < 1 ? 1 : m;
 }
-template int stream_occupancy<float>();
-template int stream_occupancy<double>();
+template int stream_occupancy<float>(int, int);
+template int stream_occupancy<double>(int, int);
 
-StreamPlan plan_stream(const Geom& g, int sm_count, int ctas_per_sm) {
+StreamPlan plan_stream(const Geom& g, int sm_count, int ctas_per_sm, int B) {
     StreamPlan s{};
-    const int bx = (g.nz + 1 + kSX - 1) / kSX, by = (g.ny + 1 + kSY - 1) / kSY;
+    s.block_y = block_rows_y(B);
+    const int rows = s.block_y / B;
+    const int bx = (g.nz + 1 + kSX - 1) / kSX, by = (g.ny + 1 + rows - 1) / rows;
     const int nplanes = g.nx + 1;
     const int per_wave = sm_count * ctas_per_sm;
     double best = -1.0;
@@ -288,20 +361,52 @@ StreamPlan plan_stream(const Geom& g, int sm_count, int ctas_per_sm) {
 }
 
 template <typename T>
-void launch_update_E_stream(StencilArgs<T> a, const StreamPlan& sp, cudaStream_t s) {
+void launch_stream_half(StencilArgs<T> a, const StreamPlan& sp, int which, cudaStream_t s) {
     a.ichunk = sp.ichunk;
-    k_update_E_stream<T><<<dim3(sp.grid_x, sp.grid_y, sp.grid_z), dim3(kSX, kSY, 1), 0, s>>>(a);
+    const dim3 grid(sp.grid_x, sp.grid_y, sp.grid_z), block(kSX, sp.block_y, 1);
+    switch (a.coef_kind * 2 + which) {
+        case 2 * kCoefF16: k_update_E_stream<T, kCoefF16><<<grid, block, 0, s>>>(a); break;
+        case 2 * kCoefF16 + 1: k_update_H_stream<T, kCoefF16><<<grid, block, 0, s>>>(a); break;
+        case 2 * kCoefBF16: k_update_E_stream<T, kCoefBF16><<<grid, block, 0, s>>>(a); break;
+        case 2 * kCoefBF16 + 1: k_update_H_stream<T, kCoefBF16><<<grid, block, 0, s>>>(a); break;
+        case 1: k_update_H_stream<T, kCoefNative><<<grid, block, 0, s>>>(a); break;
+        default: k_update_E_stream<T, kCoefNative><<<grid, block, 0, s>>>(a); break;
+    }
 }
+
+template void launch_stream_half<float>(StencilArgs<float>, const StreamPlan&, int, cudaStream_t);
+template void launch_stream_half<double>(StencilArgs<double>, const StreamPlan&, int, cudaStream_t);
+
+}  // namespace fitb
+
+namespace fitb {
+namespace {
+
+template <typename T, int CK>
+__global__ void k_compact(const T* __restrict__ src, unsigned short* __restrict__ dst, long long n, float inv_scale) {
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+        const float v = (float)src[q] * inv_scale;
+        if constexpr (CK == kCoefF16)
+            dst[q] = __half_as_ushort(__float2half_rn(v));
+        else
+            dst[q] = __bfloat16_as_ushort(__float2bfloat16_rn(v));
+    }
+}
+
+}  // namespace
 
 template <typename T>
-void launch_update_H_stream(StencilArgs<T> a, const StreamPlan& sp, cudaStream_t s) {
-    a.ichunk = sp.ichunk;
-    k_update_H_stream<T><<<dim3(sp.grid_x, sp.grid_y, sp.grid_z), dim3(kSX, kSY, 1), 0, s>>>(a);
+void launch_compact(const T* src, unsigned short* dst, long long n, float inv_scale, int coef_kind, cudaStream_t s) {
+    const int threads = 256;
+    const long long want = (n + threads - 1) / threads;
+    const int blocks = (int)(want < 148 * 16 ? want : 148 * 16);
+    if (blocks < 1) return;
+    if (coef_kind == kCoefF16)
+        k_compact<T, kCoefF16><<<blocks, threads, 0, s>>>(src, dst, n, inv_scale);
+    else
+        k_compact<T, kCoefBF16><<<blocks, threads, 0, s>>>(src, dst, n, inv_scale);
 }
-
-template void launch_update_E_stream<float>(StencilArgs<float>, const StreamPlan&, cudaStream_t);
-template void launch_update_E_stream<double>(StencilArgs<double>, const StreamPlan&, cudaStream_t);
-template void launch_update_H_stream<float>(StencilArgs<float>, const StreamPlan&, cudaStream_t);
-template void launch_update_H_stream<double>(StencilArgs<double>, const StreamPlan&, cudaStream_t);
+template void launch_compact<float>(const float*, unsigned short*, long long, float, int, cudaStream_t);
+template void launch_compact<double>(const double*, unsigned short*, long long, float, int, cudaStream_t);
 
 }  // namespace fitb

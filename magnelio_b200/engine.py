@@ -131,6 +131,18 @@ class FitEngine:
         keep = arrs  # noqa: F841 (kept alive across the call)
         check(self._lib.fitb_set_coeffs_native(self._h, *ptrs))
 
+    COEF_STORAGE = {"native": 0, "f16": 1, "bf16": 2}
+
+    def set_coefficient_storage(self, kind: str) -> None:
+        """Coefficient storage of the stencil kernels: "native" (field
+        dtype), "f16" or "bf16" (16-bit with a power-of-two scale per
+        component; arithmetic stays in the field dtype).  The 16-bit forms
+        round each coefficient, so the march departs from the reference's
+        by more than round-off."""
+        if kind not in self.COEF_STORAGE:
+            raise ValueError(f"coefficient storage {kind!r}; expected one of {sorted(self.COEF_STORAGE)}")
+        check(self._lib.fitb_set_coeff_storage(self._h, self.COEF_STORAGE[kind]))
+
     def set_fields(self, e=None, h=None, b: int = 0) -> None:
         ea = None if e is None else np.ascontiguousarray(np.asarray(e, dtype=self.dtype).ravel())
         ha = None if h is None else np.ascontiguousarray(np.asarray(h, dtype=self.dtype).ravel())

@@ -107,12 +107,16 @@ def test_graph_chunks_and_single_steps_agree(name):
 
 @pytest.mark.parametrize("name", ["cpml_box", "lumped_dft"])
 def test_stencil_variants_agree(name, monkeypatch):
-    """The software-pipelined stencil (default for one field set), the
-    bulk-copy pipeline and the batched kernel run the same arithmetic."""
+    """The software-pipelined stencil, the vectorised-plane stencil (each
+    vector width and register cap), the bulk-copy pipeline and the simple
+    kernel run the same arithmetic."""
     p, d, n = load_golden(name)
     outs = []
-    for mode in ("stream", "bulk", "simple"):
+    modes = [("stream", None), ("bulk", None), ("simple", None)] + [("vec", str(v)) for v in range(4)]
+    for mode, variant in modes:
         monkeypatch.setenv("FITB_STENCIL", mode)
+        if variant is not None:
+            monkeypatch.setenv("FITB_VEC_VARIANT", variant)
         with p.build_engine("single") as eng:
             eng.step(n)
             outs.append(eng.read_fields())
@@ -178,6 +182,39 @@ def test_batch_field_sets_are_independent(monkeypatch):
         assert np.array_equal(vis[b][0], V) and np.array_equal(vis[b][1], I)
 
 
+@pytest.mark.parametrize("batch", [2, 4])
+def test_batched_stream_kernel_matches_solo_runs(batch):
+    """The batched default kernel (coefficients read once for all field
+    sets) reproduces each field set's solo run: alone and in the mix give the
+    same result within round-off."""
+    p0, d, n = load_golden("lumped_dft")
+    rng = np.random.default_rng(9)
+    inits = [rng.standard_normal(p0.alpha_E.size) * (p0.beta_E != 0) * 1e-3 for _ in range(batch)]
+    scales = [1.0 + 0.25 * b for b in range(batch)]
+    solo = []
+    for b in range(batch):
+        q = load_golden("lumped_dft")[0]
+        q.e0 = [inits[b]]
+        q.lumped[0].v_src = [q.lumped[0].v_src[0] * scales[b]]
+        with q.build_engine("single") as eng:
+            eng.step(n)
+            solo.append((eng.read_fields(), eng.read_vi(), eng.read_dft(0, "Ez")))
+    q = load_golden("lumped_dft")[0]
+    q.batch = batch
+    q.e0 = inits
+    q.h0 = [q.h0[0]] * batch
+    q.lumped[0].v_src = [q.lumped[0].v_src[0] * s for s in scales]
+    with q.build_engine("single") as eng:
+        eng.step(n)
+        for b in range(batch):
+            (e, h), (V, I), dft = solo[b]
+            eb, hb = eng.read_fields(b)
+            Vb, Ib = eng.read_vi(b)
+            assert _rel(eb, e) < 1e-6 and _rel(hb, h) < 1e-6
+            assert _rel(Vb, V) < 1e-6 and _rel(Ib, I) < 1e-6
+            assert _rel(eng.read_dft(0, "Ez", b), dft) < 1e-6
+
+
 def test_matches_oracle_beyond_fixture_length():
     """Float64 engine vs the float64 oracle past the fixture's step count on
     the Mur/complement/DTBC-extension case (crosses the 512-sample kernel)."""
@@ -209,3 +246,79 @@ def test_missing_dtbc_table_is_an_error_not_a_fault():
             eng.step(10_000)
         eng.step(10)  # the handle stays usable
         assert eng.steps_done == 10
+
+
+def _quantize16(x, kind):
+    """Host model of the compact coefficient storage of one component:
+    power-of-two scale putting max |x| in [2^13, 2^14), 16-bit round to
+    nearest even, decoded back to float32."""
+    x = np.asarray(x, dtype=np.float32)
+    m = float(np.max(np.abs(x))) if x.size else 0.0
+    e = int(np.frexp(m)[1]) - 1 if m > 0 else 13
+    e = min(max(e, -100), 100)
+    inv, s = np.float32(2.0 ** (13 - e)), np.float32(2.0 ** (e - 13))
+    y = x * inv
+    if kind == "f16":
+        q = y.astype(np.float16).astype(np.float32)
+    else:  # bfloat16: round the float32 bits to the upper 16, nearest even
+        b = y.view(np.uint32).astype(np.uint64)
+        b = (b + 0x7FFF + ((b >> 16) & 1)) >> 16 << 16
+        q = b.astype(np.uint32).view(np.float32)
+    return q * s
+
+
+@pytest.mark.parametrize("kind", ["f16", "bf16"])
+def test_compact_coefficients_decode_exactly(kind):
+    """The 16-bit coefficient storage is the host model's quantisation
+    exactly: a native run on host-quantised coefficients and a compact run on
+    the original coefficients give the same bits."""
+    from magnelio_b200.engine import FitEngine
+
+    d = dict(np.load(__import__("conftest").GOLDEN / "kernel_sweep.npz"))
+    nx, ny, nz = (int(v) for v in d["dims"])
+    names = {"aE": ["in.aEx", "in.aEy", "in.aEz"], "bE": ["in.bEx", "in.bEy", "in.bEz"],
+             "aH": ["in.aHx", "in.aHy", "in.aHz"], "bH": ["in.bHx", "in.bHy", "in.bHz"]}
+    orig = {a: np.concatenate([d[k].ravel().astype(np.float32) for k in ks]) for a, ks in names.items()}
+    quant = {a: np.concatenate([_quantize16(d[k].ravel(), kind) for k in ks]) for a, ks in names.items()}
+    e0 = np.concatenate([d[k].ravel() for k in ("in.Ex", "in.Ey", "in.Ez")]).astype(np.float32)
+    h0 = np.concatenate([d[k].ravel() for k in ("in.Hx", "in.Hy", "in.Hz")]).astype(np.float32)
+    outs = []
+    for coefs, storage in ((quant, "native"), (orig, kind)):
+        with FitEngine(nx, ny, nz, 1e-12, precision="single") as eng:
+            eng.set_coefficient_storage(storage)
+            eng.set_coefficients_native(coefs["aE"], coefs["bE"], coefs["aH"], coefs["bH"])
+            eng.set_fields(e0, h0)
+            eng.step(3)
+            outs.append(eng.read_fields())
+    assert np.array_equal(outs[0][0], outs[1][0]) and np.array_equal(outs[0][1], outs[1][1])
+
+
+# Departure of the 16-bit coefficient storage from the reference march on a
+# pulse run, relative to the run's peak fields: float16 rounds each
+# coefficient by at most 2^-11, bfloat16 by 2^-8.
+COMPACT_TOL = {"f16": 2e-3, "bf16": 2e-2}
+
+
+@pytest.mark.parametrize("kind", ["f16", "bf16"])
+@pytest.mark.parametrize("name", ["cpml_box", "lumped_dft"])
+def test_compact_coefficients_stay_near_reference(kind, name):
+    pe, ph = _peaks(name)
+    p, d, n = load_golden(name)
+    with p.build_engine("single") as eng:
+        eng.set_coefficient_storage(kind)
+        eng.step(n)
+        e, h = eng.read_fields()
+    de, dh = _rel(e, d["out.e"], pe), _rel(h, d["out.h"], ph)
+    print(f"{name} {kind}: e {de:.3g} h {dh:.3g}")
+    assert de < COMPACT_TOL[kind] and dh < COMPACT_TOL[kind]
+
+
+def test_compact_coefficients_need_the_stream_kernels(monkeypatch):
+    from magnelio_b200._lib import FitbError
+
+    monkeypatch.setenv("FITB_STENCIL", "simple")
+    p, d, n = load_golden("cpml_box")
+    with p.build_engine("single") as eng:
+        with pytest.raises(FitbError, match="stream stencil"):
+            eng.set_coefficient_storage("f16")
+        eng.step(2)
