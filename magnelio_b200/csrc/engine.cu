@@ -94,16 +94,19 @@ struct FaceHost {
     int face = 0;
     FaceDev dev{};
     DevBuf psi, air, bcc;
+    DevBuf psi2;  // the fused step's second psi buffer
 };
 
 struct LumpedHost {
     LumpedDev dev{};
+    std::vector<long long> off_host;  // E offsets the element writes
     DevBuf off, sign, beta, src, st;
     std::vector<double> src_host;  // [B][n_src]
 };
 
 struct ModalHost {
     ModalDev dev{};
+    std::vector<long long> port_e_host;  // E offsets the port writes
     int n_modes = 0;
     DevBuf port_e, int_e, port_h, me_port, me_int, mh_port, eprof, vprof, hprof;
     DevBuf comp_r, comp_live;
@@ -124,7 +127,7 @@ struct DftHost {
     int i0, i1, j0, j1, k0, k1;
 };
 
-constexpr int kModeSimple = 0, kModeStream = 1, kModeBulk = 2, kModeVec = 3;
+constexpr int kModeSimple = 0, kModeStream = 1, kModeBulk = 2, kModeVec = 3, kModeFused = 4;
 
 }  // namespace
 
@@ -139,6 +142,12 @@ struct Handle {
     double dt = 0.0;
     cudaStream_t stream = nullptr;
     DevBuf e, h, aE, bE, aH, bH, meps, mmu, staging;
+    // Fused step: second field buffers; `cur` names the buffer set that
+    // holds the current fields (always 0 for the in-place kernels).
+    DevBuf e2, h2;
+    int cur = 0;
+    DevBuf fix_cells;  // int4 (i, j, k, 0): H cells next to port-written E edges
+    int n_fix = 0;
     bool coeffs_set = false;
     std::vector<std::unique_ptr<FaceHost>> faces;
     std::vector<std::unique_ptr<LumpedHost>> lumped;
@@ -158,8 +167,8 @@ struct Handle {
     DevBuf absmax;        // [B]
     DevBuf energy_partials, energy_out;
     int energy_blocks = 1184;
-    cudaGraphExec_t graph_chunk = nullptr;
-    cudaGraphExec_t graph_one = nullptr;
+    cudaGraphExec_t graph_chunk[2] = {nullptr, nullptr};  // per starting buffer set
+    cudaGraphExec_t graph_one[2] = {nullptr, nullptr};
     int chunk = 16;
     bool graphs_valid = false;
     long long launches = 0;
@@ -169,6 +178,7 @@ struct Handle {
     BulkPlan plan{};
     int stencil_mode = 0;  // kModeSimple / kModeStream / kModeBulk / kModeVec
     int vec_variant = 0;   // vector width x register cap of the vec kernels
+    int fused_tj = 8;      // warps (rows along j) per CTA of the fused step
     StreamPlan splan{};
     DevBuf status;
     // Compact coefficient storage of the stream kernels (kCoefF16 /
@@ -181,12 +191,18 @@ struct Handle {
     double coef_max[4][3] = {};
 
     ~Handle() {
-        if (graph_chunk) cudaGraphExecDestroy(graph_chunk);
-        if (graph_one) cudaGraphExecDestroy(graph_one);
+        for (int q = 0; q < 2; ++q) {
+            if (graph_chunk[q]) cudaGraphExecDestroy(graph_chunk[q]);
+            if (graph_one[q]) cudaGraphExecDestroy(graph_one[q]);
+        }
         if (stream) cudaStreamDestroy(stream);
     }
 
     long long e_block() const { return 3 * g.vol; }
+    DevBuf& Ec() { return cur ? e2 : e; }
+    DevBuf& Hc() { return cur ? h2 : h; }
+    DevBuf& En() { return cur ? e : e2; }
+    DevBuf& Hn() { return cur ? h : h2; }
     long long nE() const {
         return (long long)g.nx * (g.ny + 1) * (g.nz + 1) + (long long)(g.nx + 1) * g.ny * (g.nz + 1) +
                (long long)(g.nx + 1) * (g.ny + 1) * g.nz;
@@ -278,9 +294,11 @@ void unpack3(Handle& H, const T* dev_padded, T* host_flat, int c0) {
 }
 
 void invalidate_graphs(Handle& H) {
-    if (H.graph_chunk) cudaGraphExecDestroy(H.graph_chunk);
-    if (H.graph_one) cudaGraphExecDestroy(H.graph_one);
-    H.graph_chunk = H.graph_one = nullptr;
+    for (int q = 0; q < 2; ++q) {
+        if (H.graph_chunk[q]) cudaGraphExecDestroy(H.graph_chunk[q]);
+        if (H.graph_one[q]) cudaGraphExecDestroy(H.graph_one[q]);
+        H.graph_chunk[q] = H.graph_one[q] = nullptr;
+    }
     H.graphs_valid = false;
 }
 
@@ -320,6 +338,40 @@ void ensure_capacity(Handle& H, long long need) {
     invalidate_graphs(H);
 }
 
+// H cells whose update reads an E edge that a port writes between the E and
+// the H update: the H update of cell (i, j, k) reads E at (i, j, k),
+// (i+1, j, k), (i, j+1, k) and (i, j, k+1).
+void build_fix_cells(Handle& H) {
+    std::vector<long long> keys;
+    auto add_edge = [&](long long off) {
+        const long long r = off % H.g.vol;  // drop the component
+        const int i = (int)(r / H.g.si) - 2;
+        const long long rr = r % H.g.si;
+        const int j = (int)(rr / H.g.sj), k = (int)(rr % H.g.sj);
+        const int cand[4][3] = {{i, j, k}, {i - 1, j, k}, {i, j - 1, k}, {i, j, k - 1}};
+        for (auto& c : cand) {
+            if (c[0] < 0 || c[0] > H.g.nx || c[1] < 0 || c[1] > H.g.ny || c[2] < 0 || c[2] > H.g.nz) continue;
+            keys.push_back(pidx(H.g, c[0], c[1], c[2]));
+        }
+    };
+    for (auto& lp : H.lumped)
+        for (long long o : lp->off_host) add_edge(o);
+    for (auto& mp : H.modal)
+        for (long long o : mp->port_e_host) add_edge(o);
+    std::sort(keys.begin(), keys.end());
+    keys.erase(std::unique(keys.begin(), keys.end()), keys.end());
+    std::vector<int4> cells;
+    cells.reserve(keys.size());
+    for (long long key : keys) {
+        const int i = (int)(key / H.g.si) - 2;
+        const long long rr = key % H.g.si;
+        cells.push_back(make_int4(i, (int)(rr / H.g.sj), (int)(rr % H.g.sj), 0));
+    }
+    if (cells.empty()) cells.push_back(make_int4(0, 0, 0, 0));  // keep a valid pointer
+    upload(H.fix_cells, cells);
+    H.n_fix = (int)keys.size();
+}
+
 void refresh_port_tables(Handle& H) {
     if (!H.port_tables_dirty) return;
     std::vector<LumpedDev> ld;
@@ -354,6 +406,7 @@ void refresh_port_tables(Handle& H) {
         dd.push_back(d);
     }
     upload(H.d_dft, dd);
+    if (H.stencil_mode == kModeFused) build_fix_cells(H);
     H.dft_stage_blocks = sb;
     H.dft_flush_blocks = fb;
     H.dft_flush_smem = smem;
@@ -365,14 +418,19 @@ StencilArgs<T> stencil_args(Handle& H) {
     StencilArgs<T> a{};
     a.g = H.g;
     a.B = H.B;
-    a.e = H.e.as<T>();
-    a.h = H.h.as<T>();
+    a.e = H.Ec().as<T>();
+    a.h = H.Hc().as<T>();
+    a.e_next = H.En().as<T>();
+    a.h_next = H.Hn().as<T>();
     a.aE = H.aE.as<T>();
     a.bE = H.bE.as<T>();
     a.aH = H.aH.as<T>();
     a.bH = H.bH.as<T>();
     a.nfaces = (int)H.faces.size();
-    for (int q = 0; q < a.nfaces; ++q) a.f[q] = H.faces[q]->dev;
+    for (int q = 0; q < a.nfaces; ++q) {
+        a.f[q] = H.faces[q]->dev;
+        if (H.cur) std::swap(a.f[q].psi, a.f[q].psi_next);
+    }
     a.ichunk = H.ichunk;
     a.coef_kind = (H.stencil_mode == kModeStream || H.stencil_mode == kModeVec) ? H.coef_kind : kCoefNative;
     for (int q = 0; q < 4; ++q) a.cq[q] = H.cq[q].as<unsigned short>();
@@ -439,10 +497,14 @@ PortsArgs ports_args(Handle& H) {
 // Grid of the stream / vec kernels for the handle's batch and coefficient
 // storage (occupancy depends on the kernel instance).
 void plan_stencil(Handle& H) {
-    if (H.stencil_mode != kModeStream && H.stencil_mode != kModeVec) return;
+    if (H.stencil_mode != kModeStream && H.stencil_mode != kModeVec && H.stencil_mode != kModeFused) return;
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, H.desc.device);
-    if (H.stencil_mode == kModeStream) {
+    if (H.stencil_mode == kModeFused) {
+        const int tj = H.fused_tj;
+        const int occ = H.prec == 4 ? fused_occupancy<float>(tj) : fused_occupancy<double>(tj);
+        H.splan = plan_fused(H.g, sms, occ, H.B, tj);
+    } else if (H.stencil_mode == kModeStream) {
         const int occ = H.prec == 4 ? stream_occupancy<float>(H.B, H.coef_kind)
                                     : stream_occupancy<double>(H.B, H.coef_kind);
         H.splan = plan_stream(H.g, sms, occ, H.B);
@@ -475,6 +537,13 @@ void launch_half(Handle& H, int which) {
     }
 }
 
+void launch_fused_any(Handle& H) {
+    if (H.prec == 4)
+        launch_fused_step<float>(stencil_args<float>(H), H.splan, H.stream);
+    else
+        launch_fused_step<double>(stencil_args<double>(H), H.splan, H.stream);
+}
+
 void launch_stencil_half(Handle& H, int which) {
     if (H.prec == 4)
         launch_half<float>(H, which);
@@ -482,25 +551,65 @@ void launch_stencil_half(Handle& H, int which) {
         launch_half<double>(H, which);
 }
 
+// Fused step: one launch for E and H from the current buffer set into the
+// other, then the ports on the new E (with the old H, which the two-pass
+// order shows them), the H fix-up next to port edges, the monitors on the
+// new fields; the buffer sets swap.
+template <typename T>
+int enqueue_step_fused(Handle& H) {
+    int n = 0;
+    PortsArgs pa = ports_args(H);
+    StencilArgs<T> sa = stencil_args<T>(H);
+    launch_fused_step<T>(sa, H.splan, H.stream);
+    ++n;
+    T* e_new = H.En().as<T>();
+    T* h_new = H.Hn().as<T>();
+    if (!H.modal.empty()) {
+        launch_modal<T>(e_new, H.Hc().as<T>(), pa, H.d_modal.as<ModalDev>(), (int)H.modal.size(), H.stream);
+        ++n;
+    }
+    if (!H.lumped.empty()) {
+        launch_lumped<T>(e_new, pa, H.d_lumped.as<LumpedDev>(), (int)H.lumped.size(), H.stream);
+        ++n;
+    }
+    if (H.n_fix > 0) {
+        launch_fix_H<T>(sa, H.fix_cells.as<int4>(), H.n_fix, H.stream);
+        ++n;
+    }
+    if (!H.dft.empty()) {
+        launch_dft_stage_all<T>(e_new, h_new, H.e_block(), H.e_block(), H.g, H.B, H.d_dft.as<DftDev>(),
+                                (int)H.dft.size(), H.dft_stage_blocks, H.step.as<long long>(), H.stream);
+        launch_dft_flush_all(H.B, H.d_dft.as<DftDev>(), (int)H.dft.size(), H.dft_flush_blocks, H.dft_flush_smem,
+                             H.step.as<long long>(), H.ticket.as<unsigned>(), H.stream);
+        n += 2;
+    } else {
+        launch_advance(H.step.as<long long>(), H.stream);
+        ++n;
+    }
+    H.cur ^= 1;
+    return n;
+}
+
 template <typename T>
 int enqueue_step(Handle& H) {
+    if (H.stencil_mode == kModeFused) return enqueue_step_fused<T>(H);
     int n = 0;
     PortsArgs pa = ports_args(H);
     launch_half<T>(H, 0);
     ++n;
     if (!H.modal.empty()) {
-        launch_modal<T>(H.e.as<T>(), H.h.as<T>(), pa, H.d_modal.as<ModalDev>(), (int)H.modal.size(), H.stream);
+        launch_modal<T>(H.Ec().as<T>(), H.Hc().as<T>(), pa, H.d_modal.as<ModalDev>(), (int)H.modal.size(), H.stream);
         ++n;
     }
     if (!H.lumped.empty()) {
-        launch_lumped<T>(H.e.as<T>(), pa, H.d_lumped.as<LumpedDev>(), (int)H.lumped.size(), H.stream);
+        launch_lumped<T>(H.Ec().as<T>(), pa, H.d_lumped.as<LumpedDev>(), (int)H.lumped.size(), H.stream);
         ++n;
     }
     launch_half<T>(H, 1);
     ++n;
     if (!H.dft.empty()) {
         // stage + flush of all monitors; the flush launch advances the step
-        launch_dft_stage_all<T>(H.e.as<T>(), H.h.as<T>(), H.e_block(), H.e_block(), H.g, H.B,
+        launch_dft_stage_all<T>(H.Ec().as<T>(), H.Hc().as<T>(), H.e_block(), H.e_block(), H.g, H.B,
                                 H.d_dft.as<DftDev>(), (int)H.dft.size(), H.dft_stage_blocks, H.step.as<long long>(),
                                 H.stream);
         launch_dft_flush_all(H.B, H.d_dft.as<DftDev>(), (int)H.dft.size(), H.dft_flush_blocks, H.dft_flush_smem,
@@ -515,8 +624,16 @@ int enqueue_step(Handle& H) {
 
 int enqueue_step_any(Handle& H) { return H.prec == 4 ? enqueue_step<float>(H) : enqueue_step<double>(H); }
 
+// Captures nsteps steps starting from the current buffer set; the host-side
+// buffer set index is restored (the graph has not run yet).
 cudaGraphExec_t capture(Handle& H, int nsteps, int* launches_per) {
     cudaGraph_t graph = nullptr;
+    const int cur0 = H.cur;
+    struct Restore {
+        Handle& H;
+        int c;
+        ~Restore() { H.cur = c; }
+    } restore{H, cur0};
     ck(cudaStreamBeginCapture(H.stream, cudaStreamCaptureModeThreadLocal), "begin capture");
     int per = 0;
     try {
@@ -583,21 +700,31 @@ void run_steps(Handle& H, long long nsteps) {
     refresh_port_tables(H);
     int per = 0;
     if (!H.graphs_valid) {
+        // graphs for each starting buffer set (one set for in-place kernels)
+        const int nsets = H.stencil_mode == kModeFused ? 2 : 1;
+        const int cur0 = H.cur;
         int p1 = 0, pc = 0;
-        H.graph_one = capture(H, 1, &p1);
-        H.graph_chunk = capture(H, H.chunk, &pc);
+        for (int q = 0; q < nsets; ++q) {
+            H.cur = q;
+            H.graph_one[q] = capture(H, 1, &p1);
+            H.graph_chunk[q] = capture(H, H.chunk, &pc);
+        }
+        H.cur = cur0;
         H.graphs_valid = true;
         H.launches_per_step = p1;
     }
     per = H.launches_per_step;
     if (nsteps == 0) return;
     long long left = nsteps;
+    const bool swaps = H.stencil_mode == kModeFused;
     while (left >= H.chunk) {
-        ck(cudaGraphLaunch(H.graph_chunk, H.stream), "graph launch");
+        ck(cudaGraphLaunch(H.graph_chunk[H.cur], H.stream), "graph launch");
+        if (swaps && (H.chunk & 1)) H.cur ^= 1;
         left -= H.chunk;
     }
     while (left > 0) {
-        ck(cudaGraphLaunch(H.graph_one, H.stream), "graph launch");
+        ck(cudaGraphLaunch(H.graph_one[H.cur], H.stream), "graph launch");
+        if (swaps) H.cur ^= 1;
         --left;
     }
     H.launches += (long long)per * nsteps;
@@ -606,7 +733,7 @@ void run_steps(Handle& H, long long nsteps) {
 
 template <typename T>
 void energy_impl(Handle& H, int b, double* out) {
-    launch_energy<T>(H.e.as<T>(), H.h.as<T>(), H.meps.as<T>(), H.mmu.as<T>(), H.g, b, H.e_block(),
+    launch_energy<T>(H.Ec().as<T>(), H.Hc().as<T>(), H.meps.as<T>(), H.mmu.as<T>(), H.g, b, H.e_block(),
                      H.energy_partials.as<double>(), H.energy_blocks, H.energy_out.as<double>(), H.stream);
     H.launches += 2;
     ck(cudaGetLastError(), "energy");
@@ -665,6 +792,7 @@ void add_cpml_impl(Handle& H, int face, int n_pml, const double* bt, const doubl
     d.dK = axis == 2 ? n_pml : H.g.nz + 1;
     d.slab = (long long)d.dI * d.dJ * d.dK;
     f->psi.alloc((size_t)H.B * 4 * d.slab * sizeof(T));
+    if (H.stencil_mode == kModeFused) f->psi2.alloc((size_t)H.B * 4 * d.slab * sizeof(T));
     std::vector<uint8_t> air((size_t)(4 * d.slab), 0);
     for (int q = 0; q < 4; ++q) {
         int ra, rb, rc;
@@ -686,6 +814,7 @@ void add_cpml_impl(Handle& H, int face, int n_pml, const double* bt, const doubl
     }
     upload(f->bcc, bcc);
     d.psi = f->psi.p;
+    d.psi_next = f->psi2.p;
     d.air = f->air.as<unsigned char>();
     d.bcc = f->bcc.p;
     H.faces.push_back(std::move(f));
@@ -732,8 +861,8 @@ void write_state(Handle& H, Writer& w) {
         if (w.out) {
             ev.resize((size_t)H.nE());
             hv.resize((size_t)H.nH());
-            unpack3<T>(H, H.e.as<T>() + (long long)b * H.e_block(), ev.data(), 0);
-            unpack3<T>(H, H.h.as<T>() + (long long)b * H.e_block(), hv.data(), 3);
+            unpack3<T>(H, H.Ec().as<T>() + (long long)b * H.e_block(), ev.data(), 0);
+            unpack3<T>(H, H.Hc().as<T>() + (long long)b * H.e_block(), hv.data(), 3);
         }
         if (w.out) {
             w.put(ev.data(), ev.size() * sizeof(T));
@@ -742,7 +871,10 @@ void write_state(Handle& H, Writer& w) {
             w.n += (size_t)(H.nE() + H.nH()) * sizeof(T);
         }
     }
-    for (auto& f : H.faces) dev_get(w, f->psi.p, f->psi.bytes);
+    for (auto& f : H.faces) {
+        const DevBuf& ps = H.cur ? f->psi2 : f->psi;
+        dev_get(w, ps.p, ps.bytes);
+    }
     for (auto& lp : H.lumped) dev_get(w, lp->st.p, lp->st.bytes);
     for (auto& mp : H.modal) {
         dev_get(w, mp->st.p, mp->st.bytes);
@@ -799,10 +931,13 @@ void read_state(Handle& H, Reader& r) {
         std::vector<T> ev((size_t)H.nE()), hv((size_t)H.nH());
         r.get(ev.data(), ev.size() * sizeof(T));
         r.get(hv.data(), hv.size() * sizeof(T));
-        pack3<T>(H, ev.data(), H.e.as<T>() + (long long)b * H.e_block(), 0);
-        pack3<T>(H, hv.data(), H.h.as<T>() + (long long)b * H.e_block(), 3);
+        pack3<T>(H, ev.data(), H.Ec().as<T>() + (long long)b * H.e_block(), 0);
+        pack3<T>(H, hv.data(), H.Hc().as<T>() + (long long)b * H.e_block(), 3);
     }
-    for (auto& f : H.faces) r.dev(f->psi.p, f->psi.bytes);
+    for (auto& f : H.faces) {
+        DevBuf& ps = H.cur ? f->psi2 : f->psi;
+        r.dev(ps.p, ps.bytes);
+    }
     for (auto& lp : H.lumped) r.dev(lp->st.p, lp->st.bytes);
     for (auto& mp : H.modal) {
         r.dev(mp->st.p, mp->st.bytes);
@@ -921,9 +1056,10 @@ int fitb_create(const fitb_desc* desc, fitb_handle** out) {
     H.ticket.alloc(sizeof(unsigned));
     {
         // FITB_STENCIL selects the stencil kernels: "stream" (default),
-        // "vec" (vectorised planes; FITB_VEC_VARIANT picks the vector width
-        // and register cap), "bulk" (cp.async.bulk pipeline, one field set)
-        // or "simple".
+        // "fused" (E and H in one pass over ping-pong buffers;
+        // FITB_FUSED_TJ = 8 or 16 rows per CTA), "vec" (vectorised planes;
+        // FITB_VEC_VARIANT picks the vector width and register cap), "bulk"
+        // (cp.async.bulk pipeline, one field set) or "simple".
         const char* mode = getenv("FITB_STENCIL");
         const std::string m = mode ? mode : "stream";
         H.stencil_mode = fitb::kModeSimple;
@@ -936,6 +1072,12 @@ int fitb_create(const fitb_desc* desc, fitb_handle** out) {
                    "bulk stencil smem attribute");
                 H.stencil_mode = fitb::kModeBulk;
             }
+        } else if (m == "fused") {
+            const char* t = getenv("FITB_FUSED_TJ");
+            H.fused_tj = (t && atoi(t) == 16 && H.prec == 4) ? 16 : 8;
+            H.e2.alloc(blk * H.B);
+            H.h2.alloc(blk * H.B);
+            H.stencil_mode = fitb::kModeFused;
         } else if (m == "vec" && H.B <= 8 && fitb::stream_batch_supported(H.B)) {
             const char* v = getenv("FITB_VEC_VARIANT");
             H.vec_variant = v ? std::max(0, std::min(3, atoi(v))) : 0;
@@ -1046,16 +1188,16 @@ int fitb_set_fields(fitb_handle* h, int32_t b, const void* e, size_t e_bytes, co
     if (e) {
         if (e_bytes != (size_t)H.nE() * H.esz) fail(FITB_ERR_ARG, "e buffer is %zu bytes, expected %zu", e_bytes, (size_t)H.nE() * H.esz);
         if (H.prec == 4)
-            fitb::pack3<float>(H, (const float*)e, H.e.as<float>() + (long long)b * H.e_block(), 0);
+            fitb::pack3<float>(H, (const float*)e, H.Ec().as<float>() + (long long)b * H.e_block(), 0);
         else
-            fitb::pack3<double>(H, (const double*)e, H.e.as<double>() + (long long)b * H.e_block(), 0);
+            fitb::pack3<double>(H, (const double*)e, H.Ec().as<double>() + (long long)b * H.e_block(), 0);
     }
     if (hf) {
         if (h_bytes != (size_t)H.nH() * H.esz) fail(FITB_ERR_ARG, "h buffer is %zu bytes, expected %zu", h_bytes, (size_t)H.nH() * H.esz);
         if (H.prec == 4)
-            fitb::pack3<float>(H, (const float*)hf, H.h.as<float>() + (long long)b * H.e_block(), 3);
+            fitb::pack3<float>(H, (const float*)hf, H.Hc().as<float>() + (long long)b * H.e_block(), 3);
         else
-            fitb::pack3<double>(H, (const double*)hf, H.h.as<double>() + (long long)b * H.e_block(), 3);
+            fitb::pack3<double>(H, (const double*)hf, H.Hc().as<double>() + (long long)b * H.e_block(), 3);
     }
     FITB_CATCH
 }
@@ -1067,16 +1209,16 @@ int fitb_read_fields(fitb_handle* h, int32_t b, void* e, size_t e_bytes, void* h
     if (e) {
         if (e_bytes != (size_t)H.nE() * H.esz) fail(FITB_ERR_ARG, "e buffer size mismatch");
         if (H.prec == 4)
-            fitb::unpack3<float>(H, H.e.as<float>() + (long long)b * H.e_block(), (float*)e, 0);
+            fitb::unpack3<float>(H, H.Ec().as<float>() + (long long)b * H.e_block(), (float*)e, 0);
         else
-            fitb::unpack3<double>(H, H.e.as<double>() + (long long)b * H.e_block(), (double*)e, 0);
+            fitb::unpack3<double>(H, H.Ec().as<double>() + (long long)b * H.e_block(), (double*)e, 0);
     }
     if (hf) {
         if (h_bytes != (size_t)H.nH() * H.esz) fail(FITB_ERR_ARG, "h buffer size mismatch");
         if (H.prec == 4)
-            fitb::unpack3<float>(H, H.h.as<float>() + (long long)b * H.e_block(), (float*)hf, 3);
+            fitb::unpack3<float>(H, H.Hc().as<float>() + (long long)b * H.e_block(), (float*)hf, 3);
         else
-            fitb::unpack3<double>(H, H.h.as<double>() + (long long)b * H.e_block(), (double*)hf, 3);
+            fitb::unpack3<double>(H, H.Hc().as<double>() + (long long)b * H.e_block(), (double*)hf, 3);
     }
     FITB_CATCH
 }
@@ -1115,6 +1257,7 @@ int fitb_add_lumped(fitb_handle* h, int32_t n_edges, const int64_t* flat_e_idx, 
         bsum += betas[q];
     }
     fitb::upload(lp->off, off);
+    lp->off_host = off;
     fitb::upload(lp->sign, std::vector<double>(signs, signs + n_edges));
     fitb::upload(lp->beta, std::vector<double>(betas, betas + n_edges));
     lp->st.alloc(sizeof(double) * 4 * H.B);
@@ -1205,6 +1348,7 @@ int fitb_add_modal_port(fitb_handle* h, const fitb_modal_desc* d, int32_t* out_i
     }
     for (int p = 0; p < nh; ++p) ph[(size_t)p] = H.flat_to_off(true, d->port_h_idx[p]);
     fitb::upload(mp->port_e, pe);
+    mp->port_e_host = pe;
     fitb::upload(mp->int_e, ie);
     fitb::upload(mp->port_h, ph);
     fitb::upload(mp->me_port, std::vector<double>(d->me_port, d->me_port + ne));
@@ -1480,6 +1624,25 @@ int fitb_time_stencil(fitb_handle* h, int32_t n_iter, double* ms_e, double* ms_h
     if (n_iter < 1 || !ms_e || !ms_h) fail(FITB_ERR_ARG, "bad argument");
     cudaEvent_t ev[3];
     for (auto& x : ev) ck(cudaEventCreate(&x), "event");
+    if (H.stencil_mode == fitb::kModeFused) {
+        // the whole E + H pass, alternating buffer sets; an even count
+        // leaves the current set where it was
+        const int n2 = 2 * ((n_iter + 1) / 2);
+        ck(cudaEventRecord(ev[0], H.stream), "event record");
+        for (int q = 0; q < n2; ++q) {
+            fitb::launch_fused_any(H);
+            H.cur ^= 1;
+        }
+        ck(cudaEventRecord(ev[1], H.stream), "event record");
+        ck(cudaEventSynchronize(ev[1]), "event sync");
+        H.launches += n2;
+        float f1 = 0.f;
+        ck(cudaEventElapsedTime(&f1, ev[0], ev[1]), "elapsed");
+        for (auto& x : ev) cudaEventDestroy(x);
+        *ms_e = f1 / n2;
+        *ms_h = 0.0;
+        return FITB_OK;
+    }
     ck(cudaEventRecord(ev[0], H.stream), "event record");
     for (int q = 0; q < n_iter; ++q) fitb::launch_stencil_half(H, 0);
     ck(cudaEventRecord(ev[1], H.stream), "event record");

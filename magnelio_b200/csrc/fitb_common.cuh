@@ -52,6 +52,7 @@ struct FaceDev {
     int dI, dJ, dK; // slab dims
     long long slab; // dI * dJ * dK
     void* psi;      // [B][4][slab] field dtype: E1, E2, H1, H2
+    void* psi_next; // fused step: the buffer the new psi goes to
     const unsigned char* air;  // [4][slab] 0/1
     const void* bcc;           // [3][n] field dtype: b, c, ck
 };
@@ -64,6 +65,8 @@ struct StencilArgs {
     int B;
     T* e;  // [B][3][vol]
     T* h;  // [B][3][vol]
+    T* e_next;  // fused step: the buffers the new E and H go to
+    T* h_next;
     const T* aE;
     const T* bE;  // [3][vol]
     const T* aH;
@@ -114,6 +117,17 @@ int vec_occupancy(int variant, int coef_kind);
 StreamPlan plan_vec(const Geom& g, int sm_count, int ctas_per_sm, int B, int vk);
 template <typename T>
 void launch_vec_half(StencilArgs<T> a, const StreamPlan& sp, int variant, int which, cudaStream_t s);
+
+// Fused step (E then H in one i-march, stencil_fused.cu): reads e, h, psi
+// and writes e_next, h_next, psi_next.  block_y = TJ (8 or 16) warps.
+template <typename T>
+int fused_occupancy(int tj);
+StreamPlan plan_fused(const Geom& g, int sm_count, int ctas_per_sm, int B, int tj);
+template <typename T>
+void launch_fused_step(StencilArgs<T> a, const StreamPlan& sp, cudaStream_t s);
+// H update of listed cells (x, y, z = i, j, k) from h / psi and e_next.
+template <typename T>
+void launch_fix_H(const StencilArgs<T>& a, const int4* cells, int n, cudaStream_t s);
 
 // Bulk-copy (TMA) pipelined stencil kernels for a single field set.
 // status: device word set non-zero when a bounded pipeline wait gives up.

@@ -1,0 +1,392 @@
+// One leapfrog step (E update, then H update) in a single pass over the
+// grid: the fused i-march.
+//
+// Same arithmetic as the two-pass kernels (reference: numba_kernels.py:36-127
+// for the curl updates, cpml.py:343-516 for the psi recursion and its
+// correction); the step reads E, H and psi from one buffer set and writes
+// the new values to the other (the handle swaps them every step), so a CTA
+// never sees a neighbour's new values where it needs old ones.
+//
+// Work mapping: a CTA is 32 lanes along k by TJ warps along j and marches
+// over a chunk [i0, i1) of i planes.  At plane i a thread computes E_new(i)
+// of its cell (H_old at i-1 from registers, at j-1 by a load that the row
+// above has brought into L1, at k-1 by a warp shuffle) and then H_new(i-1)
+// (E_new at i from registers, at k+1 by a warp shuffle, at j+1 from the
+// next warp through shared memory).  The last lane and the last warp
+// compute E_new only as neighbours of the others' H: tiles overlap by one
+// column and one row, and those cells are stored by the neighbouring tile.
+// A chunk also computes E_new at its plane i1 (not stored) for H_new(i1-1).
+// One __syncthreads per plane orders the shared-memory exchange (written
+// after the reads of the same plane, double-buffered across planes).
+//
+// Ports write E between the E and the H update (operator.py:1351-1536,
+// lumped operator.py:134-166).  The H cells whose curl takes a port-written
+// E edge are recomputed afterwards from the old buffers by k_fix_H with the
+// same arithmetic (H_old, psi_old are still intact in the other buffers).
+#include "fitb_common.cuh"
+
+namespace fitb {
+
+namespace {
+
+template <typename T>
+struct FCoef {
+    T ax, ay, az, bx, by, bz;
+};
+
+// Everything a thread loads for one plane.
+template <typename T>
+struct FPlane {
+    T ex, ey, ez;             // E_old of the cell
+    T hx, hy, hz;             // H_old of the cell
+    T hz_jm, hx_jm;           // H_old at j-1
+    T hy_before, hx_before;   // H_old at k-1 (lane 0 only)
+    FCoef<T> ce, ch;          // alpha/beta of E and of H
+};
+
+template <typename T>
+__device__ __forceinline__ void load_coef3(FCoef<T>& c, const T* __restrict__ a, const T* __restrict__ b, long long o,
+                                           long long vol) {
+    c.ax = __ldg(a + o);
+    c.ay = __ldg(a + vol + o);
+    c.az = __ldg(a + 2 * vol + o);
+    c.bx = __ldg(b + o);
+    c.by = __ldg(b + vol + o);
+    c.bz = __ldg(b + 2 * vol + o);
+}
+
+template <typename T>
+__device__ __forceinline__ void load_plane(FPlane<T>& q, const StencilArgs<T>& p, const T* __restrict__ E,
+                                           const T* __restrict__ H, long long o, bool lane0) {
+    const long long vol = p.g.vol, sj = p.g.sj;
+    q.ex = __ldg(E + o);
+    q.ey = __ldg(E + vol + o);
+    q.ez = __ldg(E + 2 * vol + o);
+    q.hx = __ldg(H + o);
+    q.hy = __ldg(H + vol + o);
+    q.hz = __ldg(H + 2 * vol + o);
+    q.hz_jm = __ldg(H + 2 * vol + o - sj);
+    q.hx_jm = __ldg(H + o - sj);
+    q.hy_before = lane0 ? __ldg(H + vol + o - 1) : T(0);
+    q.hx_before = lane0 ? __ldg(H + o - 1) : T(0);
+    load_coef3(q.ce, p.aE, p.bE, o, vol);
+    load_coef3(q.ch, p.aH, p.bH, o, vol);
+}
+
+__device__ __forceinline__ long long slab_at(const FaceDev& f, int l, int i, int j, int k) {
+    const int a = (f.axis == 0) ? l : i;
+    const int b = (f.axis == 1) ? l : j;
+    const int c = (f.axis == 2) ? l : k;
+    return ((long long)a * f.dJ + b) * f.dK + c;
+}
+
+template <typename T>
+__device__ __forceinline__ unsigned mask_jk(const StencilArgs<T>& p, int j, int k) {
+    unsigned m = 0;
+    for (int q = 0; q < p.nfaces; ++q) {
+        const FaceDev& f = p.f[q];
+        const int c = f.axis == 1 ? j : k;
+        if (f.axis != 0 && (unsigned)(c - f.lo) < (unsigned)f.n) m |= 1u << q;
+    }
+    return m;
+}
+
+template <typename T>
+__device__ __forceinline__ unsigned mask_i(const StencilArgs<T>& p, int i) {
+    unsigned m = 0;
+    for (int q = 0; q < p.nfaces; ++q) {
+        const FaceDev& f = p.f[q];
+        if (f.axis == 0 && (unsigned)(i - f.lo) < (unsigned)f.n) m |= 1u << q;
+    }
+    return m;
+}
+
+// CPML of the E update of one cell (cpml.py:343-430): psi_next = air *
+// (b psi_old + c d), E -/+= beta (ck d + psi_next) on the two transverse
+// components, faces in `mask` order.  d1/d2 per face axis as in the
+// two-pass kernels.  `store`: write psi_next (owned cells only).
+template <typename T>
+__device__ __forceinline__ void cpml_E(const StencilArgs<T>& p, unsigned mask, int b, int i, int j, int k, T dx1,
+                                       T dx2, T dy1, T dy2, T dz1, T dz2, const FCoef<T>& c, T& ex, T& ey, T& ez,
+                                       bool store) {
+    while (mask) {
+        const int q = __ffs(mask) - 1;
+        mask &= mask - 1;
+        const FaceDev& f = p.f[q];
+        const int coord = (f.axis == 0) ? i : ((f.axis == 1) ? j : k);
+        const int l = coord - f.lo;
+        const long long s = slab_at(f, l, i, j, k);
+        const T* bcc = static_cast<const T*>(f.bcc);
+        const T cb = bcc[l], cc = bcc[f.n + l], cck = bcc[2 * f.n + l];
+        const long long off = (long long)b * 4 * f.slab;
+        const T* psi = static_cast<const T*>(f.psi) + off;
+        T* psin = static_cast<T*>(f.psi_next) + off;
+        const T d1 = f.axis == 0 ? dx1 : (f.axis == 1 ? dy1 : dz1);
+        const T d2 = f.axis == 0 ? dx2 : (f.axis == 1 ? dy2 : dz2);
+        T p1 = psi[s] * cb;
+        p1 = p1 + cc * d1;
+        if (!f.air[s]) p1 = T(0);
+        T p2 = psi[f.slab + s] * cb;
+        p2 = p2 + cc * d2;
+        if (!f.air[f.slab + s]) p2 = T(0);
+        if (store) {
+            psin[s] = p1;
+            psin[f.slab + s] = p2;
+        }
+        if (f.axis == 0) {
+            ey = ey + c.by * (cck * d1 + p1);
+            ez = ez - c.bz * (cck * d2 + p2);
+        } else if (f.axis == 1) {
+            ex = ex - c.bx * (cck * d1 + p1);
+            ez = ez + c.bz * (cck * d2 + p2);
+        } else {
+            ex = ex + c.bx * (cck * d1 + p1);
+            ey = ey - c.by * (cck * d2 + p2);
+        }
+    }
+}
+
+// CPML of the H update of one cell (cpml.py:432-516); psi components 2, 3.
+template <typename T>
+__device__ __forceinline__ void cpml_H(const StencilArgs<T>& p, unsigned mask, int b, int i, int j, int k, T dx1,
+                                       T dx2, T dy1, T dy2, T dz1, T dz2, const FCoef<T>& c, T& hx, T& hy, T& hz) {
+    while (mask) {
+        const int q = __ffs(mask) - 1;
+        mask &= mask - 1;
+        const FaceDev& f = p.f[q];
+        const int coord = (f.axis == 0) ? i : ((f.axis == 1) ? j : k);
+        const int l = coord - f.lo;
+        const long long s = slab_at(f, l, i, j, k);
+        const T* bcc = static_cast<const T*>(f.bcc);
+        const T cb = bcc[l], cc = bcc[f.n + l], cck = bcc[2 * f.n + l];
+        const long long off = (long long)b * 4 * f.slab;
+        const T* psi = static_cast<const T*>(f.psi) + off;
+        T* psin = static_cast<T*>(f.psi_next) + off;
+        const T d1 = f.axis == 0 ? dx1 : (f.axis == 1 ? dy1 : dz1);
+        const T d2 = f.axis == 0 ? dx2 : (f.axis == 1 ? dy2 : dz2);
+        const long long s1 = 2 * f.slab + s, s2 = 3 * f.slab + s;
+        T p1 = psi[s1] * cb;
+        p1 = p1 + cc * d1;
+        if (!f.air[s1]) p1 = T(0);
+        psin[s1] = p1;
+        T p2 = psi[s2] * cb;
+        p2 = p2 + cc * d2;
+        if (!f.air[s2]) p2 = T(0);
+        psin[s2] = p2;
+        if (f.axis == 0) {
+            hy = hy - c.by * (cck * d1 + p1);
+            hz = hz + c.bz * (cck * d2 + p2);
+        } else if (f.axis == 1) {
+            hx = hx + c.bx * (cck * d1 + p1);
+            hz = hz - c.bz * (cck * d2 + p2);
+        } else {
+            hx = hx - c.bx * (cck * d1 + p1);
+            hy = hy + c.by * (cck * d2 + p2);
+        }
+    }
+}
+
+constexpr unsigned kAll = 0xffffffffu;
+
+template <typename T, int TJ>
+__global__ void __launch_bounds__(32 * TJ) k_step_fused(const StencilArgs<T> p) {
+    const Geom& g = p.g;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int ntj = (g.ny + TJ - 1) / (TJ - 1);  // j tiles: ceil((ny + 1) / (TJ - 1))
+    const int b = blockIdx.y / ntj;
+    const int k = blockIdx.x * 31 + lane;
+    const int j = (blockIdx.y - b * ntj) * (TJ - 1) + w;
+    // loads stay inside the padded plane; clamped threads compute values
+    // that no owned cell uses
+    const int kl = min(k, g.nkp - 1), jl = min(j, g.njp - 1);
+    const bool cell = k <= g.nz && j <= g.ny;
+    const bool own = cell && lane < 31 && w < TJ - 1;
+    const int i0 = blockIdx.z * p.ichunk;
+    const int i1 = min(i0 + p.ichunk, g.nx + 1);
+    const long long vol = g.vol, si = g.si, fs = 3 * vol;
+    const T* __restrict__ E = p.e + b * fs;
+    const T* __restrict__ H = p.h + b * fs;
+    T* __restrict__ En = p.e_next + b * fs;
+    T* __restrict__ Hn = p.h_next + b * fs;
+    const unsigned mjk = cell ? mask_jk(p, j, k) : 0u;
+    __shared__ T s_ex[2][TJ][32];
+    __shared__ T s_ez[2][TJ][32];
+    const int wn = w + 1 < TJ ? w + 1 : w;
+
+    long long o = (long long)(i0 + 2) * si + (long long)jl * g.sj + kl;
+    T hz_im = __ldg(H + 2 * vol + o - si);
+    T hy_im = __ldg(H + vol + o - si);
+    FPlane<T> cur, nxt;
+    load_plane(cur, p, E, H, o, lane == 0);
+    // plane i-1 state for its H update
+    T ex_p = T(0), ey_p = T(0), ez_p = T(0), hx_p = T(0), hy_p = T(0), hz_p = T(0);
+    FCoef<T> ch_p = cur.ch;
+    for (int i = i0; i <= i1; ++i) {
+        if (i < i1) load_plane(nxt, p, E, H, o + si, lane == 0);
+        // j+1 neighbours of E_new(i-1), written by the next warp last plane
+        T ez_jp = T(0), ex_jp = T(0);
+        if (i > i0) {
+            ez_jp = s_ez[(i - 1) & 1][wn][lane];
+            ex_jp = s_ex[(i - 1) & 1][wn][lane];
+        }
+        // ---- E_new(i) ----
+        const T hy_up = __shfl_up_sync(kAll, cur.hy, 1);
+        const T hx_up = __shfl_up_sync(kAll, cur.hx, 1);
+        const T hy_km = lane == 0 ? cur.hy_before : hy_up;
+        const T hx_km = lane == 0 ? cur.hx_before : hx_up;
+        const T cxe = ((cur.hz - cur.hz_jm) - cur.hy) + hy_km;
+        const T cye = ((cur.hx - hx_km) - cur.hz) + hz_im;
+        const T cze = ((cur.hy - hy_im) - cur.hx) + cur.hx_jm;
+        T ex_n = cur.ce.ax * cur.ex + cur.ce.bx * cxe;
+        T ey_n = cur.ce.ay * cur.ey + cur.ce.by * cye;
+        T ez_n = cur.ce.az * cur.ez + cur.ce.bz * cze;
+        const bool e_store = own && i < i1;
+        const unsigned me = (cell && i <= g.nx) ? (mjk | mask_i(p, i)) : 0u;
+        if (me)
+            cpml_E(p, me, b, i, j, k, cur.hz - hz_im, cur.hy - hy_im, cur.hz - cur.hz_jm, cur.hx - cur.hx_jm,
+                   cur.hy - hy_km, cur.hx - hx_km, cur.ce, ex_n, ey_n, ez_n, e_store);
+        if (e_store) {
+            En[o] = ex_n;
+            En[vol + o] = ey_n;
+            En[2 * vol + o] = ez_n;
+        }
+        // ---- H_new(i-1) ----
+        const T ey_dn = __shfl_down_sync(kAll, ey_p, 1);
+        const T ex_dn = __shfl_down_sync(kAll, ex_p, 1);
+        if (i > i0 && own) {
+            const T ey_kp = ey_dn, ex_kp = ex_dn;
+            const T cxh = ((ez_jp - ez_p) - ey_kp) + ey_p;
+            const T cyh = ((ex_kp - ex_p) - ez_n) + ez_p;
+            const T czh = ((ey_n - ey_p) - ex_jp) + ex_p;
+            T hx_n = ch_p.ax * hx_p - ch_p.bx * cxh;
+            T hy_n = ch_p.ay * hy_p - ch_p.by * cyh;
+            T hz_n = ch_p.az * hz_p - ch_p.bz * czh;
+            const unsigned mh = mjk | mask_i(p, i - 1);
+            if (mh)
+                cpml_H(p, mh, b, i - 1, j, k, ez_n - ez_p, ey_n - ey_p, ez_jp - ez_p, ex_jp - ex_p, ey_kp - ey_p,
+                       ex_kp - ex_p, ch_p, hx_n, hy_n, hz_n);
+            const long long oh = o - si;
+            Hn[oh] = hx_n;
+            Hn[vol + oh] = hy_n;
+            Hn[2 * vol + oh] = hz_n;
+        }
+        s_ex[i & 1][w][lane] = ex_n;
+        s_ez[i & 1][w][lane] = ez_n;
+        __syncthreads();
+        ex_p = ex_n;
+        ey_p = ey_n;
+        ez_p = ez_n;
+        hx_p = cur.hx;
+        hy_p = cur.hy;
+        hz_p = cur.hz;
+        ch_p = cur.ch;
+        hz_im = cur.hz;
+        hy_im = cur.hy;
+        cur = nxt;
+        o += si;
+    }
+}
+
+// H update of listed cells, from the old H / psi buffers and the current
+// (port-written) E: the fused step's H at cells next to port edges.
+template <typename T>
+__global__ void k_fix_H(const StencilArgs<T> p, const int4* __restrict__ cells, int n) {
+    const Geom& g = p.g;
+    const long long vol = g.vol, si = g.si, sj = g.sj, fs = 3 * vol;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < (long long)n * p.B;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int b = (int)(t / n);
+        const int4 c = cells[t - (long long)b * n];
+        const int i = c.x, j = c.y, k = c.z;
+        const T* E = p.e_next + b * fs;
+        const T* Hold = p.h + b * fs;
+        T* Hn = p.h_next + b * fs;
+        const long long o = pidx(g, i, j, k);
+        const T ex = E[o], ey = E[vol + o], ez = E[2 * vol + o];
+        const T ez_jp = E[2 * vol + o + sj], ex_jp = E[o + sj];
+        const T ey_kp = E[vol + o + 1], ex_kp = E[o + 1];
+        const T ez_ip = E[2 * vol + o + si], ey_ip = E[vol + o + si];
+        FCoef<T> ch;
+        load_coef3(ch, p.aH, p.bH, o, vol);
+        const T cxh = ((ez_jp - ez) - ey_kp) + ey;
+        const T cyh = ((ex_kp - ex) - ez_ip) + ez;
+        const T czh = ((ey_ip - ey) - ex_jp) + ex;
+        T hx_n = ch.ax * Hold[o] - ch.bx * cxh;
+        T hy_n = ch.ay * Hold[vol + o] - ch.by * cyh;
+        T hz_n = ch.az * Hold[2 * vol + o] - ch.bz * czh;
+        const unsigned mh = mask_jk(p, j, k) | mask_i(p, i);
+        if (mh)
+            cpml_H(p, mh, b, i, j, k, ez_ip - ez, ey_ip - ey, ez_jp - ez, ex_jp - ex, ey_kp - ey, ex_kp - ex, ch,
+                   hx_n, hy_n, hz_n);
+        Hn[o] = hx_n;
+        Hn[vol + o] = hy_n;
+        Hn[2 * vol + o] = hz_n;
+    }
+}
+
+}  // namespace
+
+template <typename T>
+int fused_occupancy(int tj) {
+    int a = 0;
+    if (tj == 16)
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_step_fused<T, 16>, 512, 0);
+    else
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_step_fused<T, 8>, 256, 0);
+    return a < 1 ? 1 : a;
+}
+template int fused_occupancy<float>(int);
+template int fused_occupancy<double>(int);
+
+StreamPlan plan_fused(const Geom& g, int sm_count, int ctas_per_sm, int B, int tj) {
+    StreamPlan s{};
+    s.block_y = tj;
+    s.grid_x = (g.nz + 1 + 30) / 31;
+    const int ntj = (g.ny + tj - 1) / (tj - 1);
+    s.grid_y = ntj * B;
+    const long long tiles = (long long)s.grid_x * s.grid_y;
+    const int nplanes = g.nx + 1;
+    const int per_wave = sm_count * ctas_per_sm;
+    double best = -1.0;
+    int best_chunk = nplanes;
+    for (int ichunk = nplanes; ichunk >= 8; --ichunk) {
+        const int nch = (nplanes + ichunk - 1) / ichunk;
+        const double waves = (double)tiles * nch / per_wave;
+        const double eff = waves / (double)((long long)(waves + 0.999999));
+        // a chunk recomputes one E plane: prefer long chunks
+        const double score = eff - 1.0 / ichunk;
+        if (score > best) {
+            best = score;
+            best_chunk = ichunk;
+        }
+    }
+    s.ichunk = best_chunk;
+    s.grid_z = (nplanes + best_chunk - 1) / best_chunk;
+    return s;
+}
+
+template <typename T>
+void launch_fused_step(StencilArgs<T> a, const StreamPlan& sp, cudaStream_t s) {
+    a.ichunk = sp.ichunk;
+    const dim3 grid(sp.grid_x, sp.grid_y, sp.grid_z);
+    if (sp.block_y == 16)
+        k_step_fused<T, 16><<<grid, 512, 0, s>>>(a);
+    else
+        k_step_fused<T, 8><<<grid, 256, 0, s>>>(a);
+}
+template void launch_fused_step<float>(StencilArgs<float>, const StreamPlan&, cudaStream_t);
+template void launch_fused_step<double>(StencilArgs<double>, const StreamPlan&, cudaStream_t);
+
+template <typename T>
+void launch_fix_H(const StencilArgs<T>& a, const int4* cells, int n, cudaStream_t s) {
+    if (n <= 0) return;
+    const long long work = (long long)n * a.B;
+    const int threads = 128;
+    const long long want = (work + threads - 1) / threads;
+    const int blocks = (int)(want < 148 * 8 ? want : 148 * 8);
+    k_fix_H<T><<<blocks, threads, 0, s>>>(a, cells, n);
+}
+template void launch_fix_H<float>(const StencilArgs<float>&, const int4*, int, cudaStream_t);
+template void launch_fix_H<double>(const StencilArgs<double>&, const int4*, int, cudaStream_t);
+
+}  // namespace fitb

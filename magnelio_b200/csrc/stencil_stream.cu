@@ -120,7 +120,8 @@ __device__ __forceinline__ void load_hfld(HFld<T>& q, const T* H, const T* __res
 
 template <typename T>
 __device__ __forceinline__ void compute_E(const StencilArgs<T>& p, const Coef<T>& c, const EFld<T>& cur, T& hz_im,
-                                          T& hy_im, int b, int i, int j, int k, long long o, long long vol) {
+                                          T& hy_im, int b, int i, int j, int k, long long o, long long vol,
+                                          unsigned mask) {
     T* __restrict__ E = p.e + (long long)b * 3 * vol;
     const T cx = ((cur.hz - cur.hz_jm) - cur.hy) + cur.hy_km;
     const T cy = ((cur.hx - cur.hx_km) - cur.hz) + hz_im;
@@ -128,11 +129,12 @@ __device__ __forceinline__ void compute_E(const StencilArgs<T>& p, const Coef<T>
     T ex = c.ax * cur.ex + c.bx * cx;
     T ey = c.ay * cur.ey + c.by * cy;
     T ez = c.az * cur.ez + c.bz * cz;
-    for (int fi = 0; fi < p.nfaces; ++fi) {
+    while (mask) {
+        const int fi = __ffs(mask) - 1;
+        mask &= mask - 1;
         const FaceDev& f = p.f[fi];
         const int coord = (f.axis == 0) ? i : ((f.axis == 1) ? j : k);
         const int l = coord - f.lo;
-        if ((unsigned)l >= (unsigned)f.n) continue;
         const long long s = slab_index_s(f, l, i, j, k);
         const T* bcc = static_cast<const T*>(f.bcc);
         const T cb = bcc[l], cc = bcc[f.n + l], cck = bcc[2 * f.n + l];
@@ -176,7 +178,8 @@ __device__ __forceinline__ void compute_E(const StencilArgs<T>& p, const Coef<T>
 
 template <typename T>
 __device__ __forceinline__ void compute_H(const StencilArgs<T>& p, const Coef<T>& c, const HFld<T>& cur, T& ez_ip,
-                                          T& ey_ip, int b, int i, int j, int k, long long o, long long vol) {
+                                          T& ey_ip, int b, int i, int j, int k, long long o, long long vol,
+                                          unsigned mask) {
     T* __restrict__ H = p.h + (long long)b * 3 * vol;
     const T cx = ((cur.ez_jp - cur.ez) - cur.ey_kp) + cur.ey;
     const T cy = ((cur.ex_kp - cur.ex) - ez_ip) + cur.ez;
@@ -184,11 +187,12 @@ __device__ __forceinline__ void compute_H(const StencilArgs<T>& p, const Coef<T>
     T hx = c.ax * cur.hx - c.bx * cx;
     T hy = c.ay * cur.hy - c.by * cy;
     T hz = c.az * cur.hz - c.bz * cz;
-    for (int fi = 0; fi < p.nfaces; ++fi) {
+    while (mask) {
+        const int fi = __ffs(mask) - 1;
+        mask &= mask - 1;
         const FaceDev& f = p.f[fi];
         const int coord = (f.axis == 0) ? i : ((f.axis == 1) ? j : k);
         const int l = coord - f.lo;
-        if ((unsigned)l >= (unsigned)f.n) continue;
         const long long s = slab_index_s(f, l, i, j, k);
         const T* bcc = static_cast<const T*>(f.bcc);
         const T cb = bcc[l], cc = bcc[f.n + l], cck = bcc[2 * f.n + l];
@@ -231,6 +235,29 @@ __device__ __forceinline__ void compute_H(const StencilArgs<T>& p, const Coef<T>
     ey_ip = cur.ey;
 }
 
+// Faces (bit q = p.f[q]) that contain cell column (j, k): the y and z faces,
+// fixed for a thread; the x faces that contain plane i.
+template <typename T>
+__device__ __forceinline__ unsigned faces_jk(const StencilArgs<T>& p, int j, int k) {
+    unsigned m = 0;
+    for (int q = 0; q < p.nfaces; ++q) {
+        const FaceDev& f = p.f[q];
+        const int c = f.axis == 1 ? j : k;
+        if (f.axis != 0 && (unsigned)(c - f.lo) < (unsigned)f.n) m |= 1u << q;
+    }
+    return m;
+}
+
+template <typename T>
+__device__ __forceinline__ unsigned faces_i(const StencilArgs<T>& p, int i) {
+    unsigned m = 0;
+    for (int q = 0; q < p.nfaces; ++q) {
+        const FaceDev& f = p.f[q];
+        if (f.axis == 0 && (unsigned)(i - f.lo) < (unsigned)f.n) m |= 1u << q;
+    }
+    return m;
+}
+
 // Field sets map to the warps of one CTA: warp row ty handles field set
 // b = ty % B of grid row j = blockIdx.y * rows + ty / B.  Each thread runs the
 // single-field-set pipeline; the B warps that share a cell load the same
@@ -252,6 +279,7 @@ __global__ void __launch_bounds__(512) k_update_E_stream(const StencilArgs<T> p)
     const T* __restrict__ bE = p.bE;
     const T* E = p.e + b * fs;
     const T* __restrict__ H = p.h + b * fs;
+    const unsigned mjk = faces_jk(p, j, k);
     long long o = pidx(g, i0, j, k);
     T hz_im = __ldg(H + 2 * vol + o - si);
     T hy_im = __ldg(H + vol + o - si);
@@ -264,7 +292,7 @@ __global__ void __launch_bounds__(512) k_update_E_stream(const StencilArgs<T> p)
             load_coef_k<T, CK>(cn, p, 0, aE, bE, o + si, vol);
             load_efld(fn, E, H, o + si, vol, sj);
         }
-        compute_E(p, cc, fc, hz_im, hy_im, b, i, j, k, o, vol);
+        compute_E(p, cc, fc, hz_im, hy_im, b, i, j, k, o, vol, mjk | faces_i(p, i));
         cc = cn;
         fc = fn;
         o += si;
@@ -287,6 +315,7 @@ __global__ void __launch_bounds__(512) k_update_H_stream(const StencilArgs<T> p)
     const T* H = p.h + b * fs;
     const T* __restrict__ E = p.e + b * fs;
     // march down: the x-neighbours (E at i+1) of the first plane
+    const unsigned mjk = faces_jk(p, j, k);
     long long o = pidx(g, i1 - 1, j, k);
     T ez_ip = __ldg(E + 2 * vol + o + si);
     T ey_ip = __ldg(E + vol + o + si);
@@ -299,7 +328,7 @@ __global__ void __launch_bounds__(512) k_update_H_stream(const StencilArgs<T> p)
             load_coef_k<T, CK>(cn, p, 1, aH, bH, o - si, vol);
             load_hfld(fn, H, E, o - si, vol, sj);
         }
-        compute_H(p, cc, fc, ez_ip, ey_ip, b, i, j, k, o, vol);
+        compute_H(p, cc, fc, ez_ip, ey_ip, b, i, j, k, o, vol, mjk | faces_i(p, i));
         cc = cn;
         fc = fn;
         o -= si;
