@@ -178,7 +178,7 @@ struct Handle {
     BulkPlan plan{};
     int stencil_mode = 0;  // kModeSimple / kModeStream / kModeBulk / kModeVec
     int vec_variant = 0;   // vector width x register cap of the vec kernels
-    int fused_tj = 8;      // warps (rows along j) per CTA of the fused step
+    int fused_variant = 0; // kernel form of the fused step (stencil_fused.cu)
     StreamPlan splan{};
     DevBuf status;
     // Compact coefficient storage of the stream kernels (kCoefF16 /
@@ -501,9 +501,9 @@ void plan_stencil(Handle& H) {
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, H.desc.device);
     if (H.stencil_mode == kModeFused) {
-        const int tj = H.fused_tj;
-        const int occ = H.prec == 4 ? fused_occupancy<float>(tj) : fused_occupancy<double>(tj);
-        H.splan = plan_fused(H.g, sms, occ, H.B, tj);
+        const int v = H.fused_variant;
+        const int occ = H.prec == 4 ? fused_occupancy<float>(v) : fused_occupancy<double>(v);
+        H.splan = plan_fused(H.g, sms, occ, H.B, fused_tj_of(v));
     } else if (H.stencil_mode == kModeStream) {
         const int occ = H.prec == 4 ? stream_occupancy<float>(H.B, H.coef_kind)
                                     : stream_occupancy<double>(H.B, H.coef_kind);
@@ -539,9 +539,9 @@ void launch_half(Handle& H, int which) {
 
 void launch_fused_any(Handle& H) {
     if (H.prec == 4)
-        launch_fused_step<float>(stencil_args<float>(H), H.splan, H.stream);
+        launch_fused_step<float>(stencil_args<float>(H), H.splan, H.fused_variant, H.stream);
     else
-        launch_fused_step<double>(stencil_args<double>(H), H.splan, H.stream);
+        launch_fused_step<double>(stencil_args<double>(H), H.splan, H.fused_variant, H.stream);
 }
 
 void launch_stencil_half(Handle& H, int which) {
@@ -560,7 +560,7 @@ int enqueue_step_fused(Handle& H) {
     int n = 0;
     PortsArgs pa = ports_args(H);
     StencilArgs<T> sa = stencil_args<T>(H);
-    launch_fused_step<T>(sa, H.splan, H.stream);
+    launch_fused_step<T>(sa, H.splan, H.fused_variant, H.stream);
     ++n;
     T* e_new = H.En().as<T>();
     T* h_new = H.Hn().as<T>();
@@ -1057,7 +1057,7 @@ int fitb_create(const fitb_desc* desc, fitb_handle** out) {
     {
         // FITB_STENCIL selects the stencil kernels: "stream" (default),
         // "fused" (E and H in one pass over ping-pong buffers;
-        // FITB_FUSED_TJ = 8 or 16 rows per CTA), "vec" (vectorised planes;
+        // FITB_FUSED_VARIANT picks the kernel form), "vec" (vectorised planes;
         // FITB_VEC_VARIANT picks the vector width and register cap), "bulk"
         // (cp.async.bulk pipeline, one field set) or "simple".
         const char* mode = getenv("FITB_STENCIL");
@@ -1073,8 +1073,11 @@ int fitb_create(const fitb_desc* desc, fitb_handle** out) {
                 H.stencil_mode = fitb::kModeBulk;
             }
         } else if (m == "fused") {
-            const char* t = getenv("FITB_FUSED_TJ");
-            H.fused_tj = (t && atoi(t) == 16 && H.prec == 4) ? 16 : 8;
+            const char* t = getenv("FITB_FUSED_VARIANT");
+            H.fused_variant = t ? std::max(0, std::min(6, atoi(t))) : 2;
+            if (H.fused_variant == 1 && H.prec == 8) H.fused_variant = 0;
+            ck(H.prec == 4 ? fitb::prepare_fused<float>(H.fused_variant) : fitb::prepare_fused<double>(H.fused_variant),
+               "fused step smem attribute");
             H.e2.alloc(blk * H.B);
             H.h2.alloc(blk * H.B);
             H.stencil_mode = fitb::kModeFused;

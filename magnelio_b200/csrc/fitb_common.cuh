@@ -119,12 +119,17 @@ template <typename T>
 void launch_vec_half(StencilArgs<T> a, const StreamPlan& sp, int variant, int which, cudaStream_t s);
 
 // Fused step (E then H in one i-march, stencil_fused.cu): reads e, h, psi
-// and writes e_next, h_next, psi_next.  block_y = TJ (8 or 16) warps.
+// and writes e_next, h_next, psi_next.  variant: register prefetch with 8 or
+// 16 rows per CTA (0, 1) or the cp.async shared-memory pipeline with 3 or 4
+// stages (2, 3); block_y = rows per CTA.
+int fused_tj_of(int variant);
 template <typename T>
-int fused_occupancy(int tj);
+cudaError_t prepare_fused(int variant);
+template <typename T>
+int fused_occupancy(int variant);
 StreamPlan plan_fused(const Geom& g, int sm_count, int ctas_per_sm, int B, int tj);
 template <typename T>
-void launch_fused_step(StencilArgs<T> a, const StreamPlan& sp, cudaStream_t s);
+void launch_fused_step(StencilArgs<T> a, const StreamPlan& sp, int variant, cudaStream_t s);
 // H update of listed cells (x, y, z = i, j, k) from h / psi and e_next.
 template <typename T>
 void launch_fix_H(const StencilArgs<T>& a, const int4* cells, int n, cudaStream_t s);

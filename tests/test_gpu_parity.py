@@ -113,12 +113,12 @@ def test_stencil_variants_agree(name, monkeypatch):
     p, d, n = load_golden(name)
     outs = []
     modes = [("stream", None), ("bulk", None), ("simple", None)] + [("vec", str(v)) for v in range(4)]
-    modes += [("fused", "8"), ("fused", "16")]
+    modes += [("fused", str(v)) for v in range(7)]
     for mode, variant in modes:
         monkeypatch.setenv("FITB_STENCIL", mode)
         if variant is not None:
             monkeypatch.setenv("FITB_VEC_VARIANT", variant)
-            monkeypatch.setenv("FITB_FUSED_TJ", variant)
+            monkeypatch.setenv("FITB_FUSED_VARIANT", variant)
         with p.build_engine("single") as eng:
             eng.step(n)
             outs.append(eng.read_fields())
@@ -328,10 +328,12 @@ def test_compact_coefficients_need_the_stream_kernels(monkeypatch):
 
 @pytest.mark.parametrize("name", ["cpml_box", "mixed_box", "lumped_dft", "wg_dtbc", "wg_mur"])
 @pytest.mark.parametrize("precision,tol", [("double", F64_TOL), ("single", F32_TOL)])
-def test_fused_step_matches_reference(name, precision, tol, monkeypatch):
+@pytest.mark.parametrize("variant", ["0", "2"])
+def test_fused_step_matches_reference(name, precision, tol, variant, monkeypatch):
     """The fused E+H pass (ping-pong buffers, H fix-up next to port edges)
     reproduces the reference march: fields, energy, port V/I, DFT bins."""
     monkeypatch.setenv("FITB_STENCIL", "fused")
+    monkeypatch.setenv("FITB_FUSED_VARIANT", variant)
     pe, ph = _peaks(name)
     p, d, n, eng = _run(name, precision)
     with eng:
