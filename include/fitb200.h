@@ -104,6 +104,30 @@ typedef struct fitb_dft_desc {
     const double* dz;                /* [nz]                                 */
 } fitb_dft_desc;
 
+/* TF/SF plane-wave source (sources/plane_wave.py:65-733): ordered face
+ * patches as flat indices into the reference's e_flat / h_flat, each entry
+ * with its coefficient (beta * metric * incident amplitude, already rounded
+ * to the field dtype) and retardation delay [s].  After the E update of
+ * step n every E entry gets coef * f(n dt + dt - dt/2 - delay) added, after
+ * the H update every H entry coef * f(n dt + dt + dt/2 - dt/2 - delay);
+ * entries that appear more than once take their contributions in the order
+ * given.  f(t) = amplitude * exp(-((t - t0)^2) / den)   (FITB_WAVE_GAUSSIAN)
+ *        f(t) = amplitude * sin(omega t)                 (FITB_WAVE_SINE). */
+#define FITB_WAVE_GAUSSIAN 0
+#define FITB_WAVE_SINE 1
+typedef struct fitb_plane_wave_desc {
+    int32_t waveform;
+    double amplitude, t0, den, omega;
+    int64_t n_e;
+    const int64_t* e_idx;
+    const double* e_coef;
+    const double* e_delay;
+    int64_t n_h;
+    const int64_t* h_idx;
+    const double* h_coef;
+    const double* h_delay;
+} fitb_plane_wave_desc;
+
 /* ---- lifetime ------------------------------------------------------- */
 int fitb_abi_version(void);
 /* Replaces FITTimeDomainSolver.setup() allocation (fit_td.py:302-324). */
@@ -193,6 +217,13 @@ int fitb_set_dtbc_kernel(fitb_handle* h, int32_t port, int32_t mode,
  * (operator.py:1140-1182 set_excitation / clear_excitation). */
 int fitb_set_modal_source(fitb_handle* h, int32_t port, int32_t b, int32_t mode,
                           int64_t n_samples, const double* w);
+
+/* ---- plane waves ---------------------------------------------------- */
+/* Replaces PlaneWaveSource.attach / inject_E / inject_H (plane_wave.py:229,
+ * :720-733; called from fit_td.py:964-967, :990-993). */
+int fitb_add_plane_wave(fitb_handle* h, const fitb_plane_wave_desc* d, int32_t* out_id);
+/* Amplitude factor of plane wave `id` for field set b (default 1). */
+int fitb_set_plane_wave_scale(fitb_handle* h, int32_t id, int32_t b, double scale);
 
 /* ---- monitors ------------------------------------------------------- */
 int fitb_add_dft_monitor(fitb_handle* h, const fitb_dft_desc* d, int32_t* out_id);

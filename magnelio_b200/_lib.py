@@ -94,8 +94,28 @@ class FitbDftDesc(C.Structure):
     ]
 
 
+class FitbPlaneWaveDesc(C.Structure):
+    _fields_ = [
+        ("waveform", i32),
+        ("amplitude", C.c_double),
+        ("t0", C.c_double),
+        ("den", C.c_double),
+        ("omega", C.c_double),
+        ("n_e", C.c_int64),
+        ("e_idx", P_i64),
+        ("e_coef", P_f64),
+        ("e_delay", P_f64),
+        ("n_h", C.c_int64),
+        ("h_idx", P_i64),
+        ("h_coef", P_f64),
+        ("h_delay", P_f64),
+    ]
+
+
 SIGNATURES = {
     "fitb_abi_version": ([], C.c_int),
+    "fitb_add_plane_wave": ([vp, C.POINTER(FitbPlaneWaveDesc), P_i32], C.c_int),
+    "fitb_set_plane_wave_scale": ([vp, i32, i32, C.c_double], C.c_int),
     "fitb_create": ([C.POINTER(FitbDesc), C.POINTER(vp)], C.c_int),
     "fitb_destroy": ([vp], C.c_int),
     "fitb_last_error": ([C.c_char_p, sz], C.c_int),

@@ -17,7 +17,7 @@ from __future__ import annotations
 import numpy as np
 
 from magnelio_b200 import host
-from magnelio_b200.problem import CpmlFace, DftMonitor, FitProblem, LumpedPort, ModalPort
+from magnelio_b200.problem import CpmlFace, DftMonitor, FitProblem, LumpedPort, ModalPort, PlaneWave
 
 _FACE_EDGES = {
     # tangential E components zeroed by PECBoundary.apply (pec.py:51-78)
@@ -87,8 +87,6 @@ def problem_from_solver(solver, n_steps: int) -> FitProblem:
         raise RuntimeError("problem_from_solver needs a solver after setup()")
     if s._dispersion is not None or s._dispersion_mu is not None or s._sibc is not None:
         raise NotImplementedError("dispersive materials / SIBC walls are not on the device engine yet")
-    if s.sources:
-        raise NotImplementedError("TF/SF plane-wave sources are not on the device engine yet")
     grid = s.mesh.grid
     nx, ny, nz = s.mesh.Nx, s.mesh.Ny, s.mesh.Nz
     dt = float(s.dt)
@@ -160,9 +158,60 @@ def problem_from_solver(solver, n_steps: int) -> FitProblem:
             freqs=np.asarray(mon.freqs, float),
             stride=int(stride),
         ))
+    for src in s.sources:
+        prob.plane_waves.append(_plane_wave_from_src(src, s))
     prob.e0 = [np.array(_np(s._fields.e_flat), dtype=np.float64)]
     prob.h0 = [np.array(_np(s._fields.h_flat), dtype=np.float64)]
     return prob
+
+
+def _plane_wave_from_src(src, s) -> PlaneWave:
+    """Flatten the attached TF/SF face patches of a ``PlaneWaveSource``
+    (``sources/plane_wave.py:366-707``) into ordered (flat index,
+    coefficient, delay) lists, one entry per corrected edge / face."""
+    import math
+
+    from magnelio.sources.plane_wave import PlaneWaveSource
+
+    if not isinstance(src, PlaneWaveSource) or not src._attached:
+        raise NotImplementedError(f"source {type(src).__name__} is not on the device engine")
+    nx, ny, nz = s.mesh.Nx, s.mesh.Ny, s.mesh.Nz
+    shapes = {"Ex": (nx, ny + 1, nz + 1), "Ey": (nx + 1, ny, nz + 1), "Ez": (nx + 1, ny + 1, nz),
+              "Hx": (nx + 1, ny, nz), "Hy": (nx, ny + 1, nz), "Hz": (nx, ny, nz + 1)}
+    base = {}
+    for group in (("Ex", "Ey", "Ez"), ("Hx", "Hy", "Hz")):
+        o = 0
+        for c in group:
+            base[c] = o
+            o += int(np.prod(shapes[c]))
+
+    def flatten(patches):
+        idx, coef, delay, splits = [], [], [], []
+        for comp, index, d, c in patches:
+            flat = np.arange(int(np.prod(shapes[comp]))).reshape(shapes[comp])[index]
+            idx.append(np.asarray(flat, np.int64).ravel() + base[comp])
+            coef.append(np.broadcast_to(np.asarray(_np(c), np.float64), flat.shape).ravel())
+            delay.append(np.broadcast_to(np.asarray(_np(d), np.float64), flat.shape).ravel())
+            splits.append(flat.size)
+        cat = (lambda a, t: np.concatenate(a).astype(t) if a else np.zeros(0, t))  # noqa: E731
+        return cat(idx, np.int64), cat(coef, np.float64), cat(delay, np.float64), np.asarray(splits, np.int64)
+
+    e_idx, e_coef, e_delay, e_splits = flatten(src._patches_E)
+    h_idx, h_coef, h_delay, h_splits = flatten(src._patches_H)
+    # excitation() constants (plane_wave.py:188-204)
+    t0 = den = omega = 0.0
+    if src.waveform == "gaussian":
+        f_max = src.f_max or 1e9
+        t0 = 4.0 / f_max
+        sigma = 2.0 / (math.pi * f_max)
+        den = 2 * sigma**2
+    elif src.waveform == "sine":
+        omega = 2 * math.pi * (src.f_center or 1e9)
+    else:
+        raise NotImplementedError(f"plane-wave waveform {src.waveform!r}")
+    return PlaneWave(waveform=src.waveform, amplitude=float(src.amplitude), t0=t0, den=den, omega=omega,
+                     e_idx=e_idx, e_coef=e_coef, e_delay=e_delay, e_splits=e_splits,
+                     h_idx=h_idx, h_coef=h_coef, h_delay=h_delay, h_splits=h_splits, scale=[1.0])
 
 
 def refresh_sources(solver, prob, engine, n_steps: int) -> None:

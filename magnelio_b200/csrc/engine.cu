@@ -104,6 +104,13 @@ struct LumpedHost {
     std::vector<double> src_host;  // [B][n_src]
 };
 
+struct PlaneWaveHost {
+    PlaneWaveDev dev{};
+    DevBuf e_off, e_start, e_coef, e_delay, h_off, h_start, h_coef, h_delay, scale;
+    std::vector<double> scale_host;
+    std::vector<long long> e_off_host;  // E offsets it writes (fused-step fix-up)
+};
+
 struct ModalHost {
     ModalDev dev{};
     std::vector<long long> port_e_host;  // E offsets the port writes
@@ -153,6 +160,7 @@ struct Handle {
     std::vector<std::unique_ptr<LumpedHost>> lumped;
     std::vector<std::unique_ptr<ModalHost>> modal;
     std::vector<std::unique_ptr<DftHost>> dft;
+    std::vector<std::unique_ptr<PlaneWaveHost>> pws;
     DevBuf d_lumped, d_modal, d_dft;
     int dft_stage_blocks = 0, dft_flush_blocks = 0;
     size_t dft_flush_smem = 0;
@@ -358,6 +366,8 @@ void build_fix_cells(Handle& H) {
         for (long long o : lp->off_host) add_edge(o);
     for (auto& mp : H.modal)
         for (long long o : mp->port_e_host) add_edge(o);
+    for (auto& pw : H.pws)
+        for (long long o : pw->e_off_host) add_edge(o);
     std::sort(keys.begin(), keys.end());
     keys.erase(std::unique(keys.begin(), keys.end()), keys.end());
     std::vector<int4> cells;
@@ -564,6 +574,10 @@ int enqueue_step_fused(Handle& H) {
     ++n;
     T* e_new = H.En().as<T>();
     T* h_new = H.Hn().as<T>();
+    for (auto& pw : H.pws) {
+        launch_plane_wave<T>(e_new, H.e_block(), H.B, pw->dev, 0, H.step.as<long long>(), H.stream);
+        ++n;
+    }
     if (!H.modal.empty()) {
         launch_modal<T>(e_new, H.Hc().as<T>(), pa, H.d_modal.as<ModalDev>(), (int)H.modal.size(), H.stream);
         ++n;
@@ -574,6 +588,10 @@ int enqueue_step_fused(Handle& H) {
     }
     if (H.n_fix > 0) {
         launch_fix_H<T>(sa, H.fix_cells.as<int4>(), H.n_fix, H.stream);
+        ++n;
+    }
+    for (auto& pw : H.pws) {
+        launch_plane_wave<T>(h_new, H.e_block(), H.B, pw->dev, 1, H.step.as<long long>(), H.stream);
         ++n;
     }
     if (!H.dft.empty()) {
@@ -597,6 +615,10 @@ int enqueue_step(Handle& H) {
     PortsArgs pa = ports_args(H);
     launch_half<T>(H, 0);
     ++n;
+    for (auto& pw : H.pws) {
+        launch_plane_wave<T>(H.Ec().as<T>(), H.e_block(), H.B, pw->dev, 0, H.step.as<long long>(), H.stream);
+        ++n;
+    }
     if (!H.modal.empty()) {
         launch_modal<T>(H.Ec().as<T>(), H.Hc().as<T>(), pa, H.d_modal.as<ModalDev>(), (int)H.modal.size(), H.stream);
         ++n;
@@ -607,6 +629,10 @@ int enqueue_step(Handle& H) {
     }
     launch_half<T>(H, 1);
     ++n;
+    for (auto& pw : H.pws) {
+        launch_plane_wave<T>(H.Hc().as<T>(), H.e_block(), H.B, pw->dev, 1, H.step.as<long long>(), H.stream);
+        ++n;
+    }
     if (!H.dft.empty()) {
         // stage + flush of all monitors; the flush launch advances the step
         launch_dft_stage_all<T>(H.Ec().as<T>(), H.Hc().as<T>(), H.e_block(), H.e_block(), H.g, H.B,
@@ -1490,6 +1516,91 @@ int fitb_set_modal_source(fitb_handle* h, int32_t port, int32_t b, int32_t mode,
     mp.dev.buf_len = mp.buflen.as<int>();
     H.port_tables_dirty = true;
     fitb::invalidate_graphs(H);
+    FITB_CATCH
+}
+
+int fitb_add_plane_wave(fitb_handle* h, const fitb_plane_wave_desc* d, int32_t* out_id) {
+    FITB_TRY
+    Handle& H = H_of(h);
+    if (!d) fail(FITB_ERR_ARG, "null plane-wave descriptor");
+    if (d->waveform != FITB_WAVE_GAUSSIAN && d->waveform != FITB_WAVE_SINE)
+        fail(FITB_ERR_ARG, "plane-wave waveform %d", d->waveform);
+    if (d->waveform == FITB_WAVE_GAUSSIAN && !(d->den > 0.0)) fail(FITB_ERR_ARG, "gaussian plane wave needs den > 0");
+    if (d->n_e < 0 || d->n_h < 0 || (d->n_e > 0 && (!d->e_idx || !d->e_coef || !d->e_delay)) ||
+        (d->n_h > 0 && (!d->h_idx || !d->h_coef || !d->h_delay)))
+        fail(FITB_ERR_ARG, "plane-wave patch arrays");
+    if (H.steps_done != 0) fail(FITB_ERR_STATE, "sources must be added before the first step");
+    auto pw = std::make_unique<fitb::PlaneWaveHost>();
+    // group the contributions of each entry, keeping their given order
+    auto side = [&](bool is_h, int64_t n, const int64_t* idx, const double* coef, const double* delay,
+                    fitb::DevBuf& off_b, fitb::DevBuf& start_b, fitb::DevBuf& coef_b, fitb::DevBuf& delay_b,
+                    fitb::PlaneWaveSide& sd, std::vector<long long>* offs_out) {
+        std::vector<long long> off((size_t)n);
+        for (int64_t q = 0; q < n; ++q) off[(size_t)q] = H.flat_to_off(is_h, idx[q]);
+        std::vector<int64_t> order((size_t)n);
+        for (int64_t q = 0; q < n; ++q) order[(size_t)q] = q;
+        std::stable_sort(order.begin(), order.end(), [&](int64_t a, int64_t b) { return off[(size_t)a] < off[(size_t)b]; });
+        std::vector<long long> uoff;
+        std::vector<int> start;
+        std::vector<double> c, dl;
+        for (size_t r = 0; r < order.size(); ++r) {
+            const int64_t q = order[r];
+            if (r == 0 || off[(size_t)q] != uoff.back()) {
+                uoff.push_back(off[(size_t)q]);
+                start.push_back((int)c.size());
+            }
+            c.push_back(coef[q]);
+            dl.push_back(delay[q]);
+        }
+        start.push_back((int)c.size());
+        if (uoff.empty()) uoff.push_back(0);
+        if (c.empty()) {
+            c.push_back(0.0);
+            dl.push_back(0.0);
+        }
+        fitb::upload(off_b, uoff);
+        fitb::upload(start_b, start);
+        fitb::upload(coef_b, c);
+        fitb::upload(delay_b, dl);
+        sd.n_unique = (long long)start.size() - 1;
+        sd.off = off_b.as<long long>();
+        sd.start = start_b.as<int>();
+        sd.coef = coef_b.as<double>();
+        sd.delay = delay_b.as<double>();
+        if (offs_out) *offs_out = std::vector<long long>(uoff.begin(), uoff.begin() + sd.n_unique);
+    };
+    fitb::PlaneWaveDev& dv = pw->dev;
+    side(false, d->n_e, d->e_idx, d->e_coef, d->e_delay, pw->e_off, pw->e_start, pw->e_coef, pw->e_delay, dv.e,
+         &pw->e_off_host);
+    side(true, d->n_h, d->h_idx, d->h_coef, d->h_delay, pw->h_off, pw->h_start, pw->h_coef, pw->h_delay, dv.h,
+         nullptr);
+    dv.waveform = d->waveform;
+    dv.amplitude = d->amplitude;
+    dv.t0 = d->t0;
+    dv.den = d->den;
+    dv.omega = d->omega;
+    dv.dt = H.dt;
+    pw->scale_host.assign((size_t)H.B, 1.0);
+    fitb::upload(pw->scale, pw->scale_host);
+    dv.scale = pw->scale.as<double>();
+    H.pws.push_back(std::move(pw));
+    H.port_tables_dirty = true;
+    fitb::invalidate_graphs(H);
+    if (out_id) *out_id = (int32_t)H.pws.size() - 1;
+    FITB_CATCH
+}
+
+int fitb_set_plane_wave_scale(fitb_handle* h, int32_t id, int32_t b, double scale) {
+    FITB_TRY
+    Handle& H = H_of(h);
+    if (id < 0 || id >= (int32_t)H.pws.size()) fail(FITB_ERR_ARG, "plane wave %d out of range", id);
+    if (b < 0 || b >= H.B) fail(FITB_ERR_ARG, "field set %d out of range", b);
+    auto& pw = *H.pws[(size_t)id];
+    pw.scale_host[(size_t)b] = scale;
+    ck(cudaMemcpyAsync(pw.scale.as<double>() + b, &pw.scale_host[(size_t)b], sizeof(double), cudaMemcpyHostToDevice,
+                       H.stream),
+       "plane-wave scale");
+    ck(cudaStreamSynchronize(H.stream), "plane-wave scale sync");
     FITB_CATCH
 }
 

@@ -246,6 +246,30 @@ void launch_modal(T* e, const T* h, const PortsArgs& pa, const ModalDev* d, int 
                   cudaStream_t s);
 
 // ---------------------------------------------------------------------------
+// TF/SF plane waves: per side (E, H) the unique corrected entries (offsets
+// into a field set's block) with their contributions in patch order.
+// ---------------------------------------------------------------------------
+struct PlaneWaveSide {
+    long long n_unique;
+    const long long* off;   // [n_unique]
+    const int* start;       // [n_unique + 1] into coef / delay
+    const double* coef;     // field-dtype values held as double
+    const double* delay;    // seconds
+};
+
+struct PlaneWaveDev {
+    int waveform;           // 0 gaussian, 1 sine
+    double amplitude, t0, den, omega, dt;
+    const double* scale;    // [B]
+    PlaneWaveSide e, h;
+};
+
+// side 0: after the E update (field = E), 1: after the H update (field = H).
+template <typename T>
+void launch_plane_wave(T* field, long long blk, int B, const PlaneWaveDev& d, int side, const long long* step,
+                       cudaStream_t s);
+
+// ---------------------------------------------------------------------------
 // Running-DFT monitors, staged in blocks of K recorded samples.
 // ---------------------------------------------------------------------------
 struct DftDev {

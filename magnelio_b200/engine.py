@@ -318,6 +318,30 @@ class FitEngine:
         self._monitors.append((int(out.value), (i1 - i0, j1 - j0, k1 - k0), fr.size))
         return int(out.value)
 
+    def add_plane_wave(self, pw) -> int:
+        """Upload a TF/SF plane wave (:class:`magnelio_b200.problem.PlaneWave`):
+        its ordered E and H face patches and waveform constants."""
+        arr = {k: np.ascontiguousarray(getattr(pw, k), dtype=t) for k, t in (
+            ("e_idx", np.int64), ("e_coef", np.float64), ("e_delay", np.float64),
+            ("h_idx", np.int64), ("h_coef", np.float64), ("h_delay", np.float64))}
+        if not (arr["e_idx"].size == arr["e_coef"].size == arr["e_delay"].size and
+                arr["h_idx"].size == arr["h_coef"].size == arr["h_delay"].size):
+            raise ValueError("plane-wave patch arrays differ in length")
+        kinds = {"gaussian": 0, "sine": 1}
+        if pw.waveform not in kinds:
+            raise ValueError(f"plane-wave waveform {pw.waveform!r}")
+        d = _lib.FitbPlaneWaveDesc(
+            kinds[pw.waveform], float(pw.amplitude), float(pw.t0), float(pw.den), float(pw.omega),
+            int(arr["e_idx"].size), i64p(arr["e_idx"]), f64p(arr["e_coef"]), f64p(arr["e_delay"]),
+            int(arr["h_idx"].size), i64p(arr["h_idx"]), f64p(arr["h_coef"]), f64p(arr["h_delay"]),
+        )
+        out = C.c_int32()
+        check(self._lib.fitb_add_plane_wave(self._h, C.byref(d), C.byref(out)))
+        return int(out.value)
+
+    def set_plane_wave_scale(self, wave: int, b: int, scale: float) -> None:
+        check(self._lib.fitb_set_plane_wave_scale(self._h, int(wave), int(b), float(scale)))
+
     def read_dft(self, mon: int, comp: str, b: int = 0) -> np.ndarray:
         _, shape, nf = self._monitors[mon]
         n = int(nf * np.prod(shape))

@@ -73,6 +73,34 @@ class ModalPort:
 
 
 @dataclass
+class PlaneWave:
+    """TF/SF plane-wave source as ordered face patches
+    (``sources/plane_wave.py:387-733``): after the E update every entry
+    ``e[e_idx] += e_coef * f(t_E - dt/2 - e_delay)``, after the H update
+    ``h[h_idx] += h_coef * f(t_H - dt/2 - h_delay)``, patch by patch in the
+    reference's order (``e_splits`` / ``h_splits`` are the patch lengths).
+    ``f`` is ``amplitude * exp(-((t - t0)^2) / den)`` ("gaussian") or
+    ``amplitude * sin(omega t)`` ("sine"); coefficients are already in the
+    field dtype of the run they were built for."""
+
+    waveform: str
+    amplitude: float
+    t0: float
+    den: float
+    omega: float
+    e_idx: np.ndarray
+    e_coef: np.ndarray
+    e_delay: np.ndarray
+    e_splits: np.ndarray
+    h_idx: np.ndarray
+    h_coef: np.ndarray
+    h_delay: np.ndarray
+    h_splits: np.ndarray
+    # per field set amplitude factor (a field set beyond the list gets 1)
+    scale: list = field(default_factory=list)
+
+
+@dataclass
 class DftMonitor:
     box: tuple  # ((i0, i1), (j0, j1), (k0, k1)) cell indices, stop-exclusive
     components: tuple
@@ -99,6 +127,7 @@ class FitProblem:
     lumped: list = field(default_factory=list)
     modal: list = field(default_factory=list)
     monitors: list = field(default_factory=list)
+    plane_waves: list = field(default_factory=list)
     batch: int = 1
     e0: list = field(default_factory=list)  # per field set initial e (or empty)
     h0: list = field(default_factory=list)
@@ -149,6 +178,11 @@ class FitProblem:
                         eng.set_lumped_source(lid, b, v)
             for mon in self.monitors:
                 eng.add_dft_monitor(mon.box, mon.components, mon.freqs, self.dx, self.dy, self.dz, stride=mon.stride)
+            for pw in self.plane_waves:
+                wid = eng.add_plane_wave(pw)
+                for b, sc in enumerate(pw.scale):
+                    if sc != 1.0:
+                        eng.set_plane_wave_scale(wid, b, sc)
             for b in range(self.batch):
                 e = self.e0[b] if b < len(self.e0) else None
                 h = self.h0[b] if b < len(self.h0) else None
@@ -213,6 +247,12 @@ class FitProblem:
             put(f"mon{q}.comps", np.array([["Ex", "Ey", "Ez", "Hx", "Hy", "Hz"].index(c) for c in mon.components]))
             put(f"mon{q}.freqs", mon.freqs)
             put(f"mon{q}.stride", mon.stride)
+        put("n_pw", len(self.plane_waves))
+        for q, pw in enumerate(self.plane_waves):
+            put(f"pw{q}.waveform", ["gaussian", "sine"].index(pw.waveform))
+            for k in ("amplitude", "t0", "den", "omega", "e_idx", "e_coef", "e_delay", "e_splits", "h_idx", "h_coef",
+                      "h_delay", "h_splits", "scale"):
+                put(f"pw{q}.{k}", getattr(pw, k))
         for b, e in enumerate(self.e0):
             if e is not None:
                 put(f"e0.{b}", e)
@@ -270,6 +310,13 @@ class FitProblem:
             box = g(f"mon{q}.box")
             comps = tuple(["Ex", "Ey", "Ez", "Hx", "Hy", "Hz"][int(c)] for c in g(f"mon{q}.comps"))
             p.monitors.append(DftMonitor(tuple(tuple(int(v) for v in r) for r in box), comps, g(f"mon{q}.freqs"), int(g(f"mon{q}.stride"))))
+        for q in range(int(g("n_pw", 0))):
+            kw = {k: g(f"pw{q}.{k}") for k in ("e_idx", "e_coef", "e_delay", "e_splits", "h_idx", "h_coef", "h_delay",
+                                               "h_splits")}
+            p.plane_waves.append(PlaneWave(
+                waveform=["gaussian", "sine"][int(g(f"pw{q}.waveform"))],
+                amplitude=float(g(f"pw{q}.amplitude")), t0=float(g(f"pw{q}.t0")), den=float(g(f"pw{q}.den")),
+                omega=float(g(f"pw{q}.omega")), scale=[float(v) for v in np.atleast_1d(g(f"pw{q}.scale", []))], **kw))
         p.e0 = [g(f"e0.{b}") for b in range(p.batch)]
         p.h0 = [g(f"h0.{b}") for b in range(p.batch)]
         return p

@@ -443,6 +443,49 @@ class DftOracle:
 
 
 # ---------------------------------------------------------------------------
+# TF/SF plane wave (sources/plane_wave.py:709-733)
+# ---------------------------------------------------------------------------
+class PlaneWaveOracle:
+    """Face patches added after each E update (``inject_E``, called with
+    ``t + dt``, fit_td.py:964-967) and each H update (``inject_H`` with
+    ``t + dt + dt/2``, fit_td.py:990-993), both at ``t_arg - dt/2``; every
+    patch adds ``coef * f(t - delay)`` in patch order."""
+
+    def __init__(self, pw, scale=1.0):
+        self.pw = pw
+        self.scale = scale
+
+    def f(self, t):
+        """``PlaneWaveSource.excitation`` (plane_wave.py:188-204)."""
+        pw = self.pw
+        if pw.waveform == "gaussian":
+            return pw.amplitude * np.exp(-((t - pw.t0) ** 2) / pw.den)
+        return pw.amplitude * np.sin(pw.omega * t)
+
+    def _apply(self, vec, idx, coef, delay, splits, t):
+        o = 0
+        for n in np.asarray(splits, int):
+            sl = slice(o, o + n)
+            w = self.f(t - delay[sl])
+            if self.scale != 1.0:
+                w = self.scale * w
+            vec[idx[sl]] += coef[sl] * w
+            o += n
+
+    def inject_E(self, e, n, dt):
+        t = n * dt
+        t_E = t + dt
+        pw = self.pw
+        self._apply(e, pw.e_idx, pw.e_coef, pw.e_delay, pw.e_splits, t_E - dt / 2)
+
+    def inject_H(self, h, n, dt):
+        t = n * dt
+        t_H = t + dt + dt / 2
+        pw = self.pw
+        self._apply(h, pw.h_idx, pw.h_coef, pw.h_delay, pw.h_splits, t_H - dt / 2)
+
+
+# ---------------------------------------------------------------------------
 # Whole run
 # ---------------------------------------------------------------------------
 class OracleRun:
@@ -465,6 +508,8 @@ class OracleRun:
         self.modal = [ModalOracle(mp, prob.dt, mp.excitation[b] if b < len(mp.excitation) else None) for mp in prob.modal]
         self.lumped = [LumpedOracle(lp, prob.dt) for lp in prob.lumped]
         self.mons = [DftOracle(m, prob.dx, prob.dy, prob.dz) for m in prob.monitors]
+        self.pws = [PlaneWaveOracle(pw, pw.scale[b] if b < len(pw.scale) else 1.0)
+                    for pw in getattr(prob, "plane_waves", [])]
         self.n = 0
         self.V = []
         self.I = []
@@ -478,6 +523,8 @@ class OracleRun:
         update_E(f, self.aE, self.bE)
         for c in self.cpml:
             c.update_E(f, self.bE)
+        for pw in self.pws:
+            pw.inject_E(f.e, n, p.dt)
         V, I = [], []
         for mo in self.modal:
             mo.update_e(f.e, n)
@@ -497,6 +544,8 @@ class OracleRun:
         update_H(f, self.aH, self.bH)
         for c in self.cpml:
             c.update_H(f, self.bH)
+        for pw in self.pws:
+            pw.inject_H(f.h, n, p.dt)
         for m in self.mons:
             m.record(f, n, p.dt)
         self.peak_e = max(self.peak_e, float(np.max(np.abs(f.e))))

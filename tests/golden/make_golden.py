@@ -137,6 +137,40 @@ def case_cpml_box():
     _save("cpml_box", prob, _outputs(s, prob, {}), n, "CPML x6, dielectric + PEC block, random initial field")
 
 
+def case_planewave_box():
+    """Two TF/SF plane waves (Gaussian along +z polarised x, sine along -y
+    polarised z) in a CPML box with a dielectric brick crossing the TF/SF
+    boundary; zero initial field."""
+    from magnelio.boundaries.cpml import CPMLBoundary
+    from magnelio.materials.material import Material
+    from magnelio.mesh.mesher import Mesh
+    from magnelio.solver.fit_td import FITTimeDomainSolver
+    from magnelio.solver.stability import courant_dt
+    from magnelio.sources.plane_wave import PlaneWaveSource
+
+    rng = np.random.default_rng(21)
+    grid = _grid(rng, (12, 13, 15))
+    L = (grid.x[-1], grid.y[-1], grid.z[-1])
+    diel = Material(name="d", epsilon=(3.0, 3.0, 3.0))
+    regions = [(diel, (0.1 * L[0], 0.3 * L[1], 0.4 * L[2], 0.7 * L[0], 0.9 * L[1], 0.7 * L[2]))]
+    mesh = Mesh.from_grid(grid, regions=regions, boundary_conditions={f: "CPML" for f in FACES})
+    bcs = {f: CPMLBoundary(f, grid, thickness_cells=3) for f in FACES}
+    srcs = [
+        PlaneWaveSource(direction=(0.0, 0.0, 1.0), polarization=(1.0, 0.0, 0.0), amplitude=2.0,
+                        waveform="gaussian", f_max=100e9),
+        PlaneWaveSource(direction=(0.0, -1.0, 0.0), polarization=(0.0, 0.0, 1.0), amplitude=0.5,
+                        waveform="sine", f_center=30e9,
+                        corners=((3e-3, 2e-3, 3e-3), (0.8 * L[0], 0.75 * L[1], 0.8 * L[2]))),
+    ]
+    n = 60
+    s = FITTimeDomainSolver(mesh=mesh, boundary_conditions=bcs, sources=srcs, total_time_steps=n,
+                            dt=courant_dt(grid, "normal"), verbose=False, backend="numpy", precision="double")
+    s.setup()
+    prob = problem_from_solver(s, n)
+    s.run()
+    _save("planewave_box", prob, _outputs(s, prob, {}), n, "TF/SF plane waves (gaussian +z, sine -y) in a CPML box")
+
+
 def case_mixed_box():
     """CPML on x and zmax, PEC on ymin / zmin, PMC on ymax."""
     from magnelio.boundaries.cpml import CPMLBoundary
@@ -457,6 +491,7 @@ def case_host_setup():
 CASES = {
     "kernel_sweep": case_kernel_sweep,
     "cpml_box": case_cpml_box,
+    "planewave_box": case_planewave_box,
     "mixed_box": case_mixed_box,
     "lumped_dft": case_lumped_dft,
     "wg_dtbc": case_wg_dtbc,

@@ -69,7 +69,7 @@ def test_kernel_sweep_matches_reference_kernels(precision, tol):
     assert _rel(h, cat(["out.Hx", "out.Hy", "out.Hz"])) < tol
 
 
-@pytest.mark.parametrize("name", ["cpml_box", "mixed_box", "lumped_dft", "wg_dtbc", "wg_mur"])
+@pytest.mark.parametrize("name", ["cpml_box", "mixed_box", "lumped_dft", "wg_dtbc", "wg_mur", "planewave_box"])
 @pytest.mark.parametrize("precision,tol", [("double", F64_TOL), ("single", F32_TOL)])
 def test_fields_match_reference(name, precision, tol):
     pe, ph = _peaks(name)
@@ -326,7 +326,7 @@ def test_compact_coefficients_need_the_stream_kernels(monkeypatch):
         eng.step(2)
 
 
-@pytest.mark.parametrize("name", ["cpml_box", "mixed_box", "lumped_dft", "wg_dtbc", "wg_mur"])
+@pytest.mark.parametrize("name", ["cpml_box", "mixed_box", "lumped_dft", "wg_dtbc", "wg_mur", "planewave_box"])
 @pytest.mark.parametrize("precision,tol", [("double", F64_TOL), ("single", F32_TOL)])
 @pytest.mark.parametrize("variant", ["0", "2"])
 def test_fused_step_matches_reference(name, precision, tol, variant, monkeypatch):
