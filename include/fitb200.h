@@ -218,6 +218,20 @@ int fitb_set_dtbc_kernel(fitb_handle* h, int32_t port, int32_t mode,
 int fitb_set_modal_source(fitb_handle* h, int32_t port, int32_t b, int32_t mode,
                           int64_t n_samples, const double* w);
 
+/* ---- dispersive materials ------------------------------------------- */
+/* One dispersive material's ADE block (solver/_dispersion.py:173-210,
+ * :504-569): side 0 = eps(omega) on E edges, 1 = mu(omega) on H faces;
+ * n_states flat indices into the reference E (or H) vector with their
+ * geometry factor g; per pole its kind (0 real, 1 conjugate pair stored
+ * once), k = (1 + a dt/2)/(1 - a dt/2), c = r/(1 - a dt/2) (imaginary parts
+ * ignored for real poles) and weight (1 or 2).  Blocks of one side are kept
+ * in the order added; the alpha/beta already carry the W folding
+ * (fit_td.py:383-399, :436-446).  Not valid in the fused step mode. */
+int fitb_add_dispersion_block(fitb_handle* h, int32_t side, int64_t n_states, const int64_t* idx,
+                              const double* g, int32_t n_poles, const int32_t* kind,
+                              const double* k_re, const double* k_im, const double* c_re,
+                              const double* c_im, const double* weight);
+
 /* ---- plane waves ---------------------------------------------------- */
 /* Replaces PlaneWaveSource.attach / inject_E / inject_H (plane_wave.py:229,
  * :720-733; called from fit_td.py:964-967, :990-993). */

@@ -17,7 +17,9 @@ from __future__ import annotations
 import numpy as np
 
 from magnelio_b200 import host
-from magnelio_b200.problem import CpmlFace, DftMonitor, FitProblem, LumpedPort, ModalPort, PlaneWave
+from magnelio_b200.problem import (
+    CpmlFace, DftMonitor, Dispersion, DispersionBlock, FitProblem, LumpedPort, ModalPort, PlaneWave,
+)
 
 _FACE_EDGES = {
     # tangential E components zeroed by PECBoundary.apply (pec.py:51-78)
@@ -85,8 +87,8 @@ def problem_from_solver(solver, n_steps: int) -> FitProblem:
     s = solver
     if s._fields is None:
         raise RuntimeError("problem_from_solver needs a solver after setup()")
-    if s._dispersion is not None or s._dispersion_mu is not None or s._sibc is not None:
-        raise NotImplementedError("dispersive materials / SIBC walls are not on the device engine yet")
+    if s._sibc is not None:
+        raise NotImplementedError("SIBC walls are not on the device engine yet")
     grid = s.mesh.grid
     nx, ny, nz = s.mesh.Nx, s.mesh.Ny, s.mesh.Nz
     dt = float(s.dt)
@@ -158,11 +160,33 @@ def problem_from_solver(solver, n_steps: int) -> FitProblem:
             freqs=np.asarray(mon.freqs, float),
             stride=int(stride),
         ))
+    for side, op in (("E", s._dispersion), ("H", s._dispersion_mu)):
+        if op is not None:
+            prob.dispersion.append(_dispersion_from_op(op, side))
     for src in s.sources:
         prob.plane_waves.append(_plane_wave_from_src(src, s))
     prob.e0 = [np.array(_np(s._fields.e_flat), dtype=np.float64)]
     prob.h0 = [np.array(_np(s._fields.h_flat), dtype=np.float64)]
     return prob
+
+
+def _dispersion_from_op(op, side) -> Dispersion:
+    """Pole constants and state subsets of a bound ``DispersionOperator``
+    (``solver/_dispersion.py:212-470``)."""
+    out = Dispersion(side=side)
+    for b in op.blocks:
+        kinds, ks, cs, ws = [], [], [], []
+        for p in b.poles:
+            cplx = np.iscomplexobj(p.J)
+            kinds.append(1 if cplx else 0)
+            ks.append(complex(p.k))
+            cs.append(complex(p.c))
+            ws.append(float(p.weight))
+        out.blocks.append(DispersionBlock(
+            idx=np.asarray(_np(b.idx), np.int64), g=np.asarray(_np(b.g), np.float64),
+            kind=np.asarray(kinds, np.int32), k=np.asarray(ks, np.complex128), c=np.asarray(cs, np.complex128),
+            weight=np.asarray(ws, np.float64)))
+    return out
 
 
 def _plane_wave_from_src(src, s) -> PlaneWave:

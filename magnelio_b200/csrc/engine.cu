@@ -104,6 +104,20 @@ struct LumpedHost {
     std::vector<double> src_host;  // [B][n_src]
 };
 
+// ADE dispersion of one side: host copies of every block, merged into the
+// device tables on each addition.
+struct DispHost {
+    DispDev dev{};
+    std::vector<long long> off, slot;
+    std::vector<double> g;
+    std::vector<int> state_block, pole_start{0}, kind;
+    std::vector<double> k_re, k_im, c_re, c_im, opk_re, opk_im, hw;
+    long long n_slots = 0;
+    DevBuf d_off, d_g, d_state_block, d_slot, d_J, d_fprev, d_pole_start, d_kind, d_k_re, d_k_im, d_c_re, d_c_im,
+        d_opk_re, d_opk_im, d_hw, d_uoff, d_ustart, d_ustate;
+    bool present() const { return !off.empty(); }
+};
+
 struct PlaneWaveHost {
     PlaneWaveDev dev{};
     DevBuf e_off, e_start, e_coef, e_delay, h_off, h_start, h_coef, h_delay, scale;
@@ -161,6 +175,7 @@ struct Handle {
     std::vector<std::unique_ptr<ModalHost>> modal;
     std::vector<std::unique_ptr<DftHost>> dft;
     std::vector<std::unique_ptr<PlaneWaveHost>> pws;
+    DispHost disp[2];  // E side, H side
     DevBuf d_lumped, d_modal, d_dft;
     int dft_stage_blocks = 0, dft_flush_blocks = 0;
     size_t dft_flush_smem = 0;
@@ -527,10 +542,13 @@ void plan_stencil(Handle& H) {
 
 // One launch of the E (which == 0) or H (which == 1) update, with the
 // handle's kernel choice: the software-pipelined stencil for one field set,
-// the bulk-copy pipeline on request, the batched kernel for B > 1.
+// the bulk-copy pipeline on request, the batched kernel for B > 1.  A side
+// with dispersive materials takes its CPML corrections in separate passes
+// after the ADE update, so its stencil launch carries no faces.
 template <typename T>
 void launch_half(Handle& H, int which) {
     StencilArgs<T> sa = stencil_args<T>(H);
+    if (H.disp[which].present()) sa.nfaces = 0;
     switch (H.stencil_mode) {
         case kModeStream:
             launch_stream_half<T>(sa, H.splan, which, H.stream);
@@ -559,6 +577,24 @@ void launch_stencil_half(Handle& H, int which) {
         launch_half<float>(H, which);
     else
         launch_half<double>(H, which);
+}
+
+// After side `sd`'s stencil launch: the ADE history subtraction and pole
+// advance, then that side's CPML faces in order (the reference's order,
+// fit_td.py:833-874).  Returns the launches issued.
+template <typename T>
+int disp_complete(Handle& H, int sd) {
+    if (!H.disp[sd].present()) return 0;
+    T* F = (sd == 0 ? H.Ec() : H.Hc()).as<T>();
+    const T* beta = (sd == 0 ? H.bE : H.bH).as<T>();
+    launch_disp_update<T>(F, H.e_block(), H.B, beta, H.disp[sd].dev, H.stream);
+    int n = 2;
+    StencilArgs<T> sa = stencil_args<T>(H);
+    for (int q = 0; q < sa.nfaces; ++q) {
+        launch_cpml_pass<T>(sa, q, sd, H.stream);
+        ++n;
+    }
+    return n;
 }
 
 // Fused step: one launch for E and H from the current buffer set into the
@@ -611,10 +647,17 @@ int enqueue_step_fused(Handle& H) {
 template <typename T>
 int enqueue_step(Handle& H) {
     if (H.stencil_mode == kModeFused) return enqueue_step_fused<T>(H);
+    // in-place kernels below
     int n = 0;
     PortsArgs pa = ports_args(H);
+    for (int sd = 0; sd < 2; ++sd) {
+        if (!H.disp[sd].present()) continue;
+        launch_disp_save<T>((sd == 0 ? H.Ec() : H.Hc()).as<T>(), H.e_block(), H.B, H.disp[sd].dev, H.stream);
+        ++n;
+    }
     launch_half<T>(H, 0);
     ++n;
+    n += disp_complete<T>(H, 0);
     for (auto& pw : H.pws) {
         launch_plane_wave<T>(H.Ec().as<T>(), H.e_block(), H.B, pw->dev, 0, H.step.as<long long>(), H.stream);
         ++n;
@@ -629,6 +672,7 @@ int enqueue_step(Handle& H) {
     }
     launch_half<T>(H, 1);
     ++n;
+    n += disp_complete<T>(H, 1);
     for (auto& pw : H.pws) {
         launch_plane_wave<T>(H.Hc().as<T>(), H.e_block(), H.B, pw->dev, 1, H.step.as<long long>(), H.stream);
         ++n;
@@ -901,6 +945,7 @@ void write_state(Handle& H, Writer& w) {
         const DevBuf& ps = H.cur ? f->psi2 : f->psi;
         dev_get(w, ps.p, ps.bytes);
     }
+    for (auto& dp : H.disp) dev_get(w, dp.d_J.p, dp.d_J.bytes);
     for (auto& lp : H.lumped) dev_get(w, lp->st.p, lp->st.bytes);
     for (auto& mp : H.modal) {
         dev_get(w, mp->st.p, mp->st.bytes);
@@ -964,6 +1009,7 @@ void read_state(Handle& H, Reader& r) {
         DevBuf& ps = H.cur ? f->psi2 : f->psi;
         r.dev(ps.p, ps.bytes);
     }
+    for (auto& dp : H.disp) r.dev(dp.d_J.p, dp.d_J.bytes);
     for (auto& lp : H.lumped) r.dev(lp->st.p, lp->st.bytes);
     for (auto& mp : H.modal) {
         r.dev(mp->st.p, mp->st.bytes);
@@ -1515,6 +1561,100 @@ int fitb_set_modal_source(fitb_handle* h, int32_t port, int32_t b, int32_t mode,
     mp.dev.exc_mode = mp.exc.as<int>();
     mp.dev.buf_len = mp.buflen.as<int>();
     H.port_tables_dirty = true;
+    fitb::invalidate_graphs(H);
+    FITB_CATCH
+}
+
+int fitb_add_dispersion_block(fitb_handle* h, int32_t side, int64_t n_states, const int64_t* idx, const double* g,
+                              int32_t n_poles, const int32_t* kind, const double* k_re, const double* k_im,
+                              const double* c_re, const double* c_im, const double* weight) {
+    FITB_TRY
+    Handle& H = H_of(h);
+    if (side != 0 && side != 1) fail(FITB_ERR_ARG, "dispersion side %d (0 = E, 1 = H)", side);
+    if (n_states < 1 || n_poles < 1 || !idx || !g || !kind || !k_re || !k_im || !c_re || !c_im || !weight)
+        fail(FITB_ERR_ARG, "dispersion block needs states, poles and all arrays");
+    if (H.steps_done != 0) fail(FITB_ERR_STATE, "dispersion must be added before the first step");
+    if (H.stencil_mode == fitb::kModeFused)
+        fail(FITB_ERR_STATE, "dispersive materials need an in-place stencil mode (not the fused step)");
+    fitb::DispHost& D = H.disp[side];
+    const int blk = (int)D.pole_start.size() - 1;
+    for (int q = 0; q < n_poles; ++q) {
+        if (kind[q] != 0 && kind[q] != 1) fail(FITB_ERR_ARG, "pole kind %d", kind[q]);
+        D.kind.push_back(kind[q]);
+        D.k_re.push_back(k_re[q]);
+        D.k_im.push_back(k_im[q]);
+        D.c_re.push_back(c_re[q]);
+        D.c_im.push_back(c_im[q]);
+        D.opk_re.push_back(1.0 + k_re[q]);
+        D.opk_im.push_back(kind[q] ? k_im[q] : 0.0);
+        D.hw.push_back(0.5 * weight[q]);
+    }
+    D.pole_start.push_back(D.pole_start.back() + n_poles);
+    for (int64_t s = 0; s < n_states; ++s) {
+        D.off.push_back(H.flat_to_off(side == 1, idx[s]));
+        D.g.push_back(g[s]);
+        D.state_block.push_back(blk);
+        D.slot.push_back(D.n_slots);
+        D.n_slots += 2LL * n_poles;
+    }
+    // entries shared by several blocks take their terms in block order
+    const long long ns = (long long)D.off.size();
+    std::vector<long long> order((size_t)ns);
+    for (long long s = 0; s < ns; ++s) order[(size_t)s] = s;
+    std::stable_sort(order.begin(), order.end(), [&](long long a, long long b) { return D.off[(size_t)a] < D.off[(size_t)b]; });
+    std::vector<long long> uoff, ustate;
+    std::vector<int> ustart;
+    for (size_t r = 0; r < order.size(); ++r) {
+        const long long st = order[r];
+        if (r == 0 || D.off[(size_t)st] != uoff.back()) {
+            uoff.push_back(D.off[(size_t)st]);
+            ustart.push_back((int)ustate.size());
+        }
+        ustate.push_back(st);
+    }
+    ustart.push_back((int)ustate.size());
+    // device tables
+    fitb::upload(D.d_off, D.off);
+    if (H.prec == 4)
+        fitb::upload(D.d_g, fitb::cast_vec<float>(D.g.data(), ns));
+    else
+        fitb::upload(D.d_g, D.g);
+    fitb::upload(D.d_state_block, D.state_block);
+    fitb::upload(D.d_slot, D.slot);
+    fitb::upload(D.d_pole_start, D.pole_start);
+    fitb::upload(D.d_kind, D.kind);
+    for (auto pr : {std::make_pair(&D.d_k_re, &D.k_re), std::make_pair(&D.d_k_im, &D.k_im),
+                    std::make_pair(&D.d_c_re, &D.c_re), std::make_pair(&D.d_c_im, &D.c_im),
+                    std::make_pair(&D.d_opk_re, &D.opk_re), std::make_pair(&D.d_opk_im, &D.opk_im),
+                    std::make_pair(&D.d_hw, &D.hw)})
+        fitb::upload(*pr.first, *pr.second);
+    fitb::upload(D.d_uoff, uoff);
+    fitb::upload(D.d_ustart, ustart);
+    fitb::upload(D.d_ustate, ustate);
+    D.d_J.alloc((size_t)H.B * D.n_slots * H.esz);
+    D.d_fprev.alloc((size_t)H.B * ns * H.esz);
+    fitb::DispDev& dv = D.dev;
+    dv.n_states = ns;
+    dv.off = D.d_off.as<long long>();
+    dv.g = D.d_g.p;
+    dv.state_block = D.d_state_block.as<int>();
+    dv.slot = D.d_slot.as<long long>();
+    dv.n_slots = D.n_slots;
+    dv.J = D.d_J.p;
+    dv.fprev = D.d_fprev.p;
+    dv.pole_start = D.d_pole_start.as<int>();
+    dv.kind = D.d_kind.as<int>();
+    dv.k_re = D.d_k_re.as<double>();
+    dv.k_im = D.d_k_im.as<double>();
+    dv.c_re = D.d_c_re.as<double>();
+    dv.c_im = D.d_c_im.as<double>();
+    dv.opk_re = D.d_opk_re.as<double>();
+    dv.opk_im = D.d_opk_im.as<double>();
+    dv.hw = D.d_hw.as<double>();
+    dv.n_unique = (long long)uoff.size();
+    dv.uoff = D.d_uoff.as<long long>();
+    dv.ustart = D.d_ustart.as<int>();
+    dv.ustate = D.d_ustate.as<long long>();
     fitb::invalidate_graphs(H);
     FITB_CATCH
 }

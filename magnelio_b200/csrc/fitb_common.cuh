@@ -270,6 +270,37 @@ void launch_plane_wave(T* field, long long blk, int B, const PlaneWaveDev& d, in
                        cudaStream_t s);
 
 // ---------------------------------------------------------------------------
+// ADE dispersion of one side (dispersion.cu).  States of all blocks are
+// concatenated; a state's pole states live at J[b][slot[s] + 2 q'] (real
+// part, imaginary part; real poles use the first).
+// ---------------------------------------------------------------------------
+struct DispDev {
+    long long n_states;
+    const long long* off;        // [n_states] entry offset in a field set's block
+    const void* g;               // [n_states] field dtype
+    const int* state_block;      // [n_states]
+    const long long* slot;       // [n_states] into a field set's J
+    long long n_slots;           // J entries per field set
+    void* J;                     // [B][n_slots] field dtype
+    void* fprev;                 // [B][n_states] field dtype
+    const int* pole_start;       // [n_blocks + 1]
+    const int* kind;             // [n_poles] 0 real, 1 conjugate pair
+    const double *k_re, *k_im, *c_re, *c_im, *opk_re, *opk_im, *hw;  // [n_poles]
+    long long n_unique;          // distinct entries
+    const long long* uoff;       // [n_unique]
+    const int* ustart;           // [n_unique + 1] into ustate
+    const long long* ustate;     // states of each entry, block order
+};
+
+template <typename T>
+void launch_disp_save(const T* F, long long blk, int B, const DispDev& d, cudaStream_t s);
+template <typename T>
+void launch_disp_update(T* F, long long blk, int B, const T* beta, const DispDev& d, cudaStream_t s);
+// CPML face q of the stencil args as a separate pass; side 0 = E, 1 = H.
+template <typename T>
+void launch_cpml_pass(const StencilArgs<T>& a, int q, int side, cudaStream_t s);
+
+// ---------------------------------------------------------------------------
 // Running-DFT monitors, staged in blocks of K recorded samples.
 // ---------------------------------------------------------------------------
 struct DftDev {

@@ -318,6 +318,24 @@ class FitEngine:
         self._monitors.append((int(out.value), (i1 - i0, j1 - j0, k1 - k0), fr.size))
         return int(out.value)
 
+    def add_dispersion_block(self, side: str, block) -> None:
+        """Upload one dispersive material's ADE block
+        (:class:`magnelio_b200.problem.DispersionBlock`) on side "E" or "H"."""
+        if side not in ("E", "H"):
+            raise ValueError(f"dispersion side {side!r}")
+        idx = np.ascontiguousarray(block.idx, dtype=np.int64)
+        g = np.ascontiguousarray(block.g, dtype=np.float64)
+        if idx.size != g.size:
+            raise ValueError("dispersion block: idx and g differ in length")
+        kind = np.ascontiguousarray(block.kind, dtype=np.int32)
+        k = np.asarray(block.k, dtype=np.complex128)
+        c = np.asarray(block.c, dtype=np.complex128)
+        parts = [np.ascontiguousarray(x) for x in (k.real, k.imag, c.real, c.imag)]
+        w = np.ascontiguousarray(block.weight, dtype=np.float64)
+        check(self._lib.fitb_add_dispersion_block(
+            self._h, 0 if side == "E" else 1, int(idx.size), i64p(idx), f64p(g), int(kind.size), i32p(kind),
+            *[f64p(x) for x in parts], f64p(w)))
+
     def add_plane_wave(self, pw) -> int:
         """Upload a TF/SF plane wave (:class:`magnelio_b200.problem.PlaneWave`):
         its ordered E and H face patches and waveform constants."""

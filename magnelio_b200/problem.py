@@ -101,6 +101,32 @@ class PlaneWave:
 
 
 @dataclass
+class DispersionBlock:
+    """Pole states of one dispersive material on its state subset
+    (``solver/_dispersion.py:173-210``): flat E (or H) indices, geometry
+    factor ``g`` per state, and per pole the recursion constants
+    ``k = (1 + a dt/2)/(1 - a dt/2)``, ``c = r/(1 - a dt/2)``, the kind (0: real
+    pole, real state; 1: conjugate pair stored once, complex state) and the
+    weight (1 or 2)."""
+
+    idx: np.ndarray
+    g: np.ndarray
+    kind: np.ndarray
+    k: np.ndarray  # complex128
+    c: np.ndarray  # complex128
+    weight: np.ndarray
+
+
+@dataclass
+class Dispersion:
+    """ADE operator of one side ("E": eps(omega), "H": mu(omega));
+    blocks in the reference's material order."""
+
+    side: str
+    blocks: list = field(default_factory=list)
+
+
+@dataclass
 class DftMonitor:
     box: tuple  # ((i0, i1), (j0, j1), (k0, k1)) cell indices, stop-exclusive
     components: tuple
@@ -128,6 +154,7 @@ class FitProblem:
     modal: list = field(default_factory=list)
     monitors: list = field(default_factory=list)
     plane_waves: list = field(default_factory=list)
+    dispersion: list = field(default_factory=list)
     batch: int = 1
     e0: list = field(default_factory=list)  # per field set initial e (or empty)
     h0: list = field(default_factory=list)
@@ -178,6 +205,9 @@ class FitProblem:
                         eng.set_lumped_source(lid, b, v)
             for mon in self.monitors:
                 eng.add_dft_monitor(mon.box, mon.components, mon.freqs, self.dx, self.dy, self.dz, stride=mon.stride)
+            for dsp in self.dispersion:
+                for bl in dsp.blocks:
+                    eng.add_dispersion_block(dsp.side, bl)
             for pw in self.plane_waves:
                 wid = eng.add_plane_wave(pw)
                 for b, sc in enumerate(pw.scale):
@@ -247,6 +277,13 @@ class FitProblem:
             put(f"mon{q}.comps", np.array([["Ex", "Ey", "Ez", "Hx", "Hy", "Hz"].index(c) for c in mon.components]))
             put(f"mon{q}.freqs", mon.freqs)
             put(f"mon{q}.stride", mon.stride)
+        put("n_disp", len(self.dispersion))
+        for q, dsp in enumerate(self.dispersion):
+            put(f"disp{q}.side", ["E", "H"].index(dsp.side))
+            put(f"disp{q}.n_blocks", len(dsp.blocks))
+            for r, bl in enumerate(dsp.blocks):
+                for k in ("idx", "g", "kind", "k", "c", "weight"):
+                    put(f"disp{q}.b{r}.{k}", getattr(bl, k))
         put("n_pw", len(self.plane_waves))
         for q, pw in enumerate(self.plane_waves):
             put(f"pw{q}.waveform", ["gaussian", "sine"].index(pw.waveform))
@@ -310,6 +347,12 @@ class FitProblem:
             box = g(f"mon{q}.box")
             comps = tuple(["Ex", "Ey", "Ez", "Hx", "Hy", "Hz"][int(c)] for c in g(f"mon{q}.comps"))
             p.monitors.append(DftMonitor(tuple(tuple(int(v) for v in r) for r in box), comps, g(f"mon{q}.freqs"), int(g(f"mon{q}.stride"))))
+        for q in range(int(g("n_disp", 0))):
+            dsp = Dispersion(side=["E", "H"][int(g(f"disp{q}.side"))])
+            for r in range(int(g(f"disp{q}.n_blocks"))):
+                dsp.blocks.append(DispersionBlock(**{k: g(f"disp{q}.b{r}.{k}") for k in
+                                                     ("idx", "g", "kind", "k", "c", "weight")}))
+            p.dispersion.append(dsp)
         for q in range(int(g("n_pw", 0))):
             kw = {k: g(f"pw{q}.{k}") for k in ("e_idx", "e_coef", "e_delay", "e_splits", "h_idx", "h_coef", "h_delay",
                                                "h_splits")}

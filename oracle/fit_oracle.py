@@ -443,6 +443,49 @@ class DftOracle:
 
 
 # ---------------------------------------------------------------------------
+# ADE dispersion (solver/_dispersion.py:504-569)
+# ---------------------------------------------------------------------------
+class DispersionOracle:
+    """Pole-current states of one side.  ``save`` stashes the field on the
+    state subsets at the top of a step (:504-515); ``update`` runs right
+    after that side's curl update and before its CPML corrections
+    (fit_td.py:833-859, :906-907): first every block subtracts
+    ``beta * sum_p (w_p/2) Re((1 + k_p) J_p)``, then every block advances
+    ``J_p <- k_p J_p + c_p g (f - f_prev)`` (:517-569)."""
+
+    def __init__(self, dsp):
+        self.blocks = []
+        for bl in dsp.blocks:
+            J = [np.zeros(bl.idx.size, np.complex128 if kd else np.float64) for kd in bl.kind]
+            self.blocks.append((bl, J, np.zeros(bl.idx.size)))
+
+    @staticmethod
+    def _kc(bl, q):
+        if bl.kind[q]:
+            return complex(bl.k[q]), complex(bl.c[q])
+        return float(np.real(bl.k[q])), float(np.real(bl.c[q]))
+
+    def save(self, f):
+        for bl, _, fp in self.blocks:
+            fp[:] = f[bl.idx]
+
+    def update(self, f, beta):
+        for bl, J, _ in self.blocks:
+            jh = None
+            for q in range(len(J)):
+                k, _c = self._kc(bl, q)
+                term = (0.5 * float(bl.weight[q])) * ((1.0 + k) * J[q]).real
+                jh = term if jh is None else jh + term
+            f[bl.idx] = f[bl.idx] - beta[bl.idx] * jh
+        for bl, J, fp in self.blocks:
+            gd = bl.g * (f[bl.idx] - fp)
+            for q in range(len(J)):
+                k, c = self._kc(bl, q)
+                J[q] *= k
+                J[q] += c * gd
+
+
+# ---------------------------------------------------------------------------
 # TF/SF plane wave (sources/plane_wave.py:709-733)
 # ---------------------------------------------------------------------------
 class PlaneWaveOracle:
@@ -510,6 +553,7 @@ class OracleRun:
         self.mons = [DftOracle(m, prob.dx, prob.dy, prob.dz) for m in prob.monitors]
         self.pws = [PlaneWaveOracle(pw, pw.scale[b] if b < len(pw.scale) else 1.0)
                     for pw in getattr(prob, "plane_waves", [])]
+        self.disp = {d.side: DispersionOracle(d) for d in getattr(prob, "dispersion", [])}
         self.n = 0
         self.V = []
         self.I = []
@@ -520,7 +564,13 @@ class OracleRun:
 
     def step(self):
         f, n, p = self.f, self.n, self.p
+        if "E" in self.disp:
+            self.disp["E"].save(f.e)
+        if "H" in self.disp:
+            self.disp["H"].save(f.h)
         update_E(f, self.aE, self.bE)
+        if "E" in self.disp:
+            self.disp["E"].update(f.e, self.bE)
         for c in self.cpml:
             c.update_E(f, self.bE)
         for pw in self.pws:
@@ -542,6 +592,8 @@ class OracleRun:
         self.V.append(V)
         self.I.append(I)
         update_H(f, self.aH, self.bH)
+        if "H" in self.disp:
+            self.disp["H"].update(f.h, self.bH)
         for c in self.cpml:
             c.update_H(f, self.bH)
         for pw in self.pws:

@@ -171,6 +171,45 @@ def case_planewave_box():
     _save("planewave_box", prob, _outputs(s, prob, {}), n, "TF/SF plane waves (gaussian +z, sine -y) in a CPML box")
 
 
+def case_dispersive_box():
+    """Dispersive materials in a CPML box driven by a TF/SF plane wave: a
+    Lorentz slab (one conjugate pole pair) spanning the whole x-y section,
+    so it runs through four absorber slabs; a two-term Debye block (real
+    poles); a block with a Debye permeability (H-side ADE)."""
+    from magnelio.boundaries.cpml import CPMLBoundary
+    from magnelio.materials.dispersion import DispersionModel
+    from magnelio.materials.material import Material
+    from magnelio.mesh.mesher import Mesh
+    from magnelio.solver.fit_td import FITTimeDomainSolver
+    from magnelio.solver.stability import courant_dt
+    from magnelio.sources.plane_wave import PlaneWaveSource
+
+    rng = np.random.default_rng(31)
+    grid = _grid(rng, (11, 12, 16))
+    L = (grid.x[-1], grid.y[-1], grid.z[-1])
+    lor = DispersionModel.lorentz(eps_inf=2.2, delta_eps=2.5, omega0=2 * np.pi * 40e9, delta=2 * np.pi * 6e9)
+    deb = DispersionModel.debye(eps_inf=3.0, delta_eps=[1.5, 0.7], tau=[4e-12, 1.5e-11])
+    mud = DispersionModel.debye(eps_inf=1.5, delta_eps=[0.8], tau=[6e-12])
+    m_lor = Material(name="lorentz", epsilon=(2.2, 2.2, 2.2), dispersion=lor)
+    m_deb = Material(name="debye", epsilon=(3.0, 3.0, 3.0), dispersion=deb)
+    m_mu = Material(name="mu_debye", mu=(1.5, 1.5, 1.5), dispersion_mu=mud)
+    regions = [(m_lor, (0.0, 0.0, 0.45 * L[2], L[0], L[1], 0.6 * L[2])),
+               (m_deb, (0.25 * L[0], 0.2 * L[1], 0.15 * L[2], 0.6 * L[0], 0.5 * L[1], 0.35 * L[2])),
+               (m_mu, (0.5 * L[0], 0.55 * L[1], 0.65 * L[2], 0.85 * L[0], 0.85 * L[1], 0.85 * L[2]))]
+    mesh = Mesh.from_grid(grid, regions=regions, boundary_conditions={f: "CPML" for f in FACES})
+    bcs = {f: CPMLBoundary(f, grid, thickness_cells=3) for f in FACES}
+    srcs = [PlaneWaveSource(direction=(0.0, 0.0, 1.0), polarization=(0.0, 1.0, 0.0), amplitude=1.5,
+                            waveform="gaussian", f_max=90e9)]
+    n = 70
+    s = FITTimeDomainSolver(mesh=mesh, boundary_conditions=bcs, sources=srcs, total_time_steps=n,
+                            dt=courant_dt(grid, "normal"), verbose=False, backend="numpy", precision="double")
+    s.setup()
+    prob = problem_from_solver(s, n)
+    s.run()
+    _save("dispersive_box", prob, _outputs(s, prob, {}), n,
+          "Lorentz slab through the CPML, Debye block, mu-Debye block; TF/SF plane wave")
+
+
 def case_mixed_box():
     """CPML on x and zmax, PEC on ymin / zmin, PMC on ymax."""
     from magnelio.boundaries.cpml import CPMLBoundary
@@ -492,6 +531,7 @@ CASES = {
     "kernel_sweep": case_kernel_sweep,
     "cpml_box": case_cpml_box,
     "planewave_box": case_planewave_box,
+    "dispersive_box": case_dispersive_box,
     "mixed_box": case_mixed_box,
     "lumped_dft": case_lumped_dft,
     "wg_dtbc": case_wg_dtbc,

@@ -69,7 +69,8 @@ def test_kernel_sweep_matches_reference_kernels(precision, tol):
     assert _rel(h, cat(["out.Hx", "out.Hy", "out.Hz"])) < tol
 
 
-@pytest.mark.parametrize("name", ["cpml_box", "mixed_box", "lumped_dft", "wg_dtbc", "wg_mur", "planewave_box"])
+@pytest.mark.parametrize(
+    "name", ["cpml_box", "mixed_box", "lumped_dft", "wg_dtbc", "wg_mur", "planewave_box", "dispersive_box"])
 @pytest.mark.parametrize("precision,tol", [("double", F64_TOL), ("single", F32_TOL)])
 def test_fields_match_reference(name, precision, tol):
     pe, ph = _peaks(name)
@@ -376,3 +377,41 @@ def test_fused_buffer_swaps_are_invisible(name, monkeypatch):
         c.step(n - k)
         ec, hc = c.read_fields()
         assert np.array_equal(ea, ec) and np.array_equal(ha, hc)
+
+
+@pytest.mark.parametrize("mode", ["simple", "bulk"])
+def test_dispersion_in_other_stencil_modes(mode, monkeypatch):
+    """The ADE update with separate CPML passes works with every in-place
+    stencil form."""
+    monkeypatch.setenv("FITB_STENCIL", mode)
+    pe, ph = _peaks("dispersive_box")
+    p, d, n, eng = _run("dispersive_box", "double")
+    with eng:
+        e, h = eng.read_fields()
+    assert _rel(e, d["out.e"], pe) < F64_TOL
+    assert _rel(h, d["out.h"], ph) < F64_TOL
+
+
+def test_dispersion_is_refused_in_the_fused_mode(monkeypatch):
+    from magnelio_b200._lib import FitbError
+
+    monkeypatch.setenv("FITB_STENCIL", "fused")
+    p, d, n = load_golden("dispersive_box")
+    with pytest.raises(FitbError, match="in-place stencil"):
+        p.build_engine("single")
+
+
+def test_dispersion_checkpoint_resume_is_bit_exact():
+    """Pole-current states travel with state_export / state_import."""
+    p, d, n = load_golden("dispersive_box")
+    k = n // 2
+    with p.build_engine("single") as a:
+        a.step(k)
+        blob = a.state_export()
+        a.step(n - k)
+        ea, ha = a.read_fields()
+    with p.build_engine("single") as b:
+        b.state_import(blob)
+        b.step(n - k)
+        eb, hb = b.read_fields()
+    assert np.array_equal(ea, eb) and np.array_equal(ha, hb)
