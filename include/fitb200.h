@@ -165,6 +165,19 @@ int fitb_set_coeffs_native(fitb_handle* h, const void* alpha_e, const void* beta
 #define FITB_COEF_F16 1
 #define FITB_COEF_BF16 2
 int fitb_set_coeff_storage(fitb_handle* h, int32_t kind);
+/* Stencil form of the handle (no counterpart in the reference, whose kernels
+ * are fixed): kind FITB_STENCIL_SIMPLE / STREAM / BULK / VEC / FUSED, a
+ * variant of that form (vec 0-3, fused 0-6), and the number of i planes one
+ * CTA marches (0: the form's own plan).  The fields, psi and all other state
+ * carry over; valid between steps.  fitb_get_stencil writes kind, variant,
+ * planes per CTA and the grid (x, y, z) into out[6]. */
+#define FITB_STENCIL_SIMPLE 0
+#define FITB_STENCIL_STREAM 1
+#define FITB_STENCIL_BULK 2
+#define FITB_STENCIL_VEC 3
+#define FITB_STENCIL_FUSED 4
+int fitb_configure_stencil(fitb_handle* h, int32_t kind, int32_t variant, int32_t ichunk);
+int fitb_get_stencil(fitb_handle* h, int32_t* out);
 /* FieldState e_flat / h_flat of field set b (field_arrays.py:98-106). */
 int fitb_set_fields(fitb_handle* h, int32_t b, const void* e, size_t e_bytes,
                     const void* hf, size_t h_bytes);

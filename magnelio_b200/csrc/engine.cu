@@ -1256,6 +1256,84 @@ int fitb_set_coeff_storage(fitb_handle* h, int32_t kind) {
     FITB_CATCH
 }
 
+int fitb_configure_stencil(fitb_handle* h, int32_t kind, int32_t variant, int32_t ichunk) {
+    FITB_TRY
+    Handle& H = H_of(h);
+    if (kind < fitb::kModeSimple || kind > fitb::kModeFused) fail(FITB_ERR_ARG, "stencil kind %d", kind);
+    if (ichunk < 0) fail(FITB_ERR_ARG, "ichunk %d", ichunk);
+    const bool compact = H.coef_kind != fitb::kCoefNative;
+    if (compact && kind != fitb::kModeStream && kind != fitb::kModeVec)
+        fail(FITB_ERR_STATE, "compact coefficient storage needs the stream or vec stencil kernels");
+    if ((kind == fitb::kModeStream || kind == fitb::kModeVec) && !fitb::stream_batch_supported(H.B))
+        fail(FITB_ERR_ARG, "the stream / vec kernels take 1, 2, 4, 8 or 16 field sets, not %d", H.B);
+    if (kind == fitb::kModeVec && (H.B > 8 || variant < 0 || variant > 3))
+        fail(FITB_ERR_ARG, "vec stencil: variant %d / batch %d", variant, H.B);
+    if (kind == fitb::kModeFused) {
+        if (variant < 0 || variant > 6 || (variant == 1 && H.prec == 8)) fail(FITB_ERR_ARG, "fused variant %d", variant);
+        if (H.disp[0].present() || H.disp[1].present())
+            fail(FITB_ERR_STATE, "dispersive materials need an in-place stencil mode (not the fused step)");
+    }
+    if (kind == fitb::kModeBulk && H.B != 1) fail(FITB_ERR_ARG, "the bulk-copy stencil takes one field set");
+    ck(cudaStreamSynchronize(H.stream), "configure sync");
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, H.desc.device);
+    if (kind == fitb::kModeBulk) {
+        fitb::BulkPlan bp = H.prec == 4 ? fitb::plan_bulk<float>(H.g, sms) : fitb::plan_bulk<double>(H.g, sms);
+        if (bp.stages < 3) fail(FITB_ERR_ARG, "the bulk-copy stencil does not fit this grid's rows");
+        ck(H.prec == 4 ? fitb::prepare_bulk<float>(bp) : fitb::prepare_bulk<double>(bp), "bulk stencil smem attribute");
+        H.plan = bp;
+    }
+    const size_t blk = (size_t)H.e_block() * H.esz;
+    if (kind == fitb::kModeFused) {
+        ck(H.prec == 4 ? fitb::prepare_fused<float>(variant) : fitb::prepare_fused<double>(variant),
+           "fused step smem attribute");
+        if (!H.e2.p) H.e2.alloc(blk * H.B);
+        if (!H.h2.p) H.h2.alloc(blk * H.B);
+        for (auto& f : H.faces)
+            if (!f->psi2.p) {
+                f->psi2.alloc(f->psi.bytes);
+                f->dev.psi_next = f->psi2.p;
+            }
+        H.fused_variant = variant;
+    } else if (H.stencil_mode == fitb::kModeFused && H.cur == 1) {
+        // leave the fused step with the current fields in the first buffer set
+        ck(cudaMemcpyAsync(H.e.p, H.e2.p, blk * H.B, cudaMemcpyDeviceToDevice, H.stream), "fields copy");
+        ck(cudaMemcpyAsync(H.h.p, H.h2.p, blk * H.B, cudaMemcpyDeviceToDevice, H.stream), "fields copy");
+        for (auto& f : H.faces)
+            ck(cudaMemcpyAsync(f->psi.p, f->psi2.p, f->psi.bytes, cudaMemcpyDeviceToDevice, H.stream), "psi copy");
+        ck(cudaStreamSynchronize(H.stream), "configure copy sync");
+        H.cur = 0;
+    }
+    if (kind == fitb::kModeVec) H.vec_variant = variant;
+    H.stencil_mode = kind;
+    fitb::plan_stencil(H);
+    if (ichunk > 0) {
+        const int nplanes = H.g.nx + 1;
+        const int c = std::min(ichunk, nplanes);
+        H.ichunk = c;
+        H.splan.ichunk = c;
+        H.splan.grid_z = (nplanes + c - 1) / c;
+    }
+    H.port_tables_dirty = true;
+    fitb::invalidate_graphs(H);
+    FITB_CATCH
+}
+
+int fitb_get_stencil(fitb_handle* h, int32_t* out) {
+    FITB_TRY
+    Handle& H = H_of(h);
+    if (!out) fail(FITB_ERR_ARG, "null argument");
+    const bool planned = H.stencil_mode == fitb::kModeStream || H.stencil_mode == fitb::kModeVec ||
+                         H.stencil_mode == fitb::kModeFused;
+    out[0] = H.stencil_mode;
+    out[1] = H.stencil_mode == fitb::kModeVec ? H.vec_variant : (H.stencil_mode == fitb::kModeFused ? H.fused_variant : 0);
+    out[2] = planned ? H.splan.ichunk : (H.stencil_mode == fitb::kModeBulk ? H.plan.ichunk : H.ichunk);
+    out[3] = planned ? H.splan.grid_x : 0;
+    out[4] = planned ? H.splan.grid_y : 0;
+    out[5] = planned ? H.splan.grid_z : 0;
+    FITB_CATCH
+}
+
 int fitb_set_fields(fitb_handle* h, int32_t b, const void* e, size_t e_bytes, const void* hf, size_t h_bytes) {
     FITB_TRY
     Handle& H = H_of(h);

@@ -131,6 +131,23 @@ class FitEngine:
         keep = arrs  # noqa: F841 (kept alive across the call)
         check(self._lib.fitb_set_coeffs_native(self._h, *ptrs))
 
+    STENCIL_KINDS = {"simple": 0, "stream": 1, "bulk": 2, "vec": 3, "fused": 4}
+
+    def configure_stencil(self, kind: str, variant: int = 0, ichunk: int = 0) -> None:
+        """Switch the stencil form between steps (fields and state carry
+        over): kind in "simple", "stream", "bulk", "vec", "fused", its
+        variant, and the i planes per CTA (0: the form's own plan)."""
+        if kind not in self.STENCIL_KINDS:
+            raise ValueError(f"stencil kind {kind!r}; expected one of {sorted(self.STENCIL_KINDS)}")
+        check(self._lib.fitb_configure_stencil(self._h, self.STENCIL_KINDS[kind], int(variant), int(ichunk)))
+
+    def stencil_config(self) -> dict:
+        out = np.zeros(6, dtype=np.int32)
+        check(self._lib.fitb_get_stencil(self._h, i32p(out)))
+        names = {v: k for k, v in self.STENCIL_KINDS.items()}
+        return {"kind": names[int(out[0])], "variant": int(out[1]), "ichunk": int(out[2]),
+                "grid": (int(out[3]), int(out[4]), int(out[5]))}
+
     COEF_STORAGE = {"native": 0, "f16": 1, "bf16": 2}
 
     def set_coefficient_storage(self, kind: str) -> None:
