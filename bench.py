@@ -199,6 +199,7 @@ def main() -> int:
     ap.add_argument("--batch", type=int, default=1, help="field sets sharing one coefficient set")
     ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of CPU-port timing")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-tune", action="store_true", help="skip the autotuner (keep the default stencil plan)")
     ap.add_argument("--coef", choices=("native", "f16", "bf16"), default="native",
                     help="coefficient storage of the stencil kernels (16-bit forms round the coefficients)")
     args = ap.parse_args()
@@ -236,9 +237,20 @@ def run_b200(args, world, rank, local):
         prob.batch = B
         v = prob.lumped[0].v_src[0]
         prob.lumped[0].v_src = [v * (1.0 + 0.1 * b) for b in range(B)]
+    tuned = None
+    if not args.no_tune:
+        # stencil form, march depth: fastest on this GPU for this grid / batch
+        from magnelio_b200 import autotune
+
+        tuned = autotune.tune_problem(prob, "single", batch_widths=(B,), device=local, coef=args.coef, iters=5)
     eng = prob.build_engine("single", device=local)
     if args.coef != "native":
         eng.set_coefficient_storage(args.coef)
+    if tuned is not None:
+        from magnelio_b200 import autotune
+
+        autotune.apply(eng, tuned)
+    stencil_cfg = eng.stencil_config()
     coef_bytes = COEF_BYTES_PER_CELL if args.coef == "native" else COEF_BYTES_PER_CELL // 2
     cells = n**3 * B
     # warm-up (graph capture, clocks)
@@ -305,7 +317,9 @@ def run_b200(args, world, rank, local):
             "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded brick box, host-built coefficients)",
-            "config": _config(args, prob), "roofline": roofline, "cpu_baseline": cpu,
+            "config": dict(_config(args, prob), stencil=stencil_cfg,
+                           autotune=None if tuned is None else [list(r[:3]) + [round(r[4], 4)] for r in tuned.table]),
+            "roofline": roofline, "cpu_baseline": cpu,
             "e2e": {"value": e2e, "unit": METRIC, "h2d_bytes_per_step": 8, "d2h_bytes_per_step": 16 * nch,
                     "how": "per step: pinned H2D of the source sample, one fitb_step, D2H of the step's V/I"},
             "gpu_launches": launches, "clocks": clocks,

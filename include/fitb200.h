@@ -178,6 +178,12 @@ int fitb_set_coeff_storage(fitb_handle* h, int32_t kind);
 #define FITB_STENCIL_FUSED 4
 int fitb_configure_stencil(fitb_handle* h, int32_t kind, int32_t variant, int32_t ichunk);
 int fitb_get_stencil(fitb_handle* h, int32_t* out);
+/* Device memory the handle holds, in bytes (every buffer it allocated; the
+ * recorder and DTBC histories grow with the step capacity). */
+int fitb_device_bytes(fitb_handle* h, int64_t* out);
+/* Size the recorder and DTBC histories for n_steps completed steps up front
+ * (they otherwise grow by doubling, which re-captures the step graphs). */
+int fitb_reserve_steps(fitb_handle* h, int64_t n_steps);
 /* FieldState e_flat / h_flat of field set b (field_arrays.py:98-106). */
 int fitb_set_fields(fitb_handle* h, int32_t b, const void* e, size_t e_bytes,
                     const void* hf, size_t h_bytes);

@@ -127,6 +127,8 @@ SIGNATURES = {
     "fitb_set_coeff_storage": ([vp, i32], C.c_int),
     "fitb_configure_stencil": ([vp, i32, i32, i32], C.c_int),
     "fitb_get_stencil": ([vp, P_i32], C.c_int),
+    "fitb_device_bytes": ([vp, P_i64], C.c_int),
+    "fitb_reserve_steps": ([vp, C.c_int64], C.c_int),
     "fitb_set_fields": ([vp, i32, cvp, sz, cvp, sz], C.c_int),
     "fitb_read_fields": ([vp, i32, vp, sz, vp, sz], C.c_int),
     "fitb_add_cpml": ([vp, i32, i32, P_f64, P_f64, P_f64, P_u8, P_u8, P_u8, P_u8], C.c_int),

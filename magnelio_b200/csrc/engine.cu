@@ -316,6 +316,38 @@ void unpack3(Handle& H, const T* dev_padded, T* host_flat, int c0) {
     check_device_status(H);
 }
 
+// Device bytes the handle holds (every buffer it allocated).
+size_t device_bytes(const Handle& H) {
+    size_t n = 0;
+    for (const DevBuf* d : {&H.e, &H.h, &H.e2, &H.h2, &H.aE, &H.bE, &H.aH, &H.bH, &H.meps, &H.mmu, &H.staging,
+                            &H.fix_cells, &H.d_lumped, &H.d_modal, &H.d_dft, &H.ticket, &H.step, &H.recV, &H.recI,
+                            &H.absmax, &H.energy_partials, &H.energy_out, &H.status})
+        n += d->bytes;
+    for (const auto& q : H.cq) n += q.bytes;
+    for (const auto& f : H.faces) n += f->psi.bytes + f->psi2.bytes + f->air.bytes + f->bcc.bytes;
+    for (const auto& l : H.lumped) n += l->off.bytes + l->sign.bytes + l->beta.bytes + l->src.bytes + l->st.bytes;
+    for (const auto& m : H.modal) {
+        for (const DevBuf* d : {&m->port_e, &m->int_e, &m->port_h, &m->me_port, &m->me_int, &m->mh_port, &m->eprof,
+                                &m->vprof, &m->hprof, &m->comp_r, &m->comp_live, &m->st, &m->whist, &m->shist,
+                                &m->comp_state, &m->scratch, &m->exc, &m->wf, &m->buflen})
+            n += d->bytes;
+        for (const auto& k : m->ktab) n += k.bytes;
+    }
+    for (const auto& m : H.dft)
+        for (const DevBuf* d : {&m->omega, &m->inv, &m->dual, &m->stage, &m->wst, &m->bins, &m->cmp, &m->base})
+            n += d->bytes;
+    for (const auto& w : H.pws)
+        for (const DevBuf* d : {&w->e_off, &w->e_start, &w->e_coef, &w->e_delay, &w->h_off, &w->h_start, &w->h_coef,
+                                &w->h_delay, &w->scale})
+            n += d->bytes;
+    for (const auto& D : H.disp)
+        for (const DevBuf* d : {&D.d_off, &D.d_g, &D.d_state_block, &D.d_slot, &D.d_J, &D.d_fprev, &D.d_pole_start,
+                                &D.d_kind, &D.d_k_re, &D.d_k_im, &D.d_c_re, &D.d_c_im, &D.d_opk_re, &D.d_opk_im,
+                                &D.d_hw, &D.d_uoff, &D.d_ustart, &D.d_ustate})
+            n += d->bytes;
+    return n;
+}
+
 void invalidate_graphs(Handle& H) {
     for (int q = 0; q < 2; ++q) {
         if (H.graph_chunk[q]) cudaGraphExecDestroy(H.graph_chunk[q]);
@@ -1316,6 +1348,22 @@ int fitb_configure_stencil(fitb_handle* h, int32_t kind, int32_t variant, int32_
     }
     H.port_tables_dirty = true;
     fitb::invalidate_graphs(H);
+    FITB_CATCH
+}
+
+int fitb_reserve_steps(fitb_handle* h, int64_t n_steps) {
+    FITB_TRY
+    Handle& H = H_of(h);
+    if (n_steps < 0) fail(FITB_ERR_ARG, "n_steps must be >= 0");
+    fitb::ensure_capacity(H, n_steps);
+    FITB_CATCH
+}
+
+int fitb_device_bytes(fitb_handle* h, int64_t* out) {
+    FITB_TRY
+    Handle& H = H_of(h);
+    if (!out) fail(FITB_ERR_ARG, "null argument");
+    *out = (int64_t)fitb::device_bytes(H);
     FITB_CATCH
 }
 

@@ -148,6 +148,17 @@ class FitEngine:
         return {"kind": names[int(out[0])], "variant": int(out[1]), "ichunk": int(out[2]),
                 "grid": (int(out[3]), int(out[4]), int(out[5]))}
 
+    def reserve_steps(self, n: int) -> None:
+        """Size the step-indexed device histories for ``n`` steps up front."""
+        check(self._lib.fitb_reserve_steps(self._h, int(n)))
+
+    @property
+    def device_bytes(self) -> int:
+        """Device memory the handle holds."""
+        out = C.c_int64()
+        check(self._lib.fitb_device_bytes(self._h, C.byref(out)))
+        return int(out.value)
+
     COEF_STORAGE = {"native": 0, "f16": 1, "bf16": 2}
 
     def set_coefficient_storage(self, kind: str) -> None:

@@ -1,0 +1,267 @@
+"""Continuous-batching serving loop for S-parameter solves on one GPU.
+
+A request is one mesh with its ports; every port excitation of the request
+is one field set of a single engine handle, so the excitations of one mesh
+advance together in every launch and read the coefficients once per cell
+(the batch dimension).  The loop:
+
+* admits requests in arrival order as soon as a slot and enough device
+  memory are free (footprint estimated from the grid before the handle is
+  built, checked against the handle's own count after);
+* keeps every admitted mesh, its fields and its histories resident on the
+  device until its last step;
+* advances all admitted handles in slices of steps, each handle on its own
+  CUDA stream, so the work of different requests overlaps on the GPU, and
+  admits new arrivals between slices (requests join and leave the running
+  set continuously);
+* on completion reads back the port voltages and currents, forms the
+  S-matrix on the host and releases the device memory.
+
+Latency is measured from a request's arrival to its S-matrix; throughput is
+solves per second of wall time.  ``plain=True`` serves the same stream one
+excitation at a time (one field set per handle, one handle at a time), the
+single-excitation form the batched loop is compared with.
+"""
+
+from __future__ import annotations
+
+import time
+from collections import deque
+from dataclasses import dataclass, field
+
+import numpy as np
+
+
+@dataclass
+class Request:
+    rid: int
+    arrival: float              # seconds after the stream starts
+    build: object               # callable(batch: int | None) -> FitProblem
+    n_ports: int
+    steps: int
+    freqs: np.ndarray
+    z0: float = 50.0
+
+
+@dataclass
+class Result:
+    rid: int
+    S: np.ndarray               # (n_freq, P, P)
+    V: np.ndarray               # (P, steps, P) port voltages per excitation
+    I: np.ndarray
+    arrival: float
+    admitted: float
+    finished: float
+    footprint: int              # estimated device bytes
+    device_bytes: int           # what the handle held
+
+    @property
+    def latency(self) -> float:
+        return self.finished - self.arrival
+
+
+@dataclass
+class ServingStats:
+    n: int
+    wall: float
+    solves_per_s: float
+    p50: float
+    p99: float
+    mean_active: float
+    peak_bytes: int
+    results: list = field(default_factory=list)
+
+    def summary(self) -> dict:
+        return {"requests": self.n, "wall_s": self.wall, "solves_per_s": self.solves_per_s,
+                "p50_s": self.p50, "p99_s": self.p99, "mean_active": self.mean_active,
+                "peak_device_bytes": self.peak_bytes}
+
+
+def estimate_footprint(nx, ny, nz, batch, steps, n_channels, cpml_layers=(), precision="single",
+                       n_dispersive_states=0) -> int:
+    """Device bytes a handle for this problem holds, from the engine's
+    padded layout: fields (B sets), coefficients and mass diagonals, the
+    staging buffer, CPML psi slabs, the V/I recorder sized for ``steps``."""
+    esz = 4 if precision == "single" else 8
+    njp, nkp = ny + 2, -(-(nz + 2) // 4) * 4
+    si = njp * nkp
+    vol = (nx + 4) * si + 8 * nkp
+    n_e = 3 * (nx + 1) * (ny + 1) * (nz + 1)
+    total = 2 * batch * 3 * vol * esz          # E, H
+    total += 6 * 3 * vol * esz                 # alpha/beta E/H, M_eps, M_mu
+    total += n_e * esz                         # staging
+    for axis, n in cpml_layers:
+        dims = [nx + 1, ny + 1, nz + 1]
+        dims[axis] = n
+        slab = dims[0] * dims[1] * dims[2]
+        total += batch * 4 * slab * esz + 4 * slab + 3 * n * esz
+    cap = max(int(steps), 1024)
+    total += 2 * batch * cap * max(n_channels, 1) * 8
+    total += n_dispersive_states * batch * 8 * esz
+    return int(total + (4 << 20))              # small tables and counters
+
+
+def _footprint_of(prob, steps, precision):
+    layers = [("xyz".index(f.face[0]), len(f.b)) for f in prob.cpml]
+    nch = len(prob.lumped) + sum(m.n_modes for m in prob.modal)
+    return estimate_footprint(prob.nx, prob.ny, prob.nz, prob.batch, steps, nch, layers, precision)
+
+
+class ServingLoop:
+    """See the module docstring.  ``engine_factory(problem, precision,
+    device)`` builds the engine of an admitted problem (the default builds a
+    :class:`~magnelio_b200.engine.FitEngine` through
+    ``FitProblem.build_engine``)."""
+
+    def __init__(self, device: int = 0, precision: str = "single", hbm_budget: int | None = None,
+                 max_slots: int = 8, slice_steps: int = 512, engine_factory=None, tune=None,
+                 clock=time.perf_counter, sleep=time.sleep):
+        self.device = device
+        self.precision = precision
+        self.max_slots = max_slots
+        self.slice_steps = slice_steps
+        self.engine_factory = engine_factory or (lambda p, prec, dev: p.build_engine(prec, device=dev))
+        self.tune = tune              # callable(problem, engine) or None
+        self.clock = clock
+        self.sleep = sleep
+        self.hbm_budget = hbm_budget if hbm_budget is not None else self._default_budget()
+
+    def _default_budget(self) -> int:
+        try:
+            import torch
+
+            free, _total = torch.cuda.mem_get_info(self.device)
+            return int(0.85 * free)
+        except Exception:
+            return 16 << 30
+
+    def run(self, requests, plain: bool = False) -> ServingStats:
+        reqs = sorted(requests, key=lambda r: r.arrival)
+        if plain:
+            # one excitation per handle, one handle at a time
+            units = [(r, p) for r in reqs for p in range(r.n_ports)]
+            slots = 1
+        else:
+            units = [(r, None) for r in reqs]
+            slots = self.max_slots
+        pending = deque([list(u) + [None] for u in units])  # [request, port, built problem]
+        active = []                   # dicts: req, port, eng, prob, done, admitted, fp
+        partial = {}                  # plain mode: rid -> per-port (V, I)
+        results = []
+        used = 0
+        peak = 0
+        active_samples = []
+        t0 = self.clock()
+        while pending or active:
+            now = self.clock() - t0
+            while pending and len(active) < slots and pending[0][0].arrival <= now:
+                req, port, prob = pending[0]
+                if prob is None:
+                    prob = pending[0][2] = self._problem(req, port)
+                fp = _footprint_of(prob, req.steps, self.precision)
+                if active and used + fp > self.hbm_budget:
+                    break                         # wait for memory (arrival order kept)
+                pending.popleft()
+                eng = self.engine_factory(prob, self.precision, self.device)
+                if self.tune is not None:
+                    self.tune(prob, eng)
+                eng.reserve_steps(req.steps)
+                used += fp
+                peak = max(peak, used)
+                active.append({"req": req, "port": port, "eng": eng, "prob": prob, "done": 0,
+                               "admitted": self.clock() - t0, "fp": fp})
+            if not active:
+                nxt = pending[0][0].arrival
+                self.sleep(max(0.0, nxt - (self.clock() - t0)))
+                continue
+            active_samples.append(len(active))
+            # one slice on every admitted handle (asynchronous, own streams)
+            for a in active:
+                k = min(self.slice_steps, a["req"].steps - a["done"])
+                a["eng"].step(k)
+                a["k"] = k
+            still = []
+            for a in active:
+                a["eng"].sync()
+                a["done"] += a["k"]
+                if a["done"] < a["req"].steps:
+                    still.append(a)
+                    continue
+                req = a["req"]
+                eng = a["eng"]
+                nset = a["prob"].batch
+                VI = [eng.read_vi(b) for b in range(nset)]
+                dev_bytes = eng.device_bytes
+                eng.close()
+                used -= a["fp"]
+                fin = self.clock() - t0
+                if a["port"] is None:
+                    V = np.stack([v for v, _ in VI[:req.n_ports]])
+                    I = np.stack([i for _, i in VI[:req.n_ports]])
+                    results.append(self._result(req, V, I, a, fin, dev_bytes))
+                else:
+                    got = partial.setdefault(req.rid, {})
+                    got[a["port"]] = VI[0]
+                    if len(got) == req.n_ports:
+                        V = np.stack([got[p][0] for p in range(req.n_ports)])
+                        I = np.stack([got[p][1] for p in range(req.n_ports)])
+                        results.append(self._result(req, V, I, a, fin, dev_bytes))
+                        del partial[req.rid]
+            active = still
+        wall = self.clock() - t0
+        lat = np.array([r.latency for r in results]) if results else np.zeros(1)
+        return ServingStats(n=len(results), wall=wall, solves_per_s=len(results) / max(wall, 1e-9),
+                            p50=float(np.percentile(lat, 50)), p99=float(np.percentile(lat, 99)),
+                            mean_active=float(np.mean(active_samples)) if active_samples else 0.0,
+                            peak_bytes=int(peak), results=sorted(results, key=lambda r: r.rid))
+
+    @staticmethod
+    def _problem(req, port):
+        prob = req.build(None)
+        if port is not None:
+            # the single-excitation form: field set 0 drives `port`
+            prob.batch = 1
+            for lp in prob.lumped:
+                lp.v_src = [lp.v_src[port]]
+            prob.e0 = prob.e0[:1]
+            prob.h0 = prob.h0[:1]
+        return prob
+
+    def _result(self, req, V, I, a, fin, dev_bytes):
+        from magnelio_b200.workloads import s_matrix
+
+        dt = a["prob"].dt
+        S = s_matrix(V, I, dt, req.freqs, req.z0, req.n_ports)
+        return Result(rid=req.rid, S=S, V=V, I=I, arrival=req.arrival, admitted=a["admitted"], finished=fin,
+                      footprint=a["fp"], device_bytes=dev_bytes)
+
+
+def request_stream(n: int, seed: int = 7, mean_gap: float = 0.020, cells=(32**3, 192**3), steps=(6000, 12000),
+                   ports=(2, 4), n_freq: int = 101):
+    """The serving workload: ``n`` requests with Poisson arrivals (mean gap
+    ``mean_gap`` s), each a rectangular or single-ridge waveguide section
+    with dimensions ``U[0.7, 1.3]`` x (22.86, 10.16, 40) mm, 0-4 dielectric
+    inserts (``eps_r ~ U[2, 10]``), a log-uniform cell count in ``cells``,
+    ``ports`` lumped ports and a step count in ``steps``."""
+    from magnelio_b200.workloads import waveguide_section
+
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    out = []
+    for rid in range(n):
+        t += float(rng.exponential(mean_gap))
+        dims = np.array([22.86e-3, 10.16e-3, 40e-3]) * rng.uniform(0.7, 1.3, 3)
+        c = int(np.exp(rng.uniform(np.log(cells[0]), np.log(cells[1]))))
+        P = int(rng.integers(ports[0], ports[1] + 1))
+        st = int(rng.integers(steps[0], steps[1] + 1))
+        ins = int(rng.integers(0, 5))
+        ridged = bool(rng.integers(0, 2))
+        sub = int(rng.integers(0, 2**31 - 1))
+
+        def build(batch, dims=dims, c=c, P=P, st=st, ins=ins, ridged=ridged, sub=sub):
+            return waveguide_section(np.random.default_rng(sub), a=dims[0], b=dims[1], length=dims[2], cells=c,
+                                     n_inserts=ins, ridged=ridged, n_ports=P, steps=st, batch=batch)
+
+        out.append(Request(rid=rid, arrival=t, build=build, n_ports=P, steps=st,
+                           freqs=np.linspace(7.0e9, 13.0e9, n_freq)))
+    return out

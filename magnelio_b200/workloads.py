@@ -129,3 +129,113 @@ def cells_in_cpml(prob: FitProblem) -> int:
         dims[a] = len(f.b)
         tot += int(np.prod(dims))
     return tot
+
+
+# ---------------------------------------------------------------------------
+# Serving requests: waveguide sections with lumped ports
+# ---------------------------------------------------------------------------
+def _pec_edges_in_box(x, y, z, lo, hi) -> np.ndarray:
+    """Flat E indices of the edges lying in the closed box [lo, hi] (the
+    tangential and interior edges of a PEC block)."""
+    nx, ny, nz = len(x) - 1, len(y) - 1, len(z) - 1
+    tol = 1e-12
+    inn = [lambda v, a=a: (v >= lo[a] - tol) & (v <= hi[a] + tol) for a in range(3)]
+    out = []
+    off = 0
+    for comp in "xyz":
+        # edge spans [n_a, n_a+1] along its own axis, sits on nodes elsewhere
+        axes = []
+        for a, nodes in enumerate((x, y, z)):
+            if "xyz"[a] == comp:
+                axes.append(inn[a](nodes[:-1]) & inn[a](nodes[1:]))
+            else:
+                axes.append(inn[a](nodes))
+        m = axes[0][:, None, None] & axes[1][None, :, None] & axes[2][None, None, :]
+        out.append(np.nonzero(m.ravel())[0] + off)
+        off += m.size
+    return np.concatenate(out)
+
+
+def waveguide_section(rng, *, a: float = 22.86e-3, b: float = 10.16e-3, length: float = 40e-3,
+                      cells: int = 48**3, n_inserts: int = 2, ridged: bool = False, n_ports: int = 2,
+                      steps: int = 6000, f_min: float = 7.0e9, f_max: float = 13.0e9, cpml_cells: int = 8,
+                      z0: float = 50.0, batch: int | None = None) -> FitProblem:
+    """One S-parameter request of the serving workload: an ``a x b x length``
+    rectangular (or single-ridge) waveguide section on a uniform grid of
+    about ``cells`` cells, PEC side walls, CPML on both ends (matched guide
+    terminations), ``n_inserts`` dielectric blocks (``eps_r ~ U[2, 10]``) and
+    ``n_ports`` y-directed lumped ports (50 Ohm) spread along the guide.
+    Field set ``p`` drives port ``p`` with a modulated Gaussian over
+    ``[f_min, f_max]``, the other ports load it; field sets beyond the ports
+    (``batch`` rounds up to a width the batched kernels take) stay idle."""
+    from magnelio_b200.adapter import _pec_face_flat_indices
+
+    h = (a * b * length / cells) ** (1.0 / 3.0)
+    nx, ny, nz = (max(8, int(round(v / h))) for v in (a, b, length))
+    x, y, z = (np.linspace(0.0, v, n + 1) for v, n in ((a, nx), (b, ny), (length, nz)))
+    bricks, eps_r = [], []
+    for _ in range(n_inserts):
+        size = rng.uniform(0.15, 0.45, 3) * np.array([a, b, length])
+        lo = rng.uniform(0.0, 1.0, 3) * (np.array([a, b, length]) - size)
+        lo[2] = max(lo[2], (cpml_cells + 2) * h)
+        bricks.append((lo, lo + size))
+        eps_r.append(float(rng.uniform(2.0, 10.0)))
+    mat_id = host.assign_bricks(x, y, z, bricks) if bricks else np.zeros((nx, ny, nz), np.int32)
+    eps_table = np.concatenate([[1.0], eps_r])
+    M_eps = host.build_M_eps(x, y, z, eps_table, mat_id)
+    M_mu = host.build_M_mu(x, y, z)
+    dt = host.courant_dt(x, y, z, "normal")
+    aE, bE, aH, bH = host.leapfrog_coefficients(M_eps, M_mu, dt)
+    pec = [_pec_face_flat_indices(nx, ny, nz, f) for f in ("xmin", "xmax", "ymin", "ymax")]
+    if ridged:
+        w, d = rng.uniform(0.2, 0.4) * a, rng.uniform(0.2, 0.4) * b
+        pec.append(_pec_edges_in_box(x, y, z, (0.5 * (a - w), b - d, 0.0), (0.5 * (a + w), b, length)))
+    pec = np.concatenate(pec)
+    aE[pec] = 0.0
+    bE[pec] = 0.0
+    B = batch if batch is not None else n_ports
+    B = next(w for w in (1, 2, 4, 8, 16, B) if w >= B)
+    prob = FitProblem(nx=nx, ny=ny, nz=nz, dt=dt, dx=np.diff(x), dy=np.diff(y), dz=np.diff(z),
+                      alpha_E=aE, beta_E=bE, alpha_H=aH, beta_H=bH, M_eps=M_eps, M_mu=M_mu, batch=B)
+    for face in ("zmin", "zmax"):
+        bt, ct, ckt = host.cpml_tables(np.diff(z), face, dt, thickness_cells=cpml_cells)
+        prob.cpml.append(CpmlFace(face, bt, ct, ckt))
+    t = np.arange(steps + 1) * dt
+    drive = 2.0 * math.sqrt(z0) * host.modulated_gaussian(t + dt, f_max, f_min)
+    n_ex = nx * (ny + 1) * (nz + 1)
+    k_lo, k_hi = cpml_cells + 2, nz - cpml_cells - 3
+    for p in range(n_ports):
+        k = int(round(k_lo + (k_hi - k_lo) * (p / max(1, n_ports - 1))))
+        i = int(np.clip(nx // 2 + rng.integers(-nx // 6, nx // 6 + 1), 1, nx - 1))
+        j = max(1, ny // 4)
+        flat = n_ex + (i * ny + j) * (nz + 1) + k  # Ey (nx+1, ny, nz+1)
+        v = [drive if q == p else np.zeros_like(drive) for q in range(B)]
+        prob.lumped.append(LumpedPort(flat_idx=np.array([flat], np.int64), signs=np.ones(1),
+                                      betas=np.array([dt / M_eps[flat]]), R=z0, record_scale=1.0, v_src=v))
+    prob.e0 = [None] * B
+    prob.h0 = [None] * B
+    return prob
+
+
+def s_matrix(V, I, dt: float, freqs, z0: float = 50.0, n_ports: int | None = None) -> np.ndarray:
+    """S-parameters of lumped ports from per-excitation port voltages and
+    currents: ``V[b]``, ``I[b]`` of shape (steps, ports) for excitation b
+    (port b driven).  Power waves ``a = (V + Z0 I) / (2 sqrt Z0)``,
+    ``b = (V - Z0 I) / (2 sqrt Z0)`` from a direct DFT of the records at
+    ``t_n = (n + 1) dt``; ``S[f, j, i] = b_j / a_i`` for excitation i.
+    Returns an array of shape (n_freq, P, P)."""
+    V = np.asarray(V, float)
+    I = np.asarray(I, float)
+    P = n_ports if n_ports is not None else V.shape[0]
+    steps = V.shape[1]
+    t = (np.arange(steps) + 1) * dt
+    ph = np.exp(-2j * np.pi * np.outer(np.asarray(freqs, float), t)) * dt  # (F, steps)
+    S = np.zeros((len(freqs), P, P), complex)
+    rz = math.sqrt(z0)
+    for i in range(P):
+        Vf = ph @ V[i][:, :P]
+        If = ph @ I[i][:, :P]
+        a = (Vf + z0 * If) / (2 * rz)
+        bw = (Vf - z0 * If) / (2 * rz)
+        S[:, :, i] = bw / a[:, i:i + 1]
+    return S

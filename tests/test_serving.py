@@ -1,0 +1,159 @@
+"""Serving loop mechanics on a scripted engine and a virtual clock (no GPU):
+admission by footprint and slots, arrival order, continuous joining,
+latency accounting, batched vs single-excitation results, S-matrix
+extraction."""
+
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import pytest
+
+from magnelio_b200 import serving, workloads
+
+
+class Clock:
+    def __init__(self):
+        self.t = 0.0
+
+    def __call__(self):
+        return self.t
+
+    def sleep(self, dt):
+        self.t += max(dt, 1e-6)
+
+
+class ScriptedEngine:
+    """Steps cost virtual time; V/I of field set b depend only on the
+    problem and the excitation that field set carries."""
+
+    live = []
+
+    def __init__(self, prob, clock, cost_per_cell_step=1e-9):
+        self.p = prob
+        self.clock = clock
+        self.cost = cost_per_cell_step * prob.nx * prob.ny * prob.nz * prob.batch
+        self.n = 0
+        self.cap = 0
+        ScriptedEngine.live.append(self)
+        self.closed = False
+
+    def reserve_steps(self, n):
+        self.cap = n
+
+    def step(self, k):
+        self.n += k
+        self.clock.t += self.cost * k
+
+    def sync(self):
+        pass
+
+    def read_vi(self, b):
+        P = len(self.p.lumped)
+        V = np.zeros((self.n, P))
+        I = np.zeros((self.n, P))
+        rng = np.random.default_rng(self.p.nx * 1000 + self.p.nz)
+        coup = rng.uniform(-0.5, 0.5, (P, P)) + np.eye(P)
+        for q, lp in enumerate(self.p.lumped):
+            src = lp.v_src[b][: self.n] if len(lp.v_src[b]) else np.zeros(self.n)
+            for j in range(P):
+                V[:, j] += coup[j, q] * src
+                I[:, j] += 0.01 * coup[q, j] * src
+        return V, I
+
+    @property
+    def device_bytes(self):
+        return serving.estimate_footprint(self.p.nx, self.p.ny, self.p.nz, self.p.batch, self.cap,
+                                          len(self.p.lumped)) // 2
+
+    def close(self):
+        self.closed = True
+
+
+def _loop(clock, **kw):
+    return serving.ServingLoop(engine_factory=lambda p, prec, dev: ScriptedEngine(p, clock), clock=clock,
+                               sleep=clock.sleep, **kw)
+
+
+def _stream(n=10, steps=(200, 400)):
+    return serving.request_stream(n, seed=3, mean_gap=0.002, cells=(12**3, 20**3), steps=steps, ports=(2, 4),
+                                  n_freq=5)
+
+
+def test_every_request_completes_with_its_own_s_matrix():
+    clock = Clock()
+    ScriptedEngine.live = []
+    stats = _loop(clock, hbm_budget=1 << 40, max_slots=4, slice_steps=64).run(_stream())
+    assert stats.n == 10 and [r.rid for r in stats.results] == list(range(10))
+    assert all(e.closed for e in ScriptedEngine.live)
+    for r in stats.results:
+        P = r.S.shape[1]
+        assert r.S.shape == (5, P, P) and r.V.shape[0] == P
+        assert r.finished >= r.admitted >= r.arrival
+    assert 0 < stats.p50 <= stats.p99
+    assert stats.mean_active > 1.0  # requests overlapped
+
+
+def test_slots_and_memory_budget_bound_the_running_set():
+    clock = Clock()
+    reqs = _stream(8)
+    fps = [serving._footprint_of(serving.ServingLoop._problem(r, None), r.steps, "single") for r in reqs]
+    budget = int(2.5 * max(fps))
+    loop = _loop(clock, hbm_budget=budget, max_slots=8, slice_steps=32)
+    seen = []
+    orig = loop.engine_factory
+
+    def factory(p, prec, dev):
+        e = orig(p, prec, dev)
+        seen.append(sum(1 for x in ScriptedEngine.live if not x.closed))
+        return e
+
+    ScriptedEngine.live = []
+    loop.engine_factory = factory
+    stats = loop.run(reqs)
+    assert stats.n == 8
+    assert stats.peak_bytes <= budget
+    assert max(seen) <= 3
+
+
+def test_batched_and_single_excitation_forms_agree():
+    clock = Clock()
+    reqs = _stream(5)
+    batched = _loop(clock, hbm_budget=1 << 40, max_slots=4, slice_steps=50).run(reqs)
+    clock2 = Clock()
+    plain = _loop(clock2, hbm_budget=1 << 40, slice_steps=50).run(reqs, plain=True)
+    assert plain.n == batched.n == 5
+    for a, b in zip(batched.results, plain.results):
+        np.testing.assert_allclose(a.V, b.V, rtol=0, atol=0)
+        np.testing.assert_allclose(a.S, b.S, rtol=1e-12, atol=0)
+
+
+def test_s_matrix_of_a_matched_two_port_line():
+    """Two ports joined by an ideal delay line of Z0: S11 = S22 = 0,
+    |S21| = |S12| = 1."""
+    dt, n, z0, d = 1e-12, 4000, 50.0, 25
+    t = (np.arange(n) + 1) * dt
+    inc = np.exp(-((t - 200e-12) / 40e-12) ** 2)
+    V = np.zeros((2, n, 2))
+    I = np.zeros((2, n, 2))
+    for i in range(2):
+        j = 1 - i
+        V[i, :, i] = inc
+        I[i, :, i] = inc / z0
+        out = np.concatenate([np.zeros(d), inc[:-d]])
+        V[i, :, j] = out
+        I[i, :, j] = -out / z0
+    S = workloads.s_matrix(V, I, dt, [2e9, 4e9], z0)
+    assert np.max(np.abs(S[:, 0, 0])) < 1e-12 and np.max(np.abs(S[:, 1, 1])) < 1e-12
+    np.testing.assert_allclose(np.abs(S[:, 1, 0]), 1.0, rtol=1e-9)
+    np.testing.assert_allclose(np.angle(S[:, 1, 0]), np.angle(np.exp(-2j * math.pi * np.array([2e9, 4e9]) * d * dt)),
+                               atol=1e-9)
+
+
+def test_footprint_estimate_counts_the_big_buffers():
+    fp = serving.estimate_footprint(64, 64, 64, 4, 1000, 4, [(2, 8), (2, 8)])
+    vol = 68 * 66 * 68 + 8 * 68
+    assert fp > 2 * 4 * 3 * vol * 4 + 6 * 3 * vol * 4
+    with pytest.raises(TypeError):
+        serving.estimate_footprint(64, 64)
