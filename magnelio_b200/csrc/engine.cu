@@ -57,6 +57,13 @@ void ck(cudaError_t e, const char* what) {
 }
 
 // Owning device buffer.
+// Setup copies and fills below run on the legacy default stream, which the
+// handles' non-blocking streams do not wait for, and a pageable host-to-
+// device cudaMemcpy may return before its DMA lands: each one is finished
+// (legacy_sync) before the function that issued it returns, so no kernel on
+// a handle's stream can read a table that is still being written.
+inline void legacy_sync(const char* what) { ck(cudaStreamSynchronize(0), what); }
+
 struct DevBuf {
     void* p = nullptr;
     size_t bytes = 0;
@@ -74,7 +81,10 @@ struct DevBuf {
         if (n == 0) return;
         ck(cudaMalloc(&p, n), "cudaMalloc");
         bytes = n;
-        if (zero) ck(cudaMemset(p, 0, n), "cudaMemset");
+        if (zero) {
+            ck(cudaMemset(p, 0, n), "cudaMemset");
+            legacy_sync("cudaMemset sync");
+        }
     }
     template <typename U>
     U* as() const {
@@ -85,7 +95,10 @@ struct DevBuf {
 template <typename U>
 void upload(DevBuf& d, const std::vector<U>& v) {
     d.alloc(v.size() * sizeof(U), false);
-    if (!v.empty()) ck(cudaMemcpy(d.p, v.data(), v.size() * sizeof(U), cudaMemcpyHostToDevice), "upload");
+    if (!v.empty()) {
+        ck(cudaMemcpy(d.p, v.data(), v.size() * sizeof(U), cudaMemcpyHostToDevice), "upload");
+        legacy_sync("upload sync");
+    }
 }
 
 long long round_up(long long x, long long m) { return (x + m - 1) / m * m; }
@@ -361,6 +374,8 @@ void invalidate_graphs(Handle& H) {
 // and invalidates the captured graphs (they hold the old pointers).
 void ensure_capacity(Handle& H, long long need) {
     if (need <= H.cap) return;
+    // steps still running on the handle's stream write the old histories
+    ck(cudaStreamSynchronize(H.stream), "capacity sync");
     long long ncap = std::max(need, std::max<long long>(2 * H.cap, 1024));
     if (H.nch > 0) {
         for (DevBuf* buf : {&H.recV, &H.recI}) {
@@ -388,6 +403,7 @@ void ensure_capacity(Handle& H, long long need) {
             std::swap(buf->bytes, nb.bytes);
         }
     }
+    legacy_sync("capacity copy sync");
     H.cap = ncap;
     H.port_tables_dirty = true;
     invalidate_graphs(H);
@@ -431,6 +447,8 @@ void build_fix_cells(Handle& H) {
 
 void refresh_port_tables(Handle& H) {
     if (!H.port_tables_dirty) return;
+    // the tables below are re-allocated: no launch may still read the old ones
+    ck(cudaStreamSynchronize(H.stream), "port tables sync");
     std::vector<LumpedDev> ld;
     for (auto& lp : H.lumped) ld.push_back(lp->dev);
     upload(H.d_lumped, ld);
@@ -1029,6 +1047,7 @@ void read_state(Handle& H, Reader& r) {
     if (prec != H.prec || B != H.B || nx != H.g.nx || ny != H.g.ny || nz != H.g.nz)
         fail(FITB_ERR_ARG, "state buffer was written by a differently configured handle");
     long long steps = r.pod<long long>();
+    ck(cudaStreamSynchronize(H.stream), "state import sync");
     ensure_capacity(H, steps + 1);
     for (int b = 0; b < H.B; ++b) {
         std::vector<T> ev((size_t)H.nE()), hv((size_t)H.nH());
@@ -1067,6 +1086,7 @@ void read_state(Handle& H, Reader& r) {
         m->base_host = steps;
         ck(cudaMemcpy(m->base.p, &steps, sizeof(long long), cudaMemcpyHostToDevice), "dft base");
     }
+    legacy_sync("state import copy sync");
 }
 
 }  // namespace

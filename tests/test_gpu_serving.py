@@ -46,3 +46,31 @@ def test_batched_form_matches_one_excitation_per_handle():
         si = float(np.max(np.abs(b.I)))
         assert float(np.max(np.abs(a.V - b.V))) <= BATCH_TOL * sv
         assert float(np.max(np.abs(a.I - b.I))) <= BATCH_TOL * si
+
+
+S_TOL = 1e-3      # |S_gpu - S_oracle|, linear
+PHASE_TOL = 0.1   # degrees, where |S| > 0.05
+
+
+def test_served_s_matrix_meets_the_fp64_oracle():
+    """Float32 batched serving vs the float64 CPU oracle on the same
+    request: the S-matrix agrees to |dS| <= 1e-3 and 0.1 degree."""
+    from oracle.fit_oracle import OracleRun
+    from magnelio_b200 import serving, workloads
+
+    reqs = serving.request_stream(1, seed=5, mean_gap=0.0, cells=(14**3, 14**3), steps=(900, 900), ports=(2, 2),
+                                  n_freq=9)
+    req = reqs[0]
+    res = serving.ServingLoop(max_slots=1, slice_steps=300).run([req]).results[0]
+    prob = req.build(None)
+    Vs, Is = [], []
+    for b in range(req.n_ports):
+        r = OracleRun(prob, b=b).run(req.steps)
+        Vs.append(np.array(r.V))
+        Is.append(np.array(r.I))
+    S_ref = workloads.s_matrix(np.stack(Vs), np.stack(Is), prob.dt, req.freqs, req.z0, req.n_ports)
+    dS = np.abs(res.S - S_ref)
+    assert float(dS.max()) <= S_TOL, float(dS.max())
+    big = np.abs(S_ref) > 0.05
+    dphi = np.degrees(np.abs(np.angle(res.S[big] / S_ref[big])))
+    assert float(dphi.max()) <= PHASE_TOL, float(dphi.max())
