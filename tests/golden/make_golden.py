@@ -338,14 +338,14 @@ def _wr90(nx=9, ny=4, nz=12, length=24e-3):
                                                      "zmin": "PMC", "zmax": "PMC"})
 
 
-def _wg_solver(mesh, excited, n, modify=None):
+def _wg_solver(mesh, excited, n, modify=None, n_modes=2):
     import magnelio.analysis.scattering_td as std
     from magnelio._operators.material_matrices import build_M_eps, build_M_mu
     from magnelio.ports.declarative import PortWaveguide
     from magnelio.solver.fit_td import FITTimeDomainSolver
     from magnelio.solver.stability import spectral_dt
 
-    ports = [PortWaveguide("p1", "zmin", n_modes=2), PortWaveguide("p2", "zmax", n_modes=2)]
+    ports = [PortWaveguide("p1", "zmin", n_modes=n_modes), PortWaveguide("p2", "zmax", n_modes=n_modes)]
     an = std.AnalysisScatteringTD(mesh=mesh, f_max=25e9, ports=ports, verbose=False, backend="numpy",
                                   precision="double", n_freq=11)
     m_eps, m_mu = build_M_eps(mesh), build_M_mu(mesh)
@@ -358,6 +358,77 @@ def _wg_solver(mesh, excited, n, modify=None):
                             verbose=False, backend="numpy", precision="double")
     s.setup()
     return s
+
+
+def case_cfg1_wr90():
+    """The plain small configuration: WR-90 section 22.86 x 10.16 x 40 mm on a
+    29 x 13 x 51 grid, two waveguide ports (zmin, zmax) x 3 modes, all six
+    excitations, 8000 steps, the analysis's own 501-point S-matrix.  Stores
+    the engine problem (batched: field set b = excitation b), the
+    reference's V/I per excitation, its S-matrix, each channel's linear
+    power-wave map (a, b as functions of V(f), I(f); post/modal_sparameters.py:118-250)
+    and the final fields of the first excitation."""
+    import magnelio.analysis.scattering_td as std
+    from magnelio.ports.declarative import PortWaveguide
+    from magnelio.post.modal_sparameters import spectral_power_waves
+
+    from oracle.fit_oracle import OracleRun
+
+    n = 8000
+    mesh = _wr90(29, 13, 51, 40e-3)
+    ports = [PortWaveguide("p1", "zmin", n_modes=3), PortWaveguide("p2", "zmax", n_modes=3)]
+    an = std.AnalysisScatteringTD(mesh=mesh, f_max=25e9, ports=ports, verbose=False, backend="numpy",
+                                  precision="double", n_freq=501)
+    res = an.run(excited=[(pt, m) for pt in ("p1", "p2") for m in range(3)], total_time_steps=n,
+                 energy_stop_db=None, port_signal_stop_db=None)
+    excs = list(res.signals.keys())
+    assert len(excs) == 6, excs
+    chans = list(res.channels)
+    f_axis = np.asarray(res.f_axis, float)
+    out = {"cfg1.f_axis": f_axis, "cfg1.dt": np.asarray(res.dt)}
+    # engine problem per excitation, merged into one batched problem
+    probs = []
+    for ex in excs:
+        s = _wg_solver(mesh, ex, n, n_modes=3)
+        assert abs(s.dt - res.dt) == 0.0
+        probs.append((s, problem_from_solver(s, n)))
+    prob = probs[0][1]
+    prob.batch = len(excs)
+    for q, mp in enumerate(prob.modal):
+        mp.excitation = [pb.modal[q].excitation[0] for _, pb in probs]
+    prob.e0 = [pb.e0[0] for _, pb in probs]
+    prob.h0 = [pb.h0[0] for _, pb in probs]
+    # reference V/I per excitation in engine channel order (modal ports in order)
+    order = [(op.name, m) for op in probs[0][0].ports for m in range(op.n_modes)]
+    for b, ex in enumerate(excs):
+        sig = res.signals[ex]
+        out[f"cfg1.V{b}"] = np.stack([np.asarray(sig[c][0].values, float) for c in order], axis=1)
+        out[f"cfg1.I{b}"] = np.stack([np.asarray(sig[c][1].values, float) for c in order], axis=1)
+        # the problem reproduces the analysis run: oracle vs reference, first 400 steps
+        r = OracleRun(prob, b=b).run(400)
+        dv = np.max(np.abs(np.array(r.V) - out[f"cfg1.V{b}"][:400])) / np.max(np.abs(out[f"cfg1.V{b}"]))
+        assert dv < 1e-10, (ex, dv)
+    out["cfg1.excited"] = np.array([order.index(ex) for ex in excs])
+    # S-matrix: S[f, channel, excitation]
+    S = np.stack([np.stack([np.asarray(res.s_params.S(c[0], ex[0], mode_out=c[1], mode_in=ex[1]), complex)
+                            for c in order], axis=1) for ex in excs], axis=2)
+    out["cfg1.S"] = S
+    # linear power-wave maps per channel
+    omega = 2.0 * np.pi * f_axis
+    one, zero = np.ones_like(f_axis, complex), np.zeros_like(f_axis, complex)
+    for ci, (port, m) in enumerate(order):
+        mode = res.port_modes[port][m]
+        ndx = res.port_normal_dx.get(port) if res.port_normal_dx else None
+        lp = res.port_line_params.get((port, m)) if res.port_line_params else None
+        aV, bV = spectral_power_waves(one, zero, omega, res.dt, mode, normal_dx=ndx, line_params=lp)
+        aI, bI = spectral_power_waves(zero, one, omega, res.dt, mode, normal_dx=ndx, line_params=lp)
+        out[f"cfg1.map{ci}"] = np.stack([aV, aI, bV, bI])
+        out[f"cfg1.icot{ci}"] = np.asarray(bool(getattr(mode, "i_cotemporal", False)))
+    s0 = probs[0][0]
+    s0.run()
+    out["out.e"] = np.asarray(s0._fields.e_flat, float).copy()
+    out["out.h"] = np.asarray(s0._fields.h_flat, float).copy()
+    _save("cfg1_wr90", prob, out, n, "WR-90 29x13x51, 2 ports x 3 modes, six excitations, 8000 steps, 501-point S")
 
 
 def case_wg_dtbc():
@@ -532,6 +603,7 @@ CASES = {
     "cpml_box": case_cpml_box,
     "planewave_box": case_planewave_box,
     "dispersive_box": case_dispersive_box,
+    "cfg1_wr90": case_cfg1_wr90,
     "mixed_box": case_mixed_box,
     "lumped_dft": case_lumped_dft,
     "wg_dtbc": case_wg_dtbc,
