@@ -27,6 +27,9 @@ from magnelio_b200._lib import FitbError
 # (kind, variant, i planes per CTA; 0 = the form's own plan)
 DEFAULT_CANDIDATES = (
     ("stream", 0, 0),
+    ("stream", 1, 0),
+    ("stream", 2, 0),
+    ("stream", 3, 0),
     ("stream", 0, 8),
     ("stream", 0, 16),
     ("stream", 0, 32),

@@ -214,6 +214,7 @@ struct Handle {
     BulkPlan plan{};
     int stencil_mode = 0;  // kModeSimple / kModeStream / kModeBulk / kModeVec
     int vec_variant = 0;   // vector width x register cap of the vec kernels
+    int stream_variant = 0;  // register cap of the stream kernels
     int fused_variant = 0; // kernel form of the fused step (stencil_fused.cu)
     StreamPlan splan{};
     DevBuf status;
@@ -580,8 +581,8 @@ void plan_stencil(Handle& H) {
         const int occ = H.prec == 4 ? fused_occupancy<float>(v) : fused_occupancy<double>(v);
         H.splan = plan_fused(H.g, sms, occ, H.B, fused_tj_of(v));
     } else if (H.stencil_mode == kModeStream) {
-        const int occ = H.prec == 4 ? stream_occupancy<float>(H.B, H.coef_kind)
-                                    : stream_occupancy<double>(H.B, H.coef_kind);
+        const int occ = H.prec == 4 ? stream_occupancy<float>(H.B, H.coef_kind, H.stream_variant)
+                                    : stream_occupancy<double>(H.B, H.coef_kind, H.stream_variant);
         H.splan = plan_stream(H.g, sms, occ, H.B);
     } else {
         const int occ = H.prec == 4 ? vec_occupancy<float>(H.vec_variant, H.coef_kind)
@@ -601,7 +602,7 @@ void launch_half(Handle& H, int which) {
     if (H.disp[which].present()) sa.nfaces = 0;
     switch (H.stencil_mode) {
         case kModeStream:
-            launch_stream_half<T>(sa, H.splan, which, H.stream);
+            launch_stream_half<T>(sa, H.splan, H.stream_variant, which, H.stream);
             break;
         case kModeVec:
             launch_vec_half<T>(sa, H.splan, H.vec_variant, which, H.stream);
@@ -1318,6 +1319,8 @@ int fitb_configure_stencil(fitb_handle* h, int32_t kind, int32_t variant, int32_
         fail(FITB_ERR_STATE, "compact coefficient storage needs the stream or vec stencil kernels");
     if ((kind == fitb::kModeStream || kind == fitb::kModeVec) && !fitb::stream_batch_supported(H.B))
         fail(FITB_ERR_ARG, "the stream / vec kernels take 1, 2, 4, 8 or 16 field sets, not %d", H.B);
+    if (kind == fitb::kModeStream && !fitb::stream_variant_supported(H.B, variant))
+        fail(FITB_ERR_ARG, "stream stencil: variant %d / batch %d", variant, H.B);
     if (kind == fitb::kModeVec && (H.B > 8 || variant < 0 || variant > 3))
         fail(FITB_ERR_ARG, "vec stencil: variant %d / batch %d", variant, H.B);
     if (kind == fitb::kModeFused) {
@@ -1357,6 +1360,7 @@ int fitb_configure_stencil(fitb_handle* h, int32_t kind, int32_t variant, int32_
         H.cur = 0;
     }
     if (kind == fitb::kModeVec) H.vec_variant = variant;
+    if (kind == fitb::kModeStream) H.stream_variant = compact ? 0 : variant;
     H.stencil_mode = kind;
     fitb::plan_stencil(H);
     if (ichunk > 0) {
@@ -1394,7 +1398,10 @@ int fitb_get_stencil(fitb_handle* h, int32_t* out) {
     const bool planned = H.stencil_mode == fitb::kModeStream || H.stencil_mode == fitb::kModeVec ||
                          H.stencil_mode == fitb::kModeFused;
     out[0] = H.stencil_mode;
-    out[1] = H.stencil_mode == fitb::kModeVec ? H.vec_variant : (H.stencil_mode == fitb::kModeFused ? H.fused_variant : 0);
+    out[1] = H.stencil_mode == fitb::kModeVec     ? H.vec_variant
+             : H.stencil_mode == fitb::kModeFused ? H.fused_variant
+             : H.stencil_mode == fitb::kModeStream ? H.stream_variant
+                                                   : 0;
     out[2] = planned ? H.splan.ichunk : (H.stencil_mode == fitb::kModeBulk ? H.plan.ichunk : H.ichunk);
     out[3] = planned ? H.splan.grid_x : 0;
     out[4] = planned ? H.splan.grid_y : 0;

@@ -101,12 +101,14 @@ struct StreamPlan {
     int block_y;  // warp rows per CTA (grid rows x field sets)
 };
 bool stream_batch_supported(int B);
+// variant: register cap (0 natural, 1-3 capped; 2, 3 need B <= 8)
+bool stream_variant_supported(int B, int variant);
 template <typename T>
-int stream_occupancy(int B, int coef_kind);
+int stream_occupancy(int B, int coef_kind, int variant);
 StreamPlan plan_stream(const Geom& g, int sm_count, int ctas_per_sm, int B);
 // which: 0 = E update, 1 = H update
 template <typename T>
-void launch_stream_half(StencilArgs<T> a, const StreamPlan& sp, int which, cudaStream_t s);
+void launch_stream_half(StencilArgs<T> a, const StreamPlan& sp, int variant, int which, cudaStream_t s);
 
 // Vectorised stencil over flattened padded planes, batched like the stream
 // kernels (B <= 8); grid_y = 1 and block_y is the CTA's warp count.

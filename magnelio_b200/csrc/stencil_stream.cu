@@ -264,8 +264,10 @@ __device__ __forceinline__ unsigned faces_i(const StencilArgs<T>& p, int i) {
 // coefficients, which the first of them brings from HBM and the others find
 // in L1/L2, so the coefficients cross HBM once per cell for all field sets
 // while every thread keeps a full plane of loads in flight.
-template <typename T, int CK>
-__global__ void __launch_bounds__(512) k_update_E_stream(const StencilArgs<T> p) {
+// MAXT / MINB: launch bounds of the register-capped variants (see
+// stream_dispatch below).
+template <typename T, int CK, int MAXT = 512, int MINB = 1>
+__global__ void __launch_bounds__(MAXT, MINB) k_update_E_stream(const StencilArgs<T> p) {
     const Geom& g = p.g;
     const int B = p.B;
     const int b = threadIdx.y % B;
@@ -299,8 +301,8 @@ __global__ void __launch_bounds__(512) k_update_E_stream(const StencilArgs<T> p)
     }
 }
 
-template <typename T, int CK>
-__global__ void __launch_bounds__(512) k_update_H_stream(const StencilArgs<T> p) {
+template <typename T, int CK, int MAXT = 512, int MINB = 1>
+__global__ void __launch_bounds__(MAXT, MINB) k_update_H_stream(const StencilArgs<T> p) {
     const Geom& g = p.g;
     const int B = p.B;
     const int b = threadIdx.y % B;
@@ -337,29 +339,67 @@ __global__ void __launch_bounds__(512) k_update_H_stream(const StencilArgs<T> p)
 
 int block_rows_y(int B) { return B <= 8 ? 8 : B; }
 
+// Register-capped variants of the native-coefficient kernels (more warps
+// resident per SM; the kernels are DRAM-latency bound):
+//   0: __launch_bounds__(512, 2): <= 64 registers (the default: four CTAs
+//      of 256 per SM, no spills);
+//   1: natural allocation (72-80 registers in float32, fewer CTAs);
+//   2: __launch_bounds__(256, 5): <= 48 registers, blocks of 256 only;
+//   3: __launch_bounds__(256, 6): <= 40 registers, blocks of 256 only.
+template <typename T, typename F>
+void stream_dispatch(int variant, int coef_kind, F&& f) {
+    if (coef_kind == kCoefF16) return f.template run<kCoefF16, 512, 1>();
+    if (coef_kind == kCoefBF16) return f.template run<kCoefBF16, 512, 1>();
+    switch (variant) {
+        case 1: return f.template run<kCoefNative, 512, 1>();
+        case 2: return f.template run<kCoefNative, 256, 5>();
+        case 3: return f.template run<kCoefNative, 256, 6>();
+        default: return f.template run<kCoefNative, 512, 2>();
+    }
+}
+
+template <typename T>
+struct StreamOcc {
+    int threads, a = 0, c = 0;
+    template <int CK, int MAXT, int MINB>
+    void run() {
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_update_E_stream<T, CK, MAXT, MINB>, threads, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, k_update_H_stream<T, CK, MAXT, MINB>, threads, 0);
+    }
+};
+
+template <typename T>
+struct StreamLaunch {
+    const StencilArgs<T>& a;
+    dim3 grid, block;
+    int which;
+    cudaStream_t s;
+    template <int CK, int MAXT, int MINB>
+    void run() {
+        if (which == 0)
+            k_update_E_stream<T, CK, MAXT, MINB><<<grid, block, 0, s>>>(a);
+        else
+            k_update_H_stream<T, CK, MAXT, MINB><<<grid, block, 0, s>>>(a);
+    }
+};
+
 }  // namespace
 
 bool stream_batch_supported(int B) { return B == 1 || B == 2 || B == 4 || B == 8 || B == 16; }
 
+bool stream_variant_supported(int B, int variant) {
+    return variant == 0 || variant == 1 || ((variant == 2 || variant == 3) && B <= 8);
+}
+
 template <typename T>
-int stream_occupancy(int B, int coef_kind) {
-    int a = 0, c = 0;
-    const int threads = kSX * block_rows_y(B);
-    if (coef_kind == kCoefF16) {
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_update_E_stream<T, kCoefF16>, threads, 0);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, k_update_H_stream<T, kCoefF16>, threads, 0);
-    } else if (coef_kind == kCoefBF16) {
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_update_E_stream<T, kCoefBF16>, threads, 0);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, k_update_H_stream<T, kCoefBF16>, threads, 0);
-    } else {
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_update_E_stream<T, kCoefNative>, threads, 0);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, k_update_H_stream<T, kCoefNative>, threads, 0);
-    }
-    const int m = a < c ? a : c;
+int stream_occupancy(int B, int coef_kind, int variant) {
+    StreamOcc<T> f{kSX * block_rows_y(B)};
+    stream_dispatch<T>(variant, coef_kind, f);
+    const int m = f.a < f.c ? f.a : f.c;
     return m < 1 ? 1 : m;
 }
-template int stream_occupancy<float>(int, int);
-template int stream_occupancy<double>(int, int);
+template int stream_occupancy<float>(int, int, int);
+template int stream_occupancy<double>(int, int, int);
 
 StreamPlan plan_stream(const Geom& g, int sm_count, int ctas_per_sm, int B) {
     StreamPlan s{};
@@ -390,21 +430,14 @@ StreamPlan plan_stream(const Geom& g, int sm_count, int ctas_per_sm, int B) {
 }
 
 template <typename T>
-void launch_stream_half(StencilArgs<T> a, const StreamPlan& sp, int which, cudaStream_t s) {
+void launch_stream_half(StencilArgs<T> a, const StreamPlan& sp, int variant, int which, cudaStream_t s) {
     a.ichunk = sp.ichunk;
-    const dim3 grid(sp.grid_x, sp.grid_y, sp.grid_z), block(kSX, sp.block_y, 1);
-    switch (a.coef_kind * 2 + which) {
-        case 2 * kCoefF16: k_update_E_stream<T, kCoefF16><<<grid, block, 0, s>>>(a); break;
-        case 2 * kCoefF16 + 1: k_update_H_stream<T, kCoefF16><<<grid, block, 0, s>>>(a); break;
-        case 2 * kCoefBF16: k_update_E_stream<T, kCoefBF16><<<grid, block, 0, s>>>(a); break;
-        case 2 * kCoefBF16 + 1: k_update_H_stream<T, kCoefBF16><<<grid, block, 0, s>>>(a); break;
-        case 1: k_update_H_stream<T, kCoefNative><<<grid, block, 0, s>>>(a); break;
-        default: k_update_E_stream<T, kCoefNative><<<grid, block, 0, s>>>(a); break;
-    }
+    StreamLaunch<T> f{a, dim3(sp.grid_x, sp.grid_y, sp.grid_z), dim3(kSX, sp.block_y, 1), which, s};
+    stream_dispatch<T>(variant, a.coef_kind, f);
 }
 
-template void launch_stream_half<float>(StencilArgs<float>, const StreamPlan&, int, cudaStream_t);
-template void launch_stream_half<double>(StencilArgs<double>, const StreamPlan&, int, cudaStream_t);
+template void launch_stream_half<float>(StencilArgs<float>, const StreamPlan&, int, int, cudaStream_t);
+template void launch_stream_half<double>(StencilArgs<double>, const StreamPlan&, int, int, cudaStream_t);
 
 }  // namespace fitb
 

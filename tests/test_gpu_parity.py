@@ -107,20 +107,18 @@ def test_graph_chunks_and_single_steps_agree(name):
 
 
 @pytest.mark.parametrize("name", ["cpml_box", "lumped_dft"])
-def test_stencil_variants_agree(name, monkeypatch):
-    """The software-pipelined stencil, the vectorised-plane stencil (each
-    vector width and register cap), the bulk-copy pipeline and the simple
-    kernel run the same arithmetic."""
+def test_stencil_variants_agree(name):
+    """Every stencil form and variant (stream with each register cap, bulk
+    copy pipeline, simple, vectorised planes, fused E+H step) runs the same
+    arithmetic."""
     p, d, n = load_golden(name)
     outs = []
-    modes = [("stream", None), ("bulk", None), ("simple", None)] + [("vec", str(v)) for v in range(4)]
-    modes += [("fused", str(v)) for v in range(7)]
-    for mode, variant in modes:
-        monkeypatch.setenv("FITB_STENCIL", mode)
-        if variant is not None:
-            monkeypatch.setenv("FITB_VEC_VARIANT", variant)
-            monkeypatch.setenv("FITB_FUSED_VARIANT", variant)
+    modes = [("stream", v) for v in range(4)] + [("bulk", 0), ("simple", 0)]
+    modes += [("vec", v) for v in range(4)] + [("fused", v) for v in range(7)]
+    for kind, variant in modes:
         with p.build_engine("single") as eng:
+            eng.configure_stencil(kind, variant)
+            assert eng.stencil_config()["kind"] == kind
             eng.step(n)
             outs.append(eng.read_fields())
     pe, ph = _peaks(name)
