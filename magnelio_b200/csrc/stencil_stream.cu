@@ -348,8 +348,8 @@ int block_rows_y(int B) { return B <= 8 ? 8 : B; }
 //   3: __launch_bounds__(256, 6): <= 40 registers, blocks of 256 only.
 template <typename T, typename F>
 void stream_dispatch(int variant, int coef_kind, F&& f) {
-    if (coef_kind == kCoefF16) return f.template run<kCoefF16, 512, 1>();
-    if (coef_kind == kCoefBF16) return f.template run<kCoefBF16, 512, 1>();
+    if (coef_kind == kCoefF16) return f.template run<kCoefF16, 512, 2>();
+    if (coef_kind == kCoefBF16) return f.template run<kCoefBF16, 512, 2>();
     switch (variant) {
         case 1: return f.template run<kCoefNative, 512, 1>();
         case 2: return f.template run<kCoefNative, 256, 5>();
