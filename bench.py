@@ -200,6 +200,11 @@ def main() -> int:
     ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of CPU-port timing")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="skip the autotuner (keep the default stencil plan)")
+    ap.add_argument("--workload", choices=("brick_box", "slab"), default="brick_box",
+                    help="brick_box (plain method at scale) or slab (dispersive slab, TF/SF plane wave, 384x384x192)")
+    ap.add_argument("--precision-study", action="store_true",
+                    help="R/T of the slab workload per precision variant against its float64 run")
+    ap.add_argument("--study-size", type=int, nargs=3, default=(96, 96, 128))
     ap.add_argument("--serving", action="store_true",
                     help="serve the S-parameter request stream (batched and one excitation at a time) instead")
     ap.add_argument("--serving-requests", type=int, default=256)
@@ -224,6 +229,10 @@ def main() -> int:
             return run_reference(args, world, rank, local)
         if args.serving:
             return run_serving(args, world, rank, local)
+        if args.precision_study:
+            return run_precision_study(args, world, rank, local)
+        if args.workload == "slab":
+            return run_slab(args, world, rank, local)
         return run_b200(args, world, rank, local)
     finally:
         if world > 1:
@@ -257,6 +266,96 @@ def run_serving(args, world, rank, local):
             "p50_s": batched.p50, "p99_s": batched.p99, "wall_s": batched.wall,
             "mean_active": batched.mean_active, "peak_device_bytes": batched.peak_bytes,
             "plain": plain.summary(), "ratio_vs_plain": batched.solves_per_s / max(plain.solves_per_s, 1e-12),
+        }
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_precision_study(args, world, rank, local):
+    """Slab reflection / transmission per precision variant (float32 fields
+    with float32, float16 or bfloat16 coefficients, Kahan-compensated DFT
+    bins or not) against the float64 run of the same problem."""
+    from magnelio_b200 import precision
+
+    nx, ny, nz = args.study_size
+    res = precision.precision_study(nx, ny, nz, args.steps, device=local)
+    if rank == 0:
+        line = {"metric": "slab R/T deviation from float64", "unit": "linear |dT|, |dR|; degrees",
+                "higher_is_better": False, "n_gpus": world, "steps": args.steps,
+                "config": {"workload": f"dispersive_slab_{nx}x{ny}x{nz}", "poles": "2 Lorentz pairs, 8 and 14 GHz",
+                           "source": "TF/SF Gaussian plane wave +z, f_max 20 GHz", "band": "1-20 GHz, 64 freqs"},
+                "variants": {k: {m: v[m] for m in ("dR", "dT", "dT_phase_deg")} for k, v in res.items()
+                             if k != "freqs"}}
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_slab(args, world, rank, local):
+    """The precision configuration's workload at full size: 384 x 384 x 192
+    cells, two-pole Lorentz slab (ADE on device), TF/SF plane wave, CPML on
+    six faces (separate passes after the ADE update), two DFT planes."""
+    from magnelio_b200 import autotune, workloads
+
+    nx, ny, nz = 384, 384, 192
+    prob = workloads.dispersive_slab(nx, ny, nz)
+    tuned = None
+    if not args.no_tune:
+        tuned = autotune.tune_problem(prob, "single", device=local, coef=args.coef, iters=5)
+    eng = prob.build_engine("single", device=local)
+    if args.coef != "native":
+        eng.set_coefficient_storage(args.coef)
+    if tuned is not None:
+        autotune.apply(eng, tuned)
+    stencil_cfg = eng.stencil_config()
+    cells = nx * ny * nz
+    eng.step(args.warmup)
+    eng.sync()
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+    sampler = ClockSampler(local)
+    l0 = eng.launch_count
+    ms = eng.step_timed(args.steps)
+    launches = eng.launch_count - l0
+    clocks = sampler.stop()
+    ms = _max_over_ranks(ms, world, local)
+    value = cells * args.steps * world / (ms * 1e-3) / 1e9
+    # end to end through the public API: one fitb_step per step, the
+    # transmission plane's bins read back at the end
+    eng.sync()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        eng.step(1)
+    bins = eng.read_dft(1, "Ex")
+    e2e_s = _max_over_ranks(time.perf_counter() - t0, world, local)
+    e2e = cells * args.steps * world / e2e_s / 1e9
+    t_e, t_h = eng.time_stencil(20)
+    coef_bytes = COEF_BYTES_PER_CELL if args.coef == "native" else COEF_BYTES_PER_CELL // 2
+    # stencil launches without their CPML (it runs as passes after the ADE update)
+    alg_bytes = (FIELD_BYTES_PER_CELL + coef_bytes) * cells
+    achieved = alg_bytes / ((t_e + t_h) * 1e-3) / 1e9
+    peak, peak_kind = _peaks()
+    eng.close()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded dispersive slab, host-built setup)",
+            "config": {"workload": f"dispersive_slab_{nx}x{ny}x{nz}", "cpml": "10 layers x 6 faces",
+                       "dispersion": f"2 Lorentz pairs, {sum(b.idx.size for d in prob.dispersion for b in d.blocks)} states",
+                       "source": "TF/SF Gaussian plane wave +z, f_max 20 GHz",
+                       "monitors": "2 E-field DFT planes x 64 freq, every step",
+                       "stencil": stencil_cfg, "l2": "inputs larger than L2"},
+            "roofline": {"bound": "hbm", "kernel": "update_E + update_H (one stencil step, no CPML)",
+                         "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None, "algorithmic_bytes": alg_bytes, "ms_E": t_e,
+                         "ms_H": t_h, "step_share": (t_e + t_h) / (ms / args.steps)},
+            "cpu_baseline": None,
+            "e2e": {"value": e2e, "unit": METRIC, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": int(bins.size * 8 / args.steps),
+                    "how": "one fitb_step per step, the transmission plane's bins read back at the end"},
+            "gpu_launches": launches, "clocks": clocks,
         }
         print(json.dumps(line), flush=True)
     return 0

@@ -132,6 +132,7 @@ class DftMonitor:
     components: tuple
     freqs: np.ndarray
     stride: int = 1
+    kahan: bool = True  # compensated float32 bins
 
 
 @dataclass
@@ -204,7 +205,8 @@ class FitProblem:
                     if v is not None and len(v):
                         eng.set_lumped_source(lid, b, v)
             for mon in self.monitors:
-                eng.add_dft_monitor(mon.box, mon.components, mon.freqs, self.dx, self.dy, self.dz, stride=mon.stride)
+                eng.add_dft_monitor(mon.box, mon.components, mon.freqs, self.dx, self.dy, self.dz, stride=mon.stride,
+                                    kahan=getattr(mon, "kahan", True))
             for dsp in self.dispersion:
                 for bl in dsp.blocks:
                     eng.add_dispersion_block(dsp.side, bl)
@@ -277,6 +279,7 @@ class FitProblem:
             put(f"mon{q}.comps", np.array([["Ex", "Ey", "Ez", "Hx", "Hy", "Hz"].index(c) for c in mon.components]))
             put(f"mon{q}.freqs", mon.freqs)
             put(f"mon{q}.stride", mon.stride)
+            put(f"mon{q}.kahan", int(getattr(mon, "kahan", True)))
         put("n_disp", len(self.dispersion))
         for q, dsp in enumerate(self.dispersion):
             put(f"disp{q}.side", ["E", "H"].index(dsp.side))
@@ -346,7 +349,8 @@ class FitProblem:
         for q in range(int(g("n_mon", 0))):
             box = g(f"mon{q}.box")
             comps = tuple(["Ex", "Ey", "Ez", "Hx", "Hy", "Hz"][int(c)] for c in g(f"mon{q}.comps"))
-            p.monitors.append(DftMonitor(tuple(tuple(int(v) for v in r) for r in box), comps, g(f"mon{q}.freqs"), int(g(f"mon{q}.stride"))))
+            p.monitors.append(DftMonitor(tuple(tuple(int(v) for v in r) for r in box), comps, g(f"mon{q}.freqs"),
+                                         int(g(f"mon{q}.stride")), bool(int(g(f"mon{q}.kahan", 1)))))
         for q in range(int(g("n_disp", 0))):
             dsp = Dispersion(side=["E", "H"][int(g(f"disp{q}.side"))])
             for r in range(int(g(f"disp{q}.n_blocks"))):

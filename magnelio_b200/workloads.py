@@ -17,7 +17,7 @@ import math
 import numpy as np
 
 from magnelio_b200 import host
-from magnelio_b200.problem import CpmlFace, DftMonitor, FitProblem, LumpedPort
+from magnelio_b200.problem import CpmlFace, DftMonitor, Dispersion, FitProblem, LumpedPort
 
 FACES = ("xmin", "xmax", "ymin", "ymax", "zmin", "zmax")
 
@@ -239,3 +239,82 @@ def s_matrix(V, I, dt: float, freqs, z0: float = 50.0, n_ports: int | None = Non
         bw = (Vf - z0 * If) / (2 * rz)
         S[:, :, i] = bw / a[:, i:i + 1]
     return S
+
+
+# ---------------------------------------------------------------------------
+# Precision workload: dispersive slab, TF/SF plane wave
+# ---------------------------------------------------------------------------
+def dispersive_slab(nx: int = 384, ny: int = 384, nz: int = 192, seed: int = 2028, h: float | None = None,
+                    cpml_cells: int = 10, f_min: float = 1.0e9, f_max: float = 20.0e9, n_freq: int = 64,
+                    slab: bool = True, kahan: bool = True) -> FitProblem:
+    """A dispersive slab in a CPML box excited by a TF/SF plane wave at
+    normal incidence: uniform cells ``h`` (default 20 per vacuum wavelength
+    at ``f_max``), CPML on all six faces, a slab over the x-y section up to
+    one cell short of the absorber and ``z in [0.45, 0.6] L`` (a dispersive
+    region inside the CPML grows without bound under the reference's
+    ordering of the ADE update before the CPML correction, reference run and
+    this engine alike) of a two-pole Lorentz material (eps_inf = 2.2,
+    resonances at 8 and 14 GHz with damping ``U[0.05, 0.2] omega0`` and
+    strengths from the seed such that ``eps(0) in [4, 6]``), a Gaussian plane
+    wave along +z polarised along x (``f_max``), and two E-field DFT planes
+    over the central part of the section: one in the scattered-field region
+    before the slab (reflection) and one in the total-field region after it
+    (transmission).  ``slab=False`` builds the same box empty (the incident
+    field)."""
+    rng = np.random.default_rng(seed)
+    h = h if h is not None else host.C0 / f_max / 20.0
+    x, y, z = (np.linspace(0.0, n * h, n + 1) for n in (nx, ny, nz))
+    de_total = float(rng.uniform(1.8, 3.8))
+    split = float(rng.uniform(0.3, 0.7))
+    w1, w2 = 2 * math.pi * 8e9, 2 * math.pi * 14e9
+    poles = (host.lorentz_poles(de_total * split, w1, float(rng.uniform(0.05, 0.2)) * w1)
+             + host.lorentz_poles(de_total * (1.0 - split), w2, float(rng.uniform(0.05, 0.2)) * w2))
+    L = (x[-1], y[-1], z[-1])
+    if slab:
+        lo = (cpml_cells + 1) * h
+        mat_id = host.assign_bricks(x, y, z, [((lo, lo, 0.45 * L[2]), (L[0] - lo, L[1] - lo, 0.6 * L[2]))])
+    else:
+        mat_id = np.zeros((nx, ny, nz), np.int32)
+    M_eps = host.build_M_eps(x, y, z, [1.0, 2.2], mat_id)
+    M_mu = host.build_M_mu(x, y, z)
+    dt = host.courant_dt(x, y, z, "normal")
+    blocks, W = host.dispersion_blocks(x, y, z, mat_id, {1: poles}, dt, "E") if slab else ([], None)
+    aE, bE, aH, bH = host.leapfrog_coefficients(M_eps, M_mu, dt, W_E=W)
+    prob = FitProblem(nx=nx, ny=ny, nz=nz, dt=dt, dx=np.diff(x), dy=np.diff(y), dz=np.diff(z),
+                      alpha_E=aE, beta_E=bE, alpha_H=aH, beta_H=bH, M_eps=M_eps, M_mu=M_mu)
+    for face in FACES:
+        d = np.diff({"x": x, "y": y, "z": z}[face[0]])
+        b, c, ckt = host.cpml_tables(d, face, dt, thickness_cells=cpml_cells)
+        prob.cpml.append(CpmlFace(face, b, c, ckt))
+    if blocks:
+        prob.dispersion.append(Dispersion(side="E", blocks=blocks))
+    inset = (cpml_cells + 2) * h
+    zin = (cpml_cells + 4) * h
+    corners = ((inset, inset, zin), (L[0] - inset, L[1] - inset, L[2] - zin))
+    prob.plane_waves.append(host.plane_wave(x, y, z, bE, bH, (0.0, 0.0, 1.0), (1.0, 0.0, 0.0), amplitude=1.0,
+                                            waveform="gaussian", f_max=f_max, corners=corners))
+    iz0 = host.snap_tfsf_box(x, y, z, corners)[4]
+    c0 = cpml_cells + 4
+    box_xy = ((c0, nx - c0), (c0, ny - c0))
+    freqs = np.linspace(f_min, f_max, n_freq)
+    k_before = iz0 - 2
+    k_after = int(round(0.8 * nz))
+    for k in (k_before, k_after):
+        prob.monitors.append(DftMonitor((box_xy[0], box_xy[1], (k, k + 1)), ("Ex",), freqs, 1, kahan))
+    prob.e0 = [None]
+    prob.h0 = [None]
+    return prob
+
+
+def slab_response(bins_slab, bins_vac, band: float = 1e-2):
+    """Reflection and transmission of the slab workload from its two DFT
+    planes, averaged over the monitored section: ``R = E_before(slab) /
+    E_after(empty)``, ``T = E_after(slab) / E_after(empty)``; bins where the
+    incident spectrum is below ``band`` of its peak are NaN."""
+    before_s, after_s = (np.mean(b, axis=(1, 2, 3)) for b in bins_slab)
+    _before_v, after_v = (np.mean(b, axis=(1, 2, 3)) for b in bins_vac)
+    ok = np.abs(after_v) >= band * np.max(np.abs(after_v))
+    safe = np.where(ok, after_v, 1.0)
+    R = np.where(ok, before_s / safe, np.nan)
+    T = np.where(ok, after_s / safe, np.nan)
+    return R, T

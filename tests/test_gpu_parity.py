@@ -464,3 +464,42 @@ def test_wr90_six_excitations_batched_match_the_reference_s_matrix(precision):
         # after 8000 steps only the DTBC residual is left in the guide: the
         # final fields are compared where float64 resolves them
         assert _rel(e, d["out.e"]) < WR90_VI_TOL[precision]
+
+
+@pytest.mark.parametrize("precision,tol", [("double", F64_TOL), ("single", F32_TOL)])
+def test_slab_workload_built_on_the_host_matches_the_oracle(precision, tol):
+    """The precision workload (Lorentz ADE slab through the CPML, TF/SF plane
+    wave, DFT planes) set up by this package's host code alone: device march
+    vs the float64 oracle on the same inputs."""
+    from oracle.fit_oracle import OracleRun
+    from magnelio_b200 import workloads
+
+    p = workloads.dispersive_slab(24, 24, 40, cpml_cells=5, n_freq=8)
+    n = 260
+    ref = OracleRun(p).run(n)
+    with p.build_engine(precision) as eng:
+        eng.step(n)
+        e, h = eng.read_fields()
+        bins = [eng.read_dft(q, "Ex") for q in range(len(p.monitors))]
+    assert _rel(e, ref.f.e, ref.peak_e) < tol
+    assert _rel(h, ref.f.h, ref.peak_h) < tol
+    for q, m in enumerate(ref.mons):
+        assert _rel(bins[q], m.bins["Ex"]) < max(5 * tol, DFT_TOL)
+
+
+# float32 variants of the slab against its float64 run: reflection and
+# transmission over the excited band (linear), transmission phase (degrees).
+# float16 coefficients stay inside the |dS| <= 1e-3 / 0.1 degree budget,
+# bfloat16 coefficients do not (8-bit significand).
+SLAB_TOL = {"fp32": (1e-5, 1e-3), "fp32-no-kahan": (1e-5, 1e-3), "fp32-f16-coef": (1e-3, 0.1),
+            "fp32-bf16-coef": (5e-2, 2.0)}
+
+
+def test_slab_precision_variants():
+    from magnelio_b200 import precision
+
+    res = precision.precision_study(40, 40, 64, 900, cpml_cells=6, n_freq=16)
+    for name, (tol, ptol) in SLAB_TOL.items():
+        r = res[name]
+        print(f"{name}: dR {r['dR']:.3g} dT {r['dT']:.3g} phase {r['dT_phase_deg']:.3g} deg")
+        assert r["dT"] <= tol and r["dR"] <= tol and r["dT_phase_deg"] <= ptol, name
