@@ -200,8 +200,9 @@ def main() -> int:
     ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of CPU-port timing")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="skip the autotuner (keep the default stencil plan)")
-    ap.add_argument("--workload", choices=("brick_box", "slab"), default="brick_box",
-                    help="brick_box (plain method at scale) or slab (dispersive slab, TF/SF plane wave, 384x384x192)")
+    ap.add_argument("--workload", choices=("brick_box", "slab", "cross"), default="brick_box",
+                    help="brick_box (plain method at scale), slab (dispersive slab, TF/SF plane wave, 384x384x192) "
+                         "or cross (four-port junction, eight excitations batched vs one at a time)")
     ap.add_argument("--precision-study", action="store_true",
                     help="R/T of the slab workload per precision variant against its float64 run")
     ap.add_argument("--study-size", type=int, nargs=3, default=(96, 96, 128))
@@ -233,6 +234,8 @@ def main() -> int:
             return run_precision_study(args, world, rank, local)
         if args.workload == "slab":
             return run_slab(args, world, rank, local)
+        if args.workload == "cross":
+            return run_cross(args, world, rank, local)
         return run_b200(args, world, rank, local)
     finally:
         if world > 1:
@@ -286,6 +289,57 @@ def run_precision_study(args, world, rank, local):
                            "source": "TF/SF Gaussian plane wave +z, f_max 20 GHz", "band": "1-20 GHz, 64 freqs"},
                 "variants": {k: {m: v[m] for m in ("dR", "dT", "dT_phase_deg")} for k, v in res.items()
                              if k != "freqs"}}
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_cross(args, world, rank, local):
+    """Batching configuration: WR-90 cross junction (200 x 200 x 40 cells,
+    PEC corner blocks, 4 waveguide ports x 2 DTBC modes), the eight port x
+    mode excitations for the full 12000 steps as one batch of eight field
+    sets, then the same eight one at a time; device time of each.  The
+    problem (port modes, DTBC kernels, waveforms) was set up by the
+    reference's own analysis and is stored with the tests."""
+    sys.path.insert(0, str(ROOT / "tests"))
+    from conftest import load_golden
+
+    prob, _d, n_full = load_golden("cfg3_cross_full")
+    steps = n_full if args.steps >= n_full else args.steps
+    cells = prob.nx * prob.ny * prob.nz
+    n_exc = prob.batch
+    eng = prob.build_engine("single", device=local)
+    eng.step(args.warmup)
+    eng.close()
+    eng = prob.build_engine("single", device=local)
+    ms_batched = eng.step_timed(steps)
+    stencil_cfg = eng.stencil_config()
+    eng.close()
+    ms_seq = 0.0
+    for b in range(n_exc):
+        q = load_golden("cfg3_cross_full")[0]
+        q.batch = 1
+        for mp in q.modal:
+            mp.excitation = [mp.excitation[b]]
+        q.e0, q.h0 = [None], [None]
+        e1 = q.build_engine("single", device=local)
+        ms_seq += e1.step_timed(steps)
+        e1.close()
+    ms_batched = _max_over_ranks(ms_batched, world, local)
+    ms_seq = _max_over_ranks(ms_seq, world, local)
+    solve_steps = n_full
+    if rank == 0:
+        line = {
+            "metric": "batched S-param solves/s", "unit": "solves/s", "n_gpus": world, "steps": steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "reference-built port setup (stored), eight DTBC excitations",
+            "value": world * 1e3 / (ms_batched / steps * solve_steps),
+            "gcell_updates_per_s": cells * n_exc * steps * world / (ms_batched * 1e-3) / 1e9,
+            "sequential": {"solves_per_s": world * 1e3 / (ms_seq / steps * solve_steps),
+                           "gcell_updates_per_s": cells * n_exc * steps * world / (ms_seq * 1e-3) / 1e9},
+            "ratio_vs_sequential": ms_seq / ms_batched,
+            "config": {"workload": f"cross_junction_{prob.nx}x{prob.ny}x{prob.nz}", "field_sets": n_exc,
+                       "solve": f"all {n_exc} excitations x {solve_steps} steps", "stencil": stencil_cfg},
+        }
         print(json.dumps(line), flush=True)
     return 0
 

@@ -431,6 +431,85 @@ def case_cfg1_wr90():
     _save("cfg1_wr90", prob, out, n, "WR-90 29x13x51, 2 ports x 3 modes, six excitations, 8000 steps, 501-point S")
 
 
+def _cross_junction(nxy, nz, arm=60e-3, a=22.86e-3, b=10.16e-3):
+    """Cross junction of two WR-90 guides in the x-y plane: a square of
+    2 arm + a, height b; PEC blocks fill the four corners; the four arm
+    ends are port faces (PMC outside the windows, as the port faces of the
+    reference's own waveguide examples), the top and bottom walls PEC."""
+    from magnelio.materials.material import Material
+    from magnelio.mesh.grid import GridLines
+    from magnelio.mesh.mesher import Mesh
+    from magnelio.ports.declarative import PortWaveguide
+
+    W = 2 * arm + a
+    grid = GridLines(x=np.linspace(0, W, nxy + 1), y=np.linspace(0, W, nxy + 1), z=np.linspace(0, b, nz + 1))
+    pec = Material(name="metal", is_pec=True)
+    lo, hi = arm, arm + a
+    regions = [(pec, (0.0, 0.0, 0.0, lo, lo, b)), (pec, (hi, 0.0, 0.0, W, lo, b)),
+               (pec, (0.0, hi, 0.0, lo, W, b)), (pec, (hi, hi, 0.0, W, W, b))]
+    mesh = Mesh.from_grid(grid, regions=regions, boundary_conditions={
+        "xmin": "PMC", "xmax": "PMC", "ymin": "PMC", "ymax": "PMC", "zmin": "PEC", "zmax": "PEC"})
+    ports = [PortWaveguide("p1", "xmin", corners=((None, lo, 0.0), (None, hi, b)), n_modes=2),
+             PortWaveguide("p2", "xmax", corners=((None, lo, 0.0), (None, hi, b)), n_modes=2),
+             PortWaveguide("p3", "ymin", corners=((lo, None, 0.0), (hi, None, b)), n_modes=2),
+             PortWaveguide("p4", "ymax", corners=((lo, None, 0.0), (hi, None, b)), n_modes=2)]
+    return mesh, ports
+
+
+def _cross_problem(mesh, ports, n, f_max, run):
+    """Batched problem of all eight port x mode excitations (field set b =
+    excitation b) and, with ``run``, the reference's V/I per excitation."""
+    import magnelio.analysis.scattering_td as std
+    from magnelio._operators.material_matrices import build_M_eps, build_M_mu
+    from magnelio.solver.fit_td import FITTimeDomainSolver
+    from magnelio.solver.stability import spectral_dt
+
+    an = std.AnalysisScatteringTD(mesh=mesh, f_max=f_max, ports=ports, verbose=False, backend="numpy",
+                                  precision="double", n_freq=11)
+    m_eps, m_mu = build_M_eps(mesh), build_M_mu(mesh)
+    dt = spectral_dt(mesh, "normal", m_eps=m_eps, m_mu=m_mu)
+    excs = [(pt.name, m) for pt in ports for m in range(pt.n_modes)]
+    probs, out = [], {}
+    for b, ex in enumerate(excs):
+        ops, el_ops, wf, n_est, rec, *_ = an._prepare_excitation_run(ex, None, m_eps, m_mu, dt, f_max)
+        s = FITTimeDomainSolver(mesh=mesh, boundary_conditions=an._resolve_bc(), ports=ops + el_ops, recorder=rec,
+                                total_time_steps=n, dt=dt, energy_stop_db=None, port_signal_stop_db=None,
+                                verbose=False, backend="numpy", precision="double")
+        s.setup()
+        pb = problem_from_solver(s, n)
+        probs.append(pb)
+        if run:
+            s.run()
+            o = _outputs(s, pb, {})
+            out[f"cross.V{b}"] = o["out.V"]
+            out[f"cross.I{b}"] = o["out.I"]
+    prob = probs[0]
+    prob.batch = len(excs)
+    for q, mp in enumerate(prob.modal):
+        mp.excitation = [pb.modal[q].excitation[0] for pb in probs]
+    prob.e0 = [None] * len(excs)
+    prob.h0 = [None] * len(excs)
+    return prob, out
+
+
+def case_cfg3_cross_small():
+    """The batching configuration at reduced resolution (52 x 52 x 8 cells,
+    1500 steps): reference V/I of all eight excitations."""
+    mesh, ports = _cross_junction(52, 8)
+    n = 1500
+    prob, out = _cross_problem(mesh, ports, n, 18e9, run=True)
+    _save("cfg3_cross_small", prob, out, n, "cross junction 52x52x8, 4 ports x 2 modes, eight excitations")
+
+
+def case_cfg3_cross_full():
+    """The batching configuration at full size (200 x 200 x 40 cells, 12000
+    steps): the batched engine problem only (no reference run)."""
+    mesh, ports = _cross_junction(200, 40)
+    n = 12000
+    prob, out = _cross_problem(mesh, ports, n, 25e9, run=False)
+    _save("cfg3_cross_full", prob, out, n, "cross junction 200x200x40, 4 ports x 2 modes, eight excitations")
+
+
 def case_wg_dtbc():
     """WR-90 section, two waveguide ports x 2 modes, exact DTBC on all
     channels, port p1 mode 0 excited."""
@@ -604,6 +683,8 @@ CASES = {
     "planewave_box": case_planewave_box,
     "dispersive_box": case_dispersive_box,
     "cfg1_wr90": case_cfg1_wr90,
+    "cfg3_cross_small": case_cfg3_cross_small,
+    "cfg3_cross_full": case_cfg3_cross_full,
     "mixed_box": case_mixed_box,
     "lumped_dft": case_lumped_dft,
     "wg_dtbc": case_wg_dtbc,

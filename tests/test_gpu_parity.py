@@ -503,3 +503,37 @@ def test_slab_precision_variants():
         r = res[name]
         print(f"{name}: dR {r['dR']:.3g} dT {r['dT']:.3g} phase {r['dT_phase_deg']:.3g} deg")
         assert r["dT"] <= tol and r["dR"] <= tol and r["dT_phase_deg"] <= ptol, name
+
+
+@pytest.mark.parametrize("precision,tol", [("double", 1e-8), ("single", F32_TOL)])
+def test_cross_junction_eight_excitations_in_one_batch(precision, tol):
+    """Batching configuration (reduced grid): the four-port junction's eight
+    port x mode excitations as one batch reproduce the reference's eight
+    separate runs (V/I relative to each run's peak)."""
+    p, d, n = load_golden("cfg3_cross_small")
+    with p.build_engine(precision) as eng:
+        eng.step(n)
+        VI = [eng.read_vi(b) for b in range(p.batch)]
+    for b, (V, I) in enumerate(VI):
+        assert _rel(V, d[f"cross.V{b}"]) < tol, b
+        assert _rel(I, d[f"cross.I{b}"]) < tol, b
+
+
+def test_cross_junction_batch_equals_one_excitation_per_handle():
+    """Each excitation alone on a one-field-set handle gives what it gives
+    inside the batch of eight."""
+    p, d, n = load_golden("cfg3_cross_small")
+    k = 600
+    with p.build_engine("single") as eng:
+        eng.step(k)
+        batched = [eng.read_vi(b) for b in range(p.batch)]
+    for b in (0, 5):
+        q = load_golden("cfg3_cross_small")[0]
+        q.batch = 1
+        for mp in q.modal:
+            mp.excitation = [mp.excitation[b]]
+        q.e0, q.h0 = [None], [None]
+        with q.build_engine("single") as eng:
+            eng.step(k)
+            V, I = eng.read_vi(0)
+        assert _rel(V, batched[b][0]) < 1e-6 and _rel(I, batched[b][1]) < 1e-6

@@ -32,3 +32,16 @@ def test_wr90_problem_reproduces_the_analysis_runs():
         r = OracleRun(p, b=b).run(250)
         V = d[f"cfg1.V{b}"][:250]
         assert float(np.max(np.abs(np.array(r.V) - V))) <= 1e-10 * float(np.max(np.abs(d[f"cfg1.V{b}"])))
+
+
+def test_cross_junction_problem_reproduces_the_reference_runs():
+    """Batching configuration (reduced): the batched problem's field sets
+    march like the reference's eight separate excitation runs."""
+    from oracle.fit_oracle import OracleRun
+
+    p, d, n = load_golden("cfg3_cross_small")
+    assert p.batch == 8
+    for b in (2, 7):
+        r = OracleRun(p, b=b).run(200)
+        V = d[f"cross.V{b}"]
+        assert float(np.max(np.abs(np.array(r.V) - V[:200]))) <= 1e-10 * float(np.max(np.abs(V)))
