@@ -570,13 +570,32 @@ PortsArgs ports_args(Handle& H) {
     return pa;
 }
 
+// Fused-step variants: 0-6 the register / cp.async forms (1 in float32
+// only), kFusedTileBase + v the TMA tile forms whose shared memory fits.
+bool fused_variant_ok(int prec, int v) {
+    if (v >= 0 && v <= 6) return !(v == 1 && prec == 8);
+    const int t = v - kFusedTileBase;
+    if (t < 0 || t >= kTileVariants) return false;
+    return prec == 4 ? tile_supported<float>(t) : tile_supported<double>(t);
+}
+
+cudaError_t prepare_fused_any(int prec, int v) {
+    if (v >= kFusedTileBase)
+        return prec == 4 ? prepare_tile<float>(v - kFusedTileBase) : prepare_tile<double>(v - kFusedTileBase);
+    return prec == 4 ? prepare_fused<float>(v) : prepare_fused<double>(v);
+}
+
 // Grid of the stream / vec kernels for the handle's batch and coefficient
 // storage (occupancy depends on the kernel instance).
 void plan_stencil(Handle& H) {
     if (H.stencil_mode != kModeStream && H.stencil_mode != kModeVec && H.stencil_mode != kModeFused) return;
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, H.desc.device);
-    if (H.stencil_mode == kModeFused) {
+    if (H.stencil_mode == kModeFused && H.fused_variant >= kFusedTileBase) {
+        const int v = H.fused_variant - kFusedTileBase;
+        const int occ = H.prec == 4 ? tile_occupancy<float>(v) : tile_occupancy<double>(v);
+        H.splan = H.prec == 4 ? plan_tile<float>(H.g, sms, occ, H.B, v) : plan_tile<double>(H.g, sms, occ, H.B, v);
+    } else if (H.stencil_mode == kModeFused) {
         const int v = H.fused_variant;
         const int occ = H.prec == 4 ? fused_occupancy<float>(v) : fused_occupancy<double>(v);
         H.splan = plan_fused(H.g, sms, occ, H.B, fused_tj_of(v));
@@ -616,11 +635,35 @@ void launch_half(Handle& H, int which) {
     }
 }
 
-void launch_fused_any(Handle& H) {
-    if (H.prec == 4)
-        launch_fused_step<float>(stencil_args<float>(H), H.splan, H.fused_variant, H.stream);
-    else
-        launch_fused_step<double>(stencil_args<double>(H), H.splan, H.fused_variant, H.stream);
+// The fused-step launch of the handle's variant (register / cp.async forms
+// or the TMA tile form).
+// (the tile form: the tile kernel and its E-side CPML passes).  Returns the
+// launches issued.
+template <typename T>
+int launch_fused(Handle& H, const StencilArgs<T>& sa) {
+    if (H.fused_variant >= kFusedTileBase) {
+        if (launch_tile_step<T>(sa, H.splan, H.fused_variant - kFusedTileBase, H.status.as<int>(), H.stream) != 0)
+            fail(FITB_ERR_CUDA, "tensor maps of the tile step could not be encoded");
+        const int ne = launch_tile_cpml_E<T>(sa, H.stream);
+        if (ne < 0) fail(FITB_ERR_STATE, "the tile step does not take this CPML layout");
+        return 1 + ne;
+    }
+    launch_fused_step<T>(sa, H.splan, H.fused_variant, H.stream);
+    return 1;
+}
+
+// The whole stencil part of a fused step (measurement helper: no ports).
+int launch_fused_any(Handle& H) {
+    if (H.prec == 4) {
+        const StencilArgs<float> sa = stencil_args<float>(H);
+        int n = launch_fused<float>(H, sa);
+        if (H.fused_variant >= kFusedTileBase) n += launch_tile_cpml_H<float>(sa, H.stream);
+        return n;
+    }
+    const StencilArgs<double> sa = stencil_args<double>(H);
+    int n = launch_fused<double>(H, sa);
+    if (H.fused_variant >= kFusedTileBase) n += launch_tile_cpml_H<double>(sa, H.stream);
+    return n;
 }
 
 void launch_stencil_half(Handle& H, int which) {
@@ -657,8 +700,7 @@ int enqueue_step_fused(Handle& H) {
     int n = 0;
     PortsArgs pa = ports_args(H);
     StencilArgs<T> sa = stencil_args<T>(H);
-    launch_fused_step<T>(sa, H.splan, H.fused_variant, H.stream);
-    ++n;
+    n += launch_fused<T>(H, sa);
     T* e_new = H.En().as<T>();
     T* h_new = H.Hn().as<T>();
     for (auto& pw : H.pws) {
@@ -672,6 +714,11 @@ int enqueue_step_fused(Handle& H) {
     if (!H.lumped.empty()) {
         launch_lumped<T>(e_new, pa, H.d_lumped.as<LumpedDev>(), (int)H.lumped.size(), H.stream);
         ++n;
+    }
+    if (H.fused_variant >= kFusedTileBase) {
+        const int nh = launch_tile_cpml_H<T>(sa, H.stream);
+        if (nh < 0) fail(FITB_ERR_STATE, "the tile step does not take this CPML layout");
+        n += nh;
     }
     if (H.n_fix > 0) {
         launch_fix_H<T>(sa, H.fix_cells.as<int4>(), H.n_fix, H.stream);
@@ -777,14 +824,14 @@ cudaGraphExec_t capture(Handle& H, int nsteps, int* launches_per) {
 // kernels; a non-zero value means a bounded shared-memory pipeline wait
 // expired and the step's results are not valid.
 void check_device_status(Handle& H) {
-    if (H.stencil_mode != kModeBulk) return;
+    if (H.stencil_mode != kModeBulk && !(H.stencil_mode == kModeFused && H.fused_variant >= kFusedTileBase)) return;
     int st = 0;
     ck(cudaMemcpyAsync(&st, H.status.p, sizeof(int), cudaMemcpyDeviceToHost, H.stream), "status D2H");
     ck(cudaStreamSynchronize(H.stream), "status sync");
     if (st != 0) {
         ck(cudaMemsetAsync(H.status.p, 0, sizeof(int), H.stream), "status reset");
-        fail(FITB_ERR_CUDA, "a bounded wait in the %s-update copy pipeline expired (status %d)",
-             st == kStatusWaitTimeoutE ? "E" : "H", st);
+        fail(FITB_ERR_CUDA, "a bounded wait in the %s copy pipeline expired (status %d)",
+             st == kStatusWaitTimeoutE ? "E-update" : (st == kStatusWaitTimeoutH ? "H-update" : "tile-step"), st);
     }
 }
 
@@ -1199,10 +1246,10 @@ int fitb_create(const fitb_desc* desc, fitb_handle** out) {
             }
         } else if (m == "fused") {
             const char* t = getenv("FITB_FUSED_VARIANT");
-            H.fused_variant = t ? std::max(0, std::min(6, atoi(t))) : 2;
+            H.fused_variant = t ? std::max(0, std::min(fitb::kFusedTileBase + fitb::kTileVariants - 1, atoi(t))) : 2;
             if (H.fused_variant == 1 && H.prec == 8) H.fused_variant = 0;
-            ck(H.prec == 4 ? fitb::prepare_fused<float>(H.fused_variant) : fitb::prepare_fused<double>(H.fused_variant),
-               "fused step smem attribute");
+            if (!fitb::fused_variant_ok(H.prec, H.fused_variant)) H.fused_variant = 2;
+            ck(fitb::prepare_fused_any(H.prec, H.fused_variant), "fused step smem attribute");
             H.e2.alloc(blk * H.B);
             H.h2.alloc(blk * H.B);
             H.stencil_mode = fitb::kModeFused;
@@ -1324,9 +1371,13 @@ int fitb_configure_stencil(fitb_handle* h, int32_t kind, int32_t variant, int32_
     if (kind == fitb::kModeVec && (H.B > 8 || variant < 0 || variant > 3))
         fail(FITB_ERR_ARG, "vec stencil: variant %d / batch %d", variant, H.B);
     if (kind == fitb::kModeFused) {
-        if (variant < 0 || variant > 6 || (variant == 1 && H.prec == 8)) fail(FITB_ERR_ARG, "fused variant %d", variant);
+        if (!fitb::fused_variant_ok(H.prec, variant)) fail(FITB_ERR_ARG, "fused variant %d", variant);
         if (H.disp[0].present() || H.disp[1].present())
             fail(FITB_ERR_STATE, "dispersive materials need an in-place stencil mode (not the fused step)");
+        if (variant >= fitb::kFusedTileBase &&
+            !(H.prec == 4 ? fitb::tile_step_fits<float>(fitb::stencil_args<float>(H))
+                          : fitb::tile_step_fits<double>(fitb::stencil_args<double>(H))))
+            fail(FITB_ERR_ARG, "the tile step does not take this grid / CPML layout");
     }
     if (kind == fitb::kModeBulk && H.B != 1) fail(FITB_ERR_ARG, "the bulk-copy stencil takes one field set");
     ck(cudaStreamSynchronize(H.stream), "configure sync");
@@ -1340,8 +1391,7 @@ int fitb_configure_stencil(fitb_handle* h, int32_t kind, int32_t variant, int32_
     }
     const size_t blk = (size_t)H.e_block() * H.esz;
     if (kind == fitb::kModeFused) {
-        ck(H.prec == 4 ? fitb::prepare_fused<float>(variant) : fitb::prepare_fused<double>(variant),
-           "fused step smem attribute");
+        ck(fitb::prepare_fused_any(H.prec, variant), "fused step smem attribute");
         if (!H.e2.p) H.e2.alloc(blk * H.B);
         if (!H.h2.p) H.h2.alloc(blk * H.B);
         for (auto& f : H.faces)
@@ -2036,13 +2086,15 @@ int fitb_time_stencil(fitb_handle* h, int32_t n_iter, double* ms_e, double* ms_h
         // leaves the current set where it was
         const int n2 = 2 * ((n_iter + 1) / 2);
         ck(cudaEventRecord(ev[0], H.stream), "event record");
+        int nl = 0;
         for (int q = 0; q < n2; ++q) {
-            fitb::launch_fused_any(H);
+            nl += fitb::launch_fused_any(H);
             H.cur ^= 1;
         }
         ck(cudaEventRecord(ev[1], H.stream), "event record");
         ck(cudaEventSynchronize(ev[1]), "event sync");
-        H.launches += n2;
+        H.launches += nl;
+        fitb::check_device_status(H);
         float f1 = 0.f;
         ck(cudaEventElapsedTime(&f1, ev[0], ev[1]), "elapsed");
         for (auto& x : ev) cudaEventDestroy(x);

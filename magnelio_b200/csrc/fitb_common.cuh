@@ -132,6 +132,36 @@ int fused_occupancy(int variant);
 StreamPlan plan_fused(const Geom& g, int sm_count, int ctas_per_sm, int B, int tj);
 template <typename T>
 void launch_fused_step(StencilArgs<T> a, const StreamPlan& sp, int variant, cudaStream_t s);
+// TMA-fed shared-memory tile form of the fused step (stencil_tile.cu), the
+// fused-step variants kFusedTileBase + v for tile variant v (tile rows, ring
+// stages; 32 cells per row): 0 (4, 3), 1 (4, 4), 2 (8, 4), 3 (16, 4),
+// 4 (4, 5), 5 (8, 3), 6 (2, 4).  grid_x = k tiles x field sets, grid_y = j
+// tiles, grid_z = i chunks.  The tile kernel carries no CPML: after it,
+// launch_tile_cpml_E applies the E-side CPML face by face to e_next, and
+// after the ports' E writes launch_tile_cpml_H recomputes H on every cell
+// the CPML reaches.
+constexpr int kFusedTileBase = 7, kTileVariants = 7;
+template <typename T>
+bool tile_supported(int variant);
+template <typename T>
+cudaError_t prepare_tile(int variant);
+template <typename T>
+int tile_occupancy(int variant);
+template <typename T>
+StreamPlan plan_tile(const Geom& g, int sm_count, int ctas_per_sm, int B, int variant);
+// Encodes the tensor maps of the current buffers and launches; < 0 when the
+// maps cannot be encoded.  status: set non-zero when a bounded wait expires.
+template <typename T>
+int launch_tile_step(StencilArgs<T> a, const StreamPlan& sp, int variant, int* status, cudaStream_t s);
+// Both return the number of launches issued (< 0: more pass boxes than
+// the table holds, which tile_step_fits rules out beforehand).
+template <typename T>
+int launch_tile_cpml_E(const StencilArgs<T>& a, cudaStream_t s);
+template <typename T>
+int launch_tile_cpml_H(const StencilArgs<T>& a, cudaStream_t s);
+// Whether the tile step takes this grid and CPML layout.
+template <typename T>
+bool tile_step_fits(const StencilArgs<T>& a);
 // H update of listed cells (x, y, z = i, j, k) from h / psi and e_next.
 template <typename T>
 void launch_fix_H(const StencilArgs<T>& a, const int4* cells, int n, cudaStream_t s);
@@ -159,6 +189,7 @@ template <typename T>
 void launch_update_H_bulk(const StencilArgs<T>& a, const BulkPlan& plan, int* status, cudaStream_t s);
 constexpr int kStatusWaitTimeoutE = 1;
 constexpr int kStatusWaitTimeoutH = 2;
+constexpr int kStatusWaitTimeoutTile = 3;
 
 // ---------------------------------------------------------------------------
 // Lumped ports (Thevenin element with a series R-L-C companion).

@@ -12,6 +12,7 @@ import numpy as np
 import pytest
 
 from conftest import load_golden
+from magnelio_b200._lib import FitbError
 
 pytestmark = pytest.mark.gpu
 
@@ -114,7 +115,7 @@ def test_stencil_variants_agree(name):
     p, d, n = load_golden(name)
     outs = []
     modes = [("stream", v) for v in range(4)] + [("bulk", 0), ("simple", 0)]
-    modes += [("vec", v) for v in range(4)] + [("fused", v) for v in range(7)]
+    modes += [("vec", v) for v in range(4)] + [("fused", v) for v in range(14)]
     for kind, variant in modes:
         with p.build_engine("single") as eng:
             eng.configure_stencil(kind, variant)
@@ -327,7 +328,7 @@ def test_compact_coefficients_need_the_stream_kernels(monkeypatch):
 
 @pytest.mark.parametrize("name", ["cpml_box", "mixed_box", "lumped_dft", "wg_dtbc", "wg_mur", "planewave_box"])
 @pytest.mark.parametrize("precision,tol", [("double", F64_TOL), ("single", F32_TOL)])
-@pytest.mark.parametrize("variant", ["0", "2"])
+@pytest.mark.parametrize("variant", ["0", "2", "7", "8"])
 def test_fused_step_matches_reference(name, precision, tol, variant, monkeypatch):
     """The fused E+H pass (ping-pong buffers, H fix-up next to port edges)
     reproduces the reference march: fields, energy, port V/I, DFT bins."""
@@ -351,11 +352,13 @@ def test_fused_step_matches_reference(name, precision, tol, variant, monkeypatch
 
 
 @pytest.mark.parametrize("name", ["lumped_dft", "wg_mur"])
-def test_fused_buffer_swaps_are_invisible(name, monkeypatch):
+@pytest.mark.parametrize("variant", ["2", "8"])
+def test_fused_buffer_swaps_are_invisible(name, variant, monkeypatch):
     """Odd and even step counts, single steps, graph chunks and a resume at
     an odd step give the same bits: the buffer set that holds the current
     fields never shows through the API."""
     monkeypatch.setenv("FITB_STENCIL", "fused")
+    monkeypatch.setenv("FITB_FUSED_VARIANT", variant)
     p, d, n = load_golden(name)
     k = 2 * (n // 4) + 1  # odd
     with p.build_engine("single") as a, p.build_engine("single") as b:
@@ -537,3 +540,81 @@ def test_cross_junction_batch_equals_one_excitation_per_handle():
             eng.step(k)
             V, I = eng.read_vi(0)
         assert _rel(V, batched[b][0]) < 1e-6 and _rel(I, batched[b][1]) < 1e-6
+
+
+# ---------------------------------------------------------------------------
+# TMA tile form of the fused step on grids of many tiles and chunks.
+
+TILE_VARIANTS = range(7, 14)
+
+
+def _random_state(prob, rng, scale=1e-3):
+    """Random E and H on every live entry, so CPML, tile halos and chunk
+    seams all carry signal from the first step."""
+    e = rng.standard_normal(prob.alpha_E.size) * (prob.beta_E != 0) * scale
+    h = rng.standard_normal(prob.alpha_H.size) * (prob.beta_H != 0) * scale
+    return e, h
+
+
+def _run_mode(prob, precision, kind, variant, ichunk, steps):
+    with prob.build_engine(precision) as eng:
+        eng.configure_stencil(kind, variant, ichunk)
+        eng.step(steps)
+        e, h = eng.read_fields()
+        V, I = eng.read_vi()
+        bins = [eng.read_dft(q, c) for q, m in enumerate(prob.monitors) for c in m.components]
+        cfg = eng.stencil_config()
+    return e, h, V, bins, cfg
+
+
+@pytest.mark.parametrize("n", [64, 70])
+@pytest.mark.parametrize("precision,tol", [("single", 1e-5), ("double", 1e-12)])
+def test_tile_step_matches_stream_on_a_multi_tile_grid(n, precision, tol):
+    """Brick box 70^3 (71 cells along j and k: partial last tiles) and 64^3
+    (65 cells: the last row and column are taken by the tiles before them),
+    6-layer CPML on all faces cutting through tiles, a lumped source, DFT
+    planes, random initial fields, short i chunks (chunk seams): every tile
+    variant agrees with the stream kernels (which the golden cases pin to
+    the reference) to FMA-contraction differences."""
+    from magnelio_b200 import workloads
+
+    steps = 23
+    prob = workloads.brick_box(n, seed=5, n_bricks=8, cpml_cells=6, n_freq=4, steps=steps + 2)
+    e0, h0 = _random_state(prob, np.random.default_rng(1))
+    prob.e0, prob.h0 = [e0], [h0]
+    ref = _run_mode(prob, precision, "stream", 0, 0, steps)
+    pe, ph = float(np.max(np.abs(ref[0]))), float(np.max(np.abs(ref[1])))
+    ran = 0
+    for v in TILE_VARIANTS:
+        for ichunk in (0, 9):
+            try:
+                got = _run_mode(prob, precision, "fused", v, ichunk, steps)
+            except FitbError as exc:
+                assert precision == "double" and "fused variant" in str(exc), exc
+                continue
+            ran += 1
+            assert got[4]["kind"] == "fused" and got[4]["variant"] == v
+            if ichunk:
+                assert got[4]["ichunk"] == ichunk
+            assert _rel(got[0], ref[0], pe) < tol, (v, ichunk)
+            assert _rel(got[1], ref[1], ph) < tol, (v, ichunk)
+            assert _rel(got[2], ref[2]) < 10 * tol, (v, ichunk)
+            for a, b in zip(got[3], ref[3]):
+                assert _rel(a, b) < max(10 * tol, DFT_TOL), (v, ichunk)
+    assert ran >= (14 if precision == "single" else 12)
+
+
+def test_tile_step_batched_matches_the_plain_kernel():
+    """All six WR-90 port-mode excitations as one batch (DTBC ports, port
+    fix-up cells, two k tiles): the tile form equals the plain batched
+    kernel (the stream kernels take power-of-two batches)."""
+    p, d, n = load_golden("cfg1_wr90")
+    steps = 400
+    ref = _run_mode(p, "single", "simple", 0, 0, steps)
+    pe = float(np.max(np.abs(ref[0])))
+    for v in (7, 8, 13):
+        got = _run_mode(p, "single", "fused", v, 17, steps)
+        # float32 round-off (FMA contraction differs per kernel) grows over
+        # 400 steps of a resonant guide; the reference bar is 2e-4
+        assert _rel(got[0], ref[0], pe) < 1e-4, v
+        assert _rel(got[2], ref[2]) < 1e-4, v
