@@ -18,6 +18,7 @@ same workload.
 from __future__ import annotations
 
 import argparse
+import datetime
 import json
 import os
 import statistics
@@ -35,6 +36,7 @@ if str(ROOT) not in sys.path:
 METRIC = "Gcell-updates/s"
 BYTES_PER_CELL = 96  # E(3) H(3) read+write, alpha/beta E/H (12) read, float32
 FIELD_BYTES_PER_CELL = 48  # the field part of it, per field set
+TILE_VARIANT_BASE = 7  # fused-step variants from here on are the TMA tile form
 COEF_BYTES_PER_CELL = 48  # the coefficient part, shared by a batch of field sets
 BYTES_PER_CPML_CELL = 32  # 2 psi_E + 2 psi_H read+write per slab cell per face, float32
 
@@ -47,33 +49,53 @@ def _peaks():
     return 6650.0, "fallback"
 
 
-def _traffic(kernel_key: str, n: int):
-    """DRAM bytes per cell from a committed ncu summary, if one exists."""
+def _traffic(kernel_key: str, n: int, cpml_cells: int = 0):
+    """DRAM bytes of one step from a committed ncu summary, if one exists:
+    bytes per cell x n^3 (and, for the tile step, bytes per CPML slab cell of
+    its CPML passes)."""
     p = ROOT / "profiles" / "traffic.json"
     if not p.exists():
         return None
     d = json.loads(p.read_text())
     v = d.get(kernel_key)
-    return None if v is None else float(v) * n**3
+    if v is None:
+        return None
+    if isinstance(v, dict):
+        return float(v["per_cell"]) * n**3 + float(v["per_cpml_face_cell"]) * cpml_cells
+    return float(v) * n**3
 
 
 class ClockSampler:
-    """nvidia-smi clock / throttle sampling during the timed region."""
+    """nvidia-smi clock / throttle sampling around the timed region.
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    Sampling starts when the object is made (every 50 ms, with a timestamp)
+    and is given time to come up; ``window()`` brackets the timed region and
+    ``stop()`` keeps the samples inside it.  A region shorter than the
+    sampling interval keeps the sample nearest to its middle."""
+
+    FIELDS = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    STARTUP_S = 0.5
 
     def __init__(self, local_rank: int):
         vis = os.environ.get("CUDA_VISIBLE_DEVICES")
         idx = vis.split(",")[local_rank] if vis else str(local_rank)
         self.proc = None
+        self.t0 = self.t1 = None
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={idx}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                 "-lms", "50"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            time.sleep(self.STARTUP_S)
         except OSError:
             self.proc = None
+
+    def window(self, start: bool) -> None:
+        if start:
+            self.t0 = datetime.datetime.now()
+        else:
+            self.t1 = datetime.datetime.now()
 
     def stop(self) -> dict:
         if self.proc is None:
@@ -84,22 +106,34 @@ class ClockSampler:
         except subprocess.TimeoutExpired:
             self.proc.kill()
             out, _ = self.proc.communicate()
-        sm, smax, reasons = [], [], set()
-        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        rows = []
         for line in out.strip().splitlines():
             parts = [x.strip() for x in line.split(",")]
-            if len(parts) < 9:
+            if len(parts) < 10:
                 continue
             try:
-                sm.append(float(parts[1]))
-                smax.append(float(parts[2]))
+                ts = datetime.datetime.strptime(parts[0], "%Y/%m/%d %H:%M:%S.%f")
+                rows.append((ts, float(parts[2]), float(parts[3]), parts[6:10]))
             except ValueError:
                 continue
-            for nm, v in zip(names, parts[5:9]):
+        inside = rows
+        where = "timed region"
+        if self.t0 is not None and self.t1 is not None and rows:
+            inside = [r for r in rows if self.t0 <= r[0] <= self.t1]
+            if not inside:
+                mid = self.t0 + (self.t1 - self.t0) / 2
+                inside = [min(rows, key=lambda r: abs((r[0] - mid).total_seconds()))]
+                where = "nearest to the timed region (shorter than the 50 ms sampling interval)"
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        reasons = set()
+        for r in inside:
+            for nm, v in zip(names, r[3]):
                 if v.lower().startswith("active"):
                     reasons.add(nm)
+        sm = [r[1] for r in inside]
+        smax = [r[2] for r in inside]
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm), "sampled": where}
 
 
 def _dist():
@@ -218,8 +252,6 @@ def main() -> int:
         ap.error("--warmup must be >= 3")
     world, rank, local = _dist()
     if world > 1:
-        import datetime
-
         import torch
         import torch.distributed as dist
 
@@ -362,15 +394,17 @@ def run_slab(args, world, rank, local):
         autotune.apply(eng, tuned)
     stencil_cfg = eng.stencil_config()
     cells = nx * ny * nz
+    sampler = ClockSampler(local)
     eng.step(args.warmup)
     eng.sync()
     if world > 1:
         import torch.distributed as dist
 
         dist.barrier()
-    sampler = ClockSampler(local)
     l0 = eng.launch_count
+    sampler.window(True)
     ms = eng.step_timed(args.steps)
+    sampler.window(False)
     launches = eng.launch_count - l0
     clocks = sampler.stop()
     ms = _max_over_ranks(ms, world, local)
@@ -444,15 +478,17 @@ def run_b200(args, world, rank, local):
     coef_bytes = COEF_BYTES_PER_CELL if args.coef == "native" else COEF_BYTES_PER_CELL // 2
     cells = n**3 * B
     # warm-up (graph capture, clocks)
+    sampler = ClockSampler(local)
     eng.step(args.warmup)
     eng.sync()
     if world > 1:
         import torch.distributed as dist
 
         dist.barrier()
-    sampler = ClockSampler(local)
     l0 = eng.launch_count
+    sampler.window(True)
     ms = eng.step_timed(args.steps)
+    sampler.window(False)
     launches = eng.launch_count - l0
     clocks = sampler.stop()
     ms = _max_over_ranks(ms, world, local)
@@ -489,8 +525,14 @@ def run_b200(args, world, rank, local):
     alg_bytes = (FIELD_BYTES_PER_CELL * B + coef_bytes) * n**3 + BYTES_PER_CPML_CELL * B * cpml_cells
     achieved = alg_bytes / (t_pair * 1e-3) / 1e9
     peak, peak_kind = _peaks()
-    traffic = _traffic("update_E+update_H", n)
-    roofline = {"bound": "hbm", "kernel": "update_E + update_H (one stencil step)", "achieved": achieved,
+    tile = stencil_cfg["kind"] == "fused" and stencil_cfg["variant"] >= TILE_VARIANT_BASE
+    if tile:
+        kernel = "k_step_tile + CPML passes (one stencil step)"
+        traffic = _traffic("tile_step", n, cpml_cells) if B == 1 else None
+    else:
+        kernel = "update_E + update_H (one stencil step)"
+        traffic = _traffic("update_E+update_H", n) if stencil_cfg["kind"] == "stream" and B == 1 else None
+    roofline = {"bound": "hbm", "kernel": kernel, "achieved": achieved,
                 "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": traffic, "algorithmic_bytes": alg_bytes, "ms_E": t_e, "ms_H": t_h,
                 "step_share": t_pair / (ms / args.steps)}

@@ -37,11 +37,14 @@ DEFAULT_CANDIDATES = (
     ("stream", 0, 128),
     ("vec", 3, 0),
     ("vec", 2, 0),
+    ("fused", 7, 0),
+    ("fused", 7, 16),
+    ("fused", 8, 0),
+    ("fused", 9, 0),
     ("fused", 0, 0),
-    ("fused", 4, 0),
-    ("fused", 5, 0),
     ("bulk", 0, 0),
 )
+CANDIDATE_SET = 2  # bump when the candidates change: cached results of another set are not reused
 
 
 @dataclass
@@ -75,7 +78,7 @@ def _device_name(device: int) -> str:
 
 
 def cache_key(nx, ny, nz, batch, precision, coef, n_cpml, device_name) -> str:
-    return f"{nx}x{ny}x{nz}|B{batch}|{precision}|{coef}|cpml{n_cpml}|{device_name}"
+    return f"{nx}x{ny}x{nz}|B{batch}|{precision}|{coef}|cpml{n_cpml}|{device_name}|c{CANDIDATE_SET}"
 
 
 def _load_cache(path: Path) -> dict:

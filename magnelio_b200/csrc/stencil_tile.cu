@@ -318,19 +318,18 @@ __global__ void __launch_bounds__(32 * (TJ + 1), sizeof(T) == 4 ? MINB : 1)
 }
 
 // Disjoint cell boxes [lo, hi) of a CPML pass, each with the CPML faces
-// (bit q = face q) of all its cells.  Blocks of 256 threads cover one i
-// plane of one box each: block ranges bstart, bpp blocks per plane.
+// (bit q = face q) of all its cells.  Blocks of 256 threads cover 256
+// consecutive cells of one box (k fastest): block ranges bstart.
 constexpr int kPassThreads = 256;
 constexpr int kMaxPassBoxes = 128;  // six faces: at most 4^3 - 8 (E side), 5^3 - 8 (H side)
 struct PassBoxes {
     int n;
     int lo[kMaxPassBoxes][3], hi[kMaxPassBoxes][3];
     unsigned mask[kMaxPassBoxes];
-    int bpp[kMaxPassBoxes];
     int bstart[kMaxPassBoxes + 1];
 };
 
-// Cell (i, j, k) of this thread and its box, or false past the box's plane.
+// Cell (i, j, k) of this thread and its box, or false past the box's end.
 __device__ __forceinline__ bool pass_cell(const PassBoxes& bx, int& q, int& i, int& j, int& k) {
     int lo = 0, hi = bx.n - 1;  // last box with bstart <= blockIdx.x
     while (lo < hi) {
@@ -341,14 +340,14 @@ __device__ __forceinline__ bool pass_cell(const PassBoxes& bx, int& q, int& i, i
             hi = mid - 1;
     }
     q = lo;
-    const int lb = (int)blockIdx.x - bx.bstart[q];
-    const int nk = bx.hi[q][2] - bx.lo[q][2];
-    const int njk = (bx.hi[q][1] - bx.lo[q][1]) * nk;
-    const int jk = (lb % bx.bpp[q]) * kPassThreads + (int)threadIdx.x;
-    if (jk >= njk) return false;
-    i = bx.lo[q][0] + lb / bx.bpp[q];
-    j = bx.lo[q][1] + jk / nk;
-    k = bx.lo[q][2] + jk % nk;
+    const int nk = bx.hi[q][2] - bx.lo[q][2], nj = bx.hi[q][1] - bx.lo[q][1];
+    const int ncell = (bx.hi[q][0] - bx.lo[q][0]) * nj * nk;
+    const int u = ((int)blockIdx.x - bx.bstart[q]) * kPassThreads + (int)threadIdx.x;
+    if (u >= ncell) return false;
+    const int w = u / nk;
+    k = bx.lo[q][2] + (u - w * nk);
+    i = bx.lo[q][0] + w / nj;
+    j = bx.lo[q][1] + (w - (w / nj) * nj);
     return true;
 }
 
@@ -626,10 +625,10 @@ bool pass_boxes(PassBoxes& bx, const Geom& g, const FaceDev* f, int nfaces, bool
                 bx.lo[q][2] = z.lo;
                 bx.hi[q][2] = z.hi;
                 bx.mask[q] = x.faces | y.faces | z.faces;
-                const int njk = (y.hi - y.lo) * (z.hi - z.lo);
-                bx.bpp[q] = (njk + kPassThreads - 1) / kPassThreads;
+                const long long ncell = (long long)(x.hi - x.lo) * (y.hi - y.lo) * (z.hi - z.lo);
+                if (ncell >= (1LL << 31)) return false;
                 bx.bstart[q] = acc;
-                acc += bx.bpp[q] * (x.hi - x.lo);
+                acc += (int)((ncell + kPassThreads - 1) / kPassThreads);
             }
     bx.bstart[bx.n] = acc;
     return true;
@@ -676,12 +675,12 @@ StreamPlan plan_tile(const Geom& g, int sm_count, int ctas_per_sm, int B, int va
     const long long tiles = (long long)s.grid_x * s.grid_y;
     const int nplanes = g.nx + 1;
     const int per_wave = sm_count * ctas_per_sm;
-    // chunks of 16-32 planes measured best (a chunk re-reads two planes;
-    // long chunks let all CTAs of a wave sweep the same planes in step);
-    // among those, the one with the best wave quantisation
+    // chunks of about 16 planes measured best on 256^3 and 512^3 grids (a
+    // chunk re-reads two planes; long chunks let all CTAs of a wave sweep
+    // the same planes in step); among 12-20, the best wave quantisation
     double best = -1e30;
-    int best_chunk = std::min(nplanes, 24);
-    for (int ichunk = std::min(nplanes, 32); ichunk >= std::min(nplanes, 16); --ichunk) {
+    int best_chunk = std::min(nplanes, 16);
+    for (int ichunk = std::min(nplanes, 20); ichunk >= std::min(nplanes, 12); --ichunk) {
         const int nch = (nplanes + ichunk - 1) / ichunk;
         const double waves = (double)tiles * nch / per_wave;
         const double eff = waves / std::ceil(waves);
