@@ -408,14 +408,17 @@ StreamPlan plan_stream(const Geom& g, int sm_count, int ctas_per_sm, int B) {
     const int bx = (g.nz + 1 + kSX - 1) / kSX, by = (g.ny + 1 + rows - 1) / rows;
     const int nplanes = g.nx + 1;
     const int per_wave = sm_count * ctas_per_sm;
+    // chunks of 12-32 planes: longer ones leave few CTAs that all sweep the
+    // same planes in step with one plane of loads in flight each (measured:
+    // a single 257-plane wave at 256^3 and B = 2 runs 1.6x slower than
+    // chunks of 16); among those, prefer long chunks (fewer re-loaded
+    // boundary planes) unless the wave tail costs more than a few percent
     double best = -1.0;
-    int best_chunk = nplanes;
-    for (int ichunk = nplanes; ichunk >= 4; --ichunk) {
+    int best_chunk = std::min(nplanes, 16);
+    for (int ichunk = std::min(nplanes, 32); ichunk >= std::min(nplanes, 12); --ichunk) {
         const int nch = (nplanes + ichunk - 1) / ichunk;
         const double waves = (double)bx * by * nch / per_wave;
         const double eff = waves / (double)((long long)(waves + 0.999999));
-        // prefer long chunks (fewer re-loaded boundary planes) unless the
-        // wave tail costs more than a few percent
         const double score = eff - 0.5 / ichunk;
         if (score > best) {
             best = score;

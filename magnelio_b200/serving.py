@@ -78,33 +78,46 @@ class ServingStats:
 
 
 def estimate_footprint(nx, ny, nz, batch, steps, n_channels, cpml_layers=(), precision="single",
-                       n_dispersive_states=0) -> int:
+                       n_dispersive_states=0, fused=False) -> int:
     """Device bytes a handle for this problem holds, from the engine's
     padded layout: fields (B sets), coefficients and mass diagonals, the
-    staging buffer, CPML psi slabs, the V/I recorder sized for ``steps``."""
+    staging buffer, CPML psi slabs, the V/I recorder sized for ``steps``;
+    ``fused``: the fused step's second set of fields and psi."""
     esz = 4 if precision == "single" else 8
+    sets = 2 if fused else 1
     njp, nkp = ny + 2, -(-(nz + 2) // 4) * 4
     si = njp * nkp
     vol = (nx + 4) * si + 8 * nkp
     n_e = 3 * (nx + 1) * (ny + 1) * (nz + 1)
-    total = 2 * batch * 3 * vol * esz          # E, H
+    total = sets * 2 * batch * 3 * vol * esz   # E, H
     total += 6 * 3 * vol * esz                 # alpha/beta E/H, M_eps, M_mu
     total += n_e * esz                         # staging
     for axis, n in cpml_layers:
         dims = [nx + 1, ny + 1, nz + 1]
         dims[axis] = n
         slab = dims[0] * dims[1] * dims[2]
-        total += batch * 4 * slab * esz + 4 * slab + 3 * n * esz
+        total += sets * batch * 4 * slab * esz + 4 * slab + 3 * n * esz
     cap = max(int(steps), 1024)
     total += 2 * batch * cap * max(n_channels, 1) * 8
     total += n_dispersive_states * batch * 8 * esz
     return int(total + (4 << 20))              # small tables and counters
 
 
-def _footprint_of(prob, steps, precision):
+def _footprint_of(prob, steps, precision, fused=False):
     layers = [("xyz".index(f.face[0]), len(f.b)) for f in prob.cpml]
     nch = len(prob.lumped) + sum(m.n_modes for m in prob.modal)
-    return estimate_footprint(prob.nx, prob.ny, prob.nz, prob.batch, steps, nch, layers, precision)
+    return estimate_footprint(prob.nx, prob.ny, prob.nz, prob.batch, steps, nch, layers, precision, fused=fused)
+
+
+def serving_stencil(batch: int):
+    """Stencil form of a served handle with ``batch`` field sets, each form
+    on the kernels measured fastest for it in the served mix: one field set
+    on the TMA tile form of the fused step (96^3: 1.46x the two-pass
+    kernels; 256^3: equal), several on the batched two-pass kernels (with
+    eight requests resident the tile form's shared memory per CTA limits how
+    many CTAs of different requests share an SM: 5.9 vs 7.7 solves/s on the
+    quarter-scale stream)."""
+    return ("fused", 7) if batch == 1 else None
 
 
 class ServingLoop:
@@ -115,9 +128,10 @@ class ServingLoop:
 
     def __init__(self, device: int = 0, precision: str = "single", hbm_budget: int | None = None,
                  max_slots: int = 8, slice_steps: int = 512, engine_factory=None, tune=None,
-                 clock=time.perf_counter, sleep=time.sleep):
+                 clock=time.perf_counter, sleep=time.sleep, stencil=serving_stencil):
         self.device = device
         self.precision = precision
+        self.stencil = stencil        # callable(batch) -> (kind, variant) or None (the engine default)
         self.max_slots = max_slots
         self.slice_steps = slice_steps
         self.engine_factory = engine_factory or (lambda p, prec, dev: p.build_engine(prec, device=dev))
@@ -158,11 +172,13 @@ class ServingLoop:
                 req, port, prob = pending[0]
                 if prob is None:
                     prob = pending[0][2] = self._problem(req, port)
-                fp = _footprint_of(prob, req.steps, self.precision)
+                form = self.stencil(prob.batch) if self.stencil is not None else None
+                fp = _footprint_of(prob, req.steps, self.precision, form is not None and form[0] == "fused")
                 if active and used + fp > self.hbm_budget:
                     break                         # wait for memory (arrival order kept)
                 pending.popleft()
                 eng = self.engine_factory(prob, self.precision, self.device)
+                self._configure(eng, form)
                 if self.tune is not None:
                     self.tune(prob, eng)
                 eng.reserve_steps(req.steps)
@@ -214,6 +230,21 @@ class ServingLoop:
                             p50=float(np.percentile(lat, 50)), p99=float(np.percentile(lat, 99)),
                             mean_active=float(np.mean(active_samples)) if active_samples else 0.0,
                             peak_bytes=int(peak), results=sorted(results, key=lambda r: r.rid))
+
+    @staticmethod
+    def _configure(eng, form):
+        """The stencil form on a new handle; a handle that does not take it
+        (dispersive materials need the in-place forms) keeps the engine's
+        default kernels."""
+        configure = getattr(eng, "configure_stencil", None)
+        if form is None or configure is None:
+            return
+        from magnelio_b200._lib import FitbError
+
+        try:
+            configure(*form)
+        except FitbError:
+            pass
 
     @staticmethod
     def _problem(req, port):

@@ -155,5 +155,8 @@ def test_footprint_estimate_counts_the_big_buffers():
     fp = serving.estimate_footprint(64, 64, 64, 4, 1000, 4, [(2, 8), (2, 8)])
     vol = 68 * 66 * 68 + 8 * 68
     assert fp > 2 * 4 * 3 * vol * 4 + 6 * 3 * vol * 4
+    # the fused step's second buffer set: fields and psi once more
+    fpf = serving.estimate_footprint(64, 64, 64, 4, 1000, 4, [(2, 8), (2, 8)], fused=True)
+    assert fpf - fp == 2 * 4 * 3 * vol * 4 + 2 * 4 * 4 * (65 * 65 * 8) * 4
     with pytest.raises(TypeError):
         serving.estimate_footprint(64, 64)
