@@ -167,10 +167,14 @@ int fitb_set_coeffs_native(fitb_handle* h, const void* alpha_e, const void* beta
 int fitb_set_coeff_storage(fitb_handle* h, int32_t kind);
 /* Stencil form of the handle (no counterpart in the reference, whose kernels
  * are fixed): kind FITB_STENCIL_SIMPLE / STREAM / BULK / VEC / FUSED, a
- * variant of that form (vec 0-3, fused 0-6), and the number of i planes one
- * CTA marches (0: the form's own plan).  The fields, psi and all other state
- * carry over; valid between steps.  fitb_get_stencil writes kind, variant,
- * planes per CTA and the grid (x, y, z) into out[6]. */
+ * variant of that form (vec 0-3; fused 0-6 the register / cp.async forms,
+ * fused 7-15 the TMA tile form with its CPML slab passes, tile shapes of
+ * 2-16 rows x 32 cells and 3-5 ring stages; FITB_ERR_ARG for a form the
+ * handle's precision, dispersion or CPML layout does not take), and the
+ * number of i planes one CTA marches (0: the form's own plan).  The fields,
+ * psi and all other state carry over; valid between steps.
+ * fitb_get_stencil writes kind, variant, planes per CTA and the grid
+ * (x, y, z) into out[6]. */
 #define FITB_STENCIL_SIMPLE 0
 #define FITB_STENCIL_STREAM 1
 #define FITB_STENCIL_BULK 2
@@ -270,6 +274,11 @@ int fitb_read_dft(fitb_handle* h, int32_t mon, int32_t b, int32_t comp,
  * at fit_td.py:950-1007), replaying captured CUDA graphs. */
 int fitb_step(fitb_handle* h, int64_t n_steps);
 int fitb_sync(fitb_handle* h);
+/* Non-blocking: *done = 1 when every step issued so far has finished on the
+ * device (then also the fitb_sync checks ran), 0 while work is in flight.
+ * No counterpart in the reference (its loop is synchronous); the serving
+ * loop uses it to keep every resident handle busy. */
+int fitb_query(fitb_handle* h, int32_t* done);
 /* fitb_step bracketed by CUDA events on the handle's stream; blocks until
  * the steps are done and returns their device time in milliseconds. */
 int fitb_step_timed(fitb_handle* h, int64_t n_steps, double* ms);

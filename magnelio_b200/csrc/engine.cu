@@ -2127,6 +2127,21 @@ int fitb_sync(fitb_handle* h) {
     FITB_CATCH
 }
 
+int fitb_query(fitb_handle* h, int32_t* done) {
+    FITB_TRY
+    Handle& H = H_of(h);
+    if (!done) fail(FITB_ERR_ARG, "null argument");
+    const cudaError_t e = cudaStreamQuery(H.stream);
+    if (e == cudaErrorNotReady) {
+        *done = 0;
+    } else {
+        ck(e, "stream query");
+        fitb::check_device_status(H);
+        *done = 1;
+    }
+    FITB_CATCH
+}
+
 int fitb_steps_done(fitb_handle* h, int64_t* out) {
     FITB_TRY
     Handle& H = H_of(h);

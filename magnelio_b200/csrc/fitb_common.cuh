@@ -135,12 +135,13 @@ void launch_fused_step(StencilArgs<T> a, const StreamPlan& sp, int variant, cuda
 // TMA-fed shared-memory tile form of the fused step (stencil_tile.cu), the
 // fused-step variants kFusedTileBase + v for tile variant v (tile rows, ring
 // stages; 32 cells per row): 0 (4, 3), 1 (4, 4), 2 (8, 4), 3 (16, 4),
-// 4 (4, 5), 5 (8, 3), 6 (2, 4).  grid_x = k tiles x field sets, grid_y = j
+// 4 (4, 5), 5 (8, 3), 6 (2, 4), 7 (3, 3), 8 (2, 3).  grid_x = k tiles x
+// field sets, grid_y = j
 // tiles, grid_z = i chunks.  The tile kernel carries no CPML: after it,
 // launch_tile_cpml_E applies the E-side CPML face by face to e_next, and
 // after the ports' E writes launch_tile_cpml_H recomputes H on every cell
 // the CPML reaches.
-constexpr int kFusedTileBase = 7, kTileVariants = 7;
+constexpr int kFusedTileBase = 7, kTileVariants = 9;
 template <typename T>
 bool tile_supported(int variant);
 template <typename T>

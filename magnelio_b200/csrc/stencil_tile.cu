@@ -492,6 +492,8 @@ bool tile_dispatch(int variant, F&& f) {
         case 4: f.template run<4, 5, 3>(); return true;
         case 5: f.template run<8, 3, 2>(); return true;
         case 6: f.template run<2, 4, 6>(); return true;
+        case 7: f.template run<3, 3, 6>(); return true;
+        case 8: f.template run<2, 3, 8>(); return true;
         default: return false;
     }
 }

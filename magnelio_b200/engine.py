@@ -403,6 +403,12 @@ class FitEngine:
     def sync(self) -> None:
         check(self._lib.fitb_sync(self._h))
 
+    def query(self) -> bool:
+        """True when every step issued so far has finished (non-blocking)."""
+        done = C.c_int32()
+        check(self._lib.fitb_query(self._h, C.byref(done)))
+        return bool(done.value)
+
     def step_timed(self, n: int) -> float:
         """Advance ``n`` steps; device milliseconds from CUDA events on the
         engine's stream."""

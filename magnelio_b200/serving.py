@@ -11,9 +11,10 @@ advance together in every launch and read the coefficients once per cell
 * keeps every admitted mesh, its fields and its histories resident on the
   device until its last step;
 * advances all admitted handles in slices of steps, each handle on its own
-  CUDA stream, so the work of different requests overlaps on the GPU, and
-  admits new arrivals between slices (requests join and leave the running
-  set continuously);
+  CUDA stream, so the work of different requests overlaps on the GPU; a
+  handle gets its next slice as soon as its last one has finished (polled,
+  non-blocking), and new arrivals are admitted whenever a slice ends
+  (requests join and leave the running set continuously);
 * on completion reads back the port voltages and currents, forms the
   S-matrix on the host and releases the device memory.
 
@@ -191,14 +192,22 @@ class ServingLoop:
                 self.sleep(max(0.0, nxt - (self.clock() - t0)))
                 continue
             active_samples.append(len(active))
-            # one slice on every admitted handle (asynchronous, own streams)
+            # a slice on every idle handle (asynchronous, own streams), then
+            # wait until at least one handle has finished its slice: a small
+            # request does not wait for the largest one's slice
             for a in active:
-                k = min(self.slice_steps, a["req"].steps - a["done"])
-                a["eng"].step(k)
-                a["k"] = k
+                if not a.get("busy"):
+                    k = min(self.slice_steps, a["req"].steps - a["done"])
+                    a["eng"].step(k)
+                    a["k"] = k
+                    a["busy"] = True
+            finished = {id(a) for a in self._wait_any(active)}
             still = []
             for a in active:
-                a["eng"].sync()
+                if id(a) not in finished:
+                    still.append(a)
+                    continue
+                a["busy"] = False
                 a["done"] += a["k"]
                 if a["done"] < a["req"].steps:
                     still.append(a)
@@ -230,6 +239,22 @@ class ServingLoop:
                             p50=float(np.percentile(lat, 50)), p99=float(np.percentile(lat, 99)),
                             mean_active=float(np.mean(active_samples)) if active_samples else 0.0,
                             peak_bytes=int(peak), results=sorted(results, key=lambda r: r.rid))
+
+    def _wait_any(self, active):
+        """The handles whose slice has finished, waiting for at least one
+        (engines without a non-blocking query are synchronised in turn)."""
+        while True:
+            done = []
+            for a in active:
+                query = getattr(a["eng"], "query", None)
+                if query is None:
+                    a["eng"].sync()
+                    done.append(a)
+                elif query():
+                    done.append(a)
+            if done:
+                return done
+            self.sleep(2e-5)
 
     @staticmethod
     def _configure(eng, form):

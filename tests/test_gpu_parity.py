@@ -115,7 +115,7 @@ def test_stencil_variants_agree(name):
     p, d, n = load_golden(name)
     outs = []
     modes = [("stream", v) for v in range(4)] + [("bulk", 0), ("simple", 0)]
-    modes += [("vec", v) for v in range(4)] + [("fused", v) for v in range(14)]
+    modes += [("vec", v) for v in range(4)] + [("fused", v) for v in range(16)]
     for kind, variant in modes:
         with p.build_engine("single") as eng:
             eng.configure_stencil(kind, variant)
@@ -545,7 +545,7 @@ def test_cross_junction_batch_equals_one_excitation_per_handle():
 # ---------------------------------------------------------------------------
 # TMA tile form of the fused step on grids of many tiles and chunks.
 
-TILE_VARIANTS = range(7, 14)
+TILE_VARIANTS = range(7, 16)
 
 
 def _random_state(prob, rng, scale=1e-3):
@@ -601,7 +601,7 @@ def test_tile_step_matches_stream_on_a_multi_tile_grid(n, precision, tol):
             assert _rel(got[2], ref[2]) < 10 * tol, (v, ichunk)
             for a, b in zip(got[3], ref[3]):
                 assert _rel(a, b) < max(10 * tol, DFT_TOL), (v, ichunk)
-    assert ran >= (14 if precision == "single" else 12)
+    assert ran >= (18 if precision == "single" else 16)
 
 
 def test_tile_step_batched_matches_the_plain_kernel():

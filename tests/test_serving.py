@@ -49,6 +49,9 @@ class ScriptedEngine:
     def sync(self):
         pass
 
+    def query(self):
+        return True  # a step costs virtual time when it is issued
+
     def read_vi(self, b):
         P = len(self.p.lumped)
         V = np.zeros((self.n, P))
