@@ -279,6 +279,13 @@ int fitb_sync(fitb_handle* h);
  * No counterpart in the reference (its loop is synchronous); the serving
  * loop uses it to keep every resident handle busy. */
 int fitb_query(fitb_handle* h, int32_t* done);
+/* Self-check of the device-side timeout path (no counterpart in the
+ * reference): one CTA waits, bounded, on an mbarrier that nothing completes,
+ * the expired wait records the timeout status (FITB_STATUS_WAIT_TIMEOUT) the
+ * pipelined kernels use, and the host reads it into *status; the handle
+ * stays usable.  No fault is involved. */
+#define FITB_STATUS_WAIT_TIMEOUT 3
+int fitb_probe_wait_timeout(fitb_handle* h, int32_t* status);
 /* fitb_step bracketed by CUDA events on the handle's stream; blocks until
  * the steps are done and returns their device time in milliseconds. */
 int fitb_step_timed(fitb_handle* h, int64_t n_steps, double* ms);

@@ -143,6 +143,7 @@ SIGNATURES = {
     "fitb_step": ([vp, i64], C.c_int),
     "fitb_sync": ([vp], C.c_int),
     "fitb_query": ([vp, C.POINTER(C.c_int32)], C.c_int),
+    "fitb_probe_wait_timeout": ([vp, C.POINTER(C.c_int32)], C.c_int),
     "fitb_step_timed": ([vp, i64, P_f64], C.c_int),
     "fitb_time_stencil": ([vp, i32, P_f64, P_f64], C.c_int),
     "fitb_steps_done": ([vp, P_i64], C.c_int),

@@ -2127,6 +2127,22 @@ int fitb_sync(fitb_handle* h) {
     FITB_CATCH
 }
 
+int fitb_probe_wait_timeout(fitb_handle* h, int32_t* status) {
+    FITB_TRY
+    Handle& H = H_of(h);
+    if (!status) fail(FITB_ERR_ARG, "null argument");
+    ck(cudaStreamSynchronize(H.stream), "probe sync");
+    ck(cudaMemsetAsync(H.status.p, 0, sizeof(int), H.stream), "probe status reset");
+    ck(fitb::launch_wait_probe(H.status.as<int>(), 1u << 16, H.stream), "wait probe launch");
+    int st = 0;
+    ck(cudaMemcpyAsync(&st, H.status.p, sizeof(int), cudaMemcpyDeviceToHost, H.stream), "probe status D2H");
+    ck(cudaStreamSynchronize(H.stream), "probe sync");
+    ck(cudaMemsetAsync(H.status.p, 0, sizeof(int), H.stream), "probe status reset");
+    ck(cudaStreamSynchronize(H.stream), "probe sync");
+    *status = st;
+    FITB_CATCH
+}
+
 int fitb_query(fitb_handle* h, int32_t* done) {
     FITB_TRY
     Handle& H = H_of(h);

@@ -160,6 +160,9 @@ template <typename T>
 int launch_tile_cpml_E(const StencilArgs<T>& a, cudaStream_t s);
 template <typename T>
 int launch_tile_cpml_H(const StencilArgs<T>& a, cudaStream_t s);
+// One CTA waits, bounded by `limit` tries, on an mbarrier that nothing
+// completes; the expired wait writes kStatusWaitTimeoutTile to *status.
+cudaError_t launch_wait_probe(int* status, unsigned limit, cudaStream_t s);
 // Whether the tile step takes this grid and CPML layout.
 template <typename T>
 bool tile_step_fits(const StencilArgs<T>& a);

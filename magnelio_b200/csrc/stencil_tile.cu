@@ -481,6 +481,18 @@ __global__ void __launch_bounds__(kPassThreads) k_tile_fix_boxes(const StencilAr
     Hn[2 * vol + o] = hz;
 }
 
+// Probe of the bounded wait: an mbarrier that nothing completes, waited on
+// with `limit` tries; the expired wait sets *status and the kernel returns.
+__global__ void k_wait_probe(int* status, unsigned limit) {
+    __shared__ unsigned long long bar;
+    if (threadIdx.x != 0) return;
+    tbar_init(&bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    for (unsigned n = 0; n < limit; ++n)
+        if (tbar_try(&bar, 0u)) return;
+    atomicExch(status, kStatusWaitTimeoutTile);
+}
+
 // Tile variants: (TJ, NS, min CTAs per SM).
 template <typename T, typename F>
 bool tile_dispatch(int variant, F&& f) {
@@ -637,6 +649,11 @@ bool pass_boxes(PassBoxes& bx, const Geom& g, const FaceDev* f, int nfaces, bool
 }
 
 }  // namespace
+
+cudaError_t launch_wait_probe(int* status, unsigned limit, cudaStream_t s) {
+    k_wait_probe<<<1, 32, 0, s>>>(status, limit);
+    return cudaGetLastError();
+}
 
 template <typename T>
 bool tile_supported(int variant) {

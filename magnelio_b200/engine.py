@@ -403,6 +403,13 @@ class FitEngine:
     def sync(self) -> None:
         check(self._lib.fitb_sync(self._h))
 
+    def probe_wait_timeout(self) -> int:
+        """Status a bounded device wait records when it expires (a wait on an
+        mbarrier that nothing completes; diagnostic, no fault)."""
+        st = C.c_int32()
+        check(self._lib.fitb_probe_wait_timeout(self._h, C.byref(st)))
+        return int(st.value)
+
     def query(self) -> bool:
         """True when every step issued so far has finished (non-blocking)."""
         done = C.c_int32()

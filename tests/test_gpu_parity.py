@@ -618,3 +618,17 @@ def test_tile_step_batched_matches_the_plain_kernel():
         # 400 steps of a resonant guide; the reference bar is 2e-4
         assert _rel(got[0], ref[0], pe) < 1e-4, v
         assert _rel(got[2], ref[2]) < 1e-4, v
+
+
+def test_an_expired_device_wait_reports_its_status_and_the_handle_keeps_working():
+    """The bounded-wait path of the pipelined kernels without any fault: a
+    wait on an mbarrier that nothing completes expires, records the timeout
+    status, the host reads it, and the handle then steps as before."""
+    p, d, n = load_golden("lumped_dft")
+    with p.build_engine("single") as eng:
+        assert eng.probe_wait_timeout() == 3
+        eng.configure_stencil("fused", 7)
+        eng.step(n)
+        e, h = eng.read_fields()
+    pe, _ph = _peaks("lumped_dft")
+    assert _rel(e, d["out.e"], pe) < F32_TOL
