@@ -57,7 +57,6 @@ __device__ __forceinline__ void load_plane(FPlane<T>& q, const StencilArgs<T>& p
     load_coef3(q.ch, p.aH, p.bH, o, vol);
 }
 
-
 constexpr unsigned kAll = 0xffffffffu;
 
 template <typename T, int TJ>
