@@ -645,7 +645,7 @@ int launch_fused(Handle& H, const StencilArgs<T>& sa) {
         if (launch_tile_step<T>(sa, H.splan, H.fused_variant - kFusedTileBase, H.status.as<int>(), H.stream) != 0)
             fail(FITB_ERR_CUDA, "tensor maps of the tile step could not be encoded");
         const int ne = launch_tile_cpml_E<T>(sa, H.stream);
-        if (ne < 0) fail(FITB_ERR_STATE, "the tile step does not take this CPML layout");
+        if (ne < 0) fail(FITB_ERR_STATE, "the tile step does not take this grid / CPML layout");
         return 1 + ne;
     }
     launch_fused_step<T>(sa, H.splan, H.fused_variant, H.stream);
@@ -717,7 +717,7 @@ int enqueue_step_fused(Handle& H) {
     }
     if (H.fused_variant >= kFusedTileBase) {
         const int nh = launch_tile_cpml_H<T>(sa, H.stream);
-        if (nh < 0) fail(FITB_ERR_STATE, "the tile step does not take this CPML layout");
+        if (nh < 0) fail(FITB_ERR_STATE, "the tile step does not take this grid / CPML layout");
         n += nh;
     }
     if (H.n_fix > 0) {

@@ -154,8 +154,9 @@ StreamPlan plan_tile(const Geom& g, int sm_count, int ctas_per_sm, int B, int va
 // maps cannot be encoded.  status: set non-zero when a bounded wait expires.
 template <typename T>
 int launch_tile_step(StencilArgs<T> a, const StreamPlan& sp, int variant, int* status, cudaStream_t s);
-// Both return the number of launches issued (< 0: more pass boxes than
-// the table holds, which tile_step_fits rules out beforehand).
+// Both return the number of launches issued (< 0: a grid too large for
+// their 32-bit offsets or more pass boxes than the table holds, which
+// tile_step_fits rules out beforehand).
 template <typename T>
 int launch_tile_cpml_E(const StencilArgs<T>& a, cudaStream_t s);
 template <typename T>

@@ -510,7 +510,7 @@ bool tile_dispatch(int variant, F&& f) {
     }
 }
 
-constexpr size_t kMaxSmem = 232448;  // 227 KB opt-in per CTA
+constexpr size_t kMaxSmem = 232448;  // B200 opt-in per CTA (227 KB), when the device cannot be queried
 
 template <typename T>
 struct TileInfo {
@@ -658,7 +658,14 @@ cudaError_t launch_wait_probe(int* status, unsigned limit, cudaStream_t s) {
 template <typename T>
 bool tile_supported(int variant) {
     TileInfo<T> f;
-    return tile_dispatch<T>(variant, f) && f.smem <= kMaxSmem;
+    if (!tile_dispatch<T>(variant, f)) return false;
+    // the current device's opt-in limit per block (B200: 227 KB)
+    int dev = 0, optin = 0;
+    size_t limit = kMaxSmem;
+    if (cudaGetDevice(&dev) == cudaSuccess &&
+        cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) == cudaSuccess && optin > 0)
+        limit = (size_t)optin;
+    return f.smem <= limit;
 }
 template bool tile_supported<float>(int);
 template bool tile_supported<double>(int);
@@ -739,6 +746,7 @@ template int launch_tile_step<double>(StencilArgs<double>, const StreamPlan&, in
 template <typename T>
 int launch_tile_cpml_E(const StencilArgs<T>& a, cudaStream_t s) {
     if (a.nfaces == 0) return 0;
+    if (3 * a.g.vol >= (1LL << 31)) return -1;  // 32-bit offsets in the passes
     PassBoxes bx;
     if (!pass_boxes(bx, a.g, a.f, a.nfaces, false)) return -1;
     if (bx.n == 0) return 0;
@@ -751,6 +759,7 @@ template int launch_tile_cpml_E<double>(const StencilArgs<double>&, cudaStream_t
 template <typename T>
 int launch_tile_cpml_H(const StencilArgs<T>& a, cudaStream_t s) {
     if (a.nfaces == 0) return 0;
+    if (3 * a.g.vol >= (1LL << 31)) return -1;  // 32-bit offsets in the passes
     PassBoxes bx;
     if (!pass_boxes(bx, a.g, a.f, a.nfaces, true)) return -1;
     if (bx.n == 0) return 0;
