@@ -87,3 +87,11 @@ def test_apply_configures_the_engine():
     autotune.apply(eng, autotune.TuneResult("vec", 2, 24, 1, 1.0, 1.0))
     assert eng.cfg == ("vec", 2, 24)
     assert np.isfinite(1.0)
+
+
+def test_cache_keys_name_the_candidate_set():
+    """A result tuned over another candidate set is not reused: the key
+    carries the set's version."""
+    k = autotune.cache_key(64, 64, 64, 1, "single", "native", 6, "B200")
+    assert k.endswith(f"|c{autotune.CANDIDATE_SET}")
+    assert ("fused", 7, 0) in autotune.DEFAULT_CANDIDATES  # the tile form is tuned

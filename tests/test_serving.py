@@ -163,3 +163,28 @@ def test_footprint_estimate_counts_the_big_buffers():
     assert fpf - fp == 2 * 4 * 3 * vol * 4 + 2 * 4 * 4 * (65 * 65 * 8) * 4
     with pytest.raises(TypeError):
         serving.estimate_footprint(64, 64)
+
+
+def test_each_form_gets_its_stencil_and_a_refusal_keeps_the_default():
+    """Single-excitation handles go on the tile step, batched ones keep the
+    default kernels; a handle that refuses the form keeps its default."""
+    from magnelio_b200._lib import FitbError
+
+    assert serving.serving_stencil(1) == ("fused", 7)
+    assert serving.serving_stencil(3) is None
+
+    class Eng:
+        def __init__(self, refuse):
+            self.refuse = refuse
+            self.form = None
+
+        def configure_stencil(self, kind, variant):
+            if self.refuse:
+                raise FitbError(-4, "dispersive materials need an in-place stencil mode")
+            self.form = (kind, variant)
+
+    ok, no = Eng(False), Eng(True)
+    serving.ServingLoop._configure(ok, ("fused", 7))
+    serving.ServingLoop._configure(no, ("fused", 7))
+    serving.ServingLoop._configure(Eng(False), None)
+    assert ok.form == ("fused", 7) and no.form is None
