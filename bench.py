@@ -149,7 +149,9 @@ def _max_over_ranks(x: float, world: int, local: int) -> float:
     import torch
     import torch.distributed as dist
 
-    t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
+    # NCCL reduces on the rank's GPU; gloo (the CPU tests of this path) on the host
+    device = "cpu" if dist.get_backend() == "gloo" else f"cuda:{local}"
+    t = torch.tensor([x], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
@@ -223,7 +225,7 @@ def _config(args, prob):
     }
 
 
-def main() -> int:
+def main(argv=None) -> int:
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=2000)
@@ -247,7 +249,9 @@ def main() -> int:
                     help="scale factor on the request grid sizes and step counts (1 = the full stream)")
     ap.add_argument("--coef", choices=("native", "f16", "bf16"), default="native",
                     help="coefficient storage of the stencil kernels (16-bit forms round the coefficients)")
-    args = ap.parse_args()
+    ap.add_argument("--dist-backend", choices=("nccl", "gloo"), default="nccl",
+                    help="process-group backend for N > 1 (gloo: host-only runs of the replica path)")
+    args = ap.parse_args(argv)
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
     world, rank, local = _dist()
@@ -255,8 +259,9 @@ def main() -> int:
         import torch
         import torch.distributed as dist
 
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        if args.dist_backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(args.dist_backend, timeout=datetime.timedelta(seconds=120))
     try:
         if args.impl == "reference":
             return run_reference(args, world, rank, local)
