@@ -5,7 +5,9 @@ the B200 engine.  Importing this module needs the ``magnelio`` package.
 ``setup()`` (the reference's own host build of every constant, on the CPU
 backend), ``run()`` semantics (stop criteria, runtime cap, graceful stop,
 result attributes ``_fields``, ``_actual_steps``, ``_stop_reason``,
-``_energy_trace``, ``_final_signal_db``) and fills the same recorder and
+``_energy_trace``, ``_final_signal_db``), ``state_dict()`` /
+``load_state_dict()`` (carrying the engine's device state) and fills the
+same recorder and
 monitor objects the analysis reads afterwards
 (``src/magnelio/solver/fit_td.py:135-1386``).  The per-step work runs on the
 device: the engine is the only marching path, there is no CPU fallback.
@@ -43,6 +45,7 @@ class B200FITSolver(FITTimeDomainSolver):
     _horizon: int = field(default=0, repr=False, init=False)
     _steps_recorded: int = field(default=0, repr=False, init=False)
     _mon_base: list = field(default_factory=list, repr=False, init=False)
+    _device_state: bytes | None = field(default=None, repr=False, init=False)
 
     # ---- setup ---------------------------------------------------------
     def setup(self) -> None:
@@ -66,14 +69,24 @@ class B200FITSolver(FITTimeDomainSolver):
     def _build(self, horizon: int) -> None:
         prob = problem_from_solver(self, horizon)
         eng = prob.build_engine(self._precision(), device=self.device, max_steps=horizon)
-        # The engine counts steps from 0; a resumed solver starts further on.
+        # The engine counts steps from 0; a resumed solver starts further on,
+        # from the device state its checkpoint carries.
         if self._resume_step:
-            raise NotImplementedError(
-                "resuming a B200FITSolver from a reference checkpoint is not supported yet; "
-                "use FitEngine.state_export / state_import for device checkpoints"
-            )
+            if self._device_state is None:
+                eng.close()
+                raise NotImplementedError(
+                    "resuming a B200FITSolver needs a checkpoint from B200FITSolver.state_dict() (it carries the "
+                    "device state); a reference checkpoint holds no ADE / DFT / recorder state of the engine"
+                )
+            eng.state_import(self._device_state)
+            if eng.steps_done != self._resume_step:
+                eng.close()
+                raise ValueError(f"checkpoint device state is at step {eng.steps_done}, "
+                                 f"its n_completed is {self._resume_step}")
+            self._device_state = None
         self._engine, self._problem, self._horizon = eng, prob, horizon
-        self._steps_recorded = 0
+        # the recorder continues at the resume point, like the reference's
+        self._steps_recorded = self._resume_step
         self._mon_base = [
             {c: np.array(mon._accumulators[c]._bins, copy=True) for c in mon._components} for mon in self.monitors
         ]
@@ -124,6 +137,49 @@ class B200FITSolver(FITTimeDomainSolver):
         self._stop_requested = True
         if self._loop is not None:
             self._loop.request_stop()
+
+    # ---- checkpoint / resume (fit_td.py:1264-1353) -----------------------
+    def state_dict(self) -> dict:
+        """Checkpoint of the march for a bit-exact resume.
+
+        Same schema as the reference's (``n_completed``, the energy and
+        signal peaks, ``e`` / ``h``) plus ``"b200_state"``: the engine's own
+        export of every evolving device state (fields, CPML psi, port and
+        DTBC histories, ADE pole states, DFT bins, step count).  The
+        reference's ``boundaries`` / ``ports`` groups stay empty: those
+        states live on the device, not in the host objects.  Because the
+        DFT bins are in the device state, a resumed run's frequency monitors
+        cover the whole run (the reference keeps no frequency-monitor state
+        in its checkpoints).
+        """
+        if self._engine is None:
+            return super().state_dict()
+        return {
+            "n_completed": int(self._resume_step),
+            "peak_energy": float(self._peak_energy),
+            "peak_signal": float(self._peak_signal),
+            "e": self._fields.e_flat.copy(),
+            "h": self._fields.h_flat.copy(),
+            "boundaries": {},
+            "ports": {},
+            "b200_state": self._engine.state_export(),
+        }
+
+    def load_state_dict(self, state: dict) -> None:
+        """Restore a checkpoint of :meth:`state_dict` (the solver built
+        identically); the next :meth:`run` continues from ``n_completed``."""
+        if "b200_state" not in state:
+            super().load_state_dict(state)
+            return
+        if self._fields is None:
+            self.setup()
+        self._close_engine()
+        self._fields.e_flat[:] = np.asarray(state["e"], dtype=self._fields.e_flat.dtype)
+        self._fields.h_flat[:] = np.asarray(state["h"], dtype=self._fields.h_flat.dtype)
+        self._peak_energy = float(state["peak_energy"])
+        self._peak_signal = float(state.get("peak_signal", 0.0))
+        self._resume_step = int(state["n_completed"])
+        self._device_state = bytes(state["b200_state"])
 
     # ---- results back into the reference objects -------------------------
     def _sync_results(self, res) -> None:

@@ -68,6 +68,22 @@ class OracleEngine:
     def read_dft(self, mon, comp, b=0):
         return self.run.mons[mon].bins[comp].copy()
 
+    def state_export(self):
+        import pickle
+
+        return pickle.dumps(self.run)
+
+    def state_import(self, blob):
+        """Evolving state from the blob, constants (source tables) from this
+        engine's problem, as the device import does."""
+        import pickle
+
+        run = pickle.loads(blob)
+        run.p = self.prob
+        for lo, lp in zip(run.lumped, self.prob.lumped):
+            lo.lp = lp
+        self.run = run
+
     def set_lumped_source(self, *a):
         raise AssertionError("bounded test runs never extend their sources")
 
@@ -142,3 +158,57 @@ def test_solver_glue_matches_reference(oracle_engine, kw):
         a = got.monitors[0]._accumulators[c].result
         b = ref.monitors[0]._accumulators[c].result
         np.testing.assert_allclose(a, b, rtol=0, atol=1e-10 * np.max(np.abs(b)))
+
+
+def test_checkpoint_and_resume_match_the_reference_resume(oracle_engine):
+    """25 steps, state_dict, a fresh solver loads it and runs to 60: fields,
+    energy and port signals equal the reference's own resume; the frequency
+    monitors, whose bins travel with the device state, equal an
+    uninterrupted 60-step run."""
+    from magnelio.solver.fit_td import FITTimeDomainSolver
+
+    from magnelio_b200.solver import B200FITSolver
+
+    def resumed(cls):
+        a = _lumped_case(cls, total_time_steps=25)
+        a.run()
+        state = a.state_dict()
+        b = _lumped_case(cls, total_time_steps=60)
+        b.load_state_dict(state)
+        b.run()
+        return state, b
+
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore")
+        state, got = resumed(B200FITSolver)
+        _rstate, ref = resumed(FITTimeDomainSolver)
+        whole = _lumped_case(B200FITSolver, total_time_steps=60)
+        whole.run()
+    assert "b200_state" in state and state["n_completed"] == 25
+    assert got._actual_steps == ref._actual_steps
+    np.testing.assert_allclose(got._fields.e_flat, ref._fields.e_flat, rtol=0,
+                               atol=1e-10 * np.max(np.abs(ref._fields.e_flat)))
+    np.testing.assert_array_equal(got._fields.e_flat, whole._fields.e_flat)
+    key = ("src", 0)
+    assert len(got.recorder._V_buffers[key]) == len(ref.recorder._V_buffers[key]) == 35
+    np.testing.assert_allclose(got.recorder._V_buffers[key], ref.recorder._V_buffers[key], rtol=1e-10, atol=1e-20)
+    np.testing.assert_allclose(got._energy_trace["energy"], ref._energy_trace["energy"], rtol=1e-10)
+    for c in ("Ex", "Hz"):
+        np.testing.assert_array_equal(got.monitors[0]._accumulators[c].result,
+                                      whole.monitors[0]._accumulators[c].result)
+
+
+def test_a_reference_checkpoint_is_refused(oracle_engine):
+    """A checkpoint without the device state cannot restart the engine."""
+    from magnelio.solver.fit_td import FITTimeDomainSolver
+
+    from magnelio_b200.solver import B200FITSolver
+
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore")
+        a = _lumped_case(FITTimeDomainSolver, total_time_steps=10)
+        a.run()
+        b = _lumped_case(B200FITSolver, total_time_steps=20)
+        b.load_state_dict(a.state_dict())
+        with pytest.raises(NotImplementedError, match="device state"):
+            b.run()
