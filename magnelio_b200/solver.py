@@ -100,6 +100,13 @@ class B200FITSolver(FITTimeDomainSolver):
 
     # ---- run -----------------------------------------------------------
     def run(self):
+        if self.sink is not None:
+            # the reference flushes its streaming project sink at every energy
+            # check and writes a resume checkpoint into it on a graceful stop
+            # (fit_td.py:1024-1197); the project store is not part of this
+            # engine, and dropping those writes silently would lose data
+            raise NotImplementedError("B200FITSolver does not stream to a project sink; run with sink=None "
+                                      "and write the results (or state_dict()) after run()")
         if self._fields is None:
             self.setup()
         n_steps = self.total_time_steps

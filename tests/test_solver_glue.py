@@ -212,3 +212,13 @@ def test_a_reference_checkpoint_is_refused(oracle_engine):
         b.load_state_dict(a.state_dict())
         with pytest.raises(NotImplementedError, match="device state"):
             b.run()
+
+
+def test_a_project_sink_is_refused_not_dropped(oracle_engine):
+    from magnelio_b200.solver import B200FITSolver
+
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore")
+        s = _lumped_case(B200FITSolver, total_time_steps=10, sink=object())
+        with pytest.raises(NotImplementedError, match="sink"):
+            s.run()
