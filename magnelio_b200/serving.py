@@ -201,7 +201,13 @@ class ServingLoop:
                     a["eng"].step(k)
                     a["k"] = k
                     a["busy"] = True
-            finished = {id(a) for a in self._wait_any(active)}
+            # with a slot free, a future arrival also ends the wait (its
+            # handle starts then, not when some slice ends); one that has
+            # arrived but waits for memory waits for a slice to end
+            due = None
+            if pending and len(active) < slots and pending[0][0].arrival > self.clock() - t0:
+                due = pending[0][0].arrival
+            finished = {id(a) for a in self._wait_any(active, None if due is None else t0 + due)}
             still = []
             for a in active:
                 if id(a) not in finished:
@@ -240,19 +246,22 @@ class ServingLoop:
                             mean_active=float(np.mean(active_samples)) if active_samples else 0.0,
                             peak_bytes=int(peak), results=sorted(results, key=lambda r: r.rid))
 
-    def _wait_any(self, active):
-        """The handles whose slice has finished, waiting for at least one
-        (engines without a non-blocking query are synchronised in turn)."""
+    def _wait_any(self, active, until=None):
+        """The handles whose slice has finished, waiting for at least one or
+        until the clock reaches ``until`` (then possibly none); engines
+        without a non-blocking query are synchronised in turn."""
         while True:
             done = []
             for a in active:
+                if not a.get("busy"):
+                    continue
                 query = getattr(a["eng"], "query", None)
                 if query is None:
                     a["eng"].sync()
                     done.append(a)
                 elif query():
                     done.append(a)
-            if done:
+            if done or (until is not None and self.clock() >= until):
                 return done
             self.sleep(2e-5)
 

@@ -188,3 +188,62 @@ def test_each_form_gets_its_stencil_and_a_refusal_keeps_the_default():
     serving.ServingLoop._configure(no, ("fused", 7))
     serving.ServingLoop._configure(Eng(False), None)
     assert ok.form == ("fused", 7) and no.form is None
+
+
+class AsyncEngine(ScriptedEngine):
+    """Steps run in the background of the virtual clock: a slice issued at
+    t finishes at t + cost (handles overlap fully), query() polls it."""
+
+    def __init__(self, prob, clock, cost_per_cell_step=1e-9):
+        super().__init__(prob, clock, cost_per_cell_step)
+        self.ready_at = 0.0
+
+    def step(self, k):
+        self.n += k
+        self.ready_at = max(self.ready_at, self.clock.t) + self.cost * k
+
+    def query(self):
+        return self.clock.t >= self.ready_at
+
+
+def test_overlapping_handles_finish_independently_and_arrivals_start_on_time():
+    """With slices that overlap on the device, a small request completes
+    while a large one is still running, and a request arriving while every
+    resident handle is busy starts at its arrival, not at the next slice
+    end."""
+    clock = Clock()
+    loop = serving.ServingLoop(engine_factory=lambda p, prec, dev: AsyncEngine(p, clock), clock=clock,
+                               sleep=clock.sleep, max_slots=4, slice_steps=50, hbm_budget=1 << 40,
+                               stencil=None)
+    big = serving.request_stream(1, seed=3, mean_gap=1e-6, cells=(20**3, 20**3), steps=(400, 400), ports=(2, 2),
+                                 n_freq=5)[0]
+    small = serving.request_stream(1, seed=4, mean_gap=1e-6, cells=(8**3, 8**3), steps=(100, 100), ports=(2, 2),
+                                   n_freq=5)[0]
+    small.rid = 1
+    small.arrival = 0.5 * (big.steps * 2 * 20**3 * 1e-9) / 8  # during the big request's first slices
+    stats = loop.run([big, small])
+    res = {r.rid: r for r in stats.results}
+    assert set(res) == {big.rid, 1}
+    assert res[1].admitted - small.arrival < 5e-5          # started on arrival (a slice lasts 8e-4 s)
+    assert res[1].finished < res[big.rid].finished          # did not wait for the big one
+    for r in res.values():
+        assert r.V.shape[0] == 2 and r.V.shape[1] == (400 if r.rid == big.rid else 100)
+        assert np.isfinite(r.S).all()
+
+
+@pytest.mark.timeout(30)
+def test_a_request_waiting_for_memory_does_not_spin_the_loop():
+    """An arrived request that the memory budget holds back waits for a
+    slice to end.  A loop that polled without sleeping here would never
+    advance the virtual clock the slices finish on, and the test would run
+    into its timeout."""
+    clock = Clock()
+    reqs = serving.request_stream(3, seed=5, mean_gap=1e-6, cells=(16**3, 16**3), steps=(300, 300), ports=(2, 2),
+                                  n_freq=5)
+    one = serving._footprint_of(reqs[0].build(None), 300, "single")
+    loop = serving.ServingLoop(engine_factory=lambda p, prec, dev: AsyncEngine(p, clock), clock=clock,
+                               sleep=clock.sleep, max_slots=4, slice_steps=50, hbm_budget=int(1.5 * one),
+                               stencil=None)
+    stats = loop.run(reqs)
+    assert stats.n == 3 and stats.peak_bytes <= int(1.5 * one)
+    assert stats.mean_active <= 1.0 + 1e-9  # the budget admits one request at a time
