@@ -302,7 +302,10 @@ def run_serving(args, world, rank, local):
             "data": "synthetic (seeded waveguide-section request stream)",
             "config": {"workload": "serving_stream", "requests": len(reqs), "arrivals": "Poisson, mean gap 20 ms",
                        "cells": list(cells), "steps": list(steps), "ports": "2-4 lumped, 50 ohm",
-                       "max_slots": 8, "slice_steps": 512},
+                       "max_slots": 8, "slice_steps": 512,
+                       "stencil": {"batched": str(serving.serving_stencil(2) or "engine default (batched two-pass)"),
+                                   "plain": str(serving.serving_stencil(1) or "engine default")},
+                       "coefficients": "float32"},
             "p50_s": batched.p50, "p99_s": batched.p99, "wall_s": batched.wall,
             "mean_active": batched.mean_active, "peak_device_bytes": batched.peak_bytes,
             "plain": plain.summary(), "ratio_vs_plain": batched.solves_per_s / max(plain.solves_per_s, 1e-12),
