@@ -106,8 +106,14 @@ class ClockSampler:
         except subprocess.TimeoutExpired:
             self.proc.kill()
             out, _ = self.proc.communicate()
+        return self.summarise(out.strip().splitlines(), self.t0, self.t1)
+
+    @staticmethod
+    def summarise(lines, t0, t1) -> dict:
+        """Median SM clock, max clock and active throttle reasons of the
+        csv ``lines`` (timestamp first) taken between ``t0`` and ``t1``."""
         rows = []
-        for line in out.strip().splitlines():
+        for line in lines:
             parts = [x.strip() for x in line.split(",")]
             if len(parts) < 10:
                 continue
@@ -118,10 +124,10 @@ class ClockSampler:
                 continue
         inside = rows
         where = "timed region"
-        if self.t0 is not None and self.t1 is not None and rows:
-            inside = [r for r in rows if self.t0 <= r[0] <= self.t1]
+        if t0 is not None and t1 is not None and rows:
+            inside = [r for r in rows if t0 <= r[0] <= t1]
             if not inside:
-                mid = self.t0 + (self.t1 - self.t0) / 2
+                mid = t0 + (t1 - t0) / 2
                 inside = [min(rows, key=lambda r: abs((r[0] - mid).total_seconds()))]
                 where = "nearest to the timed region (shorter than the 50 ms sampling interval)"
         names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
