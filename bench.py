@@ -191,6 +191,30 @@ def cpu_port_rate(prob, budget_s: float = 20.0, max_steps: int = 200, warmup: in
     return cells * n / dt / 1e9, n, dt, threads
 
 
+def parity_prefix(prob, tuned, steps: int, device: int) -> dict:
+    """Checker line: the timed workload's first ``steps`` steps on the
+    engine (the tuned stencil, float32) against the float64 C port of the
+    reference step on the host cores (``oracle/prefix_parity.py``)."""
+    from oracle.prefix_parity import Fp64Prefix
+
+    t0 = time.perf_counter()
+    ref = Fp64Prefix(prob, steps)
+    eng = prob.build_engine("single", device=device)
+    try:
+        if tuned is not None:
+            from magnelio_b200 import autotune
+
+            autotune.apply(eng, tuned)
+        eng.step(steps)
+        e, h = eng.read_fields()
+        out = ref.compare(e, h, eng.read_dft)
+        out["stencil"] = eng.stencil_config()
+    finally:
+        eng.close()
+    out["seconds"] = round(time.perf_counter() - t0, 1)
+    return out
+
+
 def run_reference(args, world, rank, local):
     if rank != 0:
         return 0
@@ -241,6 +265,8 @@ def main(argv=None) -> int:
     ap.add_argument("--batch", type=int, default=1, help="field sets sharing one coefficient set")
     ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of CPU-port timing")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--parity-steps", type=int, default=300,
+                    help="steps of the float64 parity prefix on the timed workload (0: none)")
     ap.add_argument("--no-tune", action="store_true", help="skip the autotuner (keep the default stencil plan)")
     ap.add_argument("--workload", choices=("brick_box", "slab", "cross"), default="brick_box",
                     help="brick_box (plain method at scale), slab (dispersive slab, TF/SF plane wave, 384x384x192) "
@@ -553,11 +579,14 @@ def run_b200(args, world, rank, local):
     eng.close()
 
     cpu = None
+    parity = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline and B == 1:
         rate, ns, secs, threads = cpu_port_rate(prob, budget_s=args.cpu_budget)
         cpu = {"value": rate, "unit": METRIC, "cores": threads, "kind": "port",
                "sample": f"{ns} full steps of the {n}^3 workload after 2 warm-up steps "
                          f"(C+OpenMP port, float32, {threads} threads, {secs:.1f} s)"}
+        if args.parity_steps > 0:
+            parity = parity_prefix(prob, tuned, args.parity_steps, local)
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
@@ -565,7 +594,7 @@ def run_b200(args, world, rank, local):
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded brick box, host-built coefficients)",
             "config": dict(_config(args, prob), stencil=stencil_cfg,
                            autotune=None if tuned is None else [list(r[:3]) + [round(r[4], 4)] for r in tuned.table]),
-            "roofline": roofline, "cpu_baseline": cpu,
+            "roofline": roofline, "cpu_baseline": cpu, "parity": parity,
             "e2e": {"value": e2e, "unit": METRIC, "h2d_bytes_per_step": 8, "d2h_bytes_per_step": 16 * nch,
                     "how": "per step: pinned H2D of the source sample, one fitb_step, D2H of the step's V/I"},
             "gpu_launches": launches, "clocks": clocks,

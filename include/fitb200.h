@@ -312,7 +312,10 @@ int fitb_energy(fitb_handle* h, int32_t b, double* out);
  * at most 131072 * 4096 elements per (e, h) pair are accepted; larger
  * sizes return FITB_ERR_LIMIT.  The first call on a device looks the array
  * up (cudaGetSymbolAddress) and should come before any stream capture.
- * Calls share the array: calls whose work overlaps on the GPU race. */
+ * Calls share the array: calls whose work overlaps on the GPU race.  A CUDA
+ * error still pending from earlier work on the calling thread makes the call
+ * return FITB_ERR_CUDA without launching anything (the error is left for its
+ * owner to read). */
 int fitb_energy_noalloc(const void* e, const void* h, const void* m_eps, const void* m_mu,
                         int64_t n_e, int64_t n_h, int32_t precision, double* out, void* stream);
 /* max |V| * record_scale over all modal ports of field set b since the last

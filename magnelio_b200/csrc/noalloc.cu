@@ -20,6 +20,9 @@
 //     partial sums: serialise them.
 //   * The array keeps the previous call's contents; each call writes every
 //     slot it later reads, so nothing has to start at zero.
+//   * A CUDA error still pending from earlier work on the calling thread
+//     makes the call fail without launching; the error is left in place for
+//     the code that caused it.
 #include <cuda_runtime.h>
 
 #include <cstdio>
@@ -96,9 +99,11 @@ extern "C" int fitb_energy_noalloc(const void* e, const void* h, const void* m_e
                                    void* stream) {
     if (precision != 4 && precision != 8) return fail_with(FITB_ERR_ARG, "precision must be 4 or 8");
     if (n_e < 0 || n_h < 0) return fail_with(FITB_ERR_ARG, "array lengths must be >= 0");
-    const long long nb_e = (n_e + kItemsPerBlock - 1) / kItemsPerBlock;
-    const long long nb_h = (n_h + kItemsPerBlock - 1) / kItemsPerBlock;
-    if (nb_e + nb_h > kMaxPartials) {
+    // block counts without rounding overflow: lengths near INT64_MAX must
+    // still end in the limit error below
+    const long long nb_e = n_e / kItemsPerBlock + (n_e % kItemsPerBlock != 0);
+    const long long nb_h = n_h / kItemsPerBlock + (n_h % kItemsPerBlock != 0);
+    if (nb_e > kMaxPartials || nb_h > kMaxPartials || nb_e + nb_h > kMaxPartials) {
         char buf[256];
         snprintf(buf, sizeof(buf),
                  "fitb_energy_noalloc: n_e + n_h needs %lld partial sums, the fixed scratch holds %d "
@@ -108,8 +113,18 @@ extern "C" int fitb_energy_noalloc(const void* e, const void* h, const void* m_e
     }
     if (!out || (n_e > 0 && (!e || !m_eps)) || (n_h > 0 && (!h || !m_mu)))
         return fail_with(FITB_ERR_ARG, "fitb_energy_noalloc: null device pointer");
+    // An error left by earlier work on this thread is the caller's: report
+    // it without launching and without clearing it.
+    cudaError_t err = cudaPeekAtLastError();
+    if (err != cudaSuccess) {
+        char buf[256];
+        snprintf(buf, sizeof(buf),
+                 "fitb_energy_noalloc: a CUDA error from earlier work is pending (%s); nothing was launched",
+                 cudaGetErrorString(err));
+        return fail_with(FITB_ERR_CUDA, buf);
+    }
     int dev = 0;
-    cudaError_t err = cudaGetDevice(&dev);
+    err = cudaGetDevice(&dev);
     if (err != cudaSuccess) return fail_with(FITB_ERR_CUDA, cudaGetErrorString(err));
     if (dev < 0 || dev >= kMaxDevices) return fail_with(FITB_ERR_LIMIT, "device ordinal beyond the supported range");
     double* partials = nullptr;
@@ -124,15 +139,30 @@ extern "C" int fitb_energy_noalloc(const void* e, const void* h, const void* m_e
         partials = g_partials_addr[dev];
     }
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    if (precision == 4) {
-        if (nb_e) k_energy_blocks<float><<<(int)nb_e, kThreads, 0, s>>>((const float*)e, (const float*)m_eps, n_e, partials);
-        if (nb_h) k_energy_blocks<float><<<(int)nb_h, kThreads, 0, s>>>((const float*)h, (const float*)m_mu, n_h, partials + nb_e);
-    } else {
-        if (nb_e) k_energy_blocks<double><<<(int)nb_e, kThreads, 0, s>>>((const double*)e, (const double*)m_eps, n_e, partials);
-        if (nb_h) k_energy_blocks<double><<<(int)nb_h, kThreads, 0, s>>>((const double*)h, (const double*)m_mu, n_h, partials + nb_e);
+    // each launch's own error, checked right after it
+    auto launched = [](const char* what) {
+        const cudaError_t le = cudaGetLastError();
+        if (le == cudaSuccess) return true;
+        char buf[256];
+        snprintf(buf, sizeof(buf), "fitb_energy_noalloc: %s launch failed: %s", what, cudaGetErrorString(le));
+        fitb::set_last_error(buf);
+        return false;
+    };
+    if (nb_e) {
+        if (precision == 4)
+            k_energy_blocks<float><<<(int)nb_e, kThreads, 0, s>>>((const float*)e, (const float*)m_eps, n_e, partials);
+        else
+            k_energy_blocks<double><<<(int)nb_e, kThreads, 0, s>>>((const double*)e, (const double*)m_eps, n_e, partials);
+        if (!launched("E partial sums")) return FITB_ERR_CUDA;
+    }
+    if (nb_h) {
+        if (precision == 4)
+            k_energy_blocks<float><<<(int)nb_h, kThreads, 0, s>>>((const float*)h, (const float*)m_mu, n_h, partials + nb_e);
+        else
+            k_energy_blocks<double><<<(int)nb_h, kThreads, 0, s>>>((const double*)h, (const double*)m_mu, n_h, partials + nb_e);
+        if (!launched("H partial sums")) return FITB_ERR_CUDA;
     }
     k_energy_finish<<<1, kThreads, 0, s>>>(partials, (int)(nb_e + nb_h), out);
-    err = cudaGetLastError();
-    if (err != cudaSuccess) return fail_with(FITB_ERR_CUDA, cudaGetErrorString(err));
+    if (!launched("final sum")) return FITB_ERR_CUDA;
     return FITB_OK;
 }

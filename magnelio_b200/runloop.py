@@ -13,6 +13,7 @@ request is honoured at the next check point.
 
 from __future__ import annotations
 
+import collections
 import itertools
 import math
 import warnings
@@ -25,39 +26,54 @@ STALL_MIN_WINDOW_CHECKS = 10
 
 
 class SignalStallDetector:
-    """Proves the port-signal threshold unreachable before the runtime cap
-    by a least-squares line through the last ``window`` envelope samples
-    (``fit_td.py:76-132``)."""
+    """Runtime-cap watchdog of the port-signal stop (the behaviour of the
+    reference's ``_SignalStallDetector``, ``fit_td.py:76-132``), for runs
+    that do not go through the reference package.
+
+    Contract, which the stop decisions of the run loop depend on:
+
+    * a sample is ``(step, level)``, the |V| envelope in dB relative to the
+      running peak;
+    * a level above ``-arm_db`` disarms the watchdog and forgets its window;
+    * armed samples fill a window of the last ``window`` of them; until it
+      is full the watchdog abstains;
+    * with a full window, ``slope`` is the least-squares slope of level over
+      step (``numpy.polyfit`` of degree 1).  The watchdog abstains when the
+      last level already sits at or below the threshold, fires when the
+      slope is zero or positive, and otherwise fires when the extrapolated
+      crossing ``step + (threshold - level) / slope`` lies beyond
+      ``cap_step``.
+
+    The drop-in solver hands the reference's own class to the run loop, so
+    its decisions there are the reference's by construction.
+    """
 
     def __init__(self, arm_db: float, window: int, cap_step: int) -> None:
         self.arm_db = float(arm_db)
         self.window = max(int(window), 2)
         self.cap_step = int(cap_step)
         self.slope_db_per_step: float | None = None
-        self._samples: list[tuple[int, float]] = []
+        self._recent: collections.deque = collections.deque(maxlen=self.window)
 
     def reset(self) -> None:
-        self._samples.clear()
+        """A new envelope peak: the decay being watched starts over."""
+        self._recent.clear()
 
     def observe(self, n: int, sig_db: float, threshold_db: float) -> bool:
+        """Whether the threshold is provably out of reach before the cap."""
         if sig_db > -self.arm_db:
-            self._samples.clear()
+            self._recent.clear()
             return False
-        self._samples.append((n, float(sig_db)))
-        if len(self._samples) > self.window:
-            del self._samples[0]
-        elif len(self._samples) < self.window:
+        self._recent.append((int(n), float(sig_db)))
+        if len(self._recent) < self.window:
             return False
-        steps = np.array([s[0] for s in self._samples], dtype=np.float64)
-        vals = np.array([s[1] for s in self._samples], dtype=np.float64)
-        slope = float(np.polyfit(steps, vals, 1)[0])
+        xy = np.array(self._recent, dtype=np.float64)
+        slope = float(np.polyfit(xy[:, 0], xy[:, 1], 1)[0])
         self.slope_db_per_step = slope
-        remaining = threshold_db - float(vals[-1])
-        if remaining >= 0.0:
+        gap = threshold_db - xy[-1, 1]
+        if gap >= 0.0:
             return False
-        if slope >= 0.0:
-            return True
-        return n + remaining / slope > self.cap_step
+        return slope >= 0.0 or n + gap / slope > self.cap_step
 
 
 @dataclass
@@ -106,6 +122,10 @@ class FitRun:
     field_set: int = 0
     verbose: bool = False
     ensure_horizon: object = None
+    # class of the runtime-cap watchdog: (arm_db, window, cap_step) -> object
+    # with reset() / observe(n, sig_db, threshold_db) / window /
+    # slope_db_per_step
+    stall_detector: object = None
     _stop_requested: bool = field(default=False, init=False)
 
     def request_stop(self) -> None:
@@ -150,7 +170,7 @@ class FitRun:
         stall = None
         if signal_stop is not None and cap_steps is not None:
             window = max(STALL_MIN_WINDOW_CHECKS, (self.port_signal_min_steps or 0) // (2 * ci))
-            stall = SignalStallDetector(STALL_ARM_DB, window, cap_steps)
+            stall = (self.stall_detector or SignalStallDetector)(STALL_ARM_DB, window, cap_steps)
         last_sig_db = None
         self._stop_requested = False
         end = n_steps if not unbounded else cap_steps  # None: open-ended

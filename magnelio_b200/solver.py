@@ -23,7 +23,7 @@ import contextlib
 from dataclasses import dataclass, field
 
 import numpy as np
-from magnelio.solver.fit_td import FITTimeDomainSolver
+from magnelio.solver.fit_td import FITTimeDomainSolver, _SignalStallDetector
 
 from magnelio_b200.adapter import problem_from_solver, refresh_sources
 from magnelio_b200.runloop import FitRun, horizon_after
@@ -130,6 +130,8 @@ class B200FITSolver(FITTimeDomainSolver):
             has_modal_ports=bool(self._problem.modal),
             verbose=self.verbose,
             ensure_horizon=self._ensure_horizon,
+            # the reference's own watchdog: the drop-in stops where it does
+            stall_detector=_SignalStallDetector,
         )
         self._loop = loop
         self._stop_requested = False

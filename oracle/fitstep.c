@@ -277,17 +277,20 @@ static void monitor(fitc_problem *p, fitc_mon *m) {
     const double t = (double)p->n * p->dt, w = m->stride * p->dt;
     const int ni = m->i1 - m->i0, nj = m->j1 - m->j0, nk = m->k1 - m->k0;
     const int64_t cells = (int64_t)ni * nj * nk;
+    double *val = malloc(sizeof(double) * (size_t)cells);
+    double *cs = malloc(sizeof(double) * 2 * m->nf);
     for (int ci = 0; ci < m->ncomp; ++ci) {
         const int c = m->comps[ci];
         const REAL *A = comp_ptr(p, c);
         int sa, sb, sd;
         shape_of(p, c, &sa, &sb, &sd);
         const double tc = c < 3 ? t : t + 0.5 * p->dt;
-        double *cs = malloc(sizeof(double) * 2 * m->nf);
         for (int f = 0; f < m->nf; ++f) {
             cs[2 * f] = cos(m->omega[f] * tc) * w;
             cs[2 * f + 1] = sin(m->omega[f] * tc) * w;
         }
+        /* cell-centre samples first, then one contiguous pass per frequency
+           (the per-bin arithmetic is the same in either loop order) */
 #pragma omp parallel for schedule(static)
         for (int64_t cell = 0; cell < cells; ++cell) {
             const int kk = (int)(cell % nk), jj = (int)((cell / nk) % nj), ii = (int)(cell / ((int64_t)nk * nj));
@@ -303,14 +306,18 @@ static void monitor(fitc_problem *p, fitc_mon *m) {
                 default: v = 0.5 * (AT(i, j, k) / dual_w(p->dz, p->nz, k) + AT(i, j, k + 1) / dual_w(p->dz, p->nz, k + 1)); break;
             }
 #undef AT
-            double *re = m->re + (int64_t)ci * m->nf * cells, *im = m->im + (int64_t)ci * m->nf * cells;
-            for (int f = 0; f < m->nf; ++f) {
-                re[(int64_t)f * cells + cell] += cs[2 * f] * v;
-                im[(int64_t)f * cells + cell] += cs[2 * f + 1] * v;
-            }
+            val[cell] = v;
         }
-        free(cs);
+        double *re0 = m->re + (int64_t)ci * m->nf * cells, *im0 = m->im + (int64_t)ci * m->nf * cells;
+#pragma omp parallel for schedule(static) collapse(2)
+        for (int f = 0; f < m->nf; ++f)
+            for (int64_t cell = 0; cell < cells; ++cell) {
+                re0[(int64_t)f * cells + cell] += cs[2 * f] * val[cell];
+                im0[(int64_t)f * cells + cell] += cs[2 * f + 1] * val[cell];
+            }
     }
+    free(cs);
+    free(val);
 }
 
 void FN(fitc_step)(fitc_problem *p, int64_t n_steps) {
