@@ -37,6 +37,7 @@ METRIC = "Gcell-updates/s"
 BYTES_PER_CELL = 96  # E(3) H(3) read+write, alpha/beta E/H (12) read, float32
 FIELD_BYTES_PER_CELL = 48  # the field part of it, per field set
 TILE_VARIANT_BASE = 7  # fused-step variants from here on are the TMA tile form
+SLAB_VARIANT_BASE = 16  # and from here on the slab step (CPML inside the tile march)
 COEF_BYTES_PER_CELL = 48  # the coefficient part, shared by a batch of field sets
 BYTES_PER_CPML_CELL = 32  # 2 psi_E + 2 psi_H read+write per slab cell per face, float32
 
@@ -375,26 +376,45 @@ def run_cross(args, world, rank, local):
     sys.path.insert(0, str(ROOT / "tests"))
     from conftest import load_golden
 
+    from magnelio_b200 import autotune
+
     prob, _d, n_full = load_golden("cfg3_cross_full")
     steps = n_full if args.steps >= n_full else args.steps
     cells = prob.nx * prob.ny * prob.nz
     n_exc = prob.batch
-    eng = prob.build_engine("single", device=local)
-    eng.step(args.warmup)
-    eng.close()
-    eng = prob.build_engine("single", device=local)
-    ms_batched = eng.step_timed(steps)
-    stencil_cfg = eng.stencil_config()
-    eng.close()
-    ms_seq = 0.0
-    for b in range(n_exc):
+
+    def one_excitation(b):
         q = load_golden("cfg3_cross_full")[0]
         q.batch = 1
         for mp in q.modal:
             mp.excitation = [mp.excitation[b]]
         q.e0, q.h0 = [None], [None]
-        e1 = q.build_engine("single", device=local)
+        return q
+
+    tuned = tuned1 = None
+    if not args.no_tune:
+        tuned = autotune.tune_problem(prob, "single", batch_widths=(n_exc,), device=local, iters=5)
+        tuned1 = autotune.tune_problem(one_excitation(0), "single", batch_widths=(1,), device=local, iters=5)
+
+    def build(q, t):
+        e = q.build_engine("single", device=local)
+        if t is not None:
+            autotune.apply(e, t)
+        return e
+
+    eng = build(prob, tuned)
+    eng.step(args.warmup)
+    eng.close()
+    eng = build(prob, tuned)
+    ms_batched = eng.step_timed(steps)
+    stencil_cfg = eng.stencil_config()
+    units = eng.slab_units()
+    eng.close()
+    ms_seq = 0.0
+    for b in range(n_exc):
+        e1 = build(one_excitation(b), tuned1)
         ms_seq += e1.step_timed(steps)
+        stencil1 = e1.stencil_config()
         e1.close()
     ms_batched = _max_over_ranks(ms_batched, world, local)
     ms_seq = _max_over_ranks(ms_seq, world, local)
@@ -410,7 +430,10 @@ def run_cross(args, world, rank, local):
                            "gcell_updates_per_s": cells * n_exc * steps * world / (ms_seq * 1e-3) / 1e9},
             "ratio_vs_sequential": ms_seq / ms_batched,
             "config": {"workload": f"cross_junction_{prob.nx}x{prob.ny}x{prob.nz}", "field_sets": n_exc,
-                       "solve": f"all {n_exc} excitations x {solve_steps} steps", "stencil": stencil_cfg},
+                       "solve": f"all {n_exc} excitations x {solve_steps} steps", "stencil": stencil_cfg,
+                       "stencil_sequential": stencil1,
+                       "units": units if units["dead"] or sum(units["slots"]) else None,
+                       "autotune": None if tuned is None else [list(r[:3]) + [round(r[4], 4)] for r in tuned.table]},
         }
         print(json.dumps(line), flush=True)
     return 0
@@ -565,8 +588,12 @@ def run_b200(args, world, rank, local):
     alg_bytes = (FIELD_BYTES_PER_CELL * B + coef_bytes) * n**3 + BYTES_PER_CPML_CELL * B * cpml_cells
     achieved = alg_bytes / (t_pair * 1e-3) / 1e9
     peak, peak_kind = _peaks()
-    tile = stencil_cfg["kind"] == "fused" and stencil_cfg["variant"] >= TILE_VARIANT_BASE
-    if tile:
+    tile = stencil_cfg["kind"] == "fused" and TILE_VARIANT_BASE <= stencil_cfg["variant"] < SLAB_VARIANT_BASE
+    slab = stencil_cfg["kind"] == "fused" and stencil_cfg["variant"] >= SLAB_VARIANT_BASE
+    if slab:
+        kernel = "k_step_slab (one stencil step, CPML inside the march)"
+        traffic = _traffic("slab_step", n, cpml_cells) if B == 1 else None
+    elif tile:
         kernel = "k_step_tile + CPML passes (one stencil step)"
         traffic = _traffic("tile_step", n, cpml_cells) if B == 1 else None
     else:

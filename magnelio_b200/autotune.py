@@ -42,9 +42,13 @@ DEFAULT_CANDIDATES = (
     ("fused", 8, 0),
     ("fused", 9, 0),
     ("fused", 0, 0),
+    ("fused", 16, 0),
+    ("fused", 17, 0),
+    ("fused", 18, 0),
+    ("fused", 19, 0),
     ("bulk", 0, 0),
 )
-CANDIDATE_SET = 2  # bump when the candidates change: cached results of another set are not reused
+CANDIDATE_SET = 3  # bump when the candidates change: cached results of another set are not reused
 
 
 @dataclass

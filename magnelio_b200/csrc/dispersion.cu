@@ -127,8 +127,9 @@ __global__ void k_cpml_pass(const StencilArgs<T> a, int q, int side) {
          t += (long long)gridDim.x * blockDim.x) {
         const int b = (int)(t / f.slab);
         const long long s = t - (long long)b * f.slab;
-        const int c = (int)(s % f.dK);
-        const long long r = s / f.dK;
+        const int c = (int)(s % f.pk);
+        if (c >= f.dK) continue;  // row pitch padding
+        const long long r = s / f.pk;
         const int bb = (int)(r % f.dJ), aa = (int)(r / f.dJ);
         const int l = f.axis == 0 ? aa : (f.axis == 1 ? bb : c);
         const int i = f.axis == 0 ? f.lo + aa : aa;

@@ -105,6 +105,7 @@ long long round_up(long long x, long long m) { return (x + m - 1) / m * m; }
 
 struct FaceHost {
     int face = 0;
+    bool pec = false;  // some air mask entry is 0
     FaceDev dev{};
     DevBuf psi, air, bcc;
     DevBuf psi2;  // the fused step's second psi buffer
@@ -182,6 +183,15 @@ struct Handle {
     int cur = 0;
     DevBuf fix_cells;  // int4 (i, j, k, 0): H cells next to port-written E edges
     int n_fix = 0;
+    // Slab form of the fused step: unit lists by CPML face-slot count
+    DevBuf slab_units[kSlabLists];
+    int n_slab_units[kSlabLists] = {};
+    // Dead units left out of the slab step's lists (their cells need the
+    // buffer-set sync before the next step after any host write of fields)
+    DevBuf slab_dead;
+    int n_slab_dead = 0;
+    bool skip_sync = false;
+    std::vector<int4> fix_host;  // H cells next to port-written E edges (host copy)
     bool coeffs_set = false;
     std::vector<std::unique_ptr<FaceHost>> faces;
     std::vector<std::unique_ptr<LumpedHost>> lumped;
@@ -441,10 +451,13 @@ void build_fix_cells(Handle& H) {
         const long long rr = key % H.g.si;
         cells.push_back(make_int4(i, (int)(rr / H.g.sj), (int)(rr % H.g.sj), 0));
     }
+    H.fix_host = cells;
     if (cells.empty()) cells.push_back(make_int4(0, 0, 0, 0));  // keep a valid pointer
     upload(H.fix_cells, cells);
     H.n_fix = (int)keys.size();
 }
+
+void build_slab_units(Handle& H);
 
 void refresh_port_tables(Handle& H) {
     if (!H.port_tables_dirty) return;
@@ -483,6 +496,7 @@ void refresh_port_tables(Handle& H) {
     }
     upload(H.d_dft, dd);
     if (H.stencil_mode == kModeFused) build_fix_cells(H);
+    if (H.stencil_mode == kModeFused && is_slab_variant(H.fused_variant)) build_slab_units(H);
     H.dft_stage_blocks = sb;
     H.dft_flush_blocks = fb;
     H.dft_flush_smem = smem;
@@ -574,15 +588,103 @@ PortsArgs ports_args(Handle& H) {
 // only), kFusedTileBase + v the TMA tile forms whose shared memory fits.
 bool fused_variant_ok(int prec, int v) {
     if (v >= 0 && v <= 6) return !(v == 1 && prec == 8);
+    if (is_slab_variant(v))
+        return prec == 4 ? slab_supported<float>(v - kFusedSlabBase) : slab_supported<double>(v - kFusedSlabBase);
     const int t = v - kFusedTileBase;
     if (t < 0 || t >= kTileVariants) return false;
     return prec == 4 ? tile_supported<float>(t) : tile_supported<double>(t);
 }
 
 cudaError_t prepare_fused_any(int prec, int v) {
+    if (is_slab_variant(v))
+        return prec == 4 ? prepare_slab<float>(v - kFusedSlabBase) : prepare_slab<double>(v - kFusedSlabBase);
     if (v >= kFusedTileBase)
         return prec == 4 ? prepare_tile<float>(v - kFusedTileBase) : prepare_tile<double>(v - kFusedTileBase);
     return prec == 4 ? prepare_fused<float>(v) : prepare_fused<double>(v);
+}
+
+// Unit lists of the slab form for the handle's faces and march depth.
+bool slab_units_of(const Handle& H, int variant, int ichunk, std::vector<int4> out[kSlabLists]) {
+    FaceDev f[kMaxFaces];
+    const int nf = (int)H.faces.size();
+    if (nf > kMaxFaces) return false;
+    for (int q = 0; q < nf; ++q) f[q] = H.faces[q]->dev;
+    return plan_slab_units(H.g, f, nf, slab_tj_of(variant - kFusedSlabBase), ichunk, out);
+}
+
+// Dead-unit skipping of the slab step (reference: solver/_tile_skip.py,
+// on by default, MAGNELIO_TILE_SKIP=0 turns it off there; FITB_TILE_SKIP=0
+// here).  Like the reference it stays off with TF/SF plane waves (their H
+// injection can drive faces the analysis calls curl-dead).  Only units
+// without CPML are candidates (psi stays exact), and units holding a port-
+// or source-written edge or its H neighbours stay live.
+bool tile_skip_on(const Handle& H) {
+    const char* e = getenv("FITB_TILE_SKIP");
+    return !(e && std::string(e) == "0") && H.pws.empty() && !H.disp[0].present() && !H.disp[1].present();
+}
+
+void build_slab_units(Handle& H) {
+    std::vector<int4> lists[kSlabLists];
+    const int ichunk = H.splan.ichunk, tj = slab_tj_of(H.fused_variant - kFusedSlabBase);
+    if (!slab_units_of(H, H.fused_variant, ichunk, lists))
+        fail(FITB_ERR_STATE, "the slab step does not take this grid / CPML layout");
+    std::vector<int4> dead;
+    if (tile_skip_on(H) && !lists[0].empty()) {
+        const int n = (int)lists[0].size();
+        DevBuf du, fl;
+        upload(du, lists[0]);
+        fl.alloc((size_t)n * sizeof(int));
+        if (H.prec == 4)
+            slab_unit_liveness<float>(H.g, H.aE.as<float>(), H.bE.as<float>(), H.aH.as<float>(), H.bH.as<float>(), tj,
+                                      ichunk, du.as<int4>(), n, fl.as<int>(), H.stream);
+        else
+            slab_unit_liveness<double>(H.g, H.aE.as<double>(), H.bE.as<double>(), H.aH.as<double>(),
+                                       H.bH.as<double>(), tj, ichunk, du.as<int4>(), n, fl.as<int>(), H.stream);
+        ck(cudaGetLastError(), "unit liveness launch");
+        std::vector<int> flags((size_t)n);
+        ck(cudaMemcpyAsync(flags.data(), fl.p, (size_t)n * sizeof(int), cudaMemcpyDeviceToHost, H.stream),
+           "unit liveness D2H");
+        ck(cudaStreamSynchronize(H.stream), "unit liveness sync");
+        // units holding a port / source edge's H neighbours (the fix-up cells)
+        for (const int4& c : H.fix_host)
+            for (int q = 0; q < n; ++q) {
+                const int4& u = lists[0][(size_t)q];
+                const int k0 = u.x * 32, j0 = u.y * tj, i0 = u.z * ichunk;
+                if (c.x >= i0 - 1 && c.x <= i0 + ichunk && c.y >= j0 - 1 && c.y <= j0 + tj && c.z >= k0 - 1 &&
+                    c.z <= k0 + 32)
+                    flags[(size_t)q] = 1;
+            }
+        std::vector<int4> live;
+        for (int q = 0; q < n; ++q) (flags[(size_t)q] ? live : dead).push_back(lists[0][(size_t)q]);
+        lists[0].swap(live);
+    }
+    for (int q = 0; q < kSlabLists; ++q) {
+        H.n_slab_units[q] = (int)lists[q].size();
+        if (lists[q].empty()) lists[q].push_back(make_int4(0, 0, 0, 0));  // keep a valid pointer
+        upload(H.slab_units[q], lists[q]);
+    }
+    H.n_slab_dead = (int)dead.size();
+    if (dead.empty()) dead.push_back(make_int4(0, 0, 0, 0));
+    upload(H.slab_dead, dead);
+    H.skip_sync = H.n_slab_dead > 0;
+}
+
+// Makes both buffer sets agree on the skipped units' cells (after a host
+// write of fields or a new unit plan).
+void sync_dead_units(Handle& H) {
+    if (!H.skip_sync) return;
+    H.skip_sync = false;
+    if (H.stencil_mode != kModeFused || !is_slab_variant(H.fused_variant) || H.n_slab_dead == 0) return;
+    const int tj = slab_tj_of(H.fused_variant - kFusedSlabBase);
+    if (H.prec == 4)
+        slab_dead_sync<float>(H.g, H.aH.as<float>(), H.bH.as<float>(), tj, H.splan.ichunk, H.slab_dead.as<int4>(),
+                              H.n_slab_dead, H.B, H.Ec().as<float>(), H.Hc().as<float>(), H.En().as<float>(),
+                              H.Hn().as<float>(), H.stream);
+    else
+        slab_dead_sync<double>(H.g, H.aH.as<double>(), H.bH.as<double>(), tj, H.splan.ichunk, H.slab_dead.as<int4>(),
+                               H.n_slab_dead, H.B, H.Ec().as<double>(), H.Hc().as<double>(), H.En().as<double>(),
+                               H.Hn().as<double>(), H.stream);
+    ck(cudaGetLastError(), "dead unit sync launch");
 }
 
 // Grid of the stream / vec kernels for the handle's batch and coefficient
@@ -591,7 +693,11 @@ void plan_stencil(Handle& H) {
     if (H.stencil_mode != kModeStream && H.stencil_mode != kModeVec && H.stencil_mode != kModeFused) return;
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, H.desc.device);
-    if (H.stencil_mode == kModeFused && H.fused_variant >= kFusedTileBase) {
+    if (H.stencil_mode == kModeFused && is_slab_variant(H.fused_variant)) {
+        const int v = H.fused_variant - kFusedSlabBase;
+        const int occ = H.prec == 4 ? slab_occupancy<float>(v) : slab_occupancy<double>(v);
+        H.splan = H.prec == 4 ? plan_slab<float>(H.g, sms, occ, H.B, v) : plan_slab<double>(H.g, sms, occ, H.B, v);
+    } else if (H.stencil_mode == kModeFused && H.fused_variant >= kFusedTileBase) {
         const int v = H.fused_variant - kFusedTileBase;
         const int occ = H.prec == 4 ? tile_occupancy<float>(v) : tile_occupancy<double>(v);
         H.splan = H.prec == 4 ? plan_tile<float>(H.g, sms, occ, H.B, v) : plan_tile<double>(H.g, sms, occ, H.B, v);
@@ -641,6 +747,16 @@ void launch_half(Handle& H, int which) {
 // launches issued.
 template <typename T>
 int launch_fused(Handle& H, const StencilArgs<T>& sa) {
+    if (is_slab_variant(H.fused_variant)) {
+        const int4* units[kSlabLists];
+        bool air = false;
+        for (int q = 0; q < kSlabLists; ++q) units[q] = H.slab_units[q].as<int4>();
+        for (auto& f : H.faces) air = air || f->pec;
+        const int n = launch_slab_step<T>(sa, H.splan.ichunk, H.fused_variant - kFusedSlabBase, units,
+                                          H.n_slab_units, air, H.status.as<int>(), H.stream);
+        if (n < 0) fail(FITB_ERR_CUDA, "tensor maps of the slab step could not be encoded");
+        return n;
+    }
     if (H.fused_variant >= kFusedTileBase) {
         if (launch_tile_step<T>(sa, H.splan, H.fused_variant - kFusedTileBase, H.status.as<int>(), H.stream) != 0)
             fail(FITB_ERR_CUDA, "tensor maps of the tile step could not be encoded");
@@ -657,12 +773,12 @@ int launch_fused_any(Handle& H) {
     if (H.prec == 4) {
         const StencilArgs<float> sa = stencil_args<float>(H);
         int n = launch_fused<float>(H, sa);
-        if (H.fused_variant >= kFusedTileBase) n += launch_tile_cpml_H<float>(sa, H.stream);
+        if (is_tile_variant(H.fused_variant)) n += launch_tile_cpml_H<float>(sa, H.stream);
         return n;
     }
     const StencilArgs<double> sa = stencil_args<double>(H);
     int n = launch_fused<double>(H, sa);
-    if (H.fused_variant >= kFusedTileBase) n += launch_tile_cpml_H<double>(sa, H.stream);
+    if (is_tile_variant(H.fused_variant)) n += launch_tile_cpml_H<double>(sa, H.stream);
     return n;
 }
 
@@ -715,7 +831,7 @@ int enqueue_step_fused(Handle& H) {
         launch_lumped<T>(e_new, pa, H.d_lumped.as<LumpedDev>(), (int)H.lumped.size(), H.stream);
         ++n;
     }
-    if (H.fused_variant >= kFusedTileBase) {
+    if (is_tile_variant(H.fused_variant)) {
         const int nh = launch_tile_cpml_H<T>(sa, H.stream);
         if (nh < 0) fail(FITB_ERR_STATE, "the tile step does not take this grid / CPML layout");
         n += nh;
@@ -866,6 +982,7 @@ void run_steps(Handle& H, long long nsteps) {
     if (nsteps > 0) check_dtbc_tables(H, H.steps_done + nsteps - 1);
     ensure_capacity(H, H.steps_done + nsteps);
     refresh_port_tables(H);
+    sync_dead_units(H);
     int per = 0;
     if (!H.graphs_valid) {
         // graphs for each starting buffer set (one set for in-place kernels)
@@ -958,7 +1075,10 @@ void add_cpml_impl(Handle& H, int face, int n_pml, const double* bt, const doubl
     d.dI = axis == 0 ? n_pml : H.g.nx + 1;
     d.dJ = axis == 1 ? n_pml : H.g.ny + 1;
     d.dK = axis == 2 ? n_pml : H.g.nz + 1;
-    d.slab = (long long)d.dI * d.dJ * d.dK;
+    // rows padded to 16 entries: whole rows stay 16-byte aligned for the
+    // psi (field dtype) and air (byte) tensor copies of the tile step
+    d.pk = (int)round_up(d.dK, 16);
+    d.slab = (long long)d.dI * d.dJ * d.pk;
     f->psi.alloc((size_t)H.B * 4 * d.slab * sizeof(T));
     if (H.stencil_mode == kModeFused) f->psi2.alloc((size_t)H.B * 4 * d.slab * sizeof(T));
     std::vector<uint8_t> air((size_t)(4 * d.slab), 0);
@@ -969,8 +1089,9 @@ void add_cpml_impl(Handle& H, int face, int n_pml, const double* bt, const doubl
             for (int y = 0; y < rb; ++y)
                 for (int z = 0; z < rc; ++z) {
                     long long src = ((long long)x * rb + y) * rc + z;
-                    long long dst = (long long)q * d.slab + ((long long)x * d.dJ + y) * d.dK + z;
+                    long long dst = (long long)q * d.slab + ((long long)x * d.dJ + y) * d.pk + z;
                     air[(size_t)dst] = air_in[q] ? (air_in[q][src] ? 1 : 0) : 1;
+                    if (!air[(size_t)dst]) f->pec = true;
                 }
     }
     upload(f->air, air);
@@ -1246,7 +1367,7 @@ int fitb_create(const fitb_desc* desc, fitb_handle** out) {
             }
         } else if (m == "fused") {
             const char* t = getenv("FITB_FUSED_VARIANT");
-            H.fused_variant = t ? std::max(0, std::min(fitb::kFusedTileBase + fitb::kTileVariants - 1, atoi(t))) : 2;
+            H.fused_variant = t ? std::max(0, std::min(fitb::kFusedSlabBase + fitb::kSlabVariants - 1, atoi(t))) : 2;
             if (H.fused_variant == 1 && H.prec == 8) H.fused_variant = 0;
             if (!fitb::fused_variant_ok(H.prec, H.fused_variant)) H.fused_variant = 2;
             ck(fitb::prepare_fused_any(H.prec, H.fused_variant), "fused step smem attribute");
@@ -1308,6 +1429,8 @@ int fitb_set_coeffs(fitb_handle* h, const double* alpha_e, const double* beta_e,
     fitb::comp_max(H, beta_h, 3, H.coef_max[3]);
     H.coeffs_set = true;
     fitb::compact_coeffs(H);
+    H.port_tables_dirty = true;  // the slab step's dead-unit plan reads the coefficients
+    fitb::invalidate_graphs(H);
     FITB_CATCH
 }
 
@@ -1337,6 +1460,8 @@ int fitb_set_coeffs_native(fitb_handle* h, const void* alpha_e, const void* beta
     }
     H.coeffs_set = true;
     fitb::compact_coeffs(H);
+    H.port_tables_dirty = true;  // the slab step's dead-unit plan reads the coefficients
+    fitb::invalidate_graphs(H);
     FITB_CATCH
 }
 
@@ -1374,10 +1499,21 @@ int fitb_configure_stencil(fitb_handle* h, int32_t kind, int32_t variant, int32_
         if (!fitb::fused_variant_ok(H.prec, variant)) fail(FITB_ERR_ARG, "fused variant %d", variant);
         if (H.disp[0].present() || H.disp[1].present())
             fail(FITB_ERR_STATE, "dispersive materials need an in-place stencil mode (not the fused step)");
-        if (variant >= fitb::kFusedTileBase &&
+        if (fitb::is_tile_variant(variant) &&
             !(H.prec == 4 ? fitb::tile_step_fits<float>(fitb::stencil_args<float>(H))
                           : fitb::tile_step_fits<double>(fitb::stencil_args<double>(H))))
             fail(FITB_ERR_ARG, "the tile step does not take this grid / CPML layout");
+        if (fitb::is_slab_variant(variant)) {
+            // any march depth the planner may pick: check the deepest and the shallowest
+            std::vector<int4> lists[fitb::kSlabLists];
+            const int np = H.g.nx + 1;
+            std::vector<int> depths;
+            for (int c = 12; c <= 20; ++c) depths.push_back(std::min(np, c));
+            if (ichunk > 0) depths.push_back(std::min(np, (int)ichunk));
+            for (int c : depths)
+                if (!fitb::slab_units_of(H, variant, c, lists))
+                    fail(FITB_ERR_ARG, "the slab step does not take this grid / CPML layout");
+        }
     }
     if (kind == fitb::kModeBulk && H.B != 1) fail(FITB_ERR_ARG, "the bulk-copy stencil takes one field set");
     ck(cudaStreamSynchronize(H.stream), "configure sync");
@@ -1441,6 +1577,20 @@ int fitb_device_bytes(fitb_handle* h, int64_t* out) {
     FITB_CATCH
 }
 
+int fitb_slab_units(fitb_handle* h, int64_t* out) {
+    FITB_TRY
+    Handle& H = H_of(h);
+    if (!out) fail(FITB_ERR_ARG, "null argument");
+    for (int q = 0; q <= fitb::kSlabLists; ++q) out[q] = 0;
+    if (H.stencil_mode == fitb::kModeFused && fitb::is_slab_variant(H.fused_variant)) {
+        fitb::check_ready(H);
+        fitb::refresh_port_tables(H);
+        for (int q = 0; q < fitb::kSlabLists; ++q) out[q] = H.n_slab_units[q];
+        out[fitb::kSlabLists] = H.n_slab_dead;
+    }
+    FITB_CATCH
+}
+
 int fitb_get_stencil(fitb_handle* h, int32_t* out) {
     FITB_TRY
     Handle& H = H_of(h);
@@ -1477,6 +1627,7 @@ int fitb_set_fields(fitb_handle* h, int32_t b, const void* e, size_t e_bytes, co
         else
             fitb::pack3<double>(H, (const double*)hf, H.Hc().as<double>() + (long long)b * H.e_block(), 3);
     }
+    H.skip_sync = H.n_slab_dead > 0;
     FITB_CATCH
 }
 
@@ -2084,6 +2235,7 @@ int fitb_time_stencil(fitb_handle* h, int32_t n_iter, double* ms_e, double* ms_h
     if (H.stencil_mode == fitb::kModeFused) {
         // the whole E + H pass, alternating buffer sets; an even count
         // leaves the current set where it was
+        fitb::refresh_port_tables(H);  // the slab form's unit lists
         const int n2 = 2 * ((n_iter + 1) / 2);
         ck(cudaEventRecord(ev[0], H.stream), "event record");
         int nl = 0;

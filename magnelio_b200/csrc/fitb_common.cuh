@@ -6,6 +6,8 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include <vector>
+
 namespace fitb {
 
 // ---------------------------------------------------------------------------
@@ -44,13 +46,17 @@ __host__ __device__ __forceinline__ long long pidx(const Geom& g, int i, int j, 
 
 // One CPML face as the stencil kernels see it.  The psi state of all four
 // auxiliary components lives in a uniform slab of dims (dI, dJ, dK) =
-// (nx+1, ny+1, nz+1) with the face axis replaced by the layer count n.
+// (nx+1, ny+1, nz+1) with the face axis replaced by the layer count n; its
+// rows are padded to pk = round_up(dK, 16) entries (entry (a, b, c) at
+// (a dJ + b) pk + c), so every row starts 16-byte aligned for the air masks
+// (bytes) and the psi values alike.  Padding entries hold psi = 0, air = 0.
 struct FaceDev {
     int axis;       // 0 = x, 1 = y, 2 = z
     int lo;         // first layer index along the axis
     int n;          // layer count
     int dI, dJ, dK; // slab dims
-    long long slab; // dI * dJ * dK
+    int pk;         // row pitch (entries)
+    long long slab; // dI * dJ * pk
     void* psi;      // [B][4][slab] field dtype: E1, E2, H1, H2
     void* psi_next; // fused step: the buffer the new psi goes to
     const unsigned char* air;  // [4][slab] 0/1
@@ -161,6 +167,42 @@ template <typename T>
 int launch_tile_cpml_E(const StencilArgs<T>& a, cudaStream_t s);
 template <typename T>
 int launch_tile_cpml_H(const StencilArgs<T>& a, cudaStream_t s);
+// Slab form of the fused step (stencil_slab.cu): the tile march with the
+// CPML applied inside it, launched once per list of units with 0..3 CPML
+// face slots; fused-step variants kFusedSlabBase + v with (tile rows, ring
+// stages) = (4, 3), (2, 3), (3, 3), (4, 4) for v = 0..3.
+constexpr int kFusedSlabBase = kFusedTileBase + kTileVariants, kSlabVariants = 4;
+inline bool is_tile_variant(int v) { return v >= kFusedTileBase && v < kFusedSlabBase; }
+inline bool is_slab_variant(int v) { return v >= kFusedSlabBase && v < kFusedSlabBase + kSlabVariants; }
+int slab_tj_of(int variant);
+template <typename T>
+bool slab_supported(int variant);
+template <typename T>
+cudaError_t prepare_slab(int variant);
+template <typename T>
+int slab_occupancy(int variant);
+template <typename T>
+StreamPlan plan_slab(const Geom& g, int sm_count, int ctas_per_sm, int B, int variant);
+// Unit lists by face-slot count 0, 1, 2, 3 and 4-6 (int4: k tile, j tile,
+// i chunk, packed slot faces); false when the face table is too large.
+constexpr int kSlabLists = 5;
+bool plan_slab_units(const Geom& g, const FaceDev* f, int nfaces, int tj, int ichunk,
+                     std::vector<int4> out[kSlabLists]);
+// Dead-unit skipping: flags[u] = 1 for every unit with a live cell (an E
+// edge with a nonzero coefficient, an H face that is neither a no-op nor
+// curl-dead); and the sync of the skipped units' cells across both buffer
+// sets.  Both return the launches issued.
+template <typename T>
+int slab_unit_liveness(const Geom& g, const T* aE, const T* bE, const T* aH, const T* bH, int tj, int ichunk,
+                       const int4* units, int n, int* flags, cudaStream_t s);
+template <typename T>
+int slab_dead_sync(const Geom& g, const T* aH, const T* bH, int tj, int ichunk, const int4* units, int n, int B,
+                   T* e_cur, T* h_cur, T* e_oth, T* h_oth, cudaStream_t s);
+// Launches one kernel per non-empty unit list; returns the launches issued
+// (< 0: tensor maps not encodable).  air: some face has PEC masks.
+template <typename T>
+int launch_slab_step(StencilArgs<T> a, int ichunk, int variant, const int4* const units[kSlabLists],
+                     const int n_units[kSlabLists], bool air, int* status, cudaStream_t s);
 // One CTA waits, bounded by `limit` tries, on an mbarrier that nothing
 // completes; the expired wait writes kStatusWaitTimeoutTile to *status.
 cudaError_t launch_wait_probe(int* status, unsigned limit, cudaStream_t s);

@@ -78,7 +78,7 @@ __device__ __forceinline__ long long slab_at(const FaceDev& f, int l, int i, int
     const int a = (f.axis == 0) ? l : i;
     const int b = (f.axis == 1) ? l : j;
     const int c = (f.axis == 2) ? l : k;
-    return ((long long)a * f.dJ + b) * f.dK + c;
+    return ((long long)a * f.dJ + b) * f.pk + c;
 }
 
 // Shared-memory ring bookkeeping common to both kernels.

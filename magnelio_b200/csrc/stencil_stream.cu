@@ -46,7 +46,7 @@ __device__ __forceinline__ long long slab_index_s(const FaceDev& f, int l, int i
     const int a = (f.axis == 0) ? l : i;
     const int b = (f.axis == 1) ? l : j;
     const int c = (f.axis == 2) ? l : k;
-    return ((long long)a * f.dJ + b) * f.dK + c;
+    return ((long long)a * f.dJ + b) * f.pk + c;
 }
 
 template <typename T>

@@ -43,9 +43,7 @@
 // flight and returns; the host reads the status after the step.
 #include "fused_cpml.cuh"
 #include "pass_boxes.h"
-
-#include <cuda.h>
-#include <cudaTypedefs.h>
+#include "tile_common.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -55,60 +53,14 @@ namespace fitb {
 
 namespace {
 
-constexpr unsigned kTileWaitLimit = 1u << 22;
-constexpr int TK = 32;  // cells per tile row: one warp
+using tma::TK;
+using tma::compute_barrier;
+using tma::saddr;
 
 struct TileMaps {
     CUtensorMap e, h, aE, bE, aH, bH;
 };
 static_assert(sizeof(TileMaps) == 6 * 128, "tensor map size");
-
-__device__ __forceinline__ unsigned saddr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ void tbar_init(unsigned long long* bar, unsigned count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(saddr(bar)), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ void tbar_expect(unsigned long long* bar, unsigned bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(saddr(bar)), "r"(bytes) : "memory");
-}
-
-__device__ __forceinline__ void tbar_arrive(unsigned long long* bar) {
-    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(saddr(bar)) : "memory");
-}
-
-__device__ __forceinline__ bool tbar_try(unsigned long long* bar, unsigned parity) {
-    unsigned ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(ok)
-        : "r"(saddr(bar)), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-
-__device__ __forceinline__ bool tbar_wait(unsigned long long* bar, unsigned parity) {
-    for (unsigned n = 0; n < kTileWaitLimit; ++n)
-        if (tbar_try(bar, parity)) return true;
-    return false;
-}
-
-// 4-D tiled tensor copy global -> shared, completing on `bar` (no
-// multicast).
-__device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* map, int c0, int c1, int c2, int c3,
-                                            unsigned long long* bar) {
-    asm volatile(
-        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
-        " [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(saddr(dst)),
-        "l"(reinterpret_cast<unsigned long long>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(saddr(bar))
-        : "memory");
-}
-
-__device__ __forceinline__ void compute_barrier(int nthreads) {
-    asm volatile("bar.sync 1, %0;" ::"r"(nthreads) : "memory");
-}
 
 // Shared-memory layout of one tile configuration.
 template <typename T, int TJ, int NS>
@@ -221,8 +173,8 @@ __global__ void __launch_bounds__(32 * (TJ + 1), sizeof(T) == 4 ? MINB : 1)
     T* ring = reinterpret_cast<T*>(smem + G::oN);
     if (tid == 0) {
         for (int s = 0; s < NS; ++s) {
-            tbar_init(&full[s], 1);
-            tbar_init(&empty[s], TJ);
+            tma::bar_init(&full[s], 1);
+            tma::bar_init(&empty[s], TJ);
         }
         flags[0] = 0;
         flags[1] = 0;
@@ -238,7 +190,7 @@ __global__ void __launch_bounds__(32 * (TJ + 1), sizeof(T) == 4 ? MINB : 1)
             for (; t < nplanes; ++t) {
                 if (flags[0]) break;
                 const int s = t % NS;
-                if (t >= NS && !tbar_wait(&empty[s], (unsigned)(((t / NS) + 1) & 1))) {
+                if (t >= NS && !tma::bar_wait(&empty[s], (unsigned)(((t / NS) + 1) & 1))) {
                     atomicExch(status, kStatusWaitTimeoutTile);
                     flags[0] = 1;
                     break;
@@ -249,16 +201,16 @@ __global__ void __launch_bounds__(32 * (TJ + 1), sizeof(T) == 4 ? MINB : 1)
                 unsigned bytes = G::bytesH;
                 if (!first) bytes += 3 * G::bytesE;
                 if (!first && !last) bytes += 2 * G::bytesC;
-                tbar_expect(&full[s], bytes);
-                tma_load_4d(st + G::oH, &maps.h, k0 - 4, j0 - 1, plane, 3 * b, &full[s]);
+                tma::bar_expect(&full[s], bytes);
+                tma::load_4d(st + G::oH, &maps.h, k0 - 4, j0 - 1, plane, 3 * b, &full[s]);
                 if (!first) {
-                    tma_load_4d(st + G::oE, &maps.e, k0, j0, plane, 3 * b, &full[s]);
-                    tma_load_4d(st + G::oaE, &maps.aE, k0, j0, plane, 0, &full[s]);
-                    tma_load_4d(st + G::obE, &maps.bE, k0, j0, plane, 0, &full[s]);
+                    tma::load_4d(st + G::oE, &maps.e, k0, j0, plane, 3 * b, &full[s]);
+                    tma::load_4d(st + G::oaE, &maps.aE, k0, j0, plane, 0, &full[s]);
+                    tma::load_4d(st + G::obE, &maps.bE, k0, j0, plane, 0, &full[s]);
                 }
                 if (!first && !last) {
-                    tma_load_4d(st + G::oaH, &maps.aH, k0, j0, plane, 0, &full[s]);
-                    tma_load_4d(st + G::obH, &maps.bH, k0, j0, plane, 0, &full[s]);
+                    tma::load_4d(st + G::oaH, &maps.aH, k0, j0, plane, 0, &full[s]);
+                    tma::load_4d(st + G::obH, &maps.bH, k0, j0, plane, 0, &full[s]);
                 }
             }
             flags[1] = t;
@@ -281,7 +233,7 @@ __global__ void __launch_bounds__(32 * (TJ + 1), sizeof(T) == 4 ? MINB : 1)
         const bool own_x = v_x && (rx == TJ ? (absorb_j && (cx < TK || absorb_k)) : absorb_k);
         for (int t = 0; t < nplanes; ++t) {
             const int s = t % NS;
-            const bool ok = tbar_wait(&full[s], (unsigned)((t / NS) & 1));
+            const bool ok = tma::bar_wait(&full[s], (unsigned)((t / NS) & 1));
             if (!ok) {
                 atomicExch(status, kStatusWaitTimeoutTile);
                 flags[0] = 1;
@@ -308,14 +260,14 @@ __global__ void __launch_bounds__(32 * (TJ + 1), sizeof(T) == 4 ? MINB : 1)
             }
             if (t > 0) {
                 __syncwarp();
-                if (lane == 0) tbar_arrive(&empty[(t - 1) % NS]);
+                if (lane == 0) tma::bar_arrive(&empty[(t - 1) % NS]);
             }
         }
     }
     __syncthreads();
     // after an expired wait: the copies issued but not consumed
     if (tid == 0)
-        for (int t = flags[2]; t < flags[1]; ++t) tbar_wait(&full[t % NS], (unsigned)((t / NS) & 1));
+        for (int t = flags[2]; t < flags[1]; ++t) tma::bar_wait(&full[t % NS], (unsigned)((t / NS) & 1));
 }
 
 // Cell (i, j, k) of this thread and its box, or false past the box's end.
@@ -345,7 +297,7 @@ __device__ __forceinline__ int slab32(const FaceDev& f, int i, int j, int k) {
     const int a = (f.axis == 0) ? i - f.lo : i;
     const int b = (f.axis == 1) ? j - f.lo : j;
     const int c = (f.axis == 2) ? k - f.lo : k;
-    return (a * f.dJ + b) * f.dK + c;
+    return (a * f.dJ + b) * f.pk + c;
 }
 
 // E-side CPML on the fused buffers (cpml.py:343-430), every face of the
@@ -475,10 +427,10 @@ __global__ void __launch_bounds__(kPassThreads) k_tile_fix_boxes(const StencilAr
 __global__ void k_wait_probe(int* status, unsigned limit) {
     __shared__ unsigned long long bar;
     if (threadIdx.x != 0) return;
-    tbar_init(&bar, 1);
+    tma::bar_init(&bar, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     for (unsigned n = 0; n < limit; ++n)
-        if (tbar_try(&bar, 0u)) return;
+        if (tma::bar_try(&bar, 0u)) return;
     atomicExch(status, kStatusWaitTimeoutTile);
 }
 
@@ -544,36 +496,6 @@ struct TileLaunch {
         k_step_tile<T, TJ, NS, MINB><<<grid, 32 * (TJ + 1), TileGeo<T, TJ, NS>::smem, s>>>(m, a, status);
     }
 };
-
-PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
-    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-    if (!fn) {
-        void* p = nullptr;
-        cudaDriverEntryPointQueryResult q;
-        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) ==
-                cudaSuccess &&
-            q == cudaDriverEntryPointSuccess)
-            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
-    }
-    return fn;
-}
-
-// 4-D map over the padded layout: (k, j, plane, component) with `ncomp`
-// components of `vol` elements; box (bk, bj, 1, 3).
-template <typename T>
-bool encode_map(CUtensorMap* out, const void* base, const Geom& g, int ncomp, int bk, int bj) {
-    auto fn = encode_fn();
-    if (!fn) return false;
-    const cuuint64_t dims[4] = {(cuuint64_t)g.nkp, (cuuint64_t)g.njp, (cuuint64_t)(g.nx + 4), (cuuint64_t)ncomp};
-    const cuuint64_t strides[3] = {(cuuint64_t)g.sj * sizeof(T), (cuuint64_t)g.si * sizeof(T),
-                                   (cuuint64_t)g.vol * sizeof(T)};
-    const cuuint32_t box[4] = {(cuuint32_t)bk, (cuuint32_t)bj, 1, 3};
-    const cuuint32_t estr[4] = {1, 1, 1, 1};
-    const CUtensorMapDataType dt = sizeof(T) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
-    return fn(out, dt, 4, const_cast<void*>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-              CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
-}
 
 // The CPML pass boxes of this handle's faces (pass_boxes.h).
 bool pass_boxes(PassBoxes& bx, const Geom& g, const FaceDev* f, int nfaces, bool h_side) {
@@ -664,10 +586,10 @@ int launch_tile_step(StencilArgs<T> a, const StreamPlan& sp, int variant, int* s
     const int tj = info.tj;
     TileMaps m;
     const long long nset = 3LL * a.B;
-    if (!encode_map<T>(&m.e, a.e, a.g, (int)nset, TK + 4, tj + 1) ||
-        !encode_map<T>(&m.h, a.h, a.g, (int)nset, TK + 8, tj + 2) ||
-        !encode_map<T>(&m.aE, a.aE, a.g, 3, TK + 4, tj + 1) || !encode_map<T>(&m.bE, a.bE, a.g, 3, TK + 4, tj + 1) ||
-        !encode_map<T>(&m.aH, a.aH, a.g, 3, TK, tj) || !encode_map<T>(&m.bH, a.bH, a.g, 3, TK, tj))
+    if (!tma::encode_field_map<T>(&m.e, a.e, a.g, (int)nset, TK + 4, tj + 1) ||
+        !tma::encode_field_map<T>(&m.h, a.h, a.g, (int)nset, TK + 8, tj + 2) ||
+        !tma::encode_field_map<T>(&m.aE, a.aE, a.g, 3, TK + 4, tj + 1) || !tma::encode_field_map<T>(&m.bE, a.bE, a.g, 3, TK + 4, tj + 1) ||
+        !tma::encode_field_map<T>(&m.aH, a.aH, a.g, 3, TK, tj) || !tma::encode_field_map<T>(&m.bH, a.bH, a.g, 3, TK, tj))
         return -2;
     a.ichunk = sp.ichunk;
     TileLaunch<T> f{m, a, dim3(sp.grid_x, sp.grid_y, sp.grid_z), status, s};

@@ -186,7 +186,7 @@ __device__ __forceinline__ long long slab_index_v(const FaceDev& f, int l, int i
     const int a = (f.axis == 0) ? l : i;
     const int b = (f.axis == 1) ? l : j;
     const int c = (f.axis == 2) ? l : k;
-    return ((long long)a * f.dJ + b) * f.dK + c;
+    return ((long long)a * f.dJ + b) * f.pk + c;
 }
 
 // Faces (bit q = p.f[q]) whose slab a thread's cells can meet: y faces by

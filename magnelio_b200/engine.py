@@ -148,6 +148,13 @@ class FitEngine:
         return {"kind": names[int(out[0])], "variant": int(out[1]), "ichunk": int(out[2]),
                 "grid": (int(out[3]), int(out[4]), int(out[5]))}
 
+    def slab_units(self) -> dict:
+        """Work units of the slab step: launched per face-slot count
+        (0, 1, 2, 3, up to 6) and skipped as dead."""
+        out = np.zeros(6, dtype=np.int64)
+        check(self._lib.fitb_slab_units(self._h, i64p(out)))
+        return {"slots": [int(v) for v in out[:5]], "dead": int(out[5])}
+
     def reserve_steps(self, n: int) -> None:
         """Size the step-indexed device histories for ``n`` steps up front."""
         check(self._lib.fitb_reserve_steps(self._h, int(n)))

@@ -2,8 +2,9 @@
 
 The brick box (graded non-uniform grid, 32 conformal dielectric bricks,
 10-layer CPML on six faces, lumped gap source, three 64-frequency DFT
-planes) is marched in float32 by the two-pass stream kernels and by the TMA
-tile step, and compared with the float64 C port of the reference's step
+planes) is marched in float32 by the two-pass stream kernels, by the TMA
+tile step with its CPML passes and by the slab step (CPML inside the tile
+march), and compared with the float64 C port of the reference's step
 (pinned bit-exact to the reference's own float64 march by the CPU suite):
 
 * 128^3 for a 2000-step prefix (the pulse has been launched, crossed the
@@ -26,7 +27,8 @@ pytestmark = pytest.mark.gpu
 FIELD_TOL = 2e-4   # ||x - x_ref|| / max_n ||x_ref(n)||, float32 engine vs float64
 DFT_TOL = 1e-3     # max |bin - bin_ref| / max |bin_ref| per monitor component
 
-FORMS = [("stream", 0), ("fused", 7)]  # two-pass stream kernels, TMA tile step
+# two-pass stream kernels, TMA tile step with CPML passes, slab step (CPML inside the march)
+FORMS = [("stream", 0), ("fused", 7), ("fused", 16)]
 
 
 def _reference(n, steps):

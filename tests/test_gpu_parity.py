@@ -115,7 +115,7 @@ def test_stencil_variants_agree(name):
     p, d, n = load_golden(name)
     outs = []
     modes = [("stream", v) for v in range(4)] + [("bulk", 0), ("simple", 0)]
-    modes += [("vec", v) for v in range(4)] + [("fused", v) for v in range(16)]
+    modes += [("vec", v) for v in range(4)] + [("fused", v) for v in range(20)]
     for kind, variant in modes:
         with p.build_engine("single") as eng:
             eng.configure_stencil(kind, variant)
@@ -328,7 +328,7 @@ def test_compact_coefficients_need_the_stream_kernels(monkeypatch):
 
 @pytest.mark.parametrize("name", ["cpml_box", "mixed_box", "lumped_dft", "wg_dtbc", "wg_mur", "planewave_box"])
 @pytest.mark.parametrize("precision,tol", [("double", F64_TOL), ("single", F32_TOL)])
-@pytest.mark.parametrize("variant", ["0", "2", "7", "8"])
+@pytest.mark.parametrize("variant", ["0", "2", "7", "8", "16", "17"])
 def test_fused_step_matches_reference(name, precision, tol, variant, monkeypatch):
     """The fused E+H pass (ping-pong buffers, H fix-up next to port edges)
     reproduces the reference march: fields, energy, port V/I, DFT bins."""
@@ -352,7 +352,7 @@ def test_fused_step_matches_reference(name, precision, tol, variant, monkeypatch
 
 
 @pytest.mark.parametrize("name", ["lumped_dft", "wg_mur"])
-@pytest.mark.parametrize("variant", ["2", "8"])
+@pytest.mark.parametrize("variant", ["2", "8", "16"])
 def test_fused_buffer_swaps_are_invisible(name, variant, monkeypatch):
     """Odd and even step counts, single steps, graph chunks and a resume at
     an odd step give the same bits: the buffer set that holds the current
@@ -546,6 +546,7 @@ def test_cross_junction_batch_equals_one_excitation_per_handle():
 # TMA tile form of the fused step on grids of many tiles and chunks.
 
 TILE_VARIANTS = range(7, 16)
+SLAB_VARIANTS = range(16, 20)
 
 
 def _random_state(prob, rng, scale=1e-3):
@@ -604,6 +605,150 @@ def test_tile_step_matches_stream_on_a_multi_tile_grid(n, precision, tol):
     assert ran >= (18 if precision == "single" else 16)
 
 
+@pytest.mark.parametrize("n", [64, 70])
+@pytest.mark.parametrize("precision,tol", [("single", 1e-5), ("double", 1e-12)])
+def test_slab_step_matches_stream_on_a_multi_tile_grid(n, precision, tol):
+    """The slab step (CPML inside the tile march, unit lists by face-slot
+    count) on the multi-tile brick boxes of the tile-step test: 6-layer CPML
+    cutting through tiles, halo rows and columns inside the slabs, absorbed
+    last rows / columns, chunk seams, random initial fields; every variant
+    agrees with the stream kernels to FMA-contraction differences."""
+    from magnelio_b200 import workloads
+
+    steps = 23
+    prob = workloads.brick_box(n, seed=5, n_bricks=8, cpml_cells=6, n_freq=4, steps=steps + 2)
+    e0, h0 = _random_state(prob, np.random.default_rng(1))
+    prob.e0, prob.h0 = [e0], [h0]
+    ref = _run_mode(prob, precision, "stream", 0, 0, steps)
+    pe, ph = float(np.max(np.abs(ref[0]))), float(np.max(np.abs(ref[1])))
+    ran = 0
+    for v in SLAB_VARIANTS:
+        for ichunk in (0, 9):
+            try:
+                got = _run_mode(prob, precision, "fused", v, ichunk, steps)
+            except FitbError as exc:
+                assert precision == "double" and "fused variant" in str(exc), exc
+                continue
+            ran += 1
+            assert got[4]["kind"] == "fused" and got[4]["variant"] == v
+            assert _rel(got[0], ref[0], pe) < tol, (v, ichunk)
+            assert _rel(got[1], ref[1], ph) < tol, (v, ichunk)
+            assert _rel(got[2], ref[2]) < 10 * tol, (v, ichunk)
+            for a, b in zip(got[3], ref[3]):
+                assert _rel(a, b) < max(10 * tol, DFT_TOL), (v, ichunk)
+    assert ran >= (8 if precision == "single" else 6)
+
+
+@pytest.mark.parametrize("variant", [16, 17])
+def test_slab_step_with_pec_masks_in_the_cpml(variant):
+    """PEC air masks inside the CPML slabs (the air-mask boxes of the slab
+    step), on a grid whose units see both faces of an axis (six-slot
+    launches): fields match the reference march."""
+    for name in ("cpml_box", "mixed_box"):
+        pe, ph = _peaks(name)
+        p, d, n = load_golden(name)
+        assert any(a is not None and not np.all(a) for f in p.cpml for a in f.air)
+        with p.build_engine("single") as eng:
+            eng.configure_stencil("fused", variant)
+            eng.step(n)
+            e, h = eng.read_fields()
+        assert _rel(e, d["out.e"], pe) < F32_TOL, name
+        assert _rel(h, d["out.h"], ph) < F32_TOL, name
+
+
+def test_slab_step_with_cpml_on_two_field_sets_matches_stream():
+    """Two field sets with different random initial fields through the slab
+    step: each set equals the stream kernels' march."""
+    from magnelio_b200 import workloads
+
+    steps = 17
+    prob = workloads.brick_box(64, seed=9, n_bricks=4, cpml_cells=5, n_freq=3, steps=steps + 2)
+    rng = np.random.default_rng(4)
+    inits = [_random_state(prob, rng) for _ in range(2)]
+    prob.batch = 2
+    prob.lumped[0].v_src = prob.lumped[0].v_src * 2
+    prob.e0 = [a for a, _ in inits]
+    prob.h0 = [b for _, b in inits]
+    outs = {}
+    for kind, v in (("stream", 0), ("fused", 16)):
+        with prob.build_engine("single") as eng:
+            eng.configure_stencil(kind, v, 9)
+            eng.step(steps)
+            outs[kind] = [eng.read_fields(b) for b in range(2)]
+    for b in range(2):
+        (es, hs), (et, ht) = outs["stream"][b], outs["fused"][b]
+        assert _rel(et, es, float(np.max(np.abs(es)))) < 1e-5, b
+        assert _rel(ht, hs, float(np.max(np.abs(hs)))) < 1e-5, b
+    assert not np.array_equal(outs["fused"][0][0], outs["fused"][1][0])
+
+
+def test_dead_units_are_skipped_bit_identically(monkeypatch):
+    """Dead-unit skipping (the reference's tile skip) on the four-port cross
+    junction, whose PEC corner blocks freeze most of the grid: the slab step
+    leaves the dead units out, and every field set's V/I and fields equal
+    the same step with skipping turned off, bit for bit, and the reference's
+    eight runs to the float32 bar."""
+    p, d, n = load_golden("cfg3_cross_small")
+    k = 700
+    outs = {}
+    for skip in ("1", "0"):
+        monkeypatch.setenv("FITB_TILE_SKIP", skip)
+        with p.build_engine("single") as eng:
+            eng.configure_stencil("fused", 16)
+            units = eng.slab_units()
+            eng.step(k)
+            outs[skip] = ([eng.read_vi(b) for b in range(p.batch)], [eng.read_fields(b) for b in range(p.batch)],
+                          units)
+    assert outs["1"][2]["dead"] > 0 and outs["0"][2]["dead"] == 0
+    assert sum(outs["1"][2]["slots"]) + outs["1"][2]["dead"] == sum(outs["0"][2]["slots"])
+    for b in range(p.batch):
+        for a, c in zip(outs["1"][0][b] + outs["1"][1][b], outs["0"][0][b] + outs["0"][1][b]):
+            assert np.array_equal(a, c), b
+        V, I = outs["1"][0][b]
+        assert _rel(V, d[f"cross.V{b}"][:k]) < F32_TOL, b
+        assert _rel(I, d[f"cross.I{b}"][:k]) < F32_TOL, b
+
+
+def test_dead_units_survive_a_resume_and_host_field_writes(monkeypatch):
+    """A checkpoint resume into a skipping slab step, and fields written from
+    the host with junk in the frozen cells: the skipped units' cells are made
+    consistent across both buffer sets before the next step, so the
+    continuation equals the uninterrupted run bit for bit."""
+    monkeypatch.setenv("FITB_TILE_SKIP", "1")
+    p, d, n = load_golden("cfg3_cross_small")
+    k, m = 301, 200  # odd: the resume starts on the second buffer set
+    with p.build_engine("single") as a:
+        a.configure_stencil("fused", 16)
+        a.step(k)
+        blob = a.state_export()
+        e_k, h_k = a.read_fields(3)
+        a.step(m)
+        ref = [a.read_fields(b) for b in range(p.batch)]
+    with p.build_engine("single") as b_:
+        b_.configure_stencil("fused", 16)
+        b_.state_import(blob)
+        b_.step(m)
+        got = [b_.read_fields(b) for b in range(p.batch)]
+    for x, y in zip(ref, got):
+        assert np.array_equal(x[0], y[0]) and np.array_equal(x[1], y[1])
+    # junk in the frozen E edges (alpha = beta = 0): the dense step zeroes
+    # them in one step, the skipping step before its first step
+    frozen = (p.alpha_E == 0) & (p.beta_E == 0)
+    assert frozen.any()
+    e_junk = e_k.copy()
+    e_junk[frozen] = 1.0
+    outs = []
+    for skip in ("1", "0"):
+        monkeypatch.setenv("FITB_TILE_SKIP", skip)
+        with p.build_engine("single") as c:
+            c.configure_stencil("fused", 16)
+            c.state_import(blob)
+            c.set_fields(e_junk, h_k, b=3)
+            c.step(m)
+            outs.append(c.read_fields(3))
+    assert np.array_equal(outs[0][0], outs[1][0]) and np.array_equal(outs[0][1], outs[1][1])
+
+
 def test_tile_step_batched_matches_the_plain_kernel():
     """All six WR-90 port-mode excitations as one batch (DTBC ports, port
     fix-up cells, two k tiles): the tile form equals the plain batched
@@ -612,7 +757,7 @@ def test_tile_step_batched_matches_the_plain_kernel():
     steps = 400
     ref = _run_mode(p, "single", "simple", 0, 0, steps)
     pe = float(np.max(np.abs(ref[0])))
-    for v in (7, 8, 13):
+    for v in (7, 8, 13, 16, 17):
         got = _run_mode(p, "single", "fused", v, 17, steps)
         # float32 round-off (FMA contraction differs per kernel) grows over
         # 400 steps of a resonant guide; the reference bar is 2e-4
