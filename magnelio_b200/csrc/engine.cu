@@ -146,6 +146,7 @@ struct ModalHost {
     DevBuf port_e, int_e, port_h, me_port, me_int, mh_port, eprof, vprof, hprof;
     DevBuf comp_r, comp_live;
     DevBuf st, whist, shist, comp_state, scratch, exc, wf, buflen;
+    DevBuf conv;  // DTBC convolution partials of the current step
     std::vector<std::vector<double>> ktabs;  // per mode: concatenated tables
     std::vector<int> n_tables_mode;
     DevBuf ktab[kMaxModes];
@@ -176,6 +177,10 @@ struct Handle {
     int B = 1;
     double dt = 0.0;
     cudaStream_t stream = nullptr;
+    // second stream of the step graphs: the DTBC convolutions run on it
+    // beside the stencil (fork / join by events inside the capture)
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     DevBuf e, h, aE, bE, aH, bH, meps, mmu, staging;
     // Fused step: second field buffers; `cur` names the buffer set that
     // holds the current fields (always 0 for the in-place kernels).
@@ -242,7 +247,16 @@ struct Handle {
             if (graph_chunk[q]) cudaGraphExecDestroy(graph_chunk[q]);
             if (graph_one[q]) cudaGraphExecDestroy(graph_one[q]);
         }
+        if (ev_fork) cudaEventDestroy(ev_fork);
+        if (ev_join) cudaEventDestroy(ev_join);
+        if (side) cudaStreamDestroy(side);
         if (stream) cudaStreamDestroy(stream);
+    }
+    bool any_dtbc() const {
+        for (auto& mp : modal)
+            for (int m = 0; m < mp->n_modes; ++m)
+                if (mp->dev.is_dtbc[m]) return true;
+        return false;
     }
 
     long long e_block() const { return 3 * g.vol; }
@@ -403,6 +417,7 @@ void ensure_capacity(Handle& H, long long need) {
     }
     for (auto& mp : H.modal) {
         int M = mp->n_modes;
+        mp->conv.alloc((size_t)H.B * M * ((ncap + kConvChunk - 1) / kConvChunk) * 2 * sizeof(double));
         for (DevBuf* buf : {&mp->whist, &mp->shist}) {
             DevBuf nb;
             nb.alloc((size_t)H.B * M * ncap * sizeof(double));
@@ -472,6 +487,8 @@ void refresh_port_tables(Handle& H) {
         d.whist = mp->whist.as<double>();
         d.shist = mp->shist.as<double>();
         d.cap = H.cap;
+        d.conv = mp->conv.as<double>();
+        d.conv_chunks = (int)((H.cap + kConvChunk - 1) / kConvChunk);
         md.push_back(d);
     }
     upload(H.d_modal, md);
@@ -807,6 +824,24 @@ int disp_complete(Handle& H, int sd) {
     return n;
 }
 
+// Fork: the DTBC convolutions of this step start on the side stream as soon
+// as the previous step's port update has written its history; join: the
+// port update waits for them.  Returns the launches issued.
+int fork_dtbc_conv(Handle& H, const PortsArgs& pa) {
+    if (H.modal.empty() || !H.any_dtbc()) return 0;
+    ck(cudaEventRecord(H.ev_fork, H.stream), "fork record");
+    ck(cudaStreamWaitEvent(H.side, H.ev_fork, 0), "fork wait");
+    launch_dtbc_conv(pa, H.d_modal.as<ModalDev>(), (int)H.modal.size(),
+                     (int)((H.cap + kConvChunk - 1) / kConvChunk), H.side);
+    ck(cudaEventRecord(H.ev_join, H.side), "join record");
+    return 1;
+}
+
+void join_dtbc_conv(Handle& H) {
+    if (H.modal.empty() || !H.any_dtbc()) return;
+    ck(cudaStreamWaitEvent(H.stream, H.ev_join, 0), "join wait");
+}
+
 // Fused step: one launch for E and H from the current buffer set into the
 // other, then the ports on the new E (with the old H, which the two-pass
 // order shows them), the H fix-up next to port edges, the monitors on the
@@ -816,6 +851,7 @@ int enqueue_step_fused(Handle& H) {
     int n = 0;
     PortsArgs pa = ports_args(H);
     StencilArgs<T> sa = stencil_args<T>(H);
+    n += fork_dtbc_conv(H, pa);
     n += launch_fused<T>(H, sa);
     T* e_new = H.En().as<T>();
     T* h_new = H.Hn().as<T>();
@@ -824,6 +860,7 @@ int enqueue_step_fused(Handle& H) {
         ++n;
     }
     if (!H.modal.empty()) {
+        join_dtbc_conv(H);
         launch_modal<T>(e_new, H.Hc().as<T>(), pa, H.d_modal.as<ModalDev>(), (int)H.modal.size(), H.stream);
         ++n;
     }
@@ -864,6 +901,7 @@ int enqueue_step(Handle& H) {
     // in-place kernels below
     int n = 0;
     PortsArgs pa = ports_args(H);
+    n += fork_dtbc_conv(H, pa);
     for (int sd = 0; sd < 2; ++sd) {
         if (!H.disp[sd].present()) continue;
         launch_disp_save<T>((sd == 0 ? H.Ec() : H.Hc()).as<T>(), H.e_block(), H.B, H.disp[sd].dev, H.stream);
@@ -877,6 +915,7 @@ int enqueue_step(Handle& H) {
         ++n;
     }
     if (!H.modal.empty()) {
+        join_dtbc_conv(H);
         launch_modal<T>(H.Ec().as<T>(), H.Hc().as<T>(), pa, H.d_modal.as<ModalDev>(), (int)H.modal.size(), H.stream);
         ++n;
     }
@@ -1331,6 +1370,9 @@ int fitb_create(const fitb_desc* desc, fitb_handle** out) {
     g.si = (long long)g.njp * g.nkp;
     g.vol = (long long)(g.nx + 4) * g.si + (long long)fitb::kTailRows * g.sj;
     ck(cudaStreamCreateWithFlags(&H.stream, cudaStreamNonBlocking), "stream");
+    ck(cudaStreamCreateWithFlags(&H.side, cudaStreamNonBlocking), "stream");
+    ck(cudaEventCreateWithFlags(&H.ev_fork, cudaEventDisableTiming), "event");
+    ck(cudaEventCreateWithFlags(&H.ev_join, cudaEventDisableTiming), "event");
     const size_t blk = (size_t)H.e_block() * H.esz;
     H.e.alloc(blk * H.B);
     H.h.alloc(blk * H.B);

@@ -300,7 +300,13 @@ struct ModalDev {
     long long cap;            // history capacity (steps)
     int channel0;             // first recorder channel
     double dt;
+    // DTBC convolution partial sums of the current step, per history chunk
+    // of kConvChunk entries: [B][M][conv_chunks][2] (w, s)
+    double* conv;
+    int conv_chunks;
 };
+
+constexpr int kConvChunk = 1024;
 
 struct RecorderDev {
     double* V;  // [B][cap][nch]
@@ -324,6 +330,11 @@ void launch_lumped(T* e, const PortsArgs& pa, const LumpedDev* d, int n_lumped, 
 template <typename T>
 void launch_modal(T* e, const T* h, const PortsArgs& pa, const ModalDev* d, int n_modal,
                   cudaStream_t s);
+// The DTBC history convolutions of the coming port update (they read only
+// the history before the current step), spread over the history chunks of
+// every (port, field set); launch_modal sums the partials in chunk order.
+// max_chunks = the largest conv_chunks of the ports.
+void launch_dtbc_conv(const PortsArgs& pa, const ModalDev* d, int n_modal, int max_chunks, cudaStream_t s);
 
 // ---------------------------------------------------------------------------
 // TF/SF plane waves: per side (E, H) the unique corrected entries (offsets

@@ -137,32 +137,20 @@ __global__ void __launch_bounds__(kPortThreads)
     if (threadIdx.x < M) s_vint[threadIdx.x] = red[threadIdx.x];
     __syncthreads();
 
-    // 2. DTBC boundary convolutions: conv_w = sum_{m=1..n} l_m w[n-m],
-    //    u_inc = sum l_m s[n-m] with the kernel table in effect at chain
-    //    step n (auto-extended by doubling, dtbc.py:351-363).
-    long long tlen = d.n0;
-    long long toff = 0;
-    while (tlen < n + 1) {
-        toff += tlen;
-        tlen *= 2;
-    }
+    // 2. DTBC boundary convolutions conv_w = sum_{m=1..n} l_m w[n-m] and
+    //    u_inc = sum l_m s[n-m]: the partial sums k_dtbc_conv left per
+    //    history chunk, added in chunk order (a fixed order: the result does
+    //    not depend on scheduling).
     const int exc = d.exc_mode[b];
-    for (int m = 0; m < 2 * kMaxModes; ++m) acc[m] = 0.0;
-    for (int m = 0; m < M; ++m) {
-        if (!d.is_dtbc[m]) continue;
-        const double* lt = d.ktab[m] + toff;
-        const double* wh = d.whist + ((long long)b * M + m) * d.cap;
-        const double* sh = d.shist + ((long long)b * M + m) * d.cap;
-        double aw = 0.0, as = 0.0;
-        for (long long i = threadIdx.x; i < n; i += blockDim.x) {
-            const double l = lt[n - i];
-            aw += l * wh[i];
-            as += l * sh[i];
-        }
-        acc[2 * m] = aw;
-        acc[2 * m + 1] = as;
+    if (threadIdx.x < 2 * M && d.is_dtbc[threadIdx.x >> 1]) {
+        const int m = threadIdx.x >> 1, w = threadIdx.x & 1;
+        const int nck = (int)((n + kConvChunk - 1) / kConvChunk);
+        const double* part = d.conv + (((long long)b * M + m) * d.conv_chunks) * 2 + w;
+        double a = 0.0;
+        for (int c = 0; c < nck; ++c) a += part[2 * c];
+        red[threadIdx.x] = a;
     }
-    block_sum<2 * kMaxModes>(acc, 2 * M, red, wred);
+    __syncthreads();
 
     // 3. Per-mode boundary value (one thread; scalar float64 recursions).
     if (threadIdx.x == 0) {
@@ -248,7 +236,65 @@ __global__ void __launch_bounds__(kPortThreads)
     }
 }
 
+// Partial DTBC convolutions of the coming update at chain step n (the
+// step counter): chunk c of the history, i in [c K, (c + 1) K) and i < n,
+// of every DTBC mode of port blockIdx.z, field set blockIdx.y, with the
+// kernel table in effect at step n (auto-extended by doubling,
+// dtbc.py:351-363, dtbc.py:417-463).  Only history before step n is read,
+// so this runs beside the stencil of the same step.
+constexpr int kConvThreads = 128;
+
+__global__ void __launch_bounds__(kConvThreads) k_dtbc_conv(PortsArgs pa, const ModalDev* __restrict__ ports) {
+    const ModalDev& d = ports[blockIdx.z];
+    const int b = blockIdx.y, c = blockIdx.x;
+    const long long n = *pa.step;
+    const long long lo = (long long)c * kConvChunk;
+    if (c >= d.conv_chunks || lo >= n) return;
+    const long long hi = min(lo + kConvChunk, n);
+    const int M = d.n_modes;
+    long long tlen = d.n0;
+    long long toff = 0;
+    while (tlen < n + 1) {
+        toff += tlen;
+        tlen *= 2;
+    }
+    __shared__ double wsum[kConvThreads / 32][2];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int m = 0; m < M; ++m) {
+        if (!d.is_dtbc[m]) continue;
+        const double* lt = d.ktab[m] + toff;
+        const double* wh = d.whist + ((long long)b * M + m) * d.cap;
+        const double* sh = d.shist + ((long long)b * M + m) * d.cap;
+        double aw = 0.0, as = 0.0;
+        for (long long i = lo + threadIdx.x; i < hi; i += kConvThreads) {
+            const double l = lt[n - i];
+            aw += l * wh[i];
+            as += l * sh[i];
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            aw += __shfl_xor_sync(0xffffffffu, aw, o);
+            as += __shfl_xor_sync(0xffffffffu, as, o);
+        }
+        if (lane == 0) {
+            wsum[warp][0] = aw;
+            wsum[warp][1] = as;
+        }
+        __syncthreads();
+        if (threadIdx.x < 2) {
+            double a = 0.0;
+            for (int w = 0; w < kConvThreads / 32; ++w) a += wsum[w][threadIdx.x];
+            d.conv[(((long long)b * M + m) * d.conv_chunks + c) * 2 + threadIdx.x] = a;
+        }
+        __syncthreads();
+    }
+}
+
 }  // namespace
+
+void launch_dtbc_conv(const PortsArgs& pa, const ModalDev* d, int n_modal, int max_chunks, cudaStream_t s) {
+    if (n_modal <= 0 || max_chunks <= 0) return;
+    k_dtbc_conv<<<dim3(max_chunks, pa.B, n_modal), kConvThreads, 0, s>>>(pa, d);
+}
 
 template <typename T>
 void launch_lumped(T* e, const PortsArgs& pa, const LumpedDev* d, int n_lumped, cudaStream_t s) {
