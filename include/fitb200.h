@@ -337,6 +337,21 @@ int fitb_poll_signal_absmax(fitb_handle* h, int32_t b, double* out);
 int fitb_channel_count(fitb_handle* h, int32_t* out);
 int fitb_read_vi(fitb_handle* h, int32_t b, int64_t step0, int64_t n,
                  double* V, double* I);
+/* Modal S-parameters of the recorded steps [0, steps_done), computed on the
+ * device from the V/I records without reading them back (replaces the host
+ * post-step compute_s_parameters, src/magnelio/post/modal_sparameters.py
+ * :335-545, over Signal1D.at_frequencies, src/magnelio/signals/
+ * signal_1d.py:59-97): per field set and channel the direct DFT
+ * sum_n x_n exp(-2 pi j f n dt) of V and I at the nf frequencies f [Hz], I
+ * advanced by exp(+j pi f dt) unless icot[c] (I sampled with V), the power
+ * waves a = aV V + aI I, b = bV V + bI I with the caller's per-channel maps
+ * ([nch][4][nf] complex as (re, im) pairs: aV, aI, bV, bI), and
+ * S[f][c][b] = b_c / a_excited[b] (complex, (re, im) pairs) where
+ * |a_excited| >= a_threshold * its peak over f, NaN elsewhere and for field
+ * sets with excited[b] = -1.  A (optional, [nf][B] complex) receives
+ * a_excited.  Float64 throughout. */
+int fitb_s_params(fitb_handle* h, int32_t nf, const double* f, const double* maps, const int32_t* icot,
+                  const int32_t* excited, double a_threshold, double* S, double* A);
 
 /* ---- checkpoint ----------------------------------------------------- */
 /* Byte size of the full evolving state (fields, psi, port and monitor

@@ -153,6 +153,7 @@ SIGNATURES = {
     "fitb_poll_signal_absmax": ([vp, i32, P_f64], C.c_int),
     "fitb_channel_count": ([vp, P_i32], C.c_int),
     "fitb_read_vi": ([vp, i32, i64, i64, P_f64, P_f64], C.c_int),
+    "fitb_s_params": ([vp, i32, P_f64, P_f64, P_i32, P_i32, C.c_double, P_f64, P_f64], C.c_int),
     "fitb_state_size": ([vp, C.POINTER(sz)], C.c_int),
     "fitb_state_export": ([vp, vp, sz], C.c_int),
     "fitb_state_import": ([vp, cvp, sz], C.c_int),

@@ -2404,6 +2404,41 @@ int fitb_read_vi(fitb_handle* h, int32_t b, int64_t step0, int64_t n, double* V,
     FITB_CATCH
 }
 
+int fitb_s_params(fitb_handle* h, int32_t nf, const double* f, const double* maps, const int32_t* icot,
+                  const int32_t* excited, double a_threshold, double* S, double* A) {
+    FITB_TRY
+    Handle& H = H_of(h);
+    if (nf < 1 || !f || !maps || !icot || !excited || !S) fail(FITB_ERR_ARG, "bad argument");
+    if (H.nch == 0) fail(FITB_ERR_STATE, "no port channels are recorded");
+    if (H.steps_done < 1) fail(FITB_ERR_STATE, "no steps recorded");
+    for (int b = 0; b < H.B; ++b)
+        if (excited[b] < -1 || excited[b] >= H.nch) fail(FITB_ERR_ARG, "excited channel %d out of range", excited[b]);
+    ck(cudaStreamSynchronize(H.stream), "sync");
+    fitb::check_device_status(H);
+    const int nch = H.nch;
+    fitb::DevBuf df, dmaps, dicot, dexc, xv, xi, dS, dA;
+    fitb::upload(df, std::vector<double>(f, f + nf));
+    fitb::upload(dmaps, std::vector<double>(maps, maps + (size_t)nch * 4 * nf * 2));
+    fitb::upload(dicot, std::vector<int>(icot, icot + nch));
+    fitb::upload(dexc, std::vector<int>(excited, excited + H.B));
+    const size_t nx = (size_t)H.B * nch * nf;
+    xv.alloc(nx * sizeof(double2), false);
+    xi.alloc(nx * sizeof(double2), false);
+    dS.alloc((size_t)nf * nch * H.B * sizeof(double2), false);
+    if (A) dA.alloc((size_t)nf * H.B * sizeof(double2), false);
+    fitb::launch_vi_dft(H.recV.as<double>(), H.recI.as<double>(), H.cap, nch, H.steps_done, H.B, df.as<double>(), nf,
+                        H.dt, xv.as<double2>(), xi.as<double2>(), H.stream);
+    fitb::launch_s_assemble(xv.as<double2>(), xi.as<double2>(), nch, nf, df.as<double>(), H.dt,
+                            dmaps.as<double2>(), dicot.as<int>(), dexc.as<int>(), a_threshold, H.B,
+                            dS.as<double2>(), A ? dA.as<double2>() : nullptr, H.stream);
+    ck(cudaGetLastError(), "s-parameter launch");
+    ck(cudaMemcpyAsync(S, dS.p, dS.bytes, cudaMemcpyDeviceToHost, H.stream), "S D2H");
+    if (A) ck(cudaMemcpyAsync(A, dA.p, dA.bytes, cudaMemcpyDeviceToHost, H.stream), "A D2H");
+    ck(cudaStreamSynchronize(H.stream), "S sync");
+    H.launches += 2;
+    FITB_CATCH
+}
+
 int fitb_state_size(fitb_handle* h, size_t* out) {
     FITB_TRY
     Handle& H = H_of(h);

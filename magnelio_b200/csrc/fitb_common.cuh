@@ -428,6 +428,15 @@ void launch_dft_flush_all(int B, const DftDev* devs, int nmon, int nblocks, size
 // Host-requested flush of the first kc slots of one monitor.
 void launch_dft_flush_forced(int B, const DftDev& d, int kc, cudaStream_t s);
 
+// Modal S-parameters from the recorder (sparams.cu): the direct DFT of every
+// field set's V and I channels over steps [0, N), then the power-wave split
+// and S = b / a_excited per field set (excitation).
+void launch_vi_dft(const double* V, const double* I, long long cap, int nch, long long N, int B, const double* f,
+                   int nf, double dt, double2* xv, double2* xi, cudaStream_t s);
+void launch_s_assemble(const double2* xv, const double2* xi, int nch, int nf, const double* f, double dt,
+                       const double2* maps, const int* icot, const int* excited, double thr, int B, double2* S,
+                       double2* A, cudaStream_t s);
+
 // Energy: per field set 0.5 (sum m_eps e^2 + sum m_mu h^2) in float64.
 template <typename T>
 void launch_energy(const T* e, const T* h, const T* meps, const T* mmu, const Geom& g, int b,

@@ -469,6 +469,30 @@ class FitEngine:
             check(self._lib.fitb_read_vi(self._h, int(b), int(step0), int(n), f64p(V), f64p(I)))
         return V, I
 
+    def s_parameters(self, f, maps, i_cotemporal, excited, a_threshold: float = 1e-12,
+                     return_incident: bool = False):
+        """Modal S-matrix ``S[f, c, b]`` of the recorded steps, computed on the
+        device from the V/I records (the device form of
+        :func:`magnelio_b200.sparams.s_matrix`): ``maps[c]`` the (4, F)
+        power-wave coefficients of channel c, ``i_cotemporal[c]`` whether I
+        is sampled with V, ``excited[b]`` the channel field set b drives (-1:
+        none).  With ``return_incident`` also ``a_excited[f, b]``."""
+        f = np.ascontiguousarray(np.asarray(f, dtype=np.float64).ravel())
+        nch = self.n_channels
+        m = np.asarray(maps, dtype=np.complex128)
+        if m.shape != (nch, 4, f.size):
+            raise ValueError(f"maps must have shape ({nch}, 4, {f.size}), got {m.shape}")
+        mp = np.ascontiguousarray(m).view(np.float64)
+        icot = np.ascontiguousarray(np.asarray(i_cotemporal, dtype=np.int32))
+        exc = np.full(self.batch, -1, dtype=np.int32)
+        exc[: len(excited)] = np.asarray(excited, dtype=np.int32)
+        S = np.zeros((f.size, nch, self.batch), dtype=np.complex128)
+        A = np.zeros((f.size, self.batch), dtype=np.complex128) if return_incident else None
+        check(self._lib.fitb_s_params(self._h, int(f.size), f64p(f), f64p(mp), i32p(icot), i32p(exc),
+                                      float(a_threshold), f64p(S.view(np.float64)),
+                                      None if A is None else f64p(A.view(np.float64))))
+        return (S, A) if return_incident else S
+
     # ---- checkpoint ------------------------------------------------------
     def state_export(self) -> bytes:
         n = C.c_size_t()

@@ -469,6 +469,43 @@ def test_wr90_six_excitations_batched_match_the_reference_s_matrix(precision):
         assert _rel(e, d["out.e"]) < WR90_VI_TOL[precision]
 
 
+@pytest.mark.parametrize("precision", ["double", "single"])
+def test_wr90_s_matrix_on_the_device(precision):
+    """The S-parameter post-step on the device (direct DFT of the recorded
+    V/I, power waves, S = b / a_excited) equals the host assembly of the same
+    records to float64 round-off, and meets the reference S-matrix bar."""
+    from magnelio_b200 import sparams
+
+    p, d, n = load_golden("cfg1_wr90")
+    c = sparams.load_cfg1(d)
+    n_exc = p.batch
+    p.batch = 8
+    for mp in p.modal:
+        mp.excitation = list(mp.excitation) + [None] * (8 - n_exc)
+    p.e0 = list(p.e0) + [None] * (8 - n_exc)
+    p.h0 = list(p.h0) + [None] * (8 - n_exc)
+    with p.build_engine(precision) as eng:
+        eng.step(n)
+        VI = [eng.read_vi(b) for b in range(n_exc)]
+        S_dev, A_dev = eng.s_parameters(c["f"], np.stack(c["maps"]), c["icot"], c["excited"], return_incident=True)
+    assert np.all(np.isnan(S_dev[:, :, n_exc:]))  # idle field sets
+    S_dev, A_dev = S_dev[:, :, :n_exc], A_dev[:, :n_exc]
+    S_host, A_host = sparams.s_matrix([v for v, _ in VI], [i for _, i in VI], c["dt"], c["f"], c["maps"],
+                                      c["icot"], c["excited"], return_incident=True)
+    assert _rel(A_dev, A_host) < 1e-11
+    # inside each excitation's band (|a_excited| >= 1 % of its peak; outside
+    # it S divides by a vanishing wave and amplifies round-off)
+    in_band = np.abs(A_host) >= WR90_BAND * np.max(np.abs(A_host), axis=0, keepdims=True)
+    sel = np.isfinite(S_host) & in_band[:, None, :]
+    assert np.all(np.isfinite(S_dev[sel]))
+    assert float(np.max(np.abs(S_dev[sel] - S_host[sel]) / np.maximum(1.0, np.abs(S_host[sel])))) < 1e-9
+    ref, A = sparams.s_matrix(c["V"], c["I"], c["dt"], c["f"], c["maps"], c["icot"], c["excited"],
+                              return_incident=True)
+    band = np.abs(A) >= WR90_BAND * np.max(np.abs(A), axis=0, keepdims=True)
+    sel = np.isfinite(ref) & (np.abs(ref) <= 1.05) & band[:, None, :]
+    assert float(np.abs(S_dev - ref)[sel].max()) <= WR90_S_TOL[precision]
+
+
 @pytest.mark.parametrize("precision,tol", [("double", F64_TOL), ("single", F32_TOL)])
 def test_slab_workload_built_on_the_host_matches_the_oracle(precision, tol):
     """The precision workload (Lorentz ADE slab through the CPML, TF/SF plane
