@@ -266,9 +266,13 @@ def main(argv=None) -> int:
     ap.add_argument("--batch", type=int, default=1, help="field sets sharing one coefficient set")
     ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of CPU-port timing")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--sweep", type=int, nargs="*", default=[512],
+                    help="more grid sizes timed after the headline one (N=1 only; none: --sweep)")
     ap.add_argument("--parity-steps", type=int, default=300,
                     help="steps of the float64 parity prefix on the timed workload (0: none)")
     ap.add_argument("--no-tune", action="store_true", help="skip the autotuner (keep the default stencil plan)")
+    ap.add_argument("--stencil", default=None, metavar="KIND:VARIANT[:ICHUNK]",
+                    help="run this stencil form instead of the autotuner's pick (e.g. fused:16)")
     ap.add_argument("--workload", choices=("brick_box", "slab", "cross"), default="brick_box",
                     help="brick_box (plain method at scale), slab (dispersive slab, TF/SF plane wave, 384x384x192) "
                          "or cross (four-port junction, eight excitations batched vs one at a time)")
@@ -324,8 +328,9 @@ def run_serving(args, world, rank, local):
     cells = (max(8**3, int(32**3 * sc)), max(8**3, int(192**3 * sc)))
     steps = (max(100, int(6000 * sc)), max(100, int(12000 * sc)))
     reqs = serving.request_stream(args.serving_requests, seed=2027 + rank, mean_gap=0.020, cells=cells, steps=steps)
-    batched = serving.ServingLoop(device=local, max_slots=8, slice_steps=512).run(reqs)
-    plain = serving.ServingLoop(device=local, slice_steps=512).run(reqs, plain=True)
+    # S-matrices from the device post-step: the V/I histories never leave the GPU
+    batched = serving.ServingLoop(device=local, max_slots=8, slice_steps=512, records=False).run(reqs)
+    plain = serving.ServingLoop(device=local, slice_steps=512, records=False).run(reqs, plain=True)
     # the slowest replica bounds the whole job
     solves = -_max_over_ranks(-batched.solves_per_s, world, local)
     if rank == 0:
@@ -335,6 +340,7 @@ def run_serving(args, world, rank, local):
             "data": "synthetic (seeded waveguide-section request stream)",
             "config": {"workload": "serving_stream", "requests": len(reqs), "arrivals": "Poisson, mean gap 20 ms",
                        "cells": list(cells), "steps": list(steps), "ports": "2-4 lumped, 50 ohm",
+                       "s_matrix": "device post-step (fitb_s_params)",
                        "max_slots": 8, "slice_steps": 512,
                        "stencil": {"batched": str(serving.serving_stencil(2) or "engine default (batched two-pass)"),
                                    "plain": str(serving.serving_stencil(1) or "engine default")},
@@ -512,6 +518,44 @@ def run_slab(args, world, rank, local):
     return 0
 
 
+SWEEP_CANDIDATES = (("stream", 0, 0), ("fused", 7, 0), ("fused", 16, 0), ("fused", 17, 0), ("fused", 18, 0),
+                    ("fused", 19, 0))
+
+
+def sweep_point(n: int, args, local: int) -> dict:
+    """One more grid size of the same workload, timed the same way as the
+    headline (device time of graph-replayed steps, clocks sampled over the
+    timed region), with the stencil tuned over the fastest forms."""
+    from magnelio_b200 import autotune, workloads
+
+    total = args.warmup + args.steps + 8
+    prob = workloads.brick_box(n, steps=total)
+    tuned = autotune.tune_problem(prob, "single", device=local, candidates=SWEEP_CANDIDATES, iters=3)
+    eng = prob.build_engine("single", device=local)
+    try:
+        autotune.apply(eng, tuned)
+        sampler = ClockSampler(local)
+        eng.step(args.warmup)
+        eng.sync()
+        sampler.window(True)
+        ms = eng.step_timed(args.steps)
+        sampler.window(False)
+        clocks = sampler.stop()
+        t_e, t_h = eng.time_stencil(10)
+        cfg = eng.stencil_config()
+    finally:
+        eng.close()
+    cpml_cells = workloads.cells_in_cpml(prob)
+    alg = BYTES_PER_CELL * n**3 + BYTES_PER_CPML_CELL * cpml_cells
+    peak, peak_kind = _peaks()
+    achieved = alg / ((t_e + t_h) * 1e-3) / 1e9
+    return {"size": n, "value": n**3 * args.steps / (ms * 1e-3) / 1e9, "unit": METRIC,
+            "ms_per_step": ms / args.steps, "stencil": cfg,
+            "roofline": {"achieved": achieved, "peak": peak, "peak_kind": peak_kind, "frac": achieved / peak,
+                         "algorithmic_bytes": alg, "ms_stencil": t_e + t_h},
+            "clocks": clocks}
+
+
 def run_b200(args, world, rank, local):
     from magnelio_b200 import workloads
 
@@ -525,7 +569,13 @@ def run_b200(args, world, rank, local):
         v = prob.lumped[0].v_src[0]
         prob.lumped[0].v_src = [v * (1.0 + 0.1 * b) for b in range(B)]
     tuned = None
-    if not args.no_tune:
+    if args.stencil:
+        from magnelio_b200 import autotune
+
+        parts = args.stencil.split(":")
+        tuned = autotune.TuneResult(kind=parts[0], variant=int(parts[1]) if len(parts) > 1 else 0,
+                                    ichunk=int(parts[2]) if len(parts) > 2 else 0, batch=B, ms=0.0, gcells=0.0)
+    elif not args.no_tune:
         # stencil form, march depth: fastest on this GPU for this grid / batch
         from magnelio_b200 import autotune
 
@@ -614,14 +664,18 @@ def run_b200(args, world, rank, local):
                          f"(C+OpenMP port, float32, {threads} threads, {secs:.1f} s)"}
         if args.parity_steps > 0:
             parity = parity_prefix(prob, tuned, args.parity_steps, local)
+    sweep = None
+    if rank == 0 and world == 1 and B == 1 and args.sweep:
+        sweep = [sweep_point(m, args, local) for m in args.sweep if m != n]
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded brick box, host-built coefficients)",
             "config": dict(_config(args, prob), stencil=stencil_cfg,
-                           autotune=None if tuned is None else [list(r[:3]) + [round(r[4], 4)] for r in tuned.table]),
-            "roofline": roofline, "cpu_baseline": cpu, "parity": parity,
+                           autotune=None if tuned is None or not tuned.table
+                           else [list(r[:3]) + [round(r[4], 4)] for r in tuned.table]),
+            "roofline": roofline, "cpu_baseline": cpu, "parity": parity, "sweep": sweep,
             "e2e": {"value": e2e, "unit": METRIC, "h2d_bytes_per_step": 8, "d2h_bytes_per_step": 16 * nch,
                     "how": "per step: pinned H2D of the source sample, one fitb_step, D2H of the step's V/I"},
             "gpu_launches": launches, "clocks": clocks,

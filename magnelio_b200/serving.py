@@ -129,8 +129,12 @@ class ServingLoop:
 
     def __init__(self, device: int = 0, precision: str = "single", hbm_budget: int | None = None,
                  max_slots: int = 8, slice_steps: int = 512, engine_factory=None, tune=None,
-                 clock=time.perf_counter, sleep=time.sleep, stencil=serving_stencil):
+                 clock=time.perf_counter, sleep=time.sleep, stencil=serving_stencil, records: bool = True):
         self.device = device
+        # records=False: S-matrices come from the device post-step
+        # (FitEngine.s_parameters) and the V/I histories stay on the device
+        # (Result.V / Result.I are None)
+        self.records = records
         self.precision = precision
         self.stencil = stencil        # callable(batch) -> (kind, variant) or None (the engine default)
         self.max_slots = max_slots
@@ -221,12 +225,26 @@ class ServingLoop:
                 req = a["req"]
                 eng = a["eng"]
                 nset = a["prob"].batch
-                VI = [eng.read_vi(b) for b in range(nset)]
+                on_device = not self.records and hasattr(eng, "s_parameters")
+                if on_device:
+                    VI = None
+                    cols = self._device_columns(eng, req, a["port"])
+                else:
+                    VI = [eng.read_vi(b) for b in range(nset)]
                 dev_bytes = eng.device_bytes
                 eng.close()
                 used -= a["fp"]
                 fin = self.clock() - t0
-                if a["port"] is None:
+                if on_device:
+                    got = partial.setdefault(req.rid, {})
+                    got.update(cols)
+                    if len(got) == req.n_ports:
+                        S = np.stack([got[p] for p in range(req.n_ports)], axis=2)
+                        results.append(Result(rid=req.rid, S=S, V=None, I=None, arrival=req.arrival,
+                                              admitted=a["admitted"], finished=fin, footprint=a["fp"],
+                                              device_bytes=dev_bytes))
+                        del partial[req.rid]
+                elif a["port"] is None:
                     V = np.stack([v for v, _ in VI[:req.n_ports]])
                     I = np.stack([i for _, i in VI[:req.n_ports]])
                     results.append(self._result(req, V, I, a, fin, dev_bytes))
@@ -291,6 +309,23 @@ class ServingLoop:
             prob.e0 = prob.e0[:1]
             prob.h0 = prob.h0[:1]
         return prob
+
+    @staticmethod
+    def _device_columns(eng, req, port):
+        """S-matrix columns of a finished handle from the device post-step:
+        {driven port: S[:, :, port]}.  Lumped-port power waves
+        a = (V + Z0 I) / (2 sqrt Z0), b = (V - Z0 I) / (2 sqrt Z0) (the maps
+        of :func:`magnelio_b200.workloads.s_matrix`; its time origin and dt
+        factor are common to a and b and cancel in b / a), I taken with V."""
+        P, F = req.n_ports, len(req.freqs)
+        nch = eng.n_channels
+        rz = np.sqrt(req.z0)
+        maps = np.zeros((nch, 4, F), complex)
+        maps[:, 0], maps[:, 1] = 1.0 / (2 * rz), req.z0 / (2 * rz)
+        maps[:, 2], maps[:, 3] = 1.0 / (2 * rz), -req.z0 / (2 * rz)
+        driven = list(range(P)) if port is None else [port]
+        S = eng.s_parameters(req.freqs, maps, np.ones(nch, np.int32), driven, a_threshold=0.0)
+        return {p: S[:, :P, b] for b, p in enumerate(driven)}
 
     def _result(self, req, V, I, a, fin, dev_bytes):
         from magnelio_b200.workloads import s_matrix

@@ -74,3 +74,19 @@ def test_served_s_matrix_meets_the_fp64_oracle():
     big = np.abs(S_ref) > 0.05
     dphi = np.degrees(np.abs(np.angle(res.S[big] / S_ref[big])))
     assert float(dphi.max()) <= PHASE_TOL, float(dphi.max())
+
+
+@pytest.mark.parametrize("plain", [False, True])
+def test_device_s_matrix_equals_the_host_assembly_of_the_records(plain):
+    """With the V/I histories left on the device (records=False) the served
+    S-matrices come from the device post-step; they equal the host assembly
+    of the same runs' records to float64 round-off, in the batched and the
+    single-excitation forms."""
+    from magnelio_b200 import serving
+
+    reqs = _stream()[:3]
+    host = serving.ServingLoop(max_slots=4, slice_steps=128).run(reqs, plain=plain)
+    dev = serving.ServingLoop(max_slots=4, slice_steps=128, records=False).run(reqs, plain=plain)
+    for a, b in zip(host.results, dev.results):
+        assert a.rid == b.rid and b.V is None and b.S.shape == a.S.shape
+        assert float(np.max(np.abs(a.S - b.S) / np.maximum(1.0, np.abs(a.S)))) < 1e-9
