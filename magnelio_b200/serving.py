@@ -96,7 +96,7 @@ def estimate_footprint(nx, ny, nz, batch, steps, n_channels, cpml_layers=(), pre
     for axis, n in cpml_layers:
         dims = [nx + 1, ny + 1, nz + 1]
         dims[axis] = n
-        slab = dims[0] * dims[1] * dims[2]
+        slab = dims[0] * dims[1] * (-(-dims[2] // 16) * 16)  # rows padded to 16 entries
         total += sets * batch * 4 * slab * esz + 4 * slab + 3 * n * esz
     cap = max(int(steps), 1024)
     total += 2 * batch * cap * max(n_channels, 1) * 8

@@ -160,7 +160,7 @@ def test_footprint_estimate_counts_the_big_buffers():
     assert fp > 2 * 4 * 3 * vol * 4 + 6 * 3 * vol * 4
     # the fused step's second buffer set: fields and psi once more
     fpf = serving.estimate_footprint(64, 64, 64, 4, 1000, 4, [(2, 8), (2, 8)], fused=True)
-    assert fpf - fp == 2 * 4 * 3 * vol * 4 + 2 * 4 * 4 * (65 * 65 * 8) * 4
+    assert fpf - fp == 2 * 4 * 3 * vol * 4 + 2 * 4 * 4 * (65 * 65 * 16) * 4  # psi rows padded to 16
     with pytest.raises(TypeError):
         serving.estimate_footprint(64, 64)
 
