@@ -457,6 +457,11 @@ void build_fix_cells(Handle& H) {
         for (long long o : mp->port_e_host) add_edge(o);
     for (auto& pw : H.pws)
         for (long long o : pw->e_off_host) add_edge(o);
+    // the slab step with E-side dispersion: the ADE update corrects E after
+    // the step kernel's H update, so the H cells next to dispersive edges
+    // are recomputed like those next to port edges
+    if (is_slab_variant(H.fused_variant))
+        for (long long o : H.disp[0].off) add_edge(o);
     std::sort(keys.begin(), keys.end());
     keys.erase(std::unique(keys.begin(), keys.end()), keys.end());
     std::vector<int4> cells;
@@ -539,7 +544,8 @@ StencilArgs<T> stencil_args(Handle& H) {
         if (H.cur) std::swap(a.f[q].psi, a.f[q].psi_next);
     }
     a.ichunk = H.ichunk;
-    a.coef_kind = (H.stencil_mode == kModeStream || H.stencil_mode == kModeVec) ? H.coef_kind : kCoefNative;
+    const bool slab = H.stencil_mode == kModeFused && is_slab_variant(H.fused_variant);
+    a.coef_kind = (H.stencil_mode == kModeStream || H.stencil_mode == kModeVec || slab) ? H.coef_kind : kCoefNative;
     for (int q = 0; q < 4; ++q) a.cq[q] = H.cq[q].as<unsigned short>();
     for (int q = 0; q < 16; ++q) a.cs[q] = H.cs[q];
     return a;
@@ -640,7 +646,28 @@ bool tile_skip_on(const Handle& H) {
     return !(e && std::string(e) == "0") && H.pws.empty() && !H.disp[0].present() && !H.disp[1].present();
 }
 
+// Whether no dispersive state lies in a CPML slab.  The slab step applies
+// the CPML inside its kernel, before the ADE update of the same side; the
+// reference applies the ADE update first (fit_td.py:833-874), so the two
+// orders agree exactly when no entry takes both.
+bool disp_clear_of_cpml(const Handle& H) {
+    for (const DispHost& D : H.disp)
+        for (long long off : D.off) {
+            const long long r = off % H.g.vol;
+            const int i = (int)(r / H.g.si) - 2;
+            const long long rr = r % H.g.si;
+            const int j = (int)(rr / H.g.sj), k = (int)(rr % H.g.sj);
+            for (auto& f : H.faces) {
+                const int c = f->dev.axis == 0 ? i : (f->dev.axis == 1 ? j : k);
+                if (c >= f->dev.lo && c < f->dev.lo + f->dev.n) return false;
+            }
+        }
+    return true;
+}
+
 void build_slab_units(Handle& H) {
+    if ((H.disp[0].present() || H.disp[1].present()) && !disp_clear_of_cpml(H))
+        fail(FITB_ERR_STATE, "the slab step takes dispersive materials only outside the CPML slabs");
     std::vector<int4> lists[kSlabLists];
     const int ichunk = H.splan.ichunk, tj = slab_tj_of(H.fused_variant - kFusedSlabBase);
     if (!slab_units_of(H, H.fused_variant, ichunk, lists))
@@ -852,9 +879,22 @@ int enqueue_step_fused(Handle& H) {
     PortsArgs pa = ports_args(H);
     StencilArgs<T> sa = stencil_args<T>(H);
     n += fork_dtbc_conv(H, pa);
+    // ADE (slab step only): the pole histories take the fields before the
+    // step, which the current buffer set still holds
+    for (int sd = 0; sd < 2; ++sd) {
+        if (!H.disp[sd].present()) continue;
+        launch_disp_save<T>((sd == 0 ? H.Ec() : H.Hc()).as<T>(), H.e_block(), H.B, H.disp[sd].dev, H.stream);
+        ++n;
+    }
     n += launch_fused<T>(H, sa);
     T* e_new = H.En().as<T>();
     T* h_new = H.Hn().as<T>();
+    if (H.disp[0].present()) {
+        // E-side ADE after the curl update and the CPML (which never share
+        // an entry with it, disp_clear_of_cpml), before the ports
+        launch_disp_update<T>(e_new, H.e_block(), H.B, H.bE.as<T>(), H.disp[0].dev, H.stream);
+        n += 2;
+    }
     for (auto& pw : H.pws) {
         launch_plane_wave<T>(e_new, H.e_block(), H.B, pw->dev, 0, H.step.as<long long>(), H.stream);
         ++n;
@@ -876,6 +916,10 @@ int enqueue_step_fused(Handle& H) {
     if (H.n_fix > 0) {
         launch_fix_H<T>(sa, H.fix_cells.as<int4>(), H.n_fix, H.stream);
         ++n;
+    }
+    if (H.disp[1].present()) {
+        launch_disp_update<T>(h_new, H.e_block(), H.B, H.bH.as<T>(), H.disp[1].dev, H.stream);
+        n += 2;
     }
     for (auto& pw : H.pws) {
         launch_plane_wave<T>(h_new, H.e_block(), H.B, pw->dev, 1, H.step.as<long long>(), H.stream);
@@ -1365,7 +1409,7 @@ int fitb_create(const fitb_desc* desc, fitb_handle** out) {
     g.ny = desc->ny;
     g.nz = desc->nz;
     g.njp = g.ny + 2;
-    g.nkp = (int)fitb::round_up(g.nz + 2, 4);
+    g.nkp = (int)fitb::round_up(g.nz + 2, 8);
     g.sj = g.nkp;
     g.si = (long long)g.njp * g.nkp;
     g.vol = (long long)(g.nx + 4) * g.si + (long long)fitb::kTailRows * g.sj;
@@ -1511,8 +1555,12 @@ int fitb_set_coeff_storage(fitb_handle* h, int32_t kind) {
     FITB_TRY
     Handle& H = H_of(h);
     if (kind < fitb::kCoefNative || kind > fitb::kCoefBF16) fail(FITB_ERR_ARG, "coefficient storage kind %d", kind);
-    if (kind != fitb::kCoefNative && H.stencil_mode != fitb::kModeStream && H.stencil_mode != fitb::kModeVec)
-        fail(FITB_ERR_STATE, "compact coefficient storage needs the stream stencil kernels");
+    const bool slab = H.stencil_mode == fitb::kModeFused && fitb::is_slab_variant(H.fused_variant);
+    if (kind != fitb::kCoefNative && H.stencil_mode != fitb::kModeStream && H.stencil_mode != fitb::kModeVec &&
+        !(slab && kind == fitb::kCoefF16 && H.prec == 4))
+        fail(FITB_ERR_STATE,
+             "compact coefficient storage needs the stream or vec stencil kernels (float16: also the float32 slab "
+             "step)");
     H.coef_kind = kind;
     if (kind == fitb::kCoefNative) {
         for (auto& q : H.cq) q.release();
@@ -1529,8 +1577,11 @@ int fitb_configure_stencil(fitb_handle* h, int32_t kind, int32_t variant, int32_
     if (kind < fitb::kModeSimple || kind > fitb::kModeFused) fail(FITB_ERR_ARG, "stencil kind %d", kind);
     if (ichunk < 0) fail(FITB_ERR_ARG, "ichunk %d", ichunk);
     const bool compact = H.coef_kind != fitb::kCoefNative;
-    if (compact && kind != fitb::kModeStream && kind != fitb::kModeVec)
-        fail(FITB_ERR_STATE, "compact coefficient storage needs the stream or vec stencil kernels");
+    if (compact && kind != fitb::kModeStream && kind != fitb::kModeVec &&
+        !(kind == fitb::kModeFused && fitb::is_slab_variant(variant) && H.coef_kind == fitb::kCoefF16 && H.prec == 4))
+        fail(FITB_ERR_STATE,
+             "compact coefficient storage needs the stream or vec stencil kernels (float16: also the float32 slab "
+             "step)");
     if ((kind == fitb::kModeStream || kind == fitb::kModeVec) && !fitb::stream_batch_supported(H.B))
         fail(FITB_ERR_ARG, "the stream / vec kernels take 1, 2, 4, 8 or 16 field sets, not %d", H.B);
     if (kind == fitb::kModeStream && !fitb::stream_variant_supported(H.B, variant))
@@ -1539,8 +1590,11 @@ int fitb_configure_stencil(fitb_handle* h, int32_t kind, int32_t variant, int32_
         fail(FITB_ERR_ARG, "vec stencil: variant %d / batch %d", variant, H.B);
     if (kind == fitb::kModeFused) {
         if (!fitb::fused_variant_ok(H.prec, variant)) fail(FITB_ERR_ARG, "fused variant %d", variant);
-        if (H.disp[0].present() || H.disp[1].present())
-            fail(FITB_ERR_STATE, "dispersive materials need an in-place stencil mode (not the fused step)");
+        if ((H.disp[0].present() || H.disp[1].present()) && !fitb::is_slab_variant(variant))
+            fail(FITB_ERR_STATE,
+                 "dispersive materials need an in-place stencil mode or the slab step (fused 16-19)");
+        if ((H.disp[0].present() || H.disp[1].present()) && !fitb::disp_clear_of_cpml(H))
+            fail(FITB_ERR_STATE, "the slab step takes dispersive materials only outside the CPML slabs");
         if (fitb::is_tile_variant(variant) &&
             !(H.prec == 4 ? fitb::tile_step_fits<float>(fitb::stencil_args<float>(H))
                           : fitb::tile_step_fits<double>(fitb::stencil_args<double>(H))))
@@ -1970,8 +2024,8 @@ int fitb_add_dispersion_block(fitb_handle* h, int32_t side, int64_t n_states, co
     if (n_states < 1 || n_poles < 1 || !idx || !g || !kind || !k_re || !k_im || !c_re || !c_im || !weight)
         fail(FITB_ERR_ARG, "dispersion block needs states, poles and all arrays");
     if (H.steps_done != 0) fail(FITB_ERR_STATE, "dispersion must be added before the first step");
-    if (H.stencil_mode == fitb::kModeFused)
-        fail(FITB_ERR_STATE, "dispersive materials need an in-place stencil mode (not the fused step)");
+    if (H.stencil_mode == fitb::kModeFused && !fitb::is_slab_variant(H.fused_variant))
+        fail(FITB_ERR_STATE, "dispersive materials need an in-place stencil mode or the slab step (fused 16-19)");
     fitb::DispHost& D = H.disp[side];
     const int blk = (int)D.pole_start.size() - 1;
     for (int q = 0; q < n_poles; ++q) {

@@ -17,7 +17,7 @@ namespace fitb {
 // stored in one common padded box indexed (i, j, k), k fastest:
 //   i in [-2, nx+1]  (zero guard planes: two before, one after),
 //   j in [0, njp)    with njp = ny + 2,
-//   k in [0, nkp)    with nkp = round_up(nz + 2, 4),
+//   k in [0, nkp)    with nkp = round_up(nz + 2, 8),
 // followed by kTailRows zero rows.  A component occupies the sub-box of its
 // reference shape; every other entry is a pad that holds +0 forever (its
 // update coefficients are 0).  Consequences used by the kernels:
@@ -25,7 +25,8 @@ namespace fitb {
 //     as 0", numba_kernels.py:51-58) becomes a plain 4-term stencil, since
 //     index j-1 = -1 lands in the previous plane's pad row j = ny+1 and
 //     k-1 = -1 in the previous row's pad tail k >= nz+1;
-//   * every row starts on a 16-byte boundary (nkp is a multiple of 4), and a
+//   * every row starts on a 16-byte boundary (nkp is a multiple of 8: also
+//     for the 16-bit compact coefficient copies), and a
 //     run of whole rows is one contiguous, 16-byte-aligned byte range: the
 //     bulk-copy stencil kernels move row tiles with single cp.async.bulk
 //     copies, including one row above the tile (row j0-1 of plane -1 lives

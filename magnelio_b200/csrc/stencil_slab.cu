@@ -36,6 +36,8 @@
 #include "fused_cpml.cuh"
 #include "tile_common.cuh"
 
+#include <cuda_fp16.h>
+
 #include <algorithm>
 #include <cmath>
 #include <vector>
@@ -70,20 +72,24 @@ struct Slot {
     const unsigned char* air;  // [4][slab]
 };
 
-template <typename T, int TJ, int NS, int NSLOT, bool AIR>
+template <typename T, int TJ, int NS, int NSLOT, bool AIR, int CK>
 struct SlabGeo {
     static constexpr int EK = TK + 4, ER = TJ + 1;  // E, alpha_E, beta_E boxes
     static constexpr int HK = TK + 8, HR = TJ + 2;  // H box
     static constexpr int cE = ER * EK, cH = HR * HK, cC = TJ * TK;
     static constexpr int NK = TK + 1, NR = TJ + 1, cN = NR * NK;  // E_new ring
     static constexpr int cPE = ER * PW, cPH = TJ * PW, cAE = ER * AW, cAH = TJ * AW;  // per component
+    // coefficient boxes: the field dtype, or 16-bit (CK != kCoefNative) with
+    // E rows of 40 entries (a 16-byte multiple covering the 33 cells)
+    static constexpr int CB = CK == kCoefNative ? (int)sizeof(T) : 2;
+    static constexpr int EKc = CK == kCoefNative ? EK : 40, cCE = ER * EKc;
     static constexpr size_t al(size_t b) { return (b + 127) / 128 * 128; }
     static constexpr unsigned bytesE = 3u * cE * sizeof(T), bytesH = 3u * cH * sizeof(T),
-                              bytesC = 3u * cC * sizeof(T);
+                              bytesCE = 3u * cCE * CB, bytesC = 3u * cC * CB;
     static constexpr unsigned bytesPE = 2u * cPE * sizeof(T), bytesPH = 2u * cPH * sizeof(T), bytesAE = 2u * cAE,
                               bytesAH = 2u * cAH;
-    static constexpr size_t oE = 0, oH = al(bytesE), oaE = oH + al(bytesH), obE = oaE + al(bytesE),
-                            oaH = obE + al(bytesE), obH = oaH + al(bytesC), oS = obH + al(bytesC);
+    static constexpr size_t oE = 0, oH = al(bytesE), oaE = oH + al(bytesH), obE = oaE + al(bytesCE),
+                            oaH = obE + al(bytesCE), obH = oaH + al(bytesC), oS = obH + al(bytesC);
     // within a slot: psi_E, psi_H, air_E, air_H
     static constexpr size_t sPE = 0, sPH = al(bytesPE), sAE = sPH + al(bytesPH),
                             sAH = sAE + (AIR ? al(bytesAE) : 0), slot = sAH + (AIR ? al(bytesAH) : 0);
@@ -99,11 +105,11 @@ struct SlabGeo {
 };
 
 // CPML of E_new of cell (r, c) of the tile region at plane i (cpml.py:343-430).
-template <typename T, int TJ, int NS, int NSLOT, bool AIR>
+template <typename T, int TJ, int NS, int NSLOT, bool AIR, int CK>
 __device__ __forceinline__ void slab_E(const Slot<T>* sl, const unsigned char* st, int r, int c, int i, int j, int k,
                                        T hx, T hy, T hz, T hz_jm, T hx_jm, T hy_km, T hx_km, T hz_im, T hy_im, T bx,
                                        T by, T bz, T& ex, T& ey, T& ez, bool store) {
-    using G = SlabGeo<T, TJ, NS, NSLOT, AIR>;
+    using G = SlabGeo<T, TJ, NS, NSLOT, AIR, CK>;
 #pragma unroll
     for (int s = 0; s < NSLOT; ++s) {
         const Slot<T>& f = sl[s];
@@ -149,11 +155,11 @@ __device__ __forceinline__ void slab_E(const Slot<T>* sl, const unsigned char* s
 // 2 and 3.  EDGE: a cell outside the staged tile rows / columns (the last
 // row j = ny or column k = nz absorbed by this tile); its psi and air come
 // from global memory.
-template <typename T, int TJ, int NS, int NSLOT, bool AIR, bool EDGE>
+template <typename T, int TJ, int NS, int NSLOT, bool AIR, int CK, bool EDGE>
 __device__ __forceinline__ void slab_H(const Slot<T>* sl, const unsigned char* stp, int r, int c, int i, int j, int k,
                                        T ex, T ey, T ez, T ez_jp, T ex_jp, T ey_kp, T ex_kp, T ez_ip, T ey_ip, T bx,
                                        T by, T bz, T& hx, T& hy, T& hz) {
-    using G = SlabGeo<T, TJ, NS, NSLOT, AIR>;
+    using G = SlabGeo<T, TJ, NS, NSLOT, AIR, CK>;
 #pragma unroll
     for (int s = 0; s < NSLOT; ++s) {
         const Slot<T>& f = sl[s];
@@ -207,19 +213,39 @@ __device__ __forceinline__ void slab_H(const Slot<T>* sl, const unsigned char* s
     }
 }
 
+// Three components (stride `stride` entries) of one staged coefficient box
+// at entry q: the field dtype, or 16-bit storage times the per-component
+// power-of-two scale cs[0..2] (the compact storage of fitb_set_coeff_storage,
+// decoded as the stream kernels decode it).
+template <typename T, int CK>
+__device__ __forceinline__ void coef3(const unsigned char* box, int stride, int q, const float* cs, T& x, T& y,
+                                      T& z) {
+    if constexpr (CK == kCoefNative) {
+        const T* a = reinterpret_cast<const T*>(box);
+        x = a[q];
+        y = a[stride + q];
+        z = a[2 * stride + q];
+    } else {
+        const unsigned short* a = reinterpret_cast<const unsigned short*>(box);
+        x = (T)__half2float(__ushort_as_half(a[q])) * (T)cs[0];
+        y = (T)__half2float(__ushort_as_half(a[stride + q])) * (T)cs[1];
+        z = (T)__half2float(__ushort_as_half(a[2 * stride + q])) * (T)cs[2];
+    }
+}
+
 // E_new of cell (r, c) of the tile region (r <= TJ, c <= TK) at plane i,
 // CPML-corrected; stored to global memory (with psi_next) when `store`.
-template <typename T, int TJ, int NS, int NSLOT, bool AIR>
-__device__ __forceinline__ void step_E(const Geom& g, const Slot<T>* sl, const unsigned char* st,
+template <typename T, int TJ, int NS, int NSLOT, bool AIR, int CK>
+__device__ __forceinline__ void step_E(const StencilArgs<T>& p, const Slot<T>* sl, const unsigned char* st,
                                        const unsigned char* stp, T* en, int r, int c, int i, int j, int k, bool store,
                                        T* __restrict__ Eg) {
-    using G = SlabGeo<T, TJ, NS, NSLOT, AIR>;
+    using G = SlabGeo<T, TJ, NS, NSLOT, AIR, CK>;
+    const Geom& g = p.g;
     const T* E = reinterpret_cast<const T*>(st + G::oE);
     const T* Hs = reinterpret_cast<const T*>(st + G::oH);
     const T* Hp = reinterpret_cast<const T*>(stp + G::oH);
-    const T* aE = reinterpret_cast<const T*>(st + G::oaE);
-    const T* bE = reinterpret_cast<const T*>(st + G::obE);
     const int ie = r * G::EK + c;
+    const int ic = r * G::EKc + c;
     const int ih = (r + 1) * G::HK + c + 4;
     const T hx = Hs[ih], hy = Hs[G::cH + ih], hz = Hs[2 * G::cH + ih];
     const T hz_jm = Hs[2 * G::cH + ih - G::HK], hx_jm = Hs[ih - G::HK];
@@ -228,12 +254,14 @@ __device__ __forceinline__ void step_E(const Geom& g, const Slot<T>* sl, const u
     const T cx = ((hz - hz_jm) - hy) + hy_km;
     const T cy = ((hx - hx_km) - hz) + hz_im;
     const T cz = ((hy - hy_im) - hx) + hx_jm;
-    const T bx = bE[ie], by = bE[G::cE + ie], bz = bE[2 * G::cE + ie];
-    T ex = aE[ie] * E[ie] + bx * cx;
-    T ey = aE[G::cE + ie] * E[G::cE + ie] + by * cy;
-    T ez = aE[2 * G::cE + ie] * E[2 * G::cE + ie] + bz * cz;
+    T ax, ay, az, bx, by, bz;
+    coef3<T, CK>(st + G::oaE, G::cCE, ic, p.cs + 0, ax, ay, az);
+    coef3<T, CK>(st + G::obE, G::cCE, ic, p.cs + 4, bx, by, bz);
+    T ex = ax * E[ie] + bx * cx;
+    T ey = ay * E[G::cE + ie] + by * cy;
+    T ez = az * E[2 * G::cE + ie] + bz * cz;
     if constexpr (NSLOT > 0)
-        slab_E<T, TJ, NS, NSLOT, AIR>(sl, st, r, c, i, j, k, hx, hy, hz, hz_jm, hx_jm, hy_km, hx_km, hz_im, hy_im, bx,
+        slab_E<T, TJ, NS, NSLOT, AIR, CK>(sl, st, r, c, i, j, k, hx, hy, hz, hz_jm, hx_jm, hy_km, hx_km, hz_im, hy_im, bx,
                                       by, bz, ex, ey, ez, store);
     const int in = r * G::NK + c;
     en[in] = ex;
@@ -251,11 +279,11 @@ __device__ __forceinline__ void step_E(const Geom& g, const Slot<T>* sl, const u
 // the stage of plane i, CPML-corrected.  EDGE: a halo cell this tile owns
 // (last row j = ny or last column k = nz): E_new beyond the padded edge is
 // zero and its coefficients, psi and air come from global memory.
-template <typename T, int TJ, int NS, int NSLOT, bool AIR, bool EDGE>
+template <typename T, int TJ, int NS, int NSLOT, bool AIR, int CK, bool EDGE>
 __device__ __forceinline__ void step_H(const StencilArgs<T>& p, const Slot<T>* sl, const unsigned char* stp,
                                        const T* enp, const T* enc, int r, int c, int i, int j, int k,
                                        T* __restrict__ Hg) {
-    using G = SlabGeo<T, TJ, NS, NSLOT, AIR>;
+    using G = SlabGeo<T, TJ, NS, NSLOT, AIR, CK>;
     const T* Hs = reinterpret_cast<const T*>(stp + G::oH);
     const int in = r * G::NK + c;
     const T ex = enp[in], ey = enp[G::cN + in], ez = enp[2 * G::cN + in];
@@ -268,17 +296,21 @@ __device__ __forceinline__ void step_H(const StencilArgs<T>& p, const Slot<T>* s
     const long long o = pidx(p.g, i, j, k), vol = p.g.vol;
     FCoef<T> ch;
     if constexpr (EDGE) {
-        load_coef3(ch, p.aH, p.bH, o, vol);
+        if constexpr (CK == kCoefNative) {
+            load_coef3(ch, p.aH, p.bH, o, vol);
+        } else {
+            const unsigned short *qa = p.cq[2], *qb = p.cq[3];
+            ch.ax = (T)__half2float(__ushort_as_half(qa[o])) * (T)p.cs[8];
+            ch.ay = (T)__half2float(__ushort_as_half(qa[vol + o])) * (T)p.cs[9];
+            ch.az = (T)__half2float(__ushort_as_half(qa[2 * vol + o])) * (T)p.cs[10];
+            ch.bx = (T)__half2float(__ushort_as_half(qb[o])) * (T)p.cs[12];
+            ch.by = (T)__half2float(__ushort_as_half(qb[vol + o])) * (T)p.cs[13];
+            ch.bz = (T)__half2float(__ushort_as_half(qb[2 * vol + o])) * (T)p.cs[14];
+        }
     } else {
-        const T* aH = reinterpret_cast<const T*>(stp + G::oaH);
-        const T* bH = reinterpret_cast<const T*>(stp + G::obH);
         const int ic = r * TK + c;
-        ch.ax = aH[ic];
-        ch.ay = aH[G::cC + ic];
-        ch.az = aH[2 * G::cC + ic];
-        ch.bx = bH[ic];
-        ch.by = bH[G::cC + ic];
-        ch.bz = bH[2 * G::cC + ic];
+        coef3<T, CK>(stp + G::oaH, G::cC, ic, p.cs + 8, ch.ax, ch.ay, ch.az);
+        coef3<T, CK>(stp + G::obH, G::cC, ic, p.cs + 12, ch.bx, ch.by, ch.bz);
     }
     const T cx = ((ez_jp - ez) - ey_kp) + ey;
     const T cy = ((ex_kp - ex) - ez_ip) + ez;
@@ -287,7 +319,7 @@ __device__ __forceinline__ void step_H(const StencilArgs<T>& p, const Slot<T>* s
     T hy = ch.ay * Hs[G::cH + ih] - ch.by * cy;
     T hz = ch.az * Hs[2 * G::cH + ih] - ch.bz * cz;
     if constexpr (NSLOT > 0)
-        slab_H<T, TJ, NS, NSLOT, AIR, EDGE>(sl, stp, r, c, i, j, k, ex, ey, ez, ez_jp, ex_jp, ey_kp, ex_kp, ez_ip,
+        slab_H<T, TJ, NS, NSLOT, AIR, CK, EDGE>(sl, stp, r, c, i, j, k, ex, ey, ez, ez_jp, ex_jp, ey_kp, ex_kp, ez_ip,
                                             ey_ip, ch.bx, ch.by, ch.bz, hx, hy, hz);
     Hg[o] = hx;
     Hg[vol + o] = hy;
@@ -296,11 +328,11 @@ __device__ __forceinline__ void step_H(const StencilArgs<T>& p, const Slot<T>* s
 
 // Units: x = k tile, y = j tile, z = i chunk, w = the face of slot s in bits
 // 4s .. 4s+3.  blockIdx.x = unit * B + field set.
-template <typename T, int TJ, int NS, int NSLOT, bool AIR>
-__global__ void __launch_bounds__(32 * (TJ + 1), SlabGeo<T, TJ, NS, NSLOT, AIR>::minb())
+template <typename T, int TJ, int NS, int NSLOT, bool AIR, int CK>
+__global__ void __launch_bounds__(32 * (TJ + 1), SlabGeo<T, TJ, NS, NSLOT, AIR, CK>::minb())
     k_step_slab(const __grid_constant__ SlabMaps maps, const StencilArgs<T> p, const int4* __restrict__ units,
                 int* status) {
-    using G = SlabGeo<T, TJ, NS, NSLOT, AIR>;
+    using G = SlabGeo<T, TJ, NS, NSLOT, AIR, CK>;
     constexpr int NC = 32 * TJ;      // compute threads
     constexpr int NX = TK + 1 + TJ;  // halo cells (row TJ, then column TK)
     static_assert(NX <= NC, "tile shape");
@@ -378,7 +410,7 @@ __global__ void __launch_bounds__(32 * (TJ + 1), SlabGeo<T, TJ, NS, NSLOT, AIR>:
                 const int ip = i0 - 1 + t;
                 const bool first = t == 0, last = t == nplanes - 1;
                 unsigned bytes = G::bytesH;
-                if (!first) bytes += 3 * G::bytesE;
+                if (!first) bytes += G::bytesE + 2 * G::bytesCE;
                 if (!first && !last) bytes += 2 * G::bytesC;
                 unsigned smask = 0;  // slots with boxes on this plane
 #pragma unroll
@@ -446,8 +478,8 @@ __global__ void __launch_bounds__(32 * (TJ + 1), SlabGeo<T, TJ, NS, NSLOT, AIR>:
                 const unsigned char* st = smem + s * G::stage;
                 const unsigned char* stp = smem + ((t - 1) % NS) * G::stage;
                 T* en = ring + (t % 3) * 3 * G::cN;
-                step_E<T, TJ, NS, NSLOT, AIR>(g, sl, st, stp, en, warp, lane, i, jo, ko, v_own && i < i1, Eg);
-                if (has_x) step_E<T, TJ, NS, NSLOT, AIR>(g, sl, st, stp, en, rx, cx, i, jx, kx, own_x && i < i1, Eg);
+                step_E<T, TJ, NS, NSLOT, AIR, CK>(p, sl, st, stp, en, warp, lane, i, jo, ko, v_own && i < i1, Eg);
+                if (has_x) step_E<T, TJ, NS, NSLOT, AIR, CK>(p, sl, st, stp, en, rx, cx, i, jx, kx, own_x && i < i1, Eg);
             }
             tma::compute_barrier(NC);
             if (flags[0]) {
@@ -459,8 +491,8 @@ __global__ void __launch_bounds__(32 * (TJ + 1), SlabGeo<T, TJ, NS, NSLOT, AIR>:
                 const T* enp = ring + ((t - 1) % 3) * 3 * G::cN;
                 const T* enc = ring + (t % 3) * 3 * G::cN;
                 if (v_own)
-                    step_H<T, TJ, NS, NSLOT, AIR, false>(p, sl, stp, enp, enc, warp, lane, i - 1, jo, ko, Hg);
-                if (own_x) step_H<T, TJ, NS, NSLOT, AIR, true>(p, sl, stp, enp, enc, rx, cx, i - 1, jx, kx, Hg);
+                    step_H<T, TJ, NS, NSLOT, AIR, CK, false>(p, sl, stp, enp, enc, warp, lane, i - 1, jo, ko, Hg);
+                if (own_x) step_H<T, TJ, NS, NSLOT, AIR, CK, true>(p, sl, stp, enp, enc, rx, cx, i - 1, jx, kx, Hg);
             }
             if (t > 0) {
                 __syncwarp();
@@ -572,36 +604,44 @@ bool slab_dispatch(int variant, F&& f) {
     }
 }
 
-// Every kernel instance of one (TJ, NS): slot capacities 0, 1, 2, 3, 6,
-// with and without air masks.
+// Every kernel instance of one (TJ, NS) and coefficient storage CK: slot
+// capacities 0, 1, 2, 3, 6, with and without air masks.
+template <typename T, int TJ, int NS, int CK, typename G>
+void each_instance_ck(G&& g) {
+    g.template one<T, TJ, NS, 0, false, CK>();
+    g.template one<T, TJ, NS, 1, false, CK>();
+    g.template one<T, TJ, NS, 2, false, CK>();
+    g.template one<T, TJ, NS, 3, false, CK>();
+    g.template one<T, TJ, NS, 6, false, CK>();
+    g.template one<T, TJ, NS, 1, true, CK>();
+    g.template one<T, TJ, NS, 2, true, CK>();
+    g.template one<T, TJ, NS, 3, true, CK>();
+    g.template one<T, TJ, NS, 6, true, CK>();
+}
+
+// All instances of one (TJ, NS): native coefficients, and float16 storage
+// for float32 fields.
 template <typename T, int TJ, int NS, typename G>
 void each_instance(G&& g) {
-    g.template one<T, TJ, NS, 0, false>();
-    g.template one<T, TJ, NS, 1, false>();
-    g.template one<T, TJ, NS, 2, false>();
-    g.template one<T, TJ, NS, 3, false>();
-    g.template one<T, TJ, NS, 6, false>();
-    g.template one<T, TJ, NS, 1, true>();
-    g.template one<T, TJ, NS, 2, true>();
-    g.template one<T, TJ, NS, 3, true>();
-    g.template one<T, TJ, NS, 6, true>();
+    each_instance_ck<T, TJ, NS, kCoefNative>(g);
+    if constexpr (sizeof(T) == 4) each_instance_ck<T, TJ, NS, kCoefF16>(g);
 }
 
 struct MaxSmem {
     size_t v = 0;
-    template <typename T, int TJ, int NS, int NSLOT, bool AIR>
+    template <typename T, int TJ, int NS, int NSLOT, bool AIR, int CK>
     void one() {
-        v = std::max(v, SlabGeo<T, TJ, NS, NSLOT, AIR>::smem);
+        v = std::max(v, SlabGeo<T, TJ, NS, NSLOT, AIR, CK>::smem);
     }
 };
 
 struct Prepare {
     cudaError_t err = cudaSuccess;
-    template <typename T, int TJ, int NS, int NSLOT, bool AIR>
+    template <typename T, int TJ, int NS, int NSLOT, bool AIR, int CK>
     void one() {
-        const cudaError_t e = cudaFuncSetAttribute(k_step_slab<T, TJ, NS, NSLOT, AIR>,
+        const cudaError_t e = cudaFuncSetAttribute(k_step_slab<T, TJ, NS, NSLOT, AIR, CK>,
                                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                   (int)SlabGeo<T, TJ, NS, NSLOT, AIR>::smem);
+                                                   (int)SlabGeo<T, TJ, NS, NSLOT, AIR, CK>::smem);
         if (err == cudaSuccess) err = e;
     }
 };
@@ -616,8 +656,8 @@ struct SlabInfo {
         each_instance<T, TJ, NS>(m);
         smem = m.v;
         tj = TJ;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ0, k_step_slab<T, TJ, NS, 0, false>, 32 * (TJ + 1),
-                                                      SlabGeo<T, TJ, NS, 0, false>::smem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ0, k_step_slab<T, TJ, NS, 0, false, kCoefNative>,
+                                                      32 * (TJ + 1), SlabGeo<T, TJ, NS, 0, false, kCoefNative>::smem);
     }
 };
 
@@ -642,28 +682,38 @@ struct SlabLaunch {
     int* status;
     cudaStream_t s;
     int launched = 0;
-    template <int NSLOT, bool AIR, int TJ, int NS>
+    template <int NSLOT, bool AIR, int CK, int TJ, int NS>
     void go(int q) {
         if (n_units[q] <= 0) return;
-        k_step_slab<T, TJ, NS, NSLOT, AIR>
-            <<<dim3((unsigned)n_units[q] * a.B), 32 * (TJ + 1), SlabGeo<T, TJ, NS, NSLOT, AIR>::smem, s>>>(
+        k_step_slab<T, TJ, NS, NSLOT, AIR, CK>
+            <<<dim3((unsigned)n_units[q] * a.B), 32 * (TJ + 1), SlabGeo<T, TJ, NS, NSLOT, AIR, CK>::smem, s>>>(
                 m, a, units[q], status);
         ++launched;
     }
+    template <int CK, int TJ, int NS>
+    void run_ck() {
+        go<0, false, CK, TJ, NS>(0);
+        if (air) {
+            go<1, true, CK, TJ, NS>(1);
+            go<2, true, CK, TJ, NS>(2);
+            go<3, true, CK, TJ, NS>(3);
+            go<6, true, CK, TJ, NS>(4);
+        } else {
+            go<1, false, CK, TJ, NS>(1);
+            go<2, false, CK, TJ, NS>(2);
+            go<3, false, CK, TJ, NS>(3);
+            go<6, false, CK, TJ, NS>(4);
+        }
+    }
     template <int TJ, int NS>
     void run() {
-        go<0, false, TJ, NS>(0);
-        if (air) {
-            go<1, true, TJ, NS>(1);
-            go<2, true, TJ, NS>(2);
-            go<3, true, TJ, NS>(3);
-            go<6, true, TJ, NS>(4);
-        } else {
-            go<1, false, TJ, NS>(1);
-            go<2, false, TJ, NS>(2);
-            go<3, false, TJ, NS>(3);
-            go<6, false, TJ, NS>(4);
+        if constexpr (sizeof(T) == 4) {
+            if (a.coef_kind == kCoefF16) {
+                run_ck<kCoefF16, TJ, NS>();
+                return;
+            }
         }
+        run_ck<kCoefNative, TJ, NS>();
     }
 };
 
@@ -815,11 +865,26 @@ int launch_slab_step(StencilArgs<T> a, int ichunk, int variant, const int4* cons
     SlabMaps m;
     const long long nset = 3LL * a.B;
     if (!tma::encode_field_map<T>(&m.e, a.e, a.g, (int)nset, TK + 4, tj + 1) ||
-        !tma::encode_field_map<T>(&m.h, a.h, a.g, (int)nset, TK + 8, tj + 2) ||
-        !tma::encode_field_map<T>(&m.aE, a.aE, a.g, 3, TK + 4, tj + 1) ||
-        !tma::encode_field_map<T>(&m.bE, a.bE, a.g, 3, TK + 4, tj + 1) ||
-        !tma::encode_field_map<T>(&m.aH, a.aH, a.g, 3, TK, tj) || !tma::encode_field_map<T>(&m.bH, a.bH, a.g, 3, TK, tj))
+        !tma::encode_field_map<T>(&m.h, a.h, a.g, (int)nset, TK + 8, tj + 2))
         return -2;
+    if (a.coef_kind == kCoefF16) {
+        // 16-bit coefficient boxes: E rows of 40 entries (80 bytes), H rows of 32
+        if (sizeof(T) != 4 || (a.g.nkp * 2) % 16 != 0) return -3;
+        const unsigned long long dims[4] = {(unsigned long long)a.g.nkp, (unsigned long long)a.g.njp,
+                                            (unsigned long long)(a.g.nx + 4), 3ULL};
+        const unsigned long long str[3] = {(unsigned long long)a.g.sj * 2, (unsigned long long)a.g.si * 2,
+                                           (unsigned long long)a.g.vol * 2};
+        const unsigned bE_[4] = {40u, (unsigned)(tj + 1), 1, 3}, bH_[4] = {(unsigned)TK, (unsigned)tj, 1, 3};
+        const CUtensorMapDataType u16 = CU_TENSOR_MAP_DATA_TYPE_UINT16;
+        if (!tma::encode_4d(&m.aE, u16, a.cq[0], dims, str, bE_) || !tma::encode_4d(&m.bE, u16, a.cq[1], dims, str, bE_) ||
+            !tma::encode_4d(&m.aH, u16, a.cq[2], dims, str, bH_) || !tma::encode_4d(&m.bH, u16, a.cq[3], dims, str, bH_))
+            return -2;
+    } else if (!tma::encode_field_map<T>(&m.aE, a.aE, a.g, 3, TK + 4, tj + 1) ||
+               !tma::encode_field_map<T>(&m.bE, a.bE, a.g, 3, TK + 4, tj + 1) ||
+               !tma::encode_field_map<T>(&m.aH, a.aH, a.g, 3, TK, tj) ||
+               !tma::encode_field_map<T>(&m.bH, a.bH, a.g, 3, TK, tj)) {
+        return -2;
+    }
     const CUtensorMapDataType dt = sizeof(T) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
     for (int q = 0; q < a.nfaces; ++q) {
         const FaceDev& f = a.f[q];

@@ -86,7 +86,7 @@ def estimate_footprint(nx, ny, nz, batch, steps, n_channels, cpml_layers=(), pre
     ``fused``: the fused step's second set of fields and psi."""
     esz = 4 if precision == "single" else 8
     sets = 2 if fused else 1
-    njp, nkp = ny + 2, -(-(nz + 2) // 4) * 4
+    njp, nkp = ny + 2, -(-(nz + 2) // 8) * 8
     si = njp * nkp
     vol = (nx + 4) * si + 8 * nkp
     n_e = 3 * (nx + 1) * (ny + 1) * (nz + 1)

@@ -527,6 +527,57 @@ def test_slab_workload_built_on_the_host_matches_the_oracle(precision, tol):
         assert _rel(bins[q], m.bins["Ex"]) < max(5 * tol, DFT_TOL)
 
 
+@pytest.mark.parametrize("precision,tol", [("double", F64_TOL), ("single", F32_TOL)])
+def test_slab_workload_in_the_slab_step_matches_the_oracle(precision, tol):
+    """The precision workload (Lorentz ADE slab one cell short of the CPML,
+    TF/SF plane wave, DFT planes) in the slab step: the ADE update runs on
+    the new E after the step kernel and the H cells next to dispersive
+    edges are recomputed; fields and bins match the float64 oracle."""
+    from oracle.fit_oracle import OracleRun
+    from magnelio_b200 import workloads
+
+    p = workloads.dispersive_slab(24, 24, 40, cpml_cells=5, n_freq=8)
+    n = 260
+    ref = OracleRun(p).run(n)
+    with p.build_engine(precision) as eng:
+        eng.configure_stencil("fused", 16)
+        eng.step(n)
+        e, h = eng.read_fields()
+        bins = [eng.read_dft(q, "Ex") for q in range(len(p.monitors))]
+    assert _rel(e, ref.f.e, ref.peak_e) < tol
+    assert _rel(h, ref.f.h, ref.peak_h) < tol
+    for q, m in enumerate(ref.mons):
+        assert _rel(bins[q], m.bins["Ex"]) < max(5 * tol, DFT_TOL)
+
+
+@pytest.mark.parametrize("precision,tol", [("double", 1e-12), ("single", 1e-5)])
+def test_slab_step_with_e_and_h_dispersion_matches_the_in_place_kernels(precision, tol):
+    """Lorentz, Debye and mu-Debye blocks (E and H side ADE) of the
+    dispersive fixture, without its CPML (the slab step refuses dispersive
+    entries inside a CPML slab, where its order of the CPML and ADE updates
+    would differ from the reference's): the slab step equals the in-place
+    kernels with their ADE passes."""
+    p, d, n = load_golden("dispersive_box")
+    p.cpml = []
+    assert {x.side for x in p.dispersion} == {"E", "H"}
+    outs = []
+    for kind, v in (("simple", 0), ("fused", 16)):
+        with p.build_engine(precision) as eng:
+            eng.configure_stencil(kind, v)
+            eng.step(n)
+            outs.append(eng.read_fields())
+    pe, ph = float(np.max(np.abs(outs[0][0]))), float(np.max(np.abs(outs[0][1])))
+    assert _rel(outs[1][0], outs[0][0], pe) < tol
+    assert _rel(outs[1][1], outs[0][1], ph) < tol
+
+
+def test_slab_step_refuses_dispersion_inside_the_cpml():
+    p, d, n = load_golden("dispersive_box")
+    with p.build_engine("single") as eng:
+        with pytest.raises(FitbError, match="outside the CPML"):
+            eng.configure_stencil("fused", 16)
+
+
 # float32 variants of the slab against its float64 run: reflection and
 # transmission over the excited band (linear), transmission phase (degrees).
 # float16 coefficients stay inside the |dS| <= 1e-3 / 0.1 degree budget,
@@ -691,6 +742,34 @@ def test_slab_step_with_pec_masks_in_the_cpml(variant):
             e, h = eng.read_fields()
         assert _rel(e, d["out.e"], pe) < F32_TOL, name
         assert _rel(h, d["out.h"], ph) < F32_TOL, name
+
+
+@pytest.mark.parametrize("variant", [16, 18])
+def test_slab_step_with_float16_coefficients_matches_the_stream_kernels(variant):
+    """float16 coefficient storage (per-component power-of-two scales) in the
+    slab step: the same decoded coefficients as the stream kernels' 16-bit
+    form, so both marches agree to FMA-contraction differences; and the
+    slab step refuses bfloat16, which it does not decode."""
+    from magnelio_b200 import workloads
+
+    steps = 19
+    prob = workloads.brick_box(70, seed=3, n_bricks=6, cpml_cells=6, n_freq=3, steps=steps + 2)
+    e0, h0 = _random_state(prob, np.random.default_rng(8))
+    prob.e0, prob.h0 = [e0], [h0]
+    outs = []
+    for kind, v in (("stream", 0), ("fused", variant)):
+        with prob.build_engine("single") as eng:
+            eng.configure_stencil(kind, v, 9)
+            eng.set_coefficient_storage("f16")
+            eng.step(steps)
+            outs.append(eng.read_fields())
+    pe, ph = float(np.max(np.abs(outs[0][0]))), float(np.max(np.abs(outs[0][1])))
+    assert _rel(outs[1][0], outs[0][0], pe) < 1e-5
+    assert _rel(outs[1][1], outs[0][1], ph) < 1e-5
+    with prob.build_engine("single") as eng:
+        eng.configure_stencil("fused", variant)
+        with pytest.raises(FitbError):
+            eng.set_coefficient_storage("bf16")
 
 
 def test_slab_step_with_cpml_on_two_field_sets_matches_stream():
