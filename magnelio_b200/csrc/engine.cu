@@ -181,6 +181,9 @@ struct Handle {
     // beside the stencil (fork / join by events inside the capture)
     cudaStream_t side = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    // third stream: the slab step's CPML unit lists beside its CPML-free list
+    cudaStream_t side2 = nullptr;
+    cudaEvent_t ev_sfork = nullptr, ev_sjoin = nullptr;
     DevBuf e, h, aE, bE, aH, bH, meps, mmu, staging;
     // Fused step: second field buffers; `cur` names the buffer set that
     // holds the current fields (always 0 for the in-place kernels).
@@ -247,6 +250,9 @@ struct Handle {
             if (graph_chunk[q]) cudaGraphExecDestroy(graph_chunk[q]);
             if (graph_one[q]) cudaGraphExecDestroy(graph_one[q]);
         }
+        if (ev_sfork) cudaEventDestroy(ev_sfork);
+        if (ev_sjoin) cudaEventDestroy(ev_sjoin);
+        if (side2) cudaStreamDestroy(side2);
         if (ev_fork) cudaEventDestroy(ev_fork);
         if (ev_join) cudaEventDestroy(ev_join);
         if (side) cudaStreamDestroy(side);
@@ -796,9 +802,23 @@ int launch_fused(Handle& H, const StencilArgs<T>& sa) {
         bool air = false;
         for (int q = 0; q < kSlabLists; ++q) units[q] = H.slab_units[q].as<int4>();
         for (auto& f : H.faces) air = air || f->pec;
+        // the CPML lists run on a second stream beside the CPML-free list
+        // (disjoint units), joined before anything reads the new fields
+        bool cpml = false;
+        for (int q = 1; q < kSlabLists; ++q) cpml = cpml || H.n_slab_units[q] > 0;
+        const bool fork = cpml && H.n_slab_units[0] > 0;
+        if (fork) {
+            ck(cudaEventRecord(H.ev_sfork, H.stream), "slab fork record");
+            ck(cudaStreamWaitEvent(H.side2, H.ev_sfork, 0), "slab fork wait");
+        }
         const int n = launch_slab_step<T>(sa, H.splan.ichunk, H.fused_variant - kFusedSlabBase, units,
-                                          H.n_slab_units, air, H.status.as<int>(), H.stream);
+                                          H.n_slab_units, air, H.status.as<int>(), H.stream,
+                                          fork ? H.side2 : H.stream);
         if (n < 0) fail(FITB_ERR_CUDA, "tensor maps of the slab step could not be encoded");
+        if (fork) {
+            ck(cudaEventRecord(H.ev_sjoin, H.side2), "slab join record");
+            ck(cudaStreamWaitEvent(H.stream, H.ev_sjoin, 0), "slab join wait");
+        }
         return n;
     }
     if (H.fused_variant >= kFusedTileBase) {
@@ -1417,6 +1437,9 @@ int fitb_create(const fitb_desc* desc, fitb_handle** out) {
     ck(cudaStreamCreateWithFlags(&H.side, cudaStreamNonBlocking), "stream");
     ck(cudaEventCreateWithFlags(&H.ev_fork, cudaEventDisableTiming), "event");
     ck(cudaEventCreateWithFlags(&H.ev_join, cudaEventDisableTiming), "event");
+    ck(cudaStreamCreateWithFlags(&H.side2, cudaStreamNonBlocking), "stream");
+    ck(cudaEventCreateWithFlags(&H.ev_sfork, cudaEventDisableTiming), "event");
+    ck(cudaEventCreateWithFlags(&H.ev_sjoin, cudaEventDisableTiming), "event");
     const size_t blk = (size_t)H.e_block() * H.esz;
     H.e.alloc(blk * H.B);
     H.h.alloc(blk * H.B);

@@ -199,11 +199,13 @@ int slab_unit_liveness(const Geom& g, const T* aE, const T* bE, const T* aH, con
 template <typename T>
 int slab_dead_sync(const Geom& g, const T* aH, const T* bH, int tj, int ichunk, const int4* units, int n, int B,
                    T* e_cur, T* h_cur, T* e_oth, T* h_oth, cudaStream_t s);
-// Launches one kernel per non-empty unit list; returns the launches issued
-// (< 0: tensor maps not encodable).  air: some face has PEC masks.
+// Launches one kernel per non-empty unit list, the CPML-free list on s and
+// the lists with face slots on s_cpml (the units are disjoint: the caller
+// may run the two streams side by side); returns the launches issued (< 0:
+// tensor maps not encodable).  air: some face has PEC masks.
 template <typename T>
 int launch_slab_step(StencilArgs<T> a, int ichunk, int variant, const int4* const units[kSlabLists],
-                     const int n_units[kSlabLists], bool air, int* status, cudaStream_t s);
+                     const int n_units[kSlabLists], bool air, int* status, cudaStream_t s, cudaStream_t s_cpml);
 // One CTA waits, bounded by `limit` tries, on an mbarrier that nothing
 // completes; the expired wait writes kStatusWaitTimeoutTile to *status.
 cudaError_t launch_wait_probe(int* status, unsigned limit, cudaStream_t s);
