@@ -14,7 +14,10 @@ problem on the host cores.  The figures:
   vanishing signal;
 * ``rel_l2_e_final`` / ``rel_l2_h_final``: the same against the final norm;
 * ``dft_max_rel``: over every monitor and component, the largest
-  ``max |bin - bin_ref| / max |bin_ref|``.
+  ``max |bin - bin_ref| / max |bin_ref|`` (a worst case set by the weakest,
+  most cancelled bins);
+* ``dft_rel_l2``: over every monitor and component, the largest
+  ``||bins - bins_ref|| / ||bins_ref||``.
 """
 
 from __future__ import annotations
@@ -51,16 +54,18 @@ class Fp64Prefix:
         h = np.asarray(h, dtype=np.float64)
         de = float(np.linalg.norm(e - self.e))
         dh = float(np.linalg.norm(h - self.h))
-        dft = 0.0
+        dft = dft_l2 = 0.0
         for (q, c), ref in self.bins.items():
             got = np.asarray(read_dft(q, c)).reshape(ref.shape)
             dft = max(dft, float(np.max(np.abs(got - ref)) / max(float(np.max(np.abs(ref))), 1e-300)))
+            dft_l2 = max(dft_l2, float(np.linalg.norm(got - ref) / max(float(np.linalg.norm(ref)), 1e-300)))
         return {
             "rel_l2_e": de / max(self.peak_e, 1e-300),
             "rel_l2_h": dh / max(self.peak_h, 1e-300),
             "rel_l2_e_final": de / max(float(np.linalg.norm(self.e)), 1e-300),
             "rel_l2_h_final": dh / max(float(np.linalg.norm(self.h)), 1e-300),
             "dft_max_rel": dft,
+            "dft_rel_l2": dft_l2,
             "steps": self.steps,
             "vs": "float64 C port of the reference step",
         }

@@ -12,10 +12,12 @@ march), and compared with the float64 C port of the reference's step
 * 256^3 for a 500-step prefix (the source pulse at its peak).
 
 Field error: ``||x - x_ref||`` relative to the largest field norm of the run
-(``oracle/prefix_parity.py``); the reference's own float32 march departs
-from its float64 march by about 4e-7 on that measure at 2000 steps.  DFT
-bins: max abs difference relative to the largest bin of each monitor
-component.
+(``oracle/prefix_parity.py``).  DFT bins: per monitor component, the max
+abs difference relative to its largest bin and the relative L2 norm of the
+difference.  The reference's own float32 march (the C port in float32) at
+128^3 x 2000 steps departs from its float64 march by 1.5e-7 (E), 1.9e-6
+(H), 4.2e-4 (DFT max) and 2.8e-5 (DFT L2) on these measures; the bars
+below leave a few times that.
 """
 
 from __future__ import annotations
@@ -24,8 +26,9 @@ import pytest
 
 pytestmark = pytest.mark.gpu
 
-FIELD_TOL = 2e-4   # ||x - x_ref|| / max_n ||x_ref(n)||, float32 engine vs float64
-DFT_TOL = 1e-3     # max |bin - bin_ref| / max |bin_ref| per monitor component
+FIELD_TOL = 2e-4     # ||x - x_ref|| / max_n ||x_ref(n)||, float32 engine vs float64
+DFT_TOL = 2e-3       # max |bin - bin_ref| / max |bin_ref| per monitor component
+DFT_L2_TOL = 1e-4    # ||bins - bins_ref|| / ||bins_ref|| per monitor component
 
 # two-pass stream kernels, TMA tile step with CPML passes, slab step (CPML inside the march)
 FORMS = [("stream", 0), ("fused", 7), ("fused", 16)]
@@ -60,6 +63,7 @@ def _check(prob, ref, kind, variant):
     assert par["rel_l2_e"] < FIELD_TOL, par
     assert par["rel_l2_h"] < FIELD_TOL, par
     assert par["dft_max_rel"] < DFT_TOL, par
+    assert par["dft_rel_l2"] < DFT_L2_TOL, par
     return par
 
 
