@@ -699,8 +699,8 @@ void build_slab_units(Handle& H) {
         for (const int4& c : H.fix_host)
             for (int q = 0; q < n; ++q) {
                 const int4& u = lists[0][(size_t)q];
-                const int k0 = u.x * 32, j0 = u.y * tj, i0 = u.z * ichunk;
-                if (c.x >= i0 - 1 && c.x <= i0 + ichunk && c.y >= j0 - 1 && c.y <= j0 + tj && c.z >= k0 - 1 &&
+                const int k0 = (u.x & 0xffff) * 32, j0 = (u.x >> 16) * tj, i0 = u.y, i1 = u.z;
+                if (c.x >= i0 - 1 && c.x <= i1 && c.y >= j0 - 1 && c.y <= j0 + tj && c.z >= k0 - 1 &&
                     c.z <= k0 + 32)
                     flags[(size_t)q] = 1;
             }

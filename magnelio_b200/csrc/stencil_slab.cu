@@ -341,9 +341,8 @@ __global__ void __launch_bounds__(32 * (TJ + 1), SlabGeo<T, TJ, NS, NSLOT, AIR, 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int b = blockIdx.x % p.B;
     const int4 u = units[blockIdx.x / p.B];
-    const int k0 = u.x * TK, j0 = u.y * TJ;
-    const int i0 = u.z * p.ichunk;
-    const int i1 = min(i0 + p.ichunk, g.nx + 1);
+    const int k0 = (u.x & 0xffff) * TK, j0 = (u.x >> 16) * TJ;
+    const int i0 = u.y, i1 = u.z;
     const int nplanes = i1 - i0 + 2;  // planes i0-1 .. i1
     unsigned long long* full = reinterpret_cast<unsigned long long*>(smem + G::oBar);
     unsigned long long* empty = full + NS;
@@ -529,11 +528,11 @@ template <typename T>
 __global__ void k_unit_live(Geom g, const T* __restrict__ aE, const T* __restrict__ bE, const T* __restrict__ aH,
                             const T* __restrict__ bH, int tj, int ichunk, const int4* __restrict__ units, int* flags) {
     const int4 u = units[blockIdx.x];
-    const int k0 = u.x * TK, j0 = u.y * tj, i0 = u.z * ichunk;
+    const int k0 = (u.x & 0xffff) * TK, j0 = (u.x >> 16) * tj, i0 = u.y;
     // real cells only (i <= nx, j <= ny, k <= nz): their +1 neighbours stay
     // inside the padded box
     const int nk = min(k0 + TK, g.nz) - k0 + 1, nj = min(j0 + tj, g.ny) - j0 + 1;
-    const int ni = min(i0 + ichunk, g.nx) - i0 + 1;
+    const int ni = min(u.z, g.nx) - i0 + 1;
     const long long vol = g.vol, si = g.si, sj = g.sj;
     bool live = false;
     for (int t = threadIdx.x; t < ni * nj * nk && !live; t += blockDim.x) {
@@ -569,11 +568,11 @@ __global__ void k_dead_units_sync(Geom g, const T* __restrict__ aH, const T* __r
                                   const int4* __restrict__ units, T* e_cur, T* h_cur, T* e_oth, T* h_oth) {
     const int4 u = units[blockIdx.x];
     const int b = blockIdx.y;
-    const int k0 = u.x * TK, j0 = u.y * tj, i0 = u.z * ichunk;
+    const int k0 = (u.x & 0xffff) * TK, j0 = (u.x >> 16) * tj, i0 = u.y;
     // own rows / columns, with the last row / column a tile absorbs
     const int k1 = (k0 + TK == g.nz) ? g.nz + 1 : min(k0 + TK, g.nz + 1);
     const int j1 = (j0 + tj == g.ny) ? g.ny + 1 : min(j0 + tj, g.ny + 1);
-    const int i1 = min(i0 + ichunk, g.nx + 1);
+    const int i1 = u.z;
     const int nk = k1 - k0, nj = j1 - j0, ni = i1 - i0;
     if (nk <= 0 || nj <= 0 || ni <= 0) return;
     const long long vol = g.vol, fs = 3 * vol * (long long)b;
@@ -759,6 +758,38 @@ int slab_occupancy(int variant) {
 template int slab_occupancy<float>(int);
 template int slab_occupancy<double>(int);
 
+// Chunks [i0, i1) of the i march: about `ichunk` planes each, cut at the
+// x faces' slab boundaries so that a chunk either holds a slab's planes or
+// none of them (E_new(i1) is part of a chunk's work, so a chunk ending at
+// i1 = lo - 1 stays clear of a slab starting at lo), with no chunk shorter
+// than four planes (a short piece joins its neighbour).
+std::vector<int2> slab_chunks(const Geom& g, const FaceDev* f, int nfaces, int ichunk) {
+    const int nplanes = g.nx + 1;
+    std::vector<int> cuts = {0, nplanes};
+    for (int q = 0; q < nfaces; ++q) {
+        if (f[q].axis != 0) continue;
+        for (int c : {f[q].lo - 1, f[q].lo + f[q].n})
+            if (c > 0 && c < nplanes) cuts.push_back(c);
+    }
+    std::sort(cuts.begin(), cuts.end());
+    cuts.erase(std::unique(cuts.begin(), cuts.end()), cuts.end());
+    std::vector<int> kept = {0};
+    for (size_t q = 1; q < cuts.size(); ++q) {
+        const bool end = cuts[q] == nplanes;
+        if (!end && cuts[q] - kept.back() < 4) continue;
+        if (end && kept.size() > 1 && cuts[q] - kept.back() < 4) kept.pop_back();
+        kept.push_back(cuts[q]);
+    }
+    std::vector<int2> out;
+    for (size_t q = 0; q + 1 < kept.size(); ++q) {
+        const int a = kept[q], b = kept[q + 1];
+        const int m = (b - a + ichunk - 1) / ichunk;
+        for (int t = 0; t < m; ++t)
+            out.push_back(make_int2(a + (int)((long long)(b - a) * t / m), a + (int)((long long)(b - a) * (t + 1) / m)));
+    }
+    return out;
+}
+
 // Units of the slab step, sorted into lists by their number of CPML face
 // slots: lists 0-3 hold the units with that many slots, list 4 those with
 // four to six (on small grids both faces of an axis can reach one unit; its
@@ -766,14 +797,17 @@ template int slab_occupancy<double>(int);
 // j0 .. j0+TJ (its own rows and the halo row), columns k0 .. k0+TK and
 // planes i0 .. i1 (E_new(i1) feeds H_new(i1-1)); every face whose slab
 // meets those ranges on its axis gets a slot, slots in face (boundary)
-// order.  False for more faces than the packed slot indices hold.
+// order.  A unit is (k tile | j tile << 16, i0, i1, packed slot faces).
+// False for more faces than the packed slot indices hold, or tile counts
+// beyond the packing.
 bool plan_slab_units(const Geom& g, const FaceDev* f, int nfaces, int tj, int ichunk, std::vector<int4> out[5]) {
     for (int q = 0; q < 5; ++q) out[q].clear();
     if (nfaces > kMaxFaces || tj <= 0 || ichunk <= 0) return false;
     const int nkt = g.nz % TK == 0 ? g.nz / TK : (g.nz + TK) / TK;
     const int njt = g.ny % tj == 0 ? g.ny / tj : (g.ny + tj) / tj;
-    const int nplanes = g.nx + 1;
-    const int nch = (nplanes + ichunk - 1) / ichunk;
+    if (nkt > 0xffff || njt > 0x7fff) return false;
+    const std::vector<int2> chunks = slab_chunks(g, f, nfaces, ichunk);
+    const int nch = (int)chunks.size();
     // bit mask of the faces of `axis` whose slab [lo_f, lo_f + n) meets [lo, hi]
     auto faces_on = [&](int axis, int lo, int hi) {
         unsigned m = 0;
@@ -784,7 +818,7 @@ bool plan_slab_units(const Geom& g, const FaceDev* f, int nfaces, int tj, int ic
     std::vector<unsigned> fk(nkt), fj(njt), fi(nch);
     for (int t = 0; t < nkt; ++t) fk[t] = faces_on(2, t * TK, t * TK + TK);
     for (int t = 0; t < njt; ++t) fj[t] = faces_on(1, t * tj, t * tj + tj);
-    for (int c = 0; c < nch; ++c) fi[c] = faces_on(0, c * ichunk, std::min(c * ichunk + ichunk, nplanes));
+    for (int c = 0; c < nch; ++c) fi[c] = faces_on(0, chunks[c].x, chunks[c].y);
     for (int c = 0; c < nch; ++c)
         for (int jt = 0; jt < njt; ++jt)
             for (int kt = 0; kt < nkt; ++kt) {
@@ -796,7 +830,7 @@ bool plan_slab_units(const Geom& g, const FaceDev* f, int nfaces, int tj, int ic
                 for (int fq = 0; fq < nfaces; ++fq)  // ascending: boundary order
                     if (m >> fq & 1) w |= fq << (4 * q++);
                 for (; q < cap; ++q) w |= 15 << (4 * q);  // empty slots
-                out[list].push_back(make_int4(kt, jt, c, w));
+                out[list].push_back(make_int4(kt | (jt << 16), chunks[c].x, chunks[c].y, w));
             }
     return true;
 }
