@@ -282,6 +282,11 @@ def main(argv=None) -> int:
     ap.add_argument("--serving", action="store_true",
                     help="serve the S-parameter request stream (batched and one excitation at a time) instead")
     ap.add_argument("--serving-requests", type=int, default=256)
+    ap.add_argument("--serving-stencil", default=None, metavar="BATCHED[,PLAIN]",
+                    help="stencil forms of the served handles, KIND:VARIANT or 'default' each (batched, then "
+                         "one-excitation handles; the loop's own choice when absent)")
+    ap.add_argument("--serving-coef", choices=("native", "f16"), default="native",
+                    help="coefficient storage of the served handles (f16: 16-bit with per-component scales)")
     ap.add_argument("--serving-scale", type=float, default=1.0,
                     help="scale factor on the request grid sizes and step counts (1 = the full stream)")
     ap.add_argument("--coef", choices=("native", "f16", "bf16"), default="native",
@@ -328,9 +333,20 @@ def run_serving(args, world, rank, local):
     cells = (max(8**3, int(32**3 * sc)), max(8**3, int(192**3 * sc)))
     steps = (max(100, int(6000 * sc)), max(100, int(12000 * sc)))
     reqs = serving.request_stream(args.serving_requests, seed=2027 + rank, mean_gap=0.020, cells=cells, steps=steps)
+    stencil = serving.serving_stencil
+    if args.serving_stencil:
+        forms = [None if f in ("default", "") else (f.split(":")[0], int(f.split(":")[1]))
+                 for f in args.serving_stencil.split(",")]
+        forms = forms + forms[-1:] if len(forms) == 1 else forms
+
+        def stencil(batch, _f=forms):
+            return _f[0] if batch > 1 else _f[1]
+    coef = None if args.serving_coef == "native" else args.serving_coef
     # S-matrices from the device post-step: the V/I histories never leave the GPU
-    batched = serving.ServingLoop(device=local, max_slots=8, slice_steps=512, records=False).run(reqs)
-    plain = serving.ServingLoop(device=local, slice_steps=512, records=False).run(reqs, plain=True)
+    batched = serving.ServingLoop(device=local, max_slots=8, slice_steps=512, records=False, stencil=stencil,
+                                  coef=coef).run(reqs)
+    plain = serving.ServingLoop(device=local, slice_steps=512, records=False, stencil=stencil,
+                                coef=coef).run(reqs, plain=True)
     # the slowest replica bounds the whole job
     solves = -_max_over_ranks(-batched.solves_per_s, world, local)
     if rank == 0:
@@ -342,9 +358,9 @@ def run_serving(args, world, rank, local):
                        "cells": list(cells), "steps": list(steps), "ports": "2-4 lumped, 50 ohm",
                        "s_matrix": "device post-step (fitb_s_params)",
                        "max_slots": 8, "slice_steps": 512,
-                       "stencil": {"batched": str(serving.serving_stencil(2) or "engine default (batched two-pass)"),
-                                   "plain": str(serving.serving_stencil(1) or "engine default")},
-                       "coefficients": "float32"},
+                       "stencil": {"batched": str(stencil(2) or "engine default (batched two-pass)"),
+                                   "plain": str(stencil(1) or "engine default")},
+                       "coefficients": "float32" if coef is None else f"{coef} storage, float32 arithmetic"},
             "p50_s": batched.p50, "p99_s": batched.p99, "wall_s": batched.wall,
             "mean_active": batched.mean_active, "peak_device_bytes": batched.peak_bytes,
             "plain": plain.summary(), "ratio_vs_plain": batched.solves_per_s / max(plain.solves_per_s, 1e-12),

@@ -129,8 +129,12 @@ class ServingLoop:
 
     def __init__(self, device: int = 0, precision: str = "single", hbm_budget: int | None = None,
                  max_slots: int = 8, slice_steps: int = 512, engine_factory=None, tune=None,
-                 clock=time.perf_counter, sleep=time.sleep, stencil=serving_stencil, records: bool = True):
+                 clock=time.perf_counter, sleep=time.sleep, stencil=serving_stencil, records: bool = True,
+                 coef: str | None = None):
         self.device = device
+        # coefficient storage of every handle ("f16": 16-bit with per-component
+        # scales, in the forms that take it; None: the field dtype)
+        self.coef = coef
         # records=False: S-matrices come from the device post-step
         # (FitEngine.s_parameters) and the V/I histories stay on the device
         # (Result.V / Result.I are None)
@@ -184,6 +188,7 @@ class ServingLoop:
                 pending.popleft()
                 eng = self.engine_factory(prob, self.precision, self.device)
                 self._configure(eng, form)
+                self._storage(eng, self.coef)
                 if self.tune is not None:
                     self.tune(prob, eng)
                 eng.reserve_steps(req.steps)
@@ -282,6 +287,20 @@ class ServingLoop:
             if done or (until is not None and self.clock() >= until):
                 return done
             self.sleep(2e-5)
+
+    @staticmethod
+    def _storage(eng, coef):
+        """16-bit coefficient storage on a new handle whose stencil form takes
+        it; others keep the field dtype."""
+        setter = getattr(eng, "set_coefficient_storage", None)
+        if coef is None or setter is None:
+            return
+        from magnelio_b200._lib import FitbError
+
+        try:
+            setter(coef)
+        except FitbError:
+            pass
 
     @staticmethod
     def _configure(eng, form):
