@@ -150,6 +150,23 @@ int fitb_set_coeffs(fitb_handle* h, const double* alpha_e, const double* beta_e,
 int fitb_set_coeffs_native(fitb_handle* h, const void* alpha_e, const void* beta_e,
                            const void* alpha_h, const void* beta_h,
                            const void* m_eps, const void* m_mu);
+/* Material matrices and leapfrog coefficients built on the device from the
+ * grid and the cell materials, in place of fitb_set_coeffs for lossless,
+ * non-magnetic problems (replaces the host-side setup of
+ * FITTimeDomainSolver.setup, src/magnelio/solver/fit_td.py:341-514, over
+ * build_M_eps / build_M_mu, src/magnelio/_operators/material_matrices.py
+ * :334-531): dx, dy, dz the nx, ny, nz cell widths [m]; mat_id[nx][ny][nz]
+ * the material of each cell (0 .. n_mat-1) and eps_r[n_mat] its relative
+ * permittivity.  An E edge takes the permittivity of its owner cell (the
+ * cell at its (i, j, k), clamped to the grid) times EPS0 A_dual / L_primal;
+ * the n_cat1 edges cat1_idx (flat E indices) take cat1_eps instead (conformal
+ * averages); M_mu = MU0 A_primal / L_dual; alpha = 1, beta = dt / M (M = 0:
+ * frozen at (1, 0)); the n_pec edges pec_idx are frozen at (0, 0).  The
+ * float64 arithmetic is rounded as written, so the result equals the host
+ * restatement's bit for bit. */
+int fitb_build_materials(fitb_handle* h, const double* dx, const double* dy, const double* dz, const int32_t* mat_id,
+                         int32_t n_mat, const double* eps_r, int64_t n_cat1, const int64_t* cat1_idx,
+                         const double* cat1_eps, int64_t n_pec, const int64_t* pec_idx);
 /* Storage of the four update-coefficient arrays read by the stream stencil
  * kernels: FITB_COEF_NATIVE (field dtype, the default), FITB_COEF_F16 or
  * FITB_COEF_BF16 (16-bit values with a power-of-two scale per component;

@@ -133,7 +133,7 @@ def _scratch_engine(prob, batch: int, precision: str, device: int, coef: str):
     try:
         if coef != "native":
             eng.set_coefficient_storage(coef)
-        eng.set_coefficients(prob.alpha_E, prob.beta_E, prob.alpha_H, prob.beta_H)
+        prob.put_coefficients(eng)
         for f in prob.cpml:
             eng.add_cpml(f.face, f.b, f.c, f.ck, f.air)
     except Exception:

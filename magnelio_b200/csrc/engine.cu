@@ -1543,6 +1543,60 @@ int fitb_set_coeffs(fitb_handle* h, const double* alpha_e, const double* beta_e,
     FITB_CATCH
 }
 
+int fitb_build_materials(fitb_handle* h, const double* dx, const double* dy, const double* dz, const int32_t* mat_id,
+                         int32_t n_mat, const double* eps_r, int64_t n_cat1, const int64_t* cat1_idx,
+                         const double* cat1_eps, int64_t n_pec, const int64_t* pec_idx) {
+    FITB_TRY
+    Handle& H = H_of(h);
+    const fitb::Geom& g = H.g;
+    if (!dx || !dy || !dz || !mat_id || !eps_r || n_mat < 1) fail(FITB_ERR_ARG, "null array or no materials");
+    if (n_cat1 < 0 || n_pec < 0 || (n_cat1 > 0 && (!cat1_idx || !cat1_eps)) || (n_pec > 0 && !pec_idx))
+        fail(FITB_ERR_ARG, "cat-1 / PEC lists");
+    const long long cells = (long long)g.nx * g.ny * g.nz;
+    for (long long q = 0; q < cells; ++q)
+        if (mat_id[q] < 0 || mat_id[q] >= n_mat) fail(FITB_ERR_ARG, "material id %d of cell %lld", mat_id[q], q);
+    const long long nE = H.nE();
+    for (long long q = 0; q < n_cat1; ++q)
+        if (cat1_idx[q] < 0 || cat1_idx[q] >= nE) fail(FITB_ERR_ARG, "cat-1 edge %lld", (long long)cat1_idx[q]);
+    for (long long q = 0; q < n_pec; ++q)
+        if (pec_idx[q] < 0 || pec_idx[q] >= nE) fail(FITB_ERR_ARG, "PEC edge %lld", (long long)pec_idx[q]);
+    ck(cudaStreamSynchronize(H.stream), "sync");
+    fitb::DevBuf ddx, ddy, ddz, dmat, deps, dci, dce, dpi, dmax;
+    fitb::upload(ddx, std::vector<double>(dx, dx + g.nx));
+    fitb::upload(ddy, std::vector<double>(dy, dy + g.ny));
+    fitb::upload(ddz, std::vector<double>(dz, dz + g.nz));
+    fitb::upload(dmat, std::vector<int>(mat_id, mat_id + cells));
+    fitb::upload(deps, std::vector<double>(eps_r, eps_r + n_mat));
+    fitb::upload(dci, std::vector<long long>(cat1_idx, cat1_idx + n_cat1 + (n_cat1 == 0)));
+    fitb::upload(dce, std::vector<double>(cat1_eps, cat1_eps + n_cat1 + (n_cat1 == 0)));
+    fitb::upload(dpi, std::vector<long long>(pec_idx, pec_idx + n_pec + (n_pec == 0)));
+    dmax.alloc(12 * sizeof(double));
+    if (H.prec == 4)
+        fitb::launch_setup_materials<float>(g, ddx.as<double>(), ddy.as<double>(), ddz.as<double>(), dmat.as<int>(),
+                                            deps.as<double>(), H.dt, n_cat1, dci.as<long long>(), dce.as<double>(),
+                                            n_pec, dpi.as<long long>(), H.aE.as<float>(), H.bE.as<float>(),
+                                            H.aH.as<float>(), H.bH.as<float>(), H.meps.as<float>(),
+                                            H.mmu.as<float>(), dmax.as<double>(), H.stream);
+    else
+        fitb::launch_setup_materials<double>(g, ddx.as<double>(), ddy.as<double>(), ddz.as<double>(),
+                                             dmat.as<int>(), deps.as<double>(), H.dt, n_cat1, dci.as<long long>(),
+                                             dce.as<double>(), n_pec, dpi.as<long long>(), H.aE.as<double>(),
+                                             H.bE.as<double>(), H.aH.as<double>(), H.bH.as<double>(),
+                                             H.meps.as<double>(), H.mmu.as<double>(), dmax.as<double>(), H.stream);
+    ck(cudaGetLastError(), "material setup launch");
+    double mx[12];
+    ck(cudaMemcpyAsync(mx, dmax.p, sizeof(mx), cudaMemcpyDeviceToHost, H.stream), "coefficient max D2H");
+    ck(cudaStreamSynchronize(H.stream), "material setup sync");
+    for (int a = 0; a < 4; ++a)
+        for (int c = 0; c < 3; ++c) H.coef_max[a][c] = mx[3 * a + c];
+    H.launches += 5;
+    H.coeffs_set = true;
+    fitb::compact_coeffs(H);
+    H.port_tables_dirty = true;
+    fitb::invalidate_graphs(H);
+    FITB_CATCH
+}
+
 int fitb_set_coeffs_native(fitb_handle* h, const void* alpha_e, const void* beta_e, const void* alpha_h,
                            const void* beta_h, const void* m_eps, const void* m_mu) {
     FITB_TRY

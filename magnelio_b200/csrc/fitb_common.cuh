@@ -440,6 +440,15 @@ void launch_s_assemble(const double2* xv, const double2* xi, int nch, int nf, co
                        const double2* maps, const int* icot, const int* excited, double thr, int B, double2* S,
                        double2* A, cudaStream_t s);
 
+// Material matrices and leapfrog coefficients from the grid and the cell
+// materials (setup.cu): writes alpha/beta E and H, M_eps, M_mu into the
+// padded arrays and the per-component max |coefficient| into coef_max[4][3].
+template <typename T>
+void launch_setup_materials(const Geom& g, const double* dx, const double* dy, const double* dz, const int* mat,
+                            const double* eps_r, double dt, long long n_cat1, const long long* cat1_idx,
+                            const double* cat1_eps, long long n_pec, const long long* pec_idx, T* aE, T* bE, T* aH,
+                            T* bH, T* meps, T* mmu, double* coef_max, cudaStream_t s);
+
 // Energy: per field set 0.5 (sum m_eps e^2 + sum m_mu h^2) in float64.
 template <typename T>
 void launch_energy(const T* e, const T* h, const T* meps, const T* mmu, const Geom& g, int b,

@@ -112,6 +112,27 @@ class FitEngine:
         mm = None if M_mu is None else _f64(M_mu)
         check(self._lib.fitb_set_coeffs(self._h, *[f64p(a) for a in arrs], f64p(me), f64p(mm)))
 
+    def build_materials(self, dx, dy, dz, mat_id, eps_r, cat1_idx=None, cat1_eps=None, pec_idx=None) -> None:
+        """Material matrices and leapfrog coefficients of a lossless,
+        non-magnetic problem built on the device from the cell widths, the
+        cell materials ``mat_id`` (nx, ny, nz) with relative permittivities
+        ``eps_r``, conformal cat-1 edges and PEC edges (flat E indices); the
+        same bits as :mod:`magnelio_b200.host` builds on the CPU."""
+        w = [_f64(d) for d in (dx, dy, dz)]
+        if [a.size for a in w] != [self.nx, self.ny, self.nz]:
+            raise ValueError("cell widths must have nx, ny, nz entries")
+        mat = np.ascontiguousarray(np.asarray(mat_id, dtype=np.int32))
+        if mat.size != self.nx * self.ny * self.nz:
+            raise ValueError("mat_id must have nx * ny * nz entries")
+        eps = _f64(eps_r)
+        ci = np.ascontiguousarray(np.zeros(0, np.int64) if cat1_idx is None else np.asarray(cat1_idx, np.int64))
+        ce = _f64(np.zeros(0) if cat1_eps is None else cat1_eps)
+        if ci.size != ce.size:
+            raise ValueError("cat1_idx and cat1_eps must have the same length")
+        pi = np.ascontiguousarray(np.zeros(0, np.int64) if pec_idx is None else np.asarray(pec_idx, np.int64))
+        check(self._lib.fitb_build_materials(self._h, *[f64p(a) for a in w], i32p(mat), int(eps.size), f64p(eps),
+                                             int(ci.size), i64p(ci), f64p(ce), int(pi.size), i64p(pi)))
+
     def set_coefficients_native(self, alpha_E, beta_E, alpha_H, beta_H, M_eps=None, M_mu=None) -> None:
         """Upload coefficient arrays that are already in the field dtype."""
         arrs = [np.ascontiguousarray(a) for a in (alpha_E, beta_E, alpha_H, beta_H, M_eps, M_mu) if a is not None]

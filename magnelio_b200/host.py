@@ -151,6 +151,28 @@ def build_M_eps(x, y, z, eps_table, mat_id, cat1_idx=None, cat1_eps=None) -> np.
     return M
 
 
+def m_eps_edges(x, y, z, eps_table, mat_id, flat_idx) -> np.ndarray:
+    """``M_eps`` of the listed flat E edges (cat-0), the same arithmetic as
+    :func:`build_M_eps` on those entries only."""
+    nx, ny, nz = mat_id.shape
+    dx, dy, dz = np.diff(x), np.diff(y), np.diff(z)
+    ax, ay, az = _avg_d(dx), _avg_d(dy), _avg_d(dz)
+    eps_table = np.asarray(eps_table, dtype=float)
+    sizes = (nx * (ny + 1) * (nz + 1), (nx + 1) * ny * (nz + 1), (nx + 1) * (ny + 1) * nz)
+    out = np.empty(len(flat_idx))
+    for q, f in enumerate(np.asarray(flat_idx, np.int64)):
+        c = 0
+        while f >= sizes[c]:
+            f -= sizes[c]
+            c += 1
+        shape = ((nx, ny + 1, nz + 1), (nx + 1, ny, nz + 1), (nx + 1, ny + 1, nz))[c]
+        i, j, k = np.unravel_index(int(f), shape)
+        ic, jc, kc = (i if c == 0 else min(i, nx - 1)), (j if c == 1 else min(j, ny - 1)), (k if c == 2 else min(k, nz - 1))
+        g = (ay[j] * az[k] / dx[i], ax[i] * az[k] / dy[j], ax[i] * ay[j] / dz[k])[c]
+        out[q] = EPS0 * eps_table[mat_id[ic, jc, kc]] * g
+    return out
+
+
 def geom_H(x, y, z):
     """Per-face ``A_primal / L_dual`` in the flat H layout
     (``material_matrices.py:1250-1269``)."""

@@ -118,6 +118,36 @@ class DispersionBlock:
 
 
 @dataclass
+class MaterialSetup:
+    """The inputs of a lossless, non-magnetic problem's material matrices,
+    for building them on the device (``FitEngine.build_materials``) instead
+    of uploading host arrays: cell materials ``mat_id`` (nx, ny, nz),
+    relative permittivities ``eps_r`` per material, conformal cat-1 edges
+    (flat E indices and averaged permittivities) and PEC edges (flat E
+    indices)."""
+
+    mat_id: np.ndarray
+    eps_r: np.ndarray
+    cat1_idx: np.ndarray | None = None
+    cat1_eps: np.ndarray | None = None
+    pec_idx: np.ndarray | None = None
+
+    def host_arrays(self, dx, dy, dz, dt):
+        """The same constants built on the host (``magnelio_b200.host``):
+        (alpha_E, beta_E, alpha_H, beta_H, M_eps, M_mu)."""
+        from magnelio_b200 import host
+
+        x, y, z = (np.concatenate([[0.0], np.cumsum(d)]) for d in (dx, dy, dz))
+        M_eps = host.build_M_eps(x, y, z, self.eps_r, self.mat_id, self.cat1_idx, self.cat1_eps)
+        M_mu = host.build_M_mu(x, y, z)
+        aE, bE, aH, bH = host.leapfrog_coefficients(M_eps, M_mu, dt)
+        if self.pec_idx is not None and len(self.pec_idx):
+            aE[self.pec_idx] = 0.0
+            bE[self.pec_idx] = 0.0
+        return aE, bE, aH, bH, M_eps, M_mu
+
+
+@dataclass
 class Dispersion:
     """ADE operator of one side ("E": eps(omega), "H": mu(omega));
     blocks in the reference's material order."""
@@ -144,12 +174,14 @@ class FitProblem:
     dx: np.ndarray
     dy: np.ndarray
     dz: np.ndarray
-    alpha_E: np.ndarray
-    beta_E: np.ndarray
-    alpha_H: np.ndarray
-    beta_H: np.ndarray
+    alpha_E: np.ndarray | None
+    beta_E: np.ndarray | None
+    alpha_H: np.ndarray | None
+    beta_H: np.ndarray | None
     M_eps: np.ndarray | None = None
     M_mu: np.ndarray | None = None
+    # built on the device when the coefficient arrays are None
+    materials: MaterialSetup | None = None
     cpml: list = field(default_factory=list)
     lumped: list = field(default_factory=list)
     modal: list = field(default_factory=list)
@@ -161,11 +193,20 @@ class FitProblem:
     h0: list = field(default_factory=list)
 
     # ---- engine ---------------------------------------------------------
+    def put_coefficients(self, eng) -> None:
+        """The material matrices and coefficients on an engine: the host
+        arrays, or built on the device from ``materials``."""
+        if self.alpha_E is None:
+            m = self.materials
+            eng.build_materials(self.dx, self.dy, self.dz, m.mat_id, m.eps_r, m.cat1_idx, m.cat1_eps, m.pec_idx)
+        else:
+            eng.set_coefficients(self.alpha_E, self.beta_E, self.alpha_H, self.beta_H, self.M_eps, self.M_mu)
+
     def build_engine(self, precision: str = "single", device: int = 0, max_steps: int = 0) -> FitEngine:
         """Create a :class:`FitEngine` holding this problem."""
         eng = FitEngine(self.nx, self.ny, self.nz, self.dt, batch=self.batch, precision=precision, device=device)
         try:
-            eng.set_coefficients(self.alpha_E, self.beta_E, self.alpha_H, self.beta_H, self.M_eps, self.M_mu)
+            self.put_coefficients(eng)
             for f in self.cpml:
                 eng.add_cpml(f.face, f.b, f.c, f.ck, f.air)
             for mp in self.modal:
@@ -224,6 +265,14 @@ class FitProblem:
             eng.close()
             raise
         return eng
+
+    def materialize(self) -> "FitProblem":
+        """The coefficient arrays on the host (for the CPU oracle), when the
+        problem carries only its materials."""
+        if self.alpha_E is None and self.materials is not None:
+            (self.alpha_E, self.beta_E, self.alpha_H, self.beta_H, self.M_eps,
+             self.M_mu) = self.materials.host_arrays(self.dx, self.dy, self.dz, self.dt)
+        return self
 
     # ---- npz round trip ---------------------------------------------------
     def to_arrays(self, prefix: str = "p.") -> dict:

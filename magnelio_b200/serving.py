@@ -356,12 +356,15 @@ class ServingLoop:
 
 
 def request_stream(n: int, seed: int = 7, mean_gap: float = 0.020, cells=(32**3, 192**3), steps=(6000, 12000),
-                   ports=(2, 4), n_freq: int = 101):
+                   ports=(2, 4), n_freq: int = 101, device_setup: bool = True):
     """The serving workload: ``n`` requests with Poisson arrivals (mean gap
     ``mean_gap`` s), each a rectangular or single-ridge waveguide section
     with dimensions ``U[0.7, 1.3]`` x (22.86, 10.16, 40) mm, 0-4 dielectric
     inserts (``eps_r ~ U[2, 10]``), a log-uniform cell count in ``cells``,
-    ``ports`` lumped ports and a step count in ``steps``."""
+    ``ports`` lumped ports and a step count in ``steps``.  With
+    ``device_setup`` (the default) a request's material matrices and
+    coefficients are built on the device when its handle is created: the
+    host prepares the grid and the cell materials only."""
     from magnelio_b200.workloads import waveguide_section
 
     rng = np.random.default_rng(seed)
@@ -379,7 +382,8 @@ def request_stream(n: int, seed: int = 7, mean_gap: float = 0.020, cells=(32**3,
 
         def build(batch, dims=dims, c=c, P=P, st=st, ins=ins, ridged=ridged, sub=sub):
             return waveguide_section(np.random.default_rng(sub), a=dims[0], b=dims[1], length=dims[2], cells=c,
-                                     n_inserts=ins, ridged=ridged, n_ports=P, steps=st, batch=batch)
+                                     n_inserts=ins, ridged=ridged, n_ports=P, steps=st, batch=batch,
+                                     device_setup=device_setup)
 
         out.append(Request(rid=rid, arrival=t, build=build, n_ports=P, steps=st,
                            freqs=np.linspace(7.0e9, 13.0e9, n_freq)))

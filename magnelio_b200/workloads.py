@@ -17,7 +17,7 @@ import math
 import numpy as np
 
 from magnelio_b200 import host
-from magnelio_b200.problem import CpmlFace, DftMonitor, Dispersion, FitProblem, LumpedPort
+from magnelio_b200.problem import CpmlFace, DftMonitor, Dispersion, FitProblem, LumpedPort, MaterialSetup
 
 FACES = ("xmin", "xmax", "ymin", "ymax", "zmin", "zmax")
 
@@ -159,7 +159,7 @@ def _pec_edges_in_box(x, y, z, lo, hi) -> np.ndarray:
 def waveguide_section(rng, *, a: float = 22.86e-3, b: float = 10.16e-3, length: float = 40e-3,
                       cells: int = 48**3, n_inserts: int = 2, ridged: bool = False, n_ports: int = 2,
                       steps: int = 6000, f_min: float = 7.0e9, f_max: float = 13.0e9, cpml_cells: int = 8,
-                      z0: float = 50.0, batch: int | None = None) -> FitProblem:
+                      z0: float = 50.0, batch: int | None = None, device_setup: bool = False) -> FitProblem:
     """One S-parameter request of the serving workload: an ``a x b x length``
     rectangular (or single-ridge) waveguide section on a uniform grid of
     about ``cells`` cells, PEC side walls, CPML on both ends (matched guide
@@ -167,7 +167,10 @@ def waveguide_section(rng, *, a: float = 22.86e-3, b: float = 10.16e-3, length: 
     ``n_ports`` y-directed lumped ports (50 Ohm) spread along the guide.
     Field set ``p`` drives port ``p`` with a modulated Gaussian over
     ``[f_min, f_max]``, the other ports load it; field sets beyond the ports
-    (``batch`` rounds up to a width the batched kernels take) stay idle."""
+    (``batch`` rounds up to a width the batched kernels take) stay idle.
+    ``device_setup``: the problem carries its materials and PEC edges, and
+    the engine builds the material matrices and coefficients on the device
+    (``FitProblem.materialize()`` gives the host arrays)."""
     from magnelio_b200.adapter import _pec_face_flat_indices
 
     h = (a * b * length / cells) ** (1.0 / 3.0)
@@ -182,21 +185,22 @@ def waveguide_section(rng, *, a: float = 22.86e-3, b: float = 10.16e-3, length: 
         eps_r.append(float(rng.uniform(2.0, 10.0)))
     mat_id = host.assign_bricks(x, y, z, bricks) if bricks else np.zeros((nx, ny, nz), np.int32)
     eps_table = np.concatenate([[1.0], eps_r])
-    M_eps = host.build_M_eps(x, y, z, eps_table, mat_id)
-    M_mu = host.build_M_mu(x, y, z)
     dt = host.courant_dt(x, y, z, "normal")
-    aE, bE, aH, bH = host.leapfrog_coefficients(M_eps, M_mu, dt)
     pec = [_pec_face_flat_indices(nx, ny, nz, f) for f in ("xmin", "xmax", "ymin", "ymax")]
     if ridged:
         w, d = rng.uniform(0.2, 0.4) * a, rng.uniform(0.2, 0.4) * b
         pec.append(_pec_edges_in_box(x, y, z, (0.5 * (a - w), b - d, 0.0), (0.5 * (a + w), b, length)))
     pec = np.concatenate(pec)
-    aE[pec] = 0.0
-    bE[pec] = 0.0
     B = batch if batch is not None else n_ports
     B = next(w for w in (1, 2, 4, 8, 16, B) if w >= B)
-    prob = FitProblem(nx=nx, ny=ny, nz=nz, dt=dt, dx=np.diff(x), dy=np.diff(y), dz=np.diff(z),
-                      alpha_E=aE, beta_E=bE, alpha_H=aH, beta_H=bH, M_eps=M_eps, M_mu=M_mu, batch=B)
+    materials = MaterialSetup(mat_id=mat_id, eps_r=eps_table, pec_idx=pec)
+    if device_setup:
+        prob = FitProblem(nx=nx, ny=ny, nz=nz, dt=dt, dx=np.diff(x), dy=np.diff(y), dz=np.diff(z),
+                          alpha_E=None, beta_E=None, alpha_H=None, beta_H=None, materials=materials, batch=B)
+    else:
+        aE, bE, aH, bH, M_eps, M_mu = materials.host_arrays(np.diff(x), np.diff(y), np.diff(z), dt)
+        prob = FitProblem(nx=nx, ny=ny, nz=nz, dt=dt, dx=np.diff(x), dy=np.diff(y), dz=np.diff(z),
+                          alpha_E=aE, beta_E=bE, alpha_H=aH, beta_H=bH, M_eps=M_eps, M_mu=M_mu, batch=B)
     for face in ("zmin", "zmax"):
         bt, ct, ckt = host.cpml_tables(np.diff(z), face, dt, thickness_cells=cpml_cells)
         prob.cpml.append(CpmlFace(face, bt, ct, ckt))
@@ -210,8 +214,9 @@ def waveguide_section(rng, *, a: float = 22.86e-3, b: float = 10.16e-3, length: 
         j = max(1, ny // 4)
         flat = n_ex + (i * ny + j) * (nz + 1) + k  # Ey (nx+1, ny, nz+1)
         v = [drive if q == p else np.zeros_like(drive) for q in range(B)]
+        m_eps = host.m_eps_edges(x, y, z, eps_table, mat_id, [flat])[0]
         prob.lumped.append(LumpedPort(flat_idx=np.array([flat], np.int64), signs=np.ones(1),
-                                      betas=np.array([dt / M_eps[flat]]), R=z0, record_scale=1.0, v_src=v))
+                                      betas=np.array([dt / m_eps]), R=z0, record_scale=1.0, v_src=v))
     prob.e0 = [None] * B
     prob.h0 = [None] * B
     return prob

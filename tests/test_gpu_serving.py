@@ -62,7 +62,7 @@ def test_served_s_matrix_meets_the_fp64_oracle():
                                   n_freq=9)
     req = reqs[0]
     res = serving.ServingLoop(max_slots=1, slice_steps=300).run([req]).results[0]
-    prob = req.build(None)
+    prob = req.build(None).materialize()  # host arrays for the oracle
     Vs, Is = [], []
     for b in range(req.n_ports):
         r = OracleRun(prob, b=b).run(req.steps)
@@ -90,3 +90,21 @@ def test_device_s_matrix_equals_the_host_assembly_of_the_records(plain):
     for a, b in zip(host.results, dev.results):
         assert a.rid == b.rid and b.V is None and b.S.shape == a.S.shape
         assert float(np.max(np.abs(a.S - b.S) / np.maximum(1.0, np.abs(a.S)))) < 1e-9
+
+
+def test_device_built_materials_equal_the_host_build():
+    """A serving request's material matrices and coefficients built on the
+    device (fitb_build_materials) march exactly like the same constants
+    built on the host and uploaded: identical fields and V/I."""
+    from magnelio_b200 import workloads
+
+    outs = []
+    for dev in (True, False):
+        p = workloads.waveguide_section(np.random.default_rng(21), cells=22**3, n_inserts=3, ridged=True, n_ports=3,
+                                        steps=150, device_setup=dev)
+        assert (p.alpha_E is None) == dev
+        with p.build_engine("single") as eng:
+            eng.step(150)
+            outs.append([eng.read_fields(b) for b in range(p.batch)] + [eng.read_vi(b) for b in range(p.batch)])
+    for a, b in zip(outs[0], outs[1]):
+        assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
