@@ -46,9 +46,11 @@ DEFAULT_CANDIDATES = (
     ("fused", 17, 0),
     ("fused", 18, 0),
     ("fused", 19, 0),
+    ("fused", 20, 0),
+    ("fused", 21, 0),
     ("bulk", 0, 0),
 )
-CANDIDATE_SET = 3  # bump when the candidates change: cached results of another set are not reused
+CANDIDATE_SET = 4  # bump when the candidates change: cached results of another set are not reused
 
 
 @dataclass

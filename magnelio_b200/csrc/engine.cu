@@ -181,9 +181,10 @@ struct Handle {
     // beside the stencil (fork / join by events inside the capture)
     cudaStream_t side = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
-    // third stream: the slab step's CPML unit lists beside its CPML-free list
-    cudaStream_t side2 = nullptr;
-    cudaEvent_t ev_sfork = nullptr, ev_sjoin = nullptr;
+    // the slab step's CPML unit lists, one stream each beside the CPML-free
+    // list on the handle's stream
+    cudaStream_t slab_side[kSlabLists] = {};
+    cudaEvent_t ev_sfork = nullptr, ev_sjoin[kSlabLists] = {};
     DevBuf e, h, aE, bE, aH, bH, meps, mmu, staging;
     // Fused step: second field buffers; `cur` names the buffer set that
     // holds the current fields (always 0 for the in-place kernels).
@@ -251,8 +252,10 @@ struct Handle {
             if (graph_one[q]) cudaGraphExecDestroy(graph_one[q]);
         }
         if (ev_sfork) cudaEventDestroy(ev_sfork);
-        if (ev_sjoin) cudaEventDestroy(ev_sjoin);
-        if (side2) cudaStreamDestroy(side2);
+        for (int q = 0; q < kSlabLists; ++q) {
+            if (ev_sjoin[q]) cudaEventDestroy(ev_sjoin[q]);
+            if (slab_side[q]) cudaStreamDestroy(slab_side[q]);
+        }
         if (ev_fork) cudaEventDestroy(ev_fork);
         if (ev_join) cudaEventDestroy(ev_join);
         if (side) cudaStreamDestroy(side);
@@ -802,22 +805,27 @@ int launch_fused(Handle& H, const StencilArgs<T>& sa) {
         bool air = false;
         for (int q = 0; q < kSlabLists; ++q) units[q] = H.slab_units[q].as<int4>();
         for (auto& f : H.faces) air = air || f->pec;
-        // the CPML lists run on a second stream beside the CPML-free list
-        // (disjoint units), joined before anything reads the new fields
-        bool cpml = false;
-        for (int q = 1; q < kSlabLists; ++q) cpml = cpml || H.n_slab_units[q] > 0;
-        const bool fork = cpml && H.n_slab_units[0] > 0;
-        if (fork) {
-            ck(cudaEventRecord(H.ev_sfork, H.stream), "slab fork record");
-            ck(cudaStreamWaitEvent(H.side2, H.ev_sfork, 0), "slab fork wait");
+        // every CPML list runs on a stream of its own beside the CPML-free
+        // list (disjoint units), all joined before anything reads the new
+        // fields
+        cudaStream_t streams[kSlabLists];
+        streams[0] = H.stream;
+        bool forked = false;
+        for (int q = 1; q < kSlabLists; ++q) {
+            streams[q] = H.n_slab_units[q] > 0 ? H.slab_side[q] : H.stream;
+            if (H.n_slab_units[q] > 0 && !forked) {
+                ck(cudaEventRecord(H.ev_sfork, H.stream), "slab fork record");
+                forked = true;
+            }
+            if (H.n_slab_units[q] > 0) ck(cudaStreamWaitEvent(H.slab_side[q], H.ev_sfork, 0), "slab fork wait");
         }
         const int n = launch_slab_step<T>(sa, H.splan.ichunk, H.fused_variant - kFusedSlabBase, units,
-                                          H.n_slab_units, air, H.status.as<int>(), H.stream,
-                                          fork ? H.side2 : H.stream);
+                                          H.n_slab_units, air, H.status.as<int>(), streams);
         if (n < 0) fail(FITB_ERR_CUDA, "tensor maps of the slab step could not be encoded");
-        if (fork) {
-            ck(cudaEventRecord(H.ev_sjoin, H.side2), "slab join record");
-            ck(cudaStreamWaitEvent(H.stream, H.ev_sjoin, 0), "slab join wait");
+        for (int q = 1; q < kSlabLists; ++q) {
+            if (H.n_slab_units[q] <= 0) continue;
+            ck(cudaEventRecord(H.ev_sjoin[q], H.slab_side[q]), "slab join record");
+            ck(cudaStreamWaitEvent(H.stream, H.ev_sjoin[q], 0), "slab join wait");
         }
         return n;
     }
@@ -1437,9 +1445,11 @@ int fitb_create(const fitb_desc* desc, fitb_handle** out) {
     ck(cudaStreamCreateWithFlags(&H.side, cudaStreamNonBlocking), "stream");
     ck(cudaEventCreateWithFlags(&H.ev_fork, cudaEventDisableTiming), "event");
     ck(cudaEventCreateWithFlags(&H.ev_join, cudaEventDisableTiming), "event");
-    ck(cudaStreamCreateWithFlags(&H.side2, cudaStreamNonBlocking), "stream");
     ck(cudaEventCreateWithFlags(&H.ev_sfork, cudaEventDisableTiming), "event");
-    ck(cudaEventCreateWithFlags(&H.ev_sjoin, cudaEventDisableTiming), "event");
+    for (int q = 1; q < fitb::kSlabLists; ++q) {
+        ck(cudaStreamCreateWithFlags(&H.slab_side[q], cudaStreamNonBlocking), "stream");
+        ck(cudaEventCreateWithFlags(&H.ev_sjoin[q], cudaEventDisableTiming), "event");
+    }
     const size_t blk = (size_t)H.e_block() * H.esz;
     H.e.alloc(blk * H.B);
     H.h.alloc(blk * H.B);
@@ -1669,7 +1679,7 @@ int fitb_configure_stencil(fitb_handle* h, int32_t kind, int32_t variant, int32_
         if (!fitb::fused_variant_ok(H.prec, variant)) fail(FITB_ERR_ARG, "fused variant %d", variant);
         if ((H.disp[0].present() || H.disp[1].present()) && !fitb::is_slab_variant(variant))
             fail(FITB_ERR_STATE,
-                 "dispersive materials need an in-place stencil mode or the slab step (fused 16-19)");
+                 "dispersive materials need an in-place stencil mode or the slab step (fused 16-21)");
         if ((H.disp[0].present() || H.disp[1].present()) && !fitb::disp_clear_of_cpml(H))
             fail(FITB_ERR_STATE, "the slab step takes dispersive materials only outside the CPML slabs");
         if (fitb::is_tile_variant(variant) &&
@@ -2102,7 +2112,7 @@ int fitb_add_dispersion_block(fitb_handle* h, int32_t side, int64_t n_states, co
         fail(FITB_ERR_ARG, "dispersion block needs states, poles and all arrays");
     if (H.steps_done != 0) fail(FITB_ERR_STATE, "dispersion must be added before the first step");
     if (H.stencil_mode == fitb::kModeFused && !fitb::is_slab_variant(H.fused_variant))
-        fail(FITB_ERR_STATE, "dispersive materials need an in-place stencil mode or the slab step (fused 16-19)");
+        fail(FITB_ERR_STATE, "dispersive materials need an in-place stencil mode or the slab step (fused 16-21)");
     fitb::DispHost& D = H.disp[side];
     const int blk = (int)D.pole_start.size() - 1;
     for (int q = 0; q < n_poles; ++q) {

@@ -171,8 +171,8 @@ int launch_tile_cpml_H(const StencilArgs<T>& a, cudaStream_t s);
 // Slab form of the fused step (stencil_slab.cu): the tile march with the
 // CPML applied inside it, launched once per list of units with 0..3 CPML
 // face slots; fused-step variants kFusedSlabBase + v with (tile rows, ring
-// stages) = (4, 3), (2, 3), (3, 3), (4, 4) for v = 0..3.
-constexpr int kFusedSlabBase = kFusedTileBase + kTileVariants, kSlabVariants = 4;
+// stages) = (4, 3), (2, 3), (3, 3), (4, 4), (3, 4), (2, 4) for v = 0..5.
+constexpr int kFusedSlabBase = kFusedTileBase + kTileVariants, kSlabVariants = 6;
 inline bool is_tile_variant(int v) { return v >= kFusedTileBase && v < kFusedSlabBase; }
 inline bool is_slab_variant(int v) { return v >= kFusedSlabBase && v < kFusedSlabBase + kSlabVariants; }
 int slab_tj_of(int variant);
@@ -199,13 +199,13 @@ int slab_unit_liveness(const Geom& g, const T* aE, const T* bE, const T* aH, con
 template <typename T>
 int slab_dead_sync(const Geom& g, const T* aH, const T* bH, int tj, int ichunk, const int4* units, int n, int B,
                    T* e_cur, T* h_cur, T* e_oth, T* h_oth, cudaStream_t s);
-// Launches one kernel per non-empty unit list, the CPML-free list on s and
-// the lists with face slots on s_cpml (the units are disjoint: the caller
-// may run the two streams side by side); returns the launches issued (< 0:
-// tensor maps not encodable).  air: some face has PEC masks.
+// Launches one kernel per non-empty unit list, list q on streams[q] (the
+// units are disjoint: the caller may run the streams side by side); returns
+// the launches issued (< 0: tensor maps not encodable).  air: some face has
+// PEC masks.
 template <typename T>
 int launch_slab_step(StencilArgs<T> a, int ichunk, int variant, const int4* const units[kSlabLists],
-                     const int n_units[kSlabLists], bool air, int* status, cudaStream_t s, cudaStream_t s_cpml);
+                     const int n_units[kSlabLists], bool air, int* status, const cudaStream_t streams[kSlabLists]);
 // One CTA waits, bounded by `limit` tries, on an mbarrier that nothing
 // completes; the expired wait writes kStatusWaitTimeoutTile to *status.
 cudaError_t launch_wait_probe(int* status, unsigned limit, cudaStream_t s);

@@ -599,6 +599,8 @@ bool slab_dispatch(int variant, F&& f) {
         case 1: f.template run<2, 3>(); return true;
         case 2: f.template run<3, 3>(); return true;
         case 3: f.template run<4, 4>(); return true;
+        case 4: f.template run<3, 4>(); return true;
+        case 5: f.template run<2, 4>(); return true;
         default: return false;
     }
 }
@@ -679,14 +681,14 @@ struct SlabLaunch {
     const int* n_units;
     bool air;
     int* status;
-    cudaStream_t s, s_cpml;  // the CPML-free list, the lists with face slots
+    const cudaStream_t* streams;  // one per list
     int launched = 0;
     template <int NSLOT, bool AIR, int CK, int TJ, int NS>
     void go(int q) {
         if (n_units[q] <= 0) return;
         k_step_slab<T, TJ, NS, NSLOT, AIR, CK>
             <<<dim3((unsigned)n_units[q] * a.B), 32 * (TJ + 1), SlabGeo<T, TJ, NS, NSLOT, AIR, CK>::smem,
-               q == 0 ? s : s_cpml>>>(m, a, units[q], status);
+               streams[q]>>>(m, a, units[q], status);
         ++launched;
     }
     template <int CK, int TJ, int NS>
@@ -892,7 +894,7 @@ template StreamPlan plan_slab<double>(const Geom&, int, int, int, int);
 
 template <typename T>
 int launch_slab_step(StencilArgs<T> a, int ichunk, int variant, const int4* const units[5], const int n_units[5],
-                     bool air, int* status, cudaStream_t s, cudaStream_t s_cpml) {
+                     bool air, int* status, const cudaStream_t streams[5]) {
     SlabInfo<T> info;
     if (!slab_dispatch(variant, info)) return -1;
     const int tj = info.tj;
@@ -940,13 +942,13 @@ int launch_slab_step(StencilArgs<T> a, int ichunk, int variant, const int4* cons
             return -2;
     }
     a.ichunk = ichunk;
-    SlabLaunch<T> l{m, a, units, n_units, air, status, s, s_cpml};
+    SlabLaunch<T> l{m, a, units, n_units, air, status, streams};
     slab_dispatch(variant, l);
     return l.launched;
 }
 template int launch_slab_step<float>(StencilArgs<float>, int, int, const int4* const[5], const int[5], bool, int*,
-                                     cudaStream_t, cudaStream_t);
+                                     const cudaStream_t[5]);
 template int launch_slab_step<double>(StencilArgs<double>, int, int, const int4* const[5], const int[5], bool, int*,
-                                      cudaStream_t, cudaStream_t);
+                                      const cudaStream_t[5]);
 
 }  // namespace fitb
