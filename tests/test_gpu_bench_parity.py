@@ -14,10 +14,12 @@ march), and compared with the float64 C port of the reference's step
 Field error: ``||x - x_ref||`` relative to the largest field norm of the run
 (``oracle/prefix_parity.py``).  DFT bins: per monitor component, the max
 abs difference relative to its largest bin and the relative L2 norm of the
-difference.  The reference's own float32 march (the C port in float32) at
-128^3 x 2000 steps departs from its float64 march by 1.5e-7 (E), 1.9e-6
-(H), 4.2e-4 (DFT max) and 2.8e-5 (DFT L2) on these measures; the bars
-below leave a few times that.
+difference.  The reference's own float32 march (the C port in float32)
+departs from its float64 march on these measures by
+  128^3 x 2000 steps: 1.5e-7 (E), 1.9e-6 (H), 4.2e-4 (DFT max), 2.8e-5 (DFT L2);
+  256^3 x 500 steps:  2.4e-7 (E), 2.9e-6 (H), 2.7e-4 (DFT max), 1.5e-4 (DFT L2)
+(the 500-step bins are partial sums of a pulse still rising, with more
+cancellation); the bars below leave a few times that.
 """
 
 from __future__ import annotations
@@ -28,7 +30,7 @@ pytestmark = pytest.mark.gpu
 
 FIELD_TOL = 2e-4     # ||x - x_ref|| / max_n ||x_ref(n)||, float32 engine vs float64
 DFT_TOL = 2e-3       # max |bin - bin_ref| / max |bin_ref| per monitor component
-DFT_L2_TOL = 1e-4    # ||bins - bins_ref|| / ||bins_ref|| per monitor component
+DFT_L2_TOL = 5e-4    # ||bins - bins_ref|| / ||bins_ref|| per monitor component
 
 # two-pass stream kernels, TMA tile step with CPML passes, slab step (CPML inside the march)
 FORMS = [("stream", 0), ("fused", 7), ("fused", 16)]
