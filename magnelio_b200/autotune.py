@@ -48,9 +48,11 @@ DEFAULT_CANDIDATES = (
     ("fused", 19, 0),
     ("fused", 20, 0),
     ("fused", 21, 0),
+    ("fused", 22, 0),
+    ("fused", 23, 0),
     ("bulk", 0, 0),
 )
-CANDIDATE_SET = 4  # bump when the candidates change: cached results of another set are not reused
+CANDIDATE_SET = 5  # bump when the candidates change: cached results of another set are not reused
 
 
 @dataclass

@@ -1679,7 +1679,7 @@ int fitb_configure_stencil(fitb_handle* h, int32_t kind, int32_t variant, int32_
         if (!fitb::fused_variant_ok(H.prec, variant)) fail(FITB_ERR_ARG, "fused variant %d", variant);
         if ((H.disp[0].present() || H.disp[1].present()) && !fitb::is_slab_variant(variant))
             fail(FITB_ERR_STATE,
-                 "dispersive materials need an in-place stencil mode or the slab step (fused 16-21)");
+                 "dispersive materials need an in-place stencil mode or the slab step (fused 16-23)");
         if ((H.disp[0].present() || H.disp[1].present()) && !fitb::disp_clear_of_cpml(H))
             fail(FITB_ERR_STATE, "the slab step takes dispersive materials only outside the CPML slabs");
         if (fitb::is_tile_variant(variant) &&
@@ -2112,7 +2112,7 @@ int fitb_add_dispersion_block(fitb_handle* h, int32_t side, int64_t n_states, co
         fail(FITB_ERR_ARG, "dispersion block needs states, poles and all arrays");
     if (H.steps_done != 0) fail(FITB_ERR_STATE, "dispersion must be added before the first step");
     if (H.stencil_mode == fitb::kModeFused && !fitb::is_slab_variant(H.fused_variant))
-        fail(FITB_ERR_STATE, "dispersive materials need an in-place stencil mode or the slab step (fused 16-21)");
+        fail(FITB_ERR_STATE, "dispersive materials need an in-place stencil mode or the slab step (fused 16-23)");
     fitb::DispHost& D = H.disp[side];
     const int blk = (int)D.pole_start.size() - 1;
     for (int q = 0; q < n_poles; ++q) {

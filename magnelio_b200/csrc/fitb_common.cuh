@@ -171,8 +171,10 @@ int launch_tile_cpml_H(const StencilArgs<T>& a, cudaStream_t s);
 // Slab form of the fused step (stencil_slab.cu): the tile march with the
 // CPML applied inside it, launched once per list of units with 0..3 CPML
 // face slots; fused-step variants kFusedSlabBase + v with (tile rows, ring
-// stages) = (4, 3), (2, 3), (3, 3), (4, 4), (3, 4), (2, 4) for v = 0..5.
-constexpr int kFusedSlabBase = kFusedTileBase + kTileVariants, kSlabVariants = 6;
+// stages of the CPML-free list, of the CPML lists) = (4, 3, 3), (2, 3, 3),
+// (3, 3, 3), (4, 4, 4), (3, 4, 4), (2, 4, 4), (4, 3, 4), (3, 3, 4) for
+// v = 0..7.
+constexpr int kFusedSlabBase = kFusedTileBase + kTileVariants, kSlabVariants = 8;
 inline bool is_tile_variant(int v) { return v >= kFusedTileBase && v < kFusedSlabBase; }
 inline bool is_slab_variant(int v) { return v >= kFusedSlabBase && v < kFusedSlabBase + kSlabVariants; }
 int slab_tj_of(int variant);

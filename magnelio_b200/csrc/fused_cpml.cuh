@@ -4,6 +4,9 @@
 #pragma once
 #include "fitb_common.cuh"
 
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
 namespace fitb {
 
 namespace {
@@ -22,6 +25,27 @@ __device__ __forceinline__ void load_coef3(FCoef<T>& c, const T* __restrict__ a,
     c.bx = __ldg(b + o);
     c.by = __ldg(b + vol + o);
     c.bz = __ldg(b + 2 * vol + o);
+}
+
+// H coefficients of one cell in the handle's storage: the field dtype, or
+// the compact 16-bit copies times their per-component scales (decoded as
+// the stream kernels decode them).
+template <typename T>
+__device__ __forceinline__ void load_coefH_stored(FCoef<T>& c, const StencilArgs<T>& p, long long o, long long vol) {
+    if (p.coef_kind == kCoefNative) {
+        load_coef3(c, p.aH, p.bH, o, vol);
+        return;
+    }
+    const unsigned short *qa = p.cq[2], *qb = p.cq[3];
+    auto dec = [&](unsigned short u) {
+        return p.coef_kind == kCoefF16 ? __half2float(__ushort_as_half(u)) : __bfloat162float(__ushort_as_bfloat16(u));
+    };
+    c.ax = (T)dec(qa[o]) * (T)p.cs[8];
+    c.ay = (T)dec(qa[vol + o]) * (T)p.cs[9];
+    c.az = (T)dec(qa[2 * vol + o]) * (T)p.cs[10];
+    c.bx = (T)dec(qb[o]) * (T)p.cs[12];
+    c.by = (T)dec(qb[vol + o]) * (T)p.cs[13];
+    c.bz = (T)dec(qb[2 * vol + o]) * (T)p.cs[14];
 }
 
 __device__ __forceinline__ long long slab_at(const FaceDev& f, int l, int i, int j, int k) {

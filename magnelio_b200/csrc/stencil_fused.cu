@@ -178,7 +178,7 @@ __global__ void k_fix_H(const StencilArgs<T> p, const int4* __restrict__ cells, 
         const T ey_kp = E[vol + o + 1], ex_kp = E[o + 1];
         const T ez_ip = E[2 * vol + o + si], ey_ip = E[vol + o + si];
         FCoef<T> ch;
-        load_coef3(ch, p.aH, p.bH, o, vol);
+        load_coefH_stored(ch, p, o, vol);  // the storage the step kernel read
         const T cxh = ((ez_jp - ez) - ey_kp) + ey;
         const T cyh = ((ex_kp - ex) - ez_ip) + ez;
         const T czh = ((ey_ip - ey) - ex_jp) + ex;

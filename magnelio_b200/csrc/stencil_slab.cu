@@ -591,16 +591,18 @@ __global__ void k_dead_units_sync(Geom g, const T* __restrict__ aH, const T* __r
     }
 }
 
-// Slab variants: (TJ, NS).
+// Slab variants: (TJ, NS of the CPML-free list, NS of the CPML lists).
 template <typename F>
 bool slab_dispatch(int variant, F&& f) {
     switch (variant) {
-        case 0: f.template run<4, 3>(); return true;
-        case 1: f.template run<2, 3>(); return true;
-        case 2: f.template run<3, 3>(); return true;
-        case 3: f.template run<4, 4>(); return true;
-        case 4: f.template run<3, 4>(); return true;
-        case 5: f.template run<2, 4>(); return true;
+        case 0: f.template run<4, 3, 3>(); return true;
+        case 1: f.template run<2, 3, 3>(); return true;
+        case 2: f.template run<3, 3, 3>(); return true;
+        case 3: f.template run<4, 4, 4>(); return true;
+        case 4: f.template run<3, 4, 4>(); return true;
+        case 5: f.template run<2, 4, 4>(); return true;
+        case 6: f.template run<4, 3, 4>(); return true;
+        case 7: f.template run<3, 3, 4>(); return true;
         default: return false;
     }
 }
@@ -651,10 +653,11 @@ template <typename T>
 struct SlabInfo {
     size_t smem = 0;
     int tj = 0, occ0 = 1;
-    template <int TJ, int NS>
+    template <int TJ, int NS, int NSC>
     void run() {
         MaxSmem m;
         each_instance<T, TJ, NS>(m);
+        if constexpr (NSC != NS) each_instance<T, TJ, NSC>(m);
         smem = m.v;
         tj = TJ;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ0, k_step_slab<T, TJ, NS, 0, false, kCoefNative>,
@@ -665,10 +668,11 @@ struct SlabInfo {
 template <typename T>
 struct SlabPrepare {
     cudaError_t err = cudaSuccess;
-    template <int TJ, int NS>
+    template <int TJ, int NS, int NSC>
     void run() {
         Prepare pr;
         each_instance<T, TJ, NS>(pr);
+        if constexpr (NSC != NS) each_instance<T, TJ, NSC>(pr);
         err = pr.err;
     }
 };
@@ -691,30 +695,30 @@ struct SlabLaunch {
                streams[q]>>>(m, a, units[q], status);
         ++launched;
     }
-    template <int CK, int TJ, int NS>
+    template <int CK, int TJ, int NS, int NSC>
     void run_ck() {
         go<0, false, CK, TJ, NS>(0);
         if (air) {
-            go<1, true, CK, TJ, NS>(1);
-            go<2, true, CK, TJ, NS>(2);
-            go<3, true, CK, TJ, NS>(3);
-            go<6, true, CK, TJ, NS>(4);
+            go<1, true, CK, TJ, NSC>(1);
+            go<2, true, CK, TJ, NSC>(2);
+            go<3, true, CK, TJ, NSC>(3);
+            go<6, true, CK, TJ, NSC>(4);
         } else {
-            go<1, false, CK, TJ, NS>(1);
-            go<2, false, CK, TJ, NS>(2);
-            go<3, false, CK, TJ, NS>(3);
-            go<6, false, CK, TJ, NS>(4);
+            go<1, false, CK, TJ, NSC>(1);
+            go<2, false, CK, TJ, NSC>(2);
+            go<3, false, CK, TJ, NSC>(3);
+            go<6, false, CK, TJ, NSC>(4);
         }
     }
-    template <int TJ, int NS>
+    template <int TJ, int NS, int NSC>
     void run() {
         if constexpr (sizeof(T) == 4) {
             if (a.coef_kind == kCoefF16) {
-                run_ck<kCoefF16, TJ, NS>();
+                run_ck<kCoefF16, TJ, NS, NSC>();
                 return;
             }
         }
-        run_ck<kCoefNative, TJ, NS>();
+        run_ck<kCoefNative, TJ, NS, NSC>();
     }
 };
 

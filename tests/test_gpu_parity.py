@@ -115,7 +115,7 @@ def test_stencil_variants_agree(name):
     p, d, n = load_golden(name)
     outs = []
     modes = [("stream", v) for v in range(4)] + [("bulk", 0), ("simple", 0)]
-    modes += [("vec", v) for v in range(4)] + [("fused", v) for v in range(22)]
+    modes += [("vec", v) for v in range(4)] + [("fused", v) for v in range(24)]
     for kind, variant in modes:
         with p.build_engine("single") as eng:
             eng.configure_stencil(kind, variant)
@@ -634,7 +634,7 @@ def test_cross_junction_batch_equals_one_excitation_per_handle():
 # TMA tile form of the fused step on grids of many tiles and chunks.
 
 TILE_VARIANTS = range(7, 16)
-SLAB_VARIANTS = range(16, 22)
+SLAB_VARIANTS = range(16, 24)
 
 
 def _random_state(prob, rng, scale=1e-3):
