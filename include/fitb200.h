@@ -167,6 +167,20 @@ int fitb_set_coeffs_native(fitb_handle* h, const void* alpha_e, const void* beta
 int fitb_build_materials(fitb_handle* h, const double* dx, const double* dy, const double* dz, const int32_t* mat_id,
                          int32_t n_mat, const double* eps_r, int64_t n_cat1, const int64_t* cat1_idx,
                          const double* cat1_eps, int64_t n_pec, const int64_t* pec_idx);
+/* Spectral time-step limit on the device (replaces the host Lanczos of
+ * spectral_dt / _measure_lambda_max, src/magnelio/solver/stability.py
+ * :296-446): lambda_max of D^-1/2 C^T M_mu^-1 C D^-1/2 (D = M_eps) on the
+ * live E edges (beta_E != 0, M_eps > 0), measured matrix-free by a float64
+ * Lanczos iteration on the handle's M_eps, M_mu and beta_E (so after
+ * fitb_set_coeffs with both mass diagonals, or fitb_build_materials), until
+ * the largest Ritz value changes by less than tol (relative) over ten steps
+ * or after max_iter steps; dt = safety * 2 / sqrt(lambda_max) (the reference's
+ * safety factors: 0.95 "normal").  A float32 handle holds its mass diagonals
+ * in float32, which limits lambda_max to float32 accuracy; a float64 handle
+ * reproduces the reference's value to the Lanczos tolerance.  iterations
+ * (may be NULL) receives the steps taken. */
+int fitb_spectral_dt(fitb_handle* h, double safety, int32_t max_iter, double tol, double* lambda_max, double* dt,
+                     int32_t* iterations);
 /* Storage of the four update-coefficient arrays read by the stream stencil
  * kernels: FITB_COEF_NATIVE (field dtype, the default), FITB_COEF_F16 or
  * FITB_COEF_BF16 (16-bit values with a power-of-two scale per component;

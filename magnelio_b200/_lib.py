@@ -127,6 +127,7 @@ SIGNATURES = {
     "fitb_set_coeff_storage": ([vp, i32], C.c_int),
     "fitb_configure_stencil": ([vp, i32, i32, i32], C.c_int),
     "fitb_get_stencil": ([vp, P_i32], C.c_int),
+    "fitb_spectral_dt": ([vp, C.c_double, i32, C.c_double, P_f64, P_f64, P_i32], C.c_int),
     "fitb_build_materials": ([vp, P_f64, P_f64, P_f64, P_i32, i32, P_f64, i64, P_i64, P_f64, i64, P_i64], C.c_int),
     "fitb_slab_units": ([vp, P_i64], C.c_int),
     "fitb_device_bytes": ([vp, P_i64], C.c_int),

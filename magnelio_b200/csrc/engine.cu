@@ -1607,6 +1607,29 @@ int fitb_build_materials(fitb_handle* h, const double* dx, const double* dy, con
     FITB_CATCH
 }
 
+int fitb_spectral_dt(fitb_handle* h, double safety, int32_t max_iter, double tol, double* lambda_max, double* dt,
+                     int32_t* iterations) {
+    FITB_TRY
+    Handle& H = H_of(h);
+    if (!lambda_max || !dt || max_iter < 1 || !(tol > 0.0) || !(safety > 0.0)) fail(FITB_ERR_ARG, "bad argument");
+    if (!H.coeffs_set) fail(FITB_ERR_STATE, "coefficients (with M_eps and M_mu) must be set first");
+    ck(cudaStreamSynchronize(H.stream), "sync");
+    double lam = 0.0;
+    int its = 0;
+    const int rc = H.prec == 4 ? fitb::spectral_lambda<float>(H.g, H.meps.as<float>(), H.mmu.as<float>(),
+                                                              H.bE.as<float>(), max_iter, tol, &lam, &its, H.stream)
+                               : fitb::spectral_lambda<double>(H.g, H.meps.as<double>(), H.mmu.as<double>(),
+                                                               H.bE.as<double>(), max_iter, tol, &lam, &its, H.stream);
+    if (rc == -1) fail(FITB_ERR_CUDA, "spectral dt: device memory for the Lanczos vectors");
+    if (rc != 0) fail(FITB_ERR_CUDA, "spectral dt: kernel launch failed");
+    if (!(lam > 0.0) || !std::isfinite(lam)) fail(FITB_ERR_STATE, "no live update operator (lambda_max = %g)", lam);
+    *lambda_max = lam;
+    *dt = safety * 2.0 / std::sqrt(lam);
+    if (iterations) *iterations = its;
+    H.launches += 5LL * its + 2;
+    FITB_CATCH
+}
+
 int fitb_set_coeffs_native(fitb_handle* h, const void* alpha_e, const void* beta_e, const void* alpha_h,
                            const void* beta_h, const void* m_eps, const void* m_mu) {
     FITB_TRY

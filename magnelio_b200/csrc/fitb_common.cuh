@@ -451,6 +451,12 @@ void launch_setup_materials(const Geom& g, const double* dx, const double* dy, c
                             const double* cat1_eps, long long n_pec, const long long* pec_idx, T* aE, T* bE, T* aH,
                             T* bH, T* meps, T* mmu, double* coef_max, cudaStream_t s);
 
+// lambda_max of the live leapfrog update operator D^-1/2 C^T M_mu^-1 C D^-1/2
+// by a float64 Lanczos iteration (spectral.cu); 0 on success.
+template <typename T>
+int spectral_lambda(const Geom& g, const T* meps, const T* mmu, const T* bE, int max_iter, double tol, double* lambda,
+                    int* iters, cudaStream_t s);
+
 // Energy: per field set 0.5 (sum m_eps e^2 + sum m_mu h^2) in float64.
 template <typename T>
 void launch_energy(const T* e, const T* h, const T* meps, const T* mmu, const Geom& g, int b,

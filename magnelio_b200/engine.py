@@ -133,6 +133,18 @@ class FitEngine:
         check(self._lib.fitb_build_materials(self._h, *[f64p(a) for a in w], i32p(mat), int(eps.size), f64p(eps),
                                              int(ci.size), i64p(ci), f64p(ce), int(pi.size), i64p(pi)))
 
+    def spectral_dt(self, accuracy: str = "normal", max_iter: int = 5000, tol: float = 1e-12):
+        """The reference's sharp leapfrog time-step limit for this handle's
+        coefficients, ``safety * 2 / sqrt(lambda_max)``, with lambda_max
+        measured on the device by a float64 Lanczos iteration.  Returns
+        (dt, lambda_max, iterations)."""
+        from magnelio_b200.host import SAFETY_FACTORS
+
+        lam, dt, its = C.c_double(), C.c_double(), C.c_int32()
+        check(self._lib.fitb_spectral_dt(self._h, float(SAFETY_FACTORS[accuracy]), int(max_iter), float(tol),
+                                         C.byref(lam), C.byref(dt), C.byref(its)))
+        return dt.value, lam.value, its.value
+
     def set_coefficients_native(self, alpha_E, beta_E, alpha_H, beta_H, M_eps=None, M_mu=None) -> None:
         """Upload coefficient arrays that are already in the field dtype."""
         arrs = [np.ascontiguousarray(a) for a in (alpha_E, beta_E, alpha_H, beta_H, M_eps, M_mu) if a is not None]

@@ -919,3 +919,20 @@ def test_tile_step_with_cpml_on_two_field_sets_matches_stream():
         assert _rel(et, es, float(np.max(np.abs(es)))) < 1e-5, b
         assert _rel(ht, hs, float(np.max(np.abs(hs)))) < 1e-5, b
     assert not np.array_equal(outs["fused"][0][0], outs["fused"][1][0])
+
+
+@pytest.mark.parametrize("precision,tol", [("double", 1e-9), ("single", 1e-5)])
+def test_spectral_dt_on_the_device_matches_the_reference(precision, tol):
+    """The sharp leapfrog limit measured on the device (Lanczos on the live
+    update operator) reproduces the time step the reference's own
+    spectral_dt chose for the WR-90 flagship mesh (PEC walls, two port
+    planes): the fixture's dt."""
+    p, d, n = load_golden("cfg1_wr90")
+    p.batch = 1
+    for mp in p.modal:
+        mp.excitation = list(mp.excitation)[:1]
+    p.e0, p.h0 = p.e0[:1], p.h0[:1]
+    with p.build_engine(precision) as eng:
+        dt, lam, its = eng.spectral_dt("normal")
+    print(f"{precision}: dt {dt!r} vs {p.dt!r} after {its} Lanczos steps")
+    assert abs(dt / p.dt - 1.0) < tol
