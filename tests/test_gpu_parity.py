@@ -321,7 +321,7 @@ def test_compact_coefficients_need_the_stream_kernels(monkeypatch):
     monkeypatch.setenv("FITB_STENCIL", "simple")
     p, d, n = load_golden("cpml_box")
     with p.build_engine("single") as eng:
-        with pytest.raises(FitbError, match="stream stencil"):
+        with pytest.raises(FitbError, match="stream or vec stencil"):
             eng.set_coefficient_storage("f16")
         eng.step(2)
 
