@@ -9,6 +9,9 @@
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
+#include <cstdlib>
+#include <cstring>
+
 namespace fitb {
 namespace tma {
 
@@ -77,6 +80,21 @@ inline PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
     return fn;
 }
 
+// L2 fill size of the tensor copies' misses: 256 bytes unless the
+// environment variable FITB_TMA_L2_PROMOTION says none, 64 or 128 (read once
+// per process; a tuning switch, every value computes the same bits).
+inline CUtensorMapL2promotion l2_promotion() {
+    static const CUtensorMapL2promotion v = [] {
+        const char* e = std::getenv("FITB_TMA_L2_PROMOTION");
+        if (!e) return CU_TENSOR_MAP_L2_PROMOTION_L2_256B;
+        if (!std::strcmp(e, "none")) return CU_TENSOR_MAP_L2_PROMOTION_NONE;
+        if (!std::strcmp(e, "64")) return CU_TENSOR_MAP_L2_PROMOTION_L2_64B;
+        if (!std::strcmp(e, "128")) return CU_TENSOR_MAP_L2_PROMOTION_L2_128B;
+        return CU_TENSOR_MAP_L2_PROMOTION_L2_256B;
+    }();
+    return v;
+}
+
 // 4-D tiled map: dims d0..d3 (d0 innermost), byte strides of d1..d3, box
 // b0..b3; no interleave, no swizzle, zero fill outside the dims.
 inline bool encode_4d(CUtensorMap* out, CUtensorMapDataType dt, const void* base, const unsigned long long dims[4],
@@ -88,7 +106,7 @@ inline bool encode_4d(CUtensorMap* out, CUtensorMapDataType dt, const void* base
     const cuuint32_t b[4] = {box[0], box[1], box[2], box[3]};
     const cuuint32_t estr[4] = {1, 1, 1, 1};
     return fn(out, dt, 4, const_cast<void*>(base), d, s, b, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-              CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+              CU_TENSOR_MAP_SWIZZLE_NONE, l2_promotion(),
               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
