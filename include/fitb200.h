@@ -201,9 +201,10 @@ int fitb_set_coeff_storage(fitb_handle* h, int32_t kind);
  * variant of that form (vec 0-3; fused 0-6 the register / cp.async forms,
  * fused 7-15 the TMA tile form with its CPML slab passes, tile shapes of
  * 2-16 rows x 32 cells and 3-5 ring stages; fused 16-23 the slab step, the
- * TMA tile march with the CPML inside it, tiles of 4, 2, 3, 4, 3, 2, 4, 3
- * rows x 32 cells with 3, 3, 3, 4, 4, 4, 3, 3 ring stages for the units
- * without CPML and 3, 3, 3, 4, 4, 4, 4, 4 for those with CPML faces; FITB_ERR_ARG for a form the handle's
+ * TMA tile march with the CPML inside it, tiles of 4, 2, 3, 4, 3, 2, 8, 6
+ * rows x 32 cells with 3, 3, 3, 4, 4, 4, 3, 3 ring stages (variants 22 and
+ * 23 float32 only: their six-slot instances exceed the shared memory of a
+ * CTA in float64); FITB_ERR_ARG for a form the handle's
  * precision, dispersion or CPML layout does not take), and the number of i
  * planes one CTA marches (0: the form's own plan).  The fields, psi and all
  * other state carry over; valid between steps.

@@ -175,7 +175,7 @@ int launch_tile_cpml_H(const StencilArgs<T>& a, cudaStream_t s);
 // CPML applied inside it, launched once per list of units with 0..3 CPML
 // face slots; fused-step variants kFusedSlabBase + v with (tile rows, ring
 // stages of the CPML-free list, of the CPML lists) = (4, 3, 3), (2, 3, 3),
-// (3, 3, 3), (4, 4, 4), (3, 4, 4), (2, 4, 4), (4, 3, 4), (3, 3, 4) for
+// (3, 3, 3), (4, 4, 4), (3, 4, 4), (2, 4, 4), (8, 3, 3), (6, 3, 3) for
 // v = 0..7.
 constexpr int kFusedSlabBase = kFusedTileBase + kTileVariants, kSlabVariants = 8;
 inline bool is_tile_variant(int v) { return v >= kFusedTileBase && v < kFusedSlabBase; }

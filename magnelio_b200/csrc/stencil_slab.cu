@@ -610,8 +610,8 @@ bool slab_dispatch(int variant, F&& f) {
         case 3: f.template run<4, 4, 4>(); return true;
         case 4: f.template run<3, 4, 4>(); return true;
         case 5: f.template run<2, 4, 4>(); return true;
-        case 6: f.template run<4, 3, 4>(); return true;
-        case 7: f.template run<3, 3, 4>(); return true;
+        case 6: f.template run<8, 3, 3>(); return true;
+        case 7: f.template run<6, 3, 3>(); return true;
         default: return false;
     }
 }
@@ -695,13 +695,33 @@ struct SlabLaunch {
     bool air;
     int* status;
     const cudaStream_t* streams;  // one per list
+    int cluster;                  // CTAs per thread-block cluster (1: none)
     int launched = 0;
     template <int NSLOT, bool AIR, int CK, int TJ, int NS>
     void go(int q) {
         if (n_units[q] <= 0) return;
-        k_step_slab<T, TJ, NS, NSLOT, AIR, CK>
-            <<<dim3((unsigned)n_units[q] * a.B), 32 * (TJ + 1), SlabGeo<T, TJ, NS, NSLOT, AIR, CK>::smem,
-               streams[q]>>>(m, a, units[q], status);
+        const unsigned grid = (unsigned)n_units[q] * a.B;
+        const size_t smem = SlabGeo<T, TJ, NS, NSLOT, AIR, CK>::smem;
+        if (cluster > 1 && grid % cluster == 0) {
+            // consecutive CTAs (the field sets of one unit, then neighbouring
+            // units) in one cluster: co-scheduled on one GPC, so the boxes
+            // they share are fetched once into the L2 next to it
+            cudaLaunchConfig_t cfg{};
+            cfg.gridDim = dim3(grid);
+            cfg.blockDim = dim3(32 * (TJ + 1));
+            cfg.dynamicSmemBytes = smem;
+            cfg.stream = streams[q];
+            cudaLaunchAttribute at[1];
+            at[0].id = cudaLaunchAttributeClusterDimension;
+            at[0].val.clusterDim.x = (unsigned)cluster;
+            at[0].val.clusterDim.y = 1;
+            at[0].val.clusterDim.z = 1;
+            cfg.attrs = at;
+            cfg.numAttrs = 1;
+            cudaLaunchKernelEx(&cfg, k_step_slab<T, TJ, NS, NSLOT, AIR, CK>, m, a, units[q], status);
+        } else {
+            k_step_slab<T, TJ, NS, NSLOT, AIR, CK><<<dim3(grid), 32 * (TJ + 1), smem, streams[q]>>>(m, a, units[q], status);
+        }
         ++launched;
     }
     template <int CK, int TJ, int NS, int NSC>
@@ -962,7 +982,21 @@ int launch_slab_step(StencilArgs<T> a, int ichunk, int variant, const int4* cons
         return e ? std::atoi(e) : 0;
     }();
     a.store_cs = store_cs;
-    SlabLaunch<T> l{m, a, units, n_units, air, status, streams};
+    // thread-block clusters of FITB_SLAB_CLUSTER units (default 1) times the
+    // field sets of a unit, at most 8 CTAs; 0: no clusters (read once per
+    // process; a tuning switch, every value computes the same bits)
+    static const int cluster_units = [] {
+        const char* e = std::getenv("FITB_SLAB_CLUSTER");
+        return e ? std::max(0, std::atoi(e)) : 1;
+    }();
+    int cluster = 1;
+    if (cluster_units > 0) {
+        if ((long long)cluster_units * a.B <= 8)
+            cluster = cluster_units * a.B;
+        else if (a.B <= 8)
+            cluster = a.B;
+    }
+    SlabLaunch<T> l{m, a, units, n_units, air, status, streams, cluster};
     slab_dispatch(variant, l);
     return l.launched;
 }

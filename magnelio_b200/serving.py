@@ -113,12 +113,13 @@ def _footprint_of(prob, steps, precision, fused=False):
 def serving_stencil(batch: int):
     """Stencil form of a served handle with ``batch`` field sets, each form
     on the kernels measured fastest for it in the served mix: one field set
-    on the TMA tile form of the fused step (96^3: 1.46x the two-pass
-    kernels; 256^3: equal), several on the batched two-pass kernels (with
-    eight requests resident the tile form's shared memory per CTA limits how
-    many CTAs of different requests share an SM: 5.9 vs 7.7 solves/s on the
-    quarter-scale stream)."""
-    return ("fused", 7) if batch == 1 else None
+    on the slab step (the TMA tile march with the CPML inside it: 0.636
+    solves/s on the full stream against 0.48-0.51 on the tile step),
+    several on the batched two-pass kernels (with eight requests resident
+    the TMA forms' shared memory per CTA limits how many CTAs of different
+    requests share an SM: 10.64 vs 9.98 solves/s on the quarter-scale
+    stream)."""
+    return ("fused", 16) if batch == 1 else None
 
 
 class ServingLoop:

@@ -166,11 +166,11 @@ def test_footprint_estimate_counts_the_big_buffers():
 
 
 def test_each_form_gets_its_stencil_and_a_refusal_keeps_the_default():
-    """Single-excitation handles go on the tile step, batched ones keep the
+    """Single-excitation handles go on the slab step, batched ones keep the
     default kernels; a handle that refuses the form keeps its default."""
     from magnelio_b200._lib import FitbError
 
-    assert serving.serving_stencil(1) == ("fused", 7)
+    assert serving.serving_stencil(1) == ("fused", 16)
     assert serving.serving_stencil(3) is None
 
     class Eng:
@@ -184,10 +184,10 @@ def test_each_form_gets_its_stencil_and_a_refusal_keeps_the_default():
             self.form = (kind, variant)
 
     ok, no = Eng(False), Eng(True)
-    serving.ServingLoop._configure(ok, ("fused", 7))
-    serving.ServingLoop._configure(no, ("fused", 7))
+    serving.ServingLoop._configure(ok, ("fused", 16))
+    serving.ServingLoop._configure(no, ("fused", 16))
     serving.ServingLoop._configure(Eng(False), None)
-    assert ok.form == ("fused", 7) and no.form is None
+    assert ok.form == ("fused", 16) and no.form is None
 
 
 class AsyncEngine(ScriptedEngine):
