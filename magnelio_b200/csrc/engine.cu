@@ -92,6 +92,28 @@ struct DevBuf {
     }
 };
 
+// Page-locked host memory, grown on demand: small device-to-host reads (the
+// V/I of a step and the pipeline status word) land here as one batch of
+// stream-ordered copies behind a single synchronisation.
+struct HostBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    HostBuf() = default;
+    HostBuf(const HostBuf&) = delete;
+    HostBuf& operator=(const HostBuf&) = delete;
+    ~HostBuf() {
+        if (p) cudaFreeHost(p);
+    }
+    void reserve(size_t n) {
+        if (n <= bytes) return;
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        bytes = 0;
+        ck(cudaMallocHost(&p, n), "cudaMallocHost");
+        bytes = n;
+    }
+};
+
 template <typename U>
 void upload(DevBuf& d, const std::vector<U>& v) {
     d.alloc(v.size() * sizeof(U), false);
@@ -237,6 +259,7 @@ struct Handle {
     int fused_variant = 0; // kernel form of the fused step (stencil_fused.cu)
     StreamPlan splan{};
     DevBuf status;
+    HostBuf host_io;  // pinned landing area of fitb_read_vi
     // Compact coefficient storage of the stream kernels (kCoefF16 /
     // kCoefBF16): {aE, bE, aH, bH} as 16-bit [3][vol] with power-of-two
     // scales cs[4 * array + component]; coef_max holds the per-component
@@ -1050,16 +1073,26 @@ cudaGraphExec_t capture(Handle& H, int nsteps, int* launches_per) {
 // Reads (and clears) the device status word of the pipelined stencil
 // kernels; a non-zero value means a bounded shared-memory pipeline wait
 // expired and the step's results are not valid.
-void check_device_status(Handle& H) {
-    if (H.stencil_mode != kModeBulk && !(H.stencil_mode == kModeFused && H.fused_variant >= kFusedTileBase)) return;
-    int st = 0;
-    ck(cudaMemcpyAsync(&st, H.status.p, sizeof(int), cudaMemcpyDeviceToHost, H.stream), "status D2H");
-    ck(cudaStreamSynchronize(H.stream), "status sync");
+// the stencil forms whose copy pipelines record a status word
+bool has_device_status(const Handle& H) {
+    return H.stencil_mode == kModeBulk || (H.stencil_mode == kModeFused && H.fused_variant >= kFusedTileBase);
+}
+
+// error out on a nonzero status word `st` (read after the step), resetting it
+void raise_device_status(Handle& H, int st) {
     if (st != 0) {
         ck(cudaMemsetAsync(H.status.p, 0, sizeof(int), H.stream), "status reset");
         fail(FITB_ERR_CUDA, "a bounded wait in the %s copy pipeline expired (status %d)",
              st == kStatusWaitTimeoutE ? "E-update" : (st == kStatusWaitTimeoutH ? "H-update" : "tile-step"), st);
     }
+}
+
+void check_device_status(Handle& H) {
+    if (!has_device_status(H)) return;
+    int st = 0;
+    ck(cudaMemcpyAsync(&st, H.status.p, sizeof(int), cudaMemcpyDeviceToHost, H.stream), "status D2H");
+    ck(cudaStreamSynchronize(H.stream), "status sync");
+    raise_device_status(H, st);
 }
 
 void check_ready(Handle& H) {
@@ -2559,12 +2592,23 @@ int fitb_read_vi(fitb_handle* h, int32_t b, int64_t step0, int64_t n, double* V,
     if (b < 0 || b >= H.B) fail(FITB_ERR_ARG, "field set %d out of range", b);
     if (step0 < 0 || n < 0 || step0 + n > H.steps_done) fail(FITB_ERR_ARG, "steps [%lld, %lld) not recorded", (long long)step0, (long long)(step0 + n));
     if (H.nch == 0 || n == 0) return FITB_OK;
+    // status word, V and I copied behind the steps on the handle's stream
+    // into pinned memory, one synchronisation, then handed to the caller
+    const size_t off = ((size_t)b * H.cap + step0) * H.nch;
+    const size_t cnt = (size_t)n * H.nch, vb = cnt * sizeof(double);
+    H.host_io.reserve(16 + 2 * vb);
+    int* pst = static_cast<int*>(H.host_io.p);
+    double* pv = reinterpret_cast<double*>(static_cast<char*>(H.host_io.p) + 16);
+    double* pi = pv + cnt;
+    const bool status = fitb::has_device_status(H);
+    *pst = 0;
+    if (status) ck(cudaMemcpyAsync(pst, H.status.p, sizeof(int), cudaMemcpyDeviceToHost, H.stream), "status D2H");
+    if (V) ck(cudaMemcpyAsync(pv, H.recV.as<double>() + off, vb, cudaMemcpyDeviceToHost, H.stream), "read V");
+    if (I) ck(cudaMemcpyAsync(pi, H.recI.as<double>() + off, vb, cudaMemcpyDeviceToHost, H.stream), "read I");
     ck(cudaStreamSynchronize(H.stream), "sync");
-    fitb::check_device_status(H);
-    size_t off = ((size_t)b * H.cap + step0) * H.nch;
-    size_t cnt = (size_t)n * H.nch;
-    if (V) ck(cudaMemcpy(V, H.recV.as<double>() + off, cnt * sizeof(double), cudaMemcpyDeviceToHost), "read V");
-    if (I) ck(cudaMemcpy(I, H.recI.as<double>() + off, cnt * sizeof(double), cudaMemcpyDeviceToHost), "read I");
+    if (status) fitb::raise_device_status(H, *pst);
+    if (V) std::memcpy(V, pv, vb);
+    if (I) std::memcpy(I, pi, vb);
     FITB_CATCH
 }
 
