@@ -24,20 +24,26 @@ __device__ __forceinline__ void atomic_max_nonneg(double* addr, double v) {
     atomicMax(reinterpret_cast<unsigned long long*>(addr), (unsigned long long)__double_as_longlong(v));
 }
 
-// Block-wide sum of `n` per-thread values; result valid in red[m] for all
-// threads after return.  red must hold kMaxModes * 2 doubles; warp partials
-// use wred [32][kMaxModes*2].
-template <int NV>
-__device__ void block_sum(double (&v)[NV], int n, double* red, double (*wred)[NV]) {
+// Block-wide sums of the per-thread partial sums v[m], m < M, into red[m]
+// and, with PAIRS, of v[kMaxModes + m] into red[M + m]; valid in red for all
+// threads after return.  The mode loops are unrolled to kMaxModes with a
+// guard, so that v stays in registers; each value is summed by the same
+// shuffle tree and then in warp order.
+template <bool PAIRS>
+__device__ void block_sum_modes(const double (&v)[2 * kMaxModes], int M, double* red,
+                                double (*wred)[2 * kMaxModes]) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int nwarps = blockDim.x >> 5;
-    for (int m = 0; m < n; ++m) {
-        double x = v[m];
+#pragma unroll
+    for (int q = 0; q < (PAIRS ? 2 : 1) * kMaxModes; ++q) {
+        const int m = q % kMaxModes;
+        if (m >= M) continue;  // uniform over the block
+        double x = v[q];
         for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
-        if (lane == 0) wred[warp][m] = x;
+        if (lane == 0) wred[warp][q < kMaxModes ? m : M + m] = x;
     }
     __syncthreads();
-    if (threadIdx.x < n) {
+    if (threadIdx.x < (PAIRS ? 2 : 1) * M) {
         double acc = 0.0;
         for (int w = 0; w < nwarps; ++w) acc += wred[w][threadIdx.x];
         red[threadIdx.x] = acc;
@@ -125,15 +131,20 @@ __global__ void __launch_bounds__(kPortThreads)
     __shared__ double s_vc[kMaxModes];
 
     // 1. Interior-plane projection V_int_new[m] = sum me_int * (p_m * e_int).
+    //    (The mode loops are unrolled to kMaxModes with a guard so that the
+    //    partial sums stay in registers.)
     double acc[2 * kMaxModes];
+#pragma unroll
     for (int m = 0; m < 2 * kMaxModes; ++m) acc[m] = 0.0;
     for (int p = threadIdx.x; p < ne; p += blockDim.x) {
         const double v = (double)E[d.int_e[p]];
         eint[p] = v;
         const double me = d.me_int[p];
-        for (int m = 0; m < M; ++m) acc[m] += me * (d.vprof[(long long)m * ne + p] * v);
+#pragma unroll
+        for (int m = 0; m < kMaxModes; ++m)
+            if (m < M) acc[m] += me * (d.vprof[(long long)m * ne + p] * v);
     }
-    block_sum<2 * kMaxModes>(acc, M, red, wred);
+    block_sum_modes<false>(acc, M, red, wred);
     if (threadIdx.x < M) s_vint[threadIdx.x] = red[threadIdx.x];
     __syncthreads();
 
@@ -152,10 +163,12 @@ __global__ void __launch_bounds__(kPortThreads)
     }
     __syncthreads();
 
-    // 3. Per-mode boundary value (one thread; scalar float64 recursions).
-    if (threadIdx.x == 0) {
+    // 3. Per-mode boundary value: one thread per mode (the modes' scalar
+    //    float64 recursions are independent of each other).
+    if (threadIdx.x < M) {
         const double* wf = d.wf + (long long)b * d.n_wf;
-        for (int m = 0; m < M; ++m) {
+        {
+            const int m = threadIdx.x;
             const double vin = s_vint[m];
             double vc = Vint_prev[m] + d.mur_r[m] * (vin - Vport_prev[m]);
             if (m == exc && !d.is_dtbc[m]) {
@@ -209,30 +222,34 @@ __global__ void __launch_bounds__(kPortThreads)
     }
     __syncthreads();
 
-    // 5. Recorder samples: V from the corrected port plane, I from h^{n+1/2}.
+    // 5. Recorder samples: V from the corrected port plane, I from h^{n+1/2}
+    //    (the I sums in acc[kMaxModes + m]).
+#pragma unroll
     for (int m = 0; m < 2 * kMaxModes; ++m) acc[m] = 0.0;
     for (int p = threadIdx.x; p < ne; p += blockDim.x) {
         const double v = (double)E[d.port_e[p]];
         const double me = d.me_port[p];
-        for (int m = 0; m < M; ++m) acc[m] += me * (d.vprof[(long long)m * ne + p] * v);
+#pragma unroll
+        for (int m = 0; m < kMaxModes; ++m)
+            if (m < M) acc[m] += me * (d.vprof[(long long)m * ne + p] * v);
     }
     for (int p = threadIdx.x; p < nh; p += blockDim.x) {
         const double v = (double)H[d.port_h[p]];
         const double mh = d.mh_port[p];
-        for (int m = 0; m < M; ++m) acc[M + m] += mh * (d.hprof[(long long)m * nh + p] * v);
+#pragma unroll
+        for (int m = 0; m < kMaxModes; ++m)
+            if (m < M) acc[kMaxModes + m] += mh * (d.hprof[(long long)m * nh + p] * v);
     }
-    block_sum<2 * kMaxModes>(acc, 2 * M, red, wred);
-    if (threadIdx.x == 0) {
-        double amax = 0.0;
-        for (int m = 0; m < M; ++m) {
-            const long long r = ((long long)b * pa.rec.cap + n) * pa.rec.nch + d.channel0 + m;
-            pa.rec.V[r] = red[m] * d.rec_scale[m];
-            pa.rec.I[r] = red[M + m] * d.rec_scale[m];
-            Vport_prev[m] = s_vc[m];
-            Vint_prev[m] = s_vint[m];
-            amax = fmax(amax, fabs(s_vc[m]) * d.rec_scale[m]);
-        }
-        atomic_max_nonneg(pa.absmax + b, amax);
+    block_sum_modes<true>(acc, M, red, wred);
+    if (threadIdx.x < M) {
+        const int m = threadIdx.x;
+        const long long r = ((long long)b * pa.rec.cap + n) * pa.rec.nch + d.channel0 + m;
+        pa.rec.V[r] = red[m] * d.rec_scale[m];
+        pa.rec.I[r] = red[M + m] * d.rec_scale[m];
+        Vport_prev[m] = s_vc[m];
+        Vint_prev[m] = s_vint[m];
+        // fmax drops a NaN as the serial max over the modes did
+        atomic_max_nonneg(pa.absmax + b, fmax(0.0, fabs(s_vc[m]) * d.rec_scale[m]));
     }
 }
 
