@@ -87,9 +87,6 @@ struct StencilArgs {
     int coef_kind;
     const unsigned short* cq[4];
     float cs[16];
-    // slab step: write E_new, H_new and psi_next with evict-first stores
-    // (st.global.cs; none of them is read again within the step)
-    int store_cs;
 };
 
 constexpr int kCoefNative = 0, kCoefF16 = 1, kCoefBF16 = 2;

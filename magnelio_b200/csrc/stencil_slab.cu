@@ -72,15 +72,6 @@ struct Slot {
     const unsigned char* air;  // [4][slab]
 };
 
-// a store of the step's output: evict-first when `cs`
-template <typename T>
-__device__ __forceinline__ void put(T* q, T v, bool cs) {
-    if (cs)
-        __stcs(q, v);
-    else
-        *q = v;
-}
-
 template <typename T, int TJ, int NS, int NSLOT, bool AIR, int CK>
 struct SlabGeo {
     static constexpr int EK = TK + 4, ER = TJ + 1;  // E, alpha_E, beta_E boxes
@@ -117,7 +108,7 @@ struct SlabGeo {
 template <typename T, int TJ, int NS, int NSLOT, bool AIR, int CK>
 __device__ __forceinline__ void slab_E(const Slot<T>* sl, const unsigned char* st, int r, int c, int i, int j, int k,
                                        T hx, T hy, T hz, T hz_jm, T hx_jm, T hy_km, T hx_km, T hz_im, T hy_im, T bx,
-                                       T by, T bz, T& ex, T& ey, T& ez, bool store, bool cs) {
+                                       T by, T bz, T& ex, T& ey, T& ez, bool store) {
     using G = SlabGeo<T, TJ, NS, NSLOT, AIR, CK>;
 #pragma unroll
     for (int s = 0; s < NSLOT; ++s) {
@@ -144,8 +135,8 @@ __device__ __forceinline__ void slab_E(const Slot<T>* sl, const unsigned char* s
         if (store) {
             const long long o =
                 ((long long)(a == 0 ? l : i) * f.dJ + (a == 1 ? l : j)) * f.pk + (a == 2 ? l : k);
-            put(f.psin + o, p1, cs);
-            put(f.psin + f.slab + o, p2, cs);
+            f.psin[o] = p1;
+            f.psin[f.slab + o] = p2;
         }
         if (a == 0) {
             ey = ey + by * (cck * d1 + p1);
@@ -167,7 +158,7 @@ __device__ __forceinline__ void slab_E(const Slot<T>* sl, const unsigned char* s
 template <typename T, int TJ, int NS, int NSLOT, bool AIR, int CK, bool EDGE>
 __device__ __forceinline__ void slab_H(const Slot<T>* sl, const unsigned char* stp, int r, int c, int i, int j, int k,
                                        T ex, T ey, T ez, T ez_jp, T ex_jp, T ey_kp, T ex_kp, T ez_ip, T ey_ip, T bx,
-                                       T by, T bz, T& hx, T& hy, T& hz, bool cs) {
+                                       T by, T bz, T& hx, T& hy, T& hz) {
     using G = SlabGeo<T, TJ, NS, NSLOT, AIR, CK>;
 #pragma unroll
     for (int s = 0; s < NSLOT; ++s) {
@@ -207,8 +198,8 @@ __device__ __forceinline__ void slab_H(const Slot<T>* sl, const unsigned char* s
         T p2 = s2 * cb;
         p2 = p2 + cc * d2;
         if (!air2) p2 = T(0);
-        put(f.psin + 2 * f.slab + o, p1, cs);
-        put(f.psin + 3 * f.slab + o, p2, cs);
+        f.psin[2 * f.slab + o] = p1;
+        f.psin[3 * f.slab + o] = p2;
         if (a == 0) {
             hy = hy - by * (cck * d1 + p1);
             hz = hz + bz * (cck * d2 + p2);
@@ -271,16 +262,16 @@ __device__ __forceinline__ void step_E(const StencilArgs<T>& p, const Slot<T>* s
     T ez = az * E[2 * G::cE + ie] + bz * cz;
     if constexpr (NSLOT > 0)
         slab_E<T, TJ, NS, NSLOT, AIR, CK>(sl, st, r, c, i, j, k, hx, hy, hz, hz_jm, hx_jm, hy_km, hx_km, hz_im, hy_im, bx,
-                                      by, bz, ex, ey, ez, store, p.store_cs);
+                                      by, bz, ex, ey, ez, store);
     const int in = r * G::NK + c;
     en[in] = ex;
     en[G::cN + in] = ey;
     en[2 * G::cN + in] = ez;
     if (store) {
         const long long o = pidx(g, i, j, k), vol = g.vol;
-        put(Eg + o, ex, p.store_cs);
-        put(Eg + vol + o, ey, p.store_cs);
-        put(Eg + 2 * vol + o, ez, p.store_cs);
+        Eg[o] = ex;
+        Eg[vol + o] = ey;
+        Eg[2 * vol + o] = ez;
     }
 }
 
@@ -329,10 +320,10 @@ __device__ __forceinline__ void step_H(const StencilArgs<T>& p, const Slot<T>* s
     T hz = ch.az * Hs[2 * G::cH + ih] - ch.bz * cz;
     if constexpr (NSLOT > 0)
         slab_H<T, TJ, NS, NSLOT, AIR, CK, EDGE>(sl, stp, r, c, i, j, k, ex, ey, ez, ez_jp, ex_jp, ey_kp, ex_kp, ez_ip,
-                                            ey_ip, ch.bx, ch.by, ch.bz, hx, hy, hz, p.store_cs);
-    put(Hg + o, hx, p.store_cs);
-    put(Hg + vol + o, hy, p.store_cs);
-    put(Hg + 2 * vol + o, hz, p.store_cs);
+                                            ey_ip, ch.bx, ch.by, ch.bz, hx, hy, hz);
+    Hg[o] = hx;
+    Hg[vol + o] = hy;
+    Hg[2 * vol + o] = hz;
 }
 
 // Units: x = k tile, y = j tile, z = i chunk, w = the face of slot s in bits
@@ -695,33 +686,13 @@ struct SlabLaunch {
     bool air;
     int* status;
     const cudaStream_t* streams;  // one per list
-    int cluster;                  // CTAs per thread-block cluster (1: none)
     int launched = 0;
     template <int NSLOT, bool AIR, int CK, int TJ, int NS>
     void go(int q) {
         if (n_units[q] <= 0) return;
-        const unsigned grid = (unsigned)n_units[q] * a.B;
-        const size_t smem = SlabGeo<T, TJ, NS, NSLOT, AIR, CK>::smem;
-        if (cluster > 1 && grid % cluster == 0) {
-            // consecutive CTAs (the field sets of one unit, then neighbouring
-            // units) in one cluster: co-scheduled on one GPC, so the boxes
-            // they share are fetched once into the L2 next to it
-            cudaLaunchConfig_t cfg{};
-            cfg.gridDim = dim3(grid);
-            cfg.blockDim = dim3(32 * (TJ + 1));
-            cfg.dynamicSmemBytes = smem;
-            cfg.stream = streams[q];
-            cudaLaunchAttribute at[1];
-            at[0].id = cudaLaunchAttributeClusterDimension;
-            at[0].val.clusterDim.x = (unsigned)cluster;
-            at[0].val.clusterDim.y = 1;
-            at[0].val.clusterDim.z = 1;
-            cfg.attrs = at;
-            cfg.numAttrs = 1;
-            cudaLaunchKernelEx(&cfg, k_step_slab<T, TJ, NS, NSLOT, AIR, CK>, m, a, units[q], status);
-        } else {
-            k_step_slab<T, TJ, NS, NSLOT, AIR, CK><<<dim3(grid), 32 * (TJ + 1), smem, streams[q]>>>(m, a, units[q], status);
-        }
+        k_step_slab<T, TJ, NS, NSLOT, AIR, CK>
+            <<<dim3((unsigned)n_units[q] * a.B), 32 * (TJ + 1), SlabGeo<T, TJ, NS, NSLOT, AIR, CK>::smem,
+               streams[q]>>>(m, a, units[q], status);
         ++launched;
     }
     template <int CK, int TJ, int NS, int NSC>
@@ -975,28 +946,7 @@ int launch_slab_step(StencilArgs<T> a, int ichunk, int variant, const int4* cons
             return -2;
     }
     a.ichunk = ichunk;
-    // evict-first output stores when FITB_SLAB_STORE_CS=1 (read once per
-    // process; a tuning switch, both values compute the same bits)
-    static const int store_cs = [] {
-        const char* e = std::getenv("FITB_SLAB_STORE_CS");
-        return e ? std::atoi(e) : 0;
-    }();
-    a.store_cs = store_cs;
-    // thread-block clusters of FITB_SLAB_CLUSTER units (default 1) times the
-    // field sets of a unit, at most 8 CTAs; 0: no clusters (read once per
-    // process; a tuning switch, every value computes the same bits)
-    static const int cluster_units = [] {
-        const char* e = std::getenv("FITB_SLAB_CLUSTER");
-        return e ? std::max(0, std::atoi(e)) : 1;
-    }();
-    int cluster = 1;
-    if (cluster_units > 0) {
-        if ((long long)cluster_units * a.B <= 8)
-            cluster = cluster_units * a.B;
-        else if (a.B <= 8)
-            cluster = a.B;
-    }
-    SlabLaunch<T> l{m, a, units, n_units, air, status, streams, cluster};
+    SlabLaunch<T> l{m, a, units, n_units, air, status, streams};
     slab_dispatch(variant, l);
     return l.launched;
 }

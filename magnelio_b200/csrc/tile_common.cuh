@@ -80,17 +80,20 @@ inline PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
     return fn;
 }
 
-// L2 fill size of the tensor copies' misses: 256 bytes unless the
-// environment variable FITB_TMA_L2_PROMOTION says none, 64 or 128 (read once
-// per process; a tuning switch, every value computes the same bits).
+// L2 fill size of the tensor copies' misses: none (the sectors a box
+// touches) unless the environment variable FITB_TMA_L2_PROMOTION says 64,
+// 128 or 256 (read once per process; a tuning switch, every value computes
+// the same bits).  Measured on the 256^3 slab step: 256-byte fills read
+// 966 MB per step from DRAM in the CPML-free list against 901 MB without,
+// and the step took 4 % longer.
 inline CUtensorMapL2promotion l2_promotion() {
     static const CUtensorMapL2promotion v = [] {
         const char* e = std::getenv("FITB_TMA_L2_PROMOTION");
-        if (!e) return CU_TENSOR_MAP_L2_PROMOTION_L2_256B;
-        if (!std::strcmp(e, "none")) return CU_TENSOR_MAP_L2_PROMOTION_NONE;
+        if (!e) return CU_TENSOR_MAP_L2_PROMOTION_NONE;
         if (!std::strcmp(e, "64")) return CU_TENSOR_MAP_L2_PROMOTION_L2_64B;
         if (!std::strcmp(e, "128")) return CU_TENSOR_MAP_L2_PROMOTION_L2_128B;
-        return CU_TENSOR_MAP_L2_PROMOTION_L2_256B;
+        if (!std::strcmp(e, "256")) return CU_TENSOR_MAP_L2_PROMOTION_L2_256B;
+        return CU_TENSOR_MAP_L2_PROMOTION_NONE;
     }();
     return v;
 }
