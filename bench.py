@@ -593,7 +593,8 @@ def run_slab(args, world, rank, local):
 
 
 SWEEP_CANDIDATES = (("stream", 0, 0), ("fused", 7, 0), ("fused", 16, 0), ("fused", 17, 0), ("fused", 18, 0),
-                    ("fused", 19, 0), ("fused", 20, 0), ("fused", 21, 0), ("fused", 22, 0), ("fused", 23, 0))
+                    ("fused", 19, 0), ("fused", 20, 0), ("fused", 21, 0), ("fused", 22, 0), ("fused", 23, 0),
+                    ("fused", 24, 0), ("fused", 25, 0))
 
 
 def sweep_point(n: int, args, local: int) -> dict:

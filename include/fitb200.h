@@ -200,11 +200,15 @@ int fitb_set_coeff_storage(fitb_handle* h, int32_t kind);
  * are fixed): kind FITB_STENCIL_SIMPLE / STREAM / BULK / VEC / FUSED, a
  * variant of that form (vec 0-3; fused 0-6 the register / cp.async forms,
  * fused 7-15 the TMA tile form with its CPML slab passes, tile shapes of
- * 2-16 rows x 32 cells and 3-5 ring stages; fused 16-23 the slab step, the
- * TMA tile march with the CPML inside it, tiles of 4, 2, 3, 4, 3, 2, 8, 6
- * rows x 32 cells with 3, 3, 3, 4, 4, 4, 3, 3 ring stages (variants 22 and
- * 23 float32 only: their six-slot instances exceed the shared memory of a
- * CTA in float64); FITB_ERR_ARG for a form the handle's
+ * 2-16 rows x 32 cells and 3-5 ring stages; fused 16-25 the slab step, the
+ * TMA tile march with the CPML inside it, tiles of 4, 2, 3, 4, 3, 2, 8, 6,
+ * 4, 4 rows x 32 cells with 3, 3, 3, 4, 4, 4, 3, 3, 3, 3 ring stages, one
+ * field set per CTA except 24 and 25, which march 2 and 4 field sets per
+ * CTA through shared coefficient boxes (the batch a multiple of that);
+ * 22 and 25 are float32 only (their shared memory exceeds a CTA's in
+ * float64), and grids whose units reach both faces of an axis refuse the
+ * forms without a six-slot kernel (25; 23 and 24 in float64);
+ * FITB_ERR_ARG for a form the handle's
  * precision, dispersion or CPML layout does not take), and the number of i
  * planes one CTA marches (0: the form's own plan).  The fields, psi and all
  * other state carry over; valid between steps.
@@ -217,7 +221,7 @@ int fitb_set_coeff_storage(fitb_handle* h, int32_t kind);
 #define FITB_STENCIL_FUSED 4
 int fitb_configure_stencil(fitb_handle* h, int32_t kind, int32_t variant, int32_t ichunk);
 int fitb_get_stencil(fitb_handle* h, int32_t* out);
-/* Work units of the slab step (fused 16-23): out[0..4] the units launched
+/* Work units of the slab step (fused 16-25): out[0..4] the units launched
  * with 0, 1, 2, 3 and up to 6 CPML face slots, out[5] the units left out as
  * dead (every E edge frozen at zero, every H face a no-op or curl-dead; the
  * reference's tile skip, solver/_tile_skip.py:187, which this follows,

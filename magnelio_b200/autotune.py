@@ -50,9 +50,11 @@ DEFAULT_CANDIDATES = (
     ("fused", 21, 0),
     ("fused", 22, 0),
     ("fused", 23, 0),
+    ("fused", 24, 0),
+    ("fused", 25, 0),
     ("bulk", 0, 0),
 )
-CANDIDATE_SET = 5  # bump when the candidates change: cached results of another set are not reused
+CANDIDATE_SET = 6  # bump when the candidates change: cached results of another set are not reused
 
 
 @dataclass

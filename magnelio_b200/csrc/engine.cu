@@ -664,7 +664,13 @@ bool slab_units_of(const Handle& H, int variant, int ichunk, std::vector<int4> o
     const int nf = (int)H.faces.size();
     if (nf > kMaxFaces) return false;
     for (int q = 0; q < nf; ++q) f[q] = H.faces[q]->dev;
-    return plan_slab_units(H.g, f, nf, slab_tj_of(variant - kFusedSlabBase), ichunk, out);
+    const int v = variant - kFusedSlabBase;
+    if (H.B % slab_nb_of(v) != 0) return false;
+    if (!plan_slab_units(H.g, f, nf, slab_tj_of(v), ichunk, out)) return false;
+    // units reaching both faces of an axis need the six-slot instance
+    bool air = false;
+    for (auto& fh : H.faces) air = air || fh->pec;
+    return out[4].empty() || (H.prec == 4 ? slab_six_ok<float>(v, air) : slab_six_ok<double>(v, air));
 }
 
 // Dead-unit skipping of the slab step (reference: solver/_tile_skip.py,
@@ -844,6 +850,7 @@ int launch_fused(Handle& H, const StencilArgs<T>& sa) {
         }
         const int n = launch_slab_step<T>(sa, H.splan.ichunk, H.fused_variant - kFusedSlabBase, units,
                                           H.n_slab_units, air, H.status.as<int>(), streams);
+        if (n == -4) fail(FITB_ERR_STATE, "the slab step variant has no kernel for this batch / unit list");
         if (n < 0) fail(FITB_ERR_CUDA, "tensor maps of the slab step could not be encoded");
         for (int q = 1; q < kSlabLists; ++q) {
             if (H.n_slab_units[q] <= 0) continue;
@@ -1521,7 +1528,10 @@ int fitb_create(const fitb_desc* desc, fitb_handle** out) {
             const char* t = getenv("FITB_FUSED_VARIANT");
             H.fused_variant = t ? std::max(0, std::min(fitb::kFusedSlabBase + fitb::kSlabVariants - 1, atoi(t))) : 2;
             if (H.fused_variant == 1 && H.prec == 8) H.fused_variant = 0;
-            if (!fitb::fused_variant_ok(H.prec, H.fused_variant)) H.fused_variant = 2;
+            if (!fitb::fused_variant_ok(H.prec, H.fused_variant) ||
+                (fitb::is_slab_variant(H.fused_variant) &&
+                 H.B % fitb::slab_nb_of(H.fused_variant - fitb::kFusedSlabBase) != 0))
+                H.fused_variant = 2;
             ck(fitb::prepare_fused_any(H.prec, H.fused_variant), "fused step smem attribute");
             H.e2.alloc(blk * H.B);
             H.h2.alloc(blk * H.B);
@@ -1735,13 +1745,16 @@ int fitb_configure_stencil(fitb_handle* h, int32_t kind, int32_t variant, int32_
         if (!fitb::fused_variant_ok(H.prec, variant)) fail(FITB_ERR_ARG, "fused variant %d", variant);
         if ((H.disp[0].present() || H.disp[1].present()) && !fitb::is_slab_variant(variant))
             fail(FITB_ERR_STATE,
-                 "dispersive materials need an in-place stencil mode or the slab step (fused 16-23)");
+                 "dispersive materials need an in-place stencil mode or the slab step (fused 16-25)");
         if ((H.disp[0].present() || H.disp[1].present()) && !fitb::disp_clear_of_cpml(H))
             fail(FITB_ERR_STATE, "the slab step takes dispersive materials only outside the CPML slabs");
         if (fitb::is_tile_variant(variant) &&
             !(H.prec == 4 ? fitb::tile_step_fits<float>(fitb::stencil_args<float>(H))
                           : fitb::tile_step_fits<double>(fitb::stencil_args<double>(H))))
             fail(FITB_ERR_ARG, "the tile step does not take this grid / CPML layout");
+        if (fitb::is_slab_variant(variant) && H.B % fitb::slab_nb_of(variant - fitb::kFusedSlabBase) != 0)
+            fail(FITB_ERR_ARG, "fused variant %d marches %d field sets per CTA: the batch of %d is not a multiple",
+                 variant, fitb::slab_nb_of(variant - fitb::kFusedSlabBase), H.B);
         if (fitb::is_slab_variant(variant)) {
             // any march depth the planner may pick: check the deepest and the shallowest
             std::vector<int4> lists[fitb::kSlabLists];
@@ -2168,7 +2181,7 @@ int fitb_add_dispersion_block(fitb_handle* h, int32_t side, int64_t n_states, co
         fail(FITB_ERR_ARG, "dispersion block needs states, poles and all arrays");
     if (H.steps_done != 0) fail(FITB_ERR_STATE, "dispersion must be added before the first step");
     if (H.stencil_mode == fitb::kModeFused && !fitb::is_slab_variant(H.fused_variant))
-        fail(FITB_ERR_STATE, "dispersive materials need an in-place stencil mode or the slab step (fused 16-23)");
+        fail(FITB_ERR_STATE, "dispersive materials need an in-place stencil mode or the slab step (fused 16-25)");
     fitb::DispHost& D = H.disp[side];
     const int blk = (int)D.pole_start.size() - 1;
     for (int q = 0; q < n_poles; ++q) {

@@ -173,11 +173,15 @@ int launch_tile_cpml_H(const StencilArgs<T>& a, cudaStream_t s);
 // face slots; fused-step variants kFusedSlabBase + v with (tile rows, ring
 // stages of the CPML-free list, of the CPML lists) = (4, 3, 3), (2, 3, 3),
 // (3, 3, 3), (4, 4, 4), (3, 4, 4), (2, 4, 4), (8, 3, 3), (6, 3, 3) for
-// v = 0..7.
-constexpr int kFusedSlabBase = kFusedTileBase + kTileVariants, kSlabVariants = 8;
+// v = 0..7, one field set per CTA; v = 8, 9: (4, 3, 3) with 2 and 4 field
+// sets per CTA sharing the coefficient boxes.
+constexpr int kFusedSlabBase = kFusedTileBase + kTileVariants, kSlabVariants = 10;
 inline bool is_tile_variant(int v) { return v >= kFusedTileBase && v < kFusedSlabBase; }
 inline bool is_slab_variant(int v) { return v >= kFusedSlabBase && v < kFusedSlabBase + kSlabVariants; }
 int slab_tj_of(int variant);
+int slab_nb_of(int variant);  // field sets per CTA
+template <typename T>
+bool slab_six_ok(int variant, bool air);  // the six-slot instance exists
 template <typename T>
 bool slab_supported(int variant);
 template <typename T>

@@ -72,7 +72,7 @@ struct Slot {
     const unsigned char* air;  // [4][slab]
 };
 
-template <typename T, int TJ, int NS, int NSLOT, bool AIR, int CK>
+template <typename T, int TJ, int NS, int NSLOT, bool AIR, int CK, int NB>
 struct SlabGeo {
     static constexpr int EK = TK + 4, ER = TJ + 1;  // E, alpha_E, beta_E boxes
     static constexpr int HK = TK + 8, HR = TJ + 2;  // H box
@@ -84,17 +84,21 @@ struct SlabGeo {
     static constexpr int CB = CK == kCoefNative ? (int)sizeof(T) : 2;
     static constexpr int EKc = CK == kCoefNative ? EK : 40, cCE = ER * EKc;
     static constexpr size_t al(size_t b) { return (b + 127) / 128 * 128; }
-    static constexpr unsigned bytesE = 3u * cE * sizeof(T), bytesH = 3u * cH * sizeof(T),
-                              bytesCE = 3u * cCE * CB, bytesC = 3u * cC * CB;
-    static constexpr unsigned bytesPE = 2u * cPE * sizeof(T), bytesPH = 2u * cPH * sizeof(T), bytesAE = 2u * cAE,
-                              bytesAH = 2u * cAH;
+    // E and H boxes of the NB field sets one after the other (one copy of
+    // 3 NB components each), psi boxes per field set; the coefficient and
+    // air-mask boxes once for all of them
+    static constexpr unsigned setE = 3u * cE * sizeof(T), setH = 3u * cH * sizeof(T);
+    static constexpr unsigned setPE = 2u * cPE * sizeof(T), setPH = 2u * cPH * sizeof(T);
+    static constexpr unsigned bytesE = NB * setE, bytesH = NB * setH, bytesCE = 3u * cCE * CB, bytesC = 3u * cC * CB;
+    static constexpr unsigned bytesPE = NB * setPE, bytesPH = NB * setPH, bytesAE = 2u * cAE, bytesAH = 2u * cAH;
     static constexpr size_t oE = 0, oH = al(bytesE), oaE = oH + al(bytesH), obE = oaE + al(bytesCE),
                             oaH = obE + al(bytesCE), obH = oaH + al(bytesC), oS = obH + al(bytesC);
     // within a slot: psi_E, psi_H, air_E, air_H
     static constexpr size_t sPE = 0, sPH = al(bytesPE), sAE = sPH + al(bytesPH),
                             sAH = sAE + (AIR ? al(bytesAE) : 0), slot = sAH + (AIR ? al(bytesAH) : 0);
     static constexpr size_t stage = oS + NSLOT * slot;
-    static constexpr size_t oN = NS * stage, oSl = oN + al(3u * 3u * cN * sizeof(T));
+    // E_new ring: 3 planes x NB field sets x 3 components
+    static constexpr size_t oN = NS * stage, oSl = oN + al(3u * NB * 3u * cN * sizeof(T));
     static constexpr size_t oBar = oSl + al((NSLOT > 0 ? NSLOT : 1) * sizeof(Slot<T>));
     static constexpr size_t smem = oBar + 2 * NS * sizeof(unsigned long long) + 4 * sizeof(int);
     // resident CTAs per SM that the shared memory allows (launch bound)
@@ -105,11 +109,12 @@ struct SlabGeo {
 };
 
 // CPML of E_new of cell (r, c) of the tile region at plane i (cpml.py:343-430).
-template <typename T, int TJ, int NS, int NSLOT, bool AIR, int CK>
-__device__ __forceinline__ void slab_E(const Slot<T>* sl, const unsigned char* st, int r, int c, int i, int j, int k,
+template <typename T, int TJ, int NS, int NSLOT, bool AIR, int CK, int NB>
+__device__ __forceinline__ void slab_E(const Slot<T>* sl, const unsigned char* st, int sb, int r, int c, int i, int j,
+                                       int k,
                                        T hx, T hy, T hz, T hz_jm, T hx_jm, T hy_km, T hx_km, T hz_im, T hy_im, T bx,
                                        T by, T bz, T& ex, T& ey, T& ez, bool store) {
-    using G = SlabGeo<T, TJ, NS, NSLOT, AIR, CK>;
+    using G = SlabGeo<T, TJ, NS, NSLOT, AIR, CK, NB>;
 #pragma unroll
     for (int s = 0; s < NSLOT; ++s) {
         const Slot<T>& f = sl[s];
@@ -117,7 +122,7 @@ __device__ __forceinline__ void slab_E(const Slot<T>* sl, const unsigned char* s
         const int l = (a == 0 ? i : (a == 1 ? j : k)) - f.lo;
         if ((unsigned)l >= (unsigned)f.n) continue;
         const unsigned char* ss = st + G::oS + s * G::slot;
-        const T* ps = reinterpret_cast<const T*>(ss + G::sPE);
+        const T* ps = reinterpret_cast<const T*>(ss + G::sPE + sb * G::setPE);
         const int q = r * PW + c + f.co;
         const T cb = __ldg(f.bcc + l), cc = __ldg(f.bcc + f.n + l), cck = __ldg(f.bcc + 2 * f.n + l);
         const T d1 = a == 0 ? hz - hz_im : (a == 1 ? hz - hz_jm : hy - hy_km);
@@ -135,8 +140,9 @@ __device__ __forceinline__ void slab_E(const Slot<T>* sl, const unsigned char* s
         if (store) {
             const long long o =
                 ((long long)(a == 0 ? l : i) * f.dJ + (a == 1 ? l : j)) * f.pk + (a == 2 ? l : k);
-            f.psin[o] = p1;
-            f.psin[f.slab + o] = p2;
+            T* pn = f.psin + sb * 4 * f.slab;
+            pn[o] = p1;
+            pn[f.slab + o] = p2;
         }
         if (a == 0) {
             ey = ey + by * (cck * d1 + p1);
@@ -155,11 +161,12 @@ __device__ __forceinline__ void slab_E(const Slot<T>* sl, const unsigned char* s
 // 2 and 3.  EDGE: a cell outside the staged tile rows / columns (the last
 // row j = ny or column k = nz absorbed by this tile); its psi and air come
 // from global memory.
-template <typename T, int TJ, int NS, int NSLOT, bool AIR, int CK, bool EDGE>
-__device__ __forceinline__ void slab_H(const Slot<T>* sl, const unsigned char* stp, int r, int c, int i, int j, int k,
+template <typename T, int TJ, int NS, int NSLOT, bool AIR, int CK, int NB, bool EDGE>
+__device__ __forceinline__ void slab_H(const Slot<T>* sl, const unsigned char* stp, int sb, int r, int c, int i, int j,
+                                       int k,
                                        T ex, T ey, T ez, T ez_jp, T ex_jp, T ey_kp, T ex_kp, T ez_ip, T ey_ip, T bx,
                                        T by, T bz, T& hx, T& hy, T& hz) {
-    using G = SlabGeo<T, TJ, NS, NSLOT, AIR, CK>;
+    using G = SlabGeo<T, TJ, NS, NSLOT, AIR, CK, NB>;
 #pragma unroll
     for (int s = 0; s < NSLOT; ++s) {
         const Slot<T>& f = sl[s];
@@ -173,15 +180,16 @@ __device__ __forceinline__ void slab_H(const Slot<T>* sl, const unsigned char* s
         T s1, s2;
         bool air1 = true, air2 = true;
         if constexpr (EDGE) {
-            s1 = f.psi[2 * f.slab + o];
-            s2 = f.psi[3 * f.slab + o];
+            const T* po = f.psi + sb * 4 * f.slab;
+            s1 = po[2 * f.slab + o];
+            s2 = po[3 * f.slab + o];
             if constexpr (AIR) {
                 air1 = f.air[2 * f.slab + o] != 0;
                 air2 = f.air[3 * f.slab + o] != 0;
             }
         } else {
             const unsigned char* ss = stp + G::oS + s * G::slot;
-            const T* ps = reinterpret_cast<const T*>(ss + G::sPH);
+            const T* ps = reinterpret_cast<const T*>(ss + G::sPH + sb * G::setPH);
             const int q = r * PW + c + f.co;
             s1 = ps[q];
             s2 = ps[G::cPH + q];
@@ -198,8 +206,9 @@ __device__ __forceinline__ void slab_H(const Slot<T>* sl, const unsigned char* s
         T p2 = s2 * cb;
         p2 = p2 + cc * d2;
         if (!air2) p2 = T(0);
-        f.psin[2 * f.slab + o] = p1;
-        f.psin[3 * f.slab + o] = p2;
+        T* pn = f.psin + sb * 4 * f.slab;
+        pn[2 * f.slab + o] = p1;
+        pn[3 * f.slab + o] = p2;
         if (a == 0) {
             hy = hy - by * (cck * d1 + p1);
             hz = hz + bz * (cck * d2 + p2);
@@ -235,15 +244,15 @@ __device__ __forceinline__ void coef3(const unsigned char* box, int stride, int 
 
 // E_new of cell (r, c) of the tile region (r <= TJ, c <= TK) at plane i,
 // CPML-corrected; stored to global memory (with psi_next) when `store`.
-template <typename T, int TJ, int NS, int NSLOT, bool AIR, int CK>
+template <typename T, int TJ, int NS, int NSLOT, bool AIR, int CK, int NB>
 __device__ __forceinline__ void step_E(const StencilArgs<T>& p, const Slot<T>* sl, const unsigned char* st,
-                                       const unsigned char* stp, T* en, int r, int c, int i, int j, int k, bool store,
-                                       T* __restrict__ Eg) {
-    using G = SlabGeo<T, TJ, NS, NSLOT, AIR, CK>;
+                                       const unsigned char* stp, int sb, T* en, int r, int c, int i, int j, int k,
+                                       bool store, T* __restrict__ Eg) {
+    using G = SlabGeo<T, TJ, NS, NSLOT, AIR, CK, NB>;
     const Geom& g = p.g;
-    const T* E = reinterpret_cast<const T*>(st + G::oE);
-    const T* Hs = reinterpret_cast<const T*>(st + G::oH);
-    const T* Hp = reinterpret_cast<const T*>(stp + G::oH);
+    const T* E = reinterpret_cast<const T*>(st + G::oE + sb * G::setE);
+    const T* Hs = reinterpret_cast<const T*>(st + G::oH + sb * G::setH);
+    const T* Hp = reinterpret_cast<const T*>(stp + G::oH + sb * G::setH);
     const int ie = r * G::EK + c;
     const int ic = r * G::EKc + c;
     const int ih = (r + 1) * G::HK + c + 4;
@@ -261,8 +270,8 @@ __device__ __forceinline__ void step_E(const StencilArgs<T>& p, const Slot<T>* s
     T ey = ay * E[G::cE + ie] + by * cy;
     T ez = az * E[2 * G::cE + ie] + bz * cz;
     if constexpr (NSLOT > 0)
-        slab_E<T, TJ, NS, NSLOT, AIR, CK>(sl, st, r, c, i, j, k, hx, hy, hz, hz_jm, hx_jm, hy_km, hx_km, hz_im, hy_im, bx,
-                                      by, bz, ex, ey, ez, store);
+        slab_E<T, TJ, NS, NSLOT, AIR, CK, NB>(sl, st, sb, r, c, i, j, k, hx, hy, hz, hz_jm, hx_jm, hy_km, hx_km, hz_im,
+                                              hy_im, bx, by, bz, ex, ey, ez, store);
     const int in = r * G::NK + c;
     en[in] = ex;
     en[G::cN + in] = ey;
@@ -279,12 +288,12 @@ __device__ __forceinline__ void step_E(const StencilArgs<T>& p, const Slot<T>* s
 // the stage of plane i, CPML-corrected.  EDGE: a halo cell this tile owns
 // (last row j = ny or last column k = nz): E_new beyond the padded edge is
 // zero and its coefficients, psi and air come from global memory.
-template <typename T, int TJ, int NS, int NSLOT, bool AIR, int CK, bool EDGE>
-__device__ __forceinline__ void step_H(const StencilArgs<T>& p, const Slot<T>* sl, const unsigned char* stp,
+template <typename T, int TJ, int NS, int NSLOT, bool AIR, int CK, int NB, bool EDGE>
+__device__ __forceinline__ void step_H(const StencilArgs<T>& p, const Slot<T>* sl, const unsigned char* stp, int sb,
                                        const T* enp, const T* enc, int r, int c, int i, int j, int k,
                                        T* __restrict__ Hg) {
-    using G = SlabGeo<T, TJ, NS, NSLOT, AIR, CK>;
-    const T* Hs = reinterpret_cast<const T*>(stp + G::oH);
+    using G = SlabGeo<T, TJ, NS, NSLOT, AIR, CK, NB>;
+    const T* Hs = reinterpret_cast<const T*>(stp + G::oH + sb * G::setH);
     const int in = r * G::NK + c;
     const T ex = enp[in], ey = enp[G::cN + in], ez = enp[2 * G::cN + in];
     const T ez_jp = (!EDGE || r < TJ) ? enp[2 * G::cN + in + G::NK] : T(0);
@@ -319,28 +328,31 @@ __device__ __forceinline__ void step_H(const StencilArgs<T>& p, const Slot<T>* s
     T hy = ch.ay * Hs[G::cH + ih] - ch.by * cy;
     T hz = ch.az * Hs[2 * G::cH + ih] - ch.bz * cz;
     if constexpr (NSLOT > 0)
-        slab_H<T, TJ, NS, NSLOT, AIR, CK, EDGE>(sl, stp, r, c, i, j, k, ex, ey, ez, ez_jp, ex_jp, ey_kp, ex_kp, ez_ip,
-                                            ey_ip, ch.bx, ch.by, ch.bz, hx, hy, hz);
+        slab_H<T, TJ, NS, NSLOT, AIR, CK, NB, EDGE>(sl, stp, sb, r, c, i, j, k, ex, ey, ez, ez_jp, ex_jp, ey_kp, ex_kp,
+                                                    ez_ip, ey_ip, ch.bx, ch.by, ch.bz, hx, hy, hz);
     Hg[o] = hx;
     Hg[vol + o] = hy;
     Hg[2 * vol + o] = hz;
 }
 
 // Units: x = k tile, y = j tile, z = i chunk, w = the face of slot s in bits
-// 4s .. 4s+3.  blockIdx.x = unit * B + field set.
-template <typename T, int TJ, int NS, int NSLOT, bool AIR, int CK>
-__global__ void __launch_bounds__(32 * (TJ + 1), SlabGeo<T, TJ, NS, NSLOT, AIR, CK>::minb())
+// 4s .. 4s+3.  A CTA marches NB field sets b0 .. b0+NB-1 of its unit through
+// the same coefficient boxes (each compute thread updates its cell in every
+// set in turn); blockIdx.x = unit * (B / NB) + b0 / NB.
+template <typename T, int TJ, int NS, int NSLOT, bool AIR, int CK, int NB>
+__global__ void __launch_bounds__(32 * (TJ + 1), SlabGeo<T, TJ, NS, NSLOT, AIR, CK, NB>::minb())
     k_step_slab(const __grid_constant__ SlabMaps maps, const StencilArgs<T> p, const int4* __restrict__ units,
                 int* status) {
-    using G = SlabGeo<T, TJ, NS, NSLOT, AIR, CK>;
+    using G = SlabGeo<T, TJ, NS, NSLOT, AIR, CK, NB>;
     constexpr int NC = 32 * TJ;      // compute threads
     constexpr int NX = TK + 1 + TJ;  // halo cells (row TJ, then column TK)
     static_assert(NX <= NC, "tile shape");
     extern __shared__ __align__(128) unsigned char smem[];
     const Geom& g = p.g;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int b = blockIdx.x % p.B;
-    const int4 u = units[blockIdx.x / p.B];
+    const int ng = p.B / NB;  // field-set groups
+    const int b = (blockIdx.x % ng) * NB;  // first field set of the CTA
+    const int4 u = units[blockIdx.x / ng];
     const int k0 = (u.x & 0xffff) * TK, j0 = (u.x >> 16) * TJ;
     const int i0 = u.y, i1 = u.z;
     const int nplanes = i1 - i0 + 2;  // planes i0-1 .. i1
@@ -374,7 +386,7 @@ __global__ void __launch_bounds__(32 * (TJ + 1), SlabGeo<T, TJ, NS, NSLOT, AIR, 
             s.ca = d - s.ca0;
         }
         s.bcc = static_cast<const T*>(f.bcc);
-        s.psi = static_cast<const T*>(f.psi) + (long long)b * 4 * f.slab;
+        s.psi = static_cast<const T*>(f.psi) + (long long)b * 4 * f.slab;  // field set b; b+q at + 4 q slab
         s.psin = static_cast<T*>(f.psi_next) + (long long)b * 4 * f.slab;
         s.air = f.air;
         if (fq >= kMaxFaces) s.n = 0;  // an empty slot of a larger-capacity launch: never active
@@ -438,10 +450,16 @@ __global__ void __launch_bounds__(32 * (TJ + 1), SlabGeo<T, TJ, NS, NSLOT, AIR, 
                     const Slot<T>& f = sl[q];
                     const int pl = f.axis == 0 ? ip - f.lo : ip;
                     unsigned char* ss = st + G::oS + q * G::slot;
-                    tma::load_4d(ss + G::sPE, &maps.psiE[f.face], f.c0, f.c1, pl, 4 * b, &full[s]);
+#pragma unroll
+                    for (int m = 0; m < NB; ++m)
+                        tma::load_4d(ss + G::sPE + m * G::setPE, &maps.psiE[f.face], f.c0, f.c1, pl, 4 * (b + m),
+                                     &full[s]);
                     if constexpr (AIR) tma::load_4d(ss + G::sAE, &maps.airE[f.face], f.ca0, f.c1, pl, 0, &full[s]);
                     if (!last) {
-                        tma::load_4d(ss + G::sPH, &maps.psiH[f.face], f.c0, f.c1, pl, 4 * b + 2, &full[s]);
+#pragma unroll
+                        for (int m = 0; m < NB; ++m)
+                            tma::load_4d(ss + G::sPH + m * G::setPH, &maps.psiH[f.face], f.c0, f.c1, pl,
+                                         4 * (b + m) + 2, &full[s]);
                         if constexpr (AIR)
                             tma::load_4d(ss + G::sAH, &maps.airH[f.face], f.ca0, f.c1, pl, 2, &full[s]);
                     }
@@ -452,7 +470,7 @@ __global__ void __launch_bounds__(32 * (TJ + 1), SlabGeo<T, TJ, NS, NSLOT, AIR, 
     } else {
         // compute warps: owned cell (warp, lane), and halo cell x for the
         // first NX threads (row TJ, then column TK)
-        const long long fs = 3 * g.vol * (long long)b;
+        const long long fs = 3 * g.vol * (long long)b, fstride = 3 * g.vol;  // field set b, then the next ones
         T* __restrict__ Eg = p.e_next + fs;
         T* __restrict__ Hg = p.h_next + fs;
         const int jo = j0 + warp, ko = k0 + lane;
@@ -476,9 +494,15 @@ __global__ void __launch_bounds__(32 * (TJ + 1), SlabGeo<T, TJ, NS, NSLOT, AIR, 
             if (t > 0 && ok) {
                 const unsigned char* st = smem + s * G::stage;
                 const unsigned char* stp = smem + ((t - 1) % NS) * G::stage;
-                T* en = ring + (t % 3) * 3 * G::cN;
-                step_E<T, TJ, NS, NSLOT, AIR, CK>(p, sl, st, stp, en, warp, lane, i, jo, ko, v_own && i < i1, Eg);
-                if (has_x) step_E<T, TJ, NS, NSLOT, AIR, CK>(p, sl, st, stp, en, rx, cx, i, jx, kx, own_x && i < i1, Eg);
+#pragma unroll
+                for (int m = 0; m < NB; ++m) {
+                    T* en = ring + ((t % 3) * NB + m) * 3 * G::cN;
+                    step_E<T, TJ, NS, NSLOT, AIR, CK, NB>(p, sl, st, stp, m, en, warp, lane, i, jo, ko, v_own && i < i1,
+                                                          Eg + m * fstride);
+                    if (has_x)
+                        step_E<T, TJ, NS, NSLOT, AIR, CK, NB>(p, sl, st, stp, m, en, rx, cx, i, jx, kx,
+                                                              own_x && i < i1, Eg + m * fstride);
+                }
             }
             tma::compute_barrier(NC);
             if (flags[0]) {
@@ -487,11 +511,17 @@ __global__ void __launch_bounds__(32 * (TJ + 1), SlabGeo<T, TJ, NS, NSLOT, AIR, 
             }
             if (t > 1) {
                 const unsigned char* stp = smem + ((t - 1) % NS) * G::stage;
-                const T* enp = ring + ((t - 1) % 3) * 3 * G::cN;
-                const T* enc = ring + (t % 3) * 3 * G::cN;
-                if (v_own)
-                    step_H<T, TJ, NS, NSLOT, AIR, CK, false>(p, sl, stp, enp, enc, warp, lane, i - 1, jo, ko, Hg);
-                if (own_x) step_H<T, TJ, NS, NSLOT, AIR, CK, true>(p, sl, stp, enp, enc, rx, cx, i - 1, jx, kx, Hg);
+#pragma unroll
+                for (int m = 0; m < NB; ++m) {
+                    const T* enp = ring + (((t - 1) % 3) * NB + m) * 3 * G::cN;
+                    const T* enc = ring + ((t % 3) * NB + m) * 3 * G::cN;
+                    if (v_own)
+                        step_H<T, TJ, NS, NSLOT, AIR, CK, NB, false>(p, sl, stp, m, enp, enc, warp, lane, i - 1, jo, ko,
+                                                                     Hg + m * fstride);
+                    if (own_x)
+                        step_H<T, TJ, NS, NSLOT, AIR, CK, NB, true>(p, sl, stp, m, enp, enc, rx, cx, i - 1, jx, kx,
+                                                                    Hg + m * fstride);
+                }
             }
             if (t > 0) {
                 __syncwarp();
@@ -591,88 +621,107 @@ __global__ void k_dead_units_sync(Geom g, const T* __restrict__ aH, const T* __r
     }
 }
 
-// Slab variants: (TJ, NS of the CPML-free list, NS of the CPML lists).
+constexpr size_t kMaxSmemOptin = 232448;  // B200 opt-in per CTA (227 KB), when the device cannot be queried
+
+// An instance is built only when its shared memory fits one CTA.  Every
+// variant has its 0-3 slot instances; a six-slot one (both faces of an axis
+// reaching one unit: small grids) may be missing, and a plan that needs it
+// is refused when the units are planned.
+template <typename T, int TJ, int NS, int NSLOT, bool AIR, int CK, int NB>
+constexpr bool slab_fits() {
+    return SlabGeo<T, TJ, NS, NSLOT, AIR, CK, NB>::smem <= kMaxSmemOptin;
+}
+
+// Slab variants: (TJ, NS of the CPML-free list, NS of the CPML lists, NB
+// field sets per CTA).
 template <typename F>
 bool slab_dispatch(int variant, F&& f) {
     switch (variant) {
-        case 0: f.template run<4, 3, 3>(); return true;
-        case 1: f.template run<2, 3, 3>(); return true;
-        case 2: f.template run<3, 3, 3>(); return true;
-        case 3: f.template run<4, 4, 4>(); return true;
-        case 4: f.template run<3, 4, 4>(); return true;
-        case 5: f.template run<2, 4, 4>(); return true;
-        case 6: f.template run<8, 3, 3>(); return true;
-        case 7: f.template run<6, 3, 3>(); return true;
+        case 0: f.template run<4, 3, 3, 1>(); return true;
+        case 1: f.template run<2, 3, 3, 1>(); return true;
+        case 2: f.template run<3, 3, 3, 1>(); return true;
+        case 3: f.template run<4, 4, 4, 1>(); return true;
+        case 4: f.template run<3, 4, 4, 1>(); return true;
+        case 5: f.template run<2, 4, 4, 1>(); return true;
+        case 6: f.template run<8, 3, 3, 1>(); return true;
+        case 7: f.template run<6, 3, 3, 1>(); return true;
+        case 8: f.template run<4, 3, 3, 2>(); return true;
+        case 9: f.template run<4, 3, 3, 4>(); return true;
         default: return false;
     }
 }
 
-// Every kernel instance of one (TJ, NS) and coefficient storage CK: slot
+template <typename T, int TJ, int NS, int NSLOT, bool AIR, int CK, int NB, typename G>
+void one_if_fits(G&& g) {
+    if constexpr (slab_fits<T, TJ, NS, NSLOT, AIR, CK, NB>()) g.template one<T, TJ, NS, NSLOT, AIR, CK, NB>();
+}
+
+// Every kernel instance of one (TJ, NS, NB) and coefficient storage CK: slot
 // capacities 0, 1, 2, 3, 6, with and without air masks.
-template <typename T, int TJ, int NS, int CK, typename G>
+template <typename T, int TJ, int NS, int CK, int NB, typename G>
 void each_instance_ck(G&& g) {
-    g.template one<T, TJ, NS, 0, false, CK>();
-    g.template one<T, TJ, NS, 1, false, CK>();
-    g.template one<T, TJ, NS, 2, false, CK>();
-    g.template one<T, TJ, NS, 3, false, CK>();
-    g.template one<T, TJ, NS, 6, false, CK>();
-    g.template one<T, TJ, NS, 1, true, CK>();
-    g.template one<T, TJ, NS, 2, true, CK>();
-    g.template one<T, TJ, NS, 3, true, CK>();
-    g.template one<T, TJ, NS, 6, true, CK>();
+    one_if_fits<T, TJ, NS, 0, false, CK, NB>(g);
+    one_if_fits<T, TJ, NS, 1, false, CK, NB>(g);
+    one_if_fits<T, TJ, NS, 2, false, CK, NB>(g);
+    one_if_fits<T, TJ, NS, 3, false, CK, NB>(g);
+    one_if_fits<T, TJ, NS, 6, false, CK, NB>(g);
+    one_if_fits<T, TJ, NS, 1, true, CK, NB>(g);
+    one_if_fits<T, TJ, NS, 2, true, CK, NB>(g);
+    one_if_fits<T, TJ, NS, 3, true, CK, NB>(g);
+    one_if_fits<T, TJ, NS, 6, true, CK, NB>(g);
 }
 
-// All instances of one (TJ, NS): native coefficients, and float16 storage
-// for float32 fields.
-template <typename T, int TJ, int NS, typename G>
+// All instances of one (TJ, NS, NB): native coefficients, and float16
+// storage for float32 fields.
+template <typename T, int TJ, int NS, int NB, typename G>
 void each_instance(G&& g) {
-    each_instance_ck<T, TJ, NS, kCoefNative>(g);
-    if constexpr (sizeof(T) == 4) each_instance_ck<T, TJ, NS, kCoefF16>(g);
+    each_instance_ck<T, TJ, NS, kCoefNative, NB>(g);
+    if constexpr (sizeof(T) == 4) each_instance_ck<T, TJ, NS, kCoefF16, NB>(g);
 }
-
-struct MaxSmem {
-    size_t v = 0;
-    template <typename T, int TJ, int NS, int NSLOT, bool AIR, int CK>
-    void one() {
-        v = std::max(v, SlabGeo<T, TJ, NS, NSLOT, AIR, CK>::smem);
-    }
-};
 
 struct Prepare {
     cudaError_t err = cudaSuccess;
-    template <typename T, int TJ, int NS, int NSLOT, bool AIR, int CK>
+    template <typename T, int TJ, int NS, int NSLOT, bool AIR, int CK, int NB>
     void one() {
-        const cudaError_t e = cudaFuncSetAttribute(k_step_slab<T, TJ, NS, NSLOT, AIR, CK>,
+        const cudaError_t e = cudaFuncSetAttribute(k_step_slab<T, TJ, NS, NSLOT, AIR, CK, NB>,
                                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                   (int)SlabGeo<T, TJ, NS, NSLOT, AIR, CK>::smem);
+                                                   (int)SlabGeo<T, TJ, NS, NSLOT, AIR, CK, NB>::smem);
         if (err == cudaSuccess) err = e;
     }
 };
 
+// Shape of a variant: tile rows, field sets per CTA, the largest shared
+// memory of the instances every plan needs (0-3 slots, native coefficients:
+// the float16 boxes are smaller), whether the six-slot instances exist, and
+// the occupancy of the CPML-free instance.
 template <typename T>
 struct SlabInfo {
     size_t smem = 0;
-    int tj = 0, occ0 = 1;
-    template <int TJ, int NS, int NSC>
+    int tj = 0, nb = 1, occ0 = 1;
+    bool six = false, six_air = false;
+    template <int TJ, int NS, int NSC, int NB>
     void run() {
-        MaxSmem m;
-        each_instance<T, TJ, NS>(m);
-        if constexpr (NSC != NS) each_instance<T, TJ, NSC>(m);
-        smem = m.v;
+        constexpr int CK = kCoefNative;
+        smem = std::max({SlabGeo<T, TJ, NS, 0, false, CK, NB>::smem, SlabGeo<T, TJ, NSC, 3, false, CK, NB>::smem,
+                         SlabGeo<T, TJ, NSC, 3, true, CK, NB>::smem});
+        six = slab_fits<T, TJ, NSC, 6, false, CK, NB>();
+        six_air = slab_fits<T, TJ, NSC, 6, true, CK, NB>();
         tj = TJ;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ0, k_step_slab<T, TJ, NS, 0, false, kCoefNative>,
-                                                      32 * (TJ + 1), SlabGeo<T, TJ, NS, 0, false, kCoefNative>::smem);
+        nb = NB;
+        if constexpr (slab_fits<T, TJ, NS, 0, false, CK, NB>())
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ0, k_step_slab<T, TJ, NS, 0, false, CK, NB>,
+                                                          32 * (TJ + 1), SlabGeo<T, TJ, NS, 0, false, CK, NB>::smem);
     }
 };
 
 template <typename T>
 struct SlabPrepare {
     cudaError_t err = cudaSuccess;
-    template <int TJ, int NS, int NSC>
+    template <int TJ, int NS, int NSC, int NB>
     void run() {
         Prepare pr;
-        each_instance<T, TJ, NS>(pr);
-        if constexpr (NSC != NS) each_instance<T, TJ, NSC>(pr);
+        each_instance<T, TJ, NS, NB>(pr);
+        if constexpr (NSC != NS) each_instance<T, TJ, NSC, NB>(pr);
         err = pr.err;
     }
 };
@@ -687,42 +736,50 @@ struct SlabLaunch {
     int* status;
     const cudaStream_t* streams;  // one per list
     int launched = 0;
-    template <int NSLOT, bool AIR, int CK, int TJ, int NS>
+    bool missing = false;  // a list whose instance is not built (refused when planned)
+    template <int NSLOT, bool AIR, int CK, int TJ, int NS, int NB>
     void go(int q) {
         if (n_units[q] <= 0) return;
-        k_step_slab<T, TJ, NS, NSLOT, AIR, CK>
-            <<<dim3((unsigned)n_units[q] * a.B), 32 * (TJ + 1), SlabGeo<T, TJ, NS, NSLOT, AIR, CK>::smem,
-               streams[q]>>>(m, a, units[q], status);
-        ++launched;
-    }
-    template <int CK, int TJ, int NS, int NSC>
-    void run_ck() {
-        go<0, false, CK, TJ, NS>(0);
-        if (air) {
-            go<1, true, CK, TJ, NSC>(1);
-            go<2, true, CK, TJ, NSC>(2);
-            go<3, true, CK, TJ, NSC>(3);
-            go<6, true, CK, TJ, NSC>(4);
+        if constexpr (slab_fits<T, TJ, NS, NSLOT, AIR, CK, NB>()) {
+            k_step_slab<T, TJ, NS, NSLOT, AIR, CK, NB>
+                <<<dim3((unsigned)n_units[q] * (a.B / NB)), 32 * (TJ + 1), SlabGeo<T, TJ, NS, NSLOT, AIR, CK, NB>::smem,
+                   streams[q]>>>(m, a, units[q], status);
+            ++launched;
         } else {
-            go<1, false, CK, TJ, NSC>(1);
-            go<2, false, CK, TJ, NSC>(2);
-            go<3, false, CK, TJ, NSC>(3);
-            go<6, false, CK, TJ, NSC>(4);
+            missing = true;
         }
     }
-    template <int TJ, int NS, int NSC>
+    template <int CK, int TJ, int NS, int NSC, int NB>
+    void run_ck() {
+        go<0, false, CK, TJ, NS, NB>(0);
+        if (air) {
+            go<1, true, CK, TJ, NSC, NB>(1);
+            go<2, true, CK, TJ, NSC, NB>(2);
+            go<3, true, CK, TJ, NSC, NB>(3);
+            go<6, true, CK, TJ, NSC, NB>(4);
+        } else {
+            go<1, false, CK, TJ, NSC, NB>(1);
+            go<2, false, CK, TJ, NSC, NB>(2);
+            go<3, false, CK, TJ, NSC, NB>(3);
+            go<6, false, CK, TJ, NSC, NB>(4);
+        }
+    }
+    template <int TJ, int NS, int NSC, int NB>
     void run() {
+        if (a.B % NB != 0) {
+            missing = true;
+            return;
+        }
         if constexpr (sizeof(T) == 4) {
             if (a.coef_kind == kCoefF16) {
-                run_ck<kCoefF16, TJ, NS, NSC>();
+                run_ck<kCoefF16, TJ, NS, NSC, NB>();
                 return;
             }
         }
-        run_ck<kCoefNative, TJ, NS, NSC>();
+        run_ck<kCoefNative, TJ, NS, NSC, NB>();
     }
 };
 
-constexpr size_t kMaxSmemOptin = 232448;  // B200 opt-in per CTA (227 KB), when the device cannot be queried
 
 }  // namespace
 
@@ -731,6 +788,21 @@ int slab_tj_of(int variant) {
     if (!slab_dispatch(variant, f)) return 0;
     return f.tj;
 }
+
+int slab_nb_of(int variant) {
+    SlabInfo<float> f;
+    if (!slab_dispatch(variant, f)) return 1;
+    return f.nb;
+}
+
+template <typename T>
+bool slab_six_ok(int variant, bool air) {
+    SlabInfo<T> f;
+    if (!slab_dispatch(variant, f)) return false;
+    return air ? f.six_air : f.six;
+}
+template bool slab_six_ok<float>(int, bool);
+template bool slab_six_ok<double>(int, bool);
 
 template <typename T>
 bool slab_supported(int variant) {
@@ -871,7 +943,7 @@ StreamPlan plan_slab(const Geom& g, int sm_count, int ctas_per_sm, int B, int va
     slab_dispatch(variant, f);
     StreamPlan s{};
     s.block_y = f.tj;
-    s.grid_x = (g.nz % TK == 0 ? g.nz / TK : (g.nz + TK) / TK) * B;
+    s.grid_x = (g.nz % TK == 0 ? g.nz / TK : (g.nz + TK) / TK) * std::max(1, B / f.nb);
     s.grid_y = g.ny % f.tj == 0 ? g.ny / f.tj : (g.ny + f.tj) / f.tj;
     const long long tiles = (long long)s.grid_x * s.grid_y;
     const int nplanes = g.nx + 1;
@@ -901,11 +973,13 @@ int launch_slab_step(StencilArgs<T> a, int ichunk, int variant, const int4* cons
                      bool air, int* status, const cudaStream_t streams[5]) {
     SlabInfo<T> info;
     if (!slab_dispatch(variant, info)) return -1;
-    const int tj = info.tj;
+    const int tj = info.tj, nb = info.nb;
+    if (a.B % nb != 0) return -4;
     SlabMaps m;
     const long long nset = 3LL * a.B;
-    if (!tma::encode_field_map<T>(&m.e, a.e, a.g, (int)nset, TK + 4, tj + 1) ||
-        !tma::encode_field_map<T>(&m.h, a.h, a.g, (int)nset, TK + 8, tj + 2))
+    // E and H boxes: the three components of the CTA's nb field sets
+    if (!tma::encode_field_map<T>(&m.e, a.e, a.g, (int)nset, TK + 4, tj + 1, 3 * nb) ||
+        !tma::encode_field_map<T>(&m.h, a.h, a.g, (int)nset, TK + 8, tj + 2, 3 * nb))
         return -2;
     if (a.coef_kind == kCoefF16) {
         // 16-bit coefficient boxes: E rows of 40 entries (80 bytes), H rows of 32
@@ -948,7 +1022,7 @@ int launch_slab_step(StencilArgs<T> a, int ichunk, int variant, const int4* cons
     a.ichunk = ichunk;
     SlabLaunch<T> l{m, a, units, n_units, air, status, streams};
     slab_dispatch(variant, l);
-    return l.launched;
+    return l.missing ? -4 : l.launched;
 }
 template int launch_slab_step<float>(StencilArgs<float>, int, int, const int4* const[5], const int[5], bool, int*,
                                      const cudaStream_t[5]);

@@ -114,14 +114,14 @@ inline bool encode_4d(CUtensorMap* out, CUtensorMapDataType dt, const void* base
 }
 
 // 4-D map over the padded field layout: (k, j, plane, component) with
-// `ncomp` components of `vol` elements; box (bk, bj, 1, 3).
+// `ncomp` components of `vol` elements; box (bk, bj, 1, bc).
 template <typename T>
-bool encode_field_map(CUtensorMap* out, const void* base, const Geom& g, int ncomp, int bk, int bj) {
+bool encode_field_map(CUtensorMap* out, const void* base, const Geom& g, int ncomp, int bk, int bj, int bc = 3) {
     const unsigned long long dims[4] = {(unsigned long long)g.nkp, (unsigned long long)g.njp,
                                         (unsigned long long)(g.nx + 4), (unsigned long long)ncomp};
     const unsigned long long strides[3] = {(unsigned long long)g.sj * sizeof(T), (unsigned long long)g.si * sizeof(T),
                                            (unsigned long long)g.vol * sizeof(T)};
-    const unsigned box[4] = {(unsigned)bk, (unsigned)bj, 1, 3};
+    const unsigned box[4] = {(unsigned)bk, (unsigned)bj, 1, (unsigned)bc};
     return encode_4d(out, sizeof(T) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, base,
                      dims, strides, box);
 }

@@ -596,6 +596,54 @@ def test_slab_precision_variants():
         assert r["dT"] <= tol and r["dR"] <= tol and r["dT_phase_deg"] <= ptol, name
 
 
+@pytest.mark.parametrize("precision,tol", [("single", 1e-5), ("double", 1e-12)])
+def test_slab_step_with_field_sets_sharing_a_cta_matches_stream(precision, tol):
+    """Four field sets with different random initial fields on the 70^3
+    multi-tile grid (partial last tiles, 6-layer CPML, chunk seams), with one,
+    two and four field sets per CTA (fused 16, 24, 25): each set equals the
+    stream kernels' march, and the shared-CTA forms give the same bits as the
+    one-set form (each set's arithmetic is unchanged).  A batch that is not a
+    multiple of a form's sets per CTA is refused; float64 refuses the forms
+    whose shared memory does not fit."""
+    from magnelio_b200 import workloads
+
+    steps = 15
+    prob = workloads.brick_box(70, seed=6, n_bricks=6, cpml_cells=6, n_freq=3, steps=steps + 2)
+    rng = np.random.default_rng(12)
+    inits = [_random_state(prob, rng) for _ in range(4)]
+    prob.batch = 4
+    prob.lumped[0].v_src = np.tile(prob.lumped[0].v_src[:1], (4, 1)) * np.arange(1, 5)[:, None]
+    prob.e0 = [a for a, _ in inits]
+    prob.h0 = [b for _, b in inits]
+    outs = {}
+    for kind, v in (("stream", 0), ("fused", 16), ("fused", 24), ("fused", 25)):
+        with prob.build_engine(precision) as eng:
+            try:
+                eng.configure_stencil(kind, v, 9)
+            except FitbError as exc:
+                assert precision == "double" and v in (24, 25) and "fused variant" in str(exc), exc
+                continue
+            eng.step(steps)
+            outs[v if kind == "fused" else "stream"] = [eng.read_fields(b) for b in range(4)]
+    assert 16 in outs and (precision == "double" or (24 in outs and 25 in outs))
+    for b in range(4):
+        es, hs = outs["stream"][b]
+        for v in (16, 24, 25):
+            if v not in outs:
+                continue
+            et, ht = outs[v][b]
+            assert _rel(et, es, float(np.max(np.abs(es)))) < tol, (v, b)
+            assert _rel(ht, hs, float(np.max(np.abs(hs)))) < tol, (v, b)
+            assert np.array_equal(et, outs[16][b][0]) and np.array_equal(ht, outs[16][b][1]), (v, b)
+    # a batch of one refuses the shared-CTA forms
+    prob.batch = 1
+    prob.lumped[0].v_src = prob.lumped[0].v_src[:1]
+    prob.e0, prob.h0 = prob.e0[:1], prob.h0[:1]
+    with prob.build_engine("single") as eng:
+        with pytest.raises(FitbError, match="field sets per CTA"):
+            eng.configure_stencil("fused", 24, 0)
+
+
 @pytest.mark.parametrize("precision,tol", [("double", 1e-8), ("single", F32_TOL)])
 def test_cross_junction_eight_excitations_in_one_batch(precision, tol):
     """Batching configuration (reduced grid): the four-port junction's eight
