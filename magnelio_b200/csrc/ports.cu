@@ -17,7 +17,7 @@ namespace fitb {
 
 namespace {
 
-constexpr int kPortThreads = 512;
+constexpr int kPortThreads = 256;
 
 __device__ __forceinline__ void atomic_max_nonneg(double* addr, double v) {
     // Non-negative doubles order like their bit patterns.
@@ -111,6 +111,11 @@ template <typename T>
 __global__ void __launch_bounds__(kPortThreads)
     k_modal(T* __restrict__ e, const T* __restrict__ h, PortsArgs pa,
             const ModalDev* __restrict__ ports) {
+    // The phases below keep the reference's arithmetic per value; what moves
+    // is when the loads happen: everything that does not depend on this
+    // step's port update (the mode state, the DTBC partial sums, the H
+    // samples of the recorder) is read up front, so that a step costs few
+    // dependent memory round trips.
     const ModalDev& d = ports[blockIdx.x];
     const int b = blockIdx.y;
     const long long n = *pa.step;
@@ -129,10 +134,33 @@ __global__ void __launch_bounds__(kPortThreads)
     __shared__ double wred[kPortThreads / 32][2 * kMaxModes];
     __shared__ double s_vint[kMaxModes];
     __shared__ double s_vc[kMaxModes];
+    __shared__ double s_conv[2 * kMaxModes];
 
-    // 1. Interior-plane projection V_int_new[m] = sum me_int * (p_m * e_int).
-    //    (The mode loops are unrolled to kMaxModes with a guard so that the
-    //    partial sums stay in registers.)
+    // mode state of mode m = threadIdx.x (m < M)
+    const int exc = d.exc_mode[b];
+    const int tm = threadIdx.x < M ? threadIdx.x : 0;
+    const double vport0 = Vport_prev[tm], vint0 = Vint_prev[tm], u0 = u[tm], up0 = u_prev[tm];
+    const double mur = d.mur_r[tm];
+    const bool dtbc = d.is_dtbc[tm];
+
+    // 2. DTBC boundary convolutions conv_w = sum_{m=1..n} l_m w[n-m] and
+    //    u_inc = sum l_m s[n-m]: the partial sums k_dtbc_conv left per
+    //    history chunk (before this kernel, on the same stream), added in
+    //    chunk order (a fixed order: the result does not depend on
+    //    scheduling).
+    if (threadIdx.x < 2 * M && d.is_dtbc[threadIdx.x >> 1]) {
+        const int m = threadIdx.x >> 1, w = threadIdx.x & 1;
+        const int nck = (int)((n + kConvChunk - 1) / kConvChunk);
+        const double* part = d.conv + (((long long)b * M + m) * d.conv_chunks) * 2 + w;
+        double a = 0.0;
+        for (int c = 0; c < nck; ++c) a += part[2 * c];
+        s_conv[threadIdx.x] = a;
+    }
+
+    // 1. Interior-plane projection V_int_new[m] = sum me_int * (p_m * e_int),
+    //    and the recorder's I samples from h^{n+1/2} (this kernel writes no
+    //    H) into acc[kMaxModes + m].  The mode loops are unrolled to
+    //    kMaxModes with a guard so that the partial sums stay in registers.
     double acc[2 * kMaxModes];
 #pragma unroll
     for (int m = 0; m < 2 * kMaxModes; ++m) acc[m] = 0.0;
@@ -144,67 +172,59 @@ __global__ void __launch_bounds__(kPortThreads)
         for (int m = 0; m < kMaxModes; ++m)
             if (m < M) acc[m] += me * (d.vprof[(long long)m * ne + p] * v);
     }
-    block_sum_modes<false>(acc, M, red, wred);
-    if (threadIdx.x < M) s_vint[threadIdx.x] = red[threadIdx.x];
-    __syncthreads();
-
-    // 2. DTBC boundary convolutions conv_w = sum_{m=1..n} l_m w[n-m] and
-    //    u_inc = sum l_m s[n-m]: the partial sums k_dtbc_conv left per
-    //    history chunk, added in chunk order (a fixed order: the result does
-    //    not depend on scheduling).
-    const int exc = d.exc_mode[b];
-    if (threadIdx.x < 2 * M && d.is_dtbc[threadIdx.x >> 1]) {
-        const int m = threadIdx.x >> 1, w = threadIdx.x & 1;
-        const int nck = (int)((n + kConvChunk - 1) / kConvChunk);
-        const double* part = d.conv + (((long long)b * M + m) * d.conv_chunks) * 2 + w;
-        double a = 0.0;
-        for (int c = 0; c < nck; ++c) a += part[2 * c];
-        red[threadIdx.x] = a;
+    for (int p = threadIdx.x; p < nh; p += blockDim.x) {
+        const double v = (double)H[d.port_h[p]];
+        const double mh = d.mh_port[p];
+#pragma unroll
+        for (int m = 0; m < kMaxModes; ++m)
+            if (m < M) acc[kMaxModes + m] += mh * (d.hprof[(long long)m * nh + p] * v);
     }
-    __syncthreads();
+    block_sum_modes<false>(acc, M, red, wred);  // ends with a block barrier (s_conv too)
 
     // 3. Per-mode boundary value: one thread per mode (the modes' scalar
     //    float64 recursions are independent of each other).
     if (threadIdx.x < M) {
         const double* wf = d.wf + (long long)b * d.n_wf;
-        {
-            const int m = threadIdx.x;
-            const double vin = s_vint[m];
-            double vc = Vint_prev[m] + d.mur_r[m] * (vin - Vport_prev[m]);
-            if (m == exc && !d.is_dtbc[m]) {
-                const long long t1 = n + 1;
-                const double src_new = (t1 < d.n_wf) ? wf[t1] : 0.0;
-                const int maxlen = d.buf_len[b];
-                const double inc_int_now = interp_delayed(wf, d.n_wf, n, maxlen, d.tau[m], d.dt);
-                const double inc_int_prev =
-                    interp_delayed(wf, d.n_wf, n, maxlen, d.tau[m] + d.dt, d.dt);
-                const double inc_face_prev = interp_delayed(wf, d.n_wf, n, maxlen, d.dt, d.dt);
-                const double scat_int_now = vin - inc_int_now;
-                const double scat_int_prev = Vint_prev[m] - inc_int_prev;
-                const double scat_face_prev = Vport_prev[m] - inc_face_prev;
-                vc = src_new + scat_int_prev + d.mur_r[m] * (scat_int_now - scat_face_prev);
-            }
-            if (d.is_dtbc[m]) {
-                const double src = (m == exc && n < d.n_wf) ? wf[n] : 0.0;
-                const double conv_w = red[2 * m], u_inc = red[2 * m + 1];
-                const double ghost = src + conv_w;
-                double* wh = d.whist + ((long long)b * M + m) * d.cap;
-                double* sh = d.shist + ((long long)b * M + m) * d.cap;
-                wh[n] = u[m] - u_inc;
-                sh[n] = src;
-                double un = (2.0 - 2.0 * d.r2[m] - d.q2[m]) * u[m];
-                un = un - u_prev[m];
-                un = un + d.r2[m] * (ghost + Vint_prev[m]);
-                u_prev[m] = u[m];
-                u[m] = un;
-                vc = un;
-            }
-            s_vc[m] = vc;
+        const int m = threadIdx.x;
+        const double vin = red[m];
+        s_vint[m] = vin;
+        double vc = vint0 + mur * (vin - vport0);
+        if (m == exc && !dtbc) {
+            const long long t1 = n + 1;
+            const double src_new = (t1 < d.n_wf) ? wf[t1] : 0.0;
+            const int maxlen = d.buf_len[b];
+            const double inc_int_now = interp_delayed(wf, d.n_wf, n, maxlen, d.tau[m], d.dt);
+            const double inc_int_prev = interp_delayed(wf, d.n_wf, n, maxlen, d.tau[m] + d.dt, d.dt);
+            const double inc_face_prev = interp_delayed(wf, d.n_wf, n, maxlen, d.dt, d.dt);
+            const double scat_int_now = vin - inc_int_now;
+            const double scat_int_prev = vint0 - inc_int_prev;
+            const double scat_face_prev = vport0 - inc_face_prev;
+            vc = src_new + scat_int_prev + mur * (scat_int_now - scat_face_prev);
         }
+        if (dtbc) {
+            const double src = (m == exc && n < d.n_wf) ? wf[n] : 0.0;
+            const double conv_w = s_conv[2 * m], u_inc = s_conv[2 * m + 1];
+            const double ghost = src + conv_w;
+            double* wh = d.whist + ((long long)b * M + m) * d.cap;
+            double* sh = d.shist + ((long long)b * M + m) * d.cap;
+            wh[n] = u0 - u_inc;
+            sh[n] = src;
+            double un = (2.0 - 2.0 * d.r2[m] - d.q2[m]) * u0;
+            un = un - up0;
+            un = un + d.r2[m] * (ghost + vint0);
+            u_prev[m] = u0;
+            u[m] = un;
+            vc = un;
+        }
+        s_vc[m] = vc;
     }
     __syncthreads();
 
-    // 4. Reconstruct the port plane from the modal expansion (+ complement).
+    // 4. Reconstruct the port plane from the modal expansion (+ complement),
+    //    and 5. the recorder's V samples of the corrected port plane, from the
+    //    value each thread has just stored (acc[0..M)).
+#pragma unroll
+    for (int m = 0; m < kMaxModes; ++m) acc[m] = 0.0;
     for (int p = threadIdx.x; p < ne; p += blockDim.x) {
         double v = 0.0;
         for (int m = 0; m < M; ++m) v += s_vc[m] * d.eprof[(long long)m * ne + p];
@@ -218,27 +238,13 @@ __global__ void __launch_bounds__(kPortThreads)
             cs[ne + p] = cp;
         }
         enew[p] = v;
-        E[d.port_e[p]] = (T)v;
-    }
-    __syncthreads();
-
-    // 5. Recorder samples: V from the corrected port plane, I from h^{n+1/2}
-    //    (the I sums in acc[kMaxModes + m]).
-#pragma unroll
-    for (int m = 0; m < 2 * kMaxModes; ++m) acc[m] = 0.0;
-    for (int p = threadIdx.x; p < ne; p += blockDim.x) {
-        const double v = (double)E[d.port_e[p]];
+        const T stored = (T)v;
+        E[d.port_e[p]] = stored;
+        const double vr = (double)stored;
         const double me = d.me_port[p];
 #pragma unroll
         for (int m = 0; m < kMaxModes; ++m)
-            if (m < M) acc[m] += me * (d.vprof[(long long)m * ne + p] * v);
-    }
-    for (int p = threadIdx.x; p < nh; p += blockDim.x) {
-        const double v = (double)H[d.port_h[p]];
-        const double mh = d.mh_port[p];
-#pragma unroll
-        for (int m = 0; m < kMaxModes; ++m)
-            if (m < M) acc[kMaxModes + m] += mh * (d.hprof[(long long)m * nh + p] * v);
+            if (m < M) acc[m] += me * (d.vprof[(long long)m * ne + p] * vr);
     }
     block_sum_modes<true>(acc, M, red, wred);
     if (threadIdx.x < M) {
