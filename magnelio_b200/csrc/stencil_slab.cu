@@ -85,17 +85,25 @@ struct SlabGeo {
     static constexpr int EKc = CK == kCoefNative ? EK : 40, cCE = ER * EKc;
     static constexpr size_t al(size_t b) { return (b + 127) / 128 * 128; }
     // E and H boxes of the NB field sets one after the other (one copy of
-    // 3 NB components each), psi boxes per field set; the coefficient and
-    // air-mask boxes once for all of them
+    // 3 NB components each), psi boxes one copy per field set; the
+    // coefficient and air-mask boxes once for all of them.  Every tensor
+    // copy lands on a 128-byte boundary: the per-set psi boxes at a stride
+    // of setPE / setPH rounded up to 128 bytes.
     static constexpr unsigned setE = 3u * cE * sizeof(T), setH = 3u * cH * sizeof(T);
-    static constexpr unsigned setPE = 2u * cPE * sizeof(T), setPH = 2u * cPH * sizeof(T);
+    static constexpr unsigned setPE = (unsigned)al(2u * cPE * sizeof(T)), setPH = (unsigned)al(2u * cPH * sizeof(T));
     static constexpr unsigned bytesE = NB * setE, bytesH = NB * setH, bytesCE = 3u * cCE * CB, bytesC = 3u * cC * CB;
-    static constexpr unsigned bytesPE = NB * setPE, bytesPH = NB * setPH, bytesAE = 2u * cAE, bytesAH = 2u * cAH;
+    // bytes the copies deliver (the expected transaction counts)
+    static constexpr unsigned bytesPE = NB * 2u * cPE * sizeof(T), bytesPH = NB * 2u * cPH * sizeof(T),
+                              bytesAE = 2u * cAE, bytesAH = 2u * cAH;
     static constexpr size_t oE = 0, oH = al(bytesE), oaE = oH + al(bytesH), obE = oaE + al(bytesCE),
                             oaH = obE + al(bytesCE), obH = oaH + al(bytesC), oS = obH + al(bytesC);
     // within a slot: psi_E, psi_H, air_E, air_H
-    static constexpr size_t sPE = 0, sPH = al(bytesPE), sAE = sPH + al(bytesPH),
+    static constexpr size_t sPE = 0, sPH = NB * setPE, sAE = sPH + NB * setPH,
                             sAH = sAE + (AIR ? al(bytesAE) : 0), slot = sAH + (AIR ? al(bytesAH) : 0);
+    static_assert(oH % 128 == 0 && oaE % 128 == 0 && obE % 128 == 0 && oaH % 128 == 0 && obH % 128 == 0 &&
+                      oS % 128 == 0 && setPE % 128 == 0 && setPH % 128 == 0 && sAE % 128 == 0 &&
+                      sAH % 128 == 0 && slot % 128 == 0,
+                  "tensor copy destinations on 128-byte boundaries");
     static constexpr size_t stage = oS + NSLOT * slot;
     // E_new ring: 3 planes x NB field sets x 3 components
     static constexpr size_t oN = NS * stage, oSl = oN + al(3u * NB * 3u * cN * sizeof(T));
