@@ -745,13 +745,22 @@ struct SlabLaunch {
     const cudaStream_t* streams;  // one per list
     int launched = 0;
     bool missing = false;  // a list whose instance is not built (refused when planned)
+    int priority = 0;      // scheduling priority of the CPML lists' CTAs (0: the default)
     template <int NSLOT, bool AIR, int CK, int TJ, int NS, int NB>
     void go(int q) {
         if (n_units[q] <= 0) return;
         if constexpr (slab_fits<T, TJ, NS, NSLOT, AIR, CK, NB>()) {
-            k_step_slab<T, TJ, NS, NSLOT, AIR, CK, NB>
-                <<<dim3((unsigned)n_units[q] * (a.B / NB)), 32 * (TJ + 1), SlabGeo<T, TJ, NS, NSLOT, AIR, CK, NB>::smem,
-                   streams[q]>>>(m, a, units[q], status);
+            cudaLaunchConfig_t cfg{};
+            cfg.gridDim = dim3((unsigned)n_units[q] * (a.B / NB));
+            cfg.blockDim = dim3(32 * (TJ + 1));
+            cfg.dynamicSmemBytes = SlabGeo<T, TJ, NS, NSLOT, AIR, CK, NB>::smem;
+            cfg.stream = streams[q];
+            cudaLaunchAttribute at[1];
+            at[0].id = cudaLaunchAttributePriority;
+            at[0].val.priority = q > 0 ? priority : 0;
+            cfg.attrs = at;
+            cfg.numAttrs = 1;
+            cudaLaunchKernelEx(&cfg, k_step_slab<T, TJ, NS, NSLOT, AIR, CK, NB>, m, a, units[q], status);
             ++launched;
         } else {
             missing = true;
@@ -759,18 +768,30 @@ struct SlabLaunch {
     }
     template <int CK, int TJ, int NS, int NSC, int NB>
     void run_ck() {
-        go<0, false, CK, TJ, NS, NB>(0);
-        if (air) {
-            go<1, true, CK, TJ, NSC, NB>(1);
-            go<2, true, CK, TJ, NSC, NB>(2);
-            go<3, true, CK, TJ, NSC, NB>(3);
-            go<6, true, CK, TJ, NSC, NB>(4);
-        } else {
-            go<1, false, CK, TJ, NSC, NB>(1);
-            go<2, false, CK, TJ, NSC, NB>(2);
-            go<3, false, CK, TJ, NSC, NB>(3);
-            go<6, false, CK, TJ, NSC, NB>(4);
+        // the CPML lists first: their units march longer chains, the
+        // CPML-free list fills the SMs around them
+        if (order_cpml_first) {
+            // most slots (the longest marches) first
+            go_air<6, CK, TJ, NSC, NB>(4);
+            go_air<3, CK, TJ, NSC, NB>(3);
+            go_air<2, CK, TJ, NSC, NB>(2);
+            go_air<1, CK, TJ, NSC, NB>(1);
+            go<0, false, CK, TJ, NS, NB>(0);
+            return;
         }
+        go<0, false, CK, TJ, NS, NB>(0);
+        go_air<1, CK, TJ, NSC, NB>(1);
+        go_air<2, CK, TJ, NSC, NB>(2);
+        go_air<3, CK, TJ, NSC, NB>(3);
+        go_air<6, CK, TJ, NSC, NB>(4);
+    }
+    bool order_cpml_first = false;
+    template <int NSLOT, int CK, int TJ, int NS, int NB>
+    void go_air(int q) {
+        if (air)
+            go<NSLOT, true, CK, TJ, NS, NB>(q);
+        else
+            go<NSLOT, false, CK, TJ, NS, NB>(q);
     }
     template <int TJ, int NS, int NSC, int NB>
     void run() {
@@ -1029,6 +1050,22 @@ int launch_slab_step(StencilArgs<T> a, int ichunk, int variant, const int4* cons
     }
     a.ichunk = ichunk;
     SlabLaunch<T> l{m, a, units, n_units, air, status, streams};
+    // launch order and scheduling priority of the CPML lists: the
+    // environment variables FITB_SLAB_ORDER=cpml_first and
+    // FITB_SLAB_PRIORITY=1 (read once per process; tuning switches, every
+    // setting computes the same bits)
+    static const bool cpml_first = [] {
+        const char* e = std::getenv("FITB_SLAB_ORDER");
+        return e && !std::strcmp(e, "cpml_first");
+    }();
+    static const int high = [] {
+        const char* e = std::getenv("FITB_SLAB_PRIORITY");
+        int lo = 0, hi = 0;
+        if (!e || std::atoi(e) == 0 || cudaDeviceGetStreamPriorityRange(&lo, &hi) != cudaSuccess) return 0;
+        return hi;  // numerically lowest: the highest priority
+    }();
+    l.order_cpml_first = cpml_first;
+    l.priority = high;
     slab_dispatch(variant, l);
     return l.missing ? -4 : l.launched;
 }
