@@ -345,16 +345,16 @@ __device__ __forceinline__ void step_H(const StencilArgs<T>& p, const Slot<T>* s
 
 // Units: x = k tile, y = j tile, z = i chunk, w = the face of slot s in bits
 // 4s .. 4s+3.  A CTA marches NB field sets b0 .. b0+NB-1 of its unit through
-// the same coefficient boxes (each compute thread updates its cell in every
-// set in turn); blockIdx.x = unit * (B / NB) + b0 / NB.
+// the same coefficient boxes, with TJ compute warps per field set;
+// blockIdx.x = unit * (B / NB) + b0 / NB.
 template <typename T, int TJ, int NS, int NSLOT, bool AIR, int CK, int NB>
-__global__ void __launch_bounds__(32 * (TJ + 1), SlabGeo<T, TJ, NS, NSLOT, AIR, CK, NB>::minb())
+__global__ void __launch_bounds__(32 * (TJ * NB + 1), SlabGeo<T, TJ, NS, NSLOT, AIR, CK, NB>::minb())
     k_step_slab(const __grid_constant__ SlabMaps maps, const StencilArgs<T> p, const int4* __restrict__ units,
                 int* status) {
     using G = SlabGeo<T, TJ, NS, NSLOT, AIR, CK, NB>;
-    constexpr int NC = 32 * TJ;      // compute threads
-    constexpr int NX = TK + 1 + TJ;  // halo cells (row TJ, then column TK)
-    static_assert(NX <= NC, "tile shape");
+    constexpr int NC = 32 * TJ * NB;  // compute threads
+    constexpr int NX = TK + 1 + TJ;   // halo cells of a field set (row TJ, then column TK)
+    static_assert(NX <= 32 * TJ, "tile shape");
     extern __shared__ __align__(128) unsigned char smem[];
     const Geom& g = p.g;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -403,7 +403,7 @@ __global__ void __launch_bounds__(32 * (TJ + 1), SlabGeo<T, TJ, NS, NSLOT, AIR, 
     if (tid == 0) {
         for (int s = 0; s < NS; ++s) {
             tma::bar_init(&full[s], 1);
-            tma::bar_init(&empty[s], TJ);
+            tma::bar_init(&empty[s], TJ * NB);
         }
         flags[0] = 0;
         flags[1] = 0;
@@ -412,7 +412,7 @@ __global__ void __launch_bounds__(32 * (TJ + 1), SlabGeo<T, TJ, NS, NSLOT, AIR, 
     }
     __syncthreads();
 
-    if (warp == TJ) {
+    if (warp == TJ * NB) {
         // producer
         if (lane == 0) {
             int t = 0;
@@ -476,16 +476,18 @@ __global__ void __launch_bounds__(32 * (TJ + 1), SlabGeo<T, TJ, NS, NSLOT, AIR, 
             flags[1] = t;
         }
     } else {
-        // compute warps: owned cell (warp, lane), and halo cell x for the
-        // first NX threads (row TJ, then column TK)
-        const long long fs = 3 * g.vol * (long long)b, fstride = 3 * g.vol;  // field set b, then the next ones
+        // compute warps: TJ per field set; in field set m = warp / TJ, owned
+        // cell (row warp % TJ, lane), and halo cell x for the set's first NX
+        // threads (row TJ, then column TK)
+        const int m = warp / TJ, row = warp % TJ, lt = tid - 32 * TJ * m;
+        const long long fs = 3 * g.vol * (long long)(b + m);
         T* __restrict__ Eg = p.e_next + fs;
         T* __restrict__ Hg = p.h_next + fs;
-        const int jo = j0 + warp, ko = k0 + lane;
+        const int jo = j0 + row, ko = k0 + lane;
         const bool v_own = jo <= g.ny && ko <= g.nz;
-        const bool has_x = tid < NX;
-        const int rx = tid <= TK ? TJ : tid - TK - 1;
-        const int cx = tid <= TK ? tid : TK;
+        const bool has_x = lt < NX;
+        const int rx = lt <= TK ? TJ : lt - TK - 1;
+        const int cx = lt <= TK ? lt : TK;
         const int jx = j0 + rx, kx = k0 + cx;
         const bool v_x = has_x && jx <= g.ny && kx <= g.nz;
         // the last row / column of the grid with no tile of its own
@@ -502,15 +504,11 @@ __global__ void __launch_bounds__(32 * (TJ + 1), SlabGeo<T, TJ, NS, NSLOT, AIR, 
             if (t > 0 && ok) {
                 const unsigned char* st = smem + s * G::stage;
                 const unsigned char* stp = smem + ((t - 1) % NS) * G::stage;
-#pragma unroll
-                for (int m = 0; m < NB; ++m) {
-                    T* en = ring + ((t % 3) * NB + m) * 3 * G::cN;
-                    step_E<T, TJ, NS, NSLOT, AIR, CK, NB>(p, sl, st, stp, m, en, warp, lane, i, jo, ko, v_own && i < i1,
-                                                          Eg + m * fstride);
-                    if (has_x)
-                        step_E<T, TJ, NS, NSLOT, AIR, CK, NB>(p, sl, st, stp, m, en, rx, cx, i, jx, kx,
-                                                              own_x && i < i1, Eg + m * fstride);
-                }
+                T* en = ring + ((t % 3) * NB + m) * 3 * G::cN;
+                step_E<T, TJ, NS, NSLOT, AIR, CK, NB>(p, sl, st, stp, m, en, row, lane, i, jo, ko, v_own && i < i1, Eg);
+                if (has_x)
+                    step_E<T, TJ, NS, NSLOT, AIR, CK, NB>(p, sl, st, stp, m, en, rx, cx, i, jx, kx, own_x && i < i1,
+                                                          Eg);
             }
             tma::compute_barrier(NC);
             if (flags[0]) {
@@ -519,17 +517,12 @@ __global__ void __launch_bounds__(32 * (TJ + 1), SlabGeo<T, TJ, NS, NSLOT, AIR, 
             }
             if (t > 1) {
                 const unsigned char* stp = smem + ((t - 1) % NS) * G::stage;
-#pragma unroll
-                for (int m = 0; m < NB; ++m) {
-                    const T* enp = ring + (((t - 1) % 3) * NB + m) * 3 * G::cN;
-                    const T* enc = ring + ((t % 3) * NB + m) * 3 * G::cN;
-                    if (v_own)
-                        step_H<T, TJ, NS, NSLOT, AIR, CK, NB, false>(p, sl, stp, m, enp, enc, warp, lane, i - 1, jo, ko,
-                                                                     Hg + m * fstride);
-                    if (own_x)
-                        step_H<T, TJ, NS, NSLOT, AIR, CK, NB, true>(p, sl, stp, m, enp, enc, rx, cx, i - 1, jx, kx,
-                                                                    Hg + m * fstride);
-                }
+                const T* enp = ring + (((t - 1) % 3) * NB + m) * 3 * G::cN;
+                const T* enc = ring + ((t % 3) * NB + m) * 3 * G::cN;
+                if (v_own)
+                    step_H<T, TJ, NS, NSLOT, AIR, CK, NB, false>(p, sl, stp, m, enp, enc, row, lane, i - 1, jo, ko, Hg);
+                if (own_x)
+                    step_H<T, TJ, NS, NSLOT, AIR, CK, NB, true>(p, sl, stp, m, enp, enc, rx, cx, i - 1, jx, kx, Hg);
             }
             if (t > 0) {
                 __syncwarp();
@@ -718,7 +711,7 @@ struct SlabInfo {
         nb = NB;
         if constexpr (slab_fits<T, TJ, NS, 0, false, CK, NB>())
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ0, k_step_slab<T, TJ, NS, 0, false, CK, NB>,
-                                                          32 * (TJ + 1), SlabGeo<T, TJ, NS, 0, false, CK, NB>::smem);
+                                                          32 * (TJ * NB + 1), SlabGeo<T, TJ, NS, 0, false, CK, NB>::smem);
     }
 };
 
@@ -752,7 +745,7 @@ struct SlabLaunch {
         if constexpr (slab_fits<T, TJ, NS, NSLOT, AIR, CK, NB>()) {
             cudaLaunchConfig_t cfg{};
             cfg.gridDim = dim3((unsigned)n_units[q] * (a.B / NB));
-            cfg.blockDim = dim3(32 * (TJ + 1));
+            cfg.blockDim = dim3(32 * (TJ * NB + 1));
             cfg.dynamicSmemBytes = SlabGeo<T, TJ, NS, NSLOT, AIR, CK, NB>::smem;
             cfg.stream = streams[q];
             cudaLaunchAttribute at[1];
