@@ -281,6 +281,14 @@ int fitb_add_modal_port(fitb_handle* h, const fitb_modal_desc* d, int32_t* out_i
  * auto-extension :351-363).  One call per power-of-two length. */
 int fitb_set_dtbc_kernel(fitb_handle* h, int32_t port, int32_t mode,
                          int32_t n_kernel, const double* l);
+/* The same tables built on the device (per-request setup): every length
+ * n0, 2 n0, ... up to the first >= n_steps that is not set yet, from the
+ * mode's r and q given to fitb_add_modal_port.  The Laurent coefficients
+ * of the outgoing root are the inverse DFT of 8 n samples on the circle
+ * |z| = exp(4 / n) (dtbc.py:125-156), summed directly in float64 on the
+ * GPU: they agree with the reference's FFT to round-off, not bit for bit.
+ * FITB_ERR_ARG for a mode that is not DTBC. */
+int fitb_build_dtbc_kernel(fitb_handle* h, int32_t port, int32_t mode, int64_t n_steps);
 /* Excite mode `mode` of field set b with waveform samples
  * w[n] = waveform(n*dt), n = 0..n_samples-1 (zero beyond); mode = -1 clears
  * (operator.py:1140-1182 set_excitation / clear_excitation). */

@@ -140,6 +140,7 @@ SIGNATURES = {
     "fitb_push_lumped_samples": ([vp, i32, i32, i64, i64, cvp], C.c_int),
     "fitb_add_modal_port": ([vp, C.POINTER(FitbModalDesc), P_i32], C.c_int),
     "fitb_set_dtbc_kernel": ([vp, i32, i32, i32, P_f64], C.c_int),
+    "fitb_build_dtbc_kernel": ([vp, i32, i32, i64], C.c_int),
     "fitb_set_modal_source": ([vp, i32, i32, i32, i64, P_f64], C.c_int),
     "fitb_add_dft_monitor": ([vp, C.POINTER(FitbDftDesc), P_i32], C.c_int),
     "fitb_read_dft": ([vp, i32, i32, i32, P_f64, P_f64, sz], C.c_int),

@@ -171,6 +171,7 @@ struct ModalHost {
     DevBuf conv;  // DTBC convolution partials of the current step
     std::vector<std::vector<double>> ktabs;  // per mode: concatenated tables
     std::vector<int> n_tables_mode;
+    std::vector<double> dtbc_r, dtbc_q;      // per mode: the DTBC chain parameters
     DevBuf ktab[kMaxModes];
     std::vector<int> exc_host, buflen_host;
     std::vector<double> wf_host;  // [B][n_wf]
@@ -2048,6 +2049,8 @@ int fitb_add_modal_port(fitb_handle* h, const fitb_modal_desc* d, int32_t* out_i
     md.dt = H.dt;
     mp->n_tables_mode.assign((size_t)M, 0);
     mp->ktabs.assign((size_t)M, {});
+    mp->dtbc_r.assign((size_t)M, 0.0);
+    mp->dtbc_q.assign((size_t)M, 0.0);
     for (int m = 0; m < M; ++m) {
         md.mur_r[m] = d->mur_r[m];
         md.tau[m] = d->tau[m];
@@ -2057,6 +2060,8 @@ int fitb_add_modal_port(fitb_handle* h, const fitb_modal_desc* d, int32_t* out_i
             if (!d->dtbc_r || !d->dtbc_q) fail(FITB_ERR_ARG, "DTBC mode without r/q");
             md.r2[m] = d->dtbc_r[m] * d->dtbc_r[m];
             md.q2[m] = d->dtbc_q[m] * d->dtbc_q[m];
+            mp->dtbc_r[(size_t)m] = d->dtbc_r[m];
+            mp->dtbc_q[(size_t)m] = d->dtbc_q[m];
         } else {
             any_mur = true;
         }
@@ -2130,6 +2135,50 @@ int fitb_set_dtbc_kernel(fitb_handle* h, int32_t port, int32_t mode, int32_t n_k
     tab.insert(tab.end(), l, l + n_kernel);
     mp.n_tables_mode[(size_t)mode] += 1;
     fitb::upload(mp.ktab[mode], tab);
+    mp.dev.ktab[mode] = mp.ktab[mode].as<double>();
+    mp.dev.n_tables = *std::max_element(mp.n_tables_mode.begin(), mp.n_tables_mode.end());
+    H.port_tables_dirty = true;
+    fitb::invalidate_graphs(H);
+    FITB_CATCH
+}
+
+int fitb_build_dtbc_kernel(fitb_handle* h, int32_t port, int32_t mode, int64_t n_steps) {
+    FITB_TRY
+    Handle& H = H_of(h);
+    if (port < 0 || port >= (int)H.modal.size()) fail(FITB_ERR_ARG, "modal port %d does not exist", port);
+    fitb::ModalHost& mp = *H.modal[port];
+    if (mode < 0 || mode >= mp.n_modes || !mp.dev.is_dtbc[mode]) fail(FITB_ERR_ARG, "mode %d is not a DTBC mode", mode);
+    if (n_steps < 1) fail(FITB_ERR_ARG, "n_steps must be >= 1");
+    if (mp.dev.n0 < 2) fail(FITB_ERR_STATE, "the port's initial DTBC kernel length is unset");
+    // the tables a run of n_steps chain steps visits: n0, 2 n0, ... up to the
+    // first length >= n_steps (dtbc.py:351-363), those not yet set
+    std::vector<long long> lens;
+    for (long long L = mp.dev.n0;; L *= 2) {
+        lens.push_back(L);
+        if (L >= n_steps) break;
+    }
+    const size_t have = (size_t)mp.n_tables_mode[(size_t)mode];
+    if (have >= lens.size()) return FITB_OK;
+    if (lens.back() > (1LL << 26)) fail(FITB_ERR_LIMIT, "DTBC kernel of %lld entries", lens.back());
+    fitb::DevBuf x, l;
+    x.alloc((size_t)(8 * lens.back()) * sizeof(double2), false);
+    l.alloc((size_t)lens.back() * sizeof(double), false);
+    std::vector<double> host;
+    for (size_t t = have; t < lens.size(); ++t) {
+        const int n = (int)lens[t];
+        fitb::launch_dtbc_kernel(mp.dtbc_r[(size_t)mode], mp.dtbc_q[(size_t)mode], n, x.as<double2>(), l.as<double>(),
+                                 H.stream);
+        H.launches += 2;
+        ck(cudaGetLastError(), "DTBC kernel launch");
+        host.resize((size_t)n);
+        ck(cudaMemcpyAsync(host.data(), l.p, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, H.stream),
+           "DTBC kernel D2H");
+        ck(cudaStreamSynchronize(H.stream), "DTBC kernel sync");
+        auto& tab = mp.ktabs[(size_t)mode];
+        tab.insert(tab.end(), host.begin(), host.end());
+        mp.n_tables_mode[(size_t)mode] += 1;
+    }
+    fitb::upload(mp.ktab[mode], mp.ktabs[(size_t)mode]);
     mp.dev.ktab[mode] = mp.ktab[mode].as<double>();
     mp.dev.n_tables = *std::max_element(mp.n_tables_mode.begin(), mp.n_tables_mode.end());
     H.port_tables_dirty = true;

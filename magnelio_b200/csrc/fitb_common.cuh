@@ -455,6 +455,11 @@ void launch_setup_materials(const Geom& g, const double* dx, const double* dy, c
                             const double* cat1_eps, long long n_pec, const long long* pec_idx, T* aE, T* bE, T* aH,
                             T* bH, T* meps, T* mmu, double* coef_max, cudaStream_t s);
 
+// DTBC kernel table on the device (setup.cu): l_m, m < n, of the outgoing
+// root lambda(z) of the discrete Klein-Gordon chain with parameters r, q;
+// x is scratch of 8 n complex samples.
+void launch_dtbc_kernel(double r, double q, int n, double2* x, double* l, cudaStream_t s);
+
 // lambda_max of the live leapfrog update operator D^-1/2 C^T M_mu^-1 C D^-1/2
 // by a float64 Lanczos iteration (spectral.cu); 0 on success.
 template <typename T>

@@ -1,6 +1,9 @@
-// Material matrices and leapfrog coefficients built on the device from the
-// grid and the cell materials, for problems whose host would otherwise
-// compute and upload six float64 arrays of ~3 entries per cell.
+// Per-request setup on the device.
+//
+// Material matrices and leapfrog coefficients built from the grid and the
+// cell materials, for problems whose host would otherwise compute and
+// upload six float64 arrays of ~3 entries per cell.  And the DTBC kernel
+// tables of the modal ports (below).
 //
 // Reference: build_M_eps (src/magnelio/_operators/material_matrices.py
 // :334-464: cat-0 permittivity of the clamped owner cell times the edge's
@@ -173,7 +176,91 @@ __global__ void k_coef_max(long long vol, const T* aE, const T* bE, const T* aH,
 
 int grid_of(long long n) { return (int)std::min<long long>((n + 255) / 256, 148LL * 32); }
 
+// ---------------------------------------------------------------------------
+// DTBC kernel table (dtbc.py:91-156): l_m = rho^m Re(c_m), m < n, where
+// c_m = (1/N) sum_k lambda(z_k) e^{2 pi i k m / N} is the inverse DFT of the
+// outgoing root on N = 8 n points z_k = rho e^{2 pi i k / N} of the circle
+// rho = exp(4 / n).  The reference takes the inverse FFT of the N samples;
+// here each coefficient is one direct sum (N terms) in float64.
+
+struct Cx {
+    double re, im;
+};
+
+__device__ __forceinline__ Cx cx_mul(Cx a, Cx b) { return {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re}; }
+
+// principal square root by the scaled formula of Numerical Recipes (section
+// 5.5): t = sqrt((|a| + |w|) / 2), then the quotient for the other part
+__device__ __forceinline__ Cx cx_sqrt(Cx w) {
+    if (w.re == 0.0 && w.im == 0.0) return {0.0, 0.0};
+    const double t = sqrt(0.5 * (fabs(w.re) + hypot(w.re, w.im)));
+    if (w.re >= 0.0) return {t, w.im / (2.0 * t)};
+    return {fabs(w.im) / (2.0 * t), copysign(t, w.im)};
+}
+
+// lambda(z) of dtbc.py:91-122: A = 1 + (z - 2 + 1/z + q^2) / (2 r^2), the
+// root of A +- sqrt(A^2 - 1) of modulus <= 1
+__global__ void k_dtbc_samples(double r, double q, long long N, double rho, double2* x) {
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < N; k += (long long)gridDim.x * blockDim.x) {
+        double sn, cs;
+        sincospi(2.0 * (double)k / (double)N, &sn, &cs);
+        const Cx z{rho * cs, rho * sn};
+        const double zz = z.re * z.re + z.im * z.im;
+        const Cx iz{z.re / zz, -z.im / zz};
+        const double den = 2.0 * r * r;
+        const Cx A{1.0 + (z.re - 2.0 + iz.re + q * q) / den, (z.im + iz.im) / den};
+        const Cx A2 = cx_mul(A, A);
+        const Cx root = cx_sqrt({A2.re - 1.0, A2.im});
+        const Cx lm{A.re - root.re, A.im - root.im}, lp{A.re + root.re, A.im + root.im};
+        const Cx lam = hypot(lm.re, lm.im) <= hypot(lp.re, lp.im) ? lm : lp;
+        x[k] = make_double2(lam.re, lam.im);
+    }
+}
+
+// one CTA per coefficient m: thread t sums its contiguous run of k with a
+// rotated phasor restarted from sincospi every kRestart terms, then a fixed
+// reduction order (warp tree, then warps in order)
+constexpr int kDftThreads = 256, kRestart = 32;
+
+__global__ void __launch_bounds__(kDftThreads) k_dtbc_coeffs(const double2* __restrict__ x, long long N, double rho,
+                                                              double* __restrict__ l) {
+    const int m = blockIdx.x;
+    const long long per = (N + kDftThreads - 1) / kDftThreads;
+    const long long k0 = threadIdx.x * per, k1 = min(N, k0 + per);
+    double sw, cw;
+    sincospi(2.0 * (double)(m % N) / (double)N, &sw, &cw);  // e^{2 pi i m / N}
+    double acc = 0.0;
+    for (long long kb = k0; kb < k1; kb += kRestart) {
+        double sn, cs;
+        sincospi(2.0 * (double)((kb * (long long)m) % N) / (double)N, &sn, &cs);
+        const long long ke = min(k1, kb + kRestart);
+        for (long long k = kb; k < ke; ++k) {
+            const double2 v = x[k];
+            acc += v.x * cs - v.y * sn;  // Re(x_k e^{i theta_k m})
+            const double c2 = cs * cw - sn * sw, s2 = sn * cw + cs * sw;
+            cs = c2;
+            sn = s2;
+        }
+    }
+    __shared__ double ws[kDftThreads / 32];
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double a = 0.0;
+        for (int w = 0; w < kDftThreads / 32; ++w) a += ws[w];
+        l[m] = (a * (1.0 / (double)N)) * pow(rho, (double)m);
+    }
+}
+
 }  // namespace
+
+void launch_dtbc_kernel(double r, double q, int n, double2* x, double* l, cudaStream_t s) {
+    const long long N = 8LL * n;
+    const double rho = exp(4.0 / (double)n);
+    k_dtbc_samples<<<grid_of(N), 256, 0, s>>>(r, q, N, rho, x);
+    k_dtbc_coeffs<<<n, kDftThreads, 0, s>>>(x, N, rho, l);
+}
 
 template <typename T>
 void launch_setup_materials(const Geom& g, const double* dx, const double* dy, const double* dz, const int* mat,

@@ -362,6 +362,12 @@ class FitEngine:
         k = _f64(kernel)
         check(self._lib.fitb_set_dtbc_kernel(self._h, int(port), int(mode), int(k.size), f64p(k)))
 
+    def build_dtbc_kernel(self, port: int, mode: int, n_steps: int) -> None:
+        """DTBC kernel tables of ``mode`` for a run of ``n_steps`` chain steps,
+        built on the device from the mode's r and q (the device form of
+        :func:`magnelio_b200.host.dtbc_tables`)."""
+        check(self._lib.fitb_build_dtbc_kernel(self._h, int(port), int(mode), int(n_steps)))
+
     def set_modal_source(self, port: int, b: int, mode: int, samples=None) -> None:
         w = None if samples is None else _f64(samples)
         check(

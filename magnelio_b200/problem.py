@@ -63,6 +63,9 @@ class ModalPort:
     dtbc_n_kernel_init: int = 4096
     # {mode: [table n0, table 2 n0, ...]}
     dtbc_kernels: dict = field(default_factory=dict)
+    # > 0: the DTBC modes without host tables get theirs built on the
+    # device for a run of this many steps (fitb_build_dtbc_kernel)
+    dtbc_device_steps: int = 0
     complement: tuple | None = None  # (r, live)
     # per field set: (mode or -1, samples w[n] = waveform(n dt))
     excitation: list = field(default_factory=list)
@@ -235,6 +238,10 @@ class FitProblem:
                 for m, tables in sorted(mp.dtbc_kernels.items()):
                     for t in tables:
                         eng.set_dtbc_kernel(pid, int(m), t)
+                if mp.dtbc_device_steps > 0:
+                    for m in range(mp.n_modes):
+                        if int(mp.is_dtbc[m]) and m not in mp.dtbc_kernels:
+                            eng.build_dtbc_kernel(pid, m, mp.dtbc_device_steps)
                 for b, exc in enumerate(mp.excitation):
                     if exc is not None and exc[0] >= 0:
                         eng.set_modal_source(pid, b, int(exc[0]), exc[1])

@@ -239,6 +239,42 @@ def test_matches_oracle_beyond_fixture_length():
     assert _rel(V, np.array(ref.V)) < F64_TOL
 
 
+def test_dtbc_tables_built_on_the_device_match_the_host_tables():
+    """DTBC kernel tables built on the device (inverse DFT of the outgoing
+    root on the rho-circle, float64) in place of the host FFT's: the float64
+    march past the 512-sample kernel (so two table lengths) agrees with the
+    host-table run and with the float64 oracle to round-off."""
+    from oracle.fit_oracle import OracleRun
+    from magnelio_b200 import host
+
+    steps = 700
+    runs = {}
+    for where in ("host", "device"):
+        p, d, n = load_golden("wg_mur")
+        for mp in p.modal:
+            for m in list(mp.dtbc_kernels):
+                if where == "host":
+                    mp.dtbc_kernels[m] = host.dtbc_tables(float(mp.dtbc_r[m]), float(mp.dtbc_q[m]),
+                                                          mp.dtbc_n_kernel_init, steps)
+                else:
+                    del mp.dtbc_kernels[m]
+            if where == "device":
+                mp.dtbc_device_steps = steps
+            mp.excitation = [(mp.excitation[0][0], np.concatenate([mp.excitation[0][1], np.zeros(steps)]))] \
+                if mp.excitation[0] else mp.excitation
+        assert any(int(np.sum(mp.is_dtbc)) for mp in p.modal)
+        with p.build_engine("double") as eng:
+            eng.step(steps)
+            runs[where] = (*eng.read_fields(), *eng.read_vi())
+        if where == "host":
+            ref = OracleRun(p).run(steps)
+    (eh, hh, Vh, Ih), (ed, hd, Vd, Id) = runs["host"], runs["device"]
+    assert _rel(ed, eh, ref.peak_e) < 1e-12 and _rel(hd, hh, ref.peak_h) < 1e-12
+    assert _rel(Vd, Vh) < 1e-12 and _rel(Id, Ih) < 1e-12
+    assert _rel(ed, ref.f.e, ref.peak_e) < F64_TOL
+    assert _rel(Vd, np.array(ref.V)) < F64_TOL
+
+
 def test_missing_dtbc_table_is_an_error_not_a_fault():
     from magnelio_b200._lib import FitbError
 
