@@ -309,6 +309,23 @@ int fitb_add_dispersion_block(fitb_handle* h, int32_t side, int64_t n_states, co
                               const double* k_re, const double* k_im, const double* c_re,
                               const double* c_im, const double* weight);
 
+/* ---- surface-impedance walls ---------------------------------------- */
+/* One SIBC wall tag (solver/_sibc.py:88-264, hooks at fit_td.py:837-840 and
+ * :909-914): n_faces flat indices into the reference H vector with their
+ * geometry factor g = A / l_dual^2, and per Foster branch of the wall's
+ * impedance fit k = (1 - b dt/2)/(1 + b dt/2), q = c b dt/(1 + b dt/2).
+ * The instantaneous part g R_inst must already be folded into the H
+ * coefficients (the reference folds it into M_sigma_m).  Each step stashes
+ * h on the faces first, then, right after the H update and the mu-side ADE
+ * and before the H-side CPML corrections, adds beta_H g sum_p
+ * ((1 + k_p)/2) u_p (every wall in order, so a face two walls book takes
+ * both terms in wall order) and advances u_p <- k_p u_p + q_p h_mid with
+ * h_mid the mean of the stashed and the new h.  Blocks of one handle are
+ * kept in the order added; before the first step; in-place stencil modes
+ * only (FITB_ERR_STATE in the fused forms). */
+int fitb_add_sibc_block(fitb_handle* h, int64_t n_faces, const int64_t* idx, const double* g, int32_t n_branches,
+                        const double* k, const double* q);
+
 /* ---- plane waves ---------------------------------------------------- */
 /* Replaces PlaneWaveSource.attach / inject_E / inject_H (plane_wave.py:229,
  * :720-733; called from fit_td.py:964-967, :990-993). */

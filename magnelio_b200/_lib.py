@@ -115,6 +115,7 @@ class FitbPlaneWaveDesc(C.Structure):
 SIGNATURES = {
     "fitb_abi_version": ([], C.c_int),
     "fitb_add_plane_wave": ([vp, C.POINTER(FitbPlaneWaveDesc), P_i32], C.c_int),
+    "fitb_add_sibc_block": ([vp, C.c_int64, P_i64, P_f64, i32, P_f64, P_f64], C.c_int),
     "fitb_add_dispersion_block": ([vp, i32, C.c_int64, P_i64, P_f64, i32, P_i32, P_f64, P_f64, P_f64, P_f64, P_f64],
                                   C.c_int),
     "fitb_set_plane_wave_scale": ([vp, i32, i32, C.c_double], C.c_int),

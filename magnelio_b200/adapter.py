@@ -8,8 +8,9 @@ the modal / lumped port operators and the field monitors.  The engine then
 owns all evolving state on the device.  Supported per-step hooks are the
 ones on the FIT-TD hot path: PEC / PMC / CPML boundaries, modal
 (Mur / DTBC / complement absorber) and series-RLC lumped ports, running-DFT
-field monitors.  Anything else raises ``NotImplementedError`` instead of
-being silently skipped.
+field monitors, TF/SF plane waves, ADE dispersion on both sides and
+surface-impedance (SIBC) walls.  Anything else raises
+``NotImplementedError`` instead of being silently skipped.
 """
 
 from __future__ import annotations
@@ -18,7 +19,7 @@ import numpy as np
 
 from magnelio_b200 import host
 from magnelio_b200.problem import (
-    CpmlFace, DftMonitor, Dispersion, DispersionBlock, FitProblem, LumpedPort, ModalPort, PlaneWave,
+    CpmlFace, DftMonitor, Dispersion, DispersionBlock, FitProblem, LumpedPort, ModalPort, PlaneWave, SibcBlock,
 )
 
 _FACE_EDGES = {
@@ -87,8 +88,6 @@ def problem_from_solver(solver, n_steps: int) -> FitProblem:
     s = solver
     if s._fields is None:
         raise RuntimeError("problem_from_solver needs a solver after setup()")
-    if s._sibc is not None:
-        raise NotImplementedError("SIBC walls are not on the device engine yet")
     grid = s.mesh.grid
     nx, ny, nz = s.mesh.Nx, s.mesh.Ny, s.mesh.Nz
     dt = float(s.dt)
@@ -163,11 +162,25 @@ def problem_from_solver(solver, n_steps: int) -> FitProblem:
     for side, op in (("E", s._dispersion), ("H", s._dispersion_mu)):
         if op is not None:
             prob.dispersion.append(_dispersion_from_op(op, side))
+    if s._sibc is not None:
+        prob.sibc = _sibc_from_op(s._sibc)
     for src in s.sources:
         prob.plane_waves.append(_plane_wave_from_src(src, s))
     prob.e0 = [np.array(_np(s._fields.e_flat), dtype=np.float64)]
     prob.h0 = [np.array(_np(s._fields.h_flat), dtype=np.float64)]
     return prob
+
+
+def _sibc_from_op(op) -> list:
+    """Wall faces, geometry factors and branch constants of a bound
+    ``SIBCOperator`` (``solver/_sibc.py:88-191``), walls in its order; the
+    instantaneous part is already in the solver's ``alpha_H`` / ``beta_H``."""
+    out = []
+    for b in op.blocks:
+        out.append(SibcBlock(idx=np.asarray(_np(b.idx), np.int64), g=np.asarray(_np(b.g), float),
+                             k=np.array([br.k for br in b.branches], float),
+                             q=np.array([br.q for br in b.branches], float)))
+    return out
 
 
 def _dispersion_from_op(op, side) -> Dispersion:

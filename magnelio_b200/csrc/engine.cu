@@ -154,6 +154,16 @@ struct DispHost {
     bool present() const { return !off.empty(); }
 };
 
+struct SibcHost {
+    SibcDev dev{};
+    std::vector<long long> off, slot;
+    std::vector<double> g, k, q, hopk;
+    std::vector<int> state_block, br_start{0};
+    long long n_slots = 0;
+    DevBuf d_off, d_g, d_state_block, d_slot, d_u, d_hprev, d_br_start, d_k, d_q, d_hopk, d_uoff, d_ustart, d_ustate;
+    bool present() const { return !off.empty(); }
+};
+
 struct PlaneWaveHost {
     PlaneWaveDev dev{};
     DevBuf e_off, e_start, e_coef, e_delay, h_off, h_start, h_coef, h_delay, scale;
@@ -231,6 +241,7 @@ struct Handle {
     std::vector<std::unique_ptr<DftHost>> dft;
     std::vector<std::unique_ptr<PlaneWaveHost>> pws;
     DispHost disp[2];  // E side, H side
+    SibcHost sibc;     // surface-impedance walls (H side)
     DevBuf d_lumped, d_modal, d_dft;
     int dft_stage_blocks = 0, dft_flush_blocks = 0;
     size_t dft_flush_smem = 0;
@@ -416,6 +427,12 @@ size_t device_bytes(const Handle& H) {
                                 &D.d_kind, &D.d_k_re, &D.d_k_im, &D.d_c_re, &D.d_c_im, &D.d_opk_re, &D.d_opk_im,
                                 &D.d_hw, &D.d_uoff, &D.d_ustart, &D.d_ustate})
             n += d->bytes;
+    {
+        const SibcHost& S = H.sibc;
+        for (const DevBuf* d : {&S.d_off, &S.d_g, &S.d_state_block, &S.d_slot, &S.d_u, &S.d_hprev, &S.d_br_start,
+                                &S.d_k, &S.d_q, &S.d_hopk, &S.d_uoff, &S.d_ustart, &S.d_ustate})
+            n += d->bytes;
+    }
     return n;
 }
 
@@ -807,7 +824,7 @@ void plan_stencil(Handle& H) {
 template <typename T>
 void launch_half(Handle& H, int which) {
     StencilArgs<T> sa = stencil_args<T>(H);
-    if (H.disp[which].present()) sa.nfaces = 0;
+    if (H.disp[which].present() || (which == 1 && H.sibc.present())) sa.nfaces = 0;
     switch (H.stencil_mode) {
         case kModeStream:
             launch_stream_half<T>(sa, H.splan, H.stream_variant, which, H.stream);
@@ -897,11 +914,20 @@ void launch_stencil_half(Handle& H, int which) {
 // fit_td.py:833-874).  Returns the launches issued.
 template <typename T>
 int disp_complete(Handle& H, int sd) {
-    if (!H.disp[sd].present()) return 0;
+    const bool sibc = sd == 1 && H.sibc.present();
+    if (!H.disp[sd].present() && !sibc) return 0;
     T* F = (sd == 0 ? H.Ec() : H.Hc()).as<T>();
     const T* beta = (sd == 0 ? H.bE : H.bH).as<T>();
-    launch_disp_update<T>(F, H.e_block(), H.B, beta, H.disp[sd].dev, H.stream);
-    int n = 2;
+    int n = 0;
+    if (H.disp[sd].present()) {
+        launch_disp_update<T>(F, H.e_block(), H.B, beta, H.disp[sd].dev, H.stream);
+        n += 2;
+    }
+    // the SIBC walls after the mu-side ADE (fit_td.py:903-914)
+    if (sibc) {
+        launch_sibc_update<T>(F, H.e_block(), H.B, beta, H.sibc.dev, H.stream);
+        n += 2;
+    }
     StencilArgs<T> sa = stencil_args<T>(H);
     for (int q = 0; q < sa.nfaces; ++q) {
         launch_cpml_pass<T>(sa, q, sd, H.stream);
@@ -1008,6 +1034,10 @@ int enqueue_step(Handle& H) {
     for (int sd = 0; sd < 2; ++sd) {
         if (!H.disp[sd].present()) continue;
         launch_disp_save<T>((sd == 0 ? H.Ec() : H.Hc()).as<T>(), H.e_block(), H.B, H.disp[sd].dev, H.stream);
+        ++n;
+    }
+    if (H.sibc.present()) {
+        launch_sibc_save<T>(H.Hc().as<T>(), H.e_block(), H.B, H.sibc.dev, H.stream);
         ++n;
     }
     launch_half<T>(H, 0);
@@ -1317,6 +1347,7 @@ void write_state(Handle& H, Writer& w) {
         dev_get(w, ps.p, ps.bytes);
     }
     for (auto& dp : H.disp) dev_get(w, dp.d_J.p, dp.d_J.bytes);
+    dev_get(w, H.sibc.d_u.p, H.sibc.d_u.bytes);
     for (auto& lp : H.lumped) dev_get(w, lp->st.p, lp->st.bytes);
     for (auto& mp : H.modal) {
         dev_get(w, mp->st.p, mp->st.bytes);
@@ -1382,6 +1413,7 @@ void read_state(Handle& H, Reader& r) {
         r.dev(ps.p, ps.bytes);
     }
     for (auto& dp : H.disp) r.dev(dp.d_J.p, dp.d_J.bytes);
+    r.dev(H.sibc.d_u.p, H.sibc.d_u.bytes);
     for (auto& lp : H.lumped) r.dev(lp->st.p, lp->st.bytes);
     for (auto& mp : H.modal) {
         r.dev(mp->st.p, mp->st.bytes);
@@ -1744,6 +1776,7 @@ int fitb_configure_stencil(fitb_handle* h, int32_t kind, int32_t variant, int32_
         fail(FITB_ERR_ARG, "vec stencil: variant %d / batch %d", variant, H.B);
     if (kind == fitb::kModeFused) {
         if (!fitb::fused_variant_ok(H.prec, variant)) fail(FITB_ERR_ARG, "fused variant %d", variant);
+        if (H.sibc.present()) fail(FITB_ERR_STATE, "SIBC walls need an in-place stencil mode");
         if ((H.disp[0].present() || H.disp[1].present()) && !fitb::is_slab_variant(variant))
             fail(FITB_ERR_STATE,
                  "dispersive materials need an in-place stencil mode or the slab step (fused 16-25)");
@@ -2310,6 +2343,86 @@ int fitb_add_dispersion_block(fitb_handle* h, int32_t side, int64_t n_states, co
     dv.uoff = D.d_uoff.as<long long>();
     dv.ustart = D.d_ustart.as<int>();
     dv.ustate = D.d_ustate.as<long long>();
+    fitb::invalidate_graphs(H);
+    FITB_CATCH
+}
+
+int fitb_add_sibc_block(fitb_handle* h, int64_t n_faces, const int64_t* idx, const double* g, int32_t n_branches,
+                        const double* k, const double* q) {
+    FITB_TRY
+    Handle& H = H_of(h);
+    if (n_faces < 1 || !idx || !g || n_branches < 0 || (n_branches > 0 && (!k || !q)))
+        fail(FITB_ERR_ARG, "SIBC block needs faces, their g and the branch constants");
+    if (H.steps_done != 0) fail(FITB_ERR_STATE, "SIBC walls must be added before the first step");
+    if (H.stencil_mode == fitb::kModeFused) fail(FITB_ERR_STATE, "SIBC walls need an in-place stencil mode");
+    const long long nh = H.nH();
+    for (int64_t s = 0; s < n_faces; ++s)
+        if (idx[s] < 0 || idx[s] >= nh) fail(FITB_ERR_ARG, "SIBC face index %lld out of range", (long long)idx[s]);
+    fitb::SibcHost& S = H.sibc;
+    const int blk = (int)S.br_start.size() - 1;
+    for (int p = 0; p < n_branches; ++p) {
+        S.k.push_back(k[p]);
+        S.q.push_back(q[p]);
+        S.hopk.push_back(0.5 * (1.0 + k[p]));
+    }
+    S.br_start.push_back(S.br_start.back() + n_branches);
+    for (int64_t f = 0; f < n_faces; ++f) {
+        S.off.push_back(H.flat_to_off(true, idx[f]));
+        S.g.push_back(g[f]);
+        S.state_block.push_back(blk);
+        S.slot.push_back(S.n_slots);
+        S.n_slots += n_branches;
+    }
+    // faces booked by several walls take their terms in wall order
+    const long long ns = (long long)S.off.size();
+    std::vector<long long> order((size_t)ns);
+    for (long long t = 0; t < ns; ++t) order[(size_t)t] = t;
+    std::stable_sort(order.begin(), order.end(), [&](long long a, long long b) { return S.off[(size_t)a] < S.off[(size_t)b]; });
+    std::vector<long long> uoff, ustate;
+    std::vector<int> ustart;
+    for (size_t r = 0; r < order.size(); ++r) {
+        const long long st = order[r];
+        if (r == 0 || S.off[(size_t)st] != uoff.back()) {
+            uoff.push_back(S.off[(size_t)st]);
+            ustart.push_back((int)ustate.size());
+        }
+        ustate.push_back(st);
+    }
+    ustart.push_back((int)ustate.size());
+    fitb::upload(S.d_off, S.off);
+    if (H.prec == 4)
+        fitb::upload(S.d_g, fitb::cast_vec<float>(S.g.data(), ns));
+    else
+        fitb::upload(S.d_g, S.g);
+    fitb::upload(S.d_state_block, S.state_block);
+    fitb::upload(S.d_slot, S.slot);
+    fitb::upload(S.d_br_start, S.br_start);
+    // zero-length tables still get a valid pointer
+    fitb::upload(S.d_k, S.k.empty() ? std::vector<double>(1, 0.0) : S.k);
+    fitb::upload(S.d_q, S.q.empty() ? std::vector<double>(1, 0.0) : S.q);
+    fitb::upload(S.d_hopk, S.hopk.empty() ? std::vector<double>(1, 0.0) : S.hopk);
+    fitb::upload(S.d_uoff, uoff);
+    fitb::upload(S.d_ustart, ustart);
+    fitb::upload(S.d_ustate, ustate);
+    S.d_u.alloc((size_t)H.B * std::max<long long>(S.n_slots, 1) * H.esz);
+    S.d_hprev.alloc((size_t)H.B * ns * H.esz);
+    fitb::SibcDev& dv = S.dev;
+    dv.n_states = ns;
+    dv.off = S.d_off.as<long long>();
+    dv.g = S.d_g.p;
+    dv.state_block = S.d_state_block.as<int>();
+    dv.slot = S.d_slot.as<long long>();
+    dv.n_slots = S.n_slots;
+    dv.u = S.d_u.p;
+    dv.hprev = S.d_hprev.p;
+    dv.br_start = S.d_br_start.as<int>();
+    dv.k = S.d_k.as<double>();
+    dv.q = S.d_q.as<double>();
+    dv.hopk = S.d_hopk.as<double>();
+    dv.n_unique = (long long)uoff.size();
+    dv.uoff = S.d_uoff.as<long long>();
+    dv.ustart = S.d_ustart.as<int>();
+    dv.ustate = S.d_ustate.as<long long>();
     fitb::invalidate_graphs(H);
     FITB_CATCH
 }

@@ -396,6 +396,29 @@ template <typename T>
 void launch_disp_save(const T* F, long long blk, int B, const DispDev& d, cudaStream_t s);
 template <typename T>
 void launch_disp_update(T* F, long long blk, int B, const T* beta, const DispDev& d, cudaStream_t s);
+// Surface-impedance walls on the H faces (sibc.cu; solver/_sibc.py).
+struct SibcDev {
+    long long n_states;          // faces of all walls
+    const long long* off;        // [n_states] H entry offset in a field set's block
+    const void* g;               // [n_states] field dtype
+    const int* state_block;      // [n_states] wall of the face
+    const long long* slot;       // [n_states] first branch state in a field set's u
+    long long n_slots;           // branch states per field set
+    void* u;                     // [B][n_slots] field dtype
+    void* hprev;                 // [B][n_states] field dtype
+    const int* br_start;         // [n_blocks + 1] into the branch tables
+    const double *k, *q, *hopk;  // [n_branches]: k, q, (1 + k) / 2
+    long long n_unique;          // distinct faces
+    const long long* uoff;       // [n_unique]
+    const int* ustart;           // [n_unique + 1] into ustate
+    const long long* ustate;     // faces of each entry, wall order
+};
+
+template <typename T>
+void launch_sibc_save(const T* h, long long blk, int B, const SibcDev& d, cudaStream_t s);
+template <typename T>
+void launch_sibc_update(T* h, long long blk, int B, const T* beta, const SibcDev& d, cudaStream_t s);
+
 // CPML face q of the stencil args as a separate pass; side 0 = E, 1 = H.
 template <typename T>
 void launch_cpml_pass(const StencilArgs<T>& a, int q, int side, cudaStream_t s);

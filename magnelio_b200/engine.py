@@ -410,6 +410,18 @@ class FitEngine:
             self._h, 0 if side == "E" else 1, int(idx.size), i64p(idx), f64p(g), int(kind.size), i32p(kind),
             *[f64p(x) for x in parts], f64p(w)))
 
+    def add_sibc_block(self, block) -> None:
+        """Upload one surface-impedance wall (:class:`magnelio_b200.problem.SibcBlock`):
+        its driving H faces, geometry factors and Foster-branch constants."""
+        idx = np.ascontiguousarray(block.idx, dtype=np.int64)
+        g = np.ascontiguousarray(block.g, dtype=np.float64)
+        k = np.ascontiguousarray(block.k, dtype=np.float64)
+        q = np.ascontiguousarray(block.q, dtype=np.float64)
+        if idx.size != g.size or k.size != q.size:
+            raise ValueError("SIBC block: idx / g or k / q differ in length")
+        check(self._lib.fitb_add_sibc_block(self._h, int(idx.size), i64p(idx), f64p(g), int(k.size), f64p(k),
+                                            f64p(q)))
+
     def add_plane_wave(self, pw) -> int:
         """Upload a TF/SF plane wave (:class:`magnelio_b200.problem.PlaneWave`):
         its ordered E and H face patches and waveform constants."""

@@ -121,6 +121,32 @@ class DispersionBlock:
 
 
 @dataclass
+class SibcBlock:
+    """Surface-impedance wall of one tag (``solver/_sibc.py:88-111``): flat
+    H indices of its driving faces, the geometry factor ``g = A / l_dual^2``
+    per face, and per Foster branch of the impedance fit
+    ``k = (1 - b dt/2)/(1 + b dt/2)`` and ``q = c b dt/(1 + b dt/2)``.  The
+    instantaneous part ``g R_inst`` is folded into ``alpha_H`` / ``beta_H``
+    (as the reference folds it into ``M_sigma_m``)."""
+
+    idx: np.ndarray
+    g: np.ndarray
+    k: np.ndarray
+    q: np.ndarray
+
+
+def sibc_branch_constants(b, c, dt: float):
+    """``(k, q)`` of Foster branches ``c s / (s + b)`` at time step ``dt``
+    (``solver/_sibc.py:93-96``), and the instantaneous resistance
+    ``R_inst = c0 + sum c / (1 + b dt/2)`` is left to the caller."""
+    b = np.asarray(b, dtype=float)
+    c = np.asarray(c, dtype=float)
+    k = np.array([(1.0 - bp * dt / 2.0) / (1.0 + bp * dt / 2.0) for bp in b])
+    q = np.array([cp * bp * dt / (1.0 + bp * dt / 2.0) for bp, cp in zip(b, c)])
+    return k, q
+
+
+@dataclass
 class MaterialSetup:
     """The inputs of a lossless, non-magnetic problem's material matrices,
     for building them on the device (``FitEngine.build_materials``) instead
@@ -191,6 +217,7 @@ class FitProblem:
     monitors: list = field(default_factory=list)
     plane_waves: list = field(default_factory=list)
     dispersion: list = field(default_factory=list)
+    sibc: list = field(default_factory=list)  # SibcBlock, in the reference's wall-tag order
     batch: int = 1
     e0: list = field(default_factory=list)  # per field set initial e (or empty)
     h0: list = field(default_factory=list)
@@ -258,6 +285,8 @@ class FitProblem:
             for dsp in self.dispersion:
                 for bl in dsp.blocks:
                     eng.add_dispersion_block(dsp.side, bl)
+            for sb in self.sibc:
+                eng.add_sibc_block(sb)
             for pw in self.plane_waves:
                 wid = eng.add_plane_wave(pw)
                 for b, sc in enumerate(pw.scale):
@@ -343,6 +372,10 @@ class FitProblem:
             for r, bl in enumerate(dsp.blocks):
                 for k in ("idx", "g", "kind", "k", "c", "weight"):
                     put(f"disp{q}.b{r}.{k}", getattr(bl, k))
+        put("n_sibc", len(self.sibc))
+        for q, sb in enumerate(self.sibc):
+            for k in ("idx", "g", "k", "q"):
+                put(f"sibc{q}.{k}", getattr(sb, k))
         put("n_pw", len(self.plane_waves))
         for q, pw in enumerate(self.plane_waves):
             put(f"pw{q}.waveform", ["gaussian", "sine"].index(pw.waveform))
@@ -413,6 +446,8 @@ class FitProblem:
                 dsp.blocks.append(DispersionBlock(**{k: g(f"disp{q}.b{r}.{k}") for k in
                                                      ("idx", "g", "kind", "k", "c", "weight")}))
             p.dispersion.append(dsp)
+        for q in range(int(g("n_sibc", 0))):
+            p.sibc.append(SibcBlock(**{k: g(f"sibc{q}.{k}") for k in ("idx", "g", "k", "q")}))
         for q in range(int(g("n_pw", 0))):
             kw = {k: g(f"pw{q}.{k}") for k in ("e_idx", "e_coef", "e_delay", "e_splits", "h_idx", "h_coef", "h_delay",
                                                "h_splits")}

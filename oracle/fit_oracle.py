@@ -486,6 +486,42 @@ class DispersionOracle:
 
 
 # ---------------------------------------------------------------------------
+# Surface-impedance walls (solver/_sibc.py:114-264)
+# ---------------------------------------------------------------------------
+class SibcOracle:
+    """Foster-branch states of every SIBC wall on its driving H faces.
+    ``save`` stashes h on the faces at the top of a step (:213-218);
+    ``update`` runs right after the H update and the mu-side ADE, before the
+    H-side CPML (fit_td.py:903-914): every wall first adds
+    ``beta (g sum_p ((1 + k_p)/2) u_p)``, then every wall advances
+    ``u_p <- k_p u_p + q_p (h + h_prev)/2`` (:220-249)."""
+
+    def __init__(self, blocks):
+        self.blocks = [(sb, [np.zeros(np.asarray(sb.idx).size) for _ in np.asarray(sb.k)],
+                        np.zeros(np.asarray(sb.idx).size)) for sb in blocks]
+
+    def save(self, h):
+        for sb, _, hp in self.blocks:
+            hp[:] = h[sb.idx]
+
+    def update(self, h, beta):
+        for sb, U, _ in self.blocks:
+            hist = None
+            for p, u in enumerate(U):
+                term = (0.5 * (1.0 + float(sb.k[p]))) * u
+                hist = term if hist is None else hist + term
+            if hist is not None:
+                h[sb.idx] = h[sb.idx] + beta[sb.idx] * (np.asarray(sb.g, float) * hist)
+        for sb, U, hp in self.blocks:
+            if not U:
+                continue
+            h_mid = 0.5 * (h[sb.idx] + hp)
+            for p, u in enumerate(U):
+                u *= float(sb.k[p])
+                u += float(sb.q[p]) * h_mid
+
+
+# ---------------------------------------------------------------------------
 # TF/SF plane wave (sources/plane_wave.py:709-733)
 # ---------------------------------------------------------------------------
 class PlaneWaveOracle:
@@ -554,6 +590,7 @@ class OracleRun:
         self.pws = [PlaneWaveOracle(pw, pw.scale[b] if b < len(pw.scale) else 1.0)
                     for pw in getattr(prob, "plane_waves", [])]
         self.disp = {d.side: DispersionOracle(d) for d in getattr(prob, "dispersion", [])}
+        self.sibc = SibcOracle(getattr(prob, "sibc", [])) if getattr(prob, "sibc", []) else None
         self.n = 0
         self.V = []
         self.I = []
@@ -568,6 +605,8 @@ class OracleRun:
             self.disp["E"].save(f.e)
         if "H" in self.disp:
             self.disp["H"].save(f.h)
+        if self.sibc is not None:
+            self.sibc.save(f.h)
         update_E(f, self.aE, self.bE)
         if "E" in self.disp:
             self.disp["E"].update(f.e, self.bE)
@@ -594,6 +633,8 @@ class OracleRun:
         update_H(f, self.aH, self.bH)
         if "H" in self.disp:
             self.disp["H"].update(f.h, self.bH)
+        if self.sibc is not None:
+            self.sibc.update(f.h, self.bH)
         for c in self.cpml:
             c.update_H(f, self.bH)
         for pw in self.pws:

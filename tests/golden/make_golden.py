@@ -210,6 +210,50 @@ def case_dispersive_box():
           "Lorentz slab through the CPML, Debye block, mu-Debye block; TF/SF plane wave")
 
 
+def case_sibc_box():
+    """Surface-impedance walls: a copper brick inside a box with PEC walls on
+    y and z (both booked as SIBC walls of copper) and CPML on x, so that the
+    wall faces next to the absorber slabs take the SIBC history before the
+    H-side CPML; impedance fits over 1-100 GHz; random initial fields."""
+    from magnelio.boundaries.cpml import CPMLBoundary
+    from magnelio.boundaries.pec import PECBoundary
+    from magnelio.materials.material import Material
+    from magnelio.materials.surface_impedance import fit_wall_impedances
+    from magnelio.mesh._surfaces import enumerate_sibc_surfaces, resolve_wall_conductors
+    from magnelio.mesh.mesher import Mesh
+    from magnelio.solver._sibc import SIBCSpec
+    from magnelio.solver.fit_td import FITTimeDomainSolver
+    from magnelio.solver.stability import courant_dt
+
+    rng = np.random.default_rng(41)
+    grid = _grid(rng, (12, 10, 14))
+    L = (grid.x[-1], grid.y[-1], grid.z[-1])
+    cu = Material.lossy_metal("cu", sigma=5.8e7)
+    regions = [(cu, (0.45 * L[0], 0.3 * L[1], 0.35 * L[2], 0.6 * L[0], 0.65 * L[1], 0.6 * L[2]))]
+    walls = ("ymin", "ymax", "zmin", "zmax")
+    bc_types = {f: ("CPML" if f in ("xmin", "xmax") else "PEC") for f in FACES}
+    mesh = Mesh.from_grid(grid, regions=regions, boundary_conditions=bc_types)
+    surfs = enumerate_sibc_surfaces(mesh, bc_pec_faces=walls)
+    resolved = resolve_wall_conductors(mesh, surfs, sigma=5.8e7)
+    fits = fit_wall_impedances(resolved, 1e9, 1e11)
+    spec = SIBCSpec(surfaces=tuple(surfs), fits=fits)
+    bcs = {f: CPMLBoundary(f, grid, thickness_cells=3) for f in ("xmin", "xmax")}
+    bcs.update({f: PECBoundary(f) for f in walls})
+    n = 120
+    s = FITTimeDomainSolver(mesh=mesh, boundary_conditions=bcs, total_time_steps=n, dt=courant_dt(grid, "normal"),
+                            verbose=False, backend="numpy", precision="double", sibc=spec)
+    s.setup()
+    assert s._sibc is not None and any(b.branches for b in s._sibc.blocks)
+    e = s._fields.e_flat
+    h = s._fields.h_flat
+    e[:] = rng.standard_normal(e.size) * (np.asarray(s._beta_E) != 0)
+    h[:] = rng.standard_normal(h.size) * (np.asarray(s._beta_H) != 0) * 1e-3
+    prob = problem_from_solver(s, n)
+    s.run()
+    _save("sibc_box", prob, _outputs(s, prob, {}), n,
+          "copper SIBC walls on y/z and on a copper brick, CPML on x, random initial fields")
+
+
 def case_mixed_box():
     """CPML on x and zmax, PEC on ymin / zmin, PMC on ymax."""
     from magnelio.boundaries.cpml import CPMLBoundary
@@ -686,6 +730,7 @@ CASES = {
     "cfg3_cross_small": case_cfg3_cross_small,
     "cfg3_cross_full": case_cfg3_cross_full,
     "mixed_box": case_mixed_box,
+    "sibc_box": case_sibc_box,
     "lumped_dft": case_lumped_dft,
     "wg_dtbc": case_wg_dtbc,
     "wg_mur": case_wg_mur,

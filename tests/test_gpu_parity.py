@@ -71,7 +71,8 @@ def test_kernel_sweep_matches_reference_kernels(precision, tol):
 
 
 @pytest.mark.parametrize(
-    "name", ["cpml_box", "mixed_box", "lumped_dft", "wg_dtbc", "wg_mur", "planewave_box", "dispersive_box"])
+    "name", ["cpml_box", "mixed_box", "lumped_dft", "wg_dtbc", "wg_mur", "planewave_box", "dispersive_box",
+             "sibc_box"])
 @pytest.mark.parametrize("precision,tol", [("double", F64_TOL), ("single", F32_TOL)])
 def test_fields_match_reference(name, precision, tol):
     pe, ph = _peaks(name)
@@ -273,6 +274,34 @@ def test_dtbc_tables_built_on_the_device_match_the_host_tables():
     assert _rel(Vd, Vh) < 1e-12 and _rel(Id, Ih) < 1e-12
     assert _rel(ed, ref.f.e, ref.peak_e) < F64_TOL
     assert _rel(Vd, np.array(ref.V)) < F64_TOL
+
+
+def test_sibc_walls_resume_bit_exactly_and_need_an_in_place_form():
+    """The SIBC branch states travel with the device state (resume equals
+    the uninterrupted run bit for bit), every in-place stencil form gives
+    the reference march, and the fused forms refuse the walls."""
+    p, d, n = load_golden("sibc_box")
+    pe, ph = _peaks("sibc_box")
+    k = n // 2 + 3
+    with p.build_engine("single") as a:
+        a.step(k)
+        blob = a.state_export()
+        a.step(n - k)
+        ea, ha = a.read_fields()
+        with pytest.raises(FitbError, match="SIBC walls need an in-place stencil mode"):
+            a.configure_stencil("fused", 16)
+    with p.build_engine("single") as b:
+        b.state_import(blob)
+        b.step(n - k)
+        eb, hb = b.read_fields()
+    assert np.array_equal(ea, eb) and np.array_equal(ha, hb)
+    for kind, v in (("simple", 0), ("stream", 1), ("vec", 0), ("bulk", 0)):
+        with p.build_engine("single") as c:
+            c.configure_stencil(kind, v)
+            c.step(n)
+            e, h = c.read_fields()
+        assert _rel(e, d["out.e"], pe) < F32_TOL, kind
+        assert _rel(h, d["out.h"], ph) < F32_TOL, kind
 
 
 def test_missing_dtbc_table_is_an_error_not_a_fault():

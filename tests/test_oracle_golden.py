@@ -32,7 +32,8 @@ def test_kernel_sweep_matches_reference_numba_kernels():
         assert _rel(getattr(f, c), d[f"out.{c}"]) < 1e-13, c
 
 
-@pytest.mark.parametrize("name", ["cpml_box", "mixed_box", "lumped_dft", "wg_dtbc", "wg_mur", "planewave_box", "dispersive_box"])
+@pytest.mark.parametrize("name", ["cpml_box", "mixed_box", "lumped_dft", "wg_dtbc", "wg_mur", "planewave_box",
+                                  "dispersive_box", "sibc_box"])
 def test_oracle_march_matches_reference(name):
     p, d, n = load_golden(name)
     r = OracleRun(p).run(n)
