@@ -309,6 +309,38 @@ int fitb_add_dispersion_block(fitb_handle* h, int32_t side, int64_t n_states, co
                               const double* k_re, const double* k_im, const double* c_re,
                               const double* c_im, const double* weight);
 
+/* ---- band-subspace DTBC ports ---------------------------------------- */
+/* Replaces PortOperatorBandDTBC (src/magnelio/ports/_modal/band_dtbc.py:
+ * 780-1236) with its BandDTBCBoundary (:509-680).  Flat indices are into
+ * the reference E (H) vectors; matrices row-major.  The port plane is
+ * written from the p boundary coordinates (e[e_u] = Wu xt, e[e_v] = Wv xt),
+ * the boundary couples to the first interior period through
+ * M_coup (p x n1) and to the exterior through D0, Dm1 (p x p) and the
+ * matrix DTBC kernels; the recorder projects n_modes channels: V with
+ * me (n_u + n_v) and v_profile (n_modes x (n_u + n_v)) on the port plane
+ * (u part plus v part), I with mh (n_h) and h_profile (n_modes x n_h) on
+ * its dual faces, both times record_scale.  x1_prev0 may be NULL (a
+ * quiescent start).  p <= 32, n_modes <= 16; before the first step; the
+ * in-place stencil modes only (FITB_ERR_STATE in the fused forms). */
+typedef struct {
+    int32_t p, n_modes, n_kernel_init;
+    int64_t n_u, n_v, n1, n_h;
+    const int64_t *e_u_idx, *e_v_idx, *x1_idx, *h_idx;
+    const double *Wu, *Wv, *M_coup, *D0, *Dm1;
+    const double *me, *v_profile, *mh, *h_profile, *record_scale;
+    const double* x1_prev0;
+} fitb_band_desc;
+int fitb_add_band_port(fitb_handle* h, const fitb_band_desc* d, int32_t* out_id);
+/* Matrix DTBC kernel table L_m (m = 0..n_kernel-1, each p x p row-major) of
+ * band port `port`, outgoing (incoming = 0) or incoming (1, excited ports):
+ * lengths n0, 2 n0, 4 n0, ... in order, one call each; a step n uses the
+ * table of the smallest length >= n + 1 (band_dtbc.py:591-603). */
+int fitb_set_band_kernel(fitb_handle* h, int32_t port, int32_t incoming, int32_t n_kernel, const double* L);
+/* Ghost source of field set b: n_samples p-vectors s^n (n_samples x p),
+ * zero beyond (the synthesised series of set_excitation /
+ * set_excitation_band, :940-1118); needs the incoming kernel. */
+int fitb_set_band_source(fitb_handle* h, int32_t port, int32_t b, int64_t n_samples, const double* s);
+
 /* ---- surface-impedance walls ---------------------------------------- */
 /* One SIBC wall tag (solver/_sibc.py:88-264, hooks at fit_td.py:837-840 and
  * :909-914): n_faces flat indices into the reference H vector with their

@@ -75,6 +75,33 @@ class FitbModalDesc(C.Structure):
     ]
 
 
+class FitbBandDesc(C.Structure):
+    _fields_ = [
+        ("p", i32),
+        ("n_modes", i32),
+        ("n_kernel_init", i32),
+        ("n_u", i64),
+        ("n_v", i64),
+        ("n1", i64),
+        ("n_h", i64),
+        ("e_u_idx", P_i64),
+        ("e_v_idx", P_i64),
+        ("x1_idx", P_i64),
+        ("h_idx", P_i64),
+        ("Wu", P_f64),
+        ("Wv", P_f64),
+        ("M_coup", P_f64),
+        ("D0", P_f64),
+        ("Dm1", P_f64),
+        ("me", P_f64),
+        ("v_profile", P_f64),
+        ("mh", P_f64),
+        ("h_profile", P_f64),
+        ("record_scale", P_f64),
+        ("x1_prev0", P_f64),
+    ]
+
+
 class FitbDftDesc(C.Structure):
     _fields_ = [
         ("i0", i32),
@@ -140,6 +167,9 @@ SIGNATURES = {
     "fitb_set_lumped_source": ([vp, i32, i32, i64, P_f64], C.c_int),
     "fitb_push_lumped_samples": ([vp, i32, i32, i64, i64, cvp], C.c_int),
     "fitb_add_modal_port": ([vp, C.POINTER(FitbModalDesc), P_i32], C.c_int),
+    "fitb_add_band_port": ([vp, C.POINTER(FitbBandDesc), P_i32], C.c_int),
+    "fitb_set_band_kernel": ([vp, i32, i32, i32, P_f64], C.c_int),
+    "fitb_set_band_source": ([vp, i32, i32, i64, P_f64], C.c_int),
     "fitb_set_dtbc_kernel": ([vp, i32, i32, i32, P_f64], C.c_int),
     "fitb_build_dtbc_kernel": ([vp, i32, i32, i64], C.c_int),
     "fitb_set_modal_source": ([vp, i32, i32, i32, i64, P_f64], C.c_int),

@@ -19,7 +19,8 @@ import numpy as np
 
 from magnelio_b200 import host
 from magnelio_b200.problem import (
-    CpmlFace, DftMonitor, Dispersion, DispersionBlock, FitProblem, LumpedPort, ModalPort, PlaneWave, SibcBlock,
+    BandPort, CpmlFace, DftMonitor, Dispersion, DispersionBlock, FitProblem, LumpedPort, ModalPort, PlaneWave,
+    SibcBlock,
 )
 
 _FACE_EDGES = {
@@ -83,6 +84,7 @@ def problem_from_solver(solver, n_steps: int) -> FitProblem:
     from magnelio.monitors.field_frequency import MonitorFieldFrequency
     from magnelio.ports._lumped.operator import LumpedElementOperator
     from magnelio.ports._modal.operator import PortOperatorModal
+    from magnelio.ports._modal.band_dtbc import PortOperatorBandDTBC
     from magnelio.circuit.companion import SeriesRLC
 
     s = solver
@@ -127,7 +129,10 @@ def problem_from_solver(solver, n_steps: int) -> FitProblem:
         if isinstance(op, PortOperatorModal):
             prob.modal.append(_modal_from_op(op, s.recorder, dt, n_steps))
     for op in s.ports:
-        if isinstance(op, PortOperatorModal):
+        if isinstance(op, PortOperatorBandDTBC):
+            prob.band.append(_band_from_op(op, s.recorder, n_steps))
+    for op in s.ports:
+        if isinstance(op, (PortOperatorModal, PortOperatorBandDTBC)):
             continue
         if isinstance(op, LumpedElementOperator):
             el = op.element
@@ -169,6 +174,48 @@ def problem_from_solver(solver, n_steps: int) -> FitProblem:
     prob.e0 = [np.array(_np(s._fields.e_flat), dtype=np.float64)]
     prob.h0 = [np.array(_np(s._fields.h_flat), dtype=np.float64)]
     return prob
+
+
+def _band_from_op(op, recorder, n_steps) -> BandPort:
+    """The projected boundary of a ``PortOperatorBandDTBC``
+    (``ports/_modal/band_dtbc.py:780-1236``) with its matrix DTBC kernel
+    tables for a run of ``n_steps``: the lengths n0, 2 n0, ... the boundary
+    visits (it doubles its kernel whenever a step outgrows it, :591-603),
+    computed with the reference's ``matrix_dtbc_kernel`` (outgoing: the
+    swapped pencil; incoming, for an excited port: the unswapped one)."""
+    from magnelio.ports._modal.band_dtbc import matrix_dtbc_kernel
+
+    bd = op._boundary
+    n0 = int(bd._n_kernel)
+    lens = [n0]
+    while lens[-1] < n_steps:
+        lens.append(2 * lens[-1])
+    kout = [np.ascontiguousarray(matrix_dtbc_kernel(bd._Dp1, bd._D0, bd._Dm1, L)[0]) for L in lens]
+    kin = []
+    if bd._kflip_in is not None:
+        kin = [np.ascontiguousarray(matrix_dtbc_kernel(bd._Dm1, bd._D0, bd._Dp1, L)[0]) for L in lens]
+    plane = op.plane
+    M = op.n_modes
+    prof = []
+    for m, dm in enumerate(op.discrete_modes):
+        dual = op._dual_e_profiles[m] if op._dual_e_profiles is not None else None
+        pu, pv = dual if dual is not None else (dm.e_u_profile, dm.e_v_profile)
+        prof.append(np.concatenate([np.asarray(pu, float), np.asarray(pv, float)]))
+    hprof = [np.concatenate([np.asarray(dm.h_u_profile, float), np.asarray(dm.h_v_profile, float)])
+             for dm in op.discrete_modes]
+    scale = np.broadcast_to(np.asarray(_recorder_scale(recorder, op), float), (M,)).copy()
+    src = None if op._src_series is None else np.asarray(op._src_series, float).copy()
+    return BandPort(
+        e_u_idx=np.asarray(plane.e_u_indices, np.int64), e_v_idx=np.asarray(plane.e_v_indices, np.int64),
+        Wu=np.asarray(op._Wu, float), Wv=np.asarray(op._Wv, float),
+        x1_idx=np.asarray(op._x1_idx, np.int64), M_coup=np.asarray(op._M_coup, float),
+        D0=np.asarray(bd._D0, float), Dm1=np.asarray(bd._Dm1, float),
+        n_kernel_init=lens[0], kernels_out=kout, kernels_in=kin,
+        me=np.concatenate([op._me_u_port, op._me_v_port]), v_profile=np.stack(prof),
+        h_idx=np.concatenate([np.asarray(plane.h_u_indices, np.int64), np.asarray(plane.h_v_indices, np.int64)]),
+        mh=np.concatenate([op._mh_u, op._mh_v]), h_profile=np.stack(hprof), record_scale=scale,
+        x1_prev0=np.asarray(op._x1_prev, float).copy(), source=[src],
+    )
 
 
 def _sibc_from_op(op) -> list:

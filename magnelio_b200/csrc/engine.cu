@@ -188,6 +188,18 @@ struct ModalHost {
     long long n_wf = 0;
 };
 
+struct BandHost {
+    BandDev dev{};
+    int p = 0;
+    DevBuf eu, ev, x1, hh, Wu, Wv, Mc, D0, Dm1, me, vprof, mh, hprof, rec_scale;
+    DevBuf kout, kin, st, x1prev, whist, shist, src, src_on, conv;
+    std::vector<double> kout_host, kin_host;  // tables one after the other
+    int n_out = 0, n_in = 0;                  // tables set
+    std::vector<double> src_host;             // [B][n_src][p]
+    std::vector<int> src_on_host;
+    long long n_src = 0;
+};
+
 struct DftHost {
     DftDev dev{};
     DevBuf omega, inv, dual, stage, wst, bins, cmp, base;
@@ -242,6 +254,8 @@ struct Handle {
     std::vector<std::unique_ptr<PlaneWaveHost>> pws;
     DispHost disp[2];  // E side, H side
     SibcHost sibc;     // surface-impedance walls (H side)
+    std::vector<std::unique_ptr<BandHost>> band;  // band-subspace DTBC ports
+    DevBuf d_band;
     DevBuf d_lumped, d_modal, d_dft;
     int dft_stage_blocks = 0, dft_flush_blocks = 0;
     size_t dft_flush_smem = 0;
@@ -479,6 +493,20 @@ void ensure_capacity(Handle& H, long long need) {
             std::swap(buf->bytes, nb.bytes);
         }
     }
+    for (auto& bp : H.band) {
+        const int p = bp->p;
+        bp->conv.alloc((size_t)H.B * ((ncap + kConvChunk - 1) / kConvChunk) * 2 * p * sizeof(double));
+        for (DevBuf* buf : {&bp->whist, &bp->shist}) {
+            DevBuf nb;
+            nb.alloc((size_t)H.B * ncap * p * sizeof(double));
+            if (buf->p && H.cap > 0)
+                ck(cudaMemcpy2D(nb.p, (size_t)ncap * p * sizeof(double), buf->p, (size_t)H.cap * p * sizeof(double),
+                                (size_t)H.cap * p * sizeof(double), (size_t)H.B, cudaMemcpyDeviceToDevice),
+                   "grow band history");
+            std::swap(buf->p, nb.p);
+            std::swap(buf->bytes, nb.bytes);
+        }
+    }
     legacy_sync("capacity copy sync");
     H.cap = ncap;
     H.port_tables_dirty = true;
@@ -547,6 +575,23 @@ void refresh_port_tables(Handle& H) {
         md.push_back(d);
     }
     upload(H.d_modal, md);
+    std::vector<BandDev> bd;
+    for (auto& bp : H.band) {
+        BandDev d = bp->dev;
+        d.whist = bp->whist.as<double>();
+        d.shist = bp->shist.as<double>();
+        d.cap = H.cap;
+        d.conv = bp->conv.as<double>();
+        d.conv_chunks = (int)((H.cap + kConvChunk - 1) / kConvChunk);
+        d.kout = bp->kout.as<double>();
+        d.kin = bp->kin.as<double>();
+        d.has_in = bp->n_in > 0 ? 1 : 0;
+        d.src = bp->src.as<double>();
+        d.n_src = bp->n_src;
+        d.src_on = bp->src_on.as<int>();
+        bd.push_back(d);
+    }
+    upload(H.d_band, bd);
     // monitors: block ranges of the merged stage / flush launches
     std::vector<DftDev> dd;
     int sb = 0, fb = 0;
@@ -1052,6 +1097,11 @@ int enqueue_step(Handle& H) {
         launch_modal<T>(H.Ec().as<T>(), H.Hc().as<T>(), pa, H.d_modal.as<ModalDev>(), (int)H.modal.size(), H.stream);
         ++n;
     }
+    if (!H.band.empty()) {
+        launch_band<T>(H.Ec().as<T>(), H.Hc().as<T>(), pa, H.d_band.as<BandDev>(), (int)H.band.size(),
+                       (int)((H.cap + kConvChunk - 1) / kConvChunk), H.stream);
+        n += 2;
+    }
     if (!H.lumped.empty()) {
         launch_lumped<T>(H.Ec().as<T>(), pa, H.d_lumped.as<LumpedDev>(), (int)H.lumped.size(), H.stream);
         ++n;
@@ -1155,6 +1205,19 @@ void check_dtbc_tables(Handle& H, long long last_step) {
                      "(call fitb_set_dtbc_kernel)",
                      p, m, tlen, last_step);
         }
+    }
+    for (size_t q = 0; q < H.band.size(); ++q) {
+        const auto& bp = *H.band[q];
+        long long tlen = bp.dev.n0;
+        int t = 0;
+        while (tlen < last_step + 1) {
+            tlen *= 2;
+            ++t;
+        }
+        if (bp.n_out <= t || (bp.n_in > 0 && bp.n_in <= t))
+            fail(FITB_ERR_STATE,
+                 "band port %zu: DTBC kernel table of length %lld missing for step %lld (call fitb_set_band_kernel)",
+                 q, tlen, last_step);
     }
 }
 
@@ -1348,6 +1411,14 @@ void write_state(Handle& H, Writer& w) {
     }
     for (auto& dp : H.disp) dev_get(w, dp.d_J.p, dp.d_J.bytes);
     dev_get(w, H.sibc.d_u.p, H.sibc.d_u.bytes);
+    for (auto& bp : H.band) {
+        dev_get(w, bp->st.p, bp->st.bytes);
+        dev_get(w, bp->x1prev.p, bp->x1prev.bytes);
+        const size_t row = (size_t)bp->p * sizeof(double);
+        for (int b = 0; b < H.B; ++b)
+            for (DevBuf* hb : {&bp->whist, &bp->shist})
+                dev_get(w, hb->as<char>() + (size_t)b * H.cap * row, (size_t)H.steps_done * row);
+    }
     for (auto& lp : H.lumped) dev_get(w, lp->st.p, lp->st.bytes);
     for (auto& mp : H.modal) {
         dev_get(w, mp->st.p, mp->st.bytes);
@@ -1414,6 +1485,14 @@ void read_state(Handle& H, Reader& r) {
     }
     for (auto& dp : H.disp) r.dev(dp.d_J.p, dp.d_J.bytes);
     r.dev(H.sibc.d_u.p, H.sibc.d_u.bytes);
+    for (auto& bp : H.band) {
+        r.dev(bp->st.p, bp->st.bytes);
+        r.dev(bp->x1prev.p, bp->x1prev.bytes);
+        const size_t row = (size_t)bp->p * sizeof(double);
+        for (int b = 0; b < H.B; ++b)
+            for (DevBuf* hb : {&bp->whist, &bp->shist})
+                r.dev(hb->as<char>() + (size_t)b * H.cap * row, (size_t)steps * row);
+    }
     for (auto& lp : H.lumped) r.dev(lp->st.p, lp->st.bytes);
     for (auto& mp : H.modal) {
         r.dev(mp->st.p, mp->st.bytes);
@@ -1777,6 +1856,7 @@ int fitb_configure_stencil(fitb_handle* h, int32_t kind, int32_t variant, int32_
     if (kind == fitb::kModeFused) {
         if (!fitb::fused_variant_ok(H.prec, variant)) fail(FITB_ERR_ARG, "fused variant %d", variant);
         if (H.sibc.present()) fail(FITB_ERR_STATE, "SIBC walls need an in-place stencil mode");
+        if (!H.band.empty()) fail(FITB_ERR_STATE, "band DTBC ports need an in-place stencil mode");
         if ((H.disp[0].present() || H.disp[1].present()) && !fitb::is_slab_variant(variant))
             fail(FITB_ERR_STATE,
                  "dispersive materials need an in-place stencil mode or the slab step (fused 16-25)");
@@ -2343,6 +2423,143 @@ int fitb_add_dispersion_block(fitb_handle* h, int32_t side, int64_t n_states, co
     dv.uoff = D.d_uoff.as<long long>();
     dv.ustart = D.d_ustart.as<int>();
     dv.ustate = D.d_ustate.as<long long>();
+    fitb::invalidate_graphs(H);
+    FITB_CATCH
+}
+
+int fitb_add_band_port(fitb_handle* h, const fitb_band_desc* d, int32_t* out_id) {
+    FITB_TRY
+    Handle& H = H_of(h);
+    if (!d || !out_id) fail(FITB_ERR_ARG, "null argument");
+    const int p = d->p, M = d->n_modes;
+    if (p < 1 || p > fitb::kBandPMax) fail(FITB_ERR_LIMIT, "band port rank p = %d (1..%d)", p, fitb::kBandPMax);
+    if (M < 1 || M > fitb::kMaxModes) fail(FITB_ERR_LIMIT, "band port channels %d (1..%d)", M, fitb::kMaxModes);
+    if (d->n_kernel_init < 2) fail(FITB_ERR_ARG, "n_kernel_init must be >= 2");
+    if (d->n_u < 0 || d->n_v < 0 || d->n_u + d->n_v < 1 || d->n1 < 1 || d->n_h < 0)
+        fail(FITB_ERR_ARG, "band port sizes");
+    if (!d->e_u_idx && d->n_u > 0) fail(FITB_ERR_ARG, "null e_u_idx");
+    if (!d->e_v_idx && d->n_v > 0) fail(FITB_ERR_ARG, "null e_v_idx");
+    if (!d->x1_idx || !d->M_coup || !d->D0 || !d->Dm1 || !d->me || !d->v_profile || !d->record_scale ||
+        (d->n_u > 0 && !d->Wu) || (d->n_v > 0 && !d->Wv) || (d->n_h > 0 && (!d->h_idx || !d->mh || !d->h_profile)))
+        fail(FITB_ERR_ARG, "band port arrays");
+    if (H.steps_done != 0) fail(FITB_ERR_STATE, "ports must be added before the first step");
+    if (H.stencil_mode == fitb::kModeFused) fail(FITB_ERR_STATE, "band DTBC ports need an in-place stencil mode");
+    const long long ne = H.nE(), nh = H.nH();
+    auto offs = [&](const int64_t* idx, long long n, bool is_h) {
+        std::vector<long long> o((size_t)std::max<long long>(n, 1), 0);
+        for (long long q = 0; q < n; ++q) {
+            if (idx[q] < 0 || idx[q] >= (is_h ? nh : ne)) fail(FITB_ERR_ARG, "band port index %lld out of range", (long long)idx[q]);
+            o[(size_t)q] = H.flat_to_off(is_h, idx[q]);
+        }
+        return o;
+    };
+    auto vec = [](const double* a, long long n) {
+        return n > 0 ? std::vector<double>(a, a + n) : std::vector<double>(1, 0.0);
+    };
+    auto bp = std::make_unique<fitb::BandHost>();
+    bp->p = p;
+    const long long nt = d->n_u + d->n_v;
+    fitb::upload(bp->eu, offs(d->e_u_idx, d->n_u, false));
+    fitb::upload(bp->ev, offs(d->e_v_idx, d->n_v, false));
+    fitb::upload(bp->x1, offs(d->x1_idx, d->n1, false));
+    fitb::upload(bp->hh, offs(d->h_idx, d->n_h, true));
+    fitb::upload(bp->Wu, vec(d->Wu, d->n_u * p));
+    fitb::upload(bp->Wv, vec(d->Wv, d->n_v * p));
+    fitb::upload(bp->Mc, vec(d->M_coup, (long long)p * d->n1));
+    fitb::upload(bp->D0, vec(d->D0, (long long)p * p));
+    fitb::upload(bp->Dm1, vec(d->Dm1, (long long)p * p));
+    fitb::upload(bp->me, vec(d->me, nt));
+    fitb::upload(bp->vprof, vec(d->v_profile, (long long)M * nt));
+    fitb::upload(bp->mh, vec(d->mh, d->n_h));
+    fitb::upload(bp->hprof, vec(d->h_profile, (long long)M * d->n_h));
+    fitb::upload(bp->rec_scale, vec(d->record_scale, M));
+    bp->st.alloc((size_t)H.B * 2 * p * sizeof(double));
+    std::vector<double> x1p((size_t)H.B * d->n1, 0.0);
+    if (d->x1_prev0)
+        for (int b = 0; b < H.B; ++b)
+            for (long long q = 0; q < d->n1; ++q) x1p[(size_t)(b * d->n1 + q)] = d->x1_prev0[q];
+    fitb::upload(bp->x1prev, x1p);
+    bp->src_on_host.assign((size_t)H.B, 0);
+    fitb::upload(bp->src_on, bp->src_on_host);
+    fitb::upload(bp->src, std::vector<double>(1, 0.0));
+    fitb::upload(bp->kout, std::vector<double>(1, 0.0));
+    fitb::upload(bp->kin, std::vector<double>(1, 0.0));
+    fitb::BandDev& dv = bp->dev;
+    dv.p = p;
+    dv.M = M;
+    dv.channel0 = H.nch;
+    dv.n_u = d->n_u;
+    dv.n_v = d->n_v;
+    dv.n1 = d->n1;
+    dv.n_h = d->n_h;
+    dv.eu = bp->eu.as<long long>();
+    dv.ev = bp->ev.as<long long>();
+    dv.x1 = bp->x1.as<long long>();
+    dv.hh = bp->hh.as<long long>();
+    dv.Wu = bp->Wu.as<double>();
+    dv.Wv = bp->Wv.as<double>();
+    dv.Mc = bp->Mc.as<double>();
+    dv.D0 = bp->D0.as<double>();
+    dv.Dm1 = bp->Dm1.as<double>();
+    dv.me = bp->me.as<double>();
+    dv.vprof = bp->vprof.as<double>();
+    dv.mh = bp->mh.as<double>();
+    dv.hprof = bp->hprof.as<double>();
+    dv.rec_scale = bp->rec_scale.as<double>();
+    dv.n0 = d->n_kernel_init;
+    dv.st = bp->st.as<double>();
+    dv.x1prev = bp->x1prev.as<double>();
+    H.nch += M;
+    *out_id = (int32_t)H.band.size();
+    H.band.push_back(std::move(bp));
+    // the recorder and the histories are sized for the new channel count
+    H.cap = 0;
+    fitb::ensure_capacity(H, 1);
+    H.port_tables_dirty = true;
+    fitb::invalidate_graphs(H);
+    FITB_CATCH
+}
+
+int fitb_set_band_kernel(fitb_handle* h, int32_t port, int32_t incoming, int32_t n_kernel, const double* L) {
+    FITB_TRY
+    Handle& H = H_of(h);
+    if (port < 0 || port >= (int)H.band.size()) fail(FITB_ERR_ARG, "band port %d does not exist", port);
+    if (!L) fail(FITB_ERR_ARG, "null kernel");
+    fitb::BandHost& bp = *H.band[port];
+    int& nt = incoming ? bp.n_in : bp.n_out;
+    const long long expect = bp.dev.n0 << nt;
+    if (n_kernel != expect) fail(FITB_ERR_ARG, "expected the band kernel table of length %lld next, got %d", expect, n_kernel);
+    auto& tab = incoming ? bp.kin_host : bp.kout_host;
+    tab.insert(tab.end(), L, L + (size_t)n_kernel * bp.p * bp.p);
+    nt += 1;
+    fitb::upload(incoming ? bp.kin : bp.kout, tab);
+    H.port_tables_dirty = true;
+    fitb::invalidate_graphs(H);
+    FITB_CATCH
+}
+
+int fitb_set_band_source(fitb_handle* h, int32_t port, int32_t b, int64_t n_samples, const double* src) {
+    FITB_TRY
+    Handle& H = H_of(h);
+    if (port < 0 || port >= (int)H.band.size()) fail(FITB_ERR_ARG, "band port %d does not exist", port);
+    if (b < 0 || b >= H.B) fail(FITB_ERR_ARG, "field set %d out of range", b);
+    if (n_samples < 1 || !src) fail(FITB_ERR_ARG, "band source needs samples");
+    fitb::BandHost& bp = *H.band[port];
+    const int p = bp.p;
+    const long long n_old = bp.n_src, n_new = std::max<long long>(n_old, n_samples);
+    std::vector<double> tab((size_t)(H.B * n_new * p), 0.0);
+    for (int q = 0; q < H.B; ++q)
+        for (long long t = 0; t < n_old; ++t)
+            for (int i = 0; i < p; ++i)
+                tab[(size_t)((q * n_new + t) * p + i)] = bp.src_host[(size_t)((q * n_old + t) * p + i)];
+    for (long long t = 0; t < n_new; ++t)
+        for (int i = 0; i < p; ++i) tab[(size_t)((b * n_new + t) * p + i)] = t < n_samples ? src[t * p + i] : 0.0;
+    bp.src_host = tab;
+    bp.n_src = n_new;
+    bp.src_on_host[(size_t)b] = 1;
+    fitb::upload(bp.src, tab);
+    fitb::upload(bp.src_on, bp.src_on_host);
+    H.port_tables_dirty = true;
     fitb::invalidate_graphs(H);
     FITB_CATCH
 }

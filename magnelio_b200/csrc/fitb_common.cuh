@@ -339,6 +339,34 @@ void launch_lumped(T* e, const PortsArgs& pa, const LumpedDev* d, int n_lumped, 
 template <typename T>
 void launch_modal(T* e, const T* h, const PortsArgs& pa, const ModalDev* d, int n_modal,
                   cudaStream_t s);
+// Band-subspace DTBC port (ports_band.cu; ports/_modal/band_dtbc.py): the
+// projected boundary period of p <= kBandPMax coordinates with matrix DTBC
+// kernels.  Offsets are padded-layout entries of a field set's E (H) block.
+constexpr int kBandPMax = 32;
+struct BandDev {
+    int p, M, channel0, has_in;
+    long long n_u, n_v, n1, n_h;
+    const long long *eu, *ev, *x1, *hh;       // port plane E (u, v), first interior period, dual H
+    const double *Wu, *Wv;                    // [n_u][p], [n_v][p]
+    const double *Mc;                         // [p][n1]
+    const double *D0, *Dm1;                   // [p][p]
+    const double *me, *vprof, *mh, *hprof;    // [n_u + n_v], [M][n_u + n_v], [n_h], [M][n_h]
+    const double* rec_scale;                  // [M]
+    long long n0;                             // initial kernel length; table t has n0 2^t entries
+    const double *kout, *kin;                 // tables one after the other: [L][p][p]
+    double* st;                               // [B][2 p]: xt, xt_prev
+    double* x1prev;                           // [B][n1]
+    double *whist, *shist;                    // [B][cap][p]
+    long long cap;
+    const double* src;                        // [B][n_src][p]
+    long long n_src;
+    const int* src_on;                        // [B]
+    double* conv;                             // [B][conv_chunks][2][p] partial sums of the step
+    int conv_chunks;
+};
+template <typename T>
+void launch_band(T* e, const T* h, const PortsArgs& pa, const BandDev* d, int n_band, int max_chunks, cudaStream_t s);
+
 // The DTBC history convolutions of the coming port update (they read only
 // the history before the current step), spread over the history chunks of
 // every (port, field set); launch_modal sums the partials in chunk order.

@@ -358,6 +358,47 @@ class FitEngine:
         self._modal.append(int(out.value))
         return int(out.value)
 
+    def add_band_port(self, bp) -> int:
+        """Upload a band-subspace DTBC port (:class:`magnelio_b200.problem.BandPort`)
+        and return its id; its kernel tables and sources follow with
+        :meth:`set_band_kernel` and :meth:`set_band_source`."""
+        p = int(np.asarray(bp.D0).shape[0])
+        M = int(np.asarray(bp.record_scale).size)
+        i64a = lambda x: np.ascontiguousarray(np.asarray(x, dtype=np.int64).ravel())  # noqa: E731
+        f64a = lambda x: np.ascontiguousarray(np.asarray(x, dtype=np.float64).ravel())  # noqa: E731
+        keep = {
+            "e_u_idx": i64a(bp.e_u_idx), "e_v_idx": i64a(bp.e_v_idx), "x1_idx": i64a(bp.x1_idx),
+            "h_idx": i64a(bp.h_idx), "Wu": f64a(bp.Wu), "Wv": f64a(bp.Wv), "M_coup": f64a(bp.M_coup),
+            "D0": f64a(bp.D0), "Dm1": f64a(bp.Dm1), "me": f64a(bp.me), "v_profile": f64a(bp.v_profile),
+            "mh": f64a(bp.mh), "h_profile": f64a(bp.h_profile), "record_scale": f64a(bp.record_scale),
+        }
+        x1p = None if bp.x1_prev0 is None else f64a(bp.x1_prev0)
+        n_u, n_v, n1, n_h = (keep[k].size for k in ("e_u_idx", "e_v_idx", "x1_idx", "h_idx"))
+        if keep["Wu"].size != n_u * p or keep["Wv"].size != n_v * p or keep["M_coup"].size != p * n1:
+            raise ValueError("band port: W / M_coup shapes do not match the index arrays and p")
+        if keep["v_profile"].size != M * (n_u + n_v) or keep["h_profile"].size != M * n_h:
+            raise ValueError("band port: profile shapes do not match the channels and the plane")
+        d = _lib.FitbBandDesc(
+            p, M, int(bp.n_kernel_init), n_u, n_v, n1, n_h,
+            i64p(keep["e_u_idx"]), i64p(keep["e_v_idx"]), i64p(keep["x1_idx"]), i64p(keep["h_idx"]),
+            f64p(keep["Wu"]), f64p(keep["Wv"]), f64p(keep["M_coup"]), f64p(keep["D0"]), f64p(keep["Dm1"]),
+            f64p(keep["me"]), f64p(keep["v_profile"]), f64p(keep["mh"]), f64p(keep["h_profile"]),
+            f64p(keep["record_scale"]), f64p(x1p),
+        )
+        out = C.c_int32()
+        check(self._lib.fitb_add_band_port(self._h, C.byref(d), C.byref(out)))
+        return int(out.value)
+
+    def set_band_kernel(self, port: int, incoming: int, table) -> None:
+        """Append the next kernel table (L, p, p) of band port ``port``."""
+        t = np.ascontiguousarray(np.asarray(table, dtype=np.float64))
+        check(self._lib.fitb_set_band_kernel(self._h, int(port), int(incoming), int(t.shape[0]), f64p(t)))
+
+    def set_band_source(self, port: int, b: int, series) -> None:
+        """Ghost source p-vectors (n, p) of band port ``port`` for field set ``b``."""
+        s = np.ascontiguousarray(np.asarray(series, dtype=np.float64))
+        check(self._lib.fitb_set_band_source(self._h, int(port), int(b), int(s.shape[0]), f64p(s)))
+
     def set_dtbc_kernel(self, port: int, mode: int, kernel) -> None:
         k = _f64(kernel)
         check(self._lib.fitb_set_dtbc_kernel(self._h, int(port), int(mode), int(k.size), f64p(k)))

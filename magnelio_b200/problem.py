@@ -121,6 +121,50 @@ class DispersionBlock:
 
 
 @dataclass
+class BandPort:
+    """Band-subspace DTBC port (``ports/_modal/band_dtbc.py:509-1236``): the
+    projected boundary period of p coordinates, marched with the exact
+    matrix DTBC of the projected exterior.
+
+    Per step the port takes ``coup = M_coup x1_prev`` (the first interior
+    period's E one step ago), the history convolutions with the p x p
+    kernels ``L_m`` (outgoing, and incoming for an excited port), advances
+    ``xt`` and writes the port plane ``e[e_u_idx] = Wu xt``,
+    ``e[e_v_idx] = Wv xt``; the recorder projects V per channel with
+    ``me`` and ``v_profile`` on the port plane and I with ``mh`` and
+    ``h_profile`` on its dual faces."""
+
+    e_u_idx: np.ndarray      # (n_u,) flat E indices of the port plane
+    e_v_idx: np.ndarray      # (n_v,)
+    Wu: np.ndarray           # (n_u, p)
+    Wv: np.ndarray           # (n_v, p)
+    x1_idx: np.ndarray       # (n1,) flat E indices of the first interior period
+    M_coup: np.ndarray       # (p, n1)
+    D0: np.ndarray           # (p, p)
+    Dm1: np.ndarray          # (p, p)
+    n_kernel_init: int
+    kernels_out: list        # tables of lengths n0, 2 n0, ...: (L, p, p) each
+    kernels_in: list         # the same for the incoming kernel ([] for a passive port)
+    me: np.ndarray           # (n_u + n_v,) M_eps on the port plane
+    v_profile: np.ndarray    # (M, n_u + n_v)
+    h_idx: np.ndarray        # (n_h,) flat H indices of the port plane's dual faces
+    mh: np.ndarray           # (n_h,)
+    h_profile: np.ndarray    # (M, n_h)
+    record_scale: np.ndarray  # (M,)
+    x1_prev0: np.ndarray | None = None  # initial interior trace (initialize_state), zeros if None
+    # per field set: the ghost source series (n_src, p) or None
+    source: list = field(default_factory=list)
+
+    @property
+    def p(self) -> int:
+        return int(np.asarray(self.D0).shape[0])
+
+    @property
+    def n_modes(self) -> int:
+        return int(np.asarray(self.record_scale).size)
+
+
+@dataclass
 class SibcBlock:
     """Surface-impedance wall of one tag (``solver/_sibc.py:88-111``): flat
     H indices of its driving faces, the geometry factor ``g = A / l_dual^2``
@@ -218,6 +262,7 @@ class FitProblem:
     plane_waves: list = field(default_factory=list)
     dispersion: list = field(default_factory=list)
     sibc: list = field(default_factory=list)  # SibcBlock, in the reference's wall-tag order
+    band: list = field(default_factory=list)  # BandPort (channels after the modal ports)
     batch: int = 1
     e0: list = field(default_factory=list)  # per field set initial e (or empty)
     h0: list = field(default_factory=list)
@@ -272,6 +317,15 @@ class FitProblem:
                 for b, exc in enumerate(mp.excitation):
                     if exc is not None and exc[0] >= 0:
                         eng.set_modal_source(pid, b, int(exc[0]), exc[1])
+            for bp in self.band:
+                bid = eng.add_band_port(bp)
+                for t in bp.kernels_out:
+                    eng.set_band_kernel(bid, 0, t)
+                for t in bp.kernels_in:
+                    eng.set_band_kernel(bid, 1, t)
+                for b, src in enumerate(bp.source):
+                    if src is not None:
+                        eng.set_band_source(bid, b, src)
             for lp in self.lumped:
                 lid = eng.add_lumped(
                     lp.flat_idx, lp.signs, lp.betas, R=lp.R, L=lp.L, C_=lp.C, record_scale=lp.record_scale
@@ -358,6 +412,20 @@ class FitProblem:
                 if exc is not None:
                     put(f"modal{q}.exc{b}.mode", exc[0])
                     put(f"modal{q}.exc{b}.w", exc[1])
+        put("n_band", len(self.band))
+        for q, bp in enumerate(self.band):
+            for k in ("e_u_idx", "e_v_idx", "Wu", "Wv", "x1_idx", "M_coup", "D0", "Dm1", "me", "v_profile", "h_idx", "mh", "h_profile", "record_scale"):
+                put(f"band{q}.{k}", getattr(bp, k))
+            put(f"band{q}.n_kernel_init", bp.n_kernel_init)
+            for t, tab in enumerate(bp.kernels_out):
+                put(f"band{q}.kout{t}", tab)
+            for t, tab in enumerate(bp.kernels_in):
+                put(f"band{q}.kin{t}", tab)
+            if bp.x1_prev0 is not None:
+                put(f"band{q}.x1_prev0", bp.x1_prev0)
+            for b, src in enumerate(bp.source):
+                if src is not None:
+                    put(f"band{q}.src{b}", src)
         put("n_mon", len(self.monitors))
         for q, mon in enumerate(self.monitors):
             put(f"mon{q}.box", np.asarray(mon.box, dtype=np.int64))
@@ -435,6 +503,16 @@ class FitProblem:
                 mode = g(f"modal{q}.exc{b}.mode")
                 mp.excitation.append(None if mode is None else (int(mode), g(f"modal{q}.exc{b}.w")))
             p.modal.append(mp)
+        for q in range(int(g("n_band", 0))):
+            kw = {k: g(f"band{q}.{k}") for k in ("e_u_idx", "e_v_idx", "Wu", "Wv", "x1_idx", "M_coup", "D0", "Dm1", "me", "v_profile", "h_idx", "mh", "h_profile", "record_scale")}
+            kout, kin = [], []
+            while g(f"band{q}.kout{len(kout)}") is not None:
+                kout.append(g(f"band{q}.kout{len(kout)}"))
+            while g(f"band{q}.kin{len(kin)}") is not None:
+                kin.append(g(f"band{q}.kin{len(kin)}"))
+            p.band.append(BandPort(n_kernel_init=int(g(f"band{q}.n_kernel_init")), kernels_out=kout, kernels_in=kin,
+                                   x1_prev0=g(f"band{q}.x1_prev0"),
+                                   source=[g(f"band{q}.src{b}") for b in range(p.batch)], **kw))
         for q in range(int(g("n_mon", 0))):
             box = g(f"mon{q}.box")
             comps = tuple(["Ex", "Ey", "Ez", "Hx", "Hy", "Hz"][int(c)] for c in g(f"mon{q}.comps"))

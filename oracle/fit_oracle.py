@@ -486,6 +486,75 @@ class DispersionOracle:
 
 
 # ---------------------------------------------------------------------------
+# Band-subspace DTBC port (ports/_modal/band_dtbc.py:509-680, :1152-1236)
+# ---------------------------------------------------------------------------
+class BandOracle:
+    """Projected boundary period of one band port.  ``update_e`` (:1204-1236)
+    takes the interior coupling ``M_coup x1_prev`` from the previous step's
+    trace, advances the boundary (``BandDTBCBoundary.advance``, :618-668):
+    ``ghost = s + sum_{m>=1} L^out_m (xt - xt_inc)^{n-m}``,
+    ``xt_inc = sum_{m>=1} L^in_m s^{n-m}``,
+    ``xt' = 2 xt - xt_prev - (coup + D0 xt + Dm1 ghost)``, writes the port
+    plane from ``xt'`` and stores the new interior trace; the kernel in
+    effect at step n is the table of the smallest length n0 2^t >= n + 1."""
+
+    def __init__(self, bp, src):
+        self.bp = bp
+        p = bp.p
+        self.xt = np.zeros(p)
+        self.xt_prev = np.zeros(p)
+        self.w = []
+        self.s = []
+        self.x1_prev = np.zeros(np.asarray(bp.x1_idx).size) if bp.x1_prev0 is None else np.array(bp.x1_prev0, float)
+        self.src = None if src is None else np.asarray(src, float)
+        self.n = 0
+
+    def _table(self, tables, n):
+        L, t = self.bp.n_kernel_init, 0
+        while L < n + 1:
+            L *= 2
+            t += 1
+        return np.asarray(tables[t])
+
+    def update_e(self, e):
+        bp, n = self.bp, self.n
+        p = bp.p
+        s = self.src[n] if self.src is not None and n < self.src.shape[0] else np.zeros(p)
+        coup = np.asarray(bp.M_coup) @ self.x1_prev
+        if n == 0:
+            xt_inc = np.zeros(p)
+            conv_w = np.zeros(p)
+        else:
+            Lo = self._table(bp.kernels_out, n)
+            conv_w = np.einsum("mij,mj->i", Lo[n:0:-1], np.array(self.w))
+            if bp.kernels_in:
+                Li = self._table(bp.kernels_in, n)
+                xt_inc = np.einsum("mij,mj->i", Li[n:0:-1], np.array(self.s))
+            else:
+                xt_inc = np.zeros(p)
+        ghost = s + conv_w
+        self.w.append(self.xt - xt_inc)
+        self.s.append(s)
+        xt_new = 2.0 * self.xt - self.xt_prev - (coup + np.asarray(bp.D0) @ self.xt + np.asarray(bp.Dm1) @ ghost)
+        self.xt_prev = self.xt
+        self.xt = xt_new
+        self.n = n + 1
+        e[bp.e_u_idx] = np.asarray(bp.Wu) @ xt_new
+        e[bp.e_v_idx] = np.asarray(bp.Wv) @ xt_new
+        self.x1_prev = e[bp.x1_idx].copy()
+
+    def record(self, e, h):
+        bp = self.bp
+        ep = np.concatenate([e[bp.e_u_idx], e[bp.e_v_idx]])
+        hp = h[bp.h_idx]
+        V, I = [], []
+        for m in range(bp.n_modes):
+            V.append(float(np.dot(bp.me, np.asarray(bp.v_profile)[m] * ep)) * float(bp.record_scale[m]))
+            I.append(float(np.dot(bp.mh, np.asarray(bp.h_profile)[m] * hp)) * float(bp.record_scale[m]))
+        return V, I
+
+
+# ---------------------------------------------------------------------------
 # Surface-impedance walls (solver/_sibc.py:114-264)
 # ---------------------------------------------------------------------------
 class SibcOracle:
@@ -586,6 +655,8 @@ class OracleRun:
         self.cpml = [CpmlOracle(c.face, prob.nx, prob.ny, prob.nz, c.b, c.c, c.ck, c.air) for c in prob.cpml]
         self.modal = [ModalOracle(mp, prob.dt, mp.excitation[b] if b < len(mp.excitation) else None) for mp in prob.modal]
         self.lumped = [LumpedOracle(lp, prob.dt) for lp in prob.lumped]
+        self.band = [BandOracle(bp, bp.source[b] if b < len(bp.source) else None)
+                     for bp in getattr(prob, "band", [])]
         self.mons = [DftOracle(m, prob.dx, prob.dy, prob.dz) for m in prob.monitors]
         self.pws = [PlaneWaveOracle(pw, pw.scale[b] if b < len(pw.scale) else 1.0)
                     for pw in getattr(prob, "plane_waves", [])]
@@ -617,11 +688,17 @@ class OracleRun:
         V, I = [], []
         for mo in self.modal:
             mo.update_e(f.e, n)
+        for bo in self.band:
+            bo.update_e(f.e)
         for lo in self.lumped:
             v_src = lo.lp.v_src[self.b] if self.b < len(lo.lp.v_src) else None
             lo.update_e(f.e, n, v_src)
         for mo in self.modal:
             v, i = mo.record(f.e, f.h)
+            V += v
+            I += i
+        for bo in self.band:
+            v, i = bo.record(f.e, f.h)
             V += v
             I += i
         for lo in self.lumped:

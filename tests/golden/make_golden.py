@@ -50,11 +50,14 @@ def _outputs(solver, prob, out):
     rec = solver.recorder
     if rec is not None:
         rec._drain_stages()
-        # channel order of the engine: modal ports in solver order, then lumped
+        # channel order of the engine: modal ports in solver order, then band
+        # ports, then lumped
+        from magnelio.ports._modal.band_dtbc import PortOperatorBandDTBC
         from magnelio.ports._modal.operator import PortOperatorModal
 
         order = [op for op in solver.ports if isinstance(op, PortOperatorModal)]
-        order += [op for op in solver.ports if not isinstance(op, PortOperatorModal)]
+        order += [op for op in solver.ports if isinstance(op, PortOperatorBandDTBC)]
+        order += [op for op in solver.ports if not isinstance(op, (PortOperatorModal, PortOperatorBandDTBC))]
         V = np.stack([np.asarray(rec._V_buffers[(op.name, m)]) for op in order for m in range(op.n_modes)], axis=1)
         I = np.stack([np.asarray(rec._I_buffers[(op.name, m)]) for op in order for m in range(op.n_modes)], axis=1)
         out["out.V"] = V
@@ -252,6 +255,64 @@ def case_sibc_box():
     s.run()
     _save("sibc_box", prob, _outputs(s, prob, {}), n,
           "copper SIBC walls on y/z and on a copper brick, CPML on x, random initial fields")
+
+
+def case_band_line():
+    """Band-subspace DTBC ports on an inhomogeneous line: a parallel-plate
+    guide half filled with eps_r = 4 (the reference's layered QTEM fixture
+    at 2 x 8 x 16 cells), band ports (1-7.8 GHz, rank p from 3 tracking
+    frequencies) on z_min and z_max, PEC plates, PMC sides; port 1 driven
+    through its ghost period by a Gaussian-modulated pulse along its
+    mid-band subspace direction (set on the operator directly: the
+    analysis's band-limited synthesis needs windows of several thousand
+    steps), 600 steps from initial length 64 (kernel tables 64 .. 1024)."""
+    from magnelio._operators.material_matrices import build_M_eps, build_M_mu
+    from magnelio.boundaries.pec import PECBoundary
+    from magnelio.boundaries.pmc import PMCBoundary
+    from magnelio.materials.material import Material
+    from magnelio.mesh import BoxFace
+    from magnelio.mesh.grid import GridLines
+    from magnelio.mesh.mesher import Mesh
+    from magnelio.ports import PortSpecMultiConductor
+    from magnelio.ports._modal.factory import build_band_dtbc_port
+    from magnelio.ports.recorder import PortSignalRecorder
+    from magnelio.solver.fit_td import FITTimeDomainSolver
+    from magnelio.solver.stability import courant_dt
+
+    w, hy, h_if, dz, nz = 10.0e-3, 8.0e-3, 4.0e-3, 1.0e-3, 16
+    x = np.linspace(0.0, w, 3)
+    y = np.concatenate([np.linspace(0.0, h_if, 5), np.linspace(h_if, hy, 5)[1:]])
+    z = np.linspace(0.0, nz * dz, nz + 1)
+    grid = GridLines(x=x, y=y, z=z)
+    diel = Material(name="diel", epsilon=(4.0,) * 3)
+    bc = {"ymin": "PEC", "ymax": "PEC", "xmin": "PMC", "xmax": "PMC", "zmin": "PMC", "zmax": "PMC"}
+    mesh = Mesh.from_grid(grid, regions=[(diel, (0.0, 0.0, 0.0, w, h_if, nz * dz))], boundary_conditions=bc)
+    dt = courant_dt(mesh.grid, "normal")
+    m_eps, m_mu = build_M_eps(mesh), build_M_mu(mesh)
+    ops = [build_band_dtbc_port(PortSpecMultiConductor(name=nm, plane=face, epsilon_r=None), mesh, m_eps, m_mu,
+                                dt=dt, f_band=(1.0e9, 7.8e9), n_grid=3, n_kernel_init=64)
+           for nm, face in (("p1", BoxFace.Z_MIN), ("p2", BoxFace.Z_MAX))]
+    # ghost source: pulse x the real mid-band direction of channel 0
+    freqs, U = ops[0]._src_directions[0]
+    u = np.real(U[U.shape[0] // 2])
+    u = u / np.max(np.abs(u))
+    k = np.arange(300)
+    pulse = np.exp(-(((k - 110) / 28.0) ** 2)) * np.sin(2 * np.pi * 4.4e9 * k * dt)
+    ops[0]._boundary.require_in_kernel()
+    ops[0]._src_series = pulse[:, None] * u[None, :]
+    ops[0]._excitation_mode = 0
+    rec = PortSignalRecorder(dt, ops)
+    bcs = {"ymin": PECBoundary("ymin"), "ymax": PECBoundary("ymax"), "xmin": PMCBoundary("xmin", grid),
+           "xmax": PMCBoundary("xmax", grid), "zmin": PMCBoundary("zmin", grid), "zmax": PMCBoundary("zmax", grid)}
+    n = 600
+    s = FITTimeDomainSolver(mesh=mesh, boundary_conditions=bcs, ports=ops, recorder=rec, total_time_steps=n,
+                            dt=dt, energy_stop_db=None, port_signal_stop_db=None, verbose=False, backend="numpy",
+                            precision="double")
+    s.setup()
+    prob = problem_from_solver(s, n)
+    s.run()
+    _save("band_line", prob, _outputs(s, prob, {}), n,
+          "band-subspace DTBC ports on a half-filled parallel-plate line, port 1 driven, 600 steps")
 
 
 def case_mixed_box():
@@ -731,6 +792,7 @@ CASES = {
     "cfg3_cross_full": case_cfg3_cross_full,
     "mixed_box": case_mixed_box,
     "sibc_box": case_sibc_box,
+    "band_line": case_band_line,
     "lumped_dft": case_lumped_dft,
     "wg_dtbc": case_wg_dtbc,
     "wg_mur": case_wg_mur,

@@ -72,7 +72,7 @@ def test_kernel_sweep_matches_reference_kernels(precision, tol):
 
 @pytest.mark.parametrize(
     "name", ["cpml_box", "mixed_box", "lumped_dft", "wg_dtbc", "wg_mur", "planewave_box", "dispersive_box",
-             "sibc_box"])
+             "sibc_box", "band_line"])
 @pytest.mark.parametrize("precision,tol", [("double", F64_TOL), ("single", F32_TOL)])
 def test_fields_match_reference(name, precision, tol):
     pe, ph = _peaks(name)
@@ -302,6 +302,33 @@ def test_sibc_walls_resume_bit_exactly_and_need_an_in_place_form():
             e, h = c.read_fields()
         assert _rel(e, d["out.e"], pe) < F32_TOL, kind
         assert _rel(h, d["out.h"], ph) < F32_TOL, kind
+
+
+def test_band_ports_resume_bit_exactly_and_check_their_tables():
+    """Band-subspace DTBC ports: the boundary state, interior trace and
+    histories travel with the device state (resume equals the uninterrupted
+    run bit for bit); a run past the last kernel table is refused before it
+    starts and the handle stays usable; the fused forms refuse the ports."""
+    p, d, n = load_golden("band_line")
+    k = n // 2 + 7
+    with p.build_engine("double") as a:
+        a.step(k)
+        blob = a.state_export()
+        a.step(n - k)
+        ea, ha = a.read_fields()
+        Va, Ia = a.read_vi(0, k, n - k)
+        with pytest.raises(FitbError, match="band port 0: DTBC kernel table"):
+            a.step(10_000)
+        a.step(3)
+        with pytest.raises(FitbError, match="band DTBC ports need an in-place stencil mode"):
+            a.configure_stencil("fused", 16)
+    with p.build_engine("double") as b:
+        b.state_import(blob)
+        b.step(n - k)
+        eb, hb = b.read_fields()
+        Vb, Ib = b.read_vi(0, k, n - k)
+    assert np.array_equal(ea, eb) and np.array_equal(ha, hb)
+    assert np.array_equal(Va, Vb) and np.array_equal(Ia, Ib)
 
 
 def test_missing_dtbc_table_is_an_error_not_a_fault():
