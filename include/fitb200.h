@@ -431,6 +431,14 @@ int fitb_poll_signal_absmax(fitb_handle* h, int32_t b, double* out);
 int fitb_channel_count(fitb_handle* h, int32_t* out);
 int fitb_read_vi(fitb_handle* h, int32_t b, int64_t step0, int64_t n,
                  double* V, double* I);
+/* The same read, asynchronous: D2H copies of steps [step0, step0 + n) of
+ * field set b into V / I (page-locked host memory for an overlapped copy)
+ * queued behind the issued steps; the ticket's completion (fitb_wait_ticket)
+ * means the values have landed.  Statuses of the steps are checked by the
+ * next synchronising call (fitb_sync, fitb_query, fitb_read_*).  A host loop
+ * can so read each step's results while the next step runs. */
+int fitb_read_vi_async(fitb_handle* h, int32_t b, int64_t step0, int64_t n, double* V, double* I, int64_t* ticket);
+int fitb_wait_ticket(fitb_handle* h, int64_t ticket);
 /* Modal S-parameters of the recorded steps [0, steps_done), computed on the
  * device from the V/I records without reading them back (replaces the host
  * post-step compute_s_parameters, src/magnelio/post/modal_sparameters.py

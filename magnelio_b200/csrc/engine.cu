@@ -230,6 +230,10 @@ struct Handle {
     // list on the handle's stream
     cudaStream_t slab_side[kSlabLists] = {};
     cudaEvent_t ev_sfork = nullptr, ev_sjoin[kSlabLists] = {};
+    // completion tickets of asynchronous reads (fitb_read_vi_async): a ring
+    static constexpr int kTickets = 64;
+    cudaEvent_t tickets[kTickets] = {};
+    long long next_ticket = 0;
     DevBuf e, h, aE, bE, aH, bH, meps, mmu, staging;
     // Fused step: second field buffers; `cur` names the buffer set that
     // holds the current fields (always 0 for the in-place kernels).
@@ -301,6 +305,8 @@ struct Handle {
             if (graph_one[q]) cudaGraphExecDestroy(graph_one[q]);
         }
         if (ev_sfork) cudaEventDestroy(ev_sfork);
+        for (auto& t : tickets)
+            if (t) cudaEventDestroy(t);
         for (int q = 0; q < kSlabLists; ++q) {
             if (ev_sjoin[q]) cudaEventDestroy(ev_sjoin[q]);
             if (slab_side[q]) cudaStreamDestroy(slab_side[q]);
@@ -1598,6 +1604,7 @@ int fitb_create(const fitb_desc* desc, fitb_handle** out) {
     ck(cudaEventCreateWithFlags(&H.ev_fork, cudaEventDisableTiming), "event");
     ck(cudaEventCreateWithFlags(&H.ev_join, cudaEventDisableTiming), "event");
     ck(cudaEventCreateWithFlags(&H.ev_sfork, cudaEventDisableTiming), "event");
+    for (auto& t : H.tickets) ck(cudaEventCreateWithFlags(&t, cudaEventDisableTiming), "event");
     for (int q = 1; q < fitb::kSlabLists; ++q) {
         ck(cudaStreamCreateWithFlags(&H.slab_side[q], cudaStreamNonBlocking), "stream");
         ck(cudaEventCreateWithFlags(&H.ev_sjoin[q], cudaEventDisableTiming), "event");
@@ -2923,6 +2930,38 @@ int fitb_probe_wait_timeout(fitb_handle* h, int32_t* status) {
     ck(cudaMemsetAsync(H.status.p, 0, sizeof(int), H.stream), "probe status reset");
     ck(cudaStreamSynchronize(H.stream), "probe sync");
     *status = st;
+    FITB_CATCH
+}
+
+int fitb_read_vi_async(fitb_handle* h, int32_t b, int64_t step0, int64_t n, double* V, double* I, int64_t* ticket) {
+    FITB_TRY
+    Handle& H = H_of(h);
+    if (!ticket) fail(FITB_ERR_ARG, "null ticket");
+    if (b < 0 || b >= H.B) fail(FITB_ERR_ARG, "field set %d out of range", b);
+    if (step0 < 0 || n < 0 || step0 + n > H.steps_done)
+        fail(FITB_ERR_ARG, "steps [%lld, %lld) not issued", (long long)step0, (long long)(step0 + n));
+    const size_t off = ((size_t)b * H.cap + step0) * H.nch;
+    const size_t bytes = (size_t)n * H.nch * sizeof(double);
+    if (H.nch > 0 && n > 0) {
+        if (V) ck(cudaMemcpyAsync(V, H.recV.as<double>() + off, bytes, cudaMemcpyDeviceToHost, H.stream), "read V");
+        if (I) ck(cudaMemcpyAsync(I, H.recI.as<double>() + off, bytes, cudaMemcpyDeviceToHost, H.stream), "read I");
+    }
+    const long long t = H.next_ticket++;
+    ck(cudaEventRecord(H.tickets[t % Handle::kTickets], H.stream), "ticket record");
+    *ticket = t;
+    FITB_CATCH
+}
+
+int fitb_wait_ticket(fitb_handle* h, int64_t ticket) {
+    FITB_TRY
+    Handle& H = H_of(h);
+    if (ticket < 0 || ticket >= H.next_ticket) fail(FITB_ERR_ARG, "ticket %lld was not issued", (long long)ticket);
+    if (ticket < H.next_ticket - Handle::kTickets) {
+        // its event has been reused: the work is older than a later ticket
+        ck(cudaEventSynchronize(H.tickets[(H.next_ticket - Handle::kTickets) % Handle::kTickets]), "ticket wait");
+    } else {
+        ck(cudaEventSynchronize(H.tickets[ticket % Handle::kTickets]), "ticket wait");
+    }
     FITB_CATCH
 }
 

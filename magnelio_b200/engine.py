@@ -561,6 +561,19 @@ class FitEngine:
             check(self._lib.fitb_read_vi(self._h, int(b), int(step0), int(n), f64p(V), f64p(I)))
         return V, I
 
+    def read_vi_async(self, b: int, step0: int, n: int, v_ptr: int, i_ptr: int) -> int:
+        """Queue the D2H copy of the V/I records of steps [step0, step0 + n) of
+        field set ``b`` to host addresses ``v_ptr`` / ``i_ptr`` (n x channels
+        float64 each, page-locked for an overlapped copy); returns a ticket
+        for :meth:`wait_ticket`."""
+        t = C.c_int64()
+        check(self._lib.fitb_read_vi_async(self._h, int(b), int(step0), int(n), v_ptr, i_ptr, C.byref(t)))
+        return int(t.value)
+
+    def wait_ticket(self, ticket: int) -> None:
+        """Block until the asynchronous read behind ``ticket`` has landed."""
+        check(self._lib.fitb_wait_ticket(self._h, int(ticket)))
+
     def s_parameters(self, f, maps, i_cotemporal, excited, a_threshold: float = 1e-12,
                      return_incident: bool = False):
         """Modal S-matrix ``S[f, c, b]`` of the recorded steps, computed on the
