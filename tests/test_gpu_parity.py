@@ -331,6 +331,31 @@ def test_band_ports_resume_bit_exactly_and_check_their_tables():
     assert np.array_equal(Va, Vb) and np.array_equal(Ia, Ib)
 
 
+def test_async_vi_reads_land_the_recorded_values():
+    """fitb_read_vi_async into page-locked memory, one step behind the
+    stepping, gives the recorder's values; an unissued ticket is refused."""
+    import torch
+
+    p, d, n = load_golden("lumped_dft")
+    with p.build_engine("single") as eng:
+        nch = eng.n_channels
+        buf = torch.zeros((2, n, nch), dtype=torch.float64, pin_memory=True)
+        row = nch * 8
+        prev = None
+        for s in range(n):
+            eng.step(1)
+            t = eng.read_vi_async(0, s, 1, buf[0].data_ptr() + s * row, buf[1].data_ptr() + s * row)
+            if prev is not None:
+                eng.wait_ticket(prev)
+            prev = t
+        eng.wait_ticket(prev)
+        V, I = eng.read_vi()
+        assert np.array_equal(buf[0].numpy(), V) and np.array_equal(buf[1].numpy(), I)
+        with pytest.raises(FitbError, match="was not issued"):
+            eng.wait_ticket(prev + 1)
+    assert _rel(V, d["out.V"]) < F32_TOL
+
+
 def test_missing_dtbc_table_is_an_error_not_a_fault():
     from magnelio_b200._lib import FitbError
 
