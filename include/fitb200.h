@@ -341,6 +341,19 @@ int fitb_set_band_kernel(fitb_handle* h, int32_t port, int32_t incoming, int32_t
  * set_excitation_band, :940-1118); needs the incoming kernel. */
 int fitb_set_band_source(fitb_handle* h, int32_t port, int32_t b, int64_t n_samples, const double* s);
 
+/* ---- 2-D port modes --------------------------------------------------- */
+/* The numerical core of Numerical2DModeSolver._solve_te_tm
+ * (src/magnelio/ports/_modal/numerical_2d.py:454-585) on the GPU of
+ * `device`, in float64: the n_modes lowest eigenvalues above `threshold`
+ * of K v = lambda M v (K: the 2-D curl-curl stiffness on the n free port
+ * edges as CSR, M: their epsilon-mass diagonal) with eigenvectors
+ * normalised to v^T M v = 1, eigvecs [n_modes][n].  Dense Householder
+ * tridiagonalisation of M^-1/2 K M^-1/2, bisection on the Sturm sequence,
+ * inverse iteration, back-transformation.  The sign of each vector is the
+ * caller's.  n <= 16384, n_modes <= 64; needs no handle. */
+int fitb_mode_solve(int32_t device, int64_t n, const int64_t* rowptr, const int64_t* col, const double* val,
+                    const double* m_diag, int32_t n_modes, double threshold, double* eigvals, double* eigvecs);
+
 /* ---- surface-impedance walls ---------------------------------------- */
 /* One SIBC wall tag (solver/_sibc.py:88-264, hooks at fit_td.py:837-840 and
  * :909-914): n_faces flat indices into the reference H vector with their

@@ -2933,6 +2933,36 @@ int fitb_probe_wait_timeout(fitb_handle* h, int32_t* status) {
     FITB_CATCH
 }
 
+int fitb_mode_solve(int32_t device, int64_t n, const int64_t* rowptr, const int64_t* col, const double* val,
+                    const double* m_diag, int32_t n_modes, double threshold, double* eigvals, double* eigvecs) {
+    FITB_TRY
+    if (n < 3 || n > 16384) fail(FITB_ERR_LIMIT, "mode problem of %lld unknowns (3 .. 16384)", (long long)n);
+    if (n_modes < 1 || n_modes > 64 || n_modes > n - 2) fail(FITB_ERR_ARG, "n_modes %d", n_modes);
+    if (!rowptr || !col || !val || !m_diag || !eigvals || !eigvecs) fail(FITB_ERR_ARG, "null argument");
+    const long long nnz = rowptr[n];
+    if (nnz < 0 || rowptr[0] != 0) fail(FITB_ERR_ARG, "row pointers");
+    for (long long i = 0; i < n; ++i) {
+        if (rowptr[i + 1] < rowptr[i]) fail(FITB_ERR_ARG, "row pointers not ascending");
+        if (!(m_diag[i] > 0.0)) fail(FITB_ERR_ARG, "M diagonal entry %lld not positive", i);
+    }
+    for (long long q = 0; q < nnz; ++q)
+        if (col[q] < 0 || col[q] >= n) fail(FITB_ERR_ARG, "column index %lld out of range", (long long)col[q]);
+    ck(cudaSetDevice(device), "set device");
+    fitb::DevBuf drp, dcol, dval, dm;
+    fitb::upload(drp, std::vector<long long>(rowptr, rowptr + n + 1));
+    fitb::upload(dcol, std::vector<long long>(col, col + nnz));
+    fitb::upload(dval, std::vector<double>(val, val + nnz));
+    fitb::upload(dm, std::vector<double>(m_diag, m_diag + n));
+    cudaStream_t s;
+    ck(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "stream");
+    const int rc = fitb::mode_eigensolve(n, drp.as<long long>(), dcol.as<long long>(), dval.as<double>(),
+                                         dm.as<double>(), n_modes, threshold, eigvals, eigvecs, s);
+    cudaStreamDestroy(s);
+    if (rc == -3) fail(FITB_ERR_ARG, "fewer than %d eigenvalues above the threshold", n_modes);
+    if (rc != 0) fail(FITB_ERR_CUDA, "mode eigensolve failed (%d)", rc);
+    FITB_CATCH
+}
+
 int fitb_read_vi_async(fitb_handle* h, int32_t b, int64_t step0, int64_t n, double* V, double* I, int64_t* ticket) {
     FITB_TRY
     Handle& H = H_of(h);

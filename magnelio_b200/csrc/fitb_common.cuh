@@ -511,6 +511,12 @@ void launch_setup_materials(const Geom& g, const double* dx, const double* dy, c
 // x is scratch of 8 n complex samples.
 void launch_dtbc_kernel(double r, double q, int n, double2* x, double* l, cudaStream_t s);
 
+// Lowest n_modes eigenpairs above threshold of K v = lambda M v (K CSR on
+// the device, M its diagonal) in float64 (modes.cu); eigenvectors with
+// v^T M v = 1 into vec_out [n_modes][n] (host); 0 on success.
+int mode_eigensolve(long long n, const long long* rp, const long long* col, const double* val, const double* m,
+                    int n_modes, double threshold, double* lam_out, double* vec_out, cudaStream_t s);
+
 // lambda_max of the live leapfrog update operator D^-1/2 C^T M_mu^-1 C D^-1/2
 // by a float64 Lanczos iteration (spectral.cu); 0 on success.
 template <typename T>

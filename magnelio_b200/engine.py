@@ -37,6 +37,31 @@ def _f64(a) -> np.ndarray:
     return np.ascontiguousarray(np.asarray(a, dtype=np.float64))
 
 
+def port_modes(K, m_diag, n_modes: int, threshold: float, device: int = 0):
+    """The n_modes lowest eigenpairs above ``threshold`` of the 2-D port-mode
+    problem ``K v = lambda M v`` (``K`` a scipy sparse matrix on the free port
+    edges, ``m_diag`` the diagonal of ``M``), solved on the GPU in float64
+    (``fitb_mode_solve``; the numerical core of the reference's
+    ``Numerical2DModeSolver._solve_te_tm``).  Returns ``(eigvals,
+    eigvecs)`` with ``eigvecs`` of shape (n, n_modes), ``v^T M v = 1``; the
+    sign of each column is the caller's."""
+    import scipy.sparse as sp
+
+    Kc = sp.csr_matrix(K)
+    Kc.sort_indices()
+    n = Kc.shape[0]
+    rp = np.ascontiguousarray(Kc.indptr, dtype=np.int64)
+    col = np.ascontiguousarray(Kc.indices, dtype=np.int64)
+    val = np.ascontiguousarray(Kc.data, dtype=np.float64)
+    m = np.ascontiguousarray(m_diag, dtype=np.float64)
+    lam = np.zeros(n_modes)
+    vec = np.zeros((n_modes, n))
+    lib = _lib.load()
+    check(lib.fitb_mode_solve(int(device), int(n), i64p(rp), i64p(col), f64p(val), f64p(m), int(n_modes),
+                              float(threshold), f64p(lam), f64p(vec)))
+    return lam, vec.T.copy()
+
+
 class FitEngine:
     """Device-resident FIT-TD state on one GPU.
 

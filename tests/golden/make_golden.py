@@ -315,6 +315,43 @@ def case_band_line():
           "band-subspace DTBC ports on a half-filled parallel-plate line, port 1 driven, 600 steps")
 
 
+def case_modes_wr90():
+    """The 2-D port-mode eigenproblem of the WR-90 guide's z_min plane on the
+    29 x 13 cell cross-section of the flagship configuration: the free-edge
+    curl-curl stiffness K and epsilon-mass M the reference assembles, and
+    the reference's Numerical2DModeSolver TE modes (three lowest, sign
+    resolved) as the expected eigenpairs."""
+    from magnelio._operators.curl import build_curl_matrix
+    from magnelio._operators.material_matrices import build_M_eps, build_M_mu
+    from magnelio.mesh import BoxFace
+    from magnelio.ports._modal.curl_curl_2d import build_2d_curl_curl
+    from magnelio.ports._modal.factory import _resolve_pec_edge_mask
+    from magnelio.ports._modal.mode import ModeType
+    from magnelio.ports._modal.numerical_2d import Numerical2DModeSolver
+    from magnelio.ports._modal.port_plane import PortPlane
+
+    mesh = _wr90(nx=29, ny=13, nz=8, length=8e-3)
+    m_eps, m_mu = build_M_eps(mesh), build_M_mu(mesh)
+    plane = PortPlane.from_mesh(BoxFace.Z_MIN, mesh)
+    pec = _resolve_pec_edge_mask(plane, mesh)
+    K, M, primal = build_2d_curl_curl(plane, mesh.grid, m_eps, m_mu, build_curl_matrix(mesh.grid))
+    solver = Numerical2DModeSolver(plane=plane, K=K, M=M, primal_2d_indices=primal, pec_edge_mask=pec,
+                                   epsilon_r=1.0, mode_type=ModeType.TE, m_mu_flat=m_mu)
+    n_modes = 3
+    modes = solver.solve(n_modes=n_modes, f_calc=10e9)
+    free = np.where(~np.asarray(pec))[0]
+    Kf = K.tocsr()[free, :][:, free].tocsr()
+    Kf.sort_indices()
+    Mf = np.asarray(M.tocsr()[free, :][:, free].diagonal(), float)
+    sigma = solver._sigma_heuristic()
+    vec = np.stack([np.concatenate([m.discrete_e_u_profile, m.discrete_e_v_profile])[free] for m in modes], axis=1)
+    lam = np.array([m.omega_c ** 2 for m in modes])
+    np.savez_compressed(HERE / "modes_wr90.npz", indptr=Kf.indptr.astype(np.int64), indices=Kf.indices.astype(np.int64),
+                        data=Kf.data, m=Mf, threshold=np.asarray(1e-3 * sigma), n_modes=np.asarray(n_modes),
+                        eigvals=lam, eigvecs=vec)
+    print(f"modes_wr90: n_free={free.size}, nnz={Kf.nnz}, lambda={lam}")
+
+
 def case_mixed_box():
     """CPML on x and zmax, PEC on ymin / zmin, PMC on ymax."""
     from magnelio.boundaries.cpml import CPMLBoundary
@@ -793,6 +830,7 @@ CASES = {
     "mixed_box": case_mixed_box,
     "sibc_box": case_sibc_box,
     "band_line": case_band_line,
+    "modes_wr90": case_modes_wr90,
     "lumped_dft": case_lumped_dft,
     "wg_dtbc": case_wg_dtbc,
     "wg_mur": case_wg_mur,

@@ -356,6 +356,30 @@ def test_async_vi_reads_land_the_recorded_values():
     assert _rel(V, d["out.V"]) < F32_TOL
 
 
+def test_port_modes_on_the_device_match_the_reference_mode_solver():
+    """The 2-D port-mode eigenproblem of the WR-90 plane (712 free edges)
+    solved on the GPU in float64 (dense Householder tridiagonalisation,
+    bisection, inverse iteration) reproduces the reference's
+    Numerical2DModeSolver eigenvalues and, up to sign, its M-normalised
+    eigenvectors; too many requested modes is an error, not a fault."""
+    import scipy.sparse as sp
+
+    from magnelio_b200.engine import port_modes
+
+    d = np.load(__import__("conftest").GOLDEN / "modes_wr90.npz")
+    n = d["m"].size
+    K = sp.csr_matrix((d["data"], d["indices"], d["indptr"]), shape=(n, n))
+    lam, vec = port_modes(K, d["m"], int(d["n_modes"]), float(d["threshold"]))
+    assert np.allclose(lam, d["eigvals"], rtol=1e-10, atol=0.0)
+    for q in range(lam.size):
+        ref = d["eigvecs"][:, q]
+        v = vec[:, q] * np.sign(vec[:, q] @ ref)
+        assert np.max(np.abs(v - ref)) <= 1e-9 * np.max(np.abs(ref)), q
+        assert abs(v @ (d["m"] * v) - 1.0) < 1e-12
+    with pytest.raises(FitbError):
+        port_modes(K, d["m"], n, float(d["threshold"]))
+
+
 def test_missing_dtbc_table_is_an_error_not_a_fault():
     from magnelio_b200._lib import FitbError
 
