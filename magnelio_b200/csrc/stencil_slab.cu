@@ -919,33 +919,9 @@ bool plan_slab_units(const Geom& g, const FaceDev* f, int nfaces, int tj, int ic
     for (int t = 0; t < nkt; ++t) fk[t] = faces_on(2, t * TK, t * TK + TK);
     for (int t = 0; t < njt; ++t) fj[t] = faces_on(1, t * tj, t * tj + tj);
     for (int c = 0; c < nch; ++c) fi[c] = faces_on(0, chunks[c].x, chunks[c].y);
-    // columns (j tile, k tile) clear of the y and z faces may march longer
-    // chunks than the others (FITB_SLAB_FREE_ICHUNK planes; tuning switch,
-    // every value computes the same bits): fewer i planes read twice
-    static const int free_ichunk = [] {
-        const char* e = std::getenv("FITB_SLAB_FREE_ICHUNK");
-        return e ? std::max(0, std::atoi(e)) : 0;
-    }();
-    std::vector<int2> fchunks;
-    std::vector<unsigned> ffi;
-    if (free_ichunk > 0 && free_ichunk != ichunk) {
-        fchunks = slab_chunks(g, f, nfaces, free_ichunk);
-        for (const int2& c : fchunks) ffi.push_back(faces_on(0, c.x, c.y));
-    }
-    const bool split = !fchunks.empty();
-    if (split)
-        for (size_t c = 0; c < fchunks.size(); ++c)
-            for (int jt = 0; jt < njt; ++jt)
-                for (int kt = 0; kt < nkt; ++kt) {
-                    if (fj[jt] | fk[kt]) continue;
-                    const unsigned m = ffi[c];
-                    if (m) continue;  // x-slab chunks: with the other columns below
-                    out[0].push_back(make_int4(kt | (jt << 16), fchunks[c].x, fchunks[c].y, 0));
-                }
     for (int c = 0; c < nch; ++c)
         for (int jt = 0; jt < njt; ++jt)
             for (int kt = 0; kt < nkt; ++kt) {
-                if (split && !(fj[jt] | fk[kt]) && !fi[c]) continue;  // planned above
                 const unsigned m = fi[c] | fj[jt] | fk[kt];
                 const int ns = __builtin_popcount(m);
                 const int list = ns <= 3 ? ns : 4;  // capacities 0, 1, 2, 3, 6
