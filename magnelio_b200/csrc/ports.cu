@@ -142,6 +142,23 @@ __global__ void __launch_bounds__(kPortThreads)
     const double vport0 = Vport_prev[tm], vint0 = Vint_prev[tm], u0 = u[tm], up0 = u_prev[tm];
     const double mur = d.mur_r[tm];
     const bool dtbc = d.is_dtbc[tm];
+    const double r2 = d.r2[tm], q2 = d.q2[tm];
+    // the excitation samples this step needs (they do not depend on the
+    // fields): Mur TF/SF source terms, or the DTBC ghost source
+    double src_new = 0.0, inc_int_now = 0.0, inc_int_prev = 0.0, inc_face_prev = 0.0, src_dtbc = 0.0;
+    if (threadIdx.x < M && tm == exc) {
+        const double* wf = d.wf + (long long)b * d.n_wf;
+        if (!dtbc) {
+            const long long t1 = n + 1;
+            src_new = (t1 < d.n_wf) ? wf[t1] : 0.0;
+            const int maxlen = d.buf_len[b];
+            inc_int_now = interp_delayed(wf, d.n_wf, n, maxlen, d.tau[tm], d.dt);
+            inc_int_prev = interp_delayed(wf, d.n_wf, n, maxlen, d.tau[tm] + d.dt, d.dt);
+            inc_face_prev = interp_delayed(wf, d.n_wf, n, maxlen, d.dt, d.dt);
+        } else {
+            src_dtbc = n < d.n_wf ? wf[n] : 0.0;
+        }
+    }
 
     // 2. DTBC boundary convolutions conv_w = sum_{m=1..n} l_m w[n-m] and
     //    u_inc = sum l_m s[n-m]: the partial sums k_dtbc_conv left per
@@ -179,39 +196,55 @@ __global__ void __launch_bounds__(kPortThreads)
         for (int m = 0; m < kMaxModes; ++m)
             if (m < M) acc[kMaxModes + m] += mh * (d.hprof[(long long)m * nh + p] * v);
     }
+    // the port-plane data of this thread's first edge, read before the
+    // barriers (none of it depends on this step's modal values)
+    double ep0[kMaxModes], vp0[kMaxModes];
+    long long pe0 = 0;
+    double me0 = 0.0, cl0 = 0.0, cr0 = 0.0, csa0 = 0.0, csb0 = 0.0, ei0 = 0.0;
+    const int p0 = threadIdx.x;
+    double* cstate = d.comp_state + (long long)b * 2 * ne;
+    if (p0 < ne) {
+#pragma unroll
+        for (int m = 0; m < kMaxModes; ++m) {
+            ep0[m] = m < M ? d.eprof[(long long)m * ne + p0] : 0.0;
+            vp0[m] = m < M ? d.vprof[(long long)m * ne + p0] : 0.0;
+        }
+        pe0 = d.port_e[p0];
+        me0 = d.me_port[p0];
+        ei0 = eint[p0];
+        if (d.comp_on) {
+            cl0 = d.comp_live[p0];
+            cr0 = d.comp_r[p0];
+            csa0 = cstate[p0];
+            csb0 = cstate[ne + p0];
+        }
+    }
     block_sum_modes<false>(acc, M, red, wred);  // ends with a block barrier (s_conv too)
 
     // 3. Per-mode boundary value: one thread per mode (the modes' scalar
     //    float64 recursions are independent of each other).
     if (threadIdx.x < M) {
-        const double* wf = d.wf + (long long)b * d.n_wf;
         const int m = threadIdx.x;
         const double vin = red[m];
         s_vint[m] = vin;
         double vc = vint0 + mur * (vin - vport0);
         if (m == exc && !dtbc) {
-            const long long t1 = n + 1;
-            const double src_new = (t1 < d.n_wf) ? wf[t1] : 0.0;
-            const int maxlen = d.buf_len[b];
-            const double inc_int_now = interp_delayed(wf, d.n_wf, n, maxlen, d.tau[m], d.dt);
-            const double inc_int_prev = interp_delayed(wf, d.n_wf, n, maxlen, d.tau[m] + d.dt, d.dt);
-            const double inc_face_prev = interp_delayed(wf, d.n_wf, n, maxlen, d.dt, d.dt);
             const double scat_int_now = vin - inc_int_now;
             const double scat_int_prev = vint0 - inc_int_prev;
             const double scat_face_prev = vport0 - inc_face_prev;
             vc = src_new + scat_int_prev + mur * (scat_int_now - scat_face_prev);
         }
         if (dtbc) {
-            const double src = (m == exc && n < d.n_wf) ? wf[n] : 0.0;
+            const double src = m == exc ? src_dtbc : 0.0;
             const double conv_w = s_conv[2 * m], u_inc = s_conv[2 * m + 1];
             const double ghost = src + conv_w;
             double* wh = d.whist + ((long long)b * M + m) * d.cap;
             double* sh = d.shist + ((long long)b * M + m) * d.cap;
             wh[n] = u0 - u_inc;
             sh[n] = src;
-            double un = (2.0 - 2.0 * d.r2[m] - d.q2[m]) * u0;
+            double un = (2.0 - 2.0 * r2 - q2) * u0;
             un = un - up0;
-            un = un + d.r2[m] * (ghost + vint0);
+            un = un + r2 * (ghost + vint0);
             u_prev[m] = u0;
             u[m] = un;
             vc = un;
@@ -225,26 +258,41 @@ __global__ void __launch_bounds__(kPortThreads)
     //    value each thread has just stored (acc[0..M)).
 #pragma unroll
     for (int m = 0; m < kMaxModes; ++m) acc[m] = 0.0;
-    for (int p = threadIdx.x; p < ne; p += blockDim.x) {
+    auto edge = [&](int p, const double (&ep)[kMaxModes], const double (&vp)[kMaxModes], long long pe, double me,
+                    double cl, double cr, double csa, double csb, double ei) {
         double v = 0.0;
-        for (int m = 0; m < M; ++m) v += s_vc[m] * d.eprof[(long long)m * ne + p];
+#pragma unroll
+        for (int m = 0; m < kMaxModes; ++m)
+            if (m < M) v += s_vc[m] * ep[m];
         if (d.comp_on) {
-            double* cs = d.comp_state + (long long)b * 2 * ne;
-            double ci = eint[p];
-            for (int m = 0; m < M; ++m) ci -= s_vint[m] * d.eprof[(long long)m * ne + p];
-            const double cp = d.comp_live[p] * (cs[p] + d.comp_r[p] * (ci - cs[ne + p]));
+            double ci = ei;
+#pragma unroll
+            for (int m = 0; m < kMaxModes; ++m)
+                if (m < M) ci -= s_vint[m] * ep[m];
+            const double cp = cl * (csa + cr * (ci - csb));
             v += cp;
-            cs[p] = ci;
-            cs[ne + p] = cp;
+            cstate[p] = ci;
+            cstate[ne + p] = cp;
         }
         enew[p] = v;
         const T stored = (T)v;
-        E[d.port_e[p]] = stored;
+        E[pe] = stored;
         const double vr = (double)stored;
-        const double me = d.me_port[p];
 #pragma unroll
         for (int m = 0; m < kMaxModes; ++m)
-            if (m < M) acc[m] += me * (d.vprof[(long long)m * ne + p] * vr);
+            if (m < M) acc[m] += me * (vp[m] * vr);
+    };
+    if (p0 < ne) edge(p0, ep0, vp0, pe0, me0, cl0, cr0, csa0, csb0, ei0);
+    for (int p = p0 + blockDim.x; p < ne; p += blockDim.x) {
+        double ep[kMaxModes], vp[kMaxModes];
+#pragma unroll
+        for (int m = 0; m < kMaxModes; ++m) {
+            ep[m] = m < M ? d.eprof[(long long)m * ne + p] : 0.0;
+            vp[m] = m < M ? d.vprof[(long long)m * ne + p] : 0.0;
+        }
+        const bool c = d.comp_on != 0;
+        edge(p, ep, vp, d.port_e[p], d.me_port[p], c ? d.comp_live[p] : 0.0, c ? d.comp_r[p] : 0.0,
+             c ? cstate[p] : 0.0, c ? cstate[ne + p] : 0.0, eint[p]);
     }
     block_sum_modes<true>(acc, M, red, wred);
     if (threadIdx.x < M) {
