@@ -731,3 +731,18 @@ class OracleRun:
         """``fit_td.py:1014-1018``."""
         p = self.p
         return 0.5 * (float(np.sum(p.M_eps * self.f.e * self.f.e)) + float(np.sum(p.M_mu * self.f.h * self.f.h)))
+
+
+def dense_port_modes(K, m_diag, threshold: float, n_modes: int):
+    """The ``n_modes`` lowest eigenpairs above ``threshold`` of
+    ``K v = lambda diag(m) v`` by a dense float64 eigensolve of
+    ``M^-1/2 K M^-1/2``, vectors scaled to ``v^T M v = 1``: the checker-side
+    stand-in for the device mode solve (the reference solves the same
+    problem with shift-invert ARPACK, ``ports/_modal/numerical_2d.py:
+    497-544``)."""
+    m = np.asarray(m_diag, float)
+    s = 1.0 / np.sqrt(m)
+    A = K.toarray() * s[:, None] * s[None, :]
+    lam, X = np.linalg.eigh(0.5 * (A + A.T))
+    keep = np.nonzero(lam > threshold)[0][:n_modes]
+    return lam[keep], X[:, keep] * s[:, None]

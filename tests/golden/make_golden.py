@@ -502,6 +502,57 @@ def _wg_solver(mesh, excited, n, modify=None, n_modes=2):
     return s
 
 
+def case_ridge_ports():
+    """Single-ridge guide (22.86 x 10.16 mm, 14 x 8 x 10 cells, 12 mm long,
+    a PEC ridge 4 cells wide and 3 cells deep from the top wall along the
+    whole length), two waveguide ports (zmin, zmax) with 3 modes each,
+    port p1 mode 0 driven, 400 steps.  Stores the reference-built problem,
+    the mesh's flat E PEC mask, the mode-calculation frequency, each
+    channel's power-wave map and the reference's V/I: the inputs and
+    expected outputs of a port built without the reference."""
+    from magnelio.materials.material import Material
+    from magnelio.mesh.grid import GridLines
+    from magnelio.mesh.mesher import Mesh
+    from magnelio.post.modal_sparameters import spectral_power_waves
+
+    A, B, L = 22.86e-3, 10.16e-3, 12e-3
+    nx, ny, nz, n = 14, 8, 10, 400
+    grid = GridLines(x=np.linspace(0, A, nx + 1), y=np.linspace(0, B, ny + 1), z=np.linspace(0, L, nz + 1))
+    x0, x1, y0 = grid.x[5], grid.x[9], grid.y[5]
+    metal = Material(name="metal", is_pec=True)
+    mesh = Mesh.from_grid(grid, regions=[(metal, (x0, y0, 0.0, x1, B, L))], boundary_conditions={
+        "xmin": "PEC", "xmax": "PEC", "ymin": "PEC", "ymax": "PEC", "zmin": "PMC", "zmax": "PMC"})
+    s = _wg_solver(mesh, ("p1", 0), n, n_modes=3)
+    prob = problem_from_solver(s, n)
+    pm = mesh.pec_mask_edges
+    n_ex, n_ey, n_ez = nx * (ny + 1) * (nz + 1), (nx + 1) * ny * (nz + 1), (nx + 1) * (ny + 1) * nz
+    out = {"ridge.pec": np.concatenate([pm[0, :n_ex], pm[1, :n_ey], pm[2, :n_ez]]).astype(bool),
+           "ridge.f_calc": np.asarray(25e9)}
+    import magnelio.analysis.scattering_td as std
+    from magnelio._operators.material_matrices import build_M_eps, build_M_mu
+    from magnelio.ports.declarative import PortWaveguide
+
+    an = std.AnalysisScatteringTD(mesh=mesh, f_max=25e9, ports=[PortWaveguide("p1", "zmin", n_modes=3),
+                                                                PortWaveguide("p2", "zmax", n_modes=3)],
+                                  verbose=False, backend="numpy", precision="double", n_freq=11)
+    m_eps, m_mu = build_M_eps(mesh), build_M_mu(mesh)
+    _, _, _, _, _, modes, ndx, lines = an._prepare_excitation_run(("p1", 0), None, m_eps, m_mu, s.dt, 25e9)
+    f = np.linspace(6e9, 25e9, 24)
+    out["ridge.f"] = f
+    one, zero = np.ones_like(f, complex), np.zeros_like(f, complex)
+    c = 0
+    for port in ("p1", "p2"):
+        for m in range(3):
+            aV, bV = spectral_power_waves(one, zero, 2 * np.pi * f, s.dt, modes[port][m], normal_dx=ndx[port],
+                                          line_params=lines.get((port, m)))
+            aI, bI = spectral_power_waves(zero, one, 2 * np.pi * f, s.dt, modes[port][m], normal_dx=ndx[port],
+                                          line_params=lines.get((port, m)))
+            out[f"ridge.map{c}"] = np.stack([aV, aI, bV, bI])
+            c += 1
+    s.run()
+    _save("ridge_ports", prob, _outputs(s, prob, out), n, "single-ridge guide, 2 ports x 3 modes, p1 mode 0 driven")
+
+
 def case_cfg1_wr90():
     """The plain small configuration: WR-90 section 22.86 x 10.16 x 40 mm on a
     29 x 13 x 51 grid, two waveguide ports (zmin, zmax) x 3 modes, all six
@@ -833,6 +884,7 @@ CASES = {
     "modes_wr90": case_modes_wr90,
     "lumped_dft": case_lumped_dft,
     "wg_dtbc": case_wg_dtbc,
+    "ridge_ports": case_ridge_ports,
     "wg_mur": case_wg_mur,
     "wg_stop": case_wg_stop,
     "cpml_stop": case_cpml_stop,

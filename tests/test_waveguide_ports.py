@@ -1,0 +1,154 @@
+"""Modal waveguide ports built without the reference
+(``magnelio_b200/waveguide_ports.py``) against the ports the reference's
+``build_modal_port`` built for the golden fixtures: WR-90 with 2 and 3
+modes, and a single-ridge guide whose wall contour comes from the mesh's
+PEC mask.  The eigensolve here is the oracle's dense host solve; the GPU
+tests repeat the build with the device solve."""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from magnelio_b200 import waveguide_ports as wp
+from magnelio_b200.adapter import _pec_face_flat_indices
+from oracle.fit_oracle import dense_port_modes
+
+F_CALC = 25e9
+PORT_KEYS = ("port_e_idx", "int_e_idx", "port_h_idx", "me_port", "me_int", "mh_port", "e_profile", "v_profile",
+             "h_profile", "mur_r", "tau", "record_scale", "is_dtbc", "dtbc_r", "dtbc_q")
+
+
+def _inputs(d, name):
+    x, y, z = (np.concatenate([[0.0], np.cumsum(d[f"p.{k}"])]) for k in ("dx", "dy", "dz"))
+    if "ridge.pec" in d:
+        pec = np.asarray(d["ridge.pec"], bool)
+    else:
+        pec = np.zeros(d["p.M_eps"].size, bool)
+        for f in ("xmin", "xmax", "ymin", "ymax"):
+            pec[_pec_face_flat_indices(x.size - 1, y.size - 1, z.size - 1, f)] = True
+    return x, y, z, d["p.M_eps"], d["p.M_mu"], pec, float(d["p.dt"])
+
+
+def _rel(a, b):
+    a, b = np.asarray(a), np.asarray(b)
+    return float(np.max(np.abs(a - b)) / max(float(np.max(np.abs(b))), 1e-300))
+
+
+def build_fixture_ports(name, n_modes, eigensolve):
+    d = dict(np.load(__import__("conftest").GOLDEN / f"{name}.npz", allow_pickle=True))
+    x, y, z, me, mm, pec, dt = _inputs(d, name)
+    ports = [wp.build_waveguide_port(x, y, z, me, mm, pec, face, n_modes, dt, F_CALC, eigensolve=eigensolve)
+             for face in ("zmin", "zmax")]
+    return d, ports, dt
+
+
+@pytest.mark.parametrize("name,n_modes", [("wg_dtbc", 2), ("cfg1_wr90", 3), ("ridge_ports", 3)])
+def test_ports_match_the_reference_builder(name, n_modes):
+    d, ports, dt = build_fixture_ports(name, n_modes, dense_port_modes)
+    for q, w in enumerate(ports):
+        for k in PORT_KEYS:
+            got, ref = np.asarray(getattr(w.port, k)), d[f"p.modal{q}.{k}"]
+            assert got.shape == ref.shape, k
+            if k.endswith("idx") or k == "is_dtbc":
+                assert np.array_equal(got, ref), k
+            elif k in ("me_port", "me_int", "mh_port"):
+                assert np.array_equal(got, ref), k  # masses are copied, not computed
+            else:
+                # eigenvectors from a different eigensolver: round-off only
+                assert _rel(got, ref) < 5e-12, (q, k, _rel(got, ref))
+        assert np.array_equal(w.port.complement[0], d[f"p.modal{q}.comp_r"])
+        assert np.array_equal(w.port.complement[1], d[f"p.modal{q}.comp_live"])
+
+
+@pytest.mark.parametrize("name", ["cfg1_wr90", "ridge_ports"])
+def test_power_wave_maps_match_the_reference(name):
+    d, ports, dt = build_fixture_ports(name, 3, dense_port_modes)
+    f = d["cfg1.f_axis"] if name == "cfg1_wr90" else d["ridge.f"]
+    key = "cfg1.map" if name == "cfg1_wr90" else "ridge.map"
+    dtm = float(d["cfg1.dt"]) if name == "cfg1_wr90" else dt
+    c = 0
+    for w in ports:
+        for m in range(3):
+            assert _rel(wp.power_wave_maps(w.channels[m], f, dtm), d[f"{key}{c}"]) < 1e-10, c
+            c += 1
+
+
+@pytest.mark.parametrize("name,n_modes", [("wg_dtbc", 2), ("ridge_ports", 3)])
+def test_excitation_samples_match_the_reference(name, n_modes):
+    d, ports, dt = build_fixture_ports(name, n_modes, dense_port_modes)
+    ref = d["p.modal0.exc0.w"]
+    m = int(d["p.modal0.exc0.mode"])
+    w = ports[0]
+    got = wp.excitation_samples(w, m, wp.excitation_waveform(w.channels[m].omega_c, F_CALC), dt, ref.size - 2)
+    assert _rel(got, ref) < 1e-12
+
+
+def _box(nx, ny, nz, a, b, length):
+    return np.linspace(0, a, nx + 1), np.linspace(0, b, ny + 1), np.linspace(0, length, nz + 1)
+
+
+def _vacuum(x, y, z):
+    from magnelio_b200 import host
+
+    n = (x.size - 1, y.size - 1, z.size - 1)
+    me = host.build_M_eps(x, y, z, np.array([1.0]), np.zeros(n, np.int32))
+    mm = host.build_M_mu(x, y, z)
+    pec = np.zeros(me.size, bool)
+    for f in ("xmin", "xmax", "ymin", "ymax"):
+        pec[_pec_face_flat_indices(*n, f)] = True
+    return me, mm, pec
+
+
+def test_a_tm_mode_among_the_kept_ones_is_refused():
+    """Square guide: TE10 / TE01 are degenerate and TM11 sits beside TE11,
+    so three modes would keep a TM channel."""
+    x, y, z = _box(10, 10, 6, 10e-3, 10e-3, 6e-3)
+    me, mm, pec = _vacuum(x, y, z)
+    dt = 0.5 * 1e-3 / 3e8
+    with pytest.raises(NotImplementedError, match="TM mode"):
+        wp.build_waveguide_port(x, y, z, me, mm, pec, "zmin", 3, dt, 40e9, eigensolve=dense_port_modes)
+    w = wp.build_waveguide_port(x, y, z, me, mm, pec, "zmin", 2, dt, 40e9, eigensolve=dense_port_modes)
+    # the degenerate pair is rotated to the principal u-energy axes: the
+    # first vector carries (almost) all of its energy on the u-edges
+    e = w.port.e_profile
+    n_u = w.port.n_e_u
+    share = [float(np.sum(v[:n_u] ** 2) / np.sum(v ** 2)) for v in e]
+    assert share[0] > 0.99 and share[1] < 0.01
+    assert abs(w.channels[0].omega_c - w.channels[1].omega_c) < 1e-9 * w.channels[0].omega_c
+
+
+def test_ports_need_three_equidistant_cells():
+    x, y, _ = _box(8, 4, 6, 22.86e-3, 10.16e-3, 6e-3)
+    z = np.array([0.0, 1e-3, 2.5e-3, 3.5e-3, 4.5e-3, 5.5e-3, 6.5e-3])
+    me, mm, pec = _vacuum(x, y, z)
+    with pytest.raises(ValueError, match="equidistant"):
+        wp.build_waveguide_port(x, y, z, me, mm, pec, "zmin", 1, 1e-12, 20e9, eigensolve=dense_port_modes)
+    w = wp.build_waveguide_port(x, y, z, me, mm, pec, "zmax", 1, 1e-12, 20e9, eigensolve=dense_port_modes)
+    assert w.port.n_modes == 1
+
+
+def test_x_and_y_faces_mirror_the_z_faces():
+    """A guide along x has the same cut-offs and calibration as the same
+    guide along z."""
+    a, b, L = 22.86e-3, 10.16e-3, 8e-3
+    xz, yz, zz = _box(12, 6, 8, a, b, L)
+    me, mm, pec = _vacuum(xz, yz, zz)
+    dt = 1e-12
+    ref = wp.build_waveguide_port(xz, yz, zz, me, mm, pec, "zmin", 2, dt, 20e9, eigensolve=dense_port_modes)
+    # the same guide along x: cross-section (y, z) = (a, b)
+    xx, yy, z2 = np.linspace(0, L, 9), np.linspace(0, a, 13), np.linspace(0, b, 7)
+    from magnelio_b200 import host
+
+    n = (8, 12, 6)
+    me2 = host.build_M_eps(xx, yy, z2, np.array([1.0]), np.zeros(n, np.int32))
+    mm2 = host.build_M_mu(xx, yy, z2)
+    pec2 = np.zeros(me2.size, bool)
+    for f in ("ymin", "ymax", "zmin", "zmax"):
+        pec2[_pec_face_flat_indices(*n, f)] = True
+    for face in ("xmin", "xmax"):
+        got = wp.build_waveguide_port(xx, yy, z2, me2, mm2, pec2, face, 2, dt, 20e9, eigensolve=dense_port_modes)
+        for q in range(2):
+            assert abs(got.channels[q].omega_c / ref.channels[q].omega_c - 1.0) < 1e-12
+        assert np.allclose(got.port.record_scale, ref.port.record_scale, rtol=1e-10)
+        assert np.allclose(got.port.dtbc_r, ref.port.dtbc_r, rtol=1e-12)
