@@ -33,12 +33,14 @@ whole bbox face of a hollow guide with PEC side walls:
    (``post/modal_sparameters.py:118-212``, with ``dtbc_wave_impedance`` and
    ``destagger_theta`` of ``ports/_modal/dtbc.py:201-288``).
 
-Scope: the port covers the whole face, the cross-section is hollow with a
-homogeneous filling, the side walls are PEC, and the kept modes are TE.
-A TM mode among the requested lowest cut-offs, a sub-face window, a PMC side
-wall or more than one conductor group on the plane raise
-``NotImplementedError``; those ports come from the reference's own setup
-(``adapter.problem_from_solver``).
+Scope: the port covers the whole face of a hollow guide (one conductor,
+the walls) with a homogeneous filling ``eps_r`` and PEC side walls; where
+the flat PEC mask marks no edge of the plane, the four lateral bbox faces
+are the walls, as in the reference.  The caller states that geometry: this
+module does not classify conductors.  A TM mode among the requested lowest
+cut-offs raises ``NotImplementedError``.  Sub-face windows, PMC side walls,
+multi-conductor (TEM / quasi-TEM) planes and TM channels come from the
+reference's own setup (``adapter.problem_from_solver``).
 """
 
 from __future__ import annotations
@@ -61,7 +63,6 @@ FACE_AXES = {
     "ymin": (1, False, 2, 0), "ymax": (1, True, 0, 2),
     "zmin": (2, False, 0, 1), "zmax": (2, True, 1, 0),
 }
-_AXIS_FACES = (("xmin", "xmax"), ("ymin", "ymax"), ("zmin", "zmax"))
 
 # gates of the reference operator (operator.py:212-229, factory.py:1022)
 PAIR_SPREAD_TOL = 1e-8
@@ -689,3 +690,58 @@ def power_wave_maps(ch: ChannelInfo, freqs, dt: float) -> np.ndarray:
         ep, em = np.exp(theta), np.exp(-theta)
         den = ep + em
         return np.stack([ep / sZ / den, sZ / den, em / sZ / den, -sZ / den])
+
+
+SLAB_DEPTH = 4
+
+
+def _remap(idx, n_sub, n_full, na, offset, shape_of):
+    """Flat indices of a sub-grid (``offset`` cells along axis ``na``) in the
+    full grid's layout."""
+    off_s, _ = _offsets(n_sub, shape_of)
+    off_f, _ = _offsets(n_full, shape_of)
+    idx = np.asarray(idx, np.int64)
+    out = np.empty_like(idx)
+    for c in range(3):
+        size = int(np.prod(shape_of(n_sub, c)))
+        m = (idx >= off_s[c]) & (idx < off_s[c] + size)
+        if not m.any():
+            continue
+        ijk = list(np.unravel_index(idx[m] - off_s[c], shape_of(n_sub, c)))
+        ijk[na] = ijk[na] + offset
+        out[m] = _flat(shape_of(n_full, c), off_f[c], ijk)
+    return out
+
+
+def build_waveguide_port_on_slab(x, y, z, masses, face: str, n_modes: int, dt: float, f_calc: float,
+                                 eps_r: float = 1.0, eigensolve=None, depth: int = SLAB_DEPTH) -> WaveguidePort:
+    """:func:`build_waveguide_port` from the ``depth`` cells next to ``face``
+    only: ``masses(xs, ys, zs)`` returns ``(m_eps, m_mu, pec_e)`` of any
+    grid, and is called on the slab's sub-grid, so a large problem's mass
+    matrices need not exist on the host.  The port reads the first three
+    slabs behind the plane; with ``depth >= 4`` the sub-grid's own end
+    (where its dual widths differ from the full grid's) lies beyond them,
+    and the port equals the one built on the full grid with its indices
+    moved to the full layout."""
+    if depth < 4:
+        raise ValueError("the slab needs at least 4 cells")
+    nodes = [np.asarray(a, float) for a in (x, y, z)]
+    n_full = tuple(a.size - 1 for a in nodes)
+    na, is_max = FACE_AXES[face][:2]
+    if n_full[na] <= depth:
+        sub, offset = nodes, 0
+    else:
+        offset = n_full[na] - depth if is_max else 0
+        sub = list(nodes)
+        sub[na] = nodes[na][offset:offset + depth + 1]
+    me, mm, pec = masses(*sub)
+    w = build_waveguide_port(*sub, me, mm, pec, face, n_modes, dt, f_calc, eps_r, eigensolve)
+    if sub is nodes:
+        return w
+    n_sub = tuple(a.size - 1 for a in sub)
+    p = w.port
+    p.port_e_idx = _remap(p.port_e_idx, n_sub, n_full, na, offset, _e_shape)
+    p.int_e_idx = _remap(p.int_e_idx, n_sub, n_full, na, offset, _e_shape)
+    p.port_h_idx = _remap(p.port_h_idx, n_sub, n_full, na, offset, _h_shape)
+    w.plane = plane_edges(*nodes, face)
+    return w

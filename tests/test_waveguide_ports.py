@@ -152,3 +152,32 @@ def test_x_and_y_faces_mirror_the_z_faces():
             assert abs(got.channels[q].omega_c / ref.channels[q].omega_c - 1.0) < 1e-12
         assert np.allclose(got.port.record_scale, ref.port.record_scale, rtol=1e-10)
         assert np.allclose(got.port.dtbc_r, ref.port.dtbc_r, rtol=1e-12)
+
+
+def test_a_port_built_from_its_slab_equals_the_full_build():
+    """The ridge fixture's ports from the four cells next to each face (the
+    masses of the sub-grid only) equal the ports built on the whole grid,
+    bit for bit, with their indices in the full layout."""
+    from magnelio_b200 import host
+    from magnelio_b200.workloads import _pec_edges_in_box
+
+    d = dict(np.load(__import__("conftest").GOLDEN / "ridge_ports.npz"))
+    x, y, z, me, mm, pec, dt = _inputs(d, "ridge_ports")
+
+    def masses(xs, ys, zs):
+        n = (xs.size - 1, ys.size - 1, zs.size - 1)
+        m_e = host.build_M_eps(xs, ys, zs, np.array([1.0]), np.zeros(n, np.int32))
+        pe = np.zeros(m_e.size, bool)
+        for f in ("xmin", "xmax", "ymin", "ymax"):
+            pe[_pec_face_flat_indices(*n, f)] = True
+        pe[_pec_edges_in_box(xs, ys, zs, (x[5], y[5], zs[0]), (x[9], y[-1], zs[-1]))] = True
+        return m_e, host.build_M_mu(xs, ys, zs), pe
+
+    m_e, m_m, pe = masses(x, y, z)
+    assert np.array_equal(pe, pec) and np.array_equal(m_e, me)
+    for face in ("zmin", "zmax"):
+        full = wp.build_waveguide_port(x, y, z, m_e, m_m, pe, face, 3, dt, F_CALC, eigensolve=dense_port_modes)
+        slab = wp.build_waveguide_port_on_slab(x, y, z, masses, face, 3, dt, F_CALC, eigensolve=dense_port_modes)
+        for k in PORT_KEYS:
+            assert np.array_equal(getattr(full.port, k), getattr(slab.port, k)), (face, k)
+        assert all(np.array_equal(a, b) for a, b in zip(full.port.complement, slab.port.complement))
