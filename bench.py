@@ -282,6 +282,8 @@ def main(argv=None) -> int:
     ap.add_argument("--serving", action="store_true",
                     help="serve the S-parameter request stream (batched and one excitation at a time) instead")
     ap.add_argument("--serving-requests", type=int, default=256)
+    ap.add_argument("--serving-ports", choices=("modal", "lumped"), default="modal",
+                    help="waveguide ports with 1-3 modes on both ends (the configuration), or lumped ports only")
     ap.add_argument("--serving-stencil", default=None, metavar="BATCHED[,PLAIN]",
                     help="stencil forms of the served handles, KIND:VARIANT or 'default' each (batched, then "
                          "one-excitation handles; the loop's own choice when absent)")
@@ -334,7 +336,8 @@ def run_serving(args, world, rank, local):
     sc = args.serving_scale
     cells = (max(8**3, int(32**3 * sc)), max(8**3, int(192**3 * sc)))
     steps = (max(100, int(6000 * sc)), max(100, int(12000 * sc)))
-    reqs = serving.request_stream(args.serving_requests, seed=2027 + rank, mean_gap=0.020, cells=cells, steps=steps)
+    reqs = serving.request_stream(args.serving_requests, seed=2027 + rank, mean_gap=0.020, cells=cells, steps=steps,
+                                  port_kind=args.serving_ports)
     stencil = serving.serving_stencil
     if args.serving_stencil:
         forms = [None if f in ("default", "") else (f.split(":")[0], int(f.split(":")[1]))
@@ -357,7 +360,10 @@ def run_serving(args, world, rank, local):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded waveguide-section request stream)",
             "config": {"workload": "serving_stream", "requests": len(reqs), "arrivals": "Poisson, mean gap 20 ms",
-                       "cells": list(cells), "steps": list(steps), "ports": "2-4 lumped, 50 ohm",
+                       "cells": list(cells), "steps": list(steps),
+                       "ports": ("2-4: waveguide ports on both ends with 1-3 TE modes each (modes solved and DTBC "
+                                 "tables built on the device per request), the rest 50 ohm lumped"
+                                 if args.serving_ports == "modal" else "2-4 lumped, 50 ohm"),
                        "s_matrix": "device post-step (fitb_s_params)",
                        "max_slots": 8, "slice_steps": 512,
                        "stencil": {"batched": str(stencil(2) or "engine default (batched two-pass)"),

@@ -266,6 +266,13 @@ class FitProblem:
     batch: int = 1
     e0: list = field(default_factory=list)  # per field set initial e (or empty)
     h0: list = field(default_factory=list)
+    # a served request's driven channels in engine order, for the S-parameter
+    # post-step: ("modal", waveguide_ports.ChannelInfo) or ("lumped", Z0);
+    # not part of the stored arrays
+    channels: list = field(default_factory=list)
+    # a served request's S-parameter band [Hz]; its top is the ports'
+    # mode-calculation frequency
+    f_band: tuple | None = None
 
     # ---- engine ---------------------------------------------------------
     def put_coefficients(self, eng) -> None:
@@ -358,10 +365,19 @@ class FitProblem:
 
     def materialize(self) -> "FitProblem":
         """The coefficient arrays on the host (for the CPU oracle), when the
-        problem carries only its materials."""
+        problem carries only its materials, and the host DTBC kernel tables
+        of modal ports whose tables the device builds."""
         if self.alpha_E is None and self.materials is not None:
             (self.alpha_E, self.beta_E, self.alpha_H, self.beta_H, self.M_eps,
              self.M_mu) = self.materials.host_arrays(self.dx, self.dy, self.dz, self.dt)
+        from magnelio_b200 import host
+
+        for mp in self.modal:
+            if mp.dtbc_device_steps > 0:
+                for m in range(mp.n_modes):
+                    if mp.is_dtbc[m] and m not in mp.dtbc_kernels:
+                        mp.dtbc_kernels[m] = host.dtbc_tables(mp.dtbc_r[m], mp.dtbc_q[m], mp.dtbc_n_kernel_init,
+                                                              mp.dtbc_device_steps)
         return self
 
     # ---- npz round trip ---------------------------------------------------

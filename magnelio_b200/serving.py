@@ -1,7 +1,8 @@
 """Continuous-batching serving loop for S-parameter solves on one GPU.
 
-A request is one mesh with its ports; every port excitation of the request
-is one field set of a single engine handle, so the excitations of one mesh
+A request is one mesh with its ports; every driven channel of the request
+(a mode of a waveguide port, or a lumped port) is one field set of a single
+engine handle, so the excitations of one mesh
 advance together in every launch and read the coefficients once per cell
 (the batch dimension).  The loop:
 
@@ -15,8 +16,9 @@ advance together in every launch and read the coefficients once per cell
   handle gets its next slice as soon as its last one has finished (polled,
   non-blocking), and new arrivals are admitted whenever a slice ends
   (requests join and leave the running set continuously);
-* on completion reads back the port voltages and currents, forms the
-  S-matrix on the host and releases the device memory.
+* on completion forms the S-matrix (on the device by default, from the
+  recorded port voltages and currents and each channel's power-wave map)
+  and releases the device memory.
 
 Latency is measured from a request's arrival to its S-matrix; throughput is
 solves per second of wall time.  ``plain=True`` serves the same stream one
@@ -26,6 +28,8 @@ single-excitation form the batched loop is compared with.
 
 from __future__ import annotations
 
+import copy
+import dataclasses
 import time
 from collections import deque
 from dataclasses import dataclass, field
@@ -38,10 +42,13 @@ class Request:
     rid: int
     arrival: float              # seconds after the stream starts
     build: object               # callable(batch: int | None) -> FitProblem
-    n_ports: int
+    n_ports: int                # driven channels (set from the built problem)
     steps: int
     freqs: np.ndarray
     z0: float = 50.0
+    # the built problem of a request served one excitation at a time,
+    # shared by its single-excitation handles
+    cache: dict = field(default_factory=dict, repr=False)
 
 
 @dataclass
@@ -106,8 +113,12 @@ def estimate_footprint(nx, ny, nz, batch, steps, n_channels, cpml_layers=(), pre
 
 def _footprint_of(prob, steps, precision, fused=False):
     layers = [("xyz".index(f.face[0]), len(f.b)) for f in prob.cpml]
-    nch = len(prob.lumped) + sum(m.n_modes for m in prob.modal)
-    return estimate_footprint(prob.nx, prob.ny, prob.nz, prob.batch, steps, nch, layers, precision, fused=fused)
+    n_modal = sum(m.n_modes for m in prob.modal)
+    nch = len(prob.lumped) + n_modal
+    fp = estimate_footprint(prob.nx, prob.ny, prob.nz, prob.batch, steps, nch, layers, precision, fused=fused)
+    # DTBC histories (scattered and incident) and the kernel tables
+    cap = max(int(steps), 1024)
+    return fp + n_modal * (2 * prob.batch * cap + 4 * cap) * 8
 
 
 def serving_stencil(batch: int):
@@ -180,6 +191,10 @@ class ServingLoop:
             now = self.clock() - t0
             while pending and len(active) < slots and pending[0][0].arrival <= now:
                 req, port, prob = pending[0]
+                if port is not None and port >= req.n_ports:
+                    pending.popleft()             # the request kept fewer channels
+                    req.cache.clear()
+                    continue
                 if prob is None:
                     prob = pending[0][2] = self._problem(req, port)
                 form = self.stencil(prob.batch) if self.stencil is not None else None
@@ -187,6 +202,8 @@ class ServingLoop:
                 if active and used + fp > self.hbm_budget:
                     break                         # wait for memory (arrival order kept)
                 pending.popleft()
+                if port is not None and port == req.n_ports - 1:
+                    req.cache.clear()
                 eng = self.engine_factory(prob, self.precision, self.device)
                 self._configure(eng, form)
                 self._storage(eng, self.coef)
@@ -234,7 +251,7 @@ class ServingLoop:
                 on_device = not self.records and hasattr(eng, "s_parameters")
                 if on_device:
                     VI = None
-                    cols = self._device_columns(eng, req, a["port"])
+                    cols = self._device_columns(eng, req, a["port"], a["prob"])
                 else:
                     VI = [eng.read_vi(b) for b in range(nset)]
                 dev_bytes = eng.device_bytes
@@ -320,53 +337,106 @@ class ServingLoop:
 
     @staticmethod
     def _problem(req, port):
-        prob = req.build(None)
-        if port is not None:
-            # the single-excitation form: field set 0 drives `port`
+        """The request's problem; for the single-excitation form the copy
+        whose one field set drives channel ``port`` (built once per
+        request)."""
+        if port is None:
+            prob = req.build(None)
+        else:
+            proto = req.cache.get("problem")
+            if proto is None:
+                proto = req.cache["problem"] = req.build(None)
+            prob = copy.copy(proto)
             prob.batch = 1
-            for lp in prob.lumped:
-                lp.v_src = [lp.v_src[port]]
-            prob.e0 = prob.e0[:1]
-            prob.h0 = prob.h0[:1]
+            prob.lumped = [dataclasses.replace(lp, v_src=[lp.v_src[port]]) for lp in proto.lumped]
+            prob.modal = [dataclasses.replace(mp, excitation=[mp.excitation[port]] if mp.excitation else [])
+                          for mp in proto.modal]
+            prob.e0 = proto.e0[:1]
+            prob.h0 = proto.h0[:1]
+        if prob.channels:
+            req.n_ports = len(prob.channels)
+        if prob.f_band is not None:
+            req.freqs = np.linspace(prob.f_band[0], prob.f_band[1], len(req.freqs))
         return prob
 
     @staticmethod
-    def _device_columns(eng, req, port):
+    def channel_maps(req, prob, n_channels):
+        """Power-wave maps ``(n_channels, 4, F)`` and the co-temporal flags of
+        a request's channels: a modal channel's from its port
+        (``waveguide_ports.power_wave_maps``: discrete impedance and half-cell
+        de-stagger, I shifted by the Yee half step), a lumped port's
+        ``a = (V + Z0 I) / (2 sqrt Z0)``, ``b = (V - Z0 I) / (2 sqrt Z0)``
+        with I taken with V."""
+        from magnelio_b200 import waveguide_ports as wp
+
+        F = len(req.freqs)
+        maps = np.zeros((n_channels, 4, F), complex)
+        icot = np.ones(n_channels, np.int32)
+        chans = prob.channels or [("lumped", req.z0)] * n_channels
+        for c in range(n_channels):
+            kind, info = chans[c] if c < len(chans) else ("lumped", req.z0)
+            if kind == "modal":
+                maps[c] = wp.power_wave_maps(info, req.freqs, prob.dt)
+                icot[c] = 0
+            else:
+                rz = np.sqrt(info)
+                maps[c, 0], maps[c, 1] = 1.0 / (2 * rz), info / (2 * rz)
+                maps[c, 2], maps[c, 3] = 1.0 / (2 * rz), -info / (2 * rz)
+        return maps, icot
+
+    @classmethod
+    def _device_columns(cls, eng, req, port, prob):
         """S-matrix columns of a finished handle from the device post-step:
-        {driven port: S[:, :, port]}.  Lumped-port power waves
-        a = (V + Z0 I) / (2 sqrt Z0), b = (V - Z0 I) / (2 sqrt Z0) (the maps
-        of :func:`magnelio_b200.workloads.s_matrix`; its time origin and dt
-        factor are common to a and b and cancel in b / a), I taken with V."""
-        P, F = req.n_ports, len(req.freqs)
-        nch = eng.n_channels
-        rz = np.sqrt(req.z0)
-        maps = np.zeros((nch, 4, F), complex)
-        maps[:, 0], maps[:, 1] = 1.0 / (2 * rz), req.z0 / (2 * rz)
-        maps[:, 2], maps[:, 3] = 1.0 / (2 * rz), -req.z0 / (2 * rz)
+        {driven channel: S[:, :, channel]}, with each channel's power-wave
+        map (:meth:`channel_maps`; for lumped ports the time origin and dt
+        factor of :func:`magnelio_b200.workloads.s_matrix` are common to a
+        and b and cancel in b / a)."""
+        P = req.n_ports
+        maps, icot = cls.channel_maps(req, prob, eng.n_channels)
         driven = list(range(P)) if port is None else [port]
-        S = eng.s_parameters(req.freqs, maps, np.ones(nch, np.int32), driven, a_threshold=0.0)
+        S = eng.s_parameters(req.freqs, maps, icot, driven, a_threshold=0.0)
         return {p: S[:, :P, b] for b, p in enumerate(driven)}
 
     def _result(self, req, V, I, a, fin, dev_bytes):
         from magnelio_b200.workloads import s_matrix
 
-        dt = a["prob"].dt
-        S = s_matrix(V, I, dt, req.freqs, req.z0, req.n_ports)
+        prob = a["prob"]
+        dt = prob.dt
+        if prob.channels:
+            from magnelio_b200 import sparams
+
+            maps, icot = self.channel_maps(req, prob, V.shape[2])
+            S = sparams.s_matrix(list(V), list(I), dt, req.freqs, list(maps), [bool(c) for c in icot],
+                                 list(range(req.n_ports)), a_threshold=0.0)
+        else:
+            S = s_matrix(V, I, dt, req.freqs, req.z0, req.n_ports)
         return Result(rid=req.rid, S=S, V=V, I=I, arrival=req.arrival, admitted=a["admitted"], finished=fin,
                       footprint=a["fp"], device_bytes=dev_bytes)
 
 
 def request_stream(n: int, seed: int = 7, mean_gap: float = 0.020, cells=(32**3, 192**3), steps=(6000, 12000),
-                   ports=(2, 4), n_freq: int = 101, device_setup: bool = True):
+                   ports=(2, 4), n_freq: int = 101, device_setup: bool = True, port_kind: str = "modal",
+                   modes=(1, 3), eigensolve=None, device_tables: bool = True):
     """The serving workload: ``n`` requests with Poisson arrivals (mean gap
     ``mean_gap`` s), each a rectangular or single-ridge waveguide section
     with dimensions ``U[0.7, 1.3]`` x (22.86, 10.16, 40) mm, 0-4 dielectric
     inserts (``eps_r ~ U[2, 10]``), a log-uniform cell count in ``cells``,
-    ``ports`` lumped ports and a step count in ``steps``.  With
-    ``device_setup`` (the default) a request's material matrices and
+    a port count in ``ports`` and a step count in ``steps``.
+
+    ``port_kind="modal"`` (the default): the two end faces are waveguide
+    ports with a mode count in ``modes`` each (TE modes below the empty
+    guide's TM11 cut-off; ports built by
+    :func:`magnelio_b200.workloads.waveguide_section_modal`, mode solve and
+    DTBC tables on the GPU unless ``eigensolve`` / ``device_tables`` say
+    otherwise), the ports beyond two are lumped; the S-matrix band is the
+    built problem's ``f_band`` (every kept mode propagates over it; the
+    request holds an estimate from the empty guide's cut-offs until then).  ``port_kind="lumped"``: every port is a
+    50 Ohm lumped port, CPML terminates both ends, band 7-13 GHz.
+
+    With ``device_setup`` (the default) a request's material matrices and
     coefficients are built on the device when its handle is created: the
     host prepares the grid and the cell materials only."""
-    from magnelio_b200.workloads import waveguide_section
+    from magnelio_b200.workloads import te_cutoffs, te_mode_count, waveguide_section, waveguide_section_modal
 
     rng = np.random.default_rng(seed)
     t = 0.0
@@ -380,12 +450,26 @@ def request_stream(n: int, seed: int = 7, mean_gap: float = 0.020, cells=(32**3,
         ins = int(rng.integers(0, 5))
         ridged = bool(rng.integers(0, 2))
         sub = int(rng.integers(0, 2**31 - 1))
+        if port_kind == "lumped":
+            def build(batch, dims=dims, c=c, P=P, st=st, ins=ins, ridged=ridged, sub=sub):
+                return waveguide_section(np.random.default_rng(sub), a=dims[0], b=dims[1], length=dims[2], cells=c,
+                                         n_inserts=ins, ridged=ridged, n_ports=P, steps=st, batch=batch,
+                                         device_setup=device_setup)
 
-        def build(batch, dims=dims, c=c, P=P, st=st, ins=ins, ridged=ridged, sub=sub):
-            return waveguide_section(np.random.default_rng(sub), a=dims[0], b=dims[1], length=dims[2], cells=c,
-                                     n_inserts=ins, ridged=ridged, n_ports=P, steps=st, batch=batch,
-                                     device_setup=device_setup)
+            out.append(Request(rid=rid, arrival=t, build=build, n_ports=P, steps=st,
+                               freqs=np.linspace(7.0e9, 13.0e9, n_freq)))
+            continue
+        nm = [te_mode_count(dims[0], dims[1], int(rng.integers(modes[0], modes[1] + 1))) for _ in range(2)]
+        fc = te_cutoffs(dims[0], dims[1], max(nm))[0]
+        f_hi = max(13.0e9, 1.25 * float(fc[-1]))
+        f_lo = max(7.0e9, 1.05 * float(fc[-1]))
 
-        out.append(Request(rid=rid, arrival=t, build=build, n_ports=P, steps=st,
-                           freqs=np.linspace(7.0e9, 13.0e9, n_freq)))
+        def build(batch, dims=dims, c=c, P=P, st=st, ins=ins, ridged=ridged, sub=sub, nm=tuple(nm)):
+            return waveguide_section_modal(np.random.default_rng(sub), a=dims[0], b=dims[1], length=dims[2],
+                                           cells=c, n_inserts=ins, ridged=ridged, n_modes=nm, n_lumped=P - 2,
+                                           steps=st, batch=batch, device_setup=device_setup,
+                                           eigensolve=eigensolve, device_tables=device_tables)
+
+        out.append(Request(rid=rid, arrival=t, build=build, n_ports=sum(nm) + P - 2, steps=st,
+                           freqs=np.linspace(f_lo, f_hi, n_freq)))
     return out

@@ -222,6 +222,157 @@ def waveguide_section(rng, *, a: float = 22.86e-3, b: float = 10.16e-3, length: 
     return prob
 
 
+def te_cutoffs(a: float, b: float, count: int) -> tuple[np.ndarray, float]:
+    """The ``count`` lowest continuum TE cut-offs [Hz] of an empty ``a x b``
+    rectangular guide and its lowest TM cut-off (TM11)."""
+    fc = sorted(0.5 * host.C0 * math.hypot(m / a, n / b) for m in range(8) for n in range(8) if m + n > 0)
+    return np.array(fc[:count]), 0.5 * host.C0 * math.hypot(1.0 / a, 1.0 / b)
+
+
+def te_mode_count(a: float, b: float, wanted: int) -> int:
+    """At most ``wanted`` modes, all below 0.97 of the TM11 cut-off of the
+    empty rectangle (a port keeps TE channels only)."""
+    fc, f_tm = te_cutoffs(a, b, wanted)
+    return max(1, int(np.sum(fc < 0.97 * f_tm)))
+
+
+def waveguide_section_modal(rng, *, a: float = 22.86e-3, b: float = 10.16e-3, length: float = 40e-3,
+                            cells: int = 48**3, n_inserts: int = 2, ridged: bool = False, n_modes=(1, 1),
+                            n_lumped: int = 0, steps: int = 6000, f_min: float = 7.0e9, z0: float = 50.0,
+                            batch: int | None = None, device_setup: bool = True, eigensolve=None,
+                            device_tables: bool = True) -> FitProblem:
+    """One S-parameter request of the serving workload with waveguide ports:
+    an ``a x b x length`` rectangular (or single-ridge) guide on a uniform
+    grid of about ``cells`` cells, PEC side walls, ``n_inserts`` dielectric
+    blocks (``eps_r ~ U[2, 10]``) kept four cells clear of both ends, modal
+    ports on ``zmin`` and ``zmax`` with ``n_modes`` TE modes each (a port
+    whose requested modes would include a TM mode keeps fewer), and
+    ``n_lumped`` y-directed 50 Ohm lumped ports inside the guide.
+
+    The ports are built by :mod:`magnelio_b200.waveguide_ports` from the four
+    cells next to each face, the mode solve on the GPU (``eigensolve``
+    replaces it), the DTBC kernel tables on the GPU (``device_tables``;
+    else on the host).  ``f_max`` is 1.25 times the highest continuum cut-off
+    of the kept modes of the empty rectangle, at least 13 GHz; it is the
+    mode-calculation frequency.  Channels are the ports' modes in port order
+    and then the lumped ports; field set ``c`` drives channel ``c`` with the
+    analysis's pulse for it (``waveguide_ports.excitation_waveform``; the
+    lumped ports a modulated Gaussian over ``[f_min, f_max]``).  The
+    problem's ``channels`` carry what the S-parameter post-step needs and
+    ``f_band`` the band where every kept mode propagates:
+    ``[max(f_min, 1.05 f_c), f_max]`` with ``f_c`` the highest cut-off.  A
+    ridge can lift a higher mode's cut-off above the empty guide's; then
+    ``f_max`` becomes 1.25 times that cut-off and the ports are rebuilt."""
+    from magnelio_b200 import waveguide_ports as wp
+    from magnelio_b200.adapter import _pec_face_flat_indices
+
+    h = (a * b * length / cells) ** (1.0 / 3.0)
+    nx, ny = (max(8, int(round(v / h))) for v in (a, b))
+    nz = max(16, int(round(length / h)))
+    x, y, z = (np.linspace(0.0, v, n + 1) for v, n in ((a, nx), (b, ny), (length, nz)))
+    dz = length / nz
+    bricks, eps_r = [], []
+    for _ in range(n_inserts):
+        size = rng.uniform(0.15, 0.45, 3) * np.array([a, b, length])
+        size[2] = min(size[2], length - 10 * dz)
+        lo = rng.uniform(0.0, 1.0, 3) * (np.array([a, b, length]) - size)
+        lo[2] = 5 * dz + rng.uniform(0.0, 1.0) * (length - 10 * dz - size[2])
+        bricks.append((lo, lo + size))
+        eps_r.append(float(rng.uniform(2.0, 10.0)))
+    ridge = None
+    if ridged:
+        w, d = rng.uniform(0.2, 0.4) * a, rng.uniform(0.2, 0.4) * b
+        ridge = (0.5 * (a - w), b - d, 0.5 * (a + w), b)
+    eps_table = np.concatenate([[1.0], eps_r])
+    mat_id = host.assign_bricks(x, y, z, bricks) if bricks else np.zeros((nx, ny, nz), np.int32)
+    dt = host.courant_dt(x, y, z, "normal")
+
+    def pec_of(xs, ys, zs):
+        n = (xs.size - 1, ys.size - 1, zs.size - 1)
+        idx = [_pec_face_flat_indices(*n, f) for f in ("xmin", "xmax", "ymin", "ymax")]
+        if ridge is not None:
+            idx.append(_pec_edges_in_box(xs, ys, zs, (ridge[0], ridge[1], zs[0]), (ridge[2], ridge[3], zs[-1])))
+        return np.concatenate(idx)
+
+    def masses(xs, ys, zs):
+        m_id = host.assign_bricks(xs, ys, zs, bricks) if bricks else np.zeros(
+            (xs.size - 1, ys.size - 1, zs.size - 1), np.int32)
+        m_e = host.build_M_eps(xs, ys, zs, eps_table, m_id)
+        pe = np.zeros(m_e.size, bool)
+        pe[pec_of(xs, ys, zs)] = True
+        return m_e, host.build_M_mu(xs, ys, zs), pe
+
+    want = [int(m) for m in n_modes]
+    f_max = max(13.0e9, 1.25 * float(te_cutoffs(a, b, max(want))[0][-1]))
+
+    def build_ports(f_calc):
+        out = []
+        for face, m in zip(("zmin", "zmax"), want):
+            while True:
+                try:
+                    out.append(wp.build_waveguide_port_on_slab(x, y, z, masses, face, m, dt, f_calc,
+                                                               eigensolve=eigensolve))
+                    break
+                except NotImplementedError:
+                    if m == 1:
+                        raise
+                    m -= 1
+        return out
+
+    ports = build_ports(f_max)
+    # a ridge can raise a higher mode's cut-off above the empty guide's:
+    # keep f_max at least 1.2 times the highest kept cut-off
+    f_top = max(ch.omega_c for w in ports for ch in w.channels) / (2.0 * math.pi)
+    if 1.2 * f_top > f_max:
+        f_max = 1.25 * f_top
+        ports = build_ports(f_max)
+    n_ch = sum(w.port.n_modes for w in ports) + n_lumped
+    B = batch if batch is not None else n_ch
+    B = next(v for v in (1, 2, 4, 8, 16, B) if v >= B)
+    materials = MaterialSetup(mat_id=mat_id, eps_r=eps_table, pec_idx=pec_of(x, y, z))
+    if device_setup:
+        prob = FitProblem(nx=nx, ny=ny, nz=nz, dt=dt, dx=np.diff(x), dy=np.diff(y), dz=np.diff(z),
+                          alpha_E=None, beta_E=None, alpha_H=None, beta_H=None, materials=materials, batch=B)
+    else:
+        aE, bE, aH, bH, M_eps, M_mu = materials.host_arrays(np.diff(x), np.diff(y), np.diff(z), dt)
+        prob = FitProblem(nx=nx, ny=ny, nz=nz, dt=dt, dx=np.diff(x), dy=np.diff(y), dz=np.diff(z),
+                          alpha_E=aE, beta_E=bE, alpha_H=aH, beta_H=bH, M_eps=M_eps, M_mu=M_mu, batch=B)
+    c = 0
+    for w in ports:
+        mp = w.port
+        mp.excitation = [None] * B
+        for m in range(mp.n_modes):
+            wave = wp.excitation_waveform(w.channels[m].omega_c, f_max)
+            mp.excitation[c] = (m, wp.excitation_samples(w, m, wave, dt, steps))
+            prob.channels.append(("modal", w.channels[m]))
+            c += 1
+        if device_tables:
+            mp.dtbc_device_steps = steps
+        else:
+            mp.dtbc_kernels = {m: host.dtbc_tables(mp.dtbc_r[m], mp.dtbc_q[m], mp.dtbc_n_kernel_init, steps)
+                               for m in range(mp.n_modes) if mp.is_dtbc[m]}
+        prob.modal.append(mp)
+    t = np.arange(steps + 1) * dt
+    drive = 2.0 * math.sqrt(z0) * host.modulated_gaussian(t + dt, f_max, f_min)
+    n_ex = nx * (ny + 1) * (nz + 1)
+    k_lo, k_hi = 6, nz - 7
+    for p in range(n_lumped):
+        k = int(round(k_lo + (k_hi - k_lo) * ((p + 1) / (n_lumped + 1))))
+        i = int(np.clip(nx // 2 + rng.integers(-nx // 6, nx // 6 + 1), 1, nx - 1))
+        j = max(1, ny // 4)
+        flat = n_ex + (i * ny + j) * (nz + 1) + k  # Ey (nx+1, ny, nz+1)
+        v = [drive if q == c else np.zeros_like(drive) for q in range(B)]
+        m_eps = host.m_eps_edges(x, y, z, eps_table, mat_id, [flat])[0]
+        prob.lumped.append(LumpedPort(flat_idx=np.array([flat], np.int64), signs=np.ones(1),
+                                      betas=np.array([dt / m_eps]), R=z0, record_scale=1.0, v_src=v))
+        prob.channels.append(("lumped", z0))
+        c += 1
+    prob.e0 = [None] * B
+    prob.h0 = [None] * B
+    prob.f_band = (max(f_min, 1.05 * f_top), f_max)
+    return prob
+
+
 def s_matrix(V, I, dt: float, freqs, z0: float = 50.0, n_ports: int | None = None) -> np.ndarray:
     """S-parameters of lumped ports from per-excitation port voltages and
     currents: ``V[b]``, ``I[b]`` of shape (steps, ports) for excitation b

@@ -1,5 +1,7 @@
 """Serving loop on the device: each result is the same alone and in the
-mix, and the batched form reproduces the single-excitation form."""
+mix, the batched form reproduces the single-excitation form, and a served
+S-matrix (waveguide ports with their modes solved on the device, or lumped
+ports) meets the float64 oracle's."""
 
 from __future__ import annotations
 
@@ -59,7 +61,7 @@ def test_served_s_matrix_meets_the_fp64_oracle():
     from magnelio_b200 import serving, workloads
 
     reqs = serving.request_stream(1, seed=5, mean_gap=0.0, cells=(14**3, 14**3), steps=(900, 900), ports=(2, 2),
-                                  n_freq=9)
+                                  n_freq=9, port_kind="lumped")
     req = reqs[0]
     res = serving.ServingLoop(max_slots=1, slice_steps=300).run([req]).results[0]
     prob = req.build(None).materialize()  # host arrays for the oracle
@@ -90,6 +92,38 @@ def test_device_s_matrix_equals_the_host_assembly_of_the_records(plain):
     for a, b in zip(host.results, dev.results):
         assert a.rid == b.rid and b.V is None and b.S.shape == a.S.shape
         assert float(np.max(np.abs(a.S - b.S) / np.maximum(1.0, np.abs(a.S)))) < 1e-9
+
+
+@pytest.mark.parametrize("records", [True, False])
+def test_served_modal_s_matrix_meets_the_fp64_oracle(records):
+    """A request with two waveguide ports (two TE modes each, ports built
+    here with the modes solved on the device) and one lumped port, served
+    in float32 with the S-matrix from the host records or the device
+    post-step, against the float64 oracle's records through the same
+    power-wave maps: |dS| <= 1e-3 and 0.1 degree."""
+    from oracle.fit_oracle import OracleRun
+    from magnelio_b200 import serving, sparams
+
+    req = serving.request_stream(1, seed=5, mean_gap=0.0, cells=(16**3, 16**3), steps=(900, 900), ports=(3, 3),
+                                 modes=(2, 2), n_freq=9)[0]
+    res = serving.ServingLoop(max_slots=1, slice_steps=300, records=records).run([req]).results[0]
+    prob = req.build(None).materialize()
+    n = req.n_ports
+    assert n == len(prob.channels) and sum(m.n_modes for m in prob.modal) >= 3
+    Vs, Is = [], []
+    for b in range(n):
+        r = OracleRun(prob, b=b).run(req.steps)
+        Vs.append(np.array(r.V))
+        Is.append(np.array(r.I))
+    maps, icot = serving.ServingLoop.channel_maps(req, prob, n)
+    S_ref = sparams.s_matrix(Vs, Is, prob.dt, req.freqs, list(maps), [bool(c) for c in icot], list(range(n)),
+                             a_threshold=0.0)
+    assert res.S.shape == S_ref.shape
+    dS = np.abs(res.S - S_ref)
+    assert float(dS.max()) <= S_TOL, float(dS.max())
+    big = np.abs(S_ref) > 0.05
+    dphi = np.degrees(np.abs(np.angle(res.S[big] / S_ref[big])))
+    assert float(dphi.max()) <= PHASE_TOL, float(dphi.max())
 
 
 def test_device_built_materials_equal_the_host_build():

@@ -11,6 +11,7 @@ import numpy as np
 import pytest
 
 from magnelio_b200 import serving, workloads
+from oracle.fit_oracle import dense_port_modes
 
 
 class Clock:
@@ -52,14 +53,28 @@ class ScriptedEngine:
     def query(self):
         return True  # a step costs virtual time when it is issued
 
+    @property
+    def n_channels(self):
+        return sum(m.n_modes for m in self.p.modal) + len(self.p.lumped)
+
+    def _sources(self, b):
+        """Per channel the source series field set b carries."""
+        out = []
+        for mp in self.p.modal:
+            exc = mp.excitation[b] if b < len(mp.excitation) else None
+            for m in range(mp.n_modes):
+                out.append(exc[1][: self.n] if exc is not None and exc[0] == m else np.zeros(self.n))
+        for lp in self.p.lumped:
+            out.append(lp.v_src[b][: self.n] if len(lp.v_src[b]) else np.zeros(self.n))
+        return out
+
     def read_vi(self, b):
-        P = len(self.p.lumped)
+        P = self.n_channels
         V = np.zeros((self.n, P))
         I = np.zeros((self.n, P))
         rng = np.random.default_rng(self.p.nx * 1000 + self.p.nz)
         coup = rng.uniform(-0.5, 0.5, (P, P)) + np.eye(P)
-        for q, lp in enumerate(self.p.lumped):
-            src = lp.v_src[b][: self.n] if len(lp.v_src[b]) else np.zeros(self.n)
+        for q, src in enumerate(self._sources(b)):
             for j in range(P):
                 V[:, j] += coup[j, q] * src
                 I[:, j] += 0.01 * coup[q, j] * src
@@ -79,9 +94,10 @@ def _loop(clock, **kw):
                                sleep=clock.sleep, **kw)
 
 
-def _stream(n=10, steps=(200, 400)):
+def _stream(n=10, steps=(200, 400), port_kind="lumped"):
+    kw = {} if port_kind == "lumped" else {"eigensolve": dense_port_modes, "device_tables": False}
     return serving.request_stream(n, seed=3, mean_gap=0.002, cells=(12**3, 20**3), steps=steps, ports=(2, 4),
-                                  n_freq=5)
+                                  n_freq=5, port_kind=port_kind, **kw)
 
 
 def test_every_request_completes_with_its_own_s_matrix():
@@ -216,9 +232,9 @@ def test_overlapping_handles_finish_independently_and_arrivals_start_on_time():
                                sleep=clock.sleep, max_slots=4, slice_steps=50, hbm_budget=1 << 40,
                                stencil=None)
     big = serving.request_stream(1, seed=3, mean_gap=1e-6, cells=(20**3, 20**3), steps=(400, 400), ports=(2, 2),
-                                 n_freq=5)[0]
+                                 n_freq=5, port_kind="lumped")[0]
     small = serving.request_stream(1, seed=4, mean_gap=1e-6, cells=(8**3, 8**3), steps=(100, 100), ports=(2, 2),
-                                   n_freq=5)[0]
+                                   n_freq=5, port_kind="lumped")[0]
     small.rid = 1
     small.arrival = 0.5 * (big.steps * 2 * 20**3 * 1e-9) / 8  # during the big request's first slices
     stats = loop.run([big, small])
@@ -239,7 +255,7 @@ def test_a_request_waiting_for_memory_does_not_spin_the_loop():
     into its timeout."""
     clock = Clock()
     reqs = serving.request_stream(3, seed=5, mean_gap=1e-6, cells=(16**3, 16**3), steps=(300, 300), ports=(2, 2),
-                                  n_freq=5)
+                                  n_freq=5, port_kind="lumped")
     one = serving._footprint_of(reqs[0].build(None), 300, "single")
     loop = serving.ServingLoop(engine_factory=lambda p, prec, dev: AsyncEngine(p, clock), clock=clock,
                                sleep=clock.sleep, max_slots=4, slice_steps=50, hbm_budget=int(1.5 * one),
@@ -247,3 +263,43 @@ def test_a_request_waiting_for_memory_does_not_spin_the_loop():
     stats = loop.run(reqs)
     assert stats.n == 3 and stats.peak_bytes <= int(1.5 * one)
     assert stats.mean_active <= 1.0 + 1e-9  # the budget admits one request at a time
+
+
+def test_modal_requests_carry_waveguide_ports_with_one_to_three_modes():
+    """The default stream: both end faces are waveguide ports (1-3 TE modes
+    each), the ports beyond two are lumped; every channel is driven by its
+    own field set and the request's channel count is the problem's."""
+    reqs = _stream(6, port_kind="modal")
+    seen = set()
+    for r in reqs:
+        p = r.build(None)
+        assert len(p.modal) == 2 and len(p.channels) == r.n_ports
+        n_modal = sum(m.n_modes for m in p.modal)
+        assert all(1 <= m.n_modes <= 3 for m in p.modal) and len(p.lumped) == r.n_ports - n_modal
+        seen.update(m.n_modes for m in p.modal)
+        c = 0
+        for mp in p.modal:
+            for m in range(mp.n_modes):
+                assert mp.excitation[c][0] == m and np.max(np.abs(mp.excitation[c][1])) > 0
+                assert all(e is None for q, e in enumerate(mp.excitation) if q != c and q < p.batch
+                           and not (e is not None and e[0] != m))
+                c += 1
+        serving.ServingLoop._problem(r, None)  # the request takes the problem's band
+        assert r.freqs[0] >= 7e9 and r.freqs[-1] == p.f_band[1]
+        for kind, info in p.channels:
+            if kind == "modal":
+                assert info.omega_c / (2 * np.pi) < r.freqs[0]  # every mode propagates over the band
+    assert len(seen) >= 2
+
+
+def test_modal_requests_agree_between_the_batched_and_single_excitation_forms():
+    clock = Clock()
+    reqs = _stream(4, port_kind="modal")
+    batched = _loop(clock, hbm_budget=1 << 40, max_slots=4, slice_steps=50).run(reqs)
+    clock2 = Clock()
+    plain = _loop(clock2, hbm_budget=1 << 40, slice_steps=50).run(_stream(4, port_kind="modal"), plain=True)
+    assert plain.n == batched.n == 4
+    for a, b in zip(batched.results, plain.results):
+        assert a.S.shape == b.S.shape and a.S.shape[1] == a.S.shape[2]
+        np.testing.assert_allclose(a.V, b.V, rtol=0, atol=0)
+        np.testing.assert_allclose(a.S, b.S, rtol=1e-12, atol=0)
