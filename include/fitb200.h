@@ -354,6 +354,24 @@ int fitb_set_band_source(fitb_handle* h, int32_t port, int32_t b, int64_t n_samp
 int fitb_mode_solve(int32_t device, int64_t n, const int64_t* rowptr, const int64_t* col, const double* val,
                     const double* m_diag, int32_t n_modes, double threshold, double* eigvals, double* eigvecs);
 
+/* The lowest eigenpairs of a large sparse symmetric positive semi-definite
+ * matrix L (CSR, n x n, float64), orthogonal to n_null given orthonormal
+ * null vectors (row-major n_null x n): eigenvalues ascending into eigvals,
+ * orthonormal eigenvectors row-major into eigvecs (n_modes x n).
+ * Chebyshev-filtered subspace iteration on the device (degree 100 filters
+ * on [a, b], b the row-sum bound of L, a the block's largest Ritz value;
+ * Gram-Schmidt with reorthogonalisation; Rayleigh-Ritz), converged when
+ * every wanted residual |L x - theta x| is below tol b, or after 20
+ * iterations without halving once below 1e-12 b; at most 400 iterations,
+ * else FITB_ERR_LIMIT.  `residual` (the largest wanted residual over b) and
+ * `iterations` may be null.  The port-mode problems of large port planes:
+ * the TE face form and the TM problem of a hollow guide (the reference
+ * solves them with shift-invert ARPACK, numerical_2d.py:497-544, :585-650).
+ * n <= 2^26, n_modes <= 16, n_null <= 8; needs no handle. */
+int fitb_sparse_eigs(int32_t device, int64_t n, const int64_t* rowptr, const int64_t* col, const double* val,
+                     int32_t n_null, const double* null_vecs, int32_t n_modes, double tol, double* eigvals,
+                     double* eigvecs, double* residual, int32_t* iterations);
+
 /* ---- surface-impedance walls ---------------------------------------- */
 /* One SIBC wall tag (solver/_sibc.py:88-264, hooks at fit_td.py:837-840 and
  * :909-914): n_faces flat indices into the reference H vector with their

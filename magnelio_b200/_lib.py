@@ -170,6 +170,7 @@ SIGNATURES = {
     "fitb_add_band_port": ([vp, C.POINTER(FitbBandDesc), P_i32], C.c_int),
     "fitb_read_vi_async": ([vp, i32, i64, i64, vp, vp, P_i64], C.c_int),
     "fitb_mode_solve": ([i32, i64, P_i64, P_i64, P_f64, P_f64, i32, f64, P_f64, P_f64], C.c_int),
+    "fitb_sparse_eigs": ([i32, i64, P_i64, P_i64, P_f64, i32, P_f64, i32, f64, P_f64, P_f64, P_f64, P_i32], C.c_int),
     "fitb_wait_ticket": ([vp, i64], C.c_int),
     "fitb_set_band_kernel": ([vp, i32, i32, i32, P_f64], C.c_int),
     "fitb_set_band_source": ([vp, i32, i32, i64, P_f64], C.c_int),

@@ -2963,6 +2963,51 @@ int fitb_mode_solve(int32_t device, int64_t n, const int64_t* rowptr, const int6
     FITB_CATCH
 }
 
+int fitb_sparse_eigs(int32_t device, int64_t n, const int64_t* rowptr, const int64_t* col, const double* val,
+                     int32_t n_null, const double* null_vecs, int32_t n_modes, double tol, double* eigvals,
+                     double* eigvecs, double* residual, int32_t* iterations) {
+    FITB_TRY
+    if (n < 2 || n > (int64_t(1) << 26)) fail(FITB_ERR_LIMIT, "eigenproblem of %lld unknowns (2 .. 2^26)", (long long)n);
+    if (n_modes < 1 || n_modes > 16) fail(FITB_ERR_LIMIT, "n_modes %d (1 .. 16)", n_modes);
+    if (n_null < 0 || n_null > 8) fail(FITB_ERR_LIMIT, "n_null %d (0 .. 8)", n_null);
+    if (n_modes + n_null > n) fail(FITB_ERR_ARG, "n_modes + n_null above n");
+    if (!(tol > 0.0)) fail(FITB_ERR_ARG, "tolerance must be positive");
+    if (!rowptr || !col || !val || !eigvals || !eigvecs || (n_null && !null_vecs)) fail(FITB_ERR_ARG, "null argument");
+    const long long nnz = rowptr[n];
+    if (nnz < 0 || nnz > (int64_t(1) << 30) || rowptr[0] != 0) fail(FITB_ERR_ARG, "row pointers");
+    double bound = 0.0;
+    for (long long i = 0; i < n; ++i) {
+        if (rowptr[i + 1] < rowptr[i]) fail(FITB_ERR_ARG, "row pointers not ascending");
+        double r = 0.0;
+        for (long long q = rowptr[i]; q < rowptr[i + 1]; ++q) {
+            if (col[q] < 0 || col[q] >= n) fail(FITB_ERR_ARG, "column index %lld out of range", (long long)col[q]);
+            r += std::fabs(val[q]);
+        }
+        bound = std::max(bound, r);
+    }
+    if (!(bound > 0.0)) fail(FITB_ERR_ARG, "the matrix is zero");
+    ck(cudaSetDevice(device), "set device");
+    fitb::DevBuf drp, dcol, dval, dz;
+    fitb::upload(drp, std::vector<long long>(rowptr, rowptr + n + 1));
+    fitb::upload(dcol, std::vector<long long>(col, col + nnz));
+    fitb::upload(dval, std::vector<double>(val, val + nnz));
+    if (n_null) fitb::upload(dz, std::vector<double>(null_vecs, null_vecs + (size_t)n_null * n));
+    cudaStream_t s;
+    ck(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "stream");
+    double res = 0.0;
+    int its = 0;
+    const int rc = fitb::sparse_lowest_eigs(n, drp.as<long long>(), dcol.as<long long>(), dval.as<double>(), n_null,
+                                            n_null ? dz.as<double>() : nullptr, n_modes, tol, 1.0001 * bound, eigvals,
+                                            eigvecs, &res, &its, s);
+    cudaStreamDestroy(s);
+    if (residual) *residual = res;
+    if (iterations) *iterations = its;
+    if (rc == -4) fail(FITB_ERR_LIMIT, "not converged in %d iterations (residual %.3g of the spectral bound)", its, res);
+    if (rc == -5) fail(FITB_ERR_ARG, "the start block lost its rank (fewer than n_modes + n_null independent vectors?)");
+    if (rc != 0) fail(FITB_ERR_CUDA, "sparse eigensolve failed (%d)", rc);
+    FITB_CATCH
+}
+
 int fitb_read_vi_async(fitb_handle* h, int32_t b, int64_t step0, int64_t n, double* V, double* I, int64_t* ticket) {
     FITB_TRY
     Handle& H = H_of(h);

@@ -517,6 +517,16 @@ void launch_dtbc_kernel(double r, double q, int n, double2* x, double* l, cudaSt
 int mode_eigensolve(long long n, const long long* rp, const long long* col, const double* val, const double* m,
                     int n_modes, double threshold, double* lam_out, double* vec_out, cudaStream_t s);
 
+// Lowest n_modes eigenpairs of the symmetric positive semi-definite CSR
+// matrix L (on the device) orthogonal to the n_null orthonormal vectors Z
+// (device, [n_null][n]), by Chebyshev-filtered subspace iteration in float64
+// (modes_sparse.cu); b bounds the spectrum; converged when every wanted
+// residual is below tol b.  Vectors into vec_out [n_modes][n] (host).
+// 0 on success, -1 arguments, -2 CUDA, -4 not converged, -5 rank loss.
+int sparse_lowest_eigs(long long n, const long long* rp, const long long* col, const double* val, int n_null,
+                       const double* Z, int n_modes, double tol, double b, double* lam_out, double* vec_out,
+                       double* res_out, int* iters_out, cudaStream_t s);
+
 // lambda_max of the live leapfrog update operator D^-1/2 C^T M_mu^-1 C D^-1/2
 // by a float64 Lanczos iteration (spectral.cu); 0 on success.
 template <typename T>

@@ -62,6 +62,32 @@ def port_modes(K, m_diag, n_modes: int, threshold: float, device: int = 0):
     return lam, vec.T.copy()
 
 
+def sparse_eigs(L, n_modes: int, null=None, tol: float = 1e-14, device: int = 0):
+    """The ``n_modes`` lowest eigenpairs of the sparse symmetric positive
+    semi-definite matrix ``L`` orthogonal to the orthonormal rows of ``null``,
+    solved on the GPU in float64 (``fitb_sparse_eigs``: Chebyshev-filtered
+    subspace iteration).  Returns ``(eigvals, eigvecs, info)`` with
+    ``eigvecs`` of shape (n, n_modes), orthonormal, and ``info`` the final
+    residual (relative to the spectral bound) and the iteration count."""
+    import scipy.sparse as sp
+
+    Lc = sp.csr_matrix(L)
+    Lc.sort_indices()
+    n = Lc.shape[0]
+    Z = np.zeros((0, n)) if null is None else np.ascontiguousarray(np.atleast_2d(null), dtype=np.float64)
+    lam = np.zeros(n_modes)
+    vec = np.zeros((n_modes, n))
+    res = np.zeros(1)
+    its = np.zeros(1, np.int32)
+    lib = _lib.load()
+    check(lib.fitb_sparse_eigs(int(device), int(n), i64p(np.ascontiguousarray(Lc.indptr, np.int64)),
+                               i64p(np.ascontiguousarray(Lc.indices, np.int64)),
+                               f64p(np.ascontiguousarray(Lc.data, np.float64)), int(Z.shape[0]),
+                               f64p(Z) if Z.shape[0] else None, int(n_modes), float(tol), f64p(lam), f64p(vec),
+                               f64p(res), i32p(its)))
+    return lam, vec.T.copy(), {"residual": float(res[0]), "iterations": int(its[0])}
+
+
 class FitEngine:
     """Device-resident FIT-TD state on one GPU.
 

@@ -416,7 +416,7 @@ class ServingLoop:
 
 def request_stream(n: int, seed: int = 7, mean_gap: float = 0.020, cells=(32**3, 192**3), steps=(6000, 12000),
                    ports=(2, 4), n_freq: int = 101, device_setup: bool = True, port_kind: str = "modal",
-                   modes=(1, 3), eigensolve=None, device_tables: bool = True):
+                   modes=(1, 3), lowest=None, device_tables: bool = True):
     """The serving workload: ``n`` requests with Poisson arrivals (mean gap
     ``mean_gap`` s), each a rectangular or single-ridge waveguide section
     with dimensions ``U[0.7, 1.3]`` x (22.86, 10.16, 40) mm, 0-4 dielectric
@@ -427,7 +427,7 @@ def request_stream(n: int, seed: int = 7, mean_gap: float = 0.020, cells=(32**3,
     ports with a mode count in ``modes`` each (TE modes below the empty
     guide's TM11 cut-off; ports built by
     :func:`magnelio_b200.workloads.waveguide_section_modal`, mode solve and
-    DTBC tables on the GPU unless ``eigensolve`` / ``device_tables`` say
+    DTBC tables on the GPU unless ``lowest`` / ``device_tables`` say
     otherwise), the ports beyond two are lumped; the S-matrix band is the
     built problem's ``f_band`` (every kept mode propagates over it; the
     request holds an estimate from the empty guide's cut-offs until then).  ``port_kind="lumped"``: every port is a
@@ -468,7 +468,7 @@ def request_stream(n: int, seed: int = 7, mean_gap: float = 0.020, cells=(32**3,
             return waveguide_section_modal(np.random.default_rng(sub), a=dims[0], b=dims[1], length=dims[2],
                                            cells=c, n_inserts=ins, ridged=ridged, n_modes=nm, n_lumped=P - 2,
                                            steps=st, batch=batch, device_setup=device_setup,
-                                           eigensolve=eigensolve, device_tables=device_tables)
+                                           lowest=lowest, device_tables=device_tables)
 
         out.append(Request(rid=rid, arrival=t, build=build, n_ports=sum(nm) + P - 2, steps=st,
                            freqs=np.linspace(f_lo, f_hi, n_freq)))

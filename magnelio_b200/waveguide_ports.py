@@ -17,9 +17,10 @@ whole bbox face of a hollow guide with PEC side walls:
    tangential edges (``curl_curl_2d.py:52-124``) and the TM problem on the
    normal edges (``:127-218``), both assembled here from the grid's
    topology rather than by slicing a 3-D curl matrix;
-5. the TE eigenpairs, solved on the GPU by ``fitb_mode_solve`` (the
-   numerical core of ``Numerical2DModeSolver._solve_te_tm``,
-   ``numerical_2d.py:454-583``), with the reference's sign rule
+5. the TE eigenpairs (``Numerical2DModeSolver._solve_te_tm``,
+   ``numerical_2d.py:454-583``), solved on the GPU in the equivalent face
+   form by ``fitb_sparse_eigs`` (Chebyshev-filtered subspace iteration; the
+   face form has no gradient null space to filter), with the reference's sign rule
    (``_resolve_sign`` :758-802), wave impedance (``_z_real_at`` :828-853),
    travelling-wave H profiles (``tem_laplace.py:102-160``) and the basis
    rotation inside degenerate groups (``factory.py:1247-1316``);
@@ -203,12 +204,11 @@ def _safe_inv(m):
     return np.where(m > 0, 1.0 / np.where(m > 0, m, 1.0), 0.0)
 
 
-def curl_curl_2d(pl: PlaneEdges, m_eps, m_mu):
-    """``K = C2^T diag(1/M_mu) C2`` over the normal-H faces of the port slab
-    and ``diag(M_eps)`` on the plane's ``[e_u | e_v]`` edges
-    (``curl_curl_2d.py:52-124``).  Face ``(a, b)`` (u cell a, v cell b) has
-    the circulation ``E_u(a, b) + E_v(b, a+1) - E_u(a, b+1) - E_v(b, a)``;
-    a face's weight is 0 where its ``M_mu`` is 0."""
+def face_circulation(pl: PlaneEdges, m_mu):
+    """``C`` (normal-H faces of the port slab x the plane's ``[e_u | e_v]``
+    edges) with face ``(a, b)`` (u cell a, v cell b) carrying
+    ``E_u(a, b) + E_v(b, a+1) - E_u(a, b+1) - E_v(b, a)``, and the faces'
+    weights ``1/M_mu`` (0 where ``M_mu`` is 0)."""
     n = pl.n
     na, is_max, ua, va = FACE_AXES[pl.face]
     nu, nv = n[ua], n[va]
@@ -224,6 +224,16 @@ def curl_curl_2d(pl: PlaneEdges, m_eps, m_mu):
     sgn = np.tile([1.0, 1.0, -1.0, -1.0], (a.size, 1))
     n2 = n_u + nv * (nu + 1)
     C = sp.csr_matrix((sgn.ravel(), (np.repeat(np.arange(a.size), 4), cols.ravel())), shape=(a.size, n2))
+    return C, w
+
+
+def curl_curl_2d(pl: PlaneEdges, m_eps, m_mu):
+    """``K = C2^T diag(1/M_mu) C2`` over the normal-H faces of the port slab
+    and ``diag(M_eps)`` on the plane's ``[e_u | e_v]`` edges
+    (``curl_curl_2d.py:52-124``).  Face ``(a, b)`` (u cell a, v cell b) has
+    the circulation ``E_u(a, b) + E_v(b, a+1) - E_u(a, b+1) - E_v(b, a)``;
+    a face's weight is 0 where its ``M_mu`` is 0."""
+    C, w = face_circulation(pl, m_mu)
     K = (C.T @ sp.diags(w) @ C).tocsr()
     return K, np.asarray(m_eps, float)[pl.e_all]
 
@@ -332,28 +342,64 @@ class TeMode:
     eps_r: float = 1.0
 
 
-def _device_eigensolve(K, m, threshold, n_modes):
-    from magnelio_b200.engine import port_modes
+def _device_lowest(L, n_modes, null=None):
+    from magnelio_b200.engine import sparse_eigs
 
-    return port_modes(K, m, n_modes, threshold)
+    lam, vec, _info = sparse_eigs(L, n_modes, null)
+    return lam, vec
 
 
-def te_modes(pl: PlaneEdges, K, m_diag, pec_mask, m_mu, n_modes: int, f_calc: float, eps_r: float = 1.0,
-             eigensolve=None) -> list[TeMode]:
-    """The ``n_modes`` lowest TE modes above the gradient null space
-    (threshold ``1e-3 sigma``) with their travelling-wave H profiles
-    ``h_u = -e_v mu0 dn / (Z M_mu)``, ``h_v = +e_u mu0 dn / (Z M_mu)``
-    (``numerical_2d.py:454-583``, ``tem_laplace.py:102-160``).
-    ``eigensolve(K_free, m_free, threshold, n)`` returns ``(lam, vec)`` with
-    ``vec^T M vec = 1``; by default ``fitb_mode_solve`` on the GPU."""
-    solve = eigensolve or _device_eigensolve
+def te_face_problem(pl: PlaneEdges, m_eps, m_mu, pec_mask):
+    """The TE problem in face form.  With ``B = W^1/2 C_F M_F^-1/2`` (C_F the
+    circulations of the live faces over the free edges, W their 1/M_mu, M_F
+    the free edges' epsilon-masses), the edge problem
+    ``K v = lambda M v`` (``K = C^T W C``) has the nonzero eigenvalues of
+    ``L = B B^T`` on the faces, with ``v = M_F^-1/2 B^T y / sqrt(lambda)`` for
+    a unit eigenvector ``y`` (then ``v^T M v = 1``).  L's null space holds one
+    vector per connected face region, ``W^-1/2`` on its faces; the gradient
+    null space of ``K`` (one dimension per interior node) has no image, so
+    the face problem needs no threshold.  Returns ``(L, B, null, free)``."""
+    C, w = face_circulation(pl, m_mu)
     free = np.nonzero(~np.asarray(pec_mask, bool))[0]
-    Kf = K.tocsr()[free, :][:, free].tocsr()
-    lam, vec = solve(Kf, m_diag[free], 1e-3 * sigma_te(pl, eps_r), n_modes)
+    CF = C[:, free].tocsr()
+    live = np.nonzero((np.asarray(abs(CF).sum(axis=1)).ravel() > 0) & (w > 0))[0]
+    CF = CF[live]
+    mF = np.asarray(m_eps, float)[pl.e_all][free]
+    B = (sp.diags(np.sqrt(w[live])) @ CF @ sp.diags(1.0 / np.sqrt(mF))).tocsr()
+    L = (B @ B.T).tocsr()
+    from scipy.sparse.csgraph import connected_components
+
+    adj = (abs(CF) @ abs(CF).T).tocsr()
+    n_comp, label = connected_components(adj, directed=False)
+    null = np.zeros((n_comp, live.size))
+    for c in range(n_comp):
+        on = label == c
+        null[c, on] = 1.0 / np.sqrt(w[live][on])
+        null[c] /= np.linalg.norm(null[c])
+    return L, B, null, free
+
+
+def te_modes(pl: PlaneEdges, m_eps, m_mu, pec_mask, n_modes: int, f_calc: float, eps_r: float = 1.0,
+             lowest=None) -> list[TeMode]:
+    """The ``n_modes`` lowest TE modes (``numerical_2d.py:454-583``: the
+    lowest eigenvalues of ``K v = lambda M v`` above the gradient null
+    space, ``v^T M v = 1``), solved in the face form (:func:`te_face_problem`)
+    by ``lowest(L, n, null) -> (lam, Y)`` (by default ``fitb_sparse_eigs`` on
+    the GPU), with the reference's sign rule and travelling-wave H profiles
+    ``h_u = -e_v mu0 dn / (Z M_mu)``, ``h_v = +e_u mu0 dn / (Z M_mu)``
+    (``tem_laplace.py:102-160``).  Every kept eigenvalue must lie above the
+    reference's null-space threshold ``1e-3 sigma``."""
+    solve = lowest or _device_lowest
+    L, B, null, free = te_face_problem(pl, m_eps, m_mu, pec_mask)
+    if L.shape[0] - null.shape[0] < n_modes:
+        raise RuntimeError(f"the port plane holds fewer than {n_modes} modes")
+    lam, Y = solve(L, n_modes, null)
     lam = np.asarray(lam, float)
-    if lam.size < n_modes or not np.all(np.isfinite(lam)):
-        raise RuntimeError(f"only {lam.size} port modes above the null space")
-    n2 = m_diag.size
+    thr = 1e-3 * sigma_te(pl, eps_r)
+    if lam.size < n_modes or not np.all(np.isfinite(lam)) or np.any(lam <= thr):
+        raise RuntimeError(f"port modes at or below the null-space threshold: {lam}")
+    mF = np.asarray(m_eps, float)[pl.e_all][free]
+    n2 = pl.e_all.size
     n_u = pl.e_u.size
     omega = 2.0 * math.pi * f_calc
     scale_num = MU0 * pl.normal_dx
@@ -361,7 +407,7 @@ def te_modes(pl: PlaneEdges, K, m_diag, pec_mask, m_mu, n_modes: int, f_calc: fl
     out = []
     for q in range(n_modes):
         v = np.zeros(n2)
-        v[free] = vec[:, q]
+        v[free] = (B.T @ Y[:, q]) / math.sqrt(lam[q]) / np.sqrt(mF)
         v = resolve_sign(pl, v)
         e_u, e_v = v[:n_u].copy(), v[n_u:].copy()
         wc = float(math.sqrt(lam[q]))
@@ -465,14 +511,15 @@ class WaveguidePort:
 
 
 def build_waveguide_port(x, y, z, m_eps, m_mu, pec_e, face: str, n_modes: int, dt: float, f_calc: float,
-                         eps_r: float = 1.0, eigensolve=None) -> WaveguidePort:
+                         eps_r: float = 1.0, lowest=None) -> WaveguidePort:
     """A hollow-guide modal port on the whole ``face`` of the grid ``x, y, z``
     with the ``n_modes`` lowest TE modes, as ``build_modal_port`` builds it
     (``factory.py:1367-1877``): ``m_eps``, ``m_mu`` are the volume's mass
     diagonals, ``pec_e`` the flat E PEC flags, ``dt`` the solver step and
-    ``f_calc`` the mode-calculation frequency.  The port's DTBC kernel
-    tables are left to the device (``dtbc_device_steps``); excitations are
-    attached with :func:`excite`."""
+    ``f_calc`` the mode-calculation frequency; ``lowest`` replaces the
+    device eigensolve (:func:`te_modes`).  The port's DTBC kernel tables
+    are left to the caller (``dtbc_device_steps`` for the device, or host
+    tables); excitations are built with :func:`excitation_samples`."""
     if face not in FACE_AXES:
         raise ValueError(f"unknown face {face!r}")
     x, y, z = (np.asarray(a, float) for a in (x, y, z))
@@ -490,16 +537,17 @@ def build_waveguide_port(x, y, z, m_eps, m_mu, pec_e, face: str, n_modes: int, d
     pl = plane_edges(x, y, z, face)
     me, mm, pec = flatten_port_slab(n, face, m_eps, m_mu, np.asarray(pec_e, bool))
     mask = plane_pec_mask(pl, x, y, z, pec)
-    K, m2 = curl_curl_2d(pl, me, mm)
-    modes = te_modes(pl, K, m2, mask, mm, n_modes, f_calc, eps_r, eigensolve)
+    modes = te_modes(pl, me, mm, mask, n_modes, f_calc, eps_r, lowest)
     # the kept set must hold no TM mode (the reference keeps the n lowest
     # cut-offs of both families)
     plane_has_pec = bool(pec[pl.e_u].any() or pec[pl.e_v].any())
     Kz, mz, dirichlet = tm_curl_curl_2d(pl, me, mm, pec, plane_has_pec)
     free = np.nonzero(~dirichlet)[0]
     if free.size:
-        solve = eigensolve or _device_eigensolve
-        lam_tm, _ = solve(Kz.tocsr()[free, :][:, free].tocsr(), mz[free], 0.0, 1)
+        solve = lowest or _device_lowest
+        sz = 1.0 / np.sqrt(mz[free])
+        Lz = (sp.diags(sz) @ Kz.tocsr()[free, :][:, free] @ sp.diags(sz)).tocsr()
+        lam_tm, _ = solve(Lz, 1, None)
         wc_tm = math.sqrt(float(lam_tm[0]))
         if wc_tm < modes[-1].omega_c * (1.0 + DEGENERATE_RTOL):
             raise NotImplementedError(
@@ -714,7 +762,7 @@ def _remap(idx, n_sub, n_full, na, offset, shape_of):
 
 
 def build_waveguide_port_on_slab(x, y, z, masses, face: str, n_modes: int, dt: float, f_calc: float,
-                                 eps_r: float = 1.0, eigensolve=None, depth: int = SLAB_DEPTH) -> WaveguidePort:
+                                 eps_r: float = 1.0, lowest=None, depth: int = SLAB_DEPTH) -> WaveguidePort:
     """:func:`build_waveguide_port` from the ``depth`` cells next to ``face``
     only: ``masses(xs, ys, zs)`` returns ``(m_eps, m_mu, pec_e)`` of any
     grid, and is called on the slab's sub-grid, so a large problem's mass
@@ -735,7 +783,7 @@ def build_waveguide_port_on_slab(x, y, z, masses, face: str, n_modes: int, dt: f
         sub = list(nodes)
         sub[na] = nodes[na][offset:offset + depth + 1]
     me, mm, pec = masses(*sub)
-    w = build_waveguide_port(*sub, me, mm, pec, face, n_modes, dt, f_calc, eps_r, eigensolve)
+    w = build_waveguide_port(*sub, me, mm, pec, face, n_modes, dt, f_calc, eps_r, lowest)
     if sub is nodes:
         return w
     n_sub = tuple(a.size - 1 for a in sub)

@@ -239,7 +239,7 @@ def te_mode_count(a: float, b: float, wanted: int) -> int:
 def waveguide_section_modal(rng, *, a: float = 22.86e-3, b: float = 10.16e-3, length: float = 40e-3,
                             cells: int = 48**3, n_inserts: int = 2, ridged: bool = False, n_modes=(1, 1),
                             n_lumped: int = 0, steps: int = 6000, f_min: float = 7.0e9, z0: float = 50.0,
-                            batch: int | None = None, device_setup: bool = True, eigensolve=None,
+                            batch: int | None = None, device_setup: bool = True, lowest=None,
                             device_tables: bool = True) -> FitProblem:
     """One S-parameter request of the serving workload with waveguide ports:
     an ``a x b x length`` rectangular (or single-ridge) guide on a uniform
@@ -250,7 +250,7 @@ def waveguide_section_modal(rng, *, a: float = 22.86e-3, b: float = 10.16e-3, le
     ``n_lumped`` y-directed 50 Ohm lumped ports inside the guide.
 
     The ports are built by :mod:`magnelio_b200.waveguide_ports` from the four
-    cells next to each face, the mode solve on the GPU (``eigensolve``
+    cells next to each face, the mode solve on the GPU (``lowest``
     replaces it), the DTBC kernel tables on the GPU (``device_tables``;
     else on the host).  ``f_max`` is 1.25 times the highest continuum cut-off
     of the kept modes of the empty rectangle, at least 13 GHz; it is the
@@ -311,7 +311,7 @@ def waveguide_section_modal(rng, *, a: float = 22.86e-3, b: float = 10.16e-3, le
             while True:
                 try:
                     out.append(wp.build_waveguide_port_on_slab(x, y, z, masses, face, m, dt, f_calc,
-                                                               eigensolve=eigensolve))
+                                                               lowest=lowest))
                     break
                 except NotImplementedError:
                     if m == 1:

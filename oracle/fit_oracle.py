@@ -733,16 +733,18 @@ class OracleRun:
         return 0.5 * (float(np.sum(p.M_eps * self.f.e * self.f.e)) + float(np.sum(p.M_mu * self.f.h * self.f.h)))
 
 
-def dense_port_modes(K, m_diag, threshold: float, n_modes: int):
-    """The ``n_modes`` lowest eigenpairs above ``threshold`` of
-    ``K v = lambda diag(m) v`` by a dense float64 eigensolve of
-    ``M^-1/2 K M^-1/2``, vectors scaled to ``v^T M v = 1``: the checker-side
-    stand-in for the device mode solve (the reference solves the same
-    problem with shift-invert ARPACK, ``ports/_modal/numerical_2d.py:
-    497-544``)."""
-    m = np.asarray(m_diag, float)
-    s = 1.0 / np.sqrt(m)
-    A = K.toarray() * s[:, None] * s[None, :]
-    lam, X = np.linalg.eigh(0.5 * (A + A.T))
-    keep = np.nonzero(lam > threshold)[0][:n_modes]
-    return lam[keep], X[:, keep] * s[:, None]
+def dense_lowest_eigs(L, n_modes: int, null=None):
+    """The ``n_modes`` lowest eigenpairs of the symmetric positive
+    semi-definite matrix ``L`` orthogonal to the orthonormal rows of ``null``,
+    by a dense float64 eigensolve of ``L`` with the null directions shifted
+    above the spectrum: the checker-side stand-in for the device solve (the
+    reference solves the port-mode problems with shift-invert ARPACK,
+    ``ports/_modal/numerical_2d.py:497-544``)."""
+    A = L.toarray() if hasattr(L, "toarray") else np.asarray(L, float)
+    A = 0.5 * (A + A.T)
+    if null is not None and len(null):
+        Z = np.atleast_2d(np.asarray(null, float))
+        shift = 2.0 * float(np.max(np.sum(np.abs(A), axis=1))) + 1.0
+        A = A + shift * (Z.T @ Z)
+    lam, X = np.linalg.eigh(A)
+    return lam[:n_modes], X[:, :n_modes]

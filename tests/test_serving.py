@@ -11,7 +11,7 @@ import numpy as np
 import pytest
 
 from magnelio_b200 import serving, workloads
-from oracle.fit_oracle import dense_port_modes
+from oracle.fit_oracle import dense_lowest_eigs
 
 
 class Clock:
@@ -95,7 +95,7 @@ def _loop(clock, **kw):
 
 
 def _stream(n=10, steps=(200, 400), port_kind="lumped"):
-    kw = {} if port_kind == "lumped" else {"eigensolve": dense_port_modes, "device_tables": False}
+    kw = {} if port_kind == "lumped" else {"lowest": dense_lowest_eigs, "device_tables": False}
     return serving.request_stream(n, seed=3, mean_gap=0.002, cells=(12**3, 20**3), steps=steps, ports=(2, 4),
                                   n_freq=5, port_kind=port_kind, **kw)
 

@@ -12,7 +12,7 @@ import pytest
 
 from magnelio_b200 import waveguide_ports as wp
 from magnelio_b200.adapter import _pec_face_flat_indices
-from oracle.fit_oracle import dense_port_modes
+from oracle.fit_oracle import dense_lowest_eigs
 
 F_CALC = 25e9
 PORT_KEYS = ("port_e_idx", "int_e_idx", "port_h_idx", "me_port", "me_int", "mh_port", "e_profile", "v_profile",
@@ -35,17 +35,17 @@ def _rel(a, b):
     return float(np.max(np.abs(a - b)) / max(float(np.max(np.abs(b))), 1e-300))
 
 
-def build_fixture_ports(name, n_modes, eigensolve):
+def build_fixture_ports(name, n_modes, lowest):
     d = dict(np.load(__import__("conftest").GOLDEN / f"{name}.npz", allow_pickle=True))
     x, y, z, me, mm, pec, dt = _inputs(d, name)
-    ports = [wp.build_waveguide_port(x, y, z, me, mm, pec, face, n_modes, dt, F_CALC, eigensolve=eigensolve)
+    ports = [wp.build_waveguide_port(x, y, z, me, mm, pec, face, n_modes, dt, F_CALC, lowest=lowest)
              for face in ("zmin", "zmax")]
     return d, ports, dt
 
 
 @pytest.mark.parametrize("name,n_modes", [("wg_dtbc", 2), ("cfg1_wr90", 3), ("ridge_ports", 3)])
 def test_ports_match_the_reference_builder(name, n_modes):
-    d, ports, dt = build_fixture_ports(name, n_modes, dense_port_modes)
+    d, ports, dt = build_fixture_ports(name, n_modes, dense_lowest_eigs)
     for q, w in enumerate(ports):
         for k in PORT_KEYS:
             got, ref = np.asarray(getattr(w.port, k)), d[f"p.modal{q}.{k}"]
@@ -63,7 +63,7 @@ def test_ports_match_the_reference_builder(name, n_modes):
 
 @pytest.mark.parametrize("name", ["cfg1_wr90", "ridge_ports"])
 def test_power_wave_maps_match_the_reference(name):
-    d, ports, dt = build_fixture_ports(name, 3, dense_port_modes)
+    d, ports, dt = build_fixture_ports(name, 3, dense_lowest_eigs)
     f = d["cfg1.f_axis"] if name == "cfg1_wr90" else d["ridge.f"]
     key = "cfg1.map" if name == "cfg1_wr90" else "ridge.map"
     dtm = float(d["cfg1.dt"]) if name == "cfg1_wr90" else dt
@@ -76,7 +76,7 @@ def test_power_wave_maps_match_the_reference(name):
 
 @pytest.mark.parametrize("name,n_modes", [("wg_dtbc", 2), ("ridge_ports", 3)])
 def test_excitation_samples_match_the_reference(name, n_modes):
-    d, ports, dt = build_fixture_ports(name, n_modes, dense_port_modes)
+    d, ports, dt = build_fixture_ports(name, n_modes, dense_lowest_eigs)
     ref = d["p.modal0.exc0.w"]
     m = int(d["p.modal0.exc0.mode"])
     w = ports[0]
@@ -107,8 +107,8 @@ def test_a_tm_mode_among_the_kept_ones_is_refused():
     me, mm, pec = _vacuum(x, y, z)
     dt = 0.5 * 1e-3 / 3e8
     with pytest.raises(NotImplementedError, match="TM mode"):
-        wp.build_waveguide_port(x, y, z, me, mm, pec, "zmin", 3, dt, 40e9, eigensolve=dense_port_modes)
-    w = wp.build_waveguide_port(x, y, z, me, mm, pec, "zmin", 2, dt, 40e9, eigensolve=dense_port_modes)
+        wp.build_waveguide_port(x, y, z, me, mm, pec, "zmin", 3, dt, 40e9, lowest=dense_lowest_eigs)
+    w = wp.build_waveguide_port(x, y, z, me, mm, pec, "zmin", 2, dt, 40e9, lowest=dense_lowest_eigs)
     # the degenerate pair is rotated to the principal u-energy axes: the
     # first vector carries (almost) all of its energy on the u-edges
     e = w.port.e_profile
@@ -123,8 +123,8 @@ def test_ports_need_three_equidistant_cells():
     z = np.array([0.0, 1e-3, 2.5e-3, 3.5e-3, 4.5e-3, 5.5e-3, 6.5e-3])
     me, mm, pec = _vacuum(x, y, z)
     with pytest.raises(ValueError, match="equidistant"):
-        wp.build_waveguide_port(x, y, z, me, mm, pec, "zmin", 1, 1e-12, 20e9, eigensolve=dense_port_modes)
-    w = wp.build_waveguide_port(x, y, z, me, mm, pec, "zmax", 1, 1e-12, 20e9, eigensolve=dense_port_modes)
+        wp.build_waveguide_port(x, y, z, me, mm, pec, "zmin", 1, 1e-12, 20e9, lowest=dense_lowest_eigs)
+    w = wp.build_waveguide_port(x, y, z, me, mm, pec, "zmax", 1, 1e-12, 20e9, lowest=dense_lowest_eigs)
     assert w.port.n_modes == 1
 
 
@@ -135,7 +135,7 @@ def test_x_and_y_faces_mirror_the_z_faces():
     xz, yz, zz = _box(12, 6, 8, a, b, L)
     me, mm, pec = _vacuum(xz, yz, zz)
     dt = 1e-12
-    ref = wp.build_waveguide_port(xz, yz, zz, me, mm, pec, "zmin", 2, dt, 20e9, eigensolve=dense_port_modes)
+    ref = wp.build_waveguide_port(xz, yz, zz, me, mm, pec, "zmin", 2, dt, 20e9, lowest=dense_lowest_eigs)
     # the same guide along x: cross-section (y, z) = (a, b)
     xx, yy, z2 = np.linspace(0, L, 9), np.linspace(0, a, 13), np.linspace(0, b, 7)
     from magnelio_b200 import host
@@ -147,7 +147,7 @@ def test_x_and_y_faces_mirror_the_z_faces():
     for f in ("ymin", "ymax", "zmin", "zmax"):
         pec2[_pec_face_flat_indices(*n, f)] = True
     for face in ("xmin", "xmax"):
-        got = wp.build_waveguide_port(xx, yy, z2, me2, mm2, pec2, face, 2, dt, 20e9, eigensolve=dense_port_modes)
+        got = wp.build_waveguide_port(xx, yy, z2, me2, mm2, pec2, face, 2, dt, 20e9, lowest=dense_lowest_eigs)
         for q in range(2):
             assert abs(got.channels[q].omega_c / ref.channels[q].omega_c - 1.0) < 1e-12
         assert np.allclose(got.port.record_scale, ref.port.record_scale, rtol=1e-10)
@@ -176,8 +176,8 @@ def test_a_port_built_from_its_slab_equals_the_full_build():
     m_e, m_m, pe = masses(x, y, z)
     assert np.array_equal(pe, pec) and np.array_equal(m_e, me)
     for face in ("zmin", "zmax"):
-        full = wp.build_waveguide_port(x, y, z, m_e, m_m, pe, face, 3, dt, F_CALC, eigensolve=dense_port_modes)
-        slab = wp.build_waveguide_port_on_slab(x, y, z, masses, face, 3, dt, F_CALC, eigensolve=dense_port_modes)
+        full = wp.build_waveguide_port(x, y, z, m_e, m_m, pe, face, 3, dt, F_CALC, lowest=dense_lowest_eigs)
+        slab = wp.build_waveguide_port_on_slab(x, y, z, masses, face, 3, dt, F_CALC, lowest=dense_lowest_eigs)
         for k in PORT_KEYS:
             assert np.array_equal(getattr(full.port, k), getattr(slab.port, k)), (face, k)
         assert all(np.array_equal(a, b) for a, b in zip(full.port.complement, slab.port.complement))
