@@ -181,3 +181,31 @@ def test_a_port_built_from_its_slab_equals_the_full_build():
         for k in PORT_KEYS:
             assert np.array_equal(getattr(full.port, k), getattr(slab.port, k)), (face, k)
         assert all(np.array_equal(a, b) for a, b in zip(full.port.complement, slab.port.complement))
+
+
+def test_curl_curl_assembly_matches_the_reference_operators():
+    """K and M of the WR-90 z_min plane (29 x 13 cells) assembled from the
+    face circulations equal the reference's ``build_2d_curl_curl`` slice of
+    the 3-D curl (``tests/golden/modes_wr90.npz``, free edges) to one ulp;
+    the face form L = B B^T has K's nonzero eigenvalues."""
+    from magnelio_b200 import host
+    import scipy.sparse as sp
+
+    d = np.load(__import__("conftest").GOLDEN / "modes_wr90.npz")
+    nx, ny, nz = 29, 13, 8
+    x, y, z = np.linspace(0, 22.86e-3, nx + 1), np.linspace(0, 10.16e-3, ny + 1), np.linspace(0, 8e-3, nz + 1)
+    me = host.build_M_eps(x, y, z, np.array([1.0]), np.zeros((nx, ny, nz), np.int32))
+    pl = wp.plane_edges(x, y, z, "zmin")
+    me2, mm2, pec2 = wp.flatten_port_slab((nx, ny, nz), "zmin", me, host.build_M_mu(x, y, z), np.zeros(me.size, bool))
+    mask = wp.plane_pec_mask(pl, x, y, z, pec2)
+    K, m = wp.curl_curl_2d(pl, me2, mm2)
+    free = np.nonzero(~mask)[0]
+    n = d["m"].size
+    Kr = sp.csr_matrix((d["data"], d["indices"], d["indptr"]), shape=(n, n))
+    Kf = K[free][:, free].tocsr()
+    assert Kf.shape == Kr.shape
+    assert abs(Kf - Kr).max() <= 1e-15 * np.max(np.abs(Kr.data))
+    assert np.array_equal(m[free], d["m"])
+    L, _B, null, _ = wp.te_face_problem(pl, me2, mm2, mask)
+    lam = np.linalg.eigvalsh(L.toarray() + 1e30 * (null.T @ null))[:3]
+    assert np.allclose(lam, d["eigvals"], rtol=1e-12)
