@@ -207,5 +207,5 @@ def test_curl_curl_assembly_matches_the_reference_operators():
     assert abs(Kf - Kr).max() <= 1e-15 * np.max(np.abs(Kr.data))
     assert np.array_equal(m[free], d["m"])
     L, _B, null, _ = wp.te_face_problem(pl, me2, mm2, mask)
-    lam = np.linalg.eigvalsh(L.toarray() + 1e30 * (null.T @ null))[:3]
+    lam, _ = dense_lowest_eigs(L, 3, null)
     assert np.allclose(lam, d["eigvals"], rtol=1e-12)
