@@ -179,6 +179,7 @@ struct ModalHost {
     DevBuf comp_r, comp_live;
     DevBuf st, whist, shist, comp_state, scratch, exc, wf, buflen;
     DevBuf conv;  // DTBC convolution partials of the current step
+    DevBuf part, vals, done;  // the chunked path of a large plane
     std::vector<std::vector<double>> ktabs;  // per mode: concatenated tables
     std::vector<int> n_tables_mode;
     std::vector<double> dtbc_r, dtbc_q;      // per mode: the DTBC chain parameters
@@ -254,6 +255,7 @@ struct Handle {
     std::vector<std::unique_ptr<FaceHost>> faces;
     std::vector<std::unique_ptr<LumpedHost>> lumped;
     std::vector<std::unique_ptr<ModalHost>> modal;
+    int modal_chunks = 1;  // the largest chunk count of the modal ports
     std::vector<std::unique_ptr<DftHost>> dft;
     std::vector<std::unique_ptr<PlaneWaveHost>> pws;
     DispHost disp[2];  // E side, H side
@@ -431,7 +433,8 @@ size_t device_bytes(const Handle& H) {
     for (const auto& m : H.modal) {
         for (const DevBuf* d : {&m->port_e, &m->int_e, &m->port_h, &m->me_port, &m->me_int, &m->mh_port, &m->eprof,
                                 &m->vprof, &m->hprof, &m->comp_r, &m->comp_live, &m->st, &m->whist, &m->shist,
-                                &m->comp_state, &m->scratch, &m->exc, &m->wf, &m->buflen})
+                                &m->comp_state, &m->scratch, &m->exc, &m->wf, &m->buflen, &m->part, &m->vals,
+                                &m->done})
             n += d->bytes;
         for (const auto& k : m->ktab) n += k.bytes;
     }
@@ -1037,7 +1040,8 @@ int enqueue_step_fused(Handle& H) {
     }
     if (!H.modal.empty()) {
         join_dtbc_conv(H);
-        launch_modal<T>(e_new, H.Hc().as<T>(), pa, H.d_modal.as<ModalDev>(), (int)H.modal.size(), H.stream);
+        launch_modal<T>(e_new, H.Hc().as<T>(), pa, H.d_modal.as<ModalDev>(), (int)H.modal.size(), H.modal_chunks,
+                        H.stream);
         ++n;
     }
     if (!H.lumped.empty()) {
@@ -1100,7 +1104,8 @@ int enqueue_step(Handle& H) {
     }
     if (!H.modal.empty()) {
         join_dtbc_conv(H);
-        launch_modal<T>(H.Ec().as<T>(), H.Hc().as<T>(), pa, H.d_modal.as<ModalDev>(), (int)H.modal.size(), H.stream);
+        launch_modal<T>(H.Ec().as<T>(), H.Hc().as<T>(), pa, H.d_modal.as<ModalDev>(), (int)H.modal.size(),
+                        H.modal_chunks, H.stream);
         ++n;
     }
     if (!H.band.empty()) {
@@ -2197,6 +2202,25 @@ int fitb_add_modal_port(fitb_handle* h, const fitb_modal_desc* d, int32_t* out_i
     mp->st.alloc(sizeof(double) * H.B * 4 * fitb::kMaxModes);
     mp->comp_state.alloc(sizeof(double) * H.B * 2 * ne);
     mp->scratch.alloc(sizeof(double) * H.B * 2 * ne);
+    // a plane larger than one chunk runs its projections and reconstruction
+    // over many CTAs (FITB_PORT_CHUNK overrides the chunk size, 32 .. 2^20)
+    {
+        int chunk = fitb::kPortChunk;
+        if (const char* t = std::getenv("FITB_PORT_CHUNK")) chunk = std::max(32, std::min(1 << 20, atoi(t)));
+        const long long nmax = std::max<long long>(ne, nh);
+        md.chunk = chunk;
+        md.n_chunks = ne > chunk ? (int)((nmax + chunk - 1) / chunk) : 1;
+        if (md.n_chunks > 1) {
+            std::vector<double> zero((size_t)H.B * md.n_chunks * 3 * fitb::kMaxModes, 0.0);
+            fitb::upload(mp->part, zero);
+            fitb::upload(mp->vals, std::vector<double>((size_t)H.B * 2 * fitb::kMaxModes, 0.0));
+            fitb::upload(mp->done, std::vector<int>((size_t)H.B, 0));
+            md.part = mp->part.as<double>();
+            md.vals = mp->vals.as<double>();
+            md.done = mp->done.as<int>();
+        }
+        H.modal_chunks = std::max(H.modal_chunks, md.n_chunks);
+    }
     mp->exc_host.assign((size_t)H.B, -1);
     mp->buflen_host.assign((size_t)H.B, 5);
     mp->n_wf = 1;

@@ -313,7 +313,15 @@ struct ModalDev {
     // of kConvChunk entries: [B][M][conv_chunks][2] (w, s)
     double* conv;
     int conv_chunks;
+    // large planes (n_chunks > 1): the projections and the reconstruction
+    // run over n_chunks CTAs of `chunk` edges and faces each (ports.cu)
+    int n_chunks, chunk;
+    double* part;  // [B][n_chunks][2 kMaxModes] projections, then [B][n_chunks][kMaxModes] V sums
+    double* vals;  // [B][2 kMaxModes]: the step's boundary values and interior projections
+    int* done;     // [B] reconstruction CTAs finished this step (the last one resets it)
 };
+
+constexpr int kPortChunk = 1024;  // edges per CTA of a large plane
 
 constexpr int kConvChunk = 1024;
 
@@ -336,8 +344,10 @@ struct PortsArgs {
 
 template <typename T>
 void launch_lumped(T* e, const PortsArgs& pa, const LumpedDev* d, int n_lumped, cudaStream_t s);
+// max_chunks: the largest n_chunks of the ports (1: every port in one CTA
+// per field set)
 template <typename T>
-void launch_modal(T* e, const T* h, const PortsArgs& pa, const ModalDev* d, int n_modal,
+void launch_modal(T* e, const T* h, const PortsArgs& pa, const ModalDev* d, int n_modal, int max_chunks,
                   cudaStream_t s);
 // Band-subspace DTBC port (ports_band.cu; ports/_modal/band_dtbc.py): the
 // projected boundary period of p <= kBandPMax coordinates with matrix DTBC

@@ -181,7 +181,19 @@ __global__ void __launch_bounds__(kPortThreads)
     double acc[2 * kMaxModes];
 #pragma unroll
     for (int m = 0; m < 2 * kMaxModes; ++m) acc[m] = 0.0;
-    for (int p = threadIdx.x; p < ne; p += blockDim.x) {
+    const bool split = d.n_chunks > 1;
+    if (split) {
+        // a large plane: k_modal_gather left one partial sum per chunk of
+        // edges (and faces); added here in chunk order
+        if (threadIdx.x < 2 * M) {
+            const double* pp = d.part + (long long)b * d.n_chunks * 2 * kMaxModes + threadIdx.x;
+            double a = 0.0;
+            for (int c = 0; c < d.n_chunks; ++c) a += pp[(long long)c * 2 * kMaxModes];
+            red[threadIdx.x] = a;
+        }
+        __syncthreads();
+    }
+    for (int p = split ? ne : threadIdx.x; p < ne; p += blockDim.x) {
         const double v = (double)E[d.int_e[p]];
         eint[p] = v;
         const double me = d.me_int[p];
@@ -189,7 +201,7 @@ __global__ void __launch_bounds__(kPortThreads)
         for (int m = 0; m < kMaxModes; ++m)
             if (m < M) acc[m] += me * (d.vprof[(long long)m * ne + p] * v);
     }
-    for (int p = threadIdx.x; p < nh; p += blockDim.x) {
+    for (int p = split ? nh : threadIdx.x; p < nh; p += blockDim.x) {
         const double v = (double)H[d.port_h[p]];
         const double mh = d.mh_port[p];
 #pragma unroll
@@ -201,7 +213,7 @@ __global__ void __launch_bounds__(kPortThreads)
     double ep0[kMaxModes], vp0[kMaxModes];
     long long pe0 = 0;
     double me0 = 0.0, cl0 = 0.0, cr0 = 0.0, csa0 = 0.0, csb0 = 0.0, ei0 = 0.0;
-    const int p0 = threadIdx.x;
+    const int p0 = split ? ne : threadIdx.x;
     double* cstate = d.comp_state + (long long)b * 2 * ne;
     if (p0 < ne) {
 #pragma unroll
@@ -219,7 +231,9 @@ __global__ void __launch_bounds__(kPortThreads)
             csb0 = cstate[ne + p0];
         }
     }
-    block_sum_modes<false>(acc, M, red, wred);  // ends with a block barrier (s_conv too)
+    if (!split) block_sum_modes<false>(acc, M, red, wred);  // ends with a block barrier (s_conv too)
+    const double i_sum = split && threadIdx.x < M ? red[M + threadIdx.x] : 0.0;
+    __syncthreads();
 
     // 3. Per-mode boundary value: one thread per mode (the modes' scalar
     //    float64 recursions are independent of each other).
@@ -250,7 +264,20 @@ __global__ void __launch_bounds__(kPortThreads)
             vc = un;
         }
         s_vc[m] = vc;
+        if (split) {
+            // the reconstruction runs in k_modal_scatter; the scalars that
+            // need no plane sum are final here
+            double* vals = d.vals + (long long)b * 2 * kMaxModes;
+            vals[m] = vc;
+            vals[kMaxModes + m] = vin;
+            const long long r = ((long long)b * pa.rec.cap + n) * pa.rec.nch + d.channel0 + m;
+            pa.rec.I[r] = i_sum * d.rec_scale[m];
+            Vport_prev[m] = vc;
+            Vint_prev[m] = vin;
+            atomic_max_nonneg(pa.absmax + b, fmax(0.0, fabs(vc) * d.rec_scale[m]));
+        }
     }
+    if (split) return;  // uniform over the block
     __syncthreads();
 
     // 4. Reconstruct the port plane from the modal expansion (+ complement),
@@ -305,6 +332,119 @@ __global__ void __launch_bounds__(kPortThreads)
         // fmax drops a NaN as the serial max over the modes did
         atomic_max_nonneg(pa.absmax + b, fmax(0.0, fabs(s_vc[m]) * d.rec_scale[m]));
     }
+}
+
+// Large planes, before k_modal: chunk blockIdx.x of the port's edges and
+// faces: the interior-plane samples into the scratch and the partial sums
+// of the interior projection (modes 0..M) and of the recorder's I (M..2M).
+template <typename T>
+__global__ void __launch_bounds__(kPortThreads)
+    k_modal_gather(const T* __restrict__ e, const T* __restrict__ h, PortsArgs pa, const ModalDev* __restrict__ ports) {
+    const ModalDev& d = ports[blockIdx.y];
+    const int c = blockIdx.x, b = blockIdx.z;
+    if (d.n_chunks <= 1 || c >= d.n_chunks) return;  // uniform over the block
+    const int M = d.n_modes, ne = d.n_e, nh = d.n_h;
+    const T* E = e + (long long)b * pa.e_block;
+    const T* H = h + (long long)b * pa.h_block;
+    double* eint = d.scratch + (long long)b * 2 * ne;
+    __shared__ double red[2 * kMaxModes];
+    __shared__ double wred[kPortThreads / 32][2 * kMaxModes];
+    double acc[2 * kMaxModes];
+#pragma unroll
+    for (int m = 0; m < 2 * kMaxModes; ++m) acc[m] = 0.0;
+    const int e1 = min(ne, (c + 1) * d.chunk), h1 = min(nh, (c + 1) * d.chunk);
+    for (int p = c * d.chunk + threadIdx.x; p < e1; p += blockDim.x) {
+        const double v = (double)E[d.int_e[p]];
+        eint[p] = v;
+        const double me = d.me_int[p];
+#pragma unroll
+        for (int m = 0; m < kMaxModes; ++m)
+            if (m < M) acc[m] += me * (d.vprof[(long long)m * ne + p] * v);
+    }
+    for (int p = c * d.chunk + threadIdx.x; p < h1; p += blockDim.x) {
+        const double v = (double)H[d.port_h[p]];
+        const double mh = d.mh_port[p];
+#pragma unroll
+        for (int m = 0; m < kMaxModes; ++m)
+            if (m < M) acc[kMaxModes + m] += mh * (d.hprof[(long long)m * nh + p] * v);
+    }
+    block_sum_modes<true>(acc, M, red, wred);
+    if (threadIdx.x < 2 * M)
+        d.part[((long long)b * d.n_chunks + c) * 2 * kMaxModes + threadIdx.x] = red[threadIdx.x];
+}
+
+// Large planes, after k_modal: chunk blockIdx.x of the port plane rebuilt
+// from the step's boundary values (+ complement), and the partial sums of
+// the recorder's V; the last CTA of the (port, field set) to finish adds
+// the partials in chunk order and writes the V samples.
+template <typename T>
+__global__ void __launch_bounds__(kPortThreads)
+    k_modal_scatter(T* __restrict__ e, PortsArgs pa, const ModalDev* __restrict__ ports) {
+    const ModalDev& d = ports[blockIdx.y];
+    const int c = blockIdx.x, b = blockIdx.z;
+    if (d.n_chunks <= 1 || c >= d.n_chunks) return;  // uniform over the block
+    const int M = d.n_modes, ne = d.n_e;
+    const long long n = *pa.step;
+    T* E = e + (long long)b * pa.e_block;
+    double* enew = d.scratch + (long long)b * 2 * ne + ne;
+    const double* eint = d.scratch + (long long)b * 2 * ne;
+    double* cstate = d.comp_state + (long long)b * 2 * ne;
+    __shared__ double red[2 * kMaxModes];
+    __shared__ double wred[kPortThreads / 32][2 * kMaxModes];
+    __shared__ double s_vc[kMaxModes], s_vint[kMaxModes];
+    __shared__ int s_last;
+    if (threadIdx.x < M) {
+        s_vc[threadIdx.x] = d.vals[(long long)b * 2 * kMaxModes + threadIdx.x];
+        s_vint[threadIdx.x] = d.vals[(long long)b * 2 * kMaxModes + kMaxModes + threadIdx.x];
+    }
+    __syncthreads();
+    double acc[2 * kMaxModes];
+#pragma unroll
+    for (int m = 0; m < 2 * kMaxModes; ++m) acc[m] = 0.0;
+    const int e1 = min(ne, (c + 1) * d.chunk);
+    for (int p = c * d.chunk + threadIdx.x; p < e1; p += blockDim.x) {
+        double ep[kMaxModes];
+#pragma unroll
+        for (int m = 0; m < kMaxModes; ++m) ep[m] = m < M ? d.eprof[(long long)m * ne + p] : 0.0;
+        double v = 0.0;
+#pragma unroll
+        for (int m = 0; m < kMaxModes; ++m)
+            if (m < M) v += s_vc[m] * ep[m];
+        if (d.comp_on) {
+            double ci = eint[p];
+#pragma unroll
+            for (int m = 0; m < kMaxModes; ++m)
+                if (m < M) ci -= s_vint[m] * ep[m];
+            const double cp = d.comp_live[p] * (cstate[p] + d.comp_r[p] * (ci - cstate[ne + p]));
+            v += cp;
+            cstate[p] = ci;
+            cstate[ne + p] = cp;
+        }
+        enew[p] = v;
+        const T stored = (T)v;
+        E[d.port_e[p]] = stored;
+        const double vr = (double)stored, me = d.me_port[p];
+#pragma unroll
+        for (int m = 0; m < kMaxModes; ++m)
+            if (m < M) acc[m] += me * (d.vprof[(long long)m * ne + p] * vr);
+    }
+    block_sum_modes<false>(acc, M, red, wred);
+    double* part = d.part + (long long)pa.B * d.n_chunks * 2 * kMaxModes;  // V partials after the gather area
+    if (threadIdx.x < M) part[((long long)b * d.n_chunks + c) * kMaxModes + threadIdx.x] = red[threadIdx.x];
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) s_last = atomicAdd(d.done + b, 1) == d.n_chunks - 1;
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    if (threadIdx.x < M) {
+        const int m = threadIdx.x;
+        double a = 0.0;
+        for (int q = 0; q < d.n_chunks; ++q) a += __ldcg(part + ((long long)b * d.n_chunks + q) * kMaxModes + m);
+        const long long r = ((long long)b * pa.rec.cap + n) * pa.rec.nch + d.channel0 + m;
+        pa.rec.V[r] = a * d.rec_scale[m];
+    }
+    if (threadIdx.x == 0) d.done[b] = 0;
 }
 
 // Partial DTBC convolutions of the coming update at chain step n (the
@@ -374,18 +514,20 @@ void launch_lumped(T* e, const PortsArgs& pa, const LumpedDev* d, int n_lumped, 
 }
 
 template <typename T>
-void launch_modal(T* e, const T* h, const PortsArgs& pa, const ModalDev* d, int n_modal,
+void launch_modal(T* e, const T* h, const PortsArgs& pa, const ModalDev* d, int n_modal, int max_chunks,
                   cudaStream_t s) {
     if (n_modal <= 0) return;
+    if (max_chunks > 1) k_modal_gather<T><<<dim3(max_chunks, n_modal, pa.B), kPortThreads, 0, s>>>(e, h, pa, d);
     k_modal<T><<<dim3(n_modal, pa.B), kPortThreads, 0, s>>>(e, h, pa, d);
+    if (max_chunks > 1) k_modal_scatter<T><<<dim3(max_chunks, n_modal, pa.B), kPortThreads, 0, s>>>(e, pa, d);
 }
 
 template void launch_lumped<float>(float*, const PortsArgs&, const LumpedDev*, int, cudaStream_t);
 template void launch_lumped<double>(double*, const PortsArgs&, const LumpedDev*, int,
                                     cudaStream_t);
-template void launch_modal<float>(float*, const float*, const PortsArgs&, const ModalDev*, int,
+template void launch_modal<float>(float*, const float*, const PortsArgs&, const ModalDev*, int, int,
                                   cudaStream_t);
-template void launch_modal<double>(double*, const double*, const PortsArgs&, const ModalDev*, int,
+template void launch_modal<double>(double*, const double*, const PortsArgs&, const ModalDev*, int, int,
                                    cudaStream_t);
 
 }  // namespace fitb

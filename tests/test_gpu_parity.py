@@ -129,10 +129,13 @@ def test_stencil_variants_agree(name):
         assert _rel(outs[0][1], other[1], ph) < 1e-5
 
 
-@pytest.mark.parametrize("name", ["lumped_dft", "wg_mur"])
-def test_checkpoint_resume_is_bit_exact(name):
+@pytest.mark.parametrize("name,chunk", [("lumped_dft", None), ("wg_mur", None), ("wg_mur", "32")])
+def test_checkpoint_resume_is_bit_exact(name, chunk, monkeypatch):
     """state_export after k steps, import into a fresh engine, continue:
-    identical to the uninterrupted run (fit_td.py:1264-1353 contract)."""
+    identical to the uninterrupted run (fit_td.py:1264-1353 contract); also
+    with the port plane split over several CTAs (FITB_PORT_CHUNK)."""
+    if chunk is not None:
+        monkeypatch.setenv("FITB_PORT_CHUNK", chunk)
     p, d, n = load_golden(name)
     k = n // 2 + 1
     with p.build_engine("single") as a:
@@ -1125,3 +1128,28 @@ def test_spectral_dt_on_the_device_matches_the_reference(precision, tol):
         dt, lam, its = eng.spectral_dt("normal")
     print(f"{precision}: dt {dt!r} vs {p.dt!r} after {its} Lanczos steps")
     assert abs(dt / p.dt - 1.0) < tol
+
+
+@pytest.mark.parametrize("name", ["wg_dtbc", "wg_mur", "ridge_ports"])
+@pytest.mark.parametrize("precision,tol", [("double", F64_TOL), ("single", F32_TOL)])
+def test_port_planes_split_over_many_ctas_match_reference(name, precision, tol, monkeypatch):
+    """A port plane larger than one chunk runs its projections and its
+    reconstruction over many CTAs (k_modal_gather, k_modal_scatter, the
+    chunk partials added in chunk order).  Forced here with 32-edge chunks
+    (3 to 4 chunks per plane), the march matches the reference and, in
+    float64, the one-CTA path to round-off."""
+    monkeypatch.setenv("FITB_PORT_CHUNK", "32")
+    p, d, n = load_golden(name)
+    with p.build_engine(precision) as eng:
+        eng.step(n)
+        V, I = eng.read_vi()
+        e, h = eng.read_fields()
+    assert _rel(V, d["out.V"]) < tol and _rel(I, d["out.I"]) < tol
+    pe, ph = _peaks(name)
+    assert _rel(e, d["out.e"], pe) < tol and _rel(h, d["out.h"], ph) < tol
+    if precision == "double":
+        monkeypatch.delenv("FITB_PORT_CHUNK")
+        with p.build_engine(precision) as one:
+            one.step(n)
+            V1, I1 = one.read_vi()
+        assert _rel(V, V1) < 1e-12 and _rel(I, I1) < 1e-12
