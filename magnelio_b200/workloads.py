@@ -327,6 +327,8 @@ def waveguide_section_modal(rng, *, a: float = 22.86e-3, b: float = 10.16e-3, le
         f_max = 1.25 * f_top
         ports = build_ports(f_max)
     n_ch = sum(w.port.n_modes for w in ports) + n_lumped
+    if batch is not None and batch < n_ch:
+        raise ValueError(f"batch {batch} below the request's {n_ch} driven channels")
     B = batch if batch is not None else n_ch
     B = next(v for v in (1, 2, 4, 8, 16, B) if v >= B)
     materials = MaterialSetup(mat_id=mat_id, eps_r=eps_table, pec_idx=pec_of(x, y, z))

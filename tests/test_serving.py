@@ -303,3 +303,11 @@ def test_modal_requests_agree_between_the_batched_and_single_excitation_forms():
         assert a.S.shape == b.S.shape and a.S.shape[1] == a.S.shape[2]
         np.testing.assert_allclose(a.V, b.V, rtol=0, atol=0)
         np.testing.assert_allclose(a.S, b.S, rtol=1e-12, atol=0)
+
+
+def test_a_modal_request_refuses_fewer_field_sets_than_channels():
+    import numpy as np
+
+    with pytest.raises(ValueError, match="driven channels"):
+        workloads.waveguide_section_modal(np.random.default_rng(2), cells=12**3, n_modes=(2, 2), steps=50,
+                                          batch=2, lowest=dense_lowest_eigs, device_tables=False)
