@@ -54,3 +54,28 @@ def test_errors_are_reported_without_a_device():
         with pytest.raises(_lib.FitbError) as ei:
             FitEngine(4, 4, 4, 1e-12)
         assert ei.value.code in (-5, -2)
+
+
+def test_sparse_eigensolve_checks_its_arguments_before_touching_a_device():
+    """fitb_sparse_eigs validates sizes, row pointers and column indices on
+    the host and reports them as status codes (no device needed)."""
+    import numpy as np
+    import scipy.sparse as sp
+
+    from magnelio_b200 import _lib
+    from magnelio_b200.engine import sparse_eigs
+
+    L = sp.diags([2.0, 3.0, 4.0, 5.0]).tocsr()
+    with pytest.raises(_lib.FitbError, match="n_modes"):
+        sparse_eigs(L, 17)
+    with pytest.raises(_lib.FitbError, match="n_modes \\+ n_null"):
+        sparse_eigs(L, 3, null=np.eye(4)[:2])
+    lib = _lib.load()
+    rp = np.array([0, 1, 2], np.int64)
+    col = np.array([0, 5], np.int64)
+    val = np.ones(2)
+    out = np.zeros(2)
+    vec = np.zeros(4)
+    rc = lib.fitb_sparse_eigs(0, 2, _lib.i64p(rp), _lib.i64p(col), _lib.f64p(val), 0, None, 1, 1e-14,
+                              _lib.f64p(out), _lib.f64p(vec), None, None)
+    assert rc != 0 and "column index" in _lib.last_error()
