@@ -20,7 +20,9 @@ whole bbox face of a hollow guide with PEC side walls:
 5. the TE eigenpairs (``Numerical2DModeSolver._solve_te_tm``,
    ``numerical_2d.py:454-583``), solved on the GPU in the equivalent face
    form by ``fitb_sparse_eigs`` (Chebyshev-filtered subspace iteration; the
-   face form has no gradient null space to filter), with the reference's sign rule
+   face form has no gradient null space to filter), and the TM eigenpairs
+   (``_solve_tm`` :585-729) from the normal-edge problem, with the
+   reference's sign rule
    (``_resolve_sign`` :758-802), wave impedance (``_z_real_at`` :828-853),
    travelling-wave H profiles (``tem_laplace.py:102-160``) and the basis
    rotation inside degenerate groups (``factory.py:1247-1316``);
@@ -38,10 +40,11 @@ Scope: the port covers the whole face of a hollow guide (one conductor,
 the walls) with a homogeneous filling ``eps_r`` and PEC side walls; where
 the flat PEC mask marks no edge of the plane, the four lateral bbox faces
 are the walls, as in the reference.  The caller states that geometry: this
-module does not classify conductors.  A TM mode among the requested lowest
-cut-offs raises ``NotImplementedError``.  Sub-face windows, PMC side walls,
-multi-conductor (TEM / quasi-TEM) planes and TM channels come from the
-reference's own setup (``adapter.problem_from_solver``).
+module does not classify conductors.  The kept modes are the lowest
+cut-offs of both families, TE from the face form and TM from the
+normal-edge problem (gradient profiles, TM impedances).  Sub-face windows, PMC side walls and multi-conductor (TEM /
+quasi-TEM) planes come from the reference's own setup
+(``adapter.problem_from_solver``).
 """
 
 from __future__ import annotations
@@ -325,21 +328,37 @@ def z_te(omega: float, omega_c: float, eps_r: float) -> complex:
     return 1j * omega * MU0 / gamma_of(omega, omega_c, eps_r)
 
 
-def _z_real_te(omega: float, omega_c: float, eps_r: float) -> float:
+def z_tm(omega: float, omega_c: float, eps_r: float) -> complex:
+    """TM wave impedance ``gamma / (j omega eps0 eps_r)`` (``mode.py:210-211``)."""
+    return gamma_of(omega, omega_c, eps_r) / (1j * omega * EPS0 * eps_r)
+
+
+def z_wave(kind: str, omega: float, omega_c: float, eps_r: float) -> complex:
+    return z_te(omega, omega_c, eps_r) if kind == "TE" else z_tm(omega, omega_c, eps_r)
+
+
+def _z_real(kind: str, omega: float, omega_c: float, eps_r: float) -> float:
+    """``|Z|`` for the H-profile bake-in: ``omega mu0 / r`` (TE) or
+    ``r / (omega eps0 eps_r)`` (TM), ``r = sqrt|kc^2 - k^2|``
+    (``numerical_2d.py:828-853``)."""
     diff = omega_c ** 2 * MU0 * EPS0 * eps_r - omega ** 2 * MU0 * EPS0 * eps_r
     if abs(diff) < 1e-30:
         raise ValueError("the mode-calculation frequency coincides with a cut-off")
-    return omega * MU0 / math.sqrt(abs(diff))
+    r = math.sqrt(abs(diff))
+    return omega * MU0 / r if kind == "TE" else r / (omega * EPS0 * eps_r)
 
 
 @dataclass
 class TeMode:
+    """One port mode's cut-off and discrete profiles; ``kind`` "TE" or "TM"."""
+
     omega_c: float
     e_u: np.ndarray
     e_v: np.ndarray
     h_u: np.ndarray
     h_v: np.ndarray
     eps_r: float = 1.0
+    kind: str = "TE"
 
 
 def _device_lowest(L, n_modes, null=None):
@@ -411,10 +430,56 @@ def te_modes(pl: PlaneEdges, m_eps, m_mu, pec_mask, n_modes: int, f_calc: float,
         v = resolve_sign(pl, v)
         e_u, e_v = v[:n_u].copy(), v[n_u:].copy()
         wc = float(math.sqrt(lam[q]))
-        s = scale_num / _z_real_te(omega, wc, eps_r)
+        s = scale_num / _z_real("TE", omega, wc, eps_r)
         h_u = np.where(mu_u > 0, -e_v * (s / np.where(mu_u > 0, mu_u, 1.0)), 0.0)
         h_v = np.where(mu_v > 0, +e_u * (s / np.where(mu_v > 0, mu_v, 1.0)), 0.0)
         out.append(TeMode(wc, e_u, e_v, h_u, h_v, eps_r))
+    return out
+
+
+def tm_modes(pl: PlaneEdges, m_eps, m_mu, pec_e, plane_has_pec: bool, n_modes: int, f_calc: float,
+             eps_r: float = 1.0, lowest=None) -> list[TeMode]:
+    """The ``n_modes`` lowest TM modes (``numerical_2d.py:585-729``): the
+    lowest eigenpairs of the normal-edge problem (:func:`tm_curl_curl_2d`,
+    Dirichlet nodes removed, ``M_z^-1/2 K_z M_z^-1/2`` positive definite),
+    the transversal profile the topological gradient of the node values
+    (u-edge ``phi(a+1, b) - phi(a, b)``, v-edge ``phi(a, b+1) - phi(a, b)``)
+    normalised to ``e^T M_eps e = 1``, the reference's sign rule, and the
+    travelling-wave H profiles with the TM impedance."""
+    solve = lowest or _device_lowest
+    na, _, ua, va = FACE_AXES[pl.face]
+    nu, nv = pl.n[ua], pl.n[va]
+    Kz, mz, dirichlet = tm_curl_curl_2d(pl, m_eps, m_mu, pec_e, plane_has_pec)
+    free = np.nonzero(~dirichlet)[0]
+    if free.size < n_modes + 1:
+        return []
+    sz = 1.0 / np.sqrt(mz[free])
+    Lz = (sp.diags(sz) @ Kz.tocsr()[free, :][:, free] @ sp.diags(sz)).tocsr()
+    lam, Y = solve(Lz, n_modes, None)
+    lam = np.asarray(lam, float)
+    if np.any(lam <= 0.0) or not np.all(np.isfinite(lam)):
+        raise RuntimeError(f"TM eigenvalues not positive: {lam}")
+    m2 = np.asarray(m_eps, float)[pl.e_all]
+    n_u = pl.e_u.size
+    omega = 2.0 * math.pi * f_calc
+    scale_num = MU0 * pl.normal_dx
+    mu_u, mu_v = np.asarray(m_mu, float)[pl.h_u], np.asarray(m_mu, float)[pl.h_v]
+    out = []
+    for q in range(n_modes):
+        phi = np.zeros((nu + 1) * (nv + 1))
+        phi[free] = Y[:, q] * sz  # the node values of the generalised problem
+        P = phi.reshape(nu + 1, nv + 1)
+        e = np.concatenate([(P[1:, :] - P[:-1, :]).ravel(), (P[:, 1:] - P[:, :-1]).T.ravel()])
+        norm = float(np.einsum("i,i,i->", e, m2, e))
+        if not norm > 0.0:
+            raise RuntimeError("a TM profile with a non-positive M_eps norm")
+        e = resolve_sign(pl, e / math.sqrt(norm))
+        e_u, e_v = e[:n_u].copy(), e[n_u:].copy()
+        wc = float(math.sqrt(lam[q]))
+        s = scale_num / _z_real("TM", omega, wc, eps_r)
+        h_u = np.where(mu_u > 0, -e_v * (s / np.where(mu_u > 0, mu_u, 1.0)), 0.0)
+        h_v = np.where(mu_v > 0, +e_u * (s / np.where(mu_v > 0, mu_v, 1.0)), 0.0)
+        out.append(TeMode(wc, e_u, e_v, h_u, h_v, eps_r, "TM"))
     return out
 
 
@@ -427,8 +492,8 @@ def fix_degenerate_gauge(modes: list[TeMode], rtol: float = DEGENERATE_RTOL) -> 
     i = 0
     while i < len(modes):
         j = i + 1
-        while j < len(modes) and modes[i].omega_c > 0.0 and abs(modes[j].omega_c - modes[i].omega_c) < rtol * abs(
-                modes[j].omega_c):
+        while (j < len(modes) and modes[i].omega_c > 0.0 and modes[j].kind == modes[i].kind
+               and abs(modes[j].omega_c - modes[i].omega_c) < rtol * abs(modes[j].omega_c)):
             j += 1
         if j - i >= 2:
             grp = modes[i:j]
@@ -439,10 +504,15 @@ def fix_degenerate_gauge(modes: list[TeMode], rtol: float = DEGENERATE_RTOL) -> 
             R = R[:, np.argsort(vals)[::-1]]
             new = [R.T @ a for a in stacks]
             for k in range(j - i):
-                anchor = new[0][k] if np.any(new[0][k]) else new[1][k]
+                # a vector with no u-energy (numerically: below 1e-12 of
+                # its largest entry) takes its sign from e_v; the reference
+                # tests for exact zeros, which round-off never gives, so
+                # there the sign of such a vector follows the round-off
+                scale = max(float(np.max(np.abs(new[0][k]))), float(np.max(np.abs(new[1][k]))), 1e-300)
+                anchor = new[0][k] if float(np.max(np.abs(new[0][k]))) > 1e-12 * scale else new[1][k]
                 sg = -1.0 if anchor[int(np.argmax(np.abs(anchor)))] < 0.0 else 1.0
                 modes[i + k] = TeMode(grp[k].omega_c, sg * new[0][k], sg * new[1][k], sg * new[2][k],
-                                      sg * new[3][k], grp[k].eps_r)
+                                      sg * new[3][k], grp[k].eps_r, grp[k].kind)
         i = j
     return modes
 
@@ -500,6 +570,7 @@ class ChannelInfo:
     eps_r: float
     normal_dx: float
     line: tuple | None  # (r, q, z0) of a certified chain, else None
+    kind: str = "TE"
 
 
 @dataclass
@@ -537,22 +608,23 @@ def build_waveguide_port(x, y, z, m_eps, m_mu, pec_e, face: str, n_modes: int, d
     pl = plane_edges(x, y, z, face)
     me, mm, pec = flatten_port_slab(n, face, m_eps, m_mu, np.asarray(pec_e, bool))
     mask = plane_pec_mask(pl, x, y, z, pec)
-    modes = te_modes(pl, me, mm, mask, n_modes, f_calc, eps_r, lowest)
-    # the kept set must hold no TM mode (the reference keeps the n lowest
-    # cut-offs of both families)
+    # both families, the n lowest cut-offs kept, TE first on a tie, as the
+    # reference's stable sort of TE + TM (factory.py:1641-1651).  A
+    # rectangle's TE_mn and TM_mn share their discrete cut-off to round-off,
+    # so cut-offs within 1e-12 count as tied rather than letting the last
+    # bit order them.
     plane_has_pec = bool(pec[pl.e_u].any() or pec[pl.e_v].any())
-    Kz, mz, dirichlet = tm_curl_curl_2d(pl, me, mm, pec, plane_has_pec)
-    free = np.nonzero(~dirichlet)[0]
-    if free.size:
-        solve = lowest or _device_lowest
-        sz = 1.0 / np.sqrt(mz[free])
-        Lz = (sp.diags(sz) @ Kz.tocsr()[free, :][:, free] @ sp.diags(sz)).tocsr()
-        lam_tm, _ = solve(Lz, 1, None)
-        wc_tm = math.sqrt(float(lam_tm[0]))
-        if wc_tm < modes[-1].omega_c * (1.0 + DEGENERATE_RTOL):
-            raise NotImplementedError(
-                f"port {face}: a TM mode (cut-off {wc_tm / (2 * math.pi):.4g} Hz) is among the {n_modes} "
-                "lowest; TM channels are built by the reference's setup only")
+    te = te_modes(pl, me, mm, mask, n_modes, f_calc, eps_r, lowest)
+    tm = tm_modes(pl, me, mm, pec, plane_has_pec, n_modes, f_calc, eps_r, lowest)
+
+    def order(a, b):
+        if abs(a.omega_c - b.omega_c) <= 1e-12 * max(a.omega_c, b.omega_c):
+            return (a.kind == "TM") - (b.kind == "TM")
+        return -1 if a.omega_c < b.omega_c else 1
+
+    import functools
+
+    modes = sorted(te + tm, key=functools.cmp_to_key(order))[:n_modes]
     modes = fix_degenerate_gauge(modes)
 
     me_u, me_v = me[pl.e_u], me[pl.e_v]
@@ -569,7 +641,7 @@ def build_waveguide_port(x, y, z, m_eps, m_mu, pec_e, face: str, n_modes: int, d
     for q, md in enumerate(modes):
         V_t = float(np.dot(me_u, md.e_u ** 2)) + float(np.dot(me_v, md.e_v ** 2))
         I_t = float(np.dot(mh_u, md.h_u ** 2)) + float(np.dot(mh_v, md.h_v ** 2))
-        Z = z_te(omega, md.omega_c, eps_r)
+        Z = z_wave(md.kind, omega, md.omega_c, eps_r)
         Zr = float(Z.real)
         p_one = float(np.dot(md.e_u * (md.h_v * mh_v / (MU0 * ndx)), area_u)) - float(
             np.dot(md.e_v * (md.h_u * mh_u / (MU0 * ndx)), area_v))
@@ -595,7 +667,7 @@ def build_waveguide_port(x, y, z, m_eps, m_mu, pec_e, face: str, n_modes: int, d
             else:
                 record_scale[q] = kappa
                 source_scale[q] = math.sqrt(abs(Zr)) / kappa
-        cal.append(TeMode(md.omega_c, md.e_u, md.e_v, md.h_u * g, md.h_v * g, eps_r) if ok else md)
+        cal.append(TeMode(md.omega_c, md.e_u, md.e_v, md.h_u * g, md.h_v * g, eps_r, md.kind) if ok else md)
     modes = cal
 
     # Mur coefficients and TF/SF delays from the continuum phase velocity
@@ -633,7 +705,7 @@ def build_waveguide_port(x, y, z, m_eps, m_mu, pec_e, face: str, n_modes: int, d
                     z0 = r * n_v * c_pair / (dt * n_i) if qm > 0.0 else None
                     line = (r, qm, z0)
                     is_dtbc[q], r_of[q], q_of[q] = 1, r, qm
-        channels.append(ChannelInfo(md.omega_c, eps_r, ndx, line))
+        channels.append(ChannelInfo(md.omega_c, eps_r, ndx, line, md.kind))
 
     # complement absorber (factory.py:687-737)
     m_vac = flatten_port_slab(n, face, EPS0 * host.geom_E(x, y, z), mm, pec)[0]
@@ -699,14 +771,15 @@ def excitation_waveform(omega_c: float, f_max: float, f_min: float = 0.0):
     return lambda t: float(host.modulated_gaussian(t, f_max, edge))
 
 
-def dtbc_wave_impedance(w_dt, q: float, z0: float):
-    """TE wave impedance of the discrete outgoing wave,
-    ``z0 s / sqrt(s^2 - (q/2)^2)`` with ``s = sin(w dt / 2)``, the root
-    ``-j sqrt(.)`` below the discrete cut-off (``dtbc.py:234-288``)."""
+def dtbc_wave_impedance(w_dt, q: float, z0: float, kind: str = "TE"):
+    """Wave impedance of the discrete outgoing wave, ``z0 s / rad`` (TE) or
+    ``z0 rad / s`` (TM), ``s = sin(w dt / 2)``, ``rad = sqrt(s^2 - (q/2)^2)``
+    with the root ``-j sqrt(.)`` below the discrete cut-off
+    (``dtbc.py:234-288``)."""
     s = np.sin(np.asarray(w_dt, float) / 2.0)
     d = s * s - (q / 2.0) ** 2
     rad = np.where(d >= 0.0, np.sqrt(np.maximum(d, 0.0)) + 0.0j, -1j * np.sqrt(np.maximum(-d, 0.0)))
-    return z0 * s / rad
+    return z0 * s / rad if kind == "TE" else z0 * rad / s
 
 
 def destagger_theta(w_dt, r: float, q: float):
@@ -725,9 +798,9 @@ def power_wave_maps(ch: ChannelInfo, freqs, dt: float) -> np.ndarray:
     ``gamma dn / 2`` otherwise."""
     omega = 2.0 * np.pi * np.asarray(freqs, float)
     if ch.line is not None and ch.line[2] is not None:
-        Z = dtbc_wave_impedance(omega * dt, ch.line[1], ch.line[2])
+        Z = dtbc_wave_impedance(omega * dt, ch.line[1], ch.line[2], ch.kind)
     else:
-        Z = np.array([z_te(float(w), ch.omega_c, ch.eps_r) for w in omega], complex)
+        Z = np.array([z_wave(ch.kind, float(w), ch.omega_c, ch.eps_r) for w in omega], complex)
     with np.errstate(divide="ignore", invalid="ignore"):
         sZ = np.sqrt(Z)
         if ch.line is not None:

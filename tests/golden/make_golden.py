@@ -553,6 +553,49 @@ def case_ridge_ports():
     _save("ridge_ports", prob, _outputs(s, prob, out), n, "single-ridge guide, 2 ports x 3 modes, p1 mode 0 driven")
 
 
+def case_square_ports():
+    """Square guide (10 x 10 mm, 10 x 10 x 8 cells, 8 mm long), two
+    waveguide ports with 4 modes each: the degenerate TE10 / TE01 pair and
+    the TE11 / TM11 pair, so a TM channel is kept; port p1 mode 3 driven,
+    300 steps.  Stores the reference-built problem, the power-wave maps and
+    the reference's V/I."""
+    from magnelio.mesh.grid import GridLines
+    from magnelio.mesh.mesher import Mesh
+    from magnelio.post.modal_sparameters import spectral_power_waves
+
+    a, L, n = 10e-3, 8e-3, 300
+    grid = GridLines(x=np.linspace(0, a, 11), y=np.linspace(0, a, 11), z=np.linspace(0, L, 9))
+    mesh = Mesh.from_grid(grid, boundary_conditions={"xmin": "PEC", "xmax": "PEC", "ymin": "PEC", "ymax": "PEC",
+                                                     "zmin": "PMC", "zmax": "PMC"})
+    s = _wg_solver(mesh, ("p1", 3), n, n_modes=4)
+    prob = problem_from_solver(s, n)
+    import magnelio.analysis.scattering_td as std
+    from magnelio._operators.material_matrices import build_M_eps, build_M_mu
+    from magnelio.ports.declarative import PortWaveguide
+
+    an = std.AnalysisScatteringTD(mesh=mesh, f_max=25e9, ports=[PortWaveguide("p1", "zmin", n_modes=4),
+                                                                PortWaveguide("p2", "zmax", n_modes=4)],
+                                  verbose=False, backend="numpy", precision="double", n_freq=11)
+    m_eps, m_mu = build_M_eps(mesh), build_M_mu(mesh)
+    ops, _, _, _, _, modes, ndx, lines = an._prepare_excitation_run(("p1", 3), None, m_eps, m_mu, s.dt, 25e9)
+    out = {"square.kinds": np.array([[m.mode_type.value for m in modes[pt]] for pt in ("p1", "p2")])}
+    f = np.linspace(22e9, 25e9, 12)
+    out["square.f"] = f
+    one, zero = np.ones_like(f, complex), np.zeros_like(f, complex)
+    c = 0
+    for port in ("p1", "p2"):
+        for m in range(4):
+            aV, bV = spectral_power_waves(one, zero, 2 * np.pi * f, s.dt, modes[port][m], normal_dx=ndx[port],
+                                          line_params=lines.get((port, m)))
+            aI, bI = spectral_power_waves(zero, one, 2 * np.pi * f, s.dt, modes[port][m], normal_dx=ndx[port],
+                                          line_params=lines.get((port, m)))
+            out[f"square.map{c}"] = np.stack([aV, aI, bV, bI])
+            c += 1
+    print("square kinds", out["square.kinds"], [m.omega_c / 2 / np.pi for m in modes["p1"]])
+    s.run()
+    _save("square_ports", prob, _outputs(s, prob, out), n, "square guide, 2 ports x 4 modes (TE, TE, TE, TM), p1 mode 3 driven")
+
+
 def case_cfg1_wr90():
     """The plain small configuration: WR-90 section 22.86 x 10.16 x 40 mm on a
     29 x 13 x 51 grid, two waveguide ports (zmin, zmax) x 3 modes, all six
@@ -885,6 +928,7 @@ CASES = {
     "lumped_dft": case_lumped_dft,
     "wg_dtbc": case_wg_dtbc,
     "ridge_ports": case_ridge_ports,
+    "square_ports": case_square_ports,
     "wg_mur": case_wg_mur,
     "wg_stop": case_wg_stop,
     "cpml_stop": case_cpml_stop,

@@ -15,12 +15,22 @@ from magnelio_b200 import waveguide_ports as wp
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("name,n_modes", [("cfg1_wr90", 3), ("ridge_ports", 3)])
+@pytest.mark.parametrize("name,n_modes", [("cfg1_wr90", 3), ("ridge_ports", 3), ("square_ports", 4)])
 def test_device_mode_solve_builds_the_reference_ports(name, n_modes):
+    """The ports built with the device solves (TE face form and TM
+    normal-edge problem) equal the reference-built ones; for the square
+    guide's degenerate pair the sign that the reference took from round-off
+    is allowed to differ (see ``_round_off_signs``)."""
+    from test_waveguide_ports import _round_off_signs
+
     d, ports, _ = build_fixture_ports(name, n_modes, None)
     for q, w in enumerate(ports):
+        flip = _round_off_signs(d, q)
         for k in PORT_KEYS:
-            assert _rel(getattr(w.port, k), d[f"p.modal{q}.{k}"]) < 5e-12, (q, k)
+            ref = d[f"p.modal{q}.{k}"]
+            if k in ("e_profile", "v_profile", "h_profile"):
+                ref = ref * flip[:, None]
+            assert _rel(getattr(w.port, k), ref) < 5e-12, (q, k)
 
 
 @pytest.mark.parametrize("precision,tol,field_tol", [("double", 1e-9, 1e-9), ("single", 2e-4, 1e-3)])

@@ -33,7 +33,8 @@ def test_kernel_sweep_matches_reference_numba_kernels():
 
 
 @pytest.mark.parametrize("name", ["cpml_box", "mixed_box", "lumped_dft", "wg_dtbc", "wg_mur", "planewave_box",
-                                  "dispersive_box", "sibc_box", "band_line", "ridge_ports"])
+                                  "dispersive_box", "sibc_box", "band_line", "ridge_ports",
+                                  "square_ports"])
 def test_oracle_march_matches_reference(name):
     p, d, n = load_golden(name)
     r = OracleRun(p).run(n)
