@@ -231,7 +231,9 @@ def te_cutoffs(a: float, b: float, count: int) -> tuple[np.ndarray, float]:
 
 def te_mode_count(a: float, b: float, wanted: int) -> int:
     """At most ``wanted`` modes, all below 0.97 of the TM11 cut-off of the
-    empty rectangle (a port keeps TE channels only)."""
+    empty rectangle: the served requests keep clear of the degenerate
+    TE11 / TM11 pair, whose cross-coupling at a modal port the reference
+    warns of."""
     fc, f_tm = te_cutoffs(a, b, wanted)
     return max(1, int(np.sum(fc < 0.97 * f_tm)))
 
@@ -245,8 +247,7 @@ def waveguide_section_modal(rng, *, a: float = 22.86e-3, b: float = 10.16e-3, le
     an ``a x b x length`` rectangular (or single-ridge) guide on a uniform
     grid of about ``cells`` cells, PEC side walls, ``n_inserts`` dielectric
     blocks (``eps_r ~ U[2, 10]``) kept four cells clear of both ends, modal
-    ports on ``zmin`` and ``zmax`` with ``n_modes`` TE modes each (a port
-    whose requested modes would include a TM mode keeps fewer), and
+    ports on ``zmin`` and ``zmax`` with the ``n_modes`` lowest modes each, and
     ``n_lumped`` y-directed 50 Ohm lumped ports inside the guide.
 
     The ports are built by :mod:`magnelio_b200.waveguide_ports` from the four
@@ -306,18 +307,8 @@ def waveguide_section_modal(rng, *, a: float = 22.86e-3, b: float = 10.16e-3, le
     f_max = max(13.0e9, 1.25 * float(te_cutoffs(a, b, max(want))[0][-1]))
 
     def build_ports(f_calc):
-        out = []
-        for face, m in zip(("zmin", "zmax"), want):
-            while True:
-                try:
-                    out.append(wp.build_waveguide_port_on_slab(x, y, z, masses, face, m, dt, f_calc,
-                                                               lowest=lowest))
-                    break
-                except NotImplementedError:
-                    if m == 1:
-                        raise
-                    m -= 1
-        return out
+        return [wp.build_waveguide_port_on_slab(x, y, z, masses, face, m, dt, f_calc, lowest=lowest)
+                for face, m in zip(("zmin", "zmax"), want)]
 
     ports = build_ports(f_max)
     # a ridge can raise a higher mode's cut-off above the empty guide's:
