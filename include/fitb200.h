@@ -129,10 +129,17 @@ typedef struct fitb_plane_wave_desc {
 } fitb_plane_wave_desc;
 
 /* ---- lifetime ------------------------------------------------------- */
+/* FITB_ABI_VERSION of the built library; a binding compares it with the
+ * header it was written against (no counterpart in the reference). */
 int fitb_abi_version(void);
 /* Replaces FITTimeDomainSolver.setup() allocation (fit_td.py:302-324). */
 int fitb_create(const fitb_desc* desc, fitb_handle** out);
+/* Frees the handle and all device memory it owns (the reference drops its
+ * arrays with the solver object). */
 int fitb_destroy(fitb_handle* h);
+/* Message of the most recent failed call, NUL-terminated into buf (the
+ * reference raises exceptions; the binding turns a non-zero status and
+ * this message into one). */
 int fitb_last_error(char* buf, size_t len);
 /* Number of this library's kernel launches issued so far on the handle. */
 int fitb_launch_count(const fitb_handle* h, int64_t* out);
@@ -407,6 +414,9 @@ int fitb_read_dft(fitb_handle* h, int32_t mon, int32_t b, int32_t comp,
 /* Advance all field sets by n_steps leapfrog steps (the body of the loop
  * at fit_td.py:950-1007), replaying captured CUDA graphs. */
 int fitb_step(fitb_handle* h, int64_t n_steps);
+/* Blocks until every issued step has finished, then checks the device
+ * status word that the pipelined kernels' bounded waits set (an expired
+ * wait is an error); the reference's loop is synchronous at every step. */
 int fitb_sync(fitb_handle* h);
 /* Non-blocking: *done = 1 when every step issued so far has finished on the
  * device (then also the fitb_sync checks ran), 0 while work is in flight.
@@ -428,6 +438,7 @@ int fitb_step_timed(fitb_handle* h, int64_t n_steps, double* ms);
  * fields like n_iter half steps each, so call it only after the run whose
  * results are wanted. */
 int fitb_time_stencil(fitb_handle* h, int32_t n_iter, double* ms_e, double* ms_h);
+/* Steps taken so far (the solver's step counter n, fit_td.py:950). */
 int fitb_steps_done(fitb_handle* h, int64_t* out);
 /* 0.5 * (sum M_eps e^2 + sum M_mu h^2), float64 accumulation
  * (fit_td.py:1014-1018). */
