@@ -86,6 +86,8 @@ class RunResult:
     final_signal_db: float | None
     energy_trace: np.ndarray
     aborted: bool = False
+    # first check point whose stored energy was NaN or infinite (None: never)
+    non_finite_step: int | None = None
 
 
 def energy_trace_array(trace, dt) -> np.ndarray:
@@ -126,6 +128,11 @@ class FitRun:
     # with reset() / observe(n, sig_db, threshold_db) / window /
     # slope_db_per_step
     stall_detector: object = None
+    # Divergence sentinel.  A NaN or infinite stored energy at a check point
+    # is always reported (a RuntimeWarning and RunResult.non_finite_step);
+    # the reference keeps marching in that case, and so does this loop
+    # unless stop_on_non_finite ends the run there (reason "non_finite").
+    stop_on_non_finite: bool = False
     _stop_requested: bool = field(default=False, init=False)
 
     def request_stop(self) -> None:
@@ -172,13 +179,14 @@ class FitRun:
             window = max(STALL_MIN_WINDOW_CHECKS, (self.port_signal_min_steps or 0) // (2 * ci))
             stall = (self.stall_detector or SignalStallDetector)(STALL_ARM_DB, window, cap_steps)
         last_sig_db = None
+        non_finite_step = None
         self._stop_requested = False
         end = n_steps if not unbounded else cap_steps  # None: open-ended
         done = resume_step  # completed steps on the device
 
         def result(reason, steps, aborted=False):
             return RunResult(reason, steps, steps, peak_energy, peak_signal, last_sig_db,
-                             energy_trace_array(trace, self.dt), aborted)
+                             energy_trace_array(trace, self.dt), aborted, non_finite_step)
 
         counter = itertools.count(resume_step) if end is None else range(resume_step, end)
         n = resume_step
@@ -194,6 +202,16 @@ class FitRun:
             done = n + 1
             current = self.engine.energy(b)
             trace.append((n, current))
+            if non_finite_step is None and not math.isfinite(current):
+                non_finite_step = n + 1
+                warnings.warn(
+                    f"stored energy is {current!r} after step {n + 1}: the fields have diverged "
+                    f"(an unstable time step, or a NaN or infinite coefficient or source sample)",
+                    RuntimeWarning,
+                    stacklevel=2,
+                )
+                if self.stop_on_non_finite:
+                    return result("non_finite", n + 1)
             if current > peak_energy:
                 peak_energy = current
                 if energy_stop is not None:

@@ -103,3 +103,29 @@ def test_stall_detector_slope_fit():
     det = SignalStallDetector(40.0, 5, 10_000)
     fired = [det.observe(n, -50.0 - 0.0001 * n, -60.0) for n in range(0, 500, 100)]
     assert fired[-1] and det.slope_db_per_step is not None
+
+
+def test_non_finite_energy_is_reported_and_the_reference_decisions_kept():
+    # energy finite up to step 99, NaN from step 100 on: the check after
+    # step 108 (checks every 12 steps) is the first to see it
+    eng = ScriptedEngine(energy=lambda n: 1.0 if n < 100 else float("nan"))
+    with pytest.warns(RuntimeWarning, match="diverged"):
+        res = FitRun(eng, 1e-12, total_time_steps=250).run()
+    assert res.stop_reason == "steps" and res.actual_steps == 250 and eng.n == 250
+    assert res.non_finite_step == 109
+    # an infinite energy is reported too; the clean run reports nothing
+    eng = ScriptedEngine(energy=lambda n: 1.0 if n < 30 else float("inf"))
+    with pytest.warns(RuntimeWarning, match="diverged"):
+        assert FitRun(eng, 1e-12, total_time_steps=250).run().non_finite_step == 37
+    with warnings.catch_warnings():
+        warnings.simplefilter("error")
+        assert FitRun(ScriptedEngine(), 1e-12, total_time_steps=250).run().non_finite_step is None
+
+
+def test_non_finite_energy_ends_the_run_when_asked():
+    eng = ScriptedEngine(energy=lambda n: 1.0 if n < 100 else float("nan"))
+    with pytest.warns(RuntimeWarning, match="diverged"):
+        res = FitRun(eng, 1e-12, total_time_steps=250, stop_on_non_finite=True).run()
+    assert res.stop_reason == "non_finite" and res.actual_steps == 109 and eng.n == 109
+    assert res.non_finite_step == 109
+    assert np.isnan(res.energy_trace["energy"][-1]) and res.energy_trace["step"][-1] == 108
