@@ -1241,6 +1241,9 @@ void run_steps(Handle& H, long long nsteps) {
     sync_dead_units(H);
     int per = 0;
     if (!H.graphs_valid) {
+        // a capture that failed part-way left the graphs it had finished:
+        // free them before capturing again
+        invalidate_graphs(H);
         // graphs for each starting buffer set (one set for in-place kernels)
         const int nsets = H.stencil_mode == kModeFused ? 2 : 1;
         const int cur0 = H.cur;
