@@ -206,6 +206,9 @@ class FitbError(RuntimeError):
         self.code = code
 
 
+# FITB_ABI_VERSION of include/fitb200.h that the signatures above follow
+ABI_VERSION = 1
+
 _lib: C.CDLL | None = None
 
 
@@ -225,6 +228,13 @@ def load() -> C.CDLL:
         fn = getattr(lib, name)
         fn.argtypes = args
         fn.restype = res
+    built = lib.fitb_abi_version()
+    if built != ABI_VERSION:
+        raise FitbError(
+            -3,
+            f"{LIB_PATH.name} was built for ABI version {built}, these bindings are for "
+            f"{ABI_VERSION}; rebuild with magnelio_b200._build.build()",
+        )
     _lib = lib
     return lib
 

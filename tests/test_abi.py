@@ -79,3 +79,11 @@ def test_sparse_eigensolve_checks_its_arguments_before_touching_a_device():
     rc = lib.fitb_sparse_eigs(0, 2, _lib.i64p(rp), _lib.i64p(col), _lib.f64p(val), 0, None, 1, 1e-14,
                               _lib.f64p(out), _lib.f64p(vec), None, None)
     assert rc != 0 and "column index" in _lib.last_error()
+
+
+def test_bindings_follow_the_header_abi_version():
+    from magnelio_b200 import _lib
+
+    hdr = (ROOT / "include" / "fitb200.h").read_text()
+    assert int(re.search(r"#define FITB_ABI_VERSION (\d+)", hdr).group(1)) == _lib.ABI_VERSION
+    assert _lib.load().fitb_abi_version() == _lib.ABI_VERSION
